@@ -1,0 +1,306 @@
+"""Problem descriptions for the FDTD hot path.
+
+A ``Problem`` is a plain description of one grid and what acts on it during a
+time step: CPML widths, the material table and per-cell (or per-block) ids,
+soft sources, TFSF planes and DFT capture regions. The same description
+drives the GPU library (``fdtd_b200.grid.Grid.from_problem``) and the CPU
+checkers under ``oracle/`` in the tests, so both see identical inputs.
+
+Units are SI as in the reference (include/FDTDConstants.hpp:394-398). The
+configs below are written in "grid units" (one cell = dx, one step = dt) and
+converted here: frequencies in cycles/step become rad/s via 2*pi*f/dt for the
+DFT only; material rates given "in grid units" (w*dt) become w = value/dt.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+# include/FDTDConstants.hpp:394-398
+PI = 3.14159265358979323846264338327950288
+EPS0 = 8.854e-12
+MU0 = PI * 4.0e-7
+C0 = 2.99792458e8
+
+# Detail::EMMode order (include/FDTDConstants.hpp:410-415)
+TEM, TE, TM, THREED = 0, 1, 2, 3
+MODE_NAMES = {"TEM": TEM, "TE": TE, "TM": TM, "ThreeD": THREED, "3D": THREED}
+
+VACUUM, CONSTANT, DRUDE, LORENTZ = 0, 1, 2, 3
+MAX_POLES = 4
+
+
+def ref_sqrt(x: float) -> float:
+    """The reference's constexpr Newton sqrt (include/FDTDConstants.hpp:136-156)."""
+    curr, prev = x, 0.0
+    while curr != prev:
+        curr, prev = 0.5 * (curr + x / curr), curr
+    return curr
+
+
+IMP0 = ref_sqrt(MU0 / EPS0)
+
+
+@dataclass
+class Material:
+    """One row of the material table.
+
+    kind: VACUUM / CONSTANT (eps_inf) / DRUDE (one pole: plasma freq, gamma) /
+    LORENTZ (poles of (delta_eps, resonance freq, gamma)). Frequencies in
+    rad/s and gamma in 1/s as the reference's storages take them
+    (include/DispersiveMaterials.hpp:778-789, :1078-1088). The reference's
+    Lorentz ignores its Delta argument, i.e. delta_eps = 1 reproduces it.
+    """
+
+    kind: int = VACUUM
+    eps_inf: float = 1.0
+    mu_r: float = 1.0
+    poles: List[Tuple[float, float, float]] = field(default_factory=list)
+
+    @staticmethod
+    def vacuum() -> "Material":
+        return Material(VACUUM, 1.0, 1.0, [])
+
+    @staticmethod
+    def constant(eps_r: float, mu_r: float = 1.0) -> "Material":
+        return Material(CONSTANT, eps_r, mu_r, [])
+
+    @staticmethod
+    def drude(eps_inf: float, wp: float, gamma: float) -> "Material":
+        return Material(DRUDE, eps_inf, 1.0, [(1.0, wp, gamma)])
+
+    @staticmethod
+    def lorentz(eps_inf: float, poles: Sequence[Tuple[float, float, float]]) -> "Material":
+        return Material(LORENTZ, eps_inf, 1.0, [tuple(p) for p in poles])
+
+
+@dataclass
+class Source:
+    """Soft source (include/Source.hpp:183-261): values[t] added at step t to
+    component ``comp`` (0..2) of E (target 'E', after the constitutive update)
+    or of D (target 'D', before the CPML pass)."""
+
+    comp: int
+    pos: Tuple[int, int, int]
+    values: np.ndarray
+    target: str = "E"
+
+
+@dataclass
+class TFSFPlaneSpec:
+    axis: int
+    orient: int  # 0 = MIN (normal -axis), 1 = MAX (normal +axis)
+    lo: Tuple[int, int, int]
+    hi: Tuple[int, int, int]
+
+
+@dataclass
+class TFSF:
+    """Plane-wave injection: TFSF planes (include/Source.hpp:472-634), each
+    with its own Aux1D grid of ``aux_ncells`` (+50) cells whose source at aux
+    step s is aux_values[s-1]. ``origin`` (cells) is where the location
+    functor puts 0; cell (i,j,k) sits at ((i,j,k) - origin) * dx."""
+
+    aux_ncells: int
+    aux_values: np.ndarray
+    origin: Tuple[float, float, float]
+    k: Tuple[float, float, float]
+    pol_e: Tuple[float, float, float]
+    pol_h: Tuple[float, float, float]
+    planes: List[TFSFPlaneSpec] = field(default_factory=list)
+
+
+@dataclass
+class DFTRegion:
+    """Running DFT of component comp (0..2 E, 3..5 H) over the inclusive box
+    lo..hi at frequencies freqs (cycles/step). E sampled at the end of the E
+    half of step t carries time index t+1, H at the end of the H half t+1.5;
+    X_f = sum_n x[n] * exp(-2*pi*i*f*n)."""
+
+    comp: int
+    lo: Tuple[int, int, int]
+    hi: Tuple[int, int, int]
+    freqs: Sequence[float]
+
+
+@dataclass
+class Problem:
+    mode: int
+    shape: Tuple[int, int, int]  # (nx, ny, nz); nz = 1 for 2D
+    dx: float
+    dt: float
+    pml: dict = field(default_factory=dict)  # {(axis, side): ncells}
+    materials: List[Material] = field(default_factory=lambda: [Material.vacuum()])
+    ids: Optional[np.ndarray] = None  # uint8, shape (nz, ny, nx)
+    block_ids: Optional[np.ndarray] = None  # uint16, shape (nbz, nby, nbx)
+    block_shift: int = 0
+    sources: List[Source] = field(default_factory=list)
+    tfsf: Optional[TFSF] = None
+    dfts: List[DFTRegion] = field(default_factory=list)
+    steps: int = 0
+    name: str = ""
+
+    @property
+    def dim(self) -> int:
+        return 3 if self.mode == THREED else (1 if self.mode == TEM else 2)
+
+    @property
+    def ncell(self) -> int:
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    @property
+    def interior_cells(self) -> int:
+        nx, ny, nz = self.shape
+        n = (nx - 2) * (ny - 2)
+        return n * (nz - 2) if self.mode == THREED else n
+
+    def cell_ids(self) -> Optional[np.ndarray]:
+        """Per-cell material ids (expanding a block map if one is set)."""
+        if self.ids is not None:
+            return self.ids
+        if self.block_ids is None:
+            return None
+        nx, ny, nz = self.shape
+        s = self.block_shift
+        k = np.arange(nz)[:, None, None] >> s
+        j = np.arange(ny)[None, :, None] >> s
+        i = np.arange(nx)[None, None, :] >> s
+        return self.block_ids[k, j, i]
+
+
+def courant_dt(dx: float, courant: float) -> float:
+    return courant * dx / C0
+
+
+def gaussian_pulse(nsteps: int, t0: float = 60.0, spread: float = 20.0, offset: float = 0.0) -> np.ndarray:
+    """g(n) = exp(-((n + offset - t0)/spread)^2) for n = 0..nsteps-1."""
+    n = np.arange(nsteps, dtype=np.float64) + offset
+    return np.exp(-(((n - t0) / spread) ** 2))
+
+
+def ref_tm_polarisation(k):
+    """Default TM polarisation of TFSFPlane (include/Source.hpp:577-579)."""
+    return (0.0, 0.0, 1.0), (k[1], -k[0], 0.0)
+
+
+def ref_te_polarisation(k):
+    """Default TE polarisation of TFSFPlane (include/Source.hpp:573-576)."""
+    return (k[1], -k[0], 0.0), (0.0, 0.0, 1.0)
+
+
+def tfsf_box_planes(mode: int, lo: Sequence[int], hi: Sequence[int]) -> List[TFSFPlaneSpec]:
+    """TFSF planes around the total-field box whose E cells are lo..hi.
+
+    The MIN face of an axis is the plane of cells just outside the box
+    (index lo-1) and the MAX face is the box's last plane (index hi), with the
+    tangential extent of the box. With the reference's per-cell correction
+    (include/Source.hpp:506-531) this is the placement where the D correction
+    of a face and the B correction of the same face use the incident field at
+    the staggered positions the curl actually reads.
+    """
+    dim = 3 if mode == THREED else 2
+    planes = []
+    for a in range(dim):
+        for orient in (0, 1):
+            plo = list(lo) + [0] * (3 - len(lo))
+            phi = list(hi) + [0] * (3 - len(hi))
+            idx = lo[a] - 1 if orient == 0 else hi[a]
+            plo[a] = idx
+            phi[a] = idx
+            planes.append(TFSFPlaneSpec(a, orient, tuple(plo), tuple(phi)))
+    return planes
+
+
+# ---------------------------------------------------------------- configs
+
+def config1(n: int = 256, steps: int = 2000, npml: int = 16) -> Problem:
+    """2D TM FP64 vacuum, 16-cell CPML, soft Ez Gaussian at the centre, DFT of
+    Ez along the centre row at 0.02/0.04/0.06 cycles/step."""
+    dx = 1e-6
+    dt = courant_dt(dx, 0.99 / math.sqrt(2.0))
+    p = Problem(TM, (n, n, 1), dx, dt, name=f"tm{n}_vacuum_cpml{npml}")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = npml
+    c = n // 2
+    p.sources.append(Source(2, (c, c, 0), gaussian_pulse(steps), "E"))
+    p.dfts.append(DFTRegion(2, (0, c, 0), (n - 1, c, 0), [0.02, 0.04, 0.06]))
+    p.steps = steps
+    return p
+
+
+def config2(n: int = 384, steps: int = 1000, npml: int = 12, radius: Optional[int] = None,
+            tfsf_inset: Optional[int] = None, dft_inset: Optional[int] = None, nfreq: int = 8) -> Problem:
+    """3D, 12-cell CPML, Drude sphere (eps_inf 1, wp*dt 0.3, gamma*dt 0.01) of
+    radius 64 at the centre, TFSF box inset 24 with an x-propagating
+    z-polarised Gaussian plane wave, DFT at 8 frequencies of the 4 tangential
+    components on the 6 faces of the box inset 20. Smaller n scales radius
+    and insets by n/384."""
+    scale = n / 384.0
+    radius = radius if radius is not None else max(2, int(round(64 * scale)))
+    tfsf_inset = tfsf_inset if tfsf_inset is not None else max(npml + 3, int(round(24 * scale)))
+    dft_inset = dft_inset if dft_inset is not None else max(npml + 2, tfsf_inset - max(1, int(round(4 * scale))))
+    dx = 1e-6
+    dt = courant_dt(dx, 0.99 / math.sqrt(3.0))
+    p = Problem(THREED, (n, n, n), dx, dt, name=f"3d{n}_drude_sphere_tfsf_dft")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = npml
+    p.materials = [Material.vacuum(), Material.drude(1.0, 0.3 / dt, 0.01 / dt)]
+    c = n // 2
+    ax = np.arange(n) - c
+    r2 = ax[:, None, None] ** 2 + ax[None, :, None] ** 2 + ax[None, None, :] ** 2
+    p.ids = (r2 <= radius * radius).astype(np.uint8)
+    lo = (tfsf_inset,) * 3
+    hi = (n - 1 - tfsf_inset,) * 3
+    k = (1.0, 0.0, 0.0)
+    # E along z, H along y: the aux Hy already carries the sign of the
+    # incident Hy, so the H polarisation multiplying it is +y.
+    p.tfsf = TFSF(aux_ncells=n, aux_values=gaussian_pulse(steps, offset=1.0), origin=(c, c, c), k=k,
+                  pol_e=(0.0, 0.0, 1.0), pol_h=(0.0, 1.0, 0.0), planes=tfsf_box_planes(THREED, lo, hi))
+    freqs = [0.01 * (q + 1) for q in range(nfreq)]
+    a0, a1 = dft_inset, n - 1 - dft_inset
+    for a in range(3):
+        for side in (0, 1):
+            plo = [a0, a0, a0]
+            phi = [a1, a1, a1]
+            plo[a] = phi[a] = a0 if side == 0 else a1
+            tang = [b for b in range(3) if b != a]
+            for b in tang:
+                p.dfts.append(DFTRegion(b, tuple(plo), tuple(phi), freqs))
+                p.dfts.append(DFTRegion(3 + b, tuple(plo), tuple(phi), freqs))
+    p.steps = steps
+    return p
+
+
+def config5(n: int = 768, steps: int = 500, npml: int = 16, block: int = 32, seed: int = 0,
+            nfreq: int = 4) -> Problem:
+    """3D, 16-cell CPML, two-pole Lorentz everywhere (delta_eps 1.5, w0*dt
+    0.1, delta*dt 0.005 and 0.8, 0.25, 0.02), eps_inf per 32^3 block uniform
+    in [1,6] from `seed`, soft Ez dipole at the centre, DFT of Ez at 4
+    frequencies on the central z plane."""
+    dx = 1e-6
+    dt = courant_dt(dx, 0.99 / math.sqrt(3.0))
+    p = Problem(THREED, (n, n, n), dx, dt, name=f"3d{n}_lorentz2_blocks{block}")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = npml
+    shift = int(round(math.log2(block)))
+    assert 1 << shift == block
+    nb = (n + block - 1) // block
+    rng = np.random.default_rng(seed)
+    eps = rng.uniform(1.0, 6.0, size=nb ** 3)
+    poles = [(1.5, 0.1 / dt, 0.005 / dt), (0.8, 0.25 / dt, 0.02 / dt)]
+    p.materials = [Material.lorentz(float(e), poles) for e in eps]
+    p.block_ids = np.arange(nb ** 3, dtype=np.uint16).reshape(nb, nb, nb)
+    p.block_shift = shift
+    c = n // 2
+    p.sources.append(Source(2, (c, c, c), gaussian_pulse(steps), "E"))
+    freqs = [0.01 * (q + 1) for q in range(nfreq)]
+    p.dfts.append(DFTRegion(2, (0, 0, c), (n - 1, n - 1, c), freqs))
+    p.steps = steps
+    return p

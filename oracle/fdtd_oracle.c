@@ -1,0 +1,625 @@
+/* CPU oracle: plain-C restatement of pederson/fdtd's time-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker for tests/, smoke() and bench.py's
+ * CPU baseline); never part of the product.
+ *
+ * Every update below follows the reference functor it names, in the same
+ * floating-point operation order, so that with -ffp-contract=off it matches
+ * the reference compiled the same way bit for bit (pinned by
+ * tests/test_oracle_cpu.py against oracle/_ref/ref_runner and the fixtures in
+ * tests/golden/).
+ *
+ * Schedule of one step (the user loop of tests/testTM.cpp:102-113 and
+ * include/Source.hpp:413-435, with TFSF and sources placed as documented in
+ * DESIGN.md):
+ *   E half: YeeUpdate on every E flux, TFSF updateD, D-target sources,
+ *           UpdatePML<Electric, X|Y|Z>, material update, E-target sources,
+ *           DFT of E.
+ *   H half: YeeUpdate on every B flux, TFSF updateB,
+ *           UpdatePML<Magnetic, X|Y|Z>, material update, DFT of H.
+ * Only interior cells (1..n-2 along each active axis) are updated; the outer
+ * ring keeps its initial zeros, as in tests/testTM.cpp:33-40,103. */
+#include "fdtd_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* include/FDTDConstants.hpp:394-398 */
+static const double k_pi = 3.14159265358979323846264338327950288;
+static const double k_eps0 = 8.854e-12;
+#define K_MU0 (k_pi * 4.0e-7)
+
+/* include/FDTDConstants.hpp:136-156: the reference's constexpr Newton sqrt,
+ * reproduced because imp0 = sqrt(mu0/eps0) is evaluated with it. */
+static double ref_sqrt(double x) {
+  double curr = x, prev = 0.0;
+  while (curr != prev) {
+    double next = 0.5 * (curr + x / curr);
+    prev = curr;
+    curr = next;
+  }
+  return curr;
+}
+double oracle_imp0(void) { return ref_sqrt(K_MU0 / k_eps0); }
+
+enum { TEM = 0, TE = 1, TM = 2, THREED = 3 };
+
+typedef struct {
+  int axis, orient, lo[3], hi[3];
+  double origin[3], k[3], pol_e[3], pol_h[3], normal[3];
+  /* Aux1D state: TEM grid with Dz, Ez, By, Hy and CPML */
+  int L;
+  double *Dz, *Ez, *By, *Hy, *psiE, *psiH;
+  double *pB[2], *pC[2], *pF[2], *pG[2];
+  double t;
+  double* vals;
+  int nvals;
+} plane_t;
+
+typedef struct {
+  int comp, lo[3], hi[3], nf, npts;
+  double* freqs;
+  double* acc; /* [nf][npts][2] */
+} dft_t;
+
+typedef struct {
+  int comp, target, i, j, k, nvals;
+  double* vals;
+} src_t;
+
+struct oracle_grid {
+  int mode, n[3];
+  size_t ncell;
+  double dx, dt;
+  int hasE[3], hasH[3];
+  double *D[3], *E[3], *B[3], *H[3];
+  double *P[OR_MAX_POLES][3], *J[OR_MAX_POLES][3];
+  double* psi[2][3][3];
+  /* 1D CPML coefficients per (field type, axis): B, C, F, G */
+  double* cB[2][3];
+  double* cC[2][3];
+  double* cF[2][3];
+  double* cG[2][3];
+  int pml[3][2];
+  oracle_material mats[256];
+  int nmat;
+  uint8_t* ids;
+  src_t* srcs;
+  int nsrc;
+  plane_t* planes;
+  int nplanes;
+  dft_t* dfts;
+  int ndft;
+  long t; /* steps taken */
+};
+
+static int lc(int I, int J, int K) {
+  if ((I == 0 && J == 1 && K == 2) || (I == 1 && J == 2 && K == 0) || (I == 2 && J == 0 && K == 1)) return 1;
+  if ((I == 2 && J == 1 && K == 0) || (I == 0 && J == 2 && K == 1) || (I == 1 && J == 0 && K == 2)) return -1;
+  return 0;
+}
+static int third(int I, int J) { return 3 - I - J; }
+
+/* PMLParameterModel(dx) (include/PML.hpp:368-393) */
+typedef struct { double m, ma, smax, kmax, amax; } pml_model;
+static pml_model model_for(double dx) {
+  pml_model p;
+  p.m = 3; p.ma = 1;
+  p.smax = 0.8 * (p.m + 1) / (oracle_imp0() * dx);
+  p.kmax = 5; p.amax = 0.05;
+  return p;
+}
+static double mK(const pml_model* p, double x) { if (x < 0.0) return 1.0; return x > 1.0 ? 1.0 : 1.0 + pow(x, p->m) * (p->kmax - 1.0); }
+static double mS(const pml_model* p, double x) { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(x, p->m) * p->smax; }
+static double mA(const pml_model* p, double x) { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(1.0 - x, p->ma) * p->amax; }
+
+/* NewPML::setPMLParameters (include/PML.hpp:84-102) */
+static void set_params(double K, double S, double A, double dt, double* B, double* C, double* F, double* G) {
+  double nu = 1.0 / k_eps0 * (S / K + A);
+  *B = exp(-dt * nu);
+  *C = (nu == 0) ? 0.0 : S / K * 1.0 / (S + K * A) * (*B - 1.0);
+  double u = -S / (k_eps0 * K * K);
+  *F = (nu == 0) ? 1.0 / K : 1.0 / K - 1.0 / dt * (1.0 - *B - nu * dt) * u / (nu * nu);
+  *G = (nu == 0) ? 0.0 : 1.0 / dt * (1.0 - *B) / nu;
+}
+
+/* grading loop of tests/testTM.cpp:44-71 for one side of one axis */
+static void grade(double dx, double dt, int n, int np, int side, double* B[2], double* C[2], double* F[2], double* G[2]) {
+  pml_model p = model_for(dx);
+  for (int i = 1; i < np + 2; i++) {
+    double x = (double)(np - i + 1) / (double)np;
+    double xm = x - 0.5 / (double)np;
+    int ce = side == 0 ? i : n - i;
+    int cm = side == 0 ? i : n - 1 - i;
+    if (ce >= 0 && ce < n) set_params(mK(&p, x), mS(&p, x), mA(&p, x), dt, &B[0][ce], &C[0][ce], &F[0][ce], &G[0][ce]);
+    if (cm >= 0 && cm < n) set_params(mK(&p, xm), mS(&p, xm), mA(&p, xm), dt, &B[1][cm], &C[1][cm], &F[1][cm], &G[1][cm]);
+  }
+}
+
+static double* zalloc(size_t n) { return (double*)calloc(n ? n : 1, sizeof(double)); }
+
+oracle_grid* oracle_create(int mode, int nx, int ny, int nz, double dx, double dt) {
+  if (mode != TE && mode != TM && mode != THREED) return NULL;
+  if (nx < 3 || ny < 3 || nz < 1 || (mode == THREED && nz < 3) || (mode != THREED && nz != 1)) return NULL;
+  oracle_grid* g = (oracle_grid*)calloc(1, sizeof(oracle_grid));
+  g->mode = mode; g->n[0] = nx; g->n[1] = ny; g->n[2] = nz;
+  g->ncell = (size_t)nx * ny * nz;
+  g->dx = dx; g->dt = dt;
+  for (int c = 0; c < 3; c++) {
+    g->hasE[c] = mode == THREED || (mode == TE && c < 2) || (mode == TM && c == 2);
+    g->hasH[c] = mode == THREED || (mode == TE && c == 2) || (mode == TM && c < 2);
+    g->D[c] = zalloc(g->ncell); g->E[c] = zalloc(g->ncell);
+    g->B[c] = zalloc(g->ncell); g->H[c] = zalloc(g->ncell);
+    for (int q = 0; q < OR_MAX_POLES; q++) { g->P[q][c] = zalloc(g->ncell); g->J[q][c] = zalloc(g->ncell); }
+  }
+  for (int f = 0; f < 2; f++)
+    for (int I = 0; I < 3; I++)
+      for (int J = 0; J < 3; J++) g->psi[f][I][J] = zalloc(g->ncell);
+  for (int f = 0; f < 2; f++)
+    for (int a = 0; a < 3; a++) {
+      int n = g->n[a];
+      g->cB[f][a] = zalloc(n); g->cC[f][a] = zalloc(n); g->cF[f][a] = zalloc(n); g->cG[f][a] = zalloc(n);
+      for (int i = 0; i < n; i++) g->cF[f][a][i] = 1.0; /* NewPML defaults (PML.hpp:40-55) */
+    }
+  g->nmat = 1;
+  memset(&g->mats[0], 0, sizeof(oracle_material));
+  g->mats[0].kind = OR_VACUUM; g->mats[0].eps_inf = 1.0; g->mats[0].mu_r = 1.0;
+  return g;
+}
+
+void oracle_destroy(oracle_grid* g) {
+  if (!g) return;
+  for (int c = 0; c < 3; c++) {
+    free(g->D[c]); free(g->E[c]); free(g->B[c]); free(g->H[c]);
+    for (int q = 0; q < OR_MAX_POLES; q++) { free(g->P[q][c]); free(g->J[q][c]); }
+  }
+  for (int f = 0; f < 2; f++) {
+    for (int I = 0; I < 3; I++) for (int J = 0; J < 3; J++) free(g->psi[f][I][J]);
+    for (int a = 0; a < 3; a++) { free(g->cB[f][a]); free(g->cC[f][a]); free(g->cF[f][a]); free(g->cG[f][a]); }
+  }
+  free(g->ids);
+  for (int s = 0; s < g->nsrc; s++) free(g->srcs[s].vals);
+  free(g->srcs);
+  for (int p = 0; p < g->nplanes; p++) {
+    plane_t* pl = &g->planes[p];
+    free(pl->Dz); free(pl->Ez); free(pl->By); free(pl->Hy); free(pl->psiE); free(pl->psiH); free(pl->vals);
+    for (int f = 0; f < 2; f++) { free(pl->pB[f]); free(pl->pC[f]); free(pl->pF[f]); free(pl->pG[f]); }
+  }
+  free(g->planes);
+  for (int d = 0; d < g->ndft; d++) { free(g->dfts[d].freqs); free(g->dfts[d].acc); }
+  free(g->dfts);
+  free(g);
+}
+
+int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells) {
+  int dim = g->mode == THREED ? 3 : 2;
+  if (axis < 0 || axis >= dim || side < 0 || side > 1 || ncells < 1) return -1;
+  g->pml[axis][side] = ncells;
+  double* B[2] = {g->cB[0][axis], g->cB[1][axis]};
+  double* C[2] = {g->cC[0][axis], g->cC[1][axis]};
+  double* F[2] = {g->cF[0][axis], g->cF[1][axis]};
+  double* G[2] = {g->cG[0][axis], g->cG[1][axis]};
+  grade(g->dx, g->dt, g->n[axis], ncells, side, B, C, F, G);
+  return 0;
+}
+
+int oracle_pml_profile(const oracle_grid* g, int ft, int axis, double* out) {
+  if (ft < 0 || ft > 1 || axis < 0 || axis > 2) return -1;
+  int n = g->n[axis];
+  memcpy(out, g->cB[ft][axis], n * sizeof(double));
+  memcpy(out + n, g->cC[ft][axis], n * sizeof(double));
+  memcpy(out + 2 * n, g->cF[ft][axis], n * sizeof(double));
+  memcpy(out + 3 * n, g->cG[ft][axis], n * sizeof(double));
+  return 0;
+}
+
+int oracle_set_materials(oracle_grid* g, const oracle_material* m, int n) {
+  if (n < 1 || n > 256) return -1;
+  for (int q = 0; q < n; q++)
+    if (m[q].npoles < 0 || m[q].npoles > OR_MAX_POLES) return -1;
+  memcpy(g->mats, m, n * sizeof(oracle_material));
+  g->nmat = n;
+  return 0;
+}
+
+int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids) {
+  if (!g->ids) g->ids = (uint8_t*)malloc(g->ncell);
+  memcpy(g->ids, ids, g->ncell);
+  return 0;
+}
+
+int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {
+  if (comp < 0 || comp > 2 || target < 0 || target > 1) return -1;
+  if (i < 0 || i >= g->n[0] || j < 0 || j >= g->n[1] || k < 0 || k >= g->n[2]) return -1;
+  g->srcs = (src_t*)realloc(g->srcs, (g->nsrc + 1) * sizeof(src_t));
+  src_t* s = &g->srcs[g->nsrc++];
+  s->comp = comp; s->target = target; s->i = i; s->j = j; s->k = k; s->nvals = nvals;
+  s->vals = zalloc(nvals);
+  memcpy(s->vals, vals, nvals * sizeof(double));
+  return 0;
+}
+
+/* Aux1D (include/Source.hpp:280-462): TEM grid of ncells + 2*15 + 20 cells,
+ * fixed 15-cell CPML graded like the main grid, source at cell 20. */
+#define AUX_NPML 15
+int oracle_add_tfsf_plane(oracle_grid* g, int axis, int orient, const int* lo, const int* hi,
+                          const double* origin, const double* kvec, const double* pol_e,
+                          const double* pol_h, int aux_ncells, const double* aux_vals, int naux) {
+  int dim = g->mode == THREED ? 3 : 2;
+  if (axis < 0 || axis >= dim || aux_ncells < 1) return -1;
+  g->planes = (plane_t*)realloc(g->planes, (g->nplanes + 1) * sizeof(plane_t));
+  plane_t* p = &g->planes[g->nplanes++];
+  memset(p, 0, sizeof(*p));
+  p->axis = axis; p->orient = orient;
+  for (int d = 0; d < 3; d++) {
+    p->lo[d] = lo[d]; p->hi[d] = hi[d]; p->origin[d] = origin[d];
+    p->pol_e[d] = pol_e[d]; p->pol_h[d] = pol_h[d];
+    p->normal[d] = 0;
+  }
+  p->normal[axis] = orient == 1 ? 1 : -1;
+  /* TFSFPlane constructor: normalise normal and k over the mode's dims
+   * (include/Source.hpp:560-570) */
+  double N = 0;
+  for (int d = 0; d < dim; d++) N += p->normal[d] * p->normal[d];
+  N = sqrt(N);
+  for (int d = 0; d < dim; d++) p->normal[d] /= N;
+  double K = 0;
+  for (int d = 0; d < dim; d++) K += kvec[d] * kvec[d];
+  K = sqrt(K);
+  for (int d = 0; d < 3; d++) p->k[d] = d < dim ? kvec[d] / K : 0.0;
+  int L = aux_ncells + 2 * AUX_NPML + 20;
+  p->L = L;
+  p->Dz = zalloc(L); p->Ez = zalloc(L); p->By = zalloc(L); p->Hy = zalloc(L);
+  p->psiE = zalloc(L); p->psiH = zalloc(L);
+  for (int f = 0; f < 2; f++) {
+    p->pB[f] = zalloc(L); p->pC[f] = zalloc(L); p->pF[f] = zalloc(L); p->pG[f] = zalloc(L);
+    for (int i = 0; i < L; i++) p->pF[f][i] = 1.0;
+  }
+  /* Aux1D::setup_tasks (Source.hpp:380-389): both sides in one loop */
+  pml_model pm = model_for(g->dx);
+  for (int i = 1; i < AUX_NPML + 2; i++) {
+    double x = (double)(AUX_NPML - i + 1) / (double)AUX_NPML;
+    double xm = x - 0.5 / (double)AUX_NPML;
+    set_params(mK(&pm, x), mS(&pm, x), mA(&pm, x), g->dt, &p->pB[0][i], &p->pC[0][i], &p->pF[0][i], &p->pG[0][i]);
+    set_params(mK(&pm, xm), mS(&pm, xm), mA(&pm, xm), g->dt, &p->pB[1][i], &p->pC[1][i], &p->pF[1][i], &p->pG[1][i]);
+    set_params(mK(&pm, x), mS(&pm, x), mA(&pm, x), g->dt, &p->pB[0][L - i], &p->pC[0][L - i], &p->pF[0][L - i], &p->pG[0][L - i]);
+    set_params(mK(&pm, xm), mS(&pm, xm), mA(&pm, xm), g->dt, &p->pB[1][L - 1 - i], &p->pC[1][L - 1 - i], &p->pF[1][L - 1 - i], &p->pG[1][L - 1 - i]);
+  }
+  p->vals = zalloc(naux);
+  memcpy(p->vals, aux_vals, naux * sizeof(double));
+  p->nvals = naux;
+  p->t = 0;
+  return 0;
+}
+
+/* Aux1D::time_step (Source.hpp:413-435). Cells 0 and L-1 see zero ghosts. */
+static void aux_step(plane_t* p, double dt, double dx) {
+  int L = p->L;
+  p->t += dt;
+  /* the source value is looked up by aux step number, s = round(t/dt) */
+  long s = lround(p->t / dt);
+  /* YeeUpdate<TEM,Dz>: Dz + dt*(a<X> + 0.0) */
+  for (int i = 0; i < L; i++) {
+    double hm = i > 0 ? p->Hy[i - 1] : 0.0;
+    double a = 1 * p->pF[0][i] / dx * (p->Hy[i] - hm);
+    p->Dz[i] = p->Dz[i] + 1.0 * 1.0 * dt * (a + 0.0);
+  }
+  /* UpdatePML<TEM, Electric, X> */
+  for (int i = 0; i < L; i++) {
+    double hm = i > 0 ? p->Hy[i - 1] : 0.0;
+    p->Dz[i] += 1.0 * dt * p->psiE[i] * p->pG[0][i];
+    p->psiE[i] = p->pB[0][i] * p->psiE[i] + p->pC[0][i] * 1 / dx * (p->Hy[i] - hm);
+  }
+  for (int i = 0; i < L; i++) p->Ez[i] = p->Dz[i] / (1.0 * k_eps0);
+  p->Ez[AUX_NPML + 5] += (s >= 1 && s <= p->nvals) ? p->vals[s - 1] : 0.0;
+  /* YeeUpdate<TEM,By>: By + (-dt)*(0.0 + a<X>), a<X> = -F/dx*(Ez[+1]-Ez) */
+  for (int i = 0; i < L; i++) {
+    double ep = i < L - 1 ? p->Ez[i + 1] : 0.0;
+    double a = -1 * p->pF[1][i] / dx * (ep - p->Ez[i]);
+    p->By[i] = p->By[i] + -1.0 * 1.0 * dt * (0.0 + a);
+  }
+  /* UpdatePML<TEM, Magnetic, X> */
+  for (int i = 0; i < L; i++) {
+    double ep = i < L - 1 ? p->Ez[i + 1] : 0.0;
+    p->By[i] += -1.0 * dt * p->psiH[i] * p->pG[1][i];
+    p->psiH[i] = p->pB[1][i] * p->psiH[i] + p->pC[1][i] * -1 / dx * (ep - p->Ez[i]);
+  }
+  for (int i = 0; i < L; i++) p->Hy[i] = p->By[i] / (1.0 * K_MU0);
+}
+
+/* Aux1D::interpolateE / interpolateH (Source.hpp:442-458) */
+static double interp(const double* f, int L, double loc, double dx, double shift) {
+  double nd = (double)L / 2.0 + loc / dx - shift;
+  size_t n = (size_t)nd;
+  double frac = (nd - n);
+  (void)L;
+  return (1.0 - frac) * f[n] + frac * f[n + 1];
+}
+
+/* Yee staggering offsets, include/FDTDConstants.hpp:680-744 */
+static const double offE[3][3] = {{0.0, -0.5, -0.5}, {-0.5, 0.0, -0.5}, {-0.5, -0.5, 0.0}};
+static const double offH[3][3] = {{-0.5, 0.0, 0.0}, {0.0, -0.5, 0.0}, {0.0, 0.0, -0.5}};
+
+/* TFSFPlane::field_update (Source.hpp:489-554), applied to one flux component
+ * I of type ft (0 = D, 1 = B) at cell (i,j,k). */
+static void tfsf_cell(oracle_grid* g, plane_t* p, int ft, int I, int i, int j, int k) {
+  int dim = g->mode == THREED ? 3 : 2;
+  int idx3[3] = {i, j, k};
+  size_t c = ((size_t)k * g->n[1] + j) * g->n[0] + i;
+  int d1 = I == 0 ? 1 : (I == 1 ? 2 : 0);
+  int d2 = third(I, d1);
+  int ds[2] = {d1, d2};
+  double terms[2];
+  for (int q = 0; q < 2; q++) {
+    int J = ds[q], K = third(I, J);
+    int present = ft == 0 ? g->hasH[K] : g->hasE[K];
+    if (!present) { terms[q] = 0.0; continue; }
+    const double* off = ft == 0 ? offH[K] : offE[K];
+    double center[3], src[3];
+    for (int d = 0; d < dim; d++) center[d] = ((double)idx3[d] - p->origin[d]) * g->dx;
+    for (int d = 0; d < dim; d++) src[d] = center[d] + off[d] * g->dx;
+    double proj = 0;
+    for (int d = 0; d < dim; d++) proj += p->k[d] * src[d];
+    double sv = ft == 0 ? interp(p->Hy, p->L, proj, g->dx, 0.5) : interp(p->Ez, p->L, proj, g->dx, 0.0);
+    double Fj = g->cF[ft][J][idx3[J]];
+    const double* pol = ft == 0 ? p->pol_h : p->pol_e;
+    terms[q] = lc(I, J, K) * Fj / (g->dx) * p->normal[J] * sv * pol[K];
+  }
+  double coeff = ft == 0 ? 1.0 : -1.0;
+  double* F = ft == 0 ? g->D[I] : g->B[I];
+  F[c] += coeff * 1.0 * g->dt * (terms[0] + terms[1]);
+}
+
+static void tfsf_apply(oracle_grid* g, int ft) {
+  for (int q = 0; q < g->nplanes; q++) {
+    plane_t* p = &g->planes[q];
+    for (int k = p->lo[2]; k <= p->hi[2]; k++)
+      for (int j = p->lo[1]; j <= p->hi[1]; j++)
+        for (int i = p->lo[0]; i <= p->hi[0]; i++)
+          for (int I = 2; I >= 0; I--) {
+            int present = ft == 0 ? g->hasE[I] : g->hasH[I];
+            if (present) tfsf_cell(g, p, ft, I, i, j, k);
+          }
+    if (ft == 0) aux_step(p, g->dt, g->dx); /* updateD advances the aux grid */
+  }
+}
+
+static void dft_apply(oracle_grid* g, int ft, double n) {
+  for (int d = 0; d < g->ndft; d++) {
+    dft_t* r = &g->dfts[d];
+    if ((r->comp < 3) != (ft == 0)) continue;
+    const double* x = r->comp < 3 ? g->E[r->comp] : g->H[r->comp - 3];
+    for (int f = 0; f < r->nf; f++) {
+      double ph = 2.0 * k_pi * r->freqs[f] * n;
+      double wr = cos(ph), wi = -sin(ph);
+      int p = 0;
+      for (int k = r->lo[2]; k <= r->hi[2]; k++)
+        for (int j = r->lo[1]; j <= r->hi[1]; j++)
+          for (int i = r->lo[0]; i <= r->hi[0]; i++, p++) {
+            double v = x[((size_t)k * g->n[1] + j) * g->n[0] + i];
+            r->acc[((size_t)f * r->npts + p) * 2] += v * wr;
+            r->acc[((size_t)f * r->npts + p) * 2 + 1] += v * wi;
+          }
+    }
+  }
+}
+
+int oracle_add_dft(oracle_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf) {
+  if (comp < 0 || comp > 5 || nf < 1) return -1;
+  for (int d = 0; d < 3; d++)
+    if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return -1;
+  g->dfts = (dft_t*)realloc(g->dfts, (g->ndft + 1) * sizeof(dft_t));
+  dft_t* r = &g->dfts[g->ndft];
+  r->comp = comp; r->nf = nf;
+  r->npts = 1;
+  for (int d = 0; d < 3; d++) { r->lo[d] = lo[d]; r->hi[d] = hi[d]; r->npts *= hi[d] - lo[d] + 1; }
+  r->freqs = zalloc(nf);
+  memcpy(r->freqs, freqs, nf * sizeof(double));
+  r->acc = zalloc((size_t)nf * r->npts * 2);
+  return g->ndft++;
+}
+
+int oracle_dft_npoints(const oracle_grid* g, int handle) {
+  if (handle < 0 || handle >= g->ndft) return -1;
+  return g->dfts[handle].npts;
+}
+
+int oracle_dft_get(const oracle_grid* g, int handle, double* out) {
+  if (handle < 0 || handle >= g->ndft) return -1;
+  const dft_t* r = &g->dfts[handle];
+  memcpy(out, r->acc, (size_t)r->nf * r->npts * 2 * sizeof(double));
+  return 0;
+}
+
+static void step_one(oracle_grid* g) {
+  const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+  const int three = g->mode == THREED;
+  const double dt = g->dt, dx = g->dx;
+  const size_t sx = 1, sy = (size_t)nx, sz = (size_t)nx * ny;
+  const size_t str[3] = {sx, sy, sz};
+  const int k0 = three ? 1 : 0, k1 = three ? nz - 2 : 0;
+  int pmlax[3];
+  for (int a = 0; a < 3; a++) pmlax[a] = g->pml[a][0] > 0 || g->pml[a][1] > 0;
+
+  /* ---------------- E half step ---------------- */
+  for (int k = k0; k <= k1; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = k * sz + j * sy + i;
+        int idx[3] = {i, j, k};
+        /* YeeUpdate::update_all (YeeUpdates.hpp:396-405) on each E flux */
+        for (int I = 0; I < 3; I++) {
+          if (!g->hasE[I]) continue;
+          int d1 = I == 0 ? 1 : (I == 1 ? 2 : 0);
+          int d2 = third(I, d1);
+          int ds[2] = {d1, d2};
+          double a[2];
+          for (int q = 0; q < 2; q++) {
+            int J = ds[q], K = third(I, J);
+            if (!g->hasH[K]) { a[q] = 0.0; continue; }
+            /* atomic_update::get (:373-377); H difference (:107-113) */
+            double diff = g->H[K][c] - g->H[K][c - str[J]];
+            a[q] = lc(I, J, K) * g->cF[0][J][idx[J]] / (dx) * diff;
+          }
+          g->D[I][c] = g->D[I][c] + 1.0 * 1.0 * dt * (a[0] + a[1]);
+        }
+      }
+  tfsf_apply(g, 0);
+  for (int s = 0; s < g->nsrc; s++) {
+    src_t* sr = &g->srcs[s];
+    if (sr->target != 1 || !g->hasE[sr->comp]) continue;
+    size_t c = sr->k * sz + sr->j * sy + sr->i;
+    g->D[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
+  }
+  /* UpdatePML<Mode, Electric, J> (PML.hpp:306-329) per axis, in X, Y, Z order */
+  for (int J = 0; J < 3; J++) {
+    if (!pmlax[J]) continue;
+    for (int k = k0; k <= k1; k++)
+      for (int j = 1; j <= ny - 2; j++)
+        for (int i = 1; i <= nx - 2; i++) {
+          size_t c = k * sz + j * sy + i;
+          int idx[3] = {i, j, k};
+          for (int I = 2; I >= 0; I--) {
+            if (!g->hasE[I] || I == J) continue;
+            int K = third(I, J);
+            double* ps = &g->psi[0][I][J][c];
+            g->D[I][c] += 1.0 * dt * *ps * g->cG[0][J][idx[J]];
+            double diff = g->H[K][c] - g->H[K][c - str[J]];
+            *ps = g->cB[0][J][idx[J]] * *ps + g->cC[0][J][idx[J]] * lc(I, J, K) / dx * diff;
+          }
+        }
+  }
+  /* material update (DispersiveMaterials.hpp:354-359, :710-735, :979-998) */
+  for (int k = k0; k <= k1; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = k * sz + j * sy + i;
+        const oracle_material* m = &g->mats[g->ids ? g->ids[c] : 0];
+        for (int I = 2; I >= 0; I--) {
+          if (!g->hasE[I]) continue;
+          double* D = &g->D[I][c];
+          double* E = &g->E[I][c];
+          if (m->kind == OR_VACUUM) {
+            *E = *D / (1.0 * k_eps0);
+          } else if (m->kind == OR_CONSTANT) {
+            *E = *D / (m->eps_inf * k_eps0);
+          } else if (m->kind == OR_DRUDE) {
+            double* P = &g->P[0][I][c];
+            double* Jc = &g->J[0][I][c];
+            double b = m->gamma[0] * dt * 0.5;
+            double w = dt * m->freq[0];
+            *P += dt * *Jc;
+            *E = (*D - *P) / (m->eps_inf * k_eps0);
+            *Jc = *Jc * (1.0 - b) / (1.0 + b) + w * w / dt * k_eps0 * *E;
+          } else { /* Lorentz, generalised to npoles with strength delta_eps */
+            double num = *D;
+            for (int q = 0; q < m->npoles; q++) {
+              g->P[q][I][c] += dt * g->J[q][I][c];
+              num = num - g->P[q][I][c];
+            }
+            *E = num / (m->eps_inf * k_eps0);
+            for (int q = 0; q < m->npoles; q++) {
+              double b = 1.0 + m->gamma[q] * dt;
+              double bm = 1.0 - m->gamma[q] * dt;
+              double w = m->freq[q] * dt;
+              double qq = m->freq[q] * w / b;
+              double* Jc = &g->J[q][I][c];
+              *Jc = bm / b * *Jc + qq * m->delta_eps[q] * k_eps0 * *E - qq * g->P[q][I][c];
+            }
+          }
+        }
+      }
+  for (int s = 0; s < g->nsrc; s++) {
+    src_t* sr = &g->srcs[s];
+    if (sr->target != 0 || !g->hasE[sr->comp]) continue;
+    size_t c = sr->k * sz + sr->j * sy + sr->i;
+    g->E[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
+  }
+  dft_apply(g, 0, (double)(g->t + 1));
+
+  /* ---------------- H half step ---------------- */
+  for (int k = k0; k <= k1; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = k * sz + j * sy + i;
+        int idx[3] = {i, j, k};
+        for (int I = 0; I < 3; I++) {
+          if (!g->hasH[I]) continue;
+          int d1 = I == 0 ? 1 : (I == 1 ? 2 : 0);
+          int d2 = third(I, d1);
+          int ds[2] = {d1, d2};
+          double a[2];
+          for (int q = 0; q < 2; q++) {
+            int J = ds[q], K = third(I, J);
+            if (!g->hasE[K]) { a[q] = 0.0; continue; }
+            /* E difference (YeeUpdates.hpp:98-103) */
+            double diff = g->E[K][c + str[J]] - g->E[K][c];
+            a[q] = lc(I, J, K) * g->cF[1][J][idx[J]] / (dx) * diff;
+          }
+          g->B[I][c] = g->B[I][c] + -1.0 * 1.0 * dt * (a[0] + a[1]);
+        }
+      }
+  tfsf_apply(g, 1);
+  for (int J = 0; J < 3; J++) {
+    if (!pmlax[J]) continue;
+    for (int k = k0; k <= k1; k++)
+      for (int j = 1; j <= ny - 2; j++)
+        for (int i = 1; i <= nx - 2; i++) {
+          size_t c = k * sz + j * sy + i;
+          int idx[3] = {i, j, k};
+          for (int I = 2; I >= 0; I--) {
+            if (!g->hasH[I] || I == J) continue;
+            int K = third(I, J);
+            double* ps = &g->psi[1][I][J][c];
+            g->B[I][c] += -1.0 * dt * *ps * g->cG[1][J][idx[J]];
+            double diff = g->E[K][c + str[J]] - g->E[K][c];
+            *ps = g->cB[1][J][idx[J]] * *ps + g->cC[1][J][idx[J]] * lc(I, J, K) / dx * diff;
+          }
+        }
+  }
+  for (int k = k0; k <= k1; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = k * sz + j * sy + i;
+        const oracle_material* m = &g->mats[g->ids ? g->ids[c] : 0];
+        for (int I = 2; I >= 0; I--) {
+          if (!g->hasH[I]) continue;
+          g->H[I][c] = g->B[I][c] / (m->mu_r * K_MU0);
+        }
+      }
+  dft_apply(g, 1, (double)g->t + 1.5);
+  g->t++;
+}
+
+int oracle_step(oracle_grid* g, int nsteps) {
+  for (int s = 0; s < nsteps; s++) step_one(g);
+  return 0;
+}
+
+static double* which_ptr(const oracle_grid* g, int which) {
+  if (which < 0) return NULL;
+  if (which < 3) return g->D[which];
+  if (which < 6) return g->E[which - 3];
+  if (which < 9) return g->B[which - 6];
+  if (which < 12) return g->H[which - 9];
+  if (which < 15) return g->P[0][which - 12];
+  if (which < 18) return g->J[0][which - 15];
+  if (which < 36) { int q = which - 18; return g->psi[q / 9][(q / 3) % 3][q % 3]; }
+  int q = which - 36, pole = 1 + q / 6, r = q % 6;
+  if (pole >= OR_MAX_POLES) return NULL;
+  return r < 3 ? g->P[pole][r] : g->J[pole][r - 3];
+}
+
+int oracle_get(const oracle_grid* g, int which, double* out) {
+  double* p = which_ptr(g, which);
+  if (!p) return -1;
+  memcpy(out, p, g->ncell * sizeof(double));
+  return 0;
+}
+
+int oracle_set(oracle_grid* g, int which, const double* in) {
+  double* p = which_ptr(g, which);
+  if (!p) return -1;
+  memcpy(p, in, g->ncell * sizeof(double));
+  return 0;
+}

@@ -1,0 +1,71 @@
+/* CPU oracle for the FDTD time-step hot path: a plain-C restatement of
+ * pederson/fdtd's per-cell update functors, written in the reference's
+ * arithmetic order and compiled without FMA contraction.
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py as the checker. The product library never
+ * links, loads or calls it.
+ *
+ * The API mirrors the GPU C-ABI in include/fdtd_b200.h so one Python driver
+ * can set up both the same way. All units are SI, as in the reference. */
+#ifndef FDTD_ORACLE_H
+#define FDTD_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_grid oracle_grid;
+
+/* material kinds (include/DispersiveMaterials.hpp:2076-2105) */
+enum { OR_VACUUM = 0, OR_CONSTANT = 1, OR_DRUDE = 2, OR_LORENTZ = 3 };
+#define OR_MAX_POLES 4
+
+typedef struct {
+  int kind;
+  int npoles;           /* Drude: 1. Lorentz: 1..OR_MAX_POLES */
+  double eps_inf;       /* the reference's K (relative permittivity) */
+  double mu_r;          /* magnetic ConstantUpdate K; 1 = VacuumUpdate */
+  double delta_eps[OR_MAX_POLES]; /* Lorentz pole strength (reference ignores it: 1) */
+  double freq[OR_MAX_POLES];      /* Drude plasma / Lorentz resonance, rad/s */
+  double gamma[OR_MAX_POLES];     /* damping, 1/s */
+} oracle_material;
+
+oracle_grid* oracle_create(int mode, int nx, int ny, int nz, double dx, double dt);
+void oracle_destroy(oracle_grid* g);
+/* CPML of `ncells` on one side (0 = min, 1 = max) of `axis`, graded with
+ * PMLParameterModel(dx) (include/PML.hpp:368-393). */
+int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells);
+int oracle_set_materials(oracle_grid* g, const oracle_material* m, int n);
+int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids);
+/* comp 0..2 = x,y,z; target 0 = E (after the constitutive update),
+ * 1 = D (before it). vals[t] is added at step t. */
+int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k,
+                      const double* vals, int nvals);
+/* One TFSF plane (include/Source.hpp:472-634) with its own Aux1D grid.
+ * axis/orient give the normal; lo/hi are inclusive cell ranges; origin (in
+ * cells) and k define the location functor and wave vector; pol_e / pol_h are
+ * the E and H polarisation vectors; aux_vals[s-1] is the aux source value at
+ * aux step s. */
+int oracle_add_tfsf_plane(oracle_grid* g, int axis, int orient, const int* lo, const int* hi,
+                          const double* origin, const double* kvec, const double* pol_e,
+                          const double* pol_h, int aux_ncells, const double* aux_vals, int naux);
+/* Running DFT of one component (0..2 E, 3..5 H) over an inclusive box. */
+int oracle_add_dft(oracle_grid* g, int comp, const int* lo, const int* hi,
+                   const double* freqs, int nf);
+int oracle_step(oracle_grid* g, int nsteps);
+/* which: 0..2 D, 3..5 E, 6..8 B, 9..11 H, 12..14 P(pole 0), 15..17 J(pole 0),
+ * 18..35 psi[ft][I][J]; 36.. P/J of further poles (6 per pole). */
+int oracle_get(const oracle_grid* g, int which, double* out);
+int oracle_set(oracle_grid* g, int which, const double* in);
+/* out: [nf][npoints][2] (re, im) */
+int oracle_dft_get(const oracle_grid* g, int handle, double* out);
+int oracle_dft_npoints(const oracle_grid* g, int handle);
+/* the 1D CPML coefficient profile of one axis: out[4][n] = B, C, F, G */
+int oracle_pml_profile(const oracle_grid* g, int ft, int axis, double* out);
+double oracle_imp0(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,241 @@
+"""Python driver for the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+Runs a ``fdtd_b200.problem.Problem`` through
+  * ``run_oracle``: the plain-C restatement (oracle/liboracle.so), or
+  * ``run_reference``: the reference's own functors (oracle/_ref/ref_runner,
+    compiled from the reference headers by oracle/Makefile).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+from typing import Dict, List, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+RUNNER_PATH = os.path.join(HERE, "_ref", "ref_runner")
+
+# output order of oracle_get / ref_runner
+NAMES = ["Dx", "Dy", "Dz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Hx", "Hy", "Hz",
+         "Px", "Py", "Pz", "Jx", "Jy", "Jz"]
+PSI_NAMES = [f"psi{'EH'[f]}{'xyz'[i]}{'xyz'[j]}" for f in range(2) for i in range(3) for j in range(3)]
+ALL_NAMES = NAMES + PSI_NAMES
+
+
+class OracleMaterial(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("npoles", ctypes.c_int), ("eps_inf", ctypes.c_double),
+                ("mu_r", ctypes.c_double), ("delta_eps", ctypes.c_double * 4),
+                ("freq", ctypes.c_double * 4), ("gamma", ctypes.c_double * 4)]
+
+
+_lib = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile liboracle.so (and the reference runner when the reference tree
+    is present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+    if os.path.isdir("/root/reference"):
+        subprocess.run(["make", "-s", "-C", HERE, "_ref/ref_runner"], check=True,
+                       stdout=subprocess.DEVNULL if quiet else None)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.oracle_create.restype = vp
+        L.oracle_create.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 2
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_set_pml.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_set_materials.argtypes = [vp, ctypes.POINTER(OracleMaterial), ctypes.c_int]
+        L.oracle_set_material_ids.argtypes = [vp, ctypes.c_void_p]
+        L.oracle_add_source.argtypes = [vp] + [ctypes.c_int] * 5 + [dp, ctypes.c_int]
+        L.oracle_add_tfsf_plane.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, dp, dp, dp, dp,
+                                            ctypes.c_int, dp, ctypes.c_int]
+        L.oracle_add_dft.argtypes = [vp, ctypes.c_int, ip, ip, dp, ctypes.c_int]
+        L.oracle_step.argtypes = [vp, ctypes.c_int]
+        L.oracle_get.argtypes = [vp, ctypes.c_int, dp]
+        L.oracle_set.argtypes = [vp, ctypes.c_int, dp]
+        L.oracle_dft_get.argtypes = [vp, ctypes.c_int, dp]
+        L.oracle_dft_npoints.argtypes = [vp, ctypes.c_int]
+        L.oracle_pml_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.oracle_imp0.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(seq):
+    arr = (ctypes.c_int * len(seq))(*seq)
+    return arr
+
+
+def _mat_struct(m) -> OracleMaterial:
+    s = OracleMaterial()
+    s.kind = m.kind
+    s.npoles = len(m.poles)
+    s.eps_inf = m.eps_inf
+    s.mu_r = m.mu_r
+    for q, (de, f, g) in enumerate(m.poles):
+        s.delta_eps[q] = de
+        s.freq[q] = f
+        s.gamma[q] = g
+    return s
+
+
+class OracleGrid:
+    """The C restatement, set up from a Problem."""
+
+    def __init__(self, p):
+        L = lib()
+        nx, ny, nz = p.shape
+        self.p = p
+        self.h = L.oracle_create(p.mode, nx, ny, nz, p.dx, p.dt)
+        if not self.h:
+            raise ValueError("oracle_create rejected the grid")
+        for (a, s), n in sorted(p.pml.items()):
+            assert L.oracle_set_pml(self.h, a, s, n) == 0
+        if len(p.materials) > 256:
+            raise ValueError("the oracle takes at most 256 materials")
+        mats = (OracleMaterial * len(p.materials))(*[_mat_struct(m) for m in p.materials])
+        assert L.oracle_set_materials(self.h, mats, len(p.materials)) == 0
+        ids = p.cell_ids()
+        if ids is not None:
+            ids8 = np.ascontiguousarray(ids.astype(np.uint8))
+            assert L.oracle_set_material_ids(self.h, ids8.ctypes.data) == 0
+        self._keep = []
+        for s in p.sources:
+            v = np.ascontiguousarray(s.values, dtype=np.float64)
+            assert L.oracle_add_source(self.h, s.comp, 0 if s.target == "E" else 1, *s.pos, _dp(v), len(v)) == 0
+        if p.tfsf is not None:
+            t = p.tfsf
+            av = np.ascontiguousarray(t.aux_values, dtype=np.float64)
+            for pl in t.planes:
+                rc = L.oracle_add_tfsf_plane(self.h, pl.axis, pl.orient, _ip(pl.lo), _ip(pl.hi),
+                                             _dp(np.array(t.origin, float)), _dp(np.array(t.k, float)),
+                                             _dp(np.array(t.pol_e, float)), _dp(np.array(t.pol_h, float)),
+                                             t.aux_ncells, _dp(av), len(av))
+                assert rc == 0
+        self.dft_handles = []
+        for r in p.dfts:
+            fr = np.array(r.freqs, dtype=np.float64)
+            hnd = L.oracle_add_dft(self.h, r.comp, _ip(r.lo), _ip(r.hi), _dp(fr), len(fr))
+            assert hnd >= 0
+            self.dft_handles.append(hnd)
+
+    def step(self, n: int) -> None:
+        lib().oracle_step(self.h, n)
+
+    def get(self, name: str) -> np.ndarray:
+        which = ALL_NAMES.index(name) if name in ALL_NAMES else int(name)
+        nx, ny, nz = self.p.shape
+        out = np.empty(nx * ny * nz, dtype=np.float64)
+        assert lib().oracle_get(self.h, which, _dp(out)) == 0
+        return out.reshape(nz, ny, nx)
+
+    def get_pole(self, pole: int, name: str) -> np.ndarray:
+        if pole == 0:
+            return self.get(name)
+        r = ["Px", "Py", "Pz", "Jx", "Jy", "Jz"].index(name)
+        return self.get(str(36 + (pole - 1) * 6 + r))
+
+    def set(self, name: str, arr: np.ndarray) -> None:
+        which = ALL_NAMES.index(name)
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        assert lib().oracle_set(self.h, which, _dp(a)) == 0
+
+    def dft(self, q: int) -> np.ndarray:
+        """[nf][npoints] complex"""
+        L = lib()
+        n = L.oracle_dft_npoints(self.h, self.dft_handles[q])
+        nf = len(self.p.dfts[q].freqs)
+        out = np.empty(nf * n * 2, dtype=np.float64)
+        assert L.oracle_dft_get(self.h, self.dft_handles[q], _dp(out)) == 0
+        out = out.reshape(nf, n, 2)
+        return out[..., 0] + 1j * out[..., 1]
+
+    def pml_profile(self, ft: int, axis: int) -> np.ndarray:
+        n = self.p.shape[axis]
+        out = np.empty(4 * n, dtype=np.float64)
+        assert lib().oracle_pml_profile(self.h, ft, axis, _dp(out)) == 0
+        return out.reshape(4, n)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().oracle_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def run_oracle(p, steps: Optional[int] = None) -> OracleGrid:
+    g = OracleGrid(p)
+    g.step(p.steps if steps is None else steps)
+    return g
+
+
+def reference_available() -> bool:
+    return os.path.exists(RUNNER_PATH)
+
+
+def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
+    """Run the reference's own functors on the same Problem; returns every
+    output array by name (shape (nz, ny, nx))."""
+    if not reference_available():
+        raise RuntimeError("oracle/_ref/ref_runner is not built")
+    steps = p.steps if steps is None else steps
+    nx, ny, nz = p.shape
+    with tempfile.TemporaryDirectory() as td:
+        lines = [f"mode {p.mode}", f"dims {nx} {ny} {nz}", f"dxdt {p.dx!r} {p.dt!r}"]
+        pm = [p.pml.get((a, s), 0) for a in range(3) for s in range(2)]
+        lines.append("pml " + " ".join(str(x) for x in pm))
+        lines.append(f"nmat {len(p.materials)}")
+        for m in p.materials:
+            if len(m.poles) > 1:
+                raise ValueError("the reference holds one pole per cell")
+            de, f, g = m.poles[0] if m.poles else (1.0, 0.0, 0.0)
+            lines.append(f"{m.kind} {m.eps_inf!r} {de!r} {f!r} {g!r} {m.mu_r!r}")
+        ids = p.cell_ids()
+        if ids is not None:
+            ip = os.path.join(td, "ids.bin")
+            np.ascontiguousarray(ids.astype(np.uint8)).tofile(ip)
+            lines.append(f"matids {ip}")
+        else:
+            lines.append("matids none")
+        lines.append(f"nsrc {len(p.sources)}")
+        for q, s in enumerate(p.sources):
+            sp = os.path.join(td, f"src{q}.bin")
+            np.ascontiguousarray(s.values, dtype=np.float64).tofile(sp)
+            lines.append(f"{s.comp} {0 if s.target == 'E' else 1} {s.pos[0]} {s.pos[1]} {s.pos[2]} {sp}")
+        if p.tfsf is not None:
+            t = p.tfsf
+            ap = os.path.join(td, "aux.bin")
+            np.ascontiguousarray(t.aux_values, dtype=np.float64).tofile(ap)
+            lines.append(f"ntfsf {len(t.planes)} {t.aux_ncells} {ap} {t.origin[0]!r} {t.origin[1]!r} {t.origin[2]!r} "
+                         f"{t.k[0]!r} {t.k[1]!r} {t.k[2]!r}")
+            for pl in t.planes:
+                lines.append(f"{pl.axis} {pl.orient} {pl.lo[0]} {pl.hi[0]} {pl.lo[1]} {pl.hi[1]} {pl.lo[2]} {pl.hi[2]}")
+        lines.append(f"steps {steps}")
+        op = os.path.join(td, "out.bin")
+        lines.append(f"out {op}")
+        sc = os.path.join(td, "scenario.txt")
+        with open(sc, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        subprocess.run([RUNNER_PATH, sc], check=True)
+        raw = np.fromfile(op, dtype=np.float64).reshape(len(ALL_NAMES), nz, ny, nx)
+    return {n: raw[q] for q, n in enumerate(ALL_NAMES)}

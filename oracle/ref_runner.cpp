@@ -1,0 +1,394 @@
+// Reference runner: drives pederson/fdtd's own update functors (compiled from
+// the reference headers, unmodified) through a user time loop, the way the
+// reference's tests do (tests/testTM.cpp:31-113, include/Source.hpp:413-435).
+//
+// TEST INFRASTRUCTURE ONLY. This program is the checker that pins the C
+// restatement in oracle/fdtd_oracle.c and generates tests/golden fixtures.
+// It is never linked into, or called by, the product library.
+//
+// Build: see oracle/Makefile (g++ -std=c++17 -ffp-contract=off, reference
+// headers on the include path). Two compile fixes are applied here without
+// touching the reference:
+//  * DispersiveAtomicUpdate (include/DispersiveMaterials.hpp:260-282) puts
+//    enable_if on a class template parameter, which g++13 rejects when any
+//    material functor is instantiated; the partial specialisations below
+//    forward to UpdateStruct::implicit_update / explicit_update with the same
+//    argument order as :272-280.
+//  * `static constexpr double val` (:370, :745, :1047) is ODR-used; C++17
+//    makes it implicitly inline.
+//
+// Scenario file (whitespace separated tokens, see oracle/pyoracle.py writer):
+//   mode <0 TEM|1 TE|2 TM|3 ThreeD>
+//   dims nx ny nz
+//   dxdt dx dt
+//   pml nlo_x nhi_x nlo_y nhi_y nlo_z nhi_z
+//   nmat M  then M lines: kind K delta freq gamma mu_r
+//        kind 0 vacuum, 1 constant, 2 drude, 3 lorentz
+//   matids <path|none>            uint8 per cell, index (k*ny+j)*nx+i
+//   nsrc S then S lines: comp target i j k path  (comp 0..2, target 0=E 1=D,
+//        path: float64 per step, value added at step t)
+//   ntfsf T (T planes) then: aux_ncells aux_path origin_x origin_y origin_z
+//        kx ky kz, and T lines: axis orient i0 i1 j0 j1 k0 k1 (inclusive)
+//        aux_path: float64 per aux step (value for aux step s at index s-1)
+//   steps N
+//   out path
+// Output: float64 arrays in order D(3) E(3) B(3) H(3) P(3) J(3) and the CPML
+// integrators psi[ft][I][J] (18), each nx*ny*nz long.
+#include <fdtd.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <memory>
+#include <fstream>
+
+namespace fdtd {
+template <typename U, typename F>
+struct DispersiveAtomicUpdate<U, true, F> {
+  static constexpr Dir d = FieldDir<F>::value;
+  static constexpr FieldType ft = F::field_type;
+  typedef typename FluxComponent<ft, d>::type DType;
+  typedef typename FieldComponent<ft, d>::type EType;
+  typedef typename CurrentComponent<ft, d>::type JType;
+  typedef typename PolarizationComponent<ft, d>::type PType;
+  template <typename T, typename... Args>
+  static void get(T&& f, Args&&... args) {
+    U::implicit_update(GetField<DType>::get(f), GetField<EType>::get(f),
+                       GetField<PType>::get(f), GetField<JType>::get(f),
+                       std::forward<Args>(args)...);
+  }
+};
+template <typename U, typename F>
+struct DispersiveAtomicUpdate<U, false, F> {
+  static constexpr Dir d = FieldDir<F>::value;
+  static constexpr FieldType ft = F::field_type;
+  typedef typename FluxComponent<ft, d>::type DType;
+  typedef typename FieldComponent<ft, d>::type EType;
+  typedef typename CurrentComponent<ft, d>::type JType;
+  typedef typename PolarizationComponent<ft, d>::type PType;
+  template <typename T, typename... Args>
+  static void get(T&& f, Args&&... args) {
+    U::explicit_update(GetField<DType>::get(f), GetField<EType>::get(f),
+                       GetField<PType>::get(f), GetField<JType>::get(f),
+                       std::forward<Args>(args)...);
+  }
+};
+}  // namespace fdtd
+
+using namespace fdtd;
+
+static std::vector<double> read_f64(const std::string& path) {
+  std::vector<double> v;
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) { fprintf(stderr, "cannot open %s\n", path.c_str()); exit(2); }
+  fseek(f, 0, SEEK_END); long n = ftell(f); fseek(f, 0, SEEK_SET);
+  v.resize(n / 8);
+  if (fread(v.data(), 8, v.size(), f) != v.size()) { fprintf(stderr, "short read\n"); exit(2); }
+  fclose(f);
+  return v;
+}
+
+struct Mat { int kind; double K, delta, freq, gamma, mu; };
+struct Src { int comp, target, i, j, k; std::vector<double> vals; };
+struct PlaneSpec { int axis, orient, lo[3], hi[3]; };
+
+struct Scenario {
+  int mode = 2, nx = 1, ny = 1, nz = 1;
+  double dx = 1, dt = 1;
+  int pml[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  std::vector<Mat> mats;
+  std::vector<uint8_t> ids;
+  std::vector<Src> srcs;
+  int aux_ncells = 0; std::vector<double> aux_vals; double origin[3] = {0, 0, 0}, kvec[3] = {1, 0, 0};
+  std::vector<PlaneSpec> planes;
+  int steps = 0;
+  std::string out;
+};
+
+// The user-side cell: the reference's YeeCell mixins plus neighbour pointers
+// (the neighbour contract of include/DefaultInterfaces.hpp:66-79).
+template <class Mode>
+struct Cell : public YeeCell<YeeFields<Mode, double, std::array>, DoublePolarization<double>,
+                             VacuumMagnetization<double>, NewPML<Mode, double>> {
+  Cell* nmin[3] = {nullptr, nullptr, nullptr};
+  Cell* nmax[3] = {nullptr, nullptr, nullptr};
+  int ci = 0, cj = 0, ck = 0;
+  Cell& getNeighborMin(int d) { return *nmin[d]; }
+  Cell& getNeighborMax(int d) { return *nmax[d]; }
+};
+
+// Iterator over a list of cell pointers that dereferences to the cell, as
+// TFSFPlane (include/Source.hpp:595-619) expects.
+template <class C>
+struct PtrIt {
+  typename std::vector<C*>::iterator it;
+  C& operator*() const { return **it; }
+  PtrIt& operator++() { ++it; return *this; }
+  PtrIt operator++(int) { PtrIt t = *this; ++it; return t; }
+  bool operator!=(const PtrIt& o) const { return it != o.it; }
+  bool operator==(const PtrIt& o) const { return it == o.it; }
+};
+
+struct TableSignal {
+  const std::vector<double>* tab; double dt;
+  double operator()(double t) const {
+    long s = std::lround(t / dt);
+    if (s < 1 || s > (long)tab->size()) return 0.0;
+    return (*tab)[s - 1];
+  }
+};
+
+// per-step table signal for SoftSource::apply(t) with t the step index
+struct StepSignal {
+  const std::vector<double>* tab;
+  double operator()(double t) const {
+    long s = static_cast<long>(t);
+    return (s >= 0 && s < (long)tab->size()) ? (*tab)[s] : 0.0;
+  }
+};
+
+template <class Mode, class F>
+constexpr bool has_field() {
+  return Detail::tuple_contains_type<F, typename FieldComponents<Mode>::electric>::value ||
+         Detail::tuple_contains_type<F, typename FieldComponents<Mode>::magnetic>::value;
+}
+
+template <class Mode, class F, class C>
+double field_or_zero(C& c) {
+  if constexpr (Detail::tuple_contains_type<F, typename FieldComponents<Mode>::electric>::value ||
+                Detail::tuple_contains_type<F, typename FieldComponents<Mode>::magnetic>::value)
+    return GetField<F>::get(c);
+  else return 0.0;
+}
+template <class Mode, class F, class Flux, class C>
+double flux_or_zero(C& c) {
+  if constexpr (Detail::tuple_contains_type<F, typename FieldComponents<Mode>::electric>::value ||
+                Detail::tuple_contains_type<F, typename FieldComponents<Mode>::magnetic>::value)
+    return GetField<Flux>::get(c);
+  else return 0.0;
+}
+
+template <class Mode, class Flux, class C> void yee(C& c, double dt, double dx) {
+  if constexpr (Detail::tuple_contains_type<Flux, typename FieldComponents<Mode>::electric_flux>::value ||
+                Detail::tuple_contains_type<Flux, typename FieldComponents<Mode>::magnetic_flux>::value)
+    YeeUpdate<Mode, Flux>(dt, dx)(c);
+}
+
+template <class Mode>
+static int run(Scenario& s) {
+  typedef Cell<Mode> C;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  const int dim = Mode::dim;
+  std::vector<C> cells((size_t)nx * ny * nz);
+  auto at = [&](int i, int j, int k) -> C& { return cells[((size_t)k * ny + j) * nx + i]; };
+  int n[3] = {nx, ny, nz};
+  // wire neighbours of interior cells only; the outer ring is never updated
+  std::vector<C*> interior;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        C& c = at(i, j, k); c.ci = i; c.cj = j; c.ck = k;
+        int idx[3] = {i, j, k};
+        bool in = true;
+        for (int d = 0; d < dim; d++) if (idx[d] < 1 || idx[d] > n[d] - 2) in = false;
+        if (!in) continue;
+        for (int d = 0; d < dim; d++) {
+          int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+          lo[d]--; hi[d]++;
+          c.nmin[d] = &at(lo[0], lo[1], lo[2]);
+          c.nmax[d] = &at(hi[0], hi[1], hi[2]);
+        }
+        interior.push_back(&c);
+      }
+  // CPML profile, following tests/testTM.cpp:44-71 per axis and side
+  PMLParameterModel p(s.dx);
+  for (int a = 0; a < dim; a++) {
+    for (int side = 0; side < 2; side++) {
+      int np = s.pml[a][side];
+      if (np <= 0) continue;
+      for (int i = 1; i < np + 2; i++) {
+        double x = static_cast<double>(np - i + 1) / static_cast<double>(np);
+        double xm = x - 0.5 / static_cast<double>(np);
+        int ce = side == 0 ? i : n[a] - i;
+        int cm = side == 0 ? i : n[a] - 1 - i;
+        for (auto& c : cells) {
+          int idx[3] = {c.ci, c.cj, c.ck};
+          if (idx[a] == ce) {
+            if (a == 0) c.template setPMLParameters<FieldType::Electric, Dir::X>(p.K(x), p.S(x), p.A(x), s.dt);
+            if (a == 1) c.template setPMLParameters<FieldType::Electric, Dir::Y>(p.K(x), p.S(x), p.A(x), s.dt);
+            if (a == 2) c.template setPMLParameters<FieldType::Electric, Dir::Z>(p.K(x), p.S(x), p.A(x), s.dt);
+          }
+          if (idx[a] == cm) {
+            if (a == 0) c.template setPMLParameters<FieldType::Magnetic, Dir::X>(p.K(xm), p.S(xm), p.A(xm), s.dt);
+            if (a == 1) c.template setPMLParameters<FieldType::Magnetic, Dir::Y>(p.K(xm), p.S(xm), p.A(xm), s.dt);
+            if (a == 2) c.template setPMLParameters<FieldType::Magnetic, Dir::Z>(p.K(xm), p.S(xm), p.A(xm), s.dt);
+          }
+        }
+      }
+    }
+  }
+  bool pmlax[3];
+  for (int a = 0; a < 3; a++) pmlax[a] = (a < dim) && (s.pml[a][0] > 0 || s.pml[a][1] > 0);
+
+  // material functors (include/DispersiveMaterials.hpp:489-497, :881-884, :1208-1211)
+  const double dt = s.dt, dx = s.dx;
+  std::vector<std::function<void(C&)>> eupd, hupd;
+  for (auto& m : s.mats) {
+    switch (m.kind) {
+      case 0: { VacuumUpdate<Mode, FieldType::Electric> u; eupd.push_back([u](C& c) mutable { u(c); }); break; }
+      case 1: { ConstantUpdate<Mode, FieldType::Electric> u(m.K); eupd.push_back([u](C& c) mutable { u(c); }); break; }
+      case 2: { DrudeUpdate<Mode, FieldType::Electric> u(m.K, m.freq, m.gamma, dt); eupd.push_back([u](C& c) mutable { u(c); }); break; }
+      case 3: { LorentzUpdate<Mode, FieldType::Electric> u(m.K, m.delta, m.freq, m.gamma, dt); eupd.push_back([u](C& c) mutable { u(c); }); break; }
+      default: fprintf(stderr, "bad material kind\n"); return 3;
+    }
+    if (m.mu == 1.0) { VacuumUpdate<Mode, FieldType::Magnetic> u; hupd.push_back([u](C& c) mutable { u(c); }); }
+    else { ConstantUpdate<Mode, FieldType::Magnetic> u(m.mu); hupd.push_back([u](C& c) mutable { u(c); }); }
+  }
+  auto matid = [&](C& c) -> int { return s.ids.empty() ? 0 : s.ids[((size_t)c.ck * ny + c.cj) * nx + c.ci]; };
+
+  // TFSF planes over one shared 1D auxiliary grid (include/Source.hpp:280-634)
+  typedef std::array<double, Mode::dim> PT;
+  std::vector<std::vector<C*>> plane_cells(s.planes.size());
+  auto loc = [&](PtrIt<C> it) -> PT {
+    C& c = *it; PT pt; int idx[3] = {c.ci, c.cj, c.ck};
+    for (int d = 0; d < Mode::dim; d++) pt[d] = (static_cast<double>(idx[d]) - s.origin[d]) * dx;
+    return pt;
+  };
+  typedef decltype(loc) LocT;
+  typedef TFSFPlane<Mode, LocT, PtrIt<C>, Aux1D<double>> PlaneT;
+  std::vector<std::unique_ptr<PlaneT>> planes;
+  if (!s.planes.empty()) {
+    PT kv; for (int d = 0; d < Mode::dim; d++) kv[d] = s.kvec[d];
+    for (size_t q = 0; q < s.planes.size(); q++) {
+      auto& ps = s.planes[q];
+      for (int k = ps.lo[2]; k <= ps.hi[2]; k++)
+        for (int j = ps.lo[1]; j <= ps.hi[1]; j++)
+          for (int i = ps.lo[0]; i <= ps.hi[0]; i++) plane_cells[q].push_back(&at(i, j, k));
+      PT normal; for (int d = 0; d < Mode::dim; d++) normal[d] = 0;
+      normal[ps.axis] = ps.orient == 1 ? 1 : -1;
+      PtrIt<C> b{plane_cells[q].begin()}, e{plane_cells[q].end()};
+      // one aux grid per plane: every updateD advances its plane's aux grid
+      auto aux = std::make_shared<Aux1D<double>>(s.aux_ncells, dx, dt, TableSignal{&s.aux_vals, dt});
+      planes.emplace_back(new PlaneT(kv, normal, loc, b, e, aux));
+    }
+  }
+
+  std::vector<std::function<void(double)>> appliers, dappliers;
+  for (auto& sr : s.srcs) {
+    C& c = at(sr.i, sr.j, sr.k);
+    StepSignal sig{&sr.vals};
+    auto& lst = sr.target == 0 ? appliers : dappliers;
+    auto add = [&](auto src) { lst.push_back([src](double t) mutable { src.apply(t); }); };
+    if (sr.target == 0) {
+      if (sr.comp == 0) { if constexpr (has_field<Mode, Ex>()) add(make_soft_source<Ex>(sig, c)); }
+      if (sr.comp == 1) { if constexpr (has_field<Mode, Ey>()) add(make_soft_source<Ey>(sig, c)); }
+      if (sr.comp == 2) { if constexpr (has_field<Mode, Ez>()) add(make_soft_source<Ez>(sig, c)); }
+    } else {
+      if (sr.comp == 0) { if constexpr (has_field<Mode, Ex>()) add(make_soft_source<Dx>(sig, c)); }
+      if (sr.comp == 1) { if constexpr (has_field<Mode, Ey>()) add(make_soft_source<Dy>(sig, c)); }
+      if (sr.comp == 2) { if constexpr (has_field<Mode, Ez>()) add(make_soft_source<Dz>(sig, c)); }
+    }
+  }
+
+  for (int t = 0; t < s.steps; t++) {
+    // ---- E half step: curl, TFSF, CPML per axis, material, sources
+    for (C* c : interior) yee<Mode, Dx>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Dy>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Dz>(*c, dt, dx);
+    for (auto& pl : planes) pl->updateD(dt, dx);
+    for (auto& ap : dappliers) ap(static_cast<double>(t));
+    if (pmlax[0]) for (C* c : interior) UpdatePML<Mode, FieldType::Electric, Dir::X>(dt, dx)(*c);
+    if (pmlax[1]) for (C* c : interior) UpdatePML<Mode, FieldType::Electric, Dir::Y>(dt, dx)(*c);
+    if constexpr (Mode::dim == 3) { if (pmlax[2]) for (C* c : interior) UpdatePML<Mode, FieldType::Electric, Dir::Z>(dt, dx)(*c); }
+    for (C* c : interior) eupd[matid(*c)](*c);
+    for (auto& ap : appliers) ap(static_cast<double>(t));
+    // ---- H half step
+    for (C* c : interior) yee<Mode, Bx>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, By>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Bz>(*c, dt, dx);
+    for (auto& pl : planes) pl->updateB(dt, dx);
+    if (pmlax[0]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::X>(dt, dx)(*c);
+    if (pmlax[1]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::Y>(dt, dx)(*c);
+    if constexpr (Mode::dim == 3) { if (pmlax[2]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::Z>(dt, dx)(*c); }
+    for (C* c : interior) hupd[matid(*c)](*c);
+  }
+
+  FILE* f = fopen(s.out.c_str(), "wb");
+  if (!f) return 4;
+  std::vector<double> buf(cells.size());
+  auto dump = [&](auto getter) {
+    for (size_t q = 0; q < cells.size(); q++) buf[q] = getter(cells[q]);
+    fwrite(buf.data(), 8, buf.size(), f);
+  };
+  dump([](C& c) { return flux_or_zero<Mode, Ex, Dx>(c); });
+  dump([](C& c) { return flux_or_zero<Mode, Ey, Dy>(c); });
+  dump([](C& c) { return flux_or_zero<Mode, Ez, Dz>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Ex>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Ey>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Ez>(c); });
+  dump([](C& c) { return flux_or_zero<Mode, Hx, Bx>(c); });
+  dump([](C& c) { return flux_or_zero<Mode, Hy, By>(c); });
+  dump([](C& c) { return flux_or_zero<Mode, Hz, Bz>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Hx>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Hy>(c); });
+  dump([](C& c) { return field_or_zero<Mode, Hz>(c); });
+  dump([](C& c) { return c.Px(); });
+  dump([](C& c) { return c.Py(); });
+  dump([](C& c) { return c.Pz(); });
+  dump([](C& c) { return c.Jx(); });
+  dump([](C& c) { return c.Jy(); });
+  dump([](C& c) { return c.Jz(); });
+#define PSI(ft, I, J) dump([](C& c) { return c.template pmlI<FieldType::ft, Dir::I, Dir::J>(); });
+  PSI(Electric, X, X) PSI(Electric, X, Y) PSI(Electric, X, Z)
+  PSI(Electric, Y, X) PSI(Electric, Y, Y) PSI(Electric, Y, Z)
+  PSI(Electric, Z, X) PSI(Electric, Z, Y) PSI(Electric, Z, Z)
+  PSI(Magnetic, X, X) PSI(Magnetic, X, Y) PSI(Magnetic, X, Z)
+  PSI(Magnetic, Y, X) PSI(Magnetic, Y, Y) PSI(Magnetic, Y, Z)
+  PSI(Magnetic, Z, X) PSI(Magnetic, Z, Y) PSI(Magnetic, Z, Z)
+  fclose(f);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 2) { fprintf(stderr, "usage: ref_runner scenario.txt\n"); return 1; }
+  std::ifstream in(argv[1]);
+  Scenario s;
+  std::string key;
+  while (in >> key) {
+    if (key == "mode") in >> s.mode;
+    else if (key == "dims") in >> s.nx >> s.ny >> s.nz;
+    else if (key == "dxdt") in >> s.dx >> s.dt;
+    else if (key == "pml") for (int a = 0; a < 3; a++) in >> s.pml[a][0] >> s.pml[a][1];
+    else if (key == "nmat") {
+      int m; in >> m; s.mats.resize(m);
+      for (auto& x : s.mats) in >> x.kind >> x.K >> x.delta >> x.freq >> x.gamma >> x.mu;
+    } else if (key == "matids") {
+      std::string p; in >> p;
+      if (p != "none") {
+        FILE* f = fopen(p.c_str(), "rb");
+        s.ids.resize((size_t)s.nx * s.ny * s.nz);
+        if (!f || fread(s.ids.data(), 1, s.ids.size(), f) != s.ids.size()) { fprintf(stderr, "bad ids\n"); return 2; }
+        fclose(f);
+      }
+    } else if (key == "nsrc") {
+      int m; in >> m; s.srcs.resize(m);
+      for (auto& x : s.srcs) { std::string p; in >> x.comp >> x.target >> x.i >> x.j >> x.k >> p; x.vals = read_f64(p); }
+    } else if (key == "ntfsf") {
+      int m; in >> m; std::string p;
+      in >> s.aux_ncells >> p >> s.origin[0] >> s.origin[1] >> s.origin[2] >> s.kvec[0] >> s.kvec[1] >> s.kvec[2];
+      if (m > 0) s.aux_vals = read_f64(p);
+      s.planes.resize(m);
+      for (auto& x : s.planes) in >> x.axis >> x.orient >> x.lo[0] >> x.hi[0] >> x.lo[1] >> x.hi[1] >> x.lo[2] >> x.hi[2];
+    } else if (key == "steps") in >> s.steps;
+    else if (key == "out") in >> s.out;
+    else { fprintf(stderr, "unknown key %s\n", key.c_str()); return 1; }
+  }
+  switch (s.mode) {
+    case 1: return run<TE>(s);
+    case 2: return run<TM>(s);
+    case 3: return run<ThreeD>(s);
+    default: fprintf(stderr, "mode %d not supported\n", s.mode); return 1;
+  }
+}
