@@ -1,0 +1,1090 @@
+// Host implementation of the C ABI declared in include/fdtd_b200.h.
+//
+// Set-up work (CPML grading, material coefficients, TFSF plane checks) is
+// done here on the host in FP64, in the reference's operation order; this file
+// is compiled with -Xcompiler -ffp-contract=off so that, e.g., the coefficients
+// of NewPML::setPMLParameters (include/PML.hpp:84-102) round exactly as in the
+// reference. The time loop itself is a fixed sequence of stream-ordered
+// launches per step: E sweep, E-phase DFT, H sweep, H-phase DFT, step counter.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "internal.h"
+
+using namespace fdtdb;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" const char* fdtd_last_error_string(void) { return g_err.c_str(); }
+
+namespace {
+
+// the reference's constexpr Newton sqrt (include/FDTDConstants.hpp:136-156)
+double ref_sqrt(double x) {
+  double curr = x, prev = 0.0;
+  while (curr != prev) {
+    double next = 0.5 * (curr + x / curr);
+    prev = curr;
+    curr = next;
+  }
+  return curr;
+}
+double imp0() { return ref_sqrt(kMu0 / kEps0); }
+
+// PMLParameterModel(dx) (include/PML.hpp:368-393)
+struct PmlModel {
+  double m, ma, smax, kmax, amax;
+  explicit PmlModel(double dx) : m(3), ma(1), smax(0.8 * (m + 1) / (imp0() * dx)), kmax(5), amax(0.05) {}
+  double K(double x) const { if (x < 0.0) return 1.0; return x > 1.0 ? 1.0 : 1.0 + pow(x, m) * (kmax - 1.0); }
+  double S(double x) const { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(x, m) * smax; }
+  double A(double x) const { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(1.0 - x, ma) * amax; }
+};
+
+// NewPML::setPMLParameters (include/PML.hpp:84-102)
+void set_params(double K, double S, double A, double dt, double& B, double& C, double& F, double& G) {
+  double nu = 1.0 / kEps0 * (S / K + A);
+  B = exp(-dt * nu);
+  C = (nu == 0) ? 0.0 : S / K * 1.0 / (S + K * A) * (B - 1.0);
+  double u = -S / (kEps0 * K * K);
+  F = (nu == 0) ? 1.0 / K : 1.0 / K - 1.0 / dt * (1.0 - B - nu * dt) * u / (nu * nu);
+  G = (nu == 0) ? 0.0 : 1.0 / dt * (1.0 - B) / nu;
+}
+
+struct Profile {  // one (field type, axis)
+  std::vector<double> B, C, F, G;
+  void reset(int n) {
+    B.assign(n, 0.0);
+    C.assign(n, 0.0);
+    F.assign(n, 1.0);  // NewPML defaults (PML.hpp:40-55)
+    G.assign(n, 0.0);
+  }
+};
+
+// grading loop of tests/testTM.cpp:44-71 for one side of one axis
+void grade(double dx, double dt, int n, int np, int side, Profile& e, Profile& h) {
+  PmlModel p(dx);
+  for (int i = 1; i < np + 2; i++) {
+    double x = static_cast<double>(np - i + 1) / static_cast<double>(np);
+    double xm = x - 0.5 / static_cast<double>(np);
+    int ce = side == 0 ? i : n - i;
+    int cm = side == 0 ? i : n - 1 - i;
+    if (ce >= 0 && ce < n) set_params(p.K(x), p.S(x), p.A(x), dt, e.B[ce], e.C[ce], e.F[ce], e.G[ce]);
+    if (cm >= 0 && cm < n) set_params(p.K(xm), p.S(xm), p.A(xm), dt, h.B[cm], h.C[cm], h.F[cm], h.G[cm]);
+  }
+}
+
+struct SourceH {
+  int comp, target, i, j, k;
+  std::vector<double> vals;
+  double* d_vals = nullptr;
+};
+
+struct AuxH {
+  int ncells, L;
+  std::vector<double> vals;
+  double *d_state = nullptr;  // Dz, Ez, By, Hy, psiE, psiH (6L)
+  double *d_coef = nullptr;   // 8L
+  double *d_vals = nullptr;
+  double *d_tab = nullptr;    // 2 * cap * L
+  long long cap = 0;
+};
+
+struct PlaneH {
+  PlaneDev dev;
+};
+
+struct DftH {
+  int comp, nf;
+  int lo[3], hi[3];
+  long long npts;
+  std::vector<double> freqs;
+  double* d_freqs = nullptr;
+  double* d_acc = nullptr;
+};
+
+}  // namespace
+
+struct fdtd_grid {
+  fdtd_grid_desc d{};
+  int n[3]{1, 1, 1};
+  int pitch = 0;
+  bool f32 = false;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  long long bytes = 0;
+  long long launches = 0;
+  long long t = 0;
+  int pml[3][2]{};
+  Profile prof[2][3];
+  std::vector<fdtd_material> mats;
+  // device state
+  void* E[3]{};
+  void* H[3]{};
+  void* D[3]{};
+  void* B[3]{};
+  void* P[kMaxPoles][3]{};
+  void* J[kMaxPoles][3]{};
+  void* psi[2][3][3]{};
+  void* d_prof[2][3][4]{};  // F32 F array holds scaled F then raw F
+  int npoles_alloc = 0;
+  Slab slab[3]{};
+  uint8_t* d_ids = nullptr;
+  uint16_t* d_bids = nullptr;
+  int bshift = 0, nbx = 0, nby = 0, nbz = 0;
+  void* d_mats = nullptr;
+  int max_poles = 0;
+  std::vector<SourceH> srcs;
+  double* d_src_last = nullptr;
+  std::vector<PlaneH> planes;
+  std::vector<AuxH> auxes;
+  std::vector<DftH> dfts;
+  DftRegionDev* d_dft[2]{};
+  int ndft[2]{};
+  long long dft_pts[2]{};
+  void** d_fieldptrs = nullptr;  // [E0,E1,E2,H0,H1,H2]
+  Control* ctrl = nullptr;
+  int* d_flag = nullptr;
+  bool dirty_dft = true;
+};
+
+namespace {
+
+size_t elem(const fdtd_grid* g) { return g->f32 ? 4 : 8; }
+long long rowlen(const fdtd_grid* g) { return g->f32 ? g->pitch : g->n[0]; }
+long long field_elems(const fdtd_grid* g) { return rowlen(g) * g->n[1] * g->n[2]; }
+
+int dalloc(fdtd_grid* g, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? FDTD_ERR_NOMEM : FDTD_ERR_CUDA,
+                std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemsetAsync(*p, 0, bytes, g->stream);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
+  g->allocs.push_back(*p);
+  g->bytes += static_cast<long long>(bytes);
+  return FDTD_OK;
+}
+
+void dfree(fdtd_grid* g, void* p) {
+  if (!p) return;
+  for (size_t q = 0; q < g->allocs.size(); q++)
+    if (g->allocs[q] == p) {
+      g->allocs.erase(g->allocs.begin() + q);
+      break;
+    }
+  cudaFree(p);
+}
+
+int upload_vec(fdtd_grid* g, void** p, const void* src, size_t bytes) {
+  if (*p) dfree(g, *p);
+  int rc = dalloc(g, p, bytes);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(*p, src, bytes, cudaMemcpyHostToDevice, g->stream));
+  return FDTD_OK;
+}
+
+int dim_of(const fdtd_grid* g) { return g->d.mode == kThreeD ? 3 : 2; }
+
+double eta() { return imp0(); }
+double ce_of(const fdtd_grid* g) { return g->d.dt / (kEps0 * eta() * g->d.dx); }
+double ch_of(const fdtd_grid* g) { return eta() * g->d.dt / (kMu0 * g->d.dx); }
+
+int upload_profiles(fdtd_grid* g) {
+  CK(cudaStreamSynchronize(g->stream));
+  for (int ft = 0; ft < 2; ft++)
+    for (int a = 0; a < 3; a++) {
+      const Profile& p = g->prof[ft][a];
+      const int n = g->n[a];
+      for (int q = 0; q < 4; q++) {
+        if (g->f32) {
+          const double c = ft == 0 ? ce_of(g) : ch_of(g);
+          std::vector<float> v(q == 2 ? 2 * n : n);
+          for (int i = 0; i < n; i++) {
+            if (q == 0) v[i] = static_cast<float>(p.B[i]);
+            if (q == 1) v[i] = static_cast<float>(c * p.C[i]);
+            if (q == 2) {
+              v[i] = static_cast<float>(c * p.F[i]);
+              v[n + i] = static_cast<float>(p.F[i]);
+            }
+            if (q == 3) v[i] = static_cast<float>(p.G[i]);
+          }
+          int rc = upload_vec(g, &g->d_prof[ft][a][q], v.data(), v.size() * sizeof(float));
+          if (rc) return rc;
+        } else {
+          std::vector<double> v(n);
+          for (int i = 0; i < n; i++) {
+            if (q == 0) v[i] = p.B[i];
+            if (q == 1) v[i] = p.C[i] / g->d.dx;  // (C*LC)/dx = LC*(C/dx)
+            if (q == 2) v[i] = p.F[i] / g->d.dx;  // (LC*F)/dx = LC*(F/dx)
+            if (q == 3) v[i] = p.G[i];
+          }
+          int rc = upload_vec(g, &g->d_prof[ft][a][q], v.data(), v.size() * sizeof(double));
+          if (rc) return rc;
+        }
+      }
+    }
+  return FDTD_OK;
+}
+
+int alloc_psi(fdtd_grid* g) {
+  for (int ft = 0; ft < 2; ft++)
+    for (int I = 0; I < 3; I++)
+      for (int J = 0; J < 3; J++) {
+        if (g->psi[ft][I][J]) {
+          dfree(g, g->psi[ft][I][J]);
+          g->psi[ft][I][J] = nullptr;
+        }
+      }
+  for (int a = 0; a < 3; a++) {
+    const int wlo = g->pml[a][0] > 0 ? g->pml[a][0] + 1 : 0;
+    const int whi = g->pml[a][1] > 0 ? g->pml[a][1] + 1 : 0;
+    g->slab[a].wlo = wlo;
+    g->slab[a].hi0 = g->n[a] - 1 - whi;
+    g->slab[a].W = wlo + whi;
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int I = 0; I < 3; I++) {
+      const bool has = ft == 0 ? hasE(g->d.mode, I) : hasH(g->d.mode, I);
+      if (!has) continue;
+      for (int J = 0; J < 3; J++) {
+        if (J == I || g->slab[J].W == 0) continue;
+        long long cnt;
+        if (J == 0) cnt = static_cast<long long>(g->n[2]) * g->n[1] * g->slab[0].W;
+        else if (J == 1) cnt = static_cast<long long>(g->n[2]) * g->slab[1].W * rowlen(g);
+        else cnt = static_cast<long long>(g->slab[2].W) * g->n[1] * rowlen(g);
+        int rc = dalloc(g, &g->psi[ft][I][J], cnt * elem(g));
+        if (rc) return rc;
+      }
+    }
+  return FDTD_OK;
+}
+
+long long cell_index(const fdtd_grid* g, int i, int j, int k) {
+  return (static_cast<long long>(k) * g->n[1] + j) * rowlen(g) + i;
+}
+
+bool interior(const fdtd_grid* g, int i, int j, int k) {
+  if (i < 1 || i > g->n[0] - 2 || j < 1 || j > g->n[1] - 2) return false;
+  if (g->d.mode == kThreeD) return k >= 1 && k <= g->n[2] - 2;
+  return k == 0;
+}
+
+int build_materials(fdtd_grid* g) {
+  const double dt = g->d.dt;
+  int maxp = 0;
+  bool drude = false;
+  if (g->f32) {
+    std::vector<MatF32> v(g->mats.size());
+    for (size_t q = 0; q < g->mats.size(); q++) {
+      const fdtd_material& m = g->mats[q];
+      MatF32& o = v[q];
+      memset(&o, 0, sizeof(o));
+      o.inv_eps = static_cast<float>(m.kind == FDTD_VACUUM ? 1.0 : 1.0 / m.eps_inf);
+      if (m.kind == FDTD_DRUDE) {
+        const double bb = m.gamma[0] * dt * 0.5, w = dt * m.freq[0];
+        o.npoles = -1;
+        o.a[0] = static_cast<float>((1.0 - bb) / (1.0 + bb));
+        o.b[0] = static_cast<float>(w * w);
+        drude = true;
+      } else if (m.kind == FDTD_LORENTZ) {
+        if (m.npoles > 2) return fail(FDTD_ERR_UNSUPPORTED, "the FP32 fused method takes at most 2 Lorentz poles");
+        o.npoles = m.npoles;
+        for (int p = 0; p < m.npoles; p++) {
+          const double bb = 1.0 + m.gamma[p] * dt, bm = 1.0 - m.gamma[p] * dt, w = m.freq[p] * dt;
+          o.a[p] = static_cast<float>(bm / bb);
+          o.b[p] = static_cast<float>(w * w * m.delta_eps[p] / bb);
+          o.c[p] = static_cast<float>(w * w / bb);
+        }
+        maxp = std::max(maxp, m.npoles);
+      }
+    }
+    g->max_poles = maxp > 0 ? maxp : (drude ? -1 : 0);
+    if (drude && maxp == 0) maxp = 1;
+    int rc = upload_vec(g, &g->d_mats, v.data(), v.size() * sizeof(MatF32));
+    if (rc) return rc;
+  } else {
+    std::vector<MatF64> v(g->mats.size());
+    for (size_t q = 0; q < g->mats.size(); q++) {
+      const fdtd_material& m = g->mats[q];
+      MatF64& o = v[q];
+      memset(&o, 0, sizeof(o));
+      o.kind = m.kind;
+      o.npoles = m.kind == FDTD_DRUDE ? 1 : (m.kind == FDTD_LORENTZ ? m.npoles : 0);
+      // VacuumStorage K = 1 (DispersiveMaterials.hpp:446-457)
+      o.den_e = (m.kind == FDTD_VACUUM ? 1.0 : m.eps_inf) * kEps0;
+      o.den_h = m.mu_r * kMu0;
+      if (m.kind == FDTD_DRUDE) {
+        // drude::DrudeUpdate::implicit_update (DispersiveMaterials.hpp:986-996)
+        const double b = m.gamma[0] * dt * 0.5;
+        const double w = dt * m.freq[0];
+        o.c1[0] = 1.0 - b;
+        o.c2[0] = 1.0 + b;
+        o.c3[0] = w * w / dt * kEps0;
+      } else if (m.kind == FDTD_LORENTZ) {
+        // lorentz::LorentzUpdate::implicit_update (DispersiveMaterials.hpp:719-732)
+        for (int p = 0; p < m.npoles; p++) {
+          const double b = 1.0 + m.gamma[p] * dt;
+          const double bm = 1.0 - m.gamma[p] * dt;
+          const double w = m.freq[p] * dt;
+          const double qq = m.freq[p] * w / b;
+          o.c1[p] = bm / b;
+          o.c2[p] = qq * m.delta_eps[p] * kEps0;
+          o.c3[p] = qq;
+        }
+      }
+      maxp = std::max(maxp, o.npoles);
+    }
+    g->max_poles = maxp;
+    int rc = upload_vec(g, &g->d_mats, v.data(), v.size() * sizeof(MatF64));
+    if (rc) return rc;
+  }
+  // polarisation state for the poles in use
+  const int need = g->f32 ? (g->max_poles < 0 ? 1 : g->max_poles) : maxp;
+  for (int p = g->npoles_alloc; p < need; p++)
+    for (int c = 0; c < 3; c++) {
+      if (!hasE(g->d.mode, c)) continue;
+      int rc = dalloc(g, &g->P[p][c], field_elems(g) * elem(g));
+      if (rc) return rc;
+      rc = dalloc(g, &g->J[p][c], field_elems(g) * elem(g));
+      if (rc) return rc;
+    }
+  g->npoles_alloc = std::max(g->npoles_alloc, need);
+  return FDTD_OK;
+}
+
+// Aux1D set-up (include/Source.hpp:368-390): a TEM grid of ncells+50 cells
+// with a 15-cell CPML graded like the main grid, both sides in one loop.
+int build_aux(fdtd_grid* g, AuxH& a) {
+  const int L = a.L;
+  Profile e, h;
+  e.reset(L);
+  h.reset(L);
+  PmlModel pm(g->d.dx);
+  for (int i = 1; i < kAuxNpml + 2; i++) {
+    double x = static_cast<double>(kAuxNpml - i + 1) / static_cast<double>(kAuxNpml);
+    double xm = x - 0.5 / static_cast<double>(kAuxNpml);
+    set_params(pm.K(x), pm.S(x), pm.A(x), g->d.dt, e.B[i], e.C[i], e.F[i], e.G[i]);
+    set_params(pm.K(xm), pm.S(xm), pm.A(xm), g->d.dt, h.B[i], h.C[i], h.F[i], h.G[i]);
+    set_params(pm.K(x), pm.S(x), pm.A(x), g->d.dt, e.B[L - i], e.C[L - i], e.F[L - i], e.G[L - i]);
+    set_params(pm.K(xm), pm.S(xm), pm.A(xm), g->d.dt, h.B[L - 1 - i], h.C[L - 1 - i], h.F[L - 1 - i],
+               h.G[L - 1 - i]);
+  }
+  std::vector<double> coef(8 * static_cast<size_t>(L));
+  for (int i = 0; i < L; i++) {
+    coef[i] = e.B[i];
+    coef[L + i] = e.C[i] / g->d.dx;
+    coef[2 * L + i] = e.F[i] / g->d.dx;
+    coef[3 * L + i] = e.G[i];
+    coef[4 * L + i] = h.B[i];
+    coef[5 * L + i] = h.C[i] / g->d.dx;
+    coef[6 * L + i] = h.F[i] / g->d.dx;
+    coef[7 * L + i] = h.G[i];
+  }
+  int rc = upload_vec(g, reinterpret_cast<void**>(&a.d_coef), coef.data(), coef.size() * sizeof(double));
+  if (rc) return rc;
+  rc = dalloc(g, reinterpret_cast<void**>(&a.d_state), 6 * static_cast<size_t>(L) * sizeof(double));
+  if (rc) return rc;
+  return upload_vec(g, reinterpret_cast<void**>(&a.d_vals), a.vals.data(),
+                    std::max<size_t>(1, a.vals.size()) * sizeof(double));
+}
+
+int rebuild_dft(fdtd_grid* g) {
+  for (int ph = 0; ph < 2; ph++) {
+    std::vector<DftRegionDev> v;
+    long long off = 0;
+    for (auto& r : g->dfts) {
+      if ((r.comp < 3) != (ph == 0)) continue;
+      DftRegionDev o{};
+      o.comp = r.comp % 3;
+      o.nf = r.nf;
+      for (int d = 0; d < 3; d++) {
+        o.lo[d] = r.lo[d];
+        o.ext[d] = r.hi[d] - r.lo[d] + 1;
+      }
+      o.npts = r.npts;
+      o.pt_off = off;
+      o.freqs = r.d_freqs;
+      o.acc = r.d_acc;
+      off += r.npts;
+      v.push_back(o);
+    }
+    g->ndft[ph] = static_cast<int>(v.size());
+    g->dft_pts[ph] = off;
+    if (!v.empty()) {
+      int rc = upload_vec(g, reinterpret_cast<void**>(&g->d_dft[ph]), v.data(), v.size() * sizeof(DftRegionDev));
+      if (rc) return rc;
+    }
+  }
+  g->dirty_dft = false;
+  return FDTD_OK;
+}
+
+template <typename Args>
+void fill_common(fdtd_grid* g, Args& a) {
+  a.nx = g->n[0];
+  a.ny = g->n[1];
+  a.nz = g->n[2];
+  for (int x = 0; x < 3; x++) {
+    a.slab[x] = g->slab[x];
+    a.pml_axis[x] = (g->pml[x][0] > 0 || g->pml[x][1] > 0) ? 1 : 0;
+  }
+  a.ids = g->d_ids;
+  a.bids = g->d_bids;
+  a.bshift = g->bshift;
+  a.nbx = g->nbx;
+  a.nby = g->nby;
+  a.nsrc = static_cast<int>(g->srcs.size());
+  for (size_t s = 0; s < g->srcs.size(); s++) {
+    const SourceH& sh = g->srcs[s];
+    SourceDev& o = a.src[s];
+    o.cell = cell_index(g, sh.i, sh.j, sh.k);
+    o.comp = sh.comp;
+    o.target = sh.target;
+    o.nvals = static_cast<int>(sh.vals.size());
+    o.vals = sh.d_vals;
+    o.i = sh.i;
+    o.j = sh.j;
+    o.k = sh.k;
+  }
+  a.nplanes = static_cast<int>(g->planes.size());
+  for (size_t q = 0; q < g->planes.size(); q++) a.planes[q] = g->planes[q].dev;
+  for (size_t q = 0; q < g->auxes.size(); q++) {
+    const AuxH& ax = g->auxes[q];
+    a.aux[q].L = ax.L;
+    a.aux[q].Etab = ax.d_tab;
+    a.aux[q].Htab = ax.d_tab + ax.cap * ax.L;
+  }
+  a.ctrl = g->ctrl;
+}
+
+PlainArgs plain_args(fdtd_grid* g) {
+  PlainArgs a;
+  memset(&a, 0, sizeof(a));
+  fill_common(g, a);
+  a.dt = g->d.dt;
+  a.dx = g->d.dx;
+  for (int c = 0; c < 3; c++) {
+    a.D.f[c] = static_cast<double*>(g->D[c]);
+    a.E.f[c] = static_cast<double*>(g->E[c]);
+    a.B.f[c] = static_cast<double*>(g->B[c]);
+    a.H.f[c] = static_cast<double*>(g->H[c]);
+    for (int p = 0; p < kMaxPoles; p++) {
+      a.P[p].f[c] = static_cast<double*>(g->P[p][c]);
+      a.J[p].f[c] = static_cast<double*>(g->J[p][c]);
+    }
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int I = 0; I < 3; I++)
+      for (int J = 0; J < 3; J++) a.psi[ft][I][J] = static_cast<double*>(g->psi[ft][I][J]);
+  for (int ft = 0; ft < 2; ft++)
+    for (int x = 0; x < 3; x++) {
+      a.prof[ft][x].B = static_cast<const double*>(g->d_prof[ft][x][0]);
+      a.prof[ft][x].C = static_cast<const double*>(g->d_prof[ft][x][1]);
+      a.prof[ft][x].F = static_cast<const double*>(g->d_prof[ft][x][2]);
+      a.prof[ft][x].G = static_cast<const double*>(g->d_prof[ft][x][3]);
+    }
+  a.mats = static_cast<const MatF64*>(g->d_mats);
+  a.dispersive = g->max_poles;
+  return a;
+}
+
+FusedArgs fused_args(fdtd_grid* g) {
+  FusedArgs a;
+  memset(&a, 0, sizeof(a));
+  fill_common(g, a);
+  a.pitch = g->pitch;
+  a.ce = static_cast<float>(ce_of(g));
+  a.ch = static_cast<float>(ch_of(g));
+  for (int c = 0; c < 3; c++) {
+    a.E[c] = static_cast<float*>(g->E[c]);
+    a.H[c] = static_cast<float*>(g->H[c]);
+    for (int p = 0; p < 2; p++) {
+      a.P[p][c] = static_cast<float*>(g->P[p][c]);
+      a.J[p][c] = static_cast<float*>(g->J[p][c]);
+    }
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int I = 0; I < 3; I++)
+      for (int J = 0; J < 3; J++) a.psi[ft][I][J] = static_cast<float*>(g->psi[ft][I][J]);
+  for (int ft = 0; ft < 2; ft++)
+    for (int x = 0; x < 3; x++) {
+      a.prof[ft][x].B = static_cast<const float*>(g->d_prof[ft][x][0]);
+      a.prof[ft][x].C = static_cast<const float*>(g->d_prof[ft][x][1]);
+      a.prof[ft][x].F = static_cast<const float*>(g->d_prof[ft][x][2]);
+      a.prof[ft][x].G = static_cast<const float*>(g->d_prof[ft][x][3]);
+    }
+  a.mats = static_cast<const MatF32*>(g->d_mats);
+  a.max_poles = g->max_poles;
+  a.src_scale_d = static_cast<float>(1.0 / kEps0);
+  a.src_last = g->d_src_last;
+  a.dx = g->d.dx;
+  a.dt = g->d.dt;
+  a.eta = eta();
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out) {
+  if (!desc || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const fdtd_grid_desc& d = *desc;
+  if (d.mode != FDTD_TE && d.mode != FDTD_TM && d.mode != FDTD_THREED)
+    return fail(FDTD_ERR_UNSUPPORTED, "mode must be FDTD_TE, FDTD_TM or FDTD_THREED");
+  if (d.precision != FDTD_PLAIN_F64 && d.precision != FDTD_FUSED_F32)
+    return fail(FDTD_ERR_INVALID, "precision must be FDTD_PLAIN_F64 or FDTD_FUSED_F32");
+  if (d.nx < 3 || d.ny < 3 || (d.mode == FDTD_THREED ? d.nz < 3 : d.nz != 1))
+    return fail(FDTD_ERR_INVALID, "need nx, ny >= 3, and nz >= 3 in 3D or nz == 1 in 2D");
+  if (!(d.dx > 0) || !(d.dt > 0)) return fail(FDTD_ERR_INVALID, "dx and dt must be positive");
+  if (static_cast<long long>(d.nx) * d.ny * d.nz > (1LL << 40)) return fail(FDTD_ERR_INVALID, "grid too large");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "no CUDA device available");
+  }
+  if (d.device < 0 || d.device >= ndev) return fail(FDTD_ERR_INVALID, "bad device ordinal");
+  CK(cudaSetDevice(d.device));
+  fdtd_grid* g = new fdtd_grid();
+  g->d = d;
+  g->n[0] = d.nx;
+  g->n[1] = d.ny;
+  g->n[2] = d.nz;
+  g->f32 = d.precision == FDTD_FUSED_F32;
+  g->pitch = g->f32 ? ((d.nx + 31) / 32) * 32 : d.nx;
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete g;
+    return fail(FDTD_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  int rc = FDTD_OK;
+  const size_t fb = field_elems(g) * elem(g);
+  for (int c = 0; c < 3 && !rc; c++) {
+    if (hasE(d.mode, c)) {
+      rc = dalloc(g, &g->E[c], fb);
+      if (!rc && !g->f32) rc = dalloc(g, &g->D[c], fb);
+    }
+    if (!rc && hasH(d.mode, c)) {
+      rc = dalloc(g, &g->H[c], fb);
+      if (!rc && !g->f32) rc = dalloc(g, &g->B[c], fb);
+    }
+  }
+  if (!rc) rc = dalloc(g, reinterpret_cast<void**>(&g->ctrl), sizeof(Control));
+  if (!rc) rc = dalloc(g, reinterpret_cast<void**>(&g->d_flag), sizeof(int));
+  if (!rc) {
+    void* ptrs[6] = {g->E[0], g->E[1], g->E[2], g->H[0], g->H[1], g->H[2]};
+    rc = upload_vec(g, reinterpret_cast<void**>(&g->d_fieldptrs), ptrs, sizeof(ptrs));
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int a = 0; a < 3; a++) g->prof[ft][a].reset(g->n[a]);
+  if (!rc) rc = upload_profiles(g);
+  if (!rc) rc = alloc_psi(g);
+  if (!rc) {
+    fdtd_material vac;
+    memset(&vac, 0, sizeof(vac));
+    vac.kind = FDTD_VACUUM;
+    vac.eps_inf = 1.0;
+    vac.mu_r = 1.0;
+    g->mats.assign(1, vac);
+    rc = build_materials(g);
+  }
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (rc) {
+    fdtd_grid_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return FDTD_OK;
+}
+
+int fdtd_grid_destroy(fdtd_grid* g) {
+  if (!g) return FDTD_OK;
+  cudaSetDevice(g->d.device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  for (void* p : g->allocs) cudaFree(p);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+  return FDTD_OK;
+}
+
+int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (axis < 0 || axis >= dim_of(g) || side < 0 || side > 1) return fail(FDTD_ERR_INVALID, "bad axis or side");
+  if (ncells < 1) return fail(FDTD_ERR_INVALID, "ncells must be >= 1");
+  const int other = g->pml[axis][1 - side];
+  const int w = (ncells + 1) + (other > 0 ? other + 1 : 0);
+  if (w > g->n[axis] - 2) return fail(FDTD_ERR_INVALID, "CPML slabs overlap: grid too small for the widths");
+  CK(cudaSetDevice(g->d.device));
+  g->pml[axis][side] = ncells;
+  // regrade the whole axis in side order (min first), as the user loop would
+  for (int ft = 0; ft < 2; ft++) g->prof[ft][axis].reset(g->n[axis]);
+  for (int s = 0; s < 2; s++)
+    if (g->pml[axis][s] > 0)
+      grade(g->d.dx, g->d.dt, g->n[axis], g->pml[axis][s], s, g->prof[0][axis], g->prof[1][axis]);
+  int rc = upload_profiles(g);
+  if (rc) return rc;
+  return alloc_psi(g);
+}
+
+int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
+  if (!g || !mats) return fail(FDTD_ERR_INVALID, "null argument");
+  if (n < 1 || n > 65536) return fail(FDTD_ERR_INVALID, "material count must be 1..65536");
+  if (!g->f32 && n > 256) return fail(FDTD_ERR_UNSUPPORTED, "the FP64 plain method takes at most 256 materials");
+  for (int q = 0; q < n; q++) {
+    const fdtd_material& m = mats[q];
+    if (m.kind < FDTD_VACUUM || m.kind > FDTD_LORENTZ) return fail(FDTD_ERR_INVALID, "bad material kind");
+    if (m.kind == FDTD_DRUDE && m.npoles != 1) return fail(FDTD_ERR_INVALID, "Drude takes npoles = 1");
+    if (m.kind == FDTD_LORENTZ && (m.npoles < 1 || m.npoles > FDTD_MAX_POLES))
+      return fail(FDTD_ERR_INVALID, "Lorentz takes 1..4 poles");
+    if (m.kind != FDTD_VACUUM && !(m.eps_inf > 0)) return fail(FDTD_ERR_INVALID, "eps_inf must be positive");
+    if (!(m.mu_r > 0)) return fail(FDTD_ERR_INVALID, "mu_r must be positive");
+    if (g->f32 && m.mu_r != 1.0) return fail(FDTD_ERR_UNSUPPORTED, "the FP32 fused method takes mu_r = 1");
+  }
+  CK(cudaSetDevice(g->d.device));
+  g->mats.assign(mats, mats + n);
+  return build_materials(g);
+}
+
+int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) {
+  if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
+  const long long n = static_cast<long long>(g->n[0]) * g->n[1] * g->n[2];
+  std::vector<uint8_t> v(static_cast<size_t>(field_elems(g)), 0);
+  for (long long c = 0; c < n; c++) {
+    if (ids[c] >= g->mats.size()) return fail(FDTD_ERR_INVALID, "material id out of range of the material table");
+    const long long i = c % g->n[0], j = (c / g->n[0]) % g->n[1], k = c / (static_cast<long long>(g->n[0]) * g->n[1]);
+    v[(k * g->n[1] + j) * rowlen(g) + i] = ids[c];
+  }
+  CK(cudaSetDevice(g->d.device));
+  if (g->d_bids) {
+    dfree(g, g->d_bids);
+    g->d_bids = nullptr;
+  }
+  return upload_vec(g, reinterpret_cast<void**>(&g->d_ids), v.data(), v.size());
+}
+
+int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz) {
+  if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
+  if (block_shift < 0 || block_shift > 16) return fail(FDTD_ERR_INVALID, "bad block_shift");
+  for (int a = 0; a < 3; a++) {
+    const int nb = a == 0 ? nbx : (a == 1 ? nby : nbz);
+    if (nb < 1 || ((g->n[a] - 1) >> block_shift) >= nb) return fail(FDTD_ERR_INVALID, "block map does not cover the grid");
+  }
+  const size_t nb = static_cast<size_t>(nbx) * nby * nbz;
+  for (size_t q = 0; q < nb; q++)
+    if (ids[q] >= g->mats.size()) return fail(FDTD_ERR_INVALID, "material id out of range of the material table");
+  CK(cudaSetDevice(g->d.device));
+  if (g->d_ids) {
+    dfree(g, g->d_ids);
+    g->d_ids = nullptr;
+  }
+  g->bshift = block_shift;
+  g->nbx = nbx;
+  g->nby = nby;
+  g->nbz = nbz;
+  return upload_vec(g, reinterpret_cast<void**>(&g->d_bids), ids, nb * sizeof(uint16_t));
+}
+
+int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {
+  if (!g || (!vals && nvals > 0)) return fail(FDTD_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 2 || !hasE(g->d.mode, comp)) return fail(FDTD_ERR_INVALID, "component not in this mode");
+  if (target < 0 || target > 1) return fail(FDTD_ERR_INVALID, "target must be 0 (E) or 1 (D)");
+  if (!interior(g, i, j, k)) return fail(FDTD_ERR_INVALID, "source cell must be an interior cell");
+  if (g->srcs.size() >= static_cast<size_t>(kMaxSources)) return fail(FDTD_ERR_UNSUPPORTED, "too many sources");
+  if (nvals < 0) return fail(FDTD_ERR_INVALID, "nvals < 0");
+  CK(cudaSetDevice(g->d.device));
+  SourceH s;
+  s.comp = comp;
+  s.target = target;
+  s.i = i;
+  s.j = j;
+  s.k = k;
+  s.vals.assign(vals, vals + nvals);
+  int rc = upload_vec(g, reinterpret_cast<void**>(&s.d_vals), s.vals.data(),
+                      std::max<size_t>(1, s.vals.size()) * sizeof(double));
+  if (rc) return rc;
+  g->srcs.push_back(s);
+  if (g->d_src_last) dfree(g, g->d_src_last);
+  return dalloc(g, reinterpret_cast<void**>(&g->d_src_last), kMaxSources * sizeof(double));
+}
+
+int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const int* hi, const double* origin,
+                        const double* k, const double* pol_e, const double* pol_h, int aux_ncells,
+                        const double* aux_vals, int naux) {
+  if (!g || !lo || !hi || !origin || !k || !pol_e || !pol_h || (!aux_vals && naux > 0))
+    return fail(FDTD_ERR_INVALID, "null argument");
+  const int dim = dim_of(g);
+  if (axis < 0 || axis >= dim || orient < 0 || orient > 1) return fail(FDTD_ERR_INVALID, "bad axis or orientation");
+  if (aux_ncells < 1 || naux < 0) return fail(FDTD_ERR_INVALID, "bad aux grid size");
+  if (g->planes.size() >= static_cast<size_t>(kMaxPlanes)) return fail(FDTD_ERR_UNSUPPORTED, "too many TFSF planes");
+  for (int d = 0; d < 3; d++) {
+    if (lo[d] > hi[d]) return fail(FDTD_ERR_INVALID, "empty TFSF plane");
+    if (d < dim && (lo[d] < 1 || hi[d] > g->n[d] - 2)) return fail(FDTD_ERR_INVALID, "TFSF plane outside the interior");
+    if (d >= dim && (lo[d] != 0 || hi[d] != 0)) return fail(FDTD_ERR_INVALID, "2D TFSF plane needs k range 0..0");
+  }
+  PlaneDev p;
+  memset(&p, 0, sizeof(p));
+  p.axis = axis;
+  for (int d = 0; d < 3; d++) {
+    p.lo[d] = lo[d];
+    p.hi[d] = hi[d];
+    p.origin[d] = origin[d];
+    p.pol_e[d] = pol_e[d];
+    p.pol_h[d] = pol_h[d];
+  }
+  // TFSFPlane constructor (Source.hpp:556-570): unit normal and wave vector
+  p.normal[axis] = orient == 1 ? 1 : -1;
+  double N = 0;
+  for (int d = 0; d < dim; d++) N += p.normal[d] * p.normal[d];
+  N = std::sqrt(N);
+  for (int d = 0; d < dim; d++) p.normal[d] /= N;
+  double K = 0;
+  for (int d = 0; d < dim; d++) K += k[d] * k[d];
+  K = std::sqrt(K);
+  if (!(K > 0)) return fail(FDTD_ERR_INVALID, "zero wave vector");
+  for (int d = 0; d < dim; d++) p.k[d] = k[d] / K;
+  const int L = aux_ncells + 2 * kAuxNpml + 20;
+  // every interpolation the corrections make must land inside the aux grid
+  // (Aux1D::interpolateE/H have no bounds check)
+  for (int corner = 0; corner < 8; corner++) {
+    int idx[3];
+    for (int d = 0; d < 3; d++) idx[d] = (corner >> d & 1) ? hi[d] : lo[d];
+    for (int ft = 0; ft < 2; ft++)
+      for (int Kc = 0; Kc < 3; Kc++) {
+        double proj = 0;
+        for (int d = 0; d < dim; d++) {
+          const double off = ft == 0 ? (d == Kc ? -0.5 : 0.0) : (d == Kc ? 0.0 : -0.5);
+          proj += p.k[d] * ((static_cast<double>(idx[d]) - origin[d]) * g->d.dx + off * g->d.dx);
+        }
+        const double nd = static_cast<double>(L) / 2.0 + proj / g->d.dx - (ft == 0 ? 0.5 : 0.0);
+        if (!(nd >= 0.0) || std::floor(nd) + 1 > L - 1)
+          return fail(FDTD_ERR_INVALID, "TFSF plane projects outside its aux grid: raise aux_ncells");
+      }
+  }
+  CK(cudaSetDevice(g->d.device));
+  // planes with the same aux grid share one
+  int aux = -1;
+  std::vector<double> vals(aux_vals, aux_vals + naux);
+  for (size_t q = 0; q < g->auxes.size(); q++)
+    if (g->auxes[q].ncells == aux_ncells && g->auxes[q].vals == vals) aux = static_cast<int>(q);
+  if (aux < 0) {
+    if (g->t != 0) return fail(FDTD_ERR_UNSUPPORTED, "a new aux grid must be added before the first step");
+    AuxH a;
+    a.ncells = aux_ncells;
+    a.L = L;
+    a.vals = vals;
+    int rc = build_aux(g, a);
+    if (rc) return rc;
+    g->auxes.push_back(a);
+    aux = static_cast<int>(g->auxes.size()) - 1;
+  }
+  p.aux = aux;
+  PlaneH ph;
+  ph.dev = p;
+  g->planes.push_back(ph);
+  return FDTD_OK;
+}
+
+int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) {
+  if (!g || !lo || !hi || !freqs || !handle) return fail(FDTD_ERR_INVALID, "null argument");
+  if (comp < 0 || comp > 5) return fail(FDTD_ERR_INVALID, "comp must be 0..5");
+  if (comp < 3 ? !hasE(g->d.mode, comp) : !hasH(g->d.mode, comp - 3))
+    return fail(FDTD_ERR_INVALID, "component not in this mode");
+  if (nf < 1) return fail(FDTD_ERR_INVALID, "nf must be >= 1");
+  DftH r;
+  r.comp = comp;
+  r.nf = nf;
+  r.npts = 1;
+  for (int d = 0; d < 3; d++) {
+    if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return fail(FDTD_ERR_INVALID, "DFT box outside the grid");
+    r.lo[d] = lo[d];
+    r.hi[d] = hi[d];
+    r.npts *= hi[d] - lo[d] + 1;
+  }
+  CK(cudaSetDevice(g->d.device));
+  r.freqs.assign(freqs, freqs + nf);
+  int rc = upload_vec(g, reinterpret_cast<void**>(&r.d_freqs), freqs, nf * sizeof(double));
+  if (rc) return rc;
+  rc = dalloc(g, reinterpret_cast<void**>(&r.d_acc), static_cast<size_t>(nf) * r.npts * 2 * sizeof(double));
+  if (rc) return rc;
+  g->dfts.push_back(r);
+  *handle = static_cast<int>(g->dfts.size()) - 1;
+  g->dirty_dft = true;
+  return FDTD_OK;
+}
+
+int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints) {
+  if (!g || !npoints || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
+    return fail(FDTD_ERR_INVALID, "bad DFT handle");
+  *npoints = g->dfts[handle].npts;
+  return FDTD_OK;
+}
+
+int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
+  if (!g || !out || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
+    return fail(FDTD_ERR_INVALID, "bad DFT handle");
+  CK(cudaSetDevice(g->d.device));
+  const DftH& r = g->dfts[handle];
+  const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
+  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaMemcpy(out, r.d_acc, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (g->f32 && r.comp >= 3) {
+    const double s = 1.0 / eta();  // stored H is eta*H
+    for (size_t q = 0; q < n; q++) out[q] *= s;
+  }
+  return FDTD_OK;
+}
+
+int fdtd_step(fdtd_grid* g, int nsteps, void* stream) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
+  if (nsteps == 0) return FDTD_OK;
+  CK(cudaSetDevice(g->d.device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  if (s != g->stream) {
+    // order the caller's stream after any set-up work on ours
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, g->stream));
+    CK(cudaStreamWaitEvent(s, ev, 0));
+    CK(cudaEventDestroy(ev));
+  }
+  if (g->dirty_dft) {
+    int rc = rebuild_dft(g);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(g->stream));
+  }
+  // TFSF: precompute the aux grids' Ez/Hy for this chunk of steps
+  for (auto& a : g->auxes) {
+    if (a.cap < nsteps + 1) {
+      if (a.d_tab) dfree(g, a.d_tab);
+      a.d_tab = nullptr;
+      int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(nsteps + 1) * a.L * sizeof(double));
+      if (rc) return rc;
+      a.cap = nsteps + 1;
+      CK(cudaStreamSynchronize(g->stream));
+    }
+    double* st = a.d_state;
+    const int L = a.L;
+    g->launches += launch_aux_precompute(L, g->d.dt, g->d.dx, st, st + L, st + 2 * L, st + 3 * L, st + 4 * L,
+                                         st + 5 * L, a.d_coef, a.d_vals, static_cast<int>(a.vals.size()), g->t,
+                                         nsteps, a.d_tab, a.d_tab + a.cap * L, s);
+  }
+  if (!g->auxes.empty()) {
+    Control c{};
+    c.t = g->t;
+    c.t0 = g->t;
+    CK(cudaMemcpyAsync(g->ctrl, &c, sizeof(long long) * 2, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // the host value must outlive the copy
+  }
+  const int mode = g->d.mode;
+  const void* const* fE = reinterpret_cast<const void* const*>(g->d_fieldptrs);
+  const void* const* fH = fE + 3;
+  if (g->f32) {
+    FusedArgs a = fused_args(g);
+    for (int q = 0; q < nsteps; q++) {
+      g->launches += launch_fused_e(mode, a, s);
+      g->launches += launch_dft(0, 1, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1], g->pitch, g->ctrl, s);
+      g->launches += launch_fused_h(mode, a, s);
+      g->launches += launch_dft(1, 1, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1], g->pitch, g->ctrl, s);
+      g->launches += launch_step_advance(g->ctrl, s);
+    }
+  } else {
+    PlainArgs a = plain_args(g);
+    for (int q = 0; q < nsteps; q++) {
+      g->launches += launch_plain_e(mode, a, s);
+      g->launches += launch_dft(0, 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1], g->n[0], g->ctrl, s);
+      g->launches += launch_plain_h(mode, a, s);
+      g->launches += launch_dft(1, 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1], g->n[0], g->ctrl, s);
+      g->launches += launch_step_advance(g->ctrl, s);
+    }
+  }
+  CK(cudaGetLastError());
+  g->t += nsteps;
+  return FDTD_OK;
+}
+
+int fdtd_synchronize(fdtd_grid* g) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  CK(cudaSetDevice(g->d.device));
+  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaDeviceSynchronize());
+  return FDTD_OK;
+}
+
+// which -> (device pointer, scale to SI, element layout)
+static int locate(fdtd_grid* g, int which, void** p, double* scale, int* psi_axis) {
+  *p = nullptr;
+  *scale = 1.0;
+  *psi_axis = -1;
+  const double eps0 = kEps0, dt = g->d.dt;
+  if (which < 0) return fail(FDTD_ERR_INVALID, "bad field selector");
+  if (which < 3) {
+    if (g->f32) return fail(FDTD_ERR_UNSUPPORTED, "the fused method does not store D");
+    *p = g->D[which];
+  } else if (which < 6) {
+    *p = g->E[which - 3];
+  } else if (which < 9) {
+    if (g->f32) return fail(FDTD_ERR_UNSUPPORTED, "the fused method does not store B");
+    *p = g->B[which - 6];
+  } else if (which < 12) {
+    *p = g->H[which - 9];
+    if (g->f32) *scale = 1.0 / eta();
+  } else if (which < 18 || which >= 36) {
+    int pole = 0, r = 0;
+    if (which < 18) r = which - 12;
+    else {
+      pole = 1 + (which - 36) / 6;
+      r = (which - 36) % 6;
+    }
+    if (pole >= kMaxPoles) return fail(FDTD_ERR_INVALID, "bad field selector");
+    *p = r < 3 ? g->P[pole][r] : g->J[pole][r - 3];
+    if (g->f32) *scale = r < 3 ? eps0 : eps0 / dt;
+  } else {
+    const int q = which - 18, ft = q / 9, I = (q / 3) % 3, J = q % 3;
+    *p = g->psi[ft][I][J];
+    *psi_axis = J;
+    if (g->f32) *scale = ft == 0 ? eps0 / dt : kMu0 / (eta() * dt);
+  }
+  return FDTD_OK;
+}
+
+int fdtd_download(fdtd_grid* g, int which, double* host) {
+  if (!g || !host) return fail(FDTD_ERR_INVALID, "null argument");
+  void* p;
+  double scale;
+  int J;
+  int rc = locate(g, which, &p, &scale, &J);
+  if (rc) return rc;
+  CK(cudaSetDevice(g->d.device));
+  CK(cudaStreamSynchronize(g->stream));
+  const long long nx = g->n[0], ny = g->n[1], nz = g->n[2];
+  const long long ncell = nx * ny * nz;
+  if (!p) {
+    memset(host, 0, ncell * sizeof(double));
+    return FDTD_OK;
+  }
+  long long cnt = field_elems(g);
+  if (J >= 0) {
+    if (J == 0) cnt = nz * ny * g->slab[0].W;
+    else if (J == 1) cnt = nz * g->slab[1].W * rowlen(g);
+    else cnt = static_cast<long long>(g->slab[2].W) * ny * rowlen(g);
+  }
+  std::vector<char> buf(cnt * elem(g));
+  CK(cudaMemcpy(buf.data(), p, buf.size(), cudaMemcpyDeviceToHost));
+  auto val = [&](long long q) -> double {
+    return g->f32 ? static_cast<double>(reinterpret_cast<float*>(buf.data())[q])
+                  : reinterpret_cast<double*>(buf.data())[q];
+  };
+  const long long rl = rowlen(g);
+  for (long long k = 0; k < nz; k++)
+    for (long long j = 0; j < ny; j++)
+      for (long long i = 0; i < nx; i++) {
+        const long long o = (k * ny + j) * nx + i;
+        if (J < 0) {
+          host[o] = val((k * ny + j) * rl + i) * scale;
+        } else {
+          const int idx[3] = {static_cast<int>(i), static_cast<int>(j), static_cast<int>(k)};
+          const bool in = interior(g, idx[0], idx[1], idx[2]);
+          const int s = in ? slab_index(g->slab[J], idx[J]) : -1;
+          if (s < 0) {
+            host[o] = 0.0;
+            continue;
+          }
+          long long q;
+          if (J == 0) q = (k * ny + j) * g->slab[0].W + s;
+          else if (J == 1) q = (k * g->slab[1].W + s) * rl + i;
+          else q = (static_cast<long long>(s) * ny + j) * rl + i;
+          host[o] = val(q) * scale;
+        }
+      }
+  return FDTD_OK;
+}
+
+int fdtd_upload(fdtd_grid* g, int which, const double* host) {
+  if (!g || !host) return fail(FDTD_ERR_INVALID, "null argument");
+  void* p;
+  double scale;
+  int J;
+  int rc = locate(g, which, &p, &scale, &J);
+  if (rc) return rc;
+  if (!p) return fail(FDTD_ERR_UNSUPPORTED, "field not stored for this grid");
+  if (J >= 0) return fail(FDTD_ERR_UNSUPPORTED, "CPML integrators cannot be uploaded");
+  CK(cudaSetDevice(g->d.device));
+  CK(cudaStreamSynchronize(g->stream));
+  const long long nx = g->n[0], ny = g->n[1], nz = g->n[2], rl = rowlen(g);
+  std::vector<char> buf(field_elems(g) * elem(g), 0);
+  for (long long k = 0; k < nz; k++)
+    for (long long j = 0; j < ny; j++)
+      for (long long i = 0; i < nx; i++) {
+        const double v = host[(k * ny + j) * nx + i] / scale;
+        const long long q = (k * ny + j) * rl + i;
+        if (g->f32) reinterpret_cast<float*>(buf.data())[q] = static_cast<float>(v);
+        else reinterpret_cast<double*>(buf.data())[q] = v;
+      }
+  CK(cudaMemcpy(p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+  return FDTD_OK;
+}
+
+int fdtd_check_finite(fdtd_grid* g) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  CK(cudaSetDevice(g->d.device));
+  CK(cudaMemsetAsync(g->d_flag, 0, sizeof(int), g->stream));
+  std::vector<void*> arrs;
+  for (int c = 0; c < 3; c++) {
+    arrs.push_back(g->E[c]);
+    arrs.push_back(g->H[c]);
+    arrs.push_back(g->D[c]);
+    arrs.push_back(g->B[c]);
+  }
+  for (void* p : arrs)
+    if (p) g->launches += launch_finite_check(p, field_elems(g), g->f32 ? 1 : 0, g->d_flag, g->stream);
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, g->d_flag, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  if (flag) return fail(FDTD_ERR_NONFINITE, "a field holds NaN or Inf");
+  return FDTD_OK;
+}
+
+int fdtd_get_step(fdtd_grid* g, long long* step) {
+  if (!g || !step) return fail(FDTD_ERR_INVALID, "null argument");
+  *step = g->t;
+  return FDTD_OK;
+}
+
+int fdtd_launch_count(fdtd_grid* g, long long* count) {
+  if (!g || !count) return fail(FDTD_ERR_INVALID, "null argument");
+  *count = g->launches;
+  return FDTD_OK;
+}
+
+int fdtd_memory_bytes(fdtd_grid* g, long long* bytes) {
+  if (!g || !bytes) return fail(FDTD_ERR_INVALID, "null argument");
+  *bytes = g->bytes;
+  return FDTD_OK;
+}
+
+}  // extern "C"

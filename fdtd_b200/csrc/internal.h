@@ -1,0 +1,176 @@
+// Internal declarations shared by the fdtd_b200 CUDA sources.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fdtdb {
+
+constexpr int kTEM = 0, kTE = 1, kTM = 2, kThreeD = 3;
+constexpr int kMaxPoles = 4;
+constexpr int kMaxPlanes = 12;
+constexpr int kMaxSources = 16;
+constexpr int kAuxNpml = 15;  // Aux1D::mNPML (include/Source.hpp:362)
+
+// include/FDTDConstants.hpp:394-398
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kEps0 = 8.854e-12;
+constexpr double kMu0 = kPi * 4.0e-7;
+
+// Which E / H components a mode carries (FieldComponents, FDTDConstants.hpp:844-874)
+__host__ __device__ constexpr bool hasE(int mode, int c) {
+  return mode == kThreeD || (mode == kTE && c < 2) || (mode == kTM && c == 2);
+}
+__host__ __device__ constexpr bool hasH(int mode, int c) {
+  return mode == kThreeD || (mode == kTE && c == 2) || (mode == kTM && c < 2);
+}
+// LeviCivita<I,J,K>::value (FDTDConstants.hpp:602-637)
+__host__ __device__ constexpr int levi(int I, int J, int K) {
+  return ((I == 0 && J == 1 && K == 2) || (I == 1 && J == 2 && K == 0) || (I == 2 && J == 0 && K == 1)) ? 1
+         : ((I == 2 && J == 1 && K == 0) || (I == 0 && J == 2 && K == 1) || (I == 1 && J == 0 && K == 2)) ? -1
+                                                                                                            : 0;
+}
+__host__ __device__ constexpr int third(int I, int J) { return 3 - I - J; }
+// d1 of YeeUpdate::update_all (YeeUpdates.hpp:397)
+__host__ __device__ constexpr int dir1(int I) { return I == 0 ? 1 : (I == 1 ? 2 : 0); }
+
+// CPML slab of one axis: lo slab = cells 1..wlo, hi slab = hi0..hi0+whi-1
+struct Slab {
+  int wlo, hi0, W;
+};
+__host__ __device__ inline int slab_index(const Slab& s, int i) {
+  if (i <= s.wlo) return i - 1;
+  if (i >= s.hi0) return s.wlo + (i - s.hi0);
+  return -1;
+}
+
+// 1D CPML coefficients of one (field type, axis)
+template <typename R>
+struct Prof {
+  const R* B;    // exp(-nu dt)
+  const R* C;    // plain: C/dx; fused: scaled C
+  const R* F;    // plain: F/dx; fused: scaled F
+  const R* G;
+};
+
+// Material coefficients for the FP64 plain method (reference operation order)
+struct MatF64 {
+  int kind, npoles;
+  double den_e;  // eps_inf * eps0
+  double den_h;  // mu_r * mu0
+  // Drude: c1 = 1-b, c2 = 1+b, c3 = ((w*w)/dt)*eps0
+  // Lorentz: c1 = bm/b, c2 = ((q*delta)*eps0), c3 = q = (freq*w)/b
+  double c1[kMaxPoles], c2[kMaxPoles], c3[kMaxPoles];
+};
+
+// Material coefficients for the FP32 fused method (scaled variables)
+struct MatF32 {
+  float inv_eps;  // 1/eps_inf
+  int npoles;     // 0: non-dispersive; Drude: -1 (one J only)
+  float a[2], b[2], c[2];
+  // Drude: Jt' = a*Jt + b*E
+  // Lorentz pole: Pt' = Pt + Jt; Jt' = a*Jt + b*E - c*Pt'
+};
+
+struct SourceDev {
+  long long cell;  // linear index into the field arrays
+  int comp, target, nvals;
+  const double* vals;
+  int i, j, k;
+};
+
+struct PlaneDev {
+  int axis, aux;
+  int lo[3], hi[3];
+  double normal[3], k[3], pol_e[3], pol_h[3], origin[3];
+};
+
+struct AuxTab {
+  int L;
+  const double* Etab;  // [rows][L]: Ez after (t0 + row) aux steps
+  const double* Htab;  // [rows][L]: Hy after (t0 + row) aux steps
+};
+
+struct Control {
+  long long t;   // steps taken
+  long long t0;  // first step of the current aux table chunk
+  unsigned int done_blocks;
+  int error;
+};
+
+template <typename R>
+struct FieldSet {
+  R* f[3];
+};
+
+struct PlainArgs {
+  int nx, ny, nz;
+  double dt, dx;
+  FieldSet<double> D, E, B, H;
+  FieldSet<double> P[kMaxPoles], J[kMaxPoles];
+  double* psi[2][3][3];
+  Prof<double> prof[2][3];
+  Slab slab[3];
+  int pml_axis[3];
+  const uint8_t* ids;
+  const uint16_t* bids;
+  int bshift, nbx, nby;
+  const MatF64* mats;
+  int dispersive;
+  int nsrc;
+  SourceDev src[kMaxSources];
+  int nplanes;
+  PlaneDev planes[kMaxPlanes];
+  AuxTab aux[kMaxPlanes];
+  Control* ctrl;
+};
+
+struct FusedArgs {
+  int nx, ny, nz, pitch;
+  float ce, ch;  // dt/(eps0 eta dx), eta dt/(mu0 dx)
+  float* E[3];
+  float* H[3];   // eta * H
+  float* P[2][3];
+  float* J[2][3];
+  float* psi[2][3][3];
+  Prof<float> prof[2][3];
+  Slab slab[3];
+  int pml_axis[3];
+  const uint8_t* ids;
+  const uint16_t* bids;
+  int bshift, nbx, nby;
+  const MatF32* mats;
+  int max_poles;  // 0 none, -1 Drude only, 1..2 Lorentz
+  int nsrc;
+  SourceDev src[kMaxSources];
+  float src_scale_d;  // 1/eps0 for D-target sources
+  double* src_last;   // per source: value added to E at the previous step
+  int nplanes;
+  PlaneDev planes[kMaxPlanes];
+  AuxTab aux[kMaxPlanes];
+  double dx, dt;
+  double eta;
+  Control* ctrl;
+};
+
+struct DftRegionDev {
+  int comp, nf;
+  int lo[3], ext[3];
+  long long npts, pt_off;
+  const double* freqs;
+  double* acc;  // [nf][npts][2]
+};
+
+// kernel launchers (stream-ordered); each returns the number of launches
+int launch_plain_e(int mode, const PlainArgs& a, cudaStream_t s);
+int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
+int launch_fused_e(int mode, const FusedArgs& a, cudaStream_t s);
+int launch_fused_h(int mode, const FusedArgs& a, cudaStream_t s);
+int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, double* By, double* Hy,
+                          double* psiE, double* psiH, const double* coef, const double* vals, int nvals,
+                          long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);
+int launch_dft(int phase, int precision, const DftRegionDev* regions, int nreg, long long total_pts,
+               const void* const* fields, int nx, int ny, int pitch, const Control* ctrl, cudaStream_t s);
+int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
+int launch_step_advance(Control* ctrl, cudaStream_t s);
+
+}  // namespace fdtdb

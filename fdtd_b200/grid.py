@@ -1,0 +1,263 @@
+"""ctypes binding of the fdtd_b200 C ABI (include/fdtd_b200.h).
+
+``Grid`` owns one fdtd_grid handle. Every call goes through the CUDA library
+libfdtd_b200.so built in-tree by ``fdtd_b200.build_lib``; there is no CPU path:
+if the library or a GPU is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import problem as P
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfdtd_b200.so")
+
+PLAIN_F64 = 0
+FUSED_F32 = 1
+PRECISIONS = {"f64": PLAIN_F64, "plain": PLAIN_F64, "f32": FUSED_F32, "fused": FUSED_F32}
+
+FIELD_NAMES = ["Dx", "Dy", "Dz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Hx", "Hy", "Hz",
+               "Px", "Py", "Pz", "Jx", "Jy", "Jz"]
+PSI_NAMES = [f"psi{'EH'[f]}{'xyz'[i]}{'xyz'[j]}" for f in range(2) for i in range(3) for j in range(3)]
+ALL_NAMES = FIELD_NAMES + PSI_NAMES
+
+STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_ERR_UNSUPPORTED",
+          -4: "FDTD_ERR_NOMEM", -5: "FDTD_ERR_NONFINITE", -6: "FDTD_ERR_TIMEOUT"}
+
+# every symbol include/fdtd_b200.h declares
+EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
+           "fdtd_set_material_blocks", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
+           "fdtd_last_error_string"]
+
+
+class FdtdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("precision", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("dx", ctypes.c_double), ("dt", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+class MaterialC(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("npoles", ctypes.c_int), ("eps_inf", ctypes.c_double),
+                ("mu_r", ctypes.c_double), ("delta_eps", ctypes.c_double * 4),
+                ("freq", ctypes.c_double * 4), ("gamma", ctypes.c_double * 4)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libfdtd_b200.so and declare its signatures. Raises if missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is not built: run `python -m fdtd_b200.build_lib` (there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    vp, ip, dp, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    sig = {
+        "fdtd_grid_create": [ctypes.POINTER(GridDesc), ctypes.POINTER(vp)],
+        "fdtd_grid_destroy": [vp],
+        "fdtd_set_pml": [vp, i, i, i],
+        "fdtd_set_materials": [vp, ctypes.POINTER(MaterialC), i],
+        "fdtd_set_material_ids": [vp, vp],
+        "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
+        "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
+        "fdtd_add_tfsf_plane": [vp, i, i, ip, ip, dp, dp, dp, dp, i, dp, i],
+        "fdtd_add_dft": [vp, i, ip, ip, dp, i, ip],
+        "fdtd_dft_npoints": [vp, i, llp],
+        "fdtd_dft_read": [vp, i, dp],
+        "fdtd_step": [vp, i, vp],
+        "fdtd_synchronize": [vp],
+        "fdtd_download": [vp, i, dp],
+        "fdtd_upload": [vp, i, dp],
+        "fdtd_check_finite": [vp],
+        "fdtd_get_step": [vp, llp],
+        "fdtd_launch_count": [vp, llp],
+        "fdtd_memory_bytes": [vp, llp],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    L.fdtd_last_error_string.restype = ctypes.c_char_p
+    L.fdtd_last_error_string.argtypes = []
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise FdtdError(rc, load_library().fdtd_last_error_string().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(seq):
+    return (ctypes.c_int * len(seq))(*[int(x) for x in seq])
+
+
+def material_struct(m: P.Material) -> MaterialC:
+    s = MaterialC()
+    s.kind = m.kind
+    s.npoles = len(m.poles)
+    s.eps_inf = m.eps_inf
+    s.mu_r = m.mu_r
+    for q, (de, f, g) in enumerate(m.poles):
+        s.delta_eps[q] = de
+        s.freq[q] = f
+        s.gamma[q] = g
+    return s
+
+
+class Grid:
+    """One grid on one GPU, driven through the C ABI."""
+
+    def __init__(self, mode: int, shape: Sequence[int], dx: float, dt: float, precision="f64", device: int = 0):
+        L = load_library()
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        nx, ny, nz = shape
+        d = GridDesc(mode, prec, nx, ny, nz, dx, dt, device)
+        h = ctypes.c_void_p()
+        _check(L.fdtd_grid_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        self.mode, self.shape, self.dx, self.dt, self.precision = mode, (nx, ny, nz), dx, dt, prec
+        self.dft_meta = []
+
+    # ------------------------------------------------------------ set-up
+    def set_pml(self, axis: int, side: int, ncells: int) -> None:
+        _check(load_library().fdtd_set_pml(self.h, axis, side, ncells))
+
+    def set_materials(self, mats) -> None:
+        arr = (MaterialC * len(mats))(*[material_struct(m) for m in mats])
+        _check(load_library().fdtd_set_materials(self.h, arr, len(mats)))
+
+    def set_material_ids(self, ids: np.ndarray) -> None:
+        a = np.ascontiguousarray(ids, dtype=np.uint8)
+        assert a.size == self.shape[0] * self.shape[1] * self.shape[2]
+        _check(load_library().fdtd_set_material_ids(self.h, a.ctypes.data))
+
+    def set_material_blocks(self, shift: int, bids: np.ndarray) -> None:
+        a = np.ascontiguousarray(bids, dtype=np.uint16)
+        nbz, nby, nbx = a.shape
+        _check(load_library().fdtd_set_material_blocks(self.h, shift, a.ctypes.data, nbx, nby, nbz))
+
+    def add_source(self, comp: int, pos, values, target: str = "E") -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(load_library().fdtd_add_source(self.h, comp, 0 if target == "E" else 1, *pos, _dp(v), len(v)))
+
+    def add_tfsf_plane(self, axis, orient, lo, hi, origin, k, pol_e, pol_h, aux_ncells, aux_values) -> None:
+        av = np.ascontiguousarray(aux_values, dtype=np.float64)
+        f = lambda x: np.ascontiguousarray(x, dtype=np.float64)
+        _check(load_library().fdtd_add_tfsf_plane(self.h, axis, orient, _ip(lo), _ip(hi), _dp(f(origin)), _dp(f(k)),
+                                                  _dp(f(pol_e)), _dp(f(pol_h)), aux_ncells, _dp(av), len(av)))
+
+    def add_dft(self, comp: int, lo, hi, freqs) -> int:
+        fr = np.ascontiguousarray(freqs, dtype=np.float64)
+        h = ctypes.c_int()
+        _check(load_library().fdtd_add_dft(self.h, comp, _ip(lo), _ip(hi), _dp(fr), len(fr), ctypes.byref(h)))
+        self.dft_meta.append(len(fr))
+        return h.value
+
+    @classmethod
+    def from_problem(cls, p: P.Problem, precision="f64", device: int = 0) -> "Grid":
+        g = cls(p.mode, p.shape, p.dx, p.dt, precision, device)
+        for (a, s), n in sorted(p.pml.items()):
+            g.set_pml(a, s, n)
+        g.set_materials(p.materials)
+        if p.ids is not None:
+            g.set_material_ids(p.ids)
+        elif p.block_ids is not None:
+            g.set_material_blocks(p.block_shift, p.block_ids)
+        for s in p.sources:
+            g.add_source(s.comp, s.pos, s.values, s.target)
+        if p.tfsf is not None:
+            t = p.tfsf
+            for pl in t.planes:
+                g.add_tfsf_plane(pl.axis, pl.orient, pl.lo, pl.hi, t.origin, t.k, t.pol_e, t.pol_h,
+                                 t.aux_ncells, t.aux_values)
+        g.dft_handles = [g.add_dft(r.comp, r.lo, r.hi, r.freqs) for r in p.dfts]
+        return g
+
+    # ------------------------------------------------------------ run
+    def step(self, n: int, stream: Optional[int] = None) -> None:
+        _check(load_library().fdtd_step(self.h, int(n), ctypes.c_void_p(stream) if stream else None))
+
+    def synchronize(self) -> None:
+        _check(load_library().fdtd_synchronize(self.h))
+
+    # ------------------------------------------------------------ read back
+    def get(self, name: str) -> np.ndarray:
+        which = ALL_NAMES.index(name) if isinstance(name, str) and name in ALL_NAMES else int(name)
+        nx, ny, nz = self.shape
+        out = np.empty(nx * ny * nz, dtype=np.float64)
+        _check(load_library().fdtd_download(self.h, which, _dp(out)))
+        return out.reshape(nz, ny, nx)
+
+    def get_pole(self, pole: int, name: str) -> np.ndarray:
+        if pole == 0:
+            return self.get(name)
+        r = ["Px", "Py", "Pz", "Jx", "Jy", "Jz"].index(name)
+        return self.get(str(36 + (pole - 1) * 6 + r))
+
+    def set(self, name: str, arr: np.ndarray) -> None:
+        which = ALL_NAMES.index(name)
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        _check(load_library().fdtd_upload(self.h, which, _dp(a)))
+
+    def dft(self, handle: int) -> np.ndarray:
+        """[nf][npoints] complex"""
+        L = load_library()
+        n = ctypes.c_longlong()
+        _check(L.fdtd_dft_npoints(self.h, handle, ctypes.byref(n)))
+        nf = self.dft_meta[handle]
+        out = np.empty(nf * n.value * 2, dtype=np.float64)
+        _check(L.fdtd_dft_read(self.h, handle, _dp(out)))
+        out = out.reshape(nf, n.value, 2)
+        return out[..., 0] + 1j * out[..., 1]
+
+    def check_finite(self) -> None:
+        _check(load_library().fdtd_check_finite(self.h))
+
+    @property
+    def step_count(self) -> int:
+        v = ctypes.c_longlong()
+        _check(load_library().fdtd_get_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        _check(load_library().fdtd_launch_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def memory_bytes(self) -> int:
+        v = ctypes.c_longlong()
+        _check(load_library().fdtd_memory_bytes(self.h, ctypes.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            load_library().fdtd_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

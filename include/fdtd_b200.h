@@ -1,0 +1,163 @@
+/* fdtd_b200: C ABI of the B200 (sm_100a) implementation of pederson/fdtd's
+ * time-step hot path.
+ *
+ * The reference has no ABI: a user owns an AoS container of YeeCell objects
+ * and applies compile-time update functors to it in a time loop
+ * (tests/testTM.cpp:102-113). Each entry point below replaces one piece of
+ * that loop, for a whole grid held as SoA arrays in device memory:
+ *
+ *   reference                                              here
+ *   ---------------------------------------------------    ----------------------------
+ *   container of YeeCell<YeeFields<Mode,..>, ..>            fdtd_grid_create
+ *     (include/YeeCell.hpp:74-97, YeeFields.hpp:37-174)
+ *   PMLParameterModel(dx) + NewPML::setPMLParameters per     fdtd_set_pml
+ *     cell (PML.hpp:84-102, :368-393; testTM.cpp:44-71)
+ *   Vacuum/Constant/Drude/LorentzUpdate functor per cell     fdtd_set_materials,
+ *     (DispersiveMaterials.hpp:489-497, :881-884,            fdtd_set_material_ids,
+ *     :1208-1211; MaterialMap.hpp:45-70)                     fdtd_set_material_blocks
+ *   SoftSource<Signal,Cell,GetField<F>>::apply(t)            fdtd_add_source
+ *     (Source.hpp:183-261)
+ *   make_tfsf_plane + Aux1D (Source.hpp:280-634)             fdtd_add_tfsf_plane
+ *   DataCapture / VolumeData (DataCapture.hpp:23-191; a      fdtd_add_dft, fdtd_dft_read
+ *     stub in the reference: no Fourier capture exists)
+ *   one pass of the user loop: YeeUpdate<Mode,D*>,           fdtd_step
+ *     UpdatePML<Mode,Electric,d>, material E, sources,
+ *     YeeUpdate<Mode,B*>, UpdatePML<Mode,Magnetic,d>,
+ *     material H (YeeUpdates.hpp:343-405, PML.hpp:296-355)
+ *   reading cell.Ez() etc.                                   fdtd_download / fdtd_upload
+ *
+ * Ownership: the grid handle owns all device memory; host pointers passed in
+ * are read during the call only. Errors: every call returns FDTD_OK (0) or a
+ * negative fdtd_status; fdtd_last_error_string() describes the last error of
+ * the calling thread. Threading: one handle per host thread; work is ordered
+ * on the stream given to fdtd_step (NULL = the handle's own stream). */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdtd_grid fdtd_grid;
+
+/* modes: the reference's Detail::EMMode order (FDTDConstants.hpp:410-415) */
+enum { FDTD_TEM = 0, FDTD_TE = 1, FDTD_TM = 2, FDTD_THREED = 3 };
+
+/* precision / method */
+enum {
+  FDTD_PLAIN_F64 = 0, /* FP64, D/B/E/H stored, the reference's operation order */
+  FDTD_FUSED_F32 = 1  /* FP32, E/H form, fused sweeps */
+};
+
+enum {
+  FDTD_OK = 0,
+  FDTD_ERR_INVALID = -1,     /* bad argument or state */
+  FDTD_ERR_CUDA = -2,        /* a CUDA call failed */
+  FDTD_ERR_UNSUPPORTED = -3, /* valid, but not supported by this method */
+  FDTD_ERR_NOMEM = -4,       /* device allocation failed */
+  FDTD_ERR_NONFINITE = -5,   /* a field went non-finite (fdtd_check_finite) */
+  FDTD_ERR_TIMEOUT = -6      /* a bounded device wait gave up */
+};
+
+/* material kinds (DispersiveMaterials.hpp:2076-2105) */
+enum { FDTD_VACUUM = 0, FDTD_CONSTANT = 1, FDTD_DRUDE = 2, FDTD_LORENTZ = 3 };
+#define FDTD_MAX_POLES 4
+
+/* field selectors for fdtd_download / fdtd_upload */
+enum {
+  FDTD_DX = 0, FDTD_DY, FDTD_DZ, FDTD_EX, FDTD_EY, FDTD_EZ,
+  FDTD_BX, FDTD_BY, FDTD_BZ, FDTD_HX, FDTD_HY, FDTD_HZ,
+  FDTD_PX, FDTD_PY, FDTD_PZ, FDTD_JX, FDTD_JY, FDTD_JZ, /* pole 0 */
+  FDTD_PSI0 = 18 /* 18 + 9*ft + 3*I + J: CPML integrator psi[ft][I][J] */
+  /* 36 + 6*(pole-1) + {0..5}: P/J of poles 1.. */
+};
+
+typedef struct {
+  int mode;      /* FDTD_TE, FDTD_TM or FDTD_THREED */
+  int precision; /* FDTD_PLAIN_F64 or FDTD_FUSED_F32 */
+  int nx, ny, nz;/* cells per axis, including the fixed outer ring; nz = 1 in 2D */
+  double dx;     /* cell size, m */
+  double dt;     /* time step, s */
+  int device;    /* CUDA device ordinal */
+} fdtd_grid_desc;
+
+typedef struct {
+  int kind;   /* FDTD_VACUUM, FDTD_CONSTANT, FDTD_DRUDE, FDTD_LORENTZ */
+  int npoles; /* Drude: 1; Lorentz: 1..FDTD_MAX_POLES */
+  double eps_inf; /* relative permittivity: the reference storages' K */
+  double mu_r;    /* relative permeability: 1 = VacuumUpdate<Mode,Magnetic> */
+  double delta_eps[FDTD_MAX_POLES]; /* Lorentz pole strength; the reference ignores
+                                       its Delta (DispersiveMaterials.hpp:710-735), i.e. 1 */
+  double freq[FDTD_MAX_POLES];  /* Drude plasma / Lorentz resonance frequency, rad/s */
+  double gamma[FDTD_MAX_POLES]; /* damping rate, 1/s */
+} fdtd_material;
+
+/* Create a grid. All fields start at zero; every cell is material 0
+ * (vacuum unless fdtd_set_materials says otherwise). */
+int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out);
+int fdtd_grid_destroy(fdtd_grid* g);
+
+/* CPML of `ncells` on side 0 (min) or 1 (max) of `axis`, graded with
+ * PMLParameterModel(dx) (m=3, m_a=1, sigma_max=0.8(m+1)/(imp0 dx), kappa_max=5,
+ * alpha_max=0.05) and placed as in tests/testTM.cpp:44-71. */
+int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells);
+
+/* Material table (n <= 65536 entries; the FP64 plain method takes <= 256). */
+int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n);
+/* Per-cell material ids, uint8, x fastest: index (k*ny + j)*nx + i. */
+int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids);
+/* Per-block ids: cell (i,j,k) takes ids[((k>>s)*nby + (j>>s))*nbx + (i>>s)]. */
+int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz);
+
+/* Soft source: vals[t] is added at step t (counted from grid creation) to
+ * component comp (0..2) of E after the constitutive update (target 0, as
+ * SoftSource<.., GetField<Ez>>), or of D before the CPML pass (target 1). */
+int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals);
+
+/* One TFSF plane (TFSFPlane, Source.hpp:472-634): corrections on the cells
+ * lo..hi (inclusive) with normal orient (0 = -axis, 1 = +axis), wave vector
+ * k, polarisations pol_e/pol_h, location functor ((i,j,k) - origin) * dx, and
+ * an Aux1D grid of aux_ncells + 50 cells whose source value at aux step s is
+ * aux_vals[s-1]. Planes with equal aux grids share one on the device. */
+int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const int* hi,
+                        const double* origin, const double* k, const double* pol_e, const double* pol_h,
+                        int aux_ncells, const double* aux_vals, int naux);
+
+/* Running DFT of comp (0..2 E, 3..5 H) over the inclusive box lo..hi at nf
+ * frequencies (cycles per step). X_f = sum_n x[n] exp(-2 pi i f n), with
+ * n = t+1 for E at the end of step t's E half and t+1.5 for H. */
+int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle);
+int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints);
+/* host out: [nf][npoints][2] doubles (re, im), points x fastest */
+int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
+
+/* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
+ * handle's stream). Returns once the work is enqueued. */
+int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
+/* Wait for all work on the handle's streams. */
+int fdtd_synchronize(fdtd_grid* g);
+
+/* Copy one field to/from a host array of nx*ny*nz doubles (x fastest), in SI
+ * units whatever the precision. Fields the method does not store return
+ * FDTD_ERR_UNSUPPORTED. */
+int fdtd_download(fdtd_grid* g, int which, double* host);
+int fdtd_upload(fdtd_grid* g, int which, const double* host);
+
+/* Checks every stored field for NaN/Inf; FDTD_ERR_NONFINITE if any. */
+int fdtd_check_finite(fdtd_grid* g);
+
+/* Steps taken so far, and kernels this handle launched so far. */
+int fdtd_get_step(fdtd_grid* g, long long* step);
+int fdtd_launch_count(fdtd_grid* g, long long* count);
+/* Device bytes held by the grid. */
+int fdtd_memory_bytes(fdtd_grid* g, long long* bytes);
+
+/* Last error of the calling thread ("" if none). */
+const char* fdtd_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,150 @@
+"""Small seeded scenarios shared by the golden-fixture generator and the
+parity tests. Each exercises one slice of the hot path at a size the CPU
+oracle finishes in well under a second."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from fdtd_b200.problem import (TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion, courant_dt,
+                               gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, tfsf_box_planes)
+
+DX = 1e-6
+DT2 = courant_dt(DX, 0.99 / math.sqrt(2.0))
+DT3 = courant_dt(DX, 0.99 / math.sqrt(3.0))
+
+
+def tm_cpml_sources() -> Problem:
+    p = Problem(TM, (40, 36, 1), DX, DT2, name="tm_cpml_sources")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    p.sources.append(Source(2, (20, 18, 0), gaussian_pulse(80, 20, 6), "E"))
+    p.sources.append(Source(2, (12, 10, 0), 1e-12 * gaussian_pulse(80, 25, 6), "D"))
+    p.dfts.append(DFTRegion(2, (0, 18, 0), (39, 18, 0), [0.02, 0.05]))
+    p.dfts.append(DFTRegion(3, (5, 5, 0), (9, 8, 0), [0.03]))
+    p.steps = 80
+    return p
+
+
+def te_materials() -> Problem:
+    p = Problem(TE, (33, 41, 1), DX, DT2, name="te_materials")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 5 + s
+    dt = DT2
+    p.materials = [Material.vacuum(), Material.constant(4.0), Material.drude(2.0, 0.3 / dt, 0.01 / dt),
+                   Material.lorentz(1.5, [(1.0, 0.1 / dt, 0.005 / dt)])]
+    ids = np.zeros((1, 41, 33), np.uint8)
+    ids[0, 10:20, 8:14] = 1
+    ids[0, 22:30, 10:25] = 2
+    ids[0, 5:9, 15:28] = 3
+    p.ids = ids
+    p.sources.append(Source(0, (16, 20, 0), gaussian_pulse(60, 20, 6), "E"))
+    p.sources.append(Source(1, (16, 21, 0), gaussian_pulse(60, 20, 6), "E"))
+    p.dfts.append(DFTRegion(5, (3, 3, 0), (29, 37, 0), [0.04]))
+    p.steps = 60
+    return p
+
+
+def td_drude_lorentz() -> Problem:
+    nx, ny, nz = 14, 15, 16
+    p = Problem(THREED, (nx, ny, nz), DX, DT3, name="td_drude_lorentz")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 3
+    dt = DT3
+    p.materials = [Material.vacuum(), Material.drude(1.0, 0.3 / dt, 0.01 / dt),
+                   Material.lorentz(2.0, [(1.0, 0.1 / dt, 0.005 / dt)])]
+    ids = np.zeros((nz, ny, nx), np.uint8)
+    ids[6:10, 6:9, 5:9] = 1
+    ids[3:6, 8:12, 4:7] = 2
+    p.ids = ids
+    p.sources.append(Source(2, (7, 7, 8), gaussian_pulse(40, 15, 5), "E"))
+    p.sources.append(Source(0, (6, 8, 7), gaussian_pulse(40, 18, 5), "E"))
+    p.dfts.append(DFTRegion(2, (1, 1, 8), (12, 13, 8), [0.02, 0.05]))
+    p.dfts.append(DFTRegion(4, (2, 7, 2), (11, 7, 13), [0.04]))
+    p.steps = 40
+    return p
+
+
+def tm_tfsf_reference_polarisation() -> Problem:
+    n = 60
+    p = Problem(TM, (n, n, 1), DX, DT2, name="tm_tfsf_refpol")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 8
+    k = (1.0, 0.0, 0.0)
+    pe, ph = ref_tm_polarisation(k)
+    p.tfsf = TFSF(aux_ncells=n, aux_values=gaussian_pulse(100, 40, 10, offset=1.0), origin=(n / 2, n / 2, 0), k=k,
+                  pol_e=pe, pol_h=ph, planes=tfsf_box_planes(TM, (18, 18), (41, 41)))
+    p.steps = 100
+    return p
+
+
+def te_tfsf_oblique() -> Problem:
+    n = 56
+    p = Problem(TE, (n, n, 1), DX, DT2, name="te_tfsf_oblique")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 7
+    k = (math.cos(0.4), math.sin(0.4), 0.0)
+    pe, ph = ref_te_polarisation(k)
+    p.tfsf = TFSF(aux_ncells=2 * n, aux_values=gaussian_pulse(90, 35, 9, offset=1.0), origin=(n / 2, n / 2, 0), k=k,
+                  pol_e=pe, pol_h=ph, planes=tfsf_box_planes(TE, (16, 16), (39, 39)))
+    p.steps = 90
+    return p
+
+
+def td_tfsf_box() -> Problem:
+    n = 24
+    p = Problem(THREED, (n, n, n), DX, DT3, name="td_tfsf_box")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 4
+    dt = DT3
+    p.materials = [Material.vacuum(), Material.drude(1.0, 0.3 / dt, 0.01 / dt)]
+    ids = np.zeros((n, n, n), np.uint8)
+    ids[10:14, 10:14, 10:14] = 1
+    p.ids = ids
+    k = (1.0, 0.0, 0.0)
+    c = n // 2
+    p.tfsf = TFSF(aux_ncells=n, aux_values=gaussian_pulse(50, 20, 6, offset=1.0), origin=(c, c, c), k=k,
+                  pol_e=(0.0, 0.0, 1.0), pol_h=(0.0, 1.0, 0.0), planes=tfsf_box_planes(THREED, (7, 7, 7), (16, 16, 16)))
+    for a in range(3):
+        lo, hi = [6, 6, 6], [17, 17, 17]
+        lo[a] = hi[a] = 6
+        p.dfts.append(DFTRegion((a + 1) % 3, tuple(lo), tuple(hi), [0.03, 0.06]))
+        p.dfts.append(DFTRegion(3 + (a + 2) % 3, tuple(lo), tuple(hi), [0.03, 0.06]))
+    p.steps = 50
+    return p
+
+
+def td_lorentz_two_pole_blocks() -> Problem:
+    """Two-pole Lorentz on a per-block eps_inf map (an extension: the
+    reference holds one pole; at one pole with delta_eps = 1 it reduces to
+    LorentzUpdate)."""
+    n = 20
+    p = Problem(THREED, (n, n, n), DX, DT3, name="td_lorentz2_blocks")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 3
+    dt = DT3
+    rng = np.random.default_rng(0)
+    nb = (n + 7) // 8
+    eps = rng.uniform(1.0, 6.0, size=nb ** 3)
+    poles = [(1.5, 0.1 / dt, 0.005 / dt), (0.8, 0.25 / dt, 0.02 / dt)]
+    p.materials = [Material.lorentz(float(e), poles) for e in eps]
+    p.block_ids = np.arange(nb ** 3, dtype=np.uint16).reshape(nb, nb, nb)
+    p.block_shift = 3
+    p.sources.append(Source(2, (10, 10, 10), gaussian_pulse(40, 15, 5), "E"))
+    p.dfts.append(DFTRegion(2, (0, 0, 10), (n - 1, n - 1, 10), [0.02, 0.04]))
+    p.steps = 40
+    return p
+
+
+# scenarios the reference itself can run (one pole, reference polarisations in 2D)
+REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
+                       te_tfsf_oblique]
+ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_tfsf_box, td_lorentz_two_pole_blocks]

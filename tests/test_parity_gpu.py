@@ -1,0 +1,128 @@
+"""GPU parity: the CUDA library, called through the C ABI, against the CPU
+oracle on the same seeded inputs.
+
+* FP64 plain method: <= 1e-12 relative L2 on every stored field, CPML
+  integrator, polarisation state and DFT accumulator (the kernels follow the
+  reference's operation order without FMA contraction, so in practice the
+  fields come out bit-identical; the tolerance is the stated bar).
+* FP32 fused method: <= 1e-4 relative L2 on E, H, P, J and the DFTs.
+"""
+import numpy as np
+import pytest
+
+import scenarios
+from helpers import mode_fields, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_TOL = 1e-12
+FUSED_TOL = 1e-4
+
+
+def _compare(p, g, o, names, tol):
+    worst = {}
+    for n in names:
+        ref = o.get(n)
+        if not np.any(ref):
+            continue
+        worst[n] = rel_l2(g.get(n), ref)
+    for q in range(len(p.dfts)):
+        worst[f"dft{q}"] = rel_l2(g.dft(q), o.dft(q))
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, f"{p.name}: {bad}"
+    return worst
+
+
+@pytest.mark.parametrize("make", scenarios.ALL_SCENARIOS, ids=lambda f: f.__name__)
+def test_plain_f64_matches_oracle(fdtd, oracle, make):
+    p = make()
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    g.synchronize()
+    E, H, D, B = mode_fields(p.mode)
+    names = E + H + D + B + oracle.PSI_NAMES + ["Px", "Py", "Pz", "Jx", "Jy", "Jz"]
+    _compare(p, g, o, names, PLAIN_TOL)
+    npoles = max(len(m.poles) for m in p.materials)
+    for pole in range(1, npoles):
+        for n in ["Px", "Py", "Pz", "Jx", "Jy", "Jz"]:
+            ref = o.get_pole(pole, n)
+            assert rel_l2(g.get_pole(pole, n), ref) <= PLAIN_TOL
+
+
+@pytest.mark.parametrize("make", scenarios.ALL_SCENARIOS, ids=lambda f: f.__name__)
+def test_plain_f64_bitwise_fields(fdtd, oracle, make):
+    """Stronger than the bar: E and H are bit-identical to the oracle."""
+    p = make()
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    E, H, _, _ = mode_fields(p.mode)
+    for n in E + H:
+        assert np.array_equal(g.get(n), o.get(n)), n
+
+
+@pytest.mark.parametrize("make", scenarios.ALL_SCENARIOS, ids=lambda f: f.__name__)
+def test_fused_f32_matches_oracle(fdtd, oracle, make):
+    p = make()
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.step(p.steps)
+    g.synchronize()
+    E, H, _, _ = mode_fields(p.mode)
+    _compare(p, g, o, E + H, FUSED_TOL)
+
+
+def test_split_steps_equal_one_call(fdtd, oracle):
+    """fdtd_step(a) then fdtd_step(b) == fdtd_step(a+b), TFSF aux included."""
+    p = scenarios.tm_tfsf_reference_polarisation()
+    g1 = fdtd.Grid.from_problem(p, "f64")
+    g1.step(p.steps)
+    g2 = fdtd.Grid.from_problem(p, "f64")
+    g2.step(37)
+    g2.step(p.steps - 37)
+    for n in ["Ez", "Hx", "Hy", "Dz"]:
+        assert np.array_equal(g1.get(n), g2.get(n))
+    assert g2.step_count == p.steps
+
+
+def test_deterministic(fdtd):
+    p = scenarios.td_tfsf_box()
+    outs = []
+    for _ in range(2):
+        g = fdtd.Grid.from_problem(p, "f32")
+        g.step(p.steps)
+        outs.append(g.get("Ez"))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_errors_are_reported(fdtd):
+    from fdtd_b200.problem import TM, THREED
+    with pytest.raises(fdtd.FdtdError) as e:
+        fdtd.Grid(TM, (8, 8, 2), 1e-6, 1e-15)
+    assert e.value.code == -1
+    g = fdtd.Grid(TM, (16, 16, 1), 1e-6, 1e-15)
+    with pytest.raises(fdtd.FdtdError):
+        g.set_pml(0, 0, 20)  # wider than the grid
+    with pytest.raises(fdtd.FdtdError):
+        g.add_source(0, (5, 5, 0), [1.0])  # Ex is not a TM component
+    with pytest.raises(fdtd.FdtdError):
+        g.add_source(2, (0, 5, 0), [1.0])  # ring cell
+    with pytest.raises(fdtd.FdtdError):
+        g.add_tfsf_plane(0, 0, (5, 5, 0), (5, 10, 0), (8, 8, 0), (1, 0, 0), (0, 0, 1), (0, 1, 0), 1, [1.0])
+    f = fdtd.Grid(THREED, (8, 8, 8), 1e-6, 1e-15, "f32")
+    with pytest.raises(fdtd.FdtdError) as e:
+        f.get("Dx")  # the fused method stores no D
+    assert e.value.code == -3
+
+
+def test_check_finite_flags_nan(fdtd):
+    from fdtd_b200.problem import TM
+    g = fdtd.Grid(TM, (16, 16, 1), 1e-6, 1e-15)
+    g.check_finite()
+    a = np.zeros((1, 16, 16))
+    a[0, 5, 5] = np.nan
+    g.set("Ez", a)
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.check_finite()
+    assert e.value.code == -5
