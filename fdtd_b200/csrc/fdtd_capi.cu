@@ -858,7 +858,16 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   return FDTD_OK;
 }
 
-int fdtd_step(fdtd_grid* g, int nsteps, void* stream) {
+static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof);
+
+int fdtd_step(fdtd_grid* g, int nsteps, void* stream) { return step_impl(g, nsteps, stream, nullptr); }
+
+int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms) {
+  if (!ms) return fail(FDTD_ERR_INVALID, "null argument");
+  return step_impl(g, nsteps, stream, ms);
+}
+
+static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
@@ -903,25 +912,42 @@ int fdtd_step(fdtd_grid* g, int nsteps, void* stream) {
   const int mode = g->d.mode;
   const void* const* fE = reinterpret_cast<const void* const*>(g->d_fieldptrs);
   const void* const* fH = fE + 3;
-  if (g->f32) {
-    FusedArgs a = fused_args(g);
-    for (int q = 0; q < nsteps; q++) {
-      g->launches += launch_fused_e(mode, a, s);
-      g->launches += launch_dft(0, 1, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1], g->pitch, g->ctrl, s);
-      g->launches += launch_fused_h(mode, a, s);
-      g->launches += launch_dft(1, 1, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1], g->pitch, g->ctrl, s);
-      g->launches += launch_step_advance(g->ctrl, s);
-    }
-  } else {
-    PlainArgs a = plain_args(g);
-    for (int q = 0; q < nsteps; q++) {
-      g->launches += launch_plain_e(mode, a, s);
-      g->launches += launch_dft(0, 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1], g->n[0], g->ctrl, s);
-      g->launches += launch_plain_h(mode, a, s);
-      g->launches += launch_dft(1, 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1], g->n[0], g->ctrl, s);
-      g->launches += launch_step_advance(g->ctrl, s);
+  // kernel sequence of one step; with `prof`, CUDA events bracket each kernel
+  // on the launching stream and the elapsed times are summed per kernel kind
+  cudaEvent_t ev[6] = {};
+  if (prof) {
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int q = 0; q < 5; q++) prof[q] = 0.0;
+  }
+  FusedArgs fa;
+  PlainArgs pa;
+  if (g->f32) fa = fused_args(g);
+  else pa = plain_args(g);
+  for (int q = 0; q < nsteps; q++) {
+    if (prof) CK(cudaEventRecord(ev[0], s));
+    g->launches += g->f32 ? launch_fused_e(mode, fa, s) : launch_plain_e(mode, pa, s);
+    if (prof) CK(cudaEventRecord(ev[1], s));
+    g->launches += launch_dft(0, g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1],
+                              static_cast<int>(rowlen(g)), g->ctrl, s);
+    if (prof) CK(cudaEventRecord(ev[2], s));
+    g->launches += g->f32 ? launch_fused_h(mode, fa, s) : launch_plain_h(mode, pa, s);
+    if (prof) CK(cudaEventRecord(ev[3], s));
+    g->launches += launch_dft(1, g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1],
+                              static_cast<int>(rowlen(g)), g->ctrl, s);
+    if (prof) CK(cudaEventRecord(ev[4], s));
+    g->launches += launch_step_advance(g->ctrl, s);
+    if (prof) {
+      CK(cudaEventRecord(ev[5], s));
+      CK(cudaEventSynchronize(ev[5]));
+      for (int k = 0; k < 5; k++) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        prof[k] += ms / nsteps;
+      }
     }
   }
+  if (prof)
+    for (auto& e : ev) cudaEventDestroy(e);
   CK(cudaGetLastError());
   g->t += nsteps;
   return FDTD_OK;

@@ -136,6 +136,11 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
 /* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
  * handle's stream). Returns once the work is enqueued. */
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
+/* fdtd_step with CUDA events around every kernel on the launching stream:
+ * ms[0..4] receive the mean per-step time of the E sweep, the E-phase DFT,
+ * the H sweep, the H-phase DFT and the step-counter kernel (milliseconds).
+ * Synchronises after every step; for measurement, not production. */
+int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
 /* Wait for all work on the handle's streams. */
 int fdtd_synchronize(fdtd_grid* g);
 

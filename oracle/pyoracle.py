@@ -227,7 +227,8 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
             ap = os.path.join(td, "aux.bin")
             np.ascontiguousarray(t.aux_values, dtype=np.float64).tofile(ap)
             lines.append(f"ntfsf {len(t.planes)} {t.aux_ncells} {ap} {t.origin[0]!r} {t.origin[1]!r} {t.origin[2]!r} "
-                         f"{t.k[0]!r} {t.k[1]!r} {t.k[2]!r}")
+                         f"{t.k[0]!r} {t.k[1]!r} {t.k[2]!r} 1 {t.pol_e[0]!r} {t.pol_e[1]!r} {t.pol_e[2]!r} "
+                         f"{t.pol_h[0]!r} {t.pol_h[1]!r} {t.pol_h[2]!r}")
             for pl in t.planes:
                 lines.append(f"{pl.axis} {pl.orient} {pl.lo[0]} {pl.hi[0]} {pl.lo[1]} {pl.hi[1]} {pl.lo[2]} {pl.hi[2]}")
         lines.append(f"steps {steps}")

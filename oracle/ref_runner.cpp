@@ -28,7 +28,9 @@
 //   nsrc S then S lines: comp target i j k path  (comp 0..2, target 0=E 1=D,
 //        path: float64 per step, value added at step t)
 //   ntfsf T (T planes) then: aux_ncells aux_path origin_x origin_y origin_z
-//        kx ky kz, and T lines: axis orient i0 i1 j0 j1 k0 k1 (inclusive)
+//        kx ky kz set_pol pe_x pe_y pe_z ph_x ph_y ph_z, and T lines:
+//        axis orient i0 i1 j0 j1 k0 k1 (inclusive). set_pol 0 keeps the
+//        plane's own polarisation (TE/TM defaults), 1 sets pe/ph.
 //        aux_path: float64 per aux step (value for aux step s at index s-1)
 //   steps N
 //   out path
@@ -102,6 +104,7 @@ struct Scenario {
   std::vector<uint8_t> ids;
   std::vector<Src> srcs;
   int aux_ncells = 0; std::vector<double> aux_vals; double origin[3] = {0, 0, 0}, kvec[3] = {1, 0, 0};
+  int set_pol = 0; double pol_e[3] = {0, 0, 0}, pol_h[3] = {0, 0, 0};
   std::vector<PlaneSpec> planes;
   int steps = 0;
   std::string out;
@@ -148,6 +151,47 @@ struct StepSignal {
     return (s >= 0 && s < (long)tab->size()) ? (*tab)[s] : 0.0;
   }
 };
+
+// Location functor of a TFSF plane: ((i,j,k) - origin) * dx.
+template <class Mode>
+struct LocF {
+  const double* origin;
+  double dx;
+  std::array<double, Mode::dim> operator()(PtrIt<Cell<Mode>> it) const {
+    Cell<Mode>& c = *it;
+    std::array<double, Mode::dim> pt;
+    int idx[3] = {c.ci, c.cj, c.ck};
+    for (int d = 0; d < Mode::dim; d++) pt[d] = (static_cast<double>(idx[d]) - origin[d]) * dx;
+    return pt;
+  }
+};
+template <class Mode>
+using PlaneOf = TFSFPlane<Mode, LocF<Mode>, PtrIt<Cell<Mode>>, Aux1D<double>>;
+
+// TFSFPlane keeps its polarisation vectors private and, for ThreeD, leaves
+// them uninitialised (include/Source.hpp:572-584). The runner sets them
+// through member pointers obtained by explicit template instantiation, which
+// the language exempts from access checking; the reference is not modified.
+template <typename Tag, typename Tag::type M>
+struct Rob {
+  friend typename Tag::type get(Tag) { return M; }
+};
+template <class Mode>
+struct PolE {
+  typedef std::array<double, 3> PlaneOf<Mode>::*type;
+  friend type get(PolE);
+};
+template <class Mode>
+struct PolH {
+  typedef std::array<double, 3> PlaneOf<Mode>::*type;
+  friend type get(PolH);
+};
+template struct Rob<PolE<TE>, &PlaneOf<TE>::mPolarization>;
+template struct Rob<PolH<TE>, &PlaneOf<TE>::mPolarizationH>;
+template struct Rob<PolE<TM>, &PlaneOf<TM>::mPolarization>;
+template struct Rob<PolH<TM>, &PlaneOf<TM>::mPolarizationH>;
+template struct Rob<PolE<ThreeD>, &PlaneOf<ThreeD>::mPolarization>;
+template struct Rob<PolH<ThreeD>, &PlaneOf<ThreeD>::mPolarizationH>;
 
 template <class Mode, class F>
 constexpr bool has_field() {
@@ -251,13 +295,8 @@ static int run(Scenario& s) {
   // TFSF planes over one shared 1D auxiliary grid (include/Source.hpp:280-634)
   typedef std::array<double, Mode::dim> PT;
   std::vector<std::vector<C*>> plane_cells(s.planes.size());
-  auto loc = [&](PtrIt<C> it) -> PT {
-    C& c = *it; PT pt; int idx[3] = {c.ci, c.cj, c.ck};
-    for (int d = 0; d < Mode::dim; d++) pt[d] = (static_cast<double>(idx[d]) - s.origin[d]) * dx;
-    return pt;
-  };
-  typedef decltype(loc) LocT;
-  typedef TFSFPlane<Mode, LocT, PtrIt<C>, Aux1D<double>> PlaneT;
+  LocF<Mode> loc{s.origin, dx};
+  typedef PlaneOf<Mode> PlaneT;
   std::vector<std::unique_ptr<PlaneT>> planes;
   if (!s.planes.empty()) {
     PT kv; for (int d = 0; d < Mode::dim; d++) kv[d] = s.kvec[d];
@@ -272,6 +311,10 @@ static int run(Scenario& s) {
       // one aux grid per plane: every updateD advances its plane's aux grid
       auto aux = std::make_shared<Aux1D<double>>(s.aux_ncells, dx, dt, TableSignal{&s.aux_vals, dt});
       planes.emplace_back(new PlaneT(kv, normal, loc, b, e, aux));
+      if (s.set_pol) {
+        (*planes.back()).*get(PolE<Mode>()) = {s.pol_e[0], s.pol_e[1], s.pol_e[2]};
+        (*planes.back()).*get(PolH<Mode>()) = {s.pol_h[0], s.pol_h[1], s.pol_h[2]};
+      }
     }
   }
 
@@ -378,6 +421,7 @@ int main(int argc, char** argv) {
     } else if (key == "ntfsf") {
       int m; in >> m; std::string p;
       in >> s.aux_ncells >> p >> s.origin[0] >> s.origin[1] >> s.origin[2] >> s.kvec[0] >> s.kvec[1] >> s.kvec[2];
+      in >> s.set_pol >> s.pol_e[0] >> s.pol_e[1] >> s.pol_e[2] >> s.pol_h[0] >> s.pol_h[1] >> s.pol_h[2];
       if (m > 0) s.aux_vals = read_f64(p);
       s.planes.resize(m);
       for (auto& x : s.planes) in >> x.axis >> x.orient >> x.lo[0] >> x.hi[0] >> x.lo[1] >> x.hi[1] >> x.lo[2] >> x.hi[2];

@@ -144,7 +144,7 @@ def td_lorentz_two_pole_blocks() -> Problem:
     return p
 
 
-# scenarios the reference itself can run (one pole, reference polarisations in 2D)
+# scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
-                       te_tfsf_oblique]
-ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_tfsf_box, td_lorentz_two_pole_blocks]
+                       te_tfsf_oblique, td_tfsf_box]
+ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]

@@ -109,7 +109,8 @@ def test_errors_are_reported(fdtd):
     with pytest.raises(fdtd.FdtdError):
         g.add_source(2, (0, 5, 0), [1.0])  # ring cell
     with pytest.raises(fdtd.FdtdError):
-        g.add_tfsf_plane(0, 0, (5, 5, 0), (5, 10, 0), (8, 8, 0), (1, 0, 0), (0, 0, 1), (0, 1, 0), 1, [1.0])
+        # the plane projects far outside a 51-cell aux grid
+        g.add_tfsf_plane(0, 0, (5, 5, 0), (5, 10, 0), (-100, 8, 0), (1, 0, 0), (0, 0, 1), (0, 1, 0), 1, [1.0])
     f = fdtd.Grid(THREED, (8, 8, 8), 1e-6, 1e-15, "f32")
     with pytest.raises(fdtd.FdtdError) as e:
         f.get("Dx")  # the fused method stores no D
