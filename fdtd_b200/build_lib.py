@@ -27,6 +27,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = {
     "kernels_plain.cu": ["-fmad=false"],
     "kernels_fused.cu": [],
+    "kernels_fused3d.cu": [],
     "kernels_common.cu": [],
     "fdtd_capi.cu": [],
 }

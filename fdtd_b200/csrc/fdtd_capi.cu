@@ -219,13 +219,14 @@ int upload_profiles(fdtd_grid* g) {
       for (int q = 0; q < 4; q++) {
         if (g->f32) {
           const double c = ft == 0 ? ce_of(g) : ch_of(g);
-          std::vector<float> v(q == 2 ? 2 * n : n);
+          const int len = a == 0 ? g->pitch : n;  // x profiles padded to the row pitch
+          std::vector<float> v(q == 2 ? 2 * len : len, 0.0f);
           for (int i = 0; i < n; i++) {
             if (q == 0) v[i] = static_cast<float>(p.B[i]);
             if (q == 1) v[i] = static_cast<float>(c * p.C[i]);
             if (q == 2) {
               v[i] = static_cast<float>(c * p.F[i]);
-              v[n + i] = static_cast<float>(p.F[i]);
+              v[len + i] = static_cast<float>(p.F[i]);
             }
             if (q == 3) v[i] = static_cast<float>(p.G[i]);
           }
@@ -514,6 +515,9 @@ FusedArgs fused_args(fdtd_grid* g) {
   memset(&a, 0, sizeof(a));
   fill_common(g, a);
   a.pitch = g->pitch;
+  a.flen[0] = g->pitch;
+  a.flen[1] = g->n[1];
+  a.flen[2] = g->n[2];
   a.ce = static_cast<float>(ce_of(g));
   a.ch = static_cast<float>(ch_of(g));
   for (int c = 0; c < 3; c++) {
@@ -573,7 +577,9 @@ int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out) {
   g->n[1] = d.ny;
   g->n[2] = d.nz;
   g->f32 = d.precision == FDTD_FUSED_F32;
-  g->pitch = g->f32 ? ((d.nx + 31) / 32) * 32 : d.nx;
+  // FP32 rows are padded to a multiple of 128 cells: the vectorised sweeps
+  // read whole 128-cell groups of a row
+  g->pitch = g->f32 ? ((d.nx + 127) / 128) * 128 : d.nx;
   if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete g;
     return fail(FDTD_ERR_CUDA, "cudaStreamCreate failed");
@@ -923,14 +929,17 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   PlainArgs pa;
   if (g->f32) fa = fused_args(g);
   else pa = plain_args(g);
+  const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
   for (int q = 0; q < nsteps; q++) {
     if (prof) CK(cudaEventRecord(ev[0], s));
-    g->launches += g->f32 ? launch_fused_e(mode, fa, s) : launch_plain_e(mode, pa, s);
+    if (g->f32) g->launches += use3d ? launch_fused3d_e(fa, s) : launch_fused_e(mode, fa, s);
+    else g->launches += launch_plain_e(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[1], s));
     g->launches += launch_dft(0, g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1],
                               static_cast<int>(rowlen(g)), g->ctrl, s);
     if (prof) CK(cudaEventRecord(ev[2], s));
-    g->launches += g->f32 ? launch_fused_h(mode, fa, s) : launch_plain_h(mode, pa, s);
+    if (g->f32) g->launches += use3d ? launch_fused3d_h(fa, s) : launch_fused_h(mode, fa, s);
+    else g->launches += launch_plain_h(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[3], s));
     g->launches += launch_dft(1, g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1],
                               static_cast<int>(rowlen(g)), g->ctrl, s);

@@ -126,6 +126,7 @@ struct PlainArgs {
 
 struct FusedArgs {
   int nx, ny, nz, pitch;
+  int flen[3];   // length of each axis' scaled profile; the raw F follows it
   float ce, ch;  // dt/(eps0 eta dx), eta dt/(mu0 dx)
   float* E[3];
   float* H[3];   // eta * H
@@ -165,6 +166,9 @@ int launch_plain_e(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_fused_e(int mode, const FusedArgs& a, cudaStream_t s);
 int launch_fused_h(int mode, const FusedArgs& a, cudaStream_t s);
+bool fused3d_supported(const FusedArgs& a);
+int launch_fused3d_e(const FusedArgs& a, cudaStream_t s);
+int launch_fused3d_h(const FusedArgs& a, cudaStream_t s);
 int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, double* By, double* Hy,
                           double* psiE, double* psiH, const double* coef, const double* vals, int nvals,
                           long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);

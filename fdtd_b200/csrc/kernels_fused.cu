@@ -71,7 +71,6 @@ __device__ __forceinline__ bool range_hits_slab(const Slab& s, int lo, int hi) {
   return (s.wlo > 0 && lo <= s.wlo) || (s.W - s.wlo > 0 && hi >= s.hi0);
 }
 
-// Raw (unscaled) F profiles used by TFSF live after the 4 scaled arrays.
 template <int MODE, int MAXP>
 __global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kchunk) {
   const int lane = threadIdx.x;
@@ -163,9 +162,9 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kch
         if (!(plane_mask >> q & 1u)) continue;
         const PlaneDev& p = a.planes[q];
         if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-        const float* F0 = a.prof[0][0].F + a.nx;  // raw F follows the scaled F
-        const float* F1 = a.prof[0][1].F + a.ny;
-        const float* F2 = a.prof[0][2].F + a.nz;
+        const float* F0 = a.prof[0][0].F + a.flen[0];  // raw F follows the scaled F
+        const float* F1 = a.prof[0][1].F + a.flen[1];
+        const float* F2 = a.prof[0][2].F + a.flen[2];
         const double sc = a.dt / kEps0;
         if (hasE(MODE, 0)) dx_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 0, 0, idx, F0, F1, F2));
         if (hasE(MODE, 1)) dy_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 0, 1, idx, F0, F1, F2));
@@ -325,9 +324,9 @@ __global__ void __launch_bounds__(256) fused_h_kernel(const FusedArgs a, int kch
         if (!(plane_mask >> q & 1u)) continue;
         const PlaneDev& p = a.planes[q];
         if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-        const float* F0 = a.prof[1][0].F + a.nx;
-        const float* F1 = a.prof[1][1].F + a.ny;
-        const float* F2 = a.prof[1][2].F + a.nz;
+        const float* F0 = a.prof[1][0].F + a.flen[0];
+        const float* F1 = a.prof[1][1].F + a.flen[1];
+        const float* F2 = a.prof[1][2].F + a.flen[2];
         const double sc = a.eta * a.dt / kMu0;
         if (hasH(MODE, 0)) dx_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 1, 0, idx, F0, F1, F2));
         if (hasH(MODE, 1)) dy_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 1, 1, idx, F0, F1, F2));
