@@ -28,10 +28,12 @@ SOURCES = {
     "kernels_plain.cu": ["-fmad=false"],
     "kernels_fused.cu": [],
     "kernels_fused3d.cu": [],
+    "kernels_fused3d_tma.cu": [],
+    "kernels_tfsf.cu": [],
     "kernels_common.cu": [],
     "fdtd_capi.cu": [],
 }
-HEADERS = ["internal.h", os.path.join("..", "..", "include", "fdtd_b200.h")]
+HEADERS = ["internal.h", "fused3d_common.cuh", os.path.join("..", "..", "include", "fdtd_b200.h")]
 
 
 def _newer(target: str, deps) -> bool:

@@ -161,6 +161,10 @@ struct fdtd_grid {
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
   bool dirty_dft = true;
+  int sweep_kind = FDTD_SWEEP_AUTO;
+  TmaState* tma = nullptr;
+  long long* d_plane_offs = nullptr;  // prefix sums of TFSF plane cell counts
+  long long plane_cells = 0;
 };
 
 namespace {
@@ -633,6 +637,7 @@ int fdtd_grid_destroy(fdtd_grid* g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   for (void* p : g->allocs) cudaFree(p);
   if (g->stream) cudaStreamDestroy(g->stream);
+  tma_release(g->tma);
   delete g;
   return FDTD_OK;
 }
@@ -811,7 +816,14 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
   PlaneH ph;
   ph.dev = p;
   g->planes.push_back(ph);
-  return FDTD_OK;
+  std::vector<long long> offs(1, 0);
+  for (auto& q : g->planes) {
+    long long n = 1;
+    for (int d = 0; d < 3; d++) n *= q.dev.hi[d] - q.dev.lo[d] + 1;
+    offs.push_back(offs.back() + n);
+  }
+  g->plane_cells = offs.back();
+  return upload_vec(g, reinterpret_cast<void**>(&g->d_plane_offs), offs.data(), offs.size() * sizeof(long long));
 }
 
 int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) {
@@ -930,15 +942,31 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   if (g->f32) fa = fused_args(g);
   else pa = plain_args(g);
   const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
+  const bool use_tma = use3d && g->sweep_kind == FDTD_SWEEP_TMA && tma_prepare(fa, &g->tma);
+  if (g->sweep_kind == FDTD_SWEEP_TMA && !use_tma)
+    return fail(FDTD_ERR_UNSUPPORTED, "the TMA sweep is not available for this grid");
+  const bool use_flat = use3d && !use_tma && (g->sweep_kind == FDTD_SWEEP_FLAT || g->sweep_kind == FDTD_SWEEP_AUTO);
   for (int q = 0; q < nsteps; q++) {
     if (prof) CK(cudaEventRecord(ev[0], s));
-    if (g->f32) g->launches += use3d ? launch_fused3d_e(fa, s) : launch_fused_e(mode, fa, s);
+    if (g->f32) {
+      g->launches += use_tma    ? launch_tma_e(fa, g->tma, s)
+                     : use_flat ? launch_flat_e(fa, s)
+                     : use3d    ? launch_fused3d_e(fa, s)
+                                : launch_fused_e(mode, fa, s);
+      g->launches += launch_tfsf_fused(mode, fa, 0, g->d_plane_offs, g->plane_cells, s);
+    }
     else g->launches += launch_plain_e(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[1], s));
     g->launches += launch_dft(0, g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1],
                               static_cast<int>(rowlen(g)), g->ctrl, s);
     if (prof) CK(cudaEventRecord(ev[2], s));
-    if (g->f32) g->launches += use3d ? launch_fused3d_h(fa, s) : launch_fused_h(mode, fa, s);
+    if (g->f32) {
+      g->launches += use_tma    ? launch_tma_h(fa, g->tma, s)
+                     : use_flat ? launch_flat_h(fa, s)
+                     : use3d    ? launch_fused3d_h(fa, s)
+                                : launch_fused_h(mode, fa, s);
+      g->launches += launch_tfsf_fused(mode, fa, 1, g->d_plane_offs, g->plane_cells, s);
+    }
     else g->launches += launch_plain_h(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[3], s));
     g->launches += launch_dft(1, g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1],
@@ -959,6 +987,23 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
     for (auto& e : ev) cudaEventDestroy(e);
   CK(cudaGetLastError());
   g->t += nsteps;
+  return FDTD_OK;
+}
+
+int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_FLAT) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
+  g->sweep_kind = kind;
+  return FDTD_OK;
+}
+
+int fdtd_error_flags(fdtd_grid* g, int* flags) {
+  if (!g || !flags) return fail(FDTD_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(g->d.device));
+  Control c;
+  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaMemcpy(&c, g->ctrl, sizeof(c), cudaMemcpyDeviceToHost));
+  *flags = c.error;
   return FDTD_OK;
 }
 

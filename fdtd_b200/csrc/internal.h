@@ -167,6 +167,14 @@ int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_fused_e(int mode, const FusedArgs& a, cudaStream_t s);
 int launch_fused_h(int mode, const FusedArgs& a, cudaStream_t s);
 bool fused3d_supported(const FusedArgs& a);
+struct TmaState;
+bool tma_prepare(const FusedArgs& a, TmaState** state);
+void tma_release(TmaState* state);
+int launch_tma_e(const FusedArgs& a, const TmaState* st, cudaStream_t s);
+int launch_tma_h(const FusedArgs& a, const TmaState* st, cudaStream_t s);
+int launch_flat_e(const FusedArgs& a, cudaStream_t s);
+int launch_flat_h(const FusedArgs& a, cudaStream_t s);
+int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, const long long* d_offs, long long total, cudaStream_t s);
 int launch_fused3d_e(const FusedArgs& a, cudaStream_t s);
 int launch_fused3d_h(const FusedArgs& a, cudaStream_t s);
 int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, double* By, double* Hy,

@@ -17,49 +17,14 @@
 // Thread mapping: a CTA of 32 x BY threads covers a 32 x BY tile of (x, y)
 // and marches along z over a chunk of planes; the k-1 plane of the z
 // neighbours stays in registers, x neighbours come from warp shuffles.
+// These scalar sweeps carry the 2D modes; 3D grids use kernels_fused3d*.cu.
+// TFSF corrections are applied after each sweep by kernels_tfsf.cu.
 #include "internal.h"
 
 namespace fdtdb {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBY = 8;
-
-__device__ __forceinline__ double interp_aux_f(const double* row, int L, double loc, double dx, double shift) {
-  double nd = static_cast<double>(L) / 2.0 + loc / dx - shift;
-  unsigned long long n = static_cast<unsigned long long>(nd);
-  double frac = nd - static_cast<double>(n);
-  return (1.0 - frac) * row[n] + frac * row[n + 1];
-}
-
-// TFSF correction of flux I (ft 0 = D, 1 = B) in SI flux units per dt:
-// sum_J LeviCivita * F_J/dx * n_J * inc_K * pol_K (Source.hpp:506-553).
-template <int MODE>
-__device__ double tfsf_flux(const FusedArgs& a, const PlaneDev& p, long long row, int ft, int I, const int idx[3],
-                            const float* Fraw0, const float* Fraw1, const float* Fraw2) {
-  constexpr int dim = MODE == kThreeD ? 3 : 2;
-  const AuxTab& aux = a.aux[p.aux];
-  const float* Fr[3] = {Fraw0, Fraw1, Fraw2};
-  const int d1 = dir1(I);
-  const int ds[2] = {d1, third(I, d1)};
-  double sum = 0.0;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int J = ds[q], K = third(I, J);
-    const bool present = ft == 0 ? hasH(MODE, K) : hasE(MODE, K);
-    if (!present || p.normal[J] == 0.0) continue;
-    double proj = 0;
-#pragma unroll
-    for (int d = 0; d < dim; d++) {
-      const double off = ft == 0 ? (d == K ? -0.5 : 0.0) : (d == K ? 0.0 : -0.5);
-      proj += p.k[d] * ((static_cast<double>(idx[d]) - p.origin[d]) * a.dx + off * a.dx);
-    }
-    const double sv = ft == 0 ? interp_aux_f(aux.Htab + row * aux.L, aux.L, proj, a.dx, 0.5)
-                              : interp_aux_f(aux.Etab + row * aux.L, aux.L, proj, a.dx, 0.0);
-    const double* pol = ft == 0 ? p.pol_h : p.pol_e;
-    sum += levi(I, J, K) * (static_cast<double>(Fr[J][idx[J]]) / a.dx) * p.normal[J] * sv * pol[K];
-  }
-  return sum;
-}
 
 __device__ __forceinline__ long long psi_index(const FusedArgs& a, int J, int s, int i, int j, int k) {
   if (J == 0) return (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
@@ -72,7 +37,7 @@ __device__ __forceinline__ bool range_hits_slab(const Slab& s, int lo, int hi) {
 }
 
 template <int MODE, int MAXP>
-__global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kchunk) {
+__global__ void __launch_bounds__(256) fused_e_kernel(const __grid_constant__ FusedArgs a, int kchunk) {
   const int lane = threadIdx.x;
   const int i0 = blockIdx.x * 32 + 1, j0 = blockIdx.y * kBY + 1;
   const int i = i0 + lane, j = j0 + threadIdx.y;
@@ -90,12 +55,6 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kch
   bool pml_x = a.pml_axis[0] && range_hits_slab(a.slab[0], i0, i1);
   bool pml_y = a.pml_axis[1] && range_hits_slab(a.slab[1], j0, j1);
   bool pml_zr = MODE == kThreeD && a.pml_axis[2];
-  unsigned plane_mask = 0;
-  for (int q = 0; q < a.nplanes; q++) {
-    const PlaneDev& p = a.planes[q];
-    if (p.lo[0] <= i1 && p.hi[0] >= i0 && p.lo[1] <= j1 && p.hi[1] >= j0 && p.lo[2] <= kend - 1 && p.hi[2] >= kbeg)
-      plane_mask |= 1u << q;
-  }
 
   float hx_m = 0.f, hy_m = 0.f;
   if (MODE == kThreeD) {
@@ -154,23 +113,7 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kch
         }
       }
     }
-    // TFSF updateD and D-target sources add to the flux before the material update
-    if (plane_mask) {
-      const int idx[3] = {i, j, k};
-      const long long row = t - a.ctrl->t0;
-      for (int q = 0; q < a.nplanes; q++) {
-        if (!(plane_mask >> q & 1u)) continue;
-        const PlaneDev& p = a.planes[q];
-        if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-        const float* F0 = a.prof[0][0].F + a.flen[0];  // raw F follows the scaled F
-        const float* F1 = a.prof[0][1].F + a.flen[1];
-        const float* F2 = a.prof[0][2].F + a.flen[2];
-        const double sc = a.dt / kEps0;
-        if (hasE(MODE, 0)) dx_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 0, 0, idx, F0, F1, F2));
-        if (hasE(MODE, 1)) dy_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 0, 1, idx, F0, F1, F2));
-        if (hasE(MODE, 2)) dz_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 0, 2, idx, F0, F1, F2));
-      }
-    }
+    // D-target sources add to the flux before the material update
     float undo0 = 0.f, undo1 = 0.f, undo2 = 0.f, add0 = 0.f, add1 = 0.f, add2 = 0.f;
     for (int s = 0; s < a.nsrc; s++) {
       const SourceDev& sr = a.src[s];
@@ -232,7 +175,7 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const FusedArgs a, int kch
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) fused_h_kernel(const FusedArgs a, int kchunk) {
+__global__ void __launch_bounds__(256) fused_h_kernel(const __grid_constant__ FusedArgs a, int kchunk) {
   const int lane = threadIdx.x;
   const int i0 = blockIdx.x * 32 + 1, j0 = blockIdx.y * kBY + 1;
   const int i = i0 + lane, j = j0 + threadIdx.y;
@@ -244,17 +187,10 @@ __global__ void __launch_bounds__(256) fused_h_kernel(const FusedArgs a, int kch
     kend = min(kbeg + kchunk, a.nz - 1);
   }
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
-  const long long t = a.ctrl->t;
   const int i1 = min(i0 + 31, a.nx - 2), j1 = min(j0 + kBY - 1, a.ny - 2);
   bool pml_x = a.pml_axis[0] && range_hits_slab(a.slab[0], i0, i1);
   bool pml_y = a.pml_axis[1] && range_hits_slab(a.slab[1], j0, j1);
   bool pml_zr = MODE == kThreeD && a.pml_axis[2];
-  unsigned plane_mask = 0;
-  for (int q = 0; q < a.nplanes; q++) {
-    const PlaneDev& p = a.planes[q];
-    if (p.lo[0] <= i1 && p.hi[0] >= i0 && p.lo[1] <= j1 && p.hi[1] >= j0 && p.lo[2] <= kend - 1 && p.hi[2] >= kbeg)
-      plane_mask |= 1u << q;
-  }
   float ex_c = 0.f, ey_c = 0.f;
   if (MODE == kThreeD) {
     const long long c0 = kbeg * sz + jl * sy + il;
@@ -315,22 +251,6 @@ __global__ void __launch_bounds__(256) fused_h_kernel(const FusedArgs a, int kch
           *dsum[I] += psi * G;
           *ps = B * psi + Cs * raw[I][J];
         }
-      }
-    }
-    if (plane_mask) {
-      const int idx[3] = {i, j, k};
-      const long long row = t - a.ctrl->t0 + 1;
-      for (int q = 0; q < a.nplanes; q++) {
-        if (!(plane_mask >> q & 1u)) continue;
-        const PlaneDev& p = a.planes[q];
-        if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-        const float* F0 = a.prof[1][0].F + a.flen[0];
-        const float* F1 = a.prof[1][1].F + a.flen[1];
-        const float* F2 = a.prof[1][2].F + a.flen[2];
-        const double sc = a.eta * a.dt / kMu0;
-        if (hasH(MODE, 0)) dx_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 1, 0, idx, F0, F1, F2));
-        if (hasH(MODE, 1)) dy_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 1, 1, idx, F0, F1, F2));
-        if (hasH(MODE, 2)) dz_ += static_cast<float>(sc * tfsf_flux<MODE>(a, p, row, 1, 2, idx, F0, F1, F2));
       }
     }
     if (hasH(MODE, 0)) a.H[0][c] -= dx_;

@@ -65,7 +65,7 @@ __device__ double tfsf_term(const PlaneDev& p, const AuxTab& aux, long long row,
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) plain_e_kernel(const PlainArgs a) {
+__global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ PlainArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = MODE == kThreeD ? blockIdx.z + 1 : 0;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) plain_e_kernel(const PlainArgs a) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) plain_h_kernel(const PlainArgs a) {
+__global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ PlainArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = MODE == kThreeD ? blockIdx.z + 1 : 0;

@@ -141,6 +141,16 @@ int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
  * the H sweep, the H-phase DFT and the step-counter kernel (milliseconds).
  * Synchronises after every step; for measurement, not production. */
 int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
+/* Which kernels carry the 3D FP32 fused sweeps: FDTD_SWEEP_AUTO (the
+ * default: currently the flat sweeps, the fastest measured on B200), FDTD_SWEEP_REGS (z-marching, register prefetch),
+ * FDTD_SWEEP_TMA (z-marching, TMA pipeline into shared memory; or
+ * FDTD_ERR_UNSUPPORTED) or FDTD_SWEEP_FLAT (one thread per 4-cell group and
+ * plane). All compute the same update. */
+enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3 };
+int fdtd_set_sweep_kernel(fdtd_grid* g, int kind);
+/* Device-side error flags accumulated by the kernels (0 = none; bit 0: a
+ * bounded wait on a TMA stage expired and the sweep was abandoned). */
+int fdtd_error_flags(fdtd_grid* g, int* flags);
 /* Wait for all work on the handle's streams. */
 int fdtd_synchronize(fdtd_grid* g);
 

@@ -73,6 +73,22 @@ def test_fused_f32_matches_oracle(fdtd, oracle, make):
     _compare(p, g, o, E + H, FUSED_TOL)
 
 
+@pytest.mark.parametrize("sweep", ["regs", "tma", "flat"])
+@pytest.mark.parametrize("make", [m for m in scenarios.ALL_SCENARIOS if m().mode == 3], ids=lambda f: f.__name__)
+def test_fused_3d_sweep_kernels(fdtd, oracle, make, sweep):
+    """Every 3D FP32 sweep implementation (register prefetch, TMA pipeline,
+    flat) meets the bar and reports no device-side error."""
+    p = make()
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.set_sweep_kernel(sweep)
+    g.step(p.steps)
+    g.synchronize()
+    assert g.error_flags() == 0
+    E, H, _, _ = mode_fields(p.mode)
+    _compare(p, g, o, E + H, FUSED_TOL)
+
+
 def test_split_steps_equal_one_call(fdtd, oracle):
     """fdtd_step(a) then fdtd_step(b) == fdtd_step(a+b), TFSF aux included."""
     p = scenarios.tm_tfsf_reference_polarisation()
