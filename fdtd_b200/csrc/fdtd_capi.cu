@@ -157,6 +157,9 @@ struct fdtd_grid {
   DftRegionDev* d_dft[2]{};
   int ndft[2]{};
   long long dft_pts[2]{};
+  long long dft_maxpts[2]{};
+  void* d_dft_buf[2]{};   // [kDftChunk][points] samples per phase
+  int dft_pending = 0;    // samples in the buffers (host mirror of t - dft_base)
   void** d_fieldptrs = nullptr;  // [E0,E1,E2,H0,H1,H2]
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
@@ -165,6 +168,11 @@ struct fdtd_grid {
   TmaState* tma = nullptr;
   long long* d_plane_offs = nullptr;  // prefix sums of TFSF plane cell counts
   long long plane_cells = 0;
+  long long version = 0;        // bumped by every change a captured graph would bake in
+  long long graph_version = -1;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
+  bool use_graphs = true;
 };
 
 namespace {
@@ -174,6 +182,7 @@ long long rowlen(const fdtd_grid* g) { return g->f32 ? g->pitch : g->n[0]; }
 long long field_elems(const fdtd_grid* g) { return rowlen(g) * g->n[1] * g->n[2]; }
 
 int dalloc(fdtd_grid* g, void** p, size_t bytes) {
+  g->version++;
   *p = nullptr;
   if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMalloc(p, bytes);
@@ -191,6 +200,7 @@ int dalloc(fdtd_grid* g, void** p, size_t bytes) {
 }
 
 void dfree(fdtd_grid* g, void* p) {
+  g->version++;
   if (!p) return;
   for (size_t q = 0; q < g->allocs.size(); q++)
     if (g->allocs[q] == p) {
@@ -436,13 +446,29 @@ int rebuild_dft(fdtd_grid* g) {
     }
     g->ndft[ph] = static_cast<int>(v.size());
     g->dft_pts[ph] = off;
+    g->dft_maxpts[ph] = 0;
+    for (auto& o : v) g->dft_maxpts[ph] = std::max(g->dft_maxpts[ph], o.npts);
     if (!v.empty()) {
       int rc = upload_vec(g, reinterpret_cast<void**>(&g->d_dft[ph]), v.data(), v.size() * sizeof(DftRegionDev));
+      if (rc) return rc;
+      if (g->d_dft_buf[ph]) dfree(g, g->d_dft_buf[ph]);
+      rc = dalloc(g, &g->d_dft_buf[ph], static_cast<size_t>(kDftChunk) * off * elem(g));
       if (rc) return rc;
     }
   }
   g->dirty_dft = false;
   return FDTD_OK;
+}
+
+// fold the buffered DFT samples of both phases into the accumulators
+int flush_dft(fdtd_grid* g, cudaStream_t s) {
+  int n = 0;
+  for (int ph = 0; ph < 2; ph++)
+    n += launch_dft_flush(ph, g->f32 ? 1 : 0, g->d_dft[ph], g->ndft[ph], g->dft_maxpts[ph], g->dft_pts[ph],
+                          g->d_dft_buf[ph], g->ctrl, s);
+  n += launch_dft_rebase(g->ctrl, s);
+  g->dft_pending = 0;
+  return n;
 }
 
 template <typename Args>
@@ -638,6 +664,7 @@ int fdtd_grid_destroy(fdtd_grid* g) {
   for (void* p : g->allocs) cudaFree(p);
   if (g->stream) cudaStreamDestroy(g->stream);
   tma_release(g->tma);
+  if (g->graph) cudaGraphExecDestroy(g->graph);
   delete g;
   return FDTD_OK;
 }
@@ -664,7 +691,6 @@ int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) {
 int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
   if (!g || !mats) return fail(FDTD_ERR_INVALID, "null argument");
   if (n < 1 || n > 65536) return fail(FDTD_ERR_INVALID, "material count must be 1..65536");
-  if (!g->f32 && n > 256) return fail(FDTD_ERR_UNSUPPORTED, "the FP64 plain method takes at most 256 materials");
   for (int q = 0; q < n; q++) {
     const fdtd_material& m = mats[q];
     if (m.kind < FDTD_VACUUM || m.kind > FDTD_LORENTZ) return fail(FDTD_ERR_INVALID, "bad material kind");
@@ -877,12 +903,79 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
 }
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof);
+static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof);
 
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream) { return step_impl(g, nsteps, stream, nullptr); }
 
 int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms) {
   if (!ms) return fail(FDTD_ERR_INVALID, "null argument");
   return step_impl(g, nsteps, stream, ms);
+}
+
+// Enqueues nsteps steps on s (kernels only, so it can run under stream
+// capture). With `prof`, CUDA events bracket each part of every step.
+static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof) {
+  const int mode = g->d.mode;
+  const void* const* fE = reinterpret_cast<const void* const*>(g->d_fieldptrs);
+  const void* const* fH = fE + 3;
+  // kernel sequence of one step; with `prof`, CUDA events bracket each kernel
+  // on the launching stream and the elapsed times are summed per kernel kind
+  cudaEvent_t ev[6] = {};
+  if (prof) {
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int q = 0; q < 5; q++) prof[q] = 0.0;
+  }
+  FusedArgs fa;
+  PlainArgs pa;
+  if (g->f32) fa = fused_args(g);
+  else pa = plain_args(g);
+  const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
+  const bool use_tma = use3d && g->sweep_kind == FDTD_SWEEP_TMA && tma_prepare(fa, &g->tma);
+  if (g->sweep_kind == FDTD_SWEEP_TMA && !use_tma)
+    return fail(FDTD_ERR_UNSUPPORTED, "the TMA sweep is not available for this grid");
+  const bool use_flat = use3d && !use_tma && (g->sweep_kind == FDTD_SWEEP_FLAT || g->sweep_kind == FDTD_SWEEP_AUTO);
+  for (int q = 0; q < nsteps; q++) {
+    if (prof) CK(cudaEventRecord(ev[0], s));
+    if (g->f32) {
+      g->launches += use_tma    ? launch_tma_e(fa, g->tma, s)
+                     : use_flat ? launch_flat_e(fa, s)
+                     : use3d    ? launch_fused3d_e(fa, s)
+                                : launch_fused_e(mode, fa, s);
+    }
+    else g->launches += launch_plain_e(mode, pa, s);
+    if (prof) CK(cudaEventRecord(ev[1], s));
+    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, g->d_plane_offs, g->plane_cells, s);
+    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[1],
+                                     static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[0], s);
+    if (prof) CK(cudaEventRecord(ev[2], s));
+    if (g->f32) {
+      g->launches += use_tma    ? launch_tma_h(fa, g->tma, s)
+                     : use_flat ? launch_flat_h(fa, s)
+                     : use3d    ? launch_fused3d_h(fa, s)
+                                : launch_fused_h(mode, fa, s);
+    }
+    else g->launches += launch_plain_h(mode, pa, s);
+    if (prof) CK(cudaEventRecord(ev[3], s));
+    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, g->d_plane_offs, g->plane_cells, s);
+    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[1],
+                                     static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[1], s);
+    if (prof) CK(cudaEventRecord(ev[4], s));
+    g->launches += launch_step_advance(g->ctrl, s);
+    if (!g->dfts.empty() && ++g->dft_pending == kDftChunk) g->launches += flush_dft(g, s);
+    if (prof) {
+      CK(cudaEventRecord(ev[5], s));
+      CK(cudaEventSynchronize(ev[5]));
+      for (int k = 0; k < 5; k++) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        prof[k] += ms / nsteps;
+      }
+    }
+  }
+  if (prof)
+    for (auto& e : ev) cudaEventDestroy(e);
+  if (g->dft_pending > 0) g->launches += flush_dft(g, s);
+  return FDTD_OK;
 }
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
@@ -927,64 +1020,38 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
     CK(cudaMemcpyAsync(g->ctrl, &c, sizeof(long long) * 2, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));  // the host value must outlive the copy
   }
-  const int mode = g->d.mode;
-  const void* const* fE = reinterpret_cast<const void* const*>(g->d_fieldptrs);
-  const void* const* fH = fE + 3;
-  // kernel sequence of one step; with `prof`, CUDA events bracket each kernel
-  // on the launching stream and the elapsed times are summed per kernel kind
-  cudaEvent_t ev[6] = {};
-  if (prof) {
-    for (auto& e : ev) CK(cudaEventCreate(&e));
-    for (int q = 0; q < 5; q++) prof[q] = 0.0;
-  }
-  FusedArgs fa;
-  PlainArgs pa;
-  if (g->f32) fa = fused_args(g);
-  else pa = plain_args(g);
-  const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
-  const bool use_tma = use3d && g->sweep_kind == FDTD_SWEEP_TMA && tma_prepare(fa, &g->tma);
-  if (g->sweep_kind == FDTD_SWEEP_TMA && !use_tma)
-    return fail(FDTD_ERR_UNSUPPORTED, "the TMA sweep is not available for this grid");
-  const bool use_flat = use3d && !use_tma && (g->sweep_kind == FDTD_SWEEP_FLAT || g->sweep_kind == FDTD_SWEEP_AUTO);
-  for (int q = 0; q < nsteps; q++) {
-    if (prof) CK(cudaEventRecord(ev[0], s));
-    if (g->f32) {
-      g->launches += use_tma    ? launch_tma_e(fa, g->tma, s)
-                     : use_flat ? launch_flat_e(fa, s)
-                     : use3d    ? launch_fused3d_e(fa, s)
-                                : launch_fused_e(mode, fa, s);
-      g->launches += launch_tfsf_fused(mode, fa, 0, g->d_plane_offs, g->plane_cells, s);
-    }
-    else g->launches += launch_plain_e(mode, pa, s);
-    if (prof) CK(cudaEventRecord(ev[1], s));
-    g->launches += launch_dft(0, g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[0], g->n[1],
-                              static_cast<int>(rowlen(g)), g->ctrl, s);
-    if (prof) CK(cudaEventRecord(ev[2], s));
-    if (g->f32) {
-      g->launches += use_tma    ? launch_tma_h(fa, g->tma, s)
-                     : use_flat ? launch_flat_h(fa, s)
-                     : use3d    ? launch_fused3d_h(fa, s)
-                                : launch_fused_h(mode, fa, s);
-      g->launches += launch_tfsf_fused(mode, fa, 1, g->d_plane_offs, g->plane_cells, s);
-    }
-    else g->launches += launch_plain_h(mode, pa, s);
-    if (prof) CK(cudaEventRecord(ev[3], s));
-    g->launches += launch_dft(1, g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[0], g->n[1],
-                              static_cast<int>(rowlen(g)), g->ctrl, s);
-    if (prof) CK(cudaEventRecord(ev[4], s));
-    g->launches += launch_step_advance(g->ctrl, s);
-    if (prof) {
-      CK(cudaEventRecord(ev[5], s));
-      CK(cudaEventSynchronize(ev[5]));
-      for (int k = 0; k < 5; k++) {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-        prof[k] += ms / nsteps;
+  // one graph replay = kGraphSteps steps (and, with DFT regions, one flush)
+  const bool graphs = !prof && g->use_graphs && nsteps >= kGraphSteps;
+  int done = 0;
+  if (graphs) {
+    if (!g->graph || g->graph_version != g->version) {
+      if (g->graph) {
+        cudaGraphExecDestroy(g->graph);
+        g->graph = nullptr;
       }
+      const long long before = g->launches;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_steps(g, kGraphSteps, s, nullptr);
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamEndCapture(s, &graph);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&g->graph, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      g->graph_launches = g->launches - before;
+      g->launches = before;
+      g->graph_version = g->version;
+    }
+    for (; done + kGraphSteps <= nsteps; done += kGraphSteps) {
+      CK(cudaGraphLaunch(g->graph, s));
+      g->launches += g->graph_launches;
     }
   }
-  if (prof)
-    for (auto& e : ev) cudaEventDestroy(e);
+  if (done < nsteps) {
+    int rc = enqueue_steps(g, nsteps - done, s, prof);
+    if (rc) return rc;
+  }
   CK(cudaGetLastError());
   g->t += nsteps;
   return FDTD_OK;
@@ -994,6 +1061,13 @@ int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_FLAT) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
   g->sweep_kind = kind;
+  g->version++;
+  return FDTD_OK;
+}
+
+int fdtd_use_graphs(fdtd_grid* g, int enable) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  g->use_graphs = enable != 0;
   return FDTD_OK;
 }
 

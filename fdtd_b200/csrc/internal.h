@@ -10,6 +10,8 @@ constexpr int kMaxPoles = 4;
 constexpr int kMaxPlanes = 12;
 constexpr int kMaxSources = 16;
 constexpr int kAuxNpml = 15;  // Aux1D::mNPML (include/Source.hpp:362)
+constexpr int kDftChunk = 64;  // samples buffered per DFT point before a flush
+constexpr int kGraphSteps = kDftChunk;  // steps per captured CUDA graph
 
 // include/FDTDConstants.hpp:394-398
 constexpr double kPi = 3.14159265358979323846264338327950288;
@@ -93,6 +95,7 @@ struct AuxTab {
 struct Control {
   long long t;   // steps taken
   long long t0;  // first step of the current aux table chunk
+  long long dft_base;  // step of the first sample in the DFT buffers
   unsigned int done_blocks;
   int error;
 };
@@ -180,8 +183,11 @@ int launch_fused3d_h(const FusedArgs& a, cudaStream_t s);
 int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, double* By, double* Hy,
                           double* psiE, double* psiH, const double* coef, const double* vals, int nvals,
                           long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);
-int launch_dft(int phase, int precision, const DftRegionDev* regions, int nreg, long long total_pts,
-               const void* const* fields, int nx, int ny, int pitch, const Control* ctrl, cudaStream_t s);
+int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts,
+                      const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s);
+int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
+                     long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s);
+int launch_dft_rebase(Control* ctrl, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
 

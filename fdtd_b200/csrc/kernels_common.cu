@@ -9,10 +9,15 @@
 
 namespace fdtdb {
 
+// The capture is chunked: every half step a gather copies the region values
+// into slot (t - dft_base) of a ring of kDftChunk samples per point; a flush
+// folds the pending samples into the FP64 accumulators in one pass, with the
+// twiddles of the chunk computed once per block in shared memory. This reads
+// and writes each 16-byte accumulator once per chunk instead of once per step.
 template <typename R>
-__global__ void __launch_bounds__(256) dft_kernel(int phase, const DftRegionDev* __restrict__ regions, int nreg,
-                                                  long long total, const R* const* __restrict__ fields, int nx, int ny,
-                                                  int pitch, const Control* __restrict__ ctrl) {
+__global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, int nreg,
+                                                         long long total, const R* const* __restrict__ fields, int ny,
+                                                         int pitch, const Control* __restrict__ ctrl, R* buf) {
   const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (p >= total) return;
   int r = 0;
@@ -22,29 +27,85 @@ __global__ void __launch_bounds__(256) dft_kernel(int phase, const DftRegionDev*
   const int i = g.lo[0] + static_cast<int>(q % g.ext[0]);
   const int j = g.lo[1] + static_cast<int>((q / g.ext[0]) % g.ext[1]);
   const int k = g.lo[2] + static_cast<int>(q / (static_cast<long long>(g.ext[0]) * g.ext[1]));
-  const R* f = fields[g.comp];
-  const double x = static_cast<double>(f[(static_cast<long long>(k) * ny + j) * pitch + i]);
-  const double n = static_cast<double>(ctrl->t) + (phase == 0 ? 1.0 : 1.5);
-  for (int fi = 0; fi < g.nf; fi++) {
-    double s, c;
-    sincospi(2.0 * g.freqs[fi] * n, &s, &c);
-    double* acc = g.acc + (static_cast<long long>(fi) * g.npts + q) * 2;
-    acc[0] += x * c;
-    acc[1] -= x * s;
-  }
-  (void)nx;
+  const long long slot = ctrl->t - ctrl->dft_base;
+  buf[slot * total + p] = fields[g.comp][(static_cast<long long>(k) * ny + j) * pitch + i];
 }
 
-int launch_dft(int phase, int precision, const DftRegionDev* regions, int nreg, long long total_pts,
-               const void* const* fields, int nx, int ny, int pitch, const Control* ctrl, cudaStream_t s) {
+template <typename R>
+__global__ void __launch_bounds__(256) dft_flush_kernel(int phase, const DftRegionDev* __restrict__ regions,
+                                                        long long total, const R* __restrict__ buf,
+                                                        const Control* __restrict__ ctrl) {
+  __shared__ double2 tw[kDftChunk * 8];
+  const DftRegionDev& g = regions[blockIdx.y];
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (static_cast<long long>(blockIdx.x) * blockDim.x >= g.npts) return;  // block-uniform
+  const int nsamp = static_cast<int>(ctrl->t - ctrl->dft_base);
+  if (nsamp <= 0) return;
+  const double nbase = static_cast<double>(ctrl->dft_base) + (phase == 0 ? 1.0 : 1.5);
+  for (int f0 = 0; f0 < g.nf; f0 += 8) {
+    const int nfb = min(8, g.nf - f0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nsamp * nfb; e += blockDim.x) {
+      const int m = e / nfb, f = e % nfb;
+      double sn, cs;
+      sincospi(2.0 * g.freqs[f0 + f] * (nbase + m), &sn, &cs);
+      tw[m * 8 + f] = make_double2(cs, -sn);
+    }
+    __syncthreads();
+    if (q >= g.npts) continue;
+    double re[8] = {0, 0, 0, 0, 0, 0, 0, 0}, im[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < nsamp; m++) {
+      const double x = static_cast<double>(buf[static_cast<long long>(m) * total + g.pt_off + q]);
+#pragma unroll
+      for (int f = 0; f < 8; f++) {
+        if (f < nfb) {
+          const double2 w = tw[m * 8 + f];
+          re[f] += x * w.x;
+          im[f] += x * w.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 8; f++) {
+      if (f < nfb) {
+        double* acc = g.acc + (static_cast<long long>(f0 + f) * g.npts + q) * 2;
+        acc[0] += re[f];
+        acc[1] += im[f];
+      }
+    }
+  }
+}
+
+__global__ void dft_rebase_kernel(Control* ctrl) { ctrl->dft_base = ctrl->t; }
+
+int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts,
+                      const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s) {
   if (nreg == 0 || total_pts == 0) return 0;
   const unsigned blocks = static_cast<unsigned>((total_pts + 255) / 256);
   if (precision == 0)
-    dft_kernel<double><<<blocks, 256, 0, s>>>(phase, regions, nreg, total_pts,
-                                              reinterpret_cast<const double* const*>(fields), nx, ny, pitch, ctrl);
+    dft_gather_kernel<double><<<blocks, 256, 0, s>>>(regions, nreg, total_pts,
+                                                     reinterpret_cast<const double* const*>(fields), ny, pitch, ctrl,
+                                                     static_cast<double*>(buf));
   else
-    dft_kernel<float><<<blocks, 256, 0, s>>>(phase, regions, nreg, total_pts,
-                                             reinterpret_cast<const float* const*>(fields), nx, ny, pitch, ctrl);
+    dft_gather_kernel<float><<<blocks, 256, 0, s>>>(regions, nreg, total_pts,
+                                                    reinterpret_cast<const float* const*>(fields), ny, pitch, ctrl,
+                                                    static_cast<float*>(buf));
+  return 1;
+}
+
+int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
+                     long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s) {
+  if (nreg == 0 || total_pts == 0) return 0;
+  dim3 grid(static_cast<unsigned>((max_pts + 255) / 256), nreg);
+  if (precision == 0)
+    dft_flush_kernel<double><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const double*>(buf), ctrl);
+  else
+    dft_flush_kernel<float><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const float*>(buf), ctrl);
+  return 1;
+}
+
+int launch_dft_rebase(Control* ctrl, cudaStream_t s) {
+  dft_rebase_kernel<<<1, 1, 0, s>>>(ctrl);
   return 1;
 }
 

@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_last_error_string"]
 
@@ -82,6 +82,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_step": [vp, i, vp],
         "fdtd_profile_step": [vp, i, vp, dp],
         "fdtd_set_sweep_kernel": [vp, i],
+        "fdtd_use_graphs": [vp, i],
         "fdtd_error_flags": [vp, ip],
         "fdtd_synchronize": [vp],
         "fdtd_download": [vp, i, dp],
@@ -205,12 +206,15 @@ class Grid:
         recorded around each kernel on its launching stream."""
         ms = np.zeros(5, dtype=np.float64)
         _check(load_library().fdtd_profile_step(self.h, int(n), ctypes.c_void_p(stream) if stream else None, _dp(ms)))
-        return dict(zip(["e_sweep", "e_dft", "h_sweep", "h_dft", "advance"], ms.tolist()))
+        return dict(zip(["e_sweep", "e_extra", "h_sweep", "h_extra", "advance_flush"], ms.tolist()))
 
     SWEEP_KINDS = {"auto": 0, "regs": 1, "tma": 2, "flat": 3}
 
     def set_sweep_kernel(self, kind: str) -> None:
         _check(load_library().fdtd_set_sweep_kernel(self.h, self.SWEEP_KINDS[kind]))
+
+    def use_graphs(self, enable: bool) -> None:
+        _check(load_library().fdtd_use_graphs(self.h, 1 if enable else 0))
 
     def error_flags(self) -> int:
         v = ctypes.c_int()

@@ -104,7 +104,7 @@ int fdtd_grid_destroy(fdtd_grid* g);
  * alpha_max=0.05) and placed as in tests/testTM.cpp:44-71. */
 int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells);
 
-/* Material table (n <= 65536 entries; the FP64 plain method takes <= 256). */
+/* Material table (n <= 65536 entries; per-cell ids address the first 256). */
 int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n);
 /* Per-cell material ids, uint8, x fastest: index (k*ny + j)*nx + i. */
 int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids);
@@ -136,9 +136,10 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
 /* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
  * handle's stream). Returns once the work is enqueued. */
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
-/* fdtd_step with CUDA events around every kernel on the launching stream:
- * ms[0..4] receive the mean per-step time of the E sweep, the E-phase DFT,
- * the H sweep, the H-phase DFT and the step-counter kernel (milliseconds).
+/* fdtd_step with CUDA events on the launching stream around each part of a
+ * step: ms[0..4] receive the mean per-step time (milliseconds) of the E sweep,
+ * the E-phase extras (TFSF kernel of the FP32 method, DFT gather), the H sweep,
+ * the H-phase extras, and the step counter plus the amortised DFT flush.
  * Synchronises after every step; for measurement, not production. */
 int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
 /* Which kernels carry the 3D FP32 fused sweeps: FDTD_SWEEP_AUTO (the
@@ -148,6 +149,9 @@ int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
  * plane). All compute the same update. */
 enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3 };
 int fdtd_set_sweep_kernel(fdtd_grid* g, int kind);
+/* Replay a captured CUDA graph per 64 steps inside fdtd_step (default 1), or
+ * launch every kernel from the host (0). Results are identical. */
+int fdtd_use_graphs(fdtd_grid* g, int enable);
 /* Device-side error flags accumulated by the kernels (0 = none; bit 0: a
  * bounded wait on a TMA stage expired and the sweep was abandoned). */
 int fdtd_error_flags(fdtd_grid* g, int* flags);

@@ -102,6 +102,22 @@ def test_split_steps_equal_one_call(fdtd, oracle):
     assert g2.step_count == p.steps
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_graph_replay_equals_eager(fdtd, prec):
+    """150 steps as two 64-step graph replays plus 22 eager steps give the
+    same fields and spectra as 150 eagerly launched steps."""
+    p = scenarios.td_tfsf_box()
+    p.tfsf.aux_values = np.concatenate([p.tfsf.aux_values, np.zeros(200)])
+    out = []
+    for graphs in (True, False):
+        g = fdtd.Grid.from_problem(p, prec)
+        g.use_graphs(graphs)
+        g.step(150)
+        out.append((g.get("Ez"), g.get("Hy"), g.dft(0)))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
 def test_deterministic(fdtd):
     p = scenarios.td_tfsf_box()
     outs = []
