@@ -46,19 +46,20 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="drude384", choices=["drude384", "lorentz768", "tm256"])
+    ap.add_argument("--n", type=int, default=0, help="override the grid size (same physics, scaled): for profiling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
     return ap.parse_args()
 
 
-def make_problem(workload: str, steps: int):
+def make_problem(workload: str, steps: int, n: int = 0):
     from fdtd_b200 import problem as P
     if workload == "drude384":
-        return P.config2(n=384, steps=steps)
+        return P.config2(n=n or 384, steps=steps)
     if workload == "lorentz768":
-        return P.config5(n=768, steps=steps)
-    return P.config1(n=256, steps=steps)
+        return P.config5(n=n or 768, steps=steps)
+    return P.config1(n=n or 256, steps=steps)
 
 
 def small_problem(workload: str, steps: int):
@@ -248,7 +249,7 @@ def main():
 
     from fdtd_b200 import grid as G
 
-    p = make_problem(args.workload, args.steps + args.warmup)
+    p = make_problem(args.workload, args.steps + args.warmup, args.n)
     stream = torch.cuda.Stream()
     g = G.Grid.from_problem(p, "f32", device=local)
     g.step(args.warmup, stream=stream.cuda_stream)
@@ -290,7 +291,7 @@ def main():
     # FP64 plain on the same grid and GPU (the metric's comparison)
     f64 = None
     if not args.no_f64:
-        p64 = make_problem(args.workload, args.steps + args.warmup)
+        p64 = make_problem(args.workload, args.steps + args.warmup, args.n)
         g64 = G.Grid.from_problem(p64, "f64", device=local)
         n64 = max(3, min(args.steps, 200))
         g64.step(args.warmup, stream=stream.cuda_stream)
@@ -311,7 +312,7 @@ def main():
     if not args.no_e2e:
         barrier()
         t0 = time.perf_counter()
-        pe = make_problem(args.workload, args.steps)
+        pe = make_problem(args.workload, args.steps, args.n)
         ge = G.Grid.from_problem(pe, "f32", device=local)
         ge.step(args.steps)
         spectra = [ge.dft(q) for q in range(len(pe.dfts))]

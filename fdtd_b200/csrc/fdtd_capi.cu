@@ -570,6 +570,9 @@ FusedArgs fused_args(fdtd_grid* g) {
     }
   a.mats = static_cast<const MatF32*>(g->d_mats);
   a.max_poles = g->max_poles;
+  a.all_dispersive = 1;
+  for (auto& m : g->mats)
+    if (m.kind != FDTD_DRUDE && m.kind != FDTD_LORENTZ) a.all_dispersive = 0;
   a.src_scale_d = static_cast<float>(1.0 / kEps0);
   a.src_last = g->d_src_last;
   a.dx = g->d.dx;

@@ -230,14 +230,26 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
     ie = make_float4(m0.inv_eps, m0.inv_eps, m0.inv_eps, m0.inv_eps);
     disp = MAXP != 0 && m0.npoles != 0;
   } else {
+    // with every material dispersive the P/J loads need not wait for the
+    // material lookups
+    if (MAXP != 0 && a.all_dispersive) disp = true;
+    if (!a.ids && a.bshift >= 2) {
+      const int mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (x4 >> a.bshift)];
+      const MatF32& m = a.mats[mid];
+      ie = make_float4(m.inv_eps, m.inv_eps, m.inv_eps, m.inv_eps);
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      int mid;
-      if (a.ids) mid = (ids4 >> (8 * e)) & 0xff;
-      else mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (min(x4 + e, a.nx - 1) >> a.bshift)];
-      mids[e] = mid;
-      set_el(ie, e, a.mats[mid].inv_eps);
-      if (MAXP != 0 && a.mats[mid].npoles != 0) disp = true;
+      for (int e = 0; e < 4; e++) mids[e] = mid;
+      if (MAXP != 0 && m.npoles != 0) disp = true;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        int mid;
+        if (a.ids) mid = (ids4 >> (8 * e)) & 0xff;
+        else mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (min(x4 + e, a.nx - 1) >> a.bshift)];
+        mids[e] = mid;
+        set_el(ie, e, a.mats[mid].inv_eps);
+        if (MAXP != 0 && a.mats[mid].npoles != 0) disp = true;
+      }
     }
   }
   st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(exo, uX), dX, ie, g.ok, disp, g.uniform_mat, m0, mids, aX));

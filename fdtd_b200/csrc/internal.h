@@ -144,6 +144,7 @@ struct FusedArgs {
   int bshift, nbx, nby;
   const MatF32* mats;
   int max_poles;  // 0 none, -1 Drude only, 1..2 Lorentz
+  int all_dispersive;  // every material of the table has poles
   int nsrc;
   SourceDev src[kMaxSources];
   float src_scale_d;  // 1/eps0 for D-target sources

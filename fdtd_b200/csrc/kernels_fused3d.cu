@@ -114,51 +114,98 @@ __global__ void __launch_bounds__(32 * kRows) fused3d_h_kernel(const __grid_cons
   }
 }
 
-template <int MAXP>
-__global__ void __launch_bounds__(32 * kRows) flat_e_kernel(const __grid_constant__ FusedArgs a) {
+// NZ consecutive planes per thread: every load of the NZ planes is issued
+// before the first plane is computed; plane k's H (E) doubles as plane k+1's
+// z neighbour in the E (H) sweep. MINB is the CTA count per SM the register
+// allocation targets.
+template <int MAXP, int NZ, int MINB>
+__global__ void __launch_bounds__(32 * kRows, MINB) flat_e_kernel(const __grid_constant__ FusedArgs a) {
   const int lane = threadIdx.x;
   const int x4 = blockIdx.x * 128 + lane * 4;
   const int j = 1 + blockIdx.y * kRows + threadIdx.y;
   const int jl = min(j, a.ny - 2);
-  const int k = 1 + blockIdx.z;
+  const int k0 = 1 + blockIdx.z * NZ;
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
-  const GroupCtx g = make_ctx(a, 0, x4, j, lane, k, k + 1);
-  const long long c = k * sz + jl * sy + x4;
-  const float4 hx = ld4(a.H[0] + c), hy = ld4(a.H[1] + c), hz = ld4(a.H[2] + c);
-  const float4 hx_ym = ld4(a.H[0] + c - sy), hz_ym = ld4(a.H[2] + c - sy);
-  const float4 hx_km = ld4(a.H[0] + c - sz), hy_km = ld4(a.H[1] + c - sz);
-  const float4 ex = ld4(a.E[0] + c), ey = ld4(a.E[1] + c), ez = ld4(a.E[2] + c);
-  const unsigned ids = a.ids ? *reinterpret_cast<const unsigned*>(a.ids + c) : 0u;
-  float hy_xm0 = __shfl_up_sync(kFull, hy.w, 1);
-  float hz_xm0 = __shfl_up_sync(kFull, hz.w, 1);
-  if (lane == 0) {
-    hy_xm0 = a.H[1][c - 1];
-    hz_xm0 = a.H[2][c - 1];
+  const GroupCtx g = make_ctx(a, 0, x4, j, lane, k0, k0 + NZ);
+  const long long c0 = k0 * sz + jl * sy + x4;
+  float4 hx[NZ + 1], hy[NZ + 1], hz[NZ], hx_ym[NZ], hz_ym[NZ], ex[NZ], ey[NZ], ez[NZ];
+  unsigned ids[NZ];
+  hx[0] = ld4(a.H[0] + c0 - sz);
+  hy[0] = ld4(a.H[1] + c0 - sz);
+#pragma unroll
+  for (int q = 0; q < NZ; q++) {
+    const int k = k0 + q;
+    const long long c = c0 + q * sz;
+    const bool in = k <= a.nz - 2;
+    const long long cc = in ? c : c0;  // planes past the grid read a valid plane and are not computed
+    hx[q + 1] = ld4(a.H[0] + cc);
+    hy[q + 1] = ld4(a.H[1] + cc);
+    hz[q] = ld4(a.H[2] + cc);
+    hx_ym[q] = ld4(a.H[0] + cc - sy);
+    hz_ym[q] = ld4(a.H[2] + cc - sy);
+    ex[q] = ld4(a.E[0] + cc);
+    ey[q] = ld4(a.E[1] + cc);
+    ez[q] = ld4(a.E[2] + cc);
+    ids[q] = a.ids ? *reinterpret_cast<const unsigned*>(a.ids + cc) : 0u;
   }
-  e_group_update<MAXP>(a, g, k, hx, hy, hz, hx_ym, hz_ym, hx_km, hy_km, hy_xm0, hz_xm0, ex, ey, ez, ids);
+#pragma unroll
+  for (int q = 0; q < NZ; q++) {
+    const int k = k0 + q;
+    float hy_xm0 = __shfl_up_sync(kFull, hy[q + 1].w, 1);
+    float hz_xm0 = __shfl_up_sync(kFull, hz[q].w, 1);
+    if (k > a.nz - 2) break;
+    if (lane == 0) {
+      const long long c = c0 + q * sz;
+      hy_xm0 = a.H[1][c - 1];
+      hz_xm0 = a.H[2][c - 1];
+    }
+    e_group_update<MAXP>(a, g, k, hx[q + 1], hy[q + 1], hz[q], hx_ym[q], hz_ym[q], hx[q], hy[q], hy_xm0, hz_xm0, ex[q],
+                         ey[q], ez[q], ids[q]);
+  }
 }
 
-__global__ void __launch_bounds__(32 * kRows) flat_h_kernel(const __grid_constant__ FusedArgs a) {
+template <int NZ, int MINB>
+__global__ void __launch_bounds__(32 * kRows, MINB) flat_h_kernel(const __grid_constant__ FusedArgs a) {
   const int lane = threadIdx.x;
   const int x4 = blockIdx.x * 128 + lane * 4;
   const int j = 1 + blockIdx.y * kRows + threadIdx.y;
   const int jl = min(j, a.ny - 2);
-  // planes from the top down, so plane k+1 was read just before plane k
-  const int k = a.nz - 2 - blockIdx.z;
+  // groups of planes from the top down, so the planes above were read just before
+  const int ktop = a.nz - 2 - blockIdx.z * NZ;
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
-  const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
-  const long long c = k * sz + jl * sy + x4;
-  const float4 ex = ld4(a.E[0] + c), ey = ld4(a.E[1] + c), ez = ld4(a.E[2] + c);
-  const float4 ex_yp = ld4(a.E[0] + c + sy), ez_yp = ld4(a.E[2] + c + sy);
-  const float4 ex_kp = ld4(a.E[0] + c + sz), ey_kp = ld4(a.E[1] + c + sz);
-  const float4 hx = ld4(a.H[0] + c), hy = ld4(a.H[1] + c), hz = ld4(a.H[2] + c);
-  float ey_xp3 = __shfl_down_sync(kFull, ey.x, 1);
-  float ez_xp3 = __shfl_down_sync(kFull, ez.x, 1);
-  if (lane == 31) {
-    ey_xp3 = a.E[1][c + 4];
-    ez_xp3 = a.E[2][c + 4];
+  const GroupCtx g = make_ctx(a, 1, x4, j, lane, max(1, ktop - NZ + 1), ktop + 1);
+  const long long ctop = ktop * sz + jl * sy + x4;
+  // index q = 0 is plane ktop, q = 1 plane ktop-1, ...; ex/ey[q] hold plane ktop+1-q
+  float4 ex[NZ + 1], ey[NZ + 1], ez[NZ], ex_yp[NZ], ez_yp[NZ], hx[NZ], hy[NZ], hz[NZ];
+  ex[0] = ld4(a.E[0] + ctop + sz);
+  ey[0] = ld4(a.E[1] + ctop + sz);
+#pragma unroll
+  for (int q = 0; q < NZ; q++) {
+    const int k = ktop - q;
+    const long long cc = k >= 1 ? ctop - q * sz : ctop;
+    ex[q + 1] = ld4(a.E[0] + cc);
+    ey[q + 1] = ld4(a.E[1] + cc);
+    ez[q] = ld4(a.E[2] + cc);
+    ex_yp[q] = ld4(a.E[0] + cc + sy);
+    ez_yp[q] = ld4(a.E[2] + cc + sy);
+    hx[q] = ld4(a.H[0] + cc);
+    hy[q] = ld4(a.H[1] + cc);
+    hz[q] = ld4(a.H[2] + cc);
   }
-  h_group_update(a, g, k, ex, ey, ez, ex_yp, ez_yp, ex_kp, ey_kp, ey_xp3, ez_xp3, hx, hy, hz);
+#pragma unroll
+  for (int q = 0; q < NZ; q++) {
+    const int k = ktop - q;
+    float ey_xp3 = __shfl_down_sync(kFull, ey[q + 1].x, 1);
+    float ez_xp3 = __shfl_down_sync(kFull, ez[q].x, 1);
+    if (k < 1) break;
+    if (lane == 31) {
+      const long long c = ctop - q * sz;
+      ey_xp3 = a.E[1][c + 4];
+      ez_xp3 = a.E[2][c + 4];
+    }
+    h_group_update(a, g, k, ex[q + 1], ey[q + 1], ez[q], ex_yp[q], ez_yp[q], ex[q], ey[q], ey_xp3, ez_xp3, hx[q],
+                   hy[q], hz[q]);
+  }
 }
 
 static int kchunk3d(int nz, int blocks_xy) {
@@ -193,20 +240,28 @@ int launch_fused3d_h(const FusedArgs& a, cudaStream_t s) {
   return 1;
 }
 
-int launch_flat_e(const FusedArgs& a, cudaStream_t s) {
+// Register targets chosen on B200 (Gcell/s of the 384^3 Drude and 768^3
+// two-pole Lorentz workloads): 8 CTAs of 128 threads per SM (<= 64 registers)
+// except the two-pole E sweep, which spills there and takes 6.
+template <int MAXP>
+static void flat_e_dispatch(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRows - 1) / kRows, a.nz - 2), block(32, kRows, 1);
+  flat_e_kernel<MAXP, 1, (MAXP >= 2 ? 6 : 8)><<<grid, block, 0, s>>>(a);
+}
+
+int launch_flat_e(const FusedArgs& a, cudaStream_t s) {
   switch (a.max_poles) {
-    case 0: flat_e_kernel<0><<<grid, block, 0, s>>>(a); break;
-    case -1: flat_e_kernel<-1><<<grid, block, 0, s>>>(a); break;
-    case 1: flat_e_kernel<1><<<grid, block, 0, s>>>(a); break;
-    default: flat_e_kernel<2><<<grid, block, 0, s>>>(a); break;
+    case 0: flat_e_dispatch<0>(a, s); break;
+    case -1: flat_e_dispatch<-1>(a, s); break;
+    case 1: flat_e_dispatch<1>(a, s); break;
+    default: flat_e_dispatch<2>(a, s); break;
   }
   return 1;
 }
 
 int launch_flat_h(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRows - 1) / kRows, a.nz - 2), block(32, kRows, 1);
-  flat_h_kernel<<<grid, block, 0, s>>>(a);
+  flat_h_kernel<1, 8><<<grid, block, 0, s>>>(a);
   return 1;
 }
 
