@@ -1,0 +1,515 @@
+// fdtd_b200.hpp: pederson/fdtd's functor names over the fdtd_b200 C ABI.
+//
+// In the reference a user applies update functors to a container of cells,
+// once per pass of a time loop (tests/testTM.cpp:102-113). Here the same
+// functor types are handed to a gpu::Grid once, as the plan of one step; the
+// grid checks the plan against the fused schedule and then runs any number of
+// steps on the GPU:
+//
+//   gpu::Grid<TM, double> grid(256, 256, 1, dx, dt, 2000);
+//   grid.set_pml(Dir::X, 16); grid.set_pml(Dir::Y, 16);
+//   auto src = grid.add(make_soft_source<Ez>(signal, grid.cell(128, 128)));
+//   grid.plan({YeeUpdate<TM, Dz>(dt, dx),
+//              UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx), ...,
+//              VacuumUpdate<TM, FieldType::Electric>(), src, ...});
+//   grid.step(2000);
+//
+// Header-only; link with libfdtd_b200.so. Errors throw fdtd::gpu::Error
+// carrying the C status and message.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <functional>
+#include <initializer_list>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fdtd_b200.h"
+
+namespace fdtd {
+
+// ------------------------------------------------------------ vocabulary
+// Modes, field types, directions and field tags as in
+// include/FDTDConstants.hpp:410-445, :457-486, :648-744.
+struct EMMode {};
+struct TEM : EMMode { static constexpr int value = FDTD_TEM, dim = 1; };
+struct TE : EMMode { static constexpr int value = FDTD_TE, dim = 2; };
+struct TM : EMMode { static constexpr int value = FDTD_TM, dim = 2; };
+struct ThreeD : EMMode { static constexpr int value = FDTD_THREED, dim = 3; };
+
+enum class FieldType : char { Electric = 0, Magnetic, NONE };
+enum class Dir : char { X = 0, Y, Z, NONE };
+enum class Orientation : char { MIN = 0, MAX, NONE };
+
+namespace detail {
+template <int Which, FieldType FT, int Comp, bool Flux>
+struct FieldTag {
+  static constexpr int which = Which;      // fdtd_download selector
+  static constexpr FieldType field_type = FT;
+  static constexpr int comp = Comp;        // 0..2 = x, y, z
+  static constexpr bool flux = Flux;       // D/B (true) or E/H
+};
+}  // namespace detail
+struct Ex : detail::FieldTag<FDTD_EX, FieldType::Electric, 0, false> {};
+struct Ey : detail::FieldTag<FDTD_EY, FieldType::Electric, 1, false> {};
+struct Ez : detail::FieldTag<FDTD_EZ, FieldType::Electric, 2, false> {};
+struct Dx : detail::FieldTag<FDTD_DX, FieldType::Electric, 0, true> {};
+struct Dy : detail::FieldTag<FDTD_DY, FieldType::Electric, 1, true> {};
+struct Dz : detail::FieldTag<FDTD_DZ, FieldType::Electric, 2, true> {};
+struct Hx : detail::FieldTag<FDTD_HX, FieldType::Magnetic, 0, false> {};
+struct Hy : detail::FieldTag<FDTD_HY, FieldType::Magnetic, 1, false> {};
+struct Hz : detail::FieldTag<FDTD_HZ, FieldType::Magnetic, 2, false> {};
+struct Bx : detail::FieldTag<FDTD_BX, FieldType::Magnetic, 0, true> {};
+struct By : detail::FieldTag<FDTD_BY, FieldType::Magnetic, 1, true> {};
+struct Bz : detail::FieldTag<FDTD_BZ, FieldType::Magnetic, 2, true> {};
+
+// include/FDTDConstants.hpp:394-398 (imp0 with the reference's Newton sqrt)
+constexpr double pi = 3.14159265358979323846264338327950288;
+constexpr double eps0 = 8.854e-12;
+constexpr double mu0 = pi * 4.0e-7;
+constexpr double c0 = 2.99792458e+8;
+namespace detail {
+constexpr double newton_sqrt(double x, double curr, double prev) {
+  return curr == prev ? curr : newton_sqrt(x, 0.5 * (curr + x / curr), curr);
+}
+}  // namespace detail
+constexpr double imp0 = detail::newton_sqrt(mu0 / eps0, mu0 / eps0, 0);
+
+template <class Mode>
+constexpr bool has_component(FieldType ft, int c) {
+  return Mode::value == FDTD_THREED ||
+         (ft == FieldType::Electric ? ((Mode::value == FDTD_TE && c < 2) || (Mode::value == FDTD_TM && c == 2))
+                                    : ((Mode::value == FDTD_TE && c == 2) || (Mode::value == FDTD_TM && c < 2)));
+}
+
+// ------------------------------------------------------------ signals
+// SinData / RickerData (include/Source.hpp:100-167)
+struct Sinusoid {
+  double freq, phase, delay;
+  explicit Sinusoid(double f, double ph = 0) : freq(f), phase(ph), delay(10.0 / f * pi / 2.0) {}
+  double operator()(double t) const { return std::tanh(t / delay) * std::sin(freq * t + phase); }
+};
+struct Ricker {
+  double freq, delay;
+  explicit Ricker(double f) : freq(f), delay(2.0 / f) {}
+  double operator()(double t) const {
+    const double p = pi * freq * (t - delay);
+    return (1.0 - 2.0 * p * p) * std::exp(-p * p);
+  }
+};
+
+// ------------------------------------------------------------ plan ops
+namespace detail {
+enum class OpKind { Yee, Pml, Material, Source, TfsfD, TfsfB };
+struct Op {
+  OpKind kind;
+  FieldType ft = FieldType::NONE;
+  int comp = -1, axis = -1;
+  fdtd_material mat{};
+  int source = -1, plane = -1;
+};
+inline fdtd_material blank_material(int kind) {
+  fdtd_material m{};
+  m.kind = kind;
+  m.eps_inf = 1.0;
+  m.mu_r = 1.0;
+  return m;
+}
+}  // namespace detail
+
+// YeeUpdate<Mode, Flux> (include/YeeUpdates.hpp:343-405); BD1 only
+template <class Mode, class Flux>
+struct YeeUpdate {
+  static_assert(Flux::flux, "YeeUpdate acts on a flux component (D or B)");
+  double dt, dx;
+  YeeUpdate(double deltat, double deltax) : dt(deltat), dx(deltax) {}
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Yee};
+    o.ft = Flux::field_type;
+    o.comp = Flux::comp;
+    return o;
+  }
+};
+
+// UpdatePML<Mode, FieldType, Dir> (include/PML.hpp:296-355)
+template <class Mode, FieldType ft, Dir d>
+struct UpdatePML {
+  double dt, dx;
+  UpdatePML(double deltat, double deltax) : dt(deltat), dx(deltax) {}
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Pml};
+    o.ft = ft;
+    o.axis = static_cast<int>(d);
+    return o;
+  }
+};
+
+// Material updates (include/DispersiveMaterials.hpp:489-497, :881-884, :1208-1211)
+template <class Mode, FieldType ft, bool forward = false>
+struct VacuumUpdate {
+  static_assert(!forward, "only the implicit (forward = false) update is on the GPU path");
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = ft;
+    o.mat = detail::blank_material(FDTD_VACUUM);
+    return o;
+  }
+};
+template <class Mode, FieldType ft, bool forward = false>
+struct ConstantUpdate {
+  static_assert(!forward, "only the implicit (forward = false) update is on the GPU path");
+  double K;
+  explicit ConstantUpdate(double k) : K(k) {}
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = ft;
+    o.mat = detail::blank_material(FDTD_CONSTANT);
+    if (ft == FieldType::Electric) o.mat.eps_inf = K;
+    else o.mat.mu_r = K;
+    return o;
+  }
+};
+template <class Mode, FieldType ft, bool forward = false>
+struct DrudeUpdate {
+  static_assert(ft == FieldType::Electric && !forward, "Drude acts on the electric field, implicitly");
+  double K, Freq, Gamma;
+  DrudeUpdate(double k, double freq, double gamma, double /*dt*/ = 0) : K(k), Freq(freq), Gamma(gamma) {}
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = ft;
+    o.mat = detail::blank_material(FDTD_DRUDE);
+    o.mat.eps_inf = K;
+    o.mat.npoles = 1;
+    o.mat.delta_eps[0] = 1.0;
+    o.mat.freq[0] = Freq;
+    o.mat.gamma[0] = Gamma;
+    return o;
+  }
+};
+// The reference ignores Delta (include/DispersiveMaterials.hpp:710-735); so does
+// this functor. LorentzPoles below takes per-pole strengths.
+template <class Mode, FieldType ft, bool forward = false>
+struct LorentzUpdate {
+  static_assert(ft == FieldType::Electric && !forward, "Lorentz acts on the electric field, implicitly");
+  double K, Delta, Freq, Gamma;
+  LorentzUpdate(double k, double delta, double freq, double gamma, double /*dt*/ = 0)
+      : K(k), Delta(delta), Freq(freq), Gamma(gamma) {}
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = ft;
+    o.mat = detail::blank_material(FDTD_LORENTZ);
+    o.mat.eps_inf = K;
+    o.mat.npoles = 1;
+    o.mat.delta_eps[0] = 1.0;
+    o.mat.freq[0] = Freq;
+    o.mat.gamma[0] = Gamma;
+    return o;
+  }
+};
+// Multi-pole Lorentz (an extension): E = (D - sum P_q)/(eps_inf eps0),
+// J_q' = a_q J_q + b_q (delta_q eps0 E - P_q).
+struct LorentzPoles {
+  double eps_inf;
+  std::vector<std::array<double, 3>> poles;  // (delta_eps, freq, gamma)
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = FieldType::Electric;
+    o.mat = detail::blank_material(FDTD_LORENTZ);
+    o.mat.eps_inf = eps_inf;
+    o.mat.npoles = static_cast<int>(poles.size());
+    for (size_t q = 0; q < poles.size() && q < FDTD_MAX_POLES; q++) {
+      o.mat.delta_eps[q] = poles[q][0];
+      o.mat.freq[q] = poles[q][1];
+      o.mat.gamma[q] = poles[q][2];
+    }
+    return o;
+  }
+};
+
+// PMLParameterModel (include/PML.hpp:368-393): the grading the GPU applies.
+struct PMLParameterModel {
+  double mM, mMa, msMax, mkMax, maMax;
+  explicit PMLParameterModel(double dx) : mM(3), mMa(1), msMax(0.8 * (3 + 1) / (imp0 * dx)), mkMax(5), maMax(0.05) {}
+  double K(double x) const { return x < 0.0 ? 1.0 : (x > 1.0 ? 1.0 : 1.0 + std::pow(x, mM) * (mkMax - 1.0)); }
+  double S(double x) const { return x < 0.0 ? 0.0 : (x > 1.0 ? 0.0 : std::pow(x, mM) * msMax); }
+  double A(double x) const { return x < 0.0 ? 0.0 : (x > 1.0 ? 0.0 : std::pow(1.0 - x, mMa) * maMax); }
+};
+
+namespace gpu {
+
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string& msg) : std::runtime_error(msg), code(code) {}
+  int code;
+};
+inline void check(int rc) {
+  if (rc != FDTD_OK) throw Error(rc, fdtd_last_error_string());
+}
+
+struct CellRef {
+  int i, j, k;
+};
+
+}  // namespace gpu
+
+// SoftSource<Signal, Cell, GetField<F>> (include/Source.hpp:183-261):
+// the signal is evaluated at t = n*dt for step n.
+struct SoftSourceSpec {
+  int comp, target;
+  gpu::CellRef cell;
+  std::function<double(double)> signal;
+  int index = -1;
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Source};
+    o.ft = FieldType::Electric;
+    o.comp = comp;
+    o.source = index;
+    o.axis = target;
+    return o;
+  }
+};
+template <class F, class Signal>
+SoftSourceSpec make_soft_source(Signal sig, gpu::CellRef c) {
+  static_assert(F::field_type == FieldType::Electric, "soft sources act on E or D");
+  return SoftSourceSpec{F::comp, F::flux ? 1 : 0, c, std::function<double(double)>(sig)};
+}
+
+// Aux1D (include/Source.hpp:280-462): the source is evaluated at the
+// accumulated aux time t_s = t_{s-1} + dt, as Aux1D::time_step does.
+template <typename scalar = double>
+struct Aux1D {
+  int ncells;
+  double dx, dt;
+  std::function<double(double)> signal;
+  template <class Signal>
+  Aux1D(int n, double deltax, double deltat, Signal sig) : ncells(n), dx(deltax), dt(deltat), signal(sig) {}
+  std::vector<double> table(int nsteps) const {
+    std::vector<double> v(nsteps);
+    double t = 0;
+    for (int s = 0; s < nsteps; s++) {
+      t += dt;
+      v[s] = signal(t);
+    }
+    return v;
+  }
+};
+
+// TFSFPlane (include/Source.hpp:472-634): cells lo..hi, normal along dd with
+// orientation o, location functor ((i,j,k) - origin) * dx. The polarisation
+// defaults to the reference's for TE/TM; pass it for ThreeD (where the
+// reference leaves it unset) or to override.
+struct TFSFPlaneSpec {
+  int axis, orient;
+  std::array<int, 3> lo, hi;
+  std::array<double, 3> origin, k, pol_e, pol_h;
+  std::shared_ptr<Aux1D<double>> aux;
+  int index = -1;
+  struct D {
+    int index;
+    operator detail::Op() const {
+      detail::Op o{detail::OpKind::TfsfD};
+      o.plane = index;
+      return o;
+    }
+  };
+  struct B {
+    int index;
+    operator detail::Op() const {
+      detail::Op o{detail::OpKind::TfsfB};
+      o.plane = index;
+      return o;
+    }
+  };
+};
+template <class Mode, Dir dd, Orientation o>
+TFSFPlaneSpec make_tfsf_plane(std::array<int, 3> lo, std::array<int, 3> hi, std::array<double, 3> origin,
+                              std::array<double, 3> k, std::shared_ptr<Aux1D<double>> aux,
+                              const std::array<double, 3>* pol_e = nullptr, const std::array<double, 3>* pol_h = nullptr) {
+  TFSFPlaneSpec p;
+  p.axis = static_cast<int>(dd);
+  p.orient = o == Orientation::MAX ? 1 : 0;
+  p.lo = lo;
+  p.hi = hi;
+  p.origin = origin;
+  p.k = k;
+  p.aux = aux;
+  double K = 0;
+  for (int d = 0; d < Mode::dim; d++) K += k[d] * k[d];
+  K = std::sqrt(K);
+  std::array<double, 3> kn{0, 0, 0};
+  for (int d = 0; d < Mode::dim; d++) kn[d] = k[d] / K;
+  if (Mode::value == FDTD_TE) {  // Source.hpp:573-576
+    p.pol_h = {0, 0, 1};
+    p.pol_e = {kn[1], -kn[0], 0};
+  } else {  // TM and TEM (Source.hpp:577-584); ThreeD: E along z, H along the aux Hy
+    p.pol_e = {0, 0, 1};
+    p.pol_h = Mode::value == FDTD_TM ? std::array<double, 3>{kn[1], -kn[0], 0} : std::array<double, 3>{0, 1, 0};
+  }
+  if (pol_e) p.pol_e = *pol_e;
+  if (pol_h) p.pol_h = *pol_h;
+  return p;
+}
+
+namespace gpu {
+
+// A grid of Mode on one GPU; Real = double for the FP64 plain method, float
+// for the FP32 fused method. max_steps bounds the steps for which source
+// signals are tabulated.
+template <class Mode, class Real>
+class Grid {
+  static_assert(Mode::value != FDTD_TEM, "the GPU grid holds TE, TM or ThreeD");
+
+ public:
+  Grid(int nx, int ny, int nz, double dx, double dt, int max_steps, int device = 0)
+      : dx_(dx), dt_(dt), max_steps_(max_steps) {
+    fdtd_grid_desc d{Mode::value, std::is_same<Real, double>::value ? FDTD_PLAIN_F64 : FDTD_FUSED_F32,
+                     nx, ny, nz, dx, dt, device};
+    fdtd_grid* g = nullptr;
+    check(fdtd_grid_create(&d, &g));
+    g_.reset(g);
+    n_ = {nx, ny, nz};
+  }
+
+  CellRef cell(int i, int j, int k = 0) const { return CellRef{i, j, k}; }
+  fdtd_grid* handle() const { return g_.get(); }
+
+  // CPML of n cells on one side, or on both sides, of an axis
+  void set_pml(Dir d, Orientation o, int n) {
+    check(fdtd_set_pml(g_.get(), static_cast<int>(d), o == Orientation::MAX ? 1 : 0, n));
+    pml_axes_[static_cast<int>(d)] = true;
+  }
+  void set_pml(Dir d, int n) {
+    set_pml(d, Orientation::MIN, n);
+    set_pml(d, Orientation::MAX, n);
+  }
+
+  // A per-cell material map: ids index `mats` (the role of MaterialMap,
+  // include/MaterialMap.hpp:204-284). The plan's material op must then be
+  // MaterialMapUpdate.
+  void set_material_map(const std::vector<detail::Op>& mats, const std::vector<uint8_t>& ids) {
+    std::vector<fdtd_material> m;
+    for (auto& o : mats) m.push_back(o.mat);
+    check(fdtd_set_materials(g_.get(), m.data(), static_cast<int>(m.size())));
+    check(fdtd_set_material_ids(g_.get(), ids.data()));
+    has_map_ = true;
+  }
+
+  SoftSourceSpec add(SoftSourceSpec s) {
+    std::vector<double> v(max_steps_);
+    for (int n = 0; n < max_steps_; n++) v[n] = s.signal(n * dt_);
+    check(fdtd_add_source(g_.get(), s.comp, s.target, s.cell.i, s.cell.j, s.cell.k, v.data(), max_steps_));
+    s.index = nsrc_++;
+    return s;
+  }
+  TFSFPlaneSpec add(TFSFPlaneSpec p) {
+    const std::vector<double> v = p.aux->table(max_steps_ + 1);
+    check(fdtd_add_tfsf_plane(g_.get(), p.axis, p.orient, p.lo.data(), p.hi.data(), p.origin.data(), p.k.data(),
+                              p.pol_e.data(), p.pol_h.data(), p.aux->ncells, v.data(), static_cast<int>(v.size())));
+    p.index = nplanes_++;
+    return p;
+  }
+
+  // The plan of one step, checked against the fused schedule.
+  void plan(std::initializer_list<detail::Op> ops) {
+    plan_.assign(ops.begin(), ops.end());
+    validate();
+  }
+
+  void step(int n) {
+    if (!validated_) throw Error(FDTD_ERR_INVALID, "no plan: call plan() first");
+    if (steps_ + n > max_steps_) throw Error(FDTD_ERR_INVALID, "more steps than the grid was created for");
+    check(fdtd_step(g_.get(), n, nullptr));
+    steps_ += n;
+  }
+
+  template <class F>
+  std::vector<double> get() const {
+    std::vector<double> v(static_cast<size_t>(n_[0]) * n_[1] * n_[2]);
+    check(fdtd_download(g_.get(), F::which, v.data()));
+    return v;
+  }
+
+ private:
+  struct Deleter {
+    void operator()(fdtd_grid* g) const { fdtd_grid_destroy(g); }
+  };
+
+  // E half: Yee on every E flux, TFSF D, D-target sources, CPML E per axis
+  // in X, Y, Z order, material E, E-target sources; H half: Yee on every B
+  // flux, TFSF B, CPML H, material H (tests/testTM.cpp:102-113).
+  void validate() {
+    size_t q = 0;
+    auto fail = [](const std::string& m) { throw Error(FDTD_ERR_UNSUPPORTED, "plan: " + m); };
+    for (int half = 0; half < 2; half++) {
+      const FieldType ft = half == 0 ? FieldType::Electric : FieldType::Magnetic;
+      bool seen[3] = {false, false, false};
+      while (q < plan_.size() && plan_[q].kind == detail::OpKind::Yee && plan_[q].ft == ft) {
+        if (seen[plan_[q].comp]) fail("a YeeUpdate appears twice");
+        seen[plan_[q].comp] = true;
+        q++;
+      }
+      for (int c = 0; c < 3; c++)
+        if (has_component<Mode>(ft, c) != seen[c]) fail("YeeUpdate must cover exactly the mode's flux components");
+      const detail::OpKind tf = half == 0 ? detail::OpKind::TfsfD : detail::OpKind::TfsfB;
+      int planes = 0;
+      while (q < plan_.size() && plan_[q].kind == tf) {
+        planes++;
+        q++;
+      }
+      if (planes != 0 && planes != nplanes_) fail("every TFSF plane must be updated");
+      if (half == 0)
+        while (q < plan_.size() && plan_[q].kind == detail::OpKind::Source && plan_[q].axis == 1) q++;
+      int last_axis = -1;
+      bool axes[3] = {false, false, false};
+      while (q < plan_.size() && plan_[q].kind == detail::OpKind::Pml && plan_[q].ft == ft) {
+        if (plan_[q].axis <= last_axis) fail("UpdatePML axes must come in X, Y, Z order");
+        last_axis = plan_[q].axis;
+        axes[last_axis] = true;
+        q++;
+      }
+      for (int a = 0; a < 3; a++)
+        if (axes[a] != pml_axes_[a]) fail("UpdatePML must cover exactly the axes with CPML");
+      if (q >= plan_.size() || plan_[q].kind != detail::OpKind::Material || plan_[q].ft != ft)
+        fail("a material update of the half step is missing");
+      if (half == 0) mat_e_ = plan_[q].mat;
+      else mat_h_ = plan_[q].mat;
+      q++;
+      if (half == 0)
+        while (q < plan_.size() && plan_[q].kind == detail::OpKind::Source && plan_[q].axis == 0) q++;
+    }
+    if (q != plan_.size()) fail("operations after the magnetic material update");
+    if (!has_map_) {
+      fdtd_material m = mat_e_;
+      m.mu_r = mat_h_.mu_r;
+      check(fdtd_set_materials(g_.get(), &m, 1));
+    }
+    validated_ = true;
+  }
+
+  std::unique_ptr<fdtd_grid, Deleter> g_;
+  std::array<int, 3> n_{};
+  double dx_, dt_;
+  int max_steps_, steps_ = 0, nsrc_ = 0, nplanes_ = 0;
+  bool pml_axes_[3] = {false, false, false};
+  bool has_map_ = false, validated_ = false;
+  std::vector<detail::Op> plan_;
+  fdtd_material mat_e_{}, mat_h_{};
+};
+
+// The material op of a plan whose grid carries a per-cell material map.
+struct MaterialMapUpdate {
+  FieldType ft;
+  operator detail::Op() const {
+    detail::Op o{detail::OpKind::Material};
+    o.ft = ft;
+    o.mat = detail::blank_material(FDTD_VACUUM);
+    return o;
+  }
+};
+
+}  // namespace gpu
+}  // namespace fdtd

@@ -1,0 +1,53 @@
+"""The C++ drop-in layer (include/fdtd_b200.hpp): tests/cpp/drop_in.cpp writes
+the reference's time loop with the reference's functor names, runs it on the
+GPU, and its fields are compared with the CPU oracle on the same problem."""
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import scenarios
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def drop_in(fdtd, tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "drop_in")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "drop_in.cpp"), "-L" + os.path.dirname(fdtd.LIB_PATH),
+                    "-lfdtd_b200", "-Wl,-rpath," + os.path.dirname(fdtd.LIB_PATH), "-o", exe], check=True)
+    return exe
+
+
+def run(exe, which, tmp_path, nfields, shape):
+    out = str(tmp_path / f"{which}.bin")
+    subprocess.run([exe, which, out], check=True)
+    return np.fromfile(out, dtype=np.float64).reshape(nfields, *shape)
+
+
+def test_tm_plain_through_templates(drop_in, oracle, tmp_path):
+    from fdtd_b200.problem import TM, Problem, Source, courant_dt
+    p = Problem(TM, (40, 36, 1), 1e-6, courant_dt(1e-6, 0.99 / math.sqrt(2.0)))
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    n = np.arange(80, dtype=np.float64)
+    p.sources.append(Source(2, (20, 18, 0), np.exp(-(((n - 20.0) / 6.0) ** 2)), "E"))
+    o = oracle.run_oracle(p, 80)
+    got = run(drop_in, "tm", tmp_path, 3, (1, 36, 40))
+    for q, name in enumerate(["Ez", "Hx", "Hy"]):
+        assert rel_l2(got[q], o.get(name)) <= 1e-12, name
+
+
+def test_3d_fused_material_map_tfsf_through_templates(drop_in, oracle, tmp_path):
+    p = scenarios.td_tfsf_box()
+    o = oracle.run_oracle(p)
+    got = run(drop_in, "td", tmp_path, 6, (24, 24, 24))
+    for q, name in enumerate(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]):
+        assert rel_l2(got[q], o.get(name)) <= 1e-4, name
