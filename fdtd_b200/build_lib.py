@@ -30,6 +30,7 @@ SOURCES = {
     "kernels_fused3d.cu": [],
     "kernels_fused3d_tma.cu": [],
     "kernels_tfsf.cu": [],
+    "kernels_batch.cu": [],
     "kernels_common.cu": [],
     "fdtd_capi.cu": [],
 }

@@ -127,6 +127,7 @@ struct fdtd_grid {
   bool f32 = false;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
+  std::map<void*, size_t> sizes;
   long long bytes = 0;
   long long launches = 0;
   long long t = 0;
@@ -195,6 +196,7 @@ int dalloc(fdtd_grid* g, void** p, size_t bytes) {
   e = cudaMemsetAsync(*p, 0, bytes, g->stream);
   if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
   g->allocs.push_back(*p);
+  g->sizes[*p] = bytes;
   g->bytes += static_cast<long long>(bytes);
   return FDTD_OK;
 }
@@ -207,6 +209,11 @@ void dfree(fdtd_grid* g, void* p) {
       g->allocs.erase(g->allocs.begin() + q);
       break;
     }
+  auto it = g->sizes.find(p);
+  if (it != g->sizes.end()) {
+    g->bytes -= static_cast<long long>(it->second);
+    g->sizes.erase(it);
+  }
   cudaFree(p);
 }
 
@@ -574,6 +581,8 @@ FusedArgs fused_args(fdtd_grid* g) {
   for (auto& m : g->mats)
     if (m.kind != FDTD_DRUDE && m.kind != FDTD_LORENTZ) a.all_dispersive = 0;
   a.src_scale_d = static_cast<float>(1.0 / kEps0);
+  a.src_scale_b = static_cast<float>(eta() / kMu0);
+  a.src_scale_h = static_cast<float>(eta());
   a.src_last = g->d_src_last;
   a.dx = g->d.dx;
   a.dt = g->d.dt;
@@ -750,8 +759,9 @@ int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids,
 
 int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {
   if (!g || (!vals && nvals > 0)) return fail(FDTD_ERR_INVALID, "null argument");
-  if (comp < 0 || comp > 2 || !hasE(g->d.mode, comp)) return fail(FDTD_ERR_INVALID, "component not in this mode");
-  if (target < 0 || target > 1) return fail(FDTD_ERR_INVALID, "target must be 0 (E) or 1 (D)");
+  if (target < 0 || target > 3) return fail(FDTD_ERR_INVALID, "target must be 0 (E), 1 (D), 2 (H) or 3 (B)");
+  if (comp < 0 || comp > 2 || !(target < 2 ? hasE(g->d.mode, comp) : hasH(g->d.mode, comp)))
+    return fail(FDTD_ERR_INVALID, "component not in this mode");
   if (!interior(g, i, j, k)) return fail(FDTD_ERR_INVALID, "source cell must be an interior cell");
   if (g->srcs.size() >= static_cast<size_t>(kMaxSources)) return fail(FDTD_ERR_UNSUPPORTED, "too many sources");
   if (nvals < 0) return fail(FDTD_ERR_INVALID, "nvals < 0");
@@ -1241,6 +1251,289 @@ int fdtd_launch_count(fdtd_grid* g, long long* count) {
 int fdtd_memory_bytes(fdtd_grid* g, long long* bytes) {
   if (!g || !bytes) return fail(FDTD_ERR_INVALID, "null argument");
   *bytes = g->bytes;
+  return FDTD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches
+
+struct fdtd_batch {
+  std::vector<fdtd_grid*> grids;
+  int mode = 0, maxp = 0, device = 0;
+  FusedArgs* d_args = nullptr;
+  Control** d_ctrls = nullptr;
+  BatchCtl* d_ctl = nullptr;
+  unsigned* d_items = nullptr;
+  int nitems = 0, rows = 0, blocks = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;  // keyed by steps per launch
+  std::vector<float> tune_ms;            // measured ms per step of rows 1, 2, 4, 8
+};
+
+namespace {
+
+// the mutable state of a grid (what a step changes): fields, poles, CPML
+// integrators, source bookkeeping and the step counter
+std::vector<std::pair<void*, size_t>> grid_state(fdtd_grid* g) {
+  std::vector<void*> ptrs;
+  for (int c = 0; c < 3; c++) {
+    ptrs.push_back(g->E[c]);
+    ptrs.push_back(g->H[c]);
+    for (int q = 0; q < kMaxPoles; q++) {
+      ptrs.push_back(g->P[q][c]);
+      ptrs.push_back(g->J[q][c]);
+    }
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int I = 0; I < 3; I++)
+      for (int J = 0; J < 3; J++) ptrs.push_back(g->psi[ft][I][J]);
+  ptrs.push_back(g->d_src_last);
+  ptrs.push_back(g->ctrl);
+  std::vector<std::pair<void*, size_t>> out;
+  for (void* p : ptrs)
+    if (p && g->sizes.count(p)) out.emplace_back(p, g->sizes[p]);
+  return out;
+}
+
+int batch_items(fdtd_batch* b, int rows) {
+  std::vector<unsigned> items;
+  for (size_t q = 0; q < b->grids.size(); q++) {
+    const fdtd_grid* g = b->grids[q];
+    const int tx = g->pitch / 128, ty = (g->n[1] - 2 + rows - 1) / rows;
+    for (int t = 0; t < tx * ty; t++) items.push_back(static_cast<unsigned>(q) << 24 | static_cast<unsigned>(t));
+  }
+  // consecutive items (tiles of one grid) go to consecutive CTAs
+  b->nitems = static_cast<int>(items.size());
+  if (b->d_items) cudaFree(b->d_items);
+  b->d_items = nullptr;
+  CK(cudaMalloc(&b->d_items, items.size() * sizeof(unsigned)));
+  CK(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  void* fn = batch_kernel_ptr(b->mode, b->maxp, rows);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * rows, 0));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  if (per_sm < 1) return fail(FDTD_ERR_CUDA, "batch kernel does not fit on an SM");
+  b->blocks = std::min(b->nitems, per_sm * sms);
+  b->rows = rows;
+  return FDTD_OK;
+}
+
+int batch_launch(fdtd_batch* b, int nsteps, cudaStream_t s) {
+  void* fn = batch_kernel_ptr(b->mode, b->maxp, b->rows);
+  const FusedArgs* args = b->d_args;
+  const unsigned* items = b->d_items;
+  int nitems = b->nitems;
+  BatchCtl* ctl = b->d_ctl;
+  void* params[] = {&args, &items, &nitems, &ctl, &nsteps};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(b->blocks);
+  cfg.blockDim = dim3(32, b->rows);
+  cfg.stream = s;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeCooperative;
+  attr.val.cooperative = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelExC(&cfg, fn, params));
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
+  if (!grids || !out || n < 1) return fail(FDTD_ERR_INVALID, "need at least one grid");
+  if (n > 255) return fail(FDTD_ERR_UNSUPPORTED, "at most 255 grids per batch");
+  *out = nullptr;
+  fdtd_batch* b = new fdtd_batch();
+  b->grids.assign(grids, grids + n);
+  const fdtd_grid* g0 = grids[0];
+  b->mode = g0->d.mode;
+  b->device = g0->d.device;
+  for (auto* g : b->grids) {
+    const char* why = nullptr;
+    if (!g) why = "null grid";
+    else if (!g->f32) why = "batched grids use the FP32 fused method";
+    else if (g->d.mode != FDTD_TE && g->d.mode != FDTD_TM) why = "batched grids are 2D (TE or TM)";
+    else if (g->d.mode != b->mode) why = "batched grids share one mode";
+    else if (g->d.device != b->device) why = "batched grids share one device";
+    else if (!g->planes.empty() || !g->dfts.empty()) why = "batched grids carry no TFSF planes or DFT regions";
+    else if (g->t != g0->t) why = "batched grids must have taken the same number of steps";
+    else if (static_cast<long long>(g->pitch / 128) * g->n[1] >= (1 << 24)) why = "grid too large to batch";
+    if (why) {
+      delete b;
+      return fail(FDTD_ERR_UNSUPPORTED, why);
+    }
+    b->maxp = std::max(b->maxp, g->max_poles == -1 ? 1 : g->max_poles);
+  }
+  if (b->maxp == 1) {
+    // Drude-only batches keep the Drude kernel (no P arrays)
+    bool lorentz = false;
+    for (auto* g : b->grids) lorentz = lorentz || g->max_poles > 0;
+    if (!lorentz) b->maxp = -1;
+  }
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  std::vector<FusedArgs> args;
+  std::vector<Control*> ctrls;
+  for (auto* g : b->grids) {
+    CK(cudaStreamSynchronize(g->stream));
+    args.push_back(fused_args(g));
+    ctrls.push_back(g->ctrl);
+  }
+  CK(cudaMalloc(&b->d_args, args.size() * sizeof(FusedArgs)));
+  CK(cudaMemcpy(b->d_args, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&b->d_ctrls, ctrls.size() * sizeof(Control*)));
+  CK(cudaMemcpy(b->d_ctrls, ctrls.data(), ctrls.size() * sizeof(Control*), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&b->d_ctl, sizeof(BatchCtl)));
+  CK(cudaMemset(b->d_ctl, 0, sizeof(BatchCtl)));
+  int rc = batch_items(b, 4);
+  if (rc) {
+    fdtd_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return FDTD_OK;
+}
+
+int fdtd_batch_destroy(fdtd_batch* b) {
+  if (!b) return FDTD_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  cudaFree(b->d_args);
+  cudaFree(b->d_ctrls);
+  cudaFree(b->d_ctl);
+  cudaFree(b->d_items);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return FDTD_OK;
+}
+
+// Times every tile height on a copy of the state (restored afterwards) and
+// keeps the fastest.
+int fdtd_batch_tune(fdtd_batch* b, int steps) {
+  if (!b || steps < 1) return fail(FDTD_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(b->device));
+  CK(cudaDeviceSynchronize());
+  std::vector<std::pair<void*, size_t>> state;
+  for (auto* g : b->grids)
+    for (auto& st : grid_state(g)) state.push_back(st);
+  size_t total = 0;
+  for (auto& st : state) total += (st.second + 255) / 256 * 256;
+  void* scratch = nullptr;
+  CK(cudaMalloc(&scratch, total));
+  auto copy = [&](bool save) -> int {
+    size_t off = 0;
+    for (auto& st : state) {
+      char* sp = static_cast<char*>(scratch) + off;
+      CK(cudaMemcpyAsync(save ? sp : st.first, save ? st.first : sp, st.second, cudaMemcpyDeviceToDevice, b->stream));
+      off += (st.second + 255) / 256 * 256;
+    }
+    return FDTD_OK;
+  };
+  int rc = copy(true);
+  const int cand[4] = {1, 2, 4, 8};
+  float best = 1e30f;
+  int best_rows = 4;
+  b->tune_ms.assign(4, 0.f);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int q = 0; q < 4 && !rc; q++) {
+    rc = batch_items(b, cand[q]);
+    if (!rc) rc = batch_launch(b, 1, b->stream);  // warm-up
+    if (!rc) rc = copy(false);
+    CK(cudaEventRecord(e0, b->stream));
+    if (!rc) rc = batch_launch(b, steps, b->stream);
+    CK(cudaEventRecord(e1, b->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    b->tune_ms[q] = ms / steps;
+    if (ms < best) {
+      best = ms;
+      best_rows = cand[q];
+    }
+    if (!rc) rc = copy(false);
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (rc) return rc;
+  int err = 0;
+  CK(cudaMemcpy(&err, &b->d_ctl->error, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return fail(FDTD_ERR_TIMEOUT, "a batch grid barrier expired while tuning");
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  return batch_items(b, best_rows);
+}
+
+int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
+  if (!b || nsteps < 0) return fail(FDTD_ERR_INVALID, "bad argument");
+  if (nsteps == 0) return FDTD_OK;
+  CK(cudaSetDevice(b->device));
+  for (auto* g : b->grids)
+    if (g->t != b->grids[0]->t) return fail(FDTD_ERR_INVALID, "a batched grid was stepped on its own");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  for (auto* g : b->grids) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, g->stream));
+    CK(cudaStreamWaitEvent(s, ev, 0));
+    CK(cudaEventDestroy(ev));
+  }
+  // one persistent kernel for all the steps and the step counters, replayed
+  // from a CUDA graph
+  auto it = b->graphs.find(nsteps);
+  if (it == b->graphs.end()) {
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_launch(b, nsteps, s);
+    if (!rc) launch_batch_advance(b->d_ctrls, static_cast<int>(b->grids.size()), nsteps, s);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(e));
+    it = b->graphs.emplace(nsteps, exec).first;
+  }
+  CK(cudaGraphLaunch(it->second, s));
+  for (auto* g : b->grids) {
+    g->t += nsteps;
+    g->launches += 2;
+  }
+  // later work on any member grid's own stream follows the batch
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, s));
+  for (auto* g : b->grids) CK(cudaStreamWaitEvent(g->stream, ev, 0));
+  CK(cudaEventDestroy(ev));
+  return FDTD_OK;
+}
+
+int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, float* tune_ms) {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch");
+  if (rows) *rows = b->rows;
+  if (blocks) *blocks = b->blocks;
+  if (items) *items = b->nitems;
+  if (tune_ms)
+    for (int q = 0; q < 4; q++) tune_ms[q] = q < static_cast<int>(b->tune_ms.size()) ? b->tune_ms[q] : 0.f;
+  return FDTD_OK;
+}
+
+int fdtd_batch_error_flags(fdtd_batch* b, int* flags) {
+  if (!b || !flags) return fail(FDTD_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(flags, &b->d_ctl->error, sizeof(int), cudaMemcpyDeviceToHost));
   return FDTD_OK;
 }
 

@@ -104,10 +104,10 @@ __device__ __forceinline__ GroupCtx make_ctx(const FusedArgs& a, int ft, int x4,
   g.pml_x = a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
   g.pml_y = a.pml_axis[1] && slab_index(a.slab[1], min(j, a.ny - 2)) >= 0;
   g.src_here = false;
-  if (ft == 0)
-    for (int s = 0; s < a.nsrc; s++)
-      if (a.src[s].j == j && a.src[s].i >= x4 && a.src[s].i < x4 + 4 && a.src[s].k >= kbeg && a.src[s].k < kend)
-        g.src_here = true;
+  for (int s = 0; s < a.nsrc; s++)
+    if ((a.src[s].target < 2) == (ft == 0) && a.src[s].j == j && a.src[s].i >= x4 && a.src[s].i < x4 + 4 &&
+        a.src[s].k >= kbeg && a.src[s].k < kend)
+      g.src_here = true;
   g.uniform_mat = !a.ids && !a.bids;
   g.fsx = ld4(a.prof[ft][0].F + x4);
   g.fsy = a.prof[ft][1].F[min(j, a.ny - 2)];
@@ -197,7 +197,7 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
   if (g.src_here) {
     for (int q = 0; q < a.nsrc; q++) {
       const SourceDev& sr = a.src[q];
-      if (sr.j != j || sr.k != k || sr.i < x4 || sr.i >= x4 + 4) continue;
+      if (sr.target > 1 || sr.j != j || sr.k != k || sr.i < x4 || sr.i >= x4 + 4) continue;
       const int e = sr.i - x4;
       const double v = g.t < sr.nvals ? sr.vals[g.t] : 0.0;
       if (sr.target == 1) {
@@ -329,12 +329,42 @@ __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCt
       a.psi[1][2][0][pi] = B * pz + Cs * el(rzx, e);
     }
   }
+  // sources: B-target adds to the flux; H-target undoes last step's value
+  // and adds this step's after the update (H is stored as eta*H)
+  float4 aX = make_float4(0.f, 0.f, 0.f, 0.f), aY = aX, aZ = aX;
+  if (g.src_here) {
+    for (int q = 0; q < a.nsrc; q++) {
+      const SourceDev& sr = a.src[q];
+      if (sr.target < 2 || sr.j != j || sr.k != k || sr.i < x4 || sr.i >= x4 + 4) continue;
+      const int e = sr.i - x4;
+      const double v = g.t < sr.nvals ? sr.vals[g.t] : 0.0;
+      if (sr.target == 3) {
+        const float dv = static_cast<float>(v * a.src_scale_b);
+        if (sr.comp == 0) set_el(dX, e, el(dX, e) - dv);
+        else if (sr.comp == 1) set_el(dY, e, el(dY, e) - dv);
+        else set_el(dZ, e, el(dZ, e) - dv);
+      } else {
+        const float u = static_cast<float>(a.src_last[q] * a.src_scale_h), ad = static_cast<float>(v * a.src_scale_h);
+        if (sr.comp == 0) {
+          set_el(hx, e, el(hx, e) - u);
+          set_el(aX, e, el(aX, e) + ad);
+        } else if (sr.comp == 1) {
+          set_el(hy, e, el(hy, e) - u);
+          set_el(aY, e, el(aY, e) + ad);
+        } else {
+          set_el(hz, e, el(hz, e) - u);
+          set_el(aZ, e, el(aZ, e) + ad);
+        }
+        a.src_last[q] = v;
+      }
+    }
+  }
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     if (!g.ok[e]) continue;
-    set_el(hx, e, el(hx, e) - el(dX, e));
-    set_el(hy, e, el(hy, e) - el(dY, e));
-    set_el(hz, e, el(hz, e) - el(dZ, e));
+    set_el(hx, e, el(hx, e) - el(dX, e) + el(aX, e));
+    set_el(hy, e, el(hy, e) - el(dY, e) + el(aY, e));
+    set_el(hz, e, el(hz, e) - el(dZ, e) + el(aZ, e));
   }
   st4(a.H[0] + c, hx);
   st4(a.H[1] + c, hy);

@@ -148,6 +148,8 @@ struct FusedArgs {
   int nsrc;
   SourceDev src[kMaxSources];
   float src_scale_d;  // 1/eps0 for D-target sources
+  float src_scale_b;  // eta/mu0 for B-target sources
+  float src_scale_h;  // eta for H-target sources (H is stored as eta*H)
   double* src_last;   // per source: value added to E at the previous step
   int nplanes;
   PlaneDev planes[kMaxPlanes];
@@ -191,5 +193,14 @@ int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int 
 int launch_dft_rebase(Control* ctrl, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
+// control block of a batch's persistent kernel (grid barrier + error flag)
+struct BatchCtl {
+  unsigned count;  // CTAs arrived at the current barrier
+  unsigned gen;    // barrier generation
+  int error;       // bit 0: a barrier wait expired
+  int pad;
+};
+void* batch_kernel_ptr(int mode, int maxp, int rows);
+int launch_batch_advance(Control* const* ctrls, int n, int nsteps, cudaStream_t s);
 
 }  // namespace fdtdb

@@ -1,0 +1,334 @@
+// Batched 2D FP32 grids in one persistent launch.
+//
+// Many independent TE/TM grids of uneven sizes (each an fdtd_grid set up with
+// the ordinary calls) are advanced together by ONE cooperative kernel that
+// runs every requested step: the work list holds (grid, 128 x ROWS tile)
+// items; each CTA takes items round-robin; the E phase of all grids, a grid
+// barrier, the H phase, a barrier, next step. The update per 4-cell group is
+// the fused E/H form of kernels_fused.cu restated for 2D with 128-bit access.
+//
+// The grid barrier spins with a bound: after kBarrierLimit polls a CTA sets
+// the batch error flag and returns, and a CTA that sees the flag set returns
+// too, so a lost CTA cannot hang the GPU. Loads of cells another CTA may have
+// written in the previous phase go through L2 (__ldcg): L1 is not coherent
+// across CTAs.
+#include "fused3d_common.cuh"
+
+namespace fdtdb {
+
+namespace {
+
+using namespace f3d;
+constexpr long long kBarrierLimit = 1LL << 26;
+
+__device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+
+__device__ bool grid_barrier(BatchCtl* ctl, unsigned nblocks) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    volatile unsigned* gen = &ctl->gen;
+    volatile int* err = &ctl->error;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(&ctl->count, 1u) == nblocks - 1) {
+      ctl->count = 0;
+      __threadfence();
+      atomicAdd(&ctl->gen, 1u);
+    } else {
+      long long n = 0;
+      while (*gen == g) {
+        if (*err) {
+          ok = 0;
+          break;
+        }
+        if (++n > kBarrierLimit) {
+          atomicOr(&ctl->error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+// E update of one 4-cell group of a 2D grid
+template <int MODE, int MAXP>
+__device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long long t) {
+  const bool row_ok = j <= a.ny - 2;
+  const int jl = min(j, a.ny - 2);
+  bool ok[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) ok[e] = row_ok && x4 + e >= 1 && x4 + e <= a.nx - 2;
+  const long long c = static_cast<long long>(jl) * a.pitch + x4;
+  const float4 fsx = ld4(a.prof[0][0].F + x4);
+  const float fsy = a.prof[0][1].F[jl];
+  float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
+  if (MODE == kTE) {
+    const float4 hz = ldcg4(a.H[2] + c), hz_ym = ldcg4(a.H[2] + c - a.pitch);
+    float hz_xm0 = __shfl_up_sync(0xffffffffu, hz.w, 1);
+    if (lane == 0) hz_xm0 = __ldcg(a.H[2] + c - 1);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      set_el(rxy, e, el(hz, e) - el(hz_ym, e));
+      set_el(ryx, e, -(el(hz, e) - (e == 0 ? hz_xm0 : el(hz, e - 1))));
+      set_el(dX, e, fsy * el(rxy, e));
+      set_el(dY, e, el(fsx, e) * el(ryx, e));
+    }
+  } else {
+    const float4 hx = ldcg4(a.H[0] + c), hy = ldcg4(a.H[1] + c), hx_ym = ldcg4(a.H[0] + c - a.pitch);
+    float hy_xm0 = __shfl_up_sync(0xffffffffu, hy.w, 1);
+    if (lane == 0) hy_xm0 = __ldcg(a.H[1] + c - 1);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      set_el(rzx, e, el(hy, e) - (e == 0 ? hy_xm0 : el(hy, e - 1)));
+      set_el(rzy, e, -(el(hx, e) - el(hx_ym, e)));
+      set_el(dZ, e, el(fsx, e) * el(rzx, e) + fsy * el(rzy, e));
+    }
+  }
+  if (!row_ok) return;
+  // CPML: y slab rows share the field layout; x slab cells are compact
+  if (a.pml_axis[1]) {
+    const int sj = slab_index(a.slab[1], j);
+    if (sj >= 0) {
+      const long long pi = static_cast<long long>(sj) * a.pitch + x4;
+      const float B = a.prof[0][1].B[j], Cs = a.prof[0][1].C[j], G = a.prof[0][1].G[j];
+      const int I = MODE == kTE ? 0 : 2;
+      float4 ps = ldcg4(a.psi[0][I][1] + pi);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        if (!ok[e]) continue;
+        const float raw = MODE == kTE ? el(rxy, e) : el(rzy, e);
+        if (MODE == kTE) set_el(dX, e, el(dX, e) + el(ps, e) * G);
+        else set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
+        set_el(ps, e, B * el(ps, e) + Cs * raw);
+      }
+      st4(a.psi[0][I][1] + pi, ps);
+    }
+  }
+  if (a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3)) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int i = x4 + e;
+      if (!ok[e]) continue;
+      const int sx = slab_index(a.slab[0], i);
+      if (sx < 0) continue;
+      const long long pi = static_cast<long long>(j) * a.slab[0].W + sx;
+      const float B = a.prof[0][0].B[i], Cs = a.prof[0][0].C[i], G = a.prof[0][0].G[i];
+      const int I = MODE == kTE ? 1 : 2;
+      const float ps = __ldcg(a.psi[0][I][0] + pi);
+      const float raw = MODE == kTE ? el(ryx, e) : el(rzx, e);
+      if (MODE == kTE) set_el(dY, e, el(dY, e) + ps * G);
+      else set_el(dZ, e, el(dZ, e) + ps * G);
+      a.psi[0][I][0][pi] = B * ps + Cs * raw;
+    }
+  }
+  // sources and material update (shared with the 3D sweeps)
+  float4 uX = make_float4(0.f, 0.f, 0.f, 0.f), uY = uX, uZ = uX, aX = uX, aY = uX, aZ = uX;
+  for (int q = 0; q < a.nsrc; q++) {
+    const SourceDev& sr = a.src[q];
+    if (sr.target > 1 || sr.j != j || sr.i < x4 || sr.i >= x4 + 4) continue;
+    const int e = sr.i - x4;
+    const double v = t < sr.nvals ? sr.vals[t] : 0.0;
+    if (sr.target == 1) {
+      const float dv = static_cast<float>(v * a.src_scale_d);
+      if (sr.comp == 0) set_el(dX, e, el(dX, e) + dv);
+      else if (sr.comp == 1) set_el(dY, e, el(dY, e) + dv);
+      else set_el(dZ, e, el(dZ, e) + dv);
+    } else {
+      const float u = static_cast<float>(a.src_last[q]), ad = static_cast<float>(v);
+      if (sr.comp == 0) { set_el(uX, e, el(uX, e) + u); set_el(aX, e, el(aX, e) + ad); }
+      else if (sr.comp == 1) { set_el(uY, e, el(uY, e) + u); set_el(aY, e, el(aY, e) + ad); }
+      else { set_el(uZ, e, el(uZ, e) + u); set_el(aZ, e, el(aZ, e) + ad); }
+      a.src_last[q] = v;
+    }
+  }
+  const bool uniform = !a.ids;
+  const MatF32& m0 = a.mats[0];
+  float4 ie;
+  int mids[4] = {0, 0, 0, 0};
+  bool disp = false;
+  const unsigned ids4 = a.ids ? __ldcg(reinterpret_cast<const unsigned*>(a.ids + c)) : 0u;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int mid = uniform ? 0 : static_cast<int>((ids4 >> (8 * e)) & 0xff);
+    mids[e] = mid;
+    set_el(ie, e, a.mats[mid].inv_eps);
+    if (MAXP != 0 && a.mats[mid].npoles != 0) disp = true;
+  }
+  if (MODE == kTE) {
+    st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(ldcg4(a.E[0] + c), uX), dX, ie, ok, disp, uniform, m0, mids, aX));
+    st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(ldcg4(a.E[1] + c), uY), dY, ie, ok, disp, uniform, m0, mids, aY));
+  } else {
+    st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(ldcg4(a.E[2] + c), uZ), dZ, ie, ok, disp, uniform, m0, mids, aZ));
+  }
+}
+
+// H update of one 4-cell group of a 2D grid
+template <int MODE>
+__device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long long t) {
+  const bool row_ok = j <= a.ny - 2;
+  const int jl = min(j, a.ny - 2);
+  bool ok[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) ok[e] = row_ok && x4 + e >= 1 && x4 + e <= a.nx - 2;
+  const long long c = static_cast<long long>(jl) * a.pitch + x4;
+  const float4 fsx = ld4(a.prof[1][0].F + x4);
+  const float fsy = a.prof[1][1].F[jl];
+  float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
+  if (MODE == kTE) {
+    const float4 ex = ldcg4(a.E[0] + c), ey = ldcg4(a.E[1] + c), ex_yp = ldcg4(a.E[0] + c + a.pitch);
+    float ey_xp3 = __shfl_down_sync(0xffffffffu, ey.x, 1);
+    if (lane == 31) ey_xp3 = __ldcg(a.E[1] + c + 4);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      set_el(rzx, e, (e == 3 ? ey_xp3 : el(ey, e + 1)) - el(ey, e));
+      set_el(rzy, e, -(el(ex_yp, e) - el(ex, e)));
+      set_el(dZ, e, el(fsx, e) * el(rzx, e) + fsy * el(rzy, e));
+    }
+  } else {
+    const float4 ez = ldcg4(a.E[2] + c), ez_yp = ldcg4(a.E[2] + c + a.pitch);
+    float ez_xp3 = __shfl_down_sync(0xffffffffu, ez.x, 1);
+    if (lane == 31) ez_xp3 = __ldcg(a.E[2] + c + 4);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      set_el(rxy, e, el(ez_yp, e) - el(ez, e));
+      set_el(ryx, e, -((e == 3 ? ez_xp3 : el(ez, e + 1)) - el(ez, e)));
+      set_el(dX, e, fsy * el(rxy, e));
+      set_el(dY, e, el(fsx, e) * el(ryx, e));
+    }
+  }
+  if (!row_ok) return;
+  if (a.pml_axis[1]) {
+    const int sj = slab_index(a.slab[1], j);
+    if (sj >= 0) {
+      const long long pi = static_cast<long long>(sj) * a.pitch + x4;
+      const float B = a.prof[1][1].B[j], Cs = a.prof[1][1].C[j], G = a.prof[1][1].G[j];
+      const int I = MODE == kTE ? 2 : 0;
+      float4 ps = ldcg4(a.psi[1][I][1] + pi);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        if (!ok[e]) continue;
+        const float raw = MODE == kTE ? el(rzy, e) : el(rxy, e);
+        if (MODE == kTE) set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
+        else set_el(dX, e, el(dX, e) + el(ps, e) * G);
+        set_el(ps, e, B * el(ps, e) + Cs * raw);
+      }
+      st4(a.psi[1][I][1] + pi, ps);
+    }
+  }
+  if (a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3)) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int i = x4 + e;
+      if (!ok[e]) continue;
+      const int sx = slab_index(a.slab[0], i);
+      if (sx < 0) continue;
+      const long long pi = static_cast<long long>(j) * a.slab[0].W + sx;
+      const float B = a.prof[1][0].B[i], Cs = a.prof[1][0].C[i], G = a.prof[1][0].G[i];
+      const int I = MODE == kTE ? 2 : 1;
+      const float ps = __ldcg(a.psi[1][I][0] + pi);
+      const float raw = MODE == kTE ? el(rzx, e) : el(ryx, e);
+      if (MODE == kTE) set_el(dZ, e, el(dZ, e) + ps * G);
+      else set_el(dY, e, el(dY, e) + ps * G);
+      a.psi[1][I][0][pi] = B * ps + Cs * raw;
+    }
+  }
+  float4 uX = make_float4(0.f, 0.f, 0.f, 0.f), uY = uX, uZ = uX, aX = uX, aY = uX, aZ = uX;
+  for (int q = 0; q < a.nsrc; q++) {
+    const SourceDev& sr = a.src[q];
+    if (sr.target < 2 || sr.j != j || sr.i < x4 || sr.i >= x4 + 4) continue;
+    const int e = sr.i - x4;
+    const double v = t < sr.nvals ? sr.vals[t] : 0.0;
+    if (sr.target == 3) {
+      const float dv = static_cast<float>(v * a.src_scale_b);
+      if (sr.comp == 0) set_el(dX, e, el(dX, e) - dv);
+      else if (sr.comp == 1) set_el(dY, e, el(dY, e) - dv);
+      else set_el(dZ, e, el(dZ, e) - dv);
+    } else {
+      const float u = static_cast<float>(a.src_last[q] * a.src_scale_h), ad = static_cast<float>(v * a.src_scale_h);
+      if (sr.comp == 0) { set_el(uX, e, el(uX, e) + u); set_el(aX, e, el(aX, e) + ad); }
+      else if (sr.comp == 1) { set_el(uY, e, el(uY, e) + u); set_el(aY, e, el(aY, e) + ad); }
+      else { set_el(uZ, e, el(uZ, e) + u); set_el(aZ, e, el(aZ, e) + ad); }
+      a.src_last[q] = v;
+    }
+  }
+  auto upd = [&](int I, float4 d, float4 u, float4 ad) {
+    float4 h = ldcg4(a.H[I] + c);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (ok[e]) set_el(h, e, el(h, e) - el(u, e) - el(d, e) + el(ad, e));
+    st4(a.H[I] + c, h);
+  };
+  if (MODE == kTE) {
+    upd(2, dZ, uZ, aZ);
+  } else {
+    upd(0, dX, uX, aX);
+    upd(1, dY, uY, aY);
+  }
+}
+
+}  // namespace
+
+// item = (grid index << 24) | tile; tile = ty * (pitch/128) + tx
+template <int MODE, int MAXP, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS) batch_kernel(const FusedArgs* __restrict__ grids,
+                                                          const unsigned* __restrict__ items, int nitems,
+                                                          BatchCtl* ctl, int nsteps) {
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  // every grid of a batch has taken the same number of steps; the counters
+  // are advanced by a separate kernel after this one
+  const long long t0 = grids[0].ctrl->t;
+  for (int s = 0; s < nsteps; s++) {
+    const long long t = t0 + s;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+      const unsigned w = items[it];
+      const FusedArgs& a = grids[w >> 24];
+      const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
+      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
+      e_group_2d<MODE, MAXP>(a, x4, j, lane, t);
+    }
+    if (!grid_barrier(ctl, gridDim.x)) return;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+      const unsigned w = items[it];
+      const FusedArgs& a = grids[w >> 24];
+      const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
+      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
+      h_group_2d<MODE>(a, x4, j, lane, t);
+    }
+    if (!grid_barrier(ctl, gridDim.x)) return;
+  }
+}
+
+template <int MODE, int MAXP, int ROWS>
+static void* batch_fn() {
+  return reinterpret_cast<void*>(batch_kernel<MODE, MAXP, ROWS>);
+}
+
+void* batch_kernel_ptr(int mode, int maxp, int rows) {
+#define FDTD_BATCH_ROWS(M, P)                 \
+  switch (rows) {                             \
+    case 1: return batch_fn<M, P, 1>();       \
+    case 2: return batch_fn<M, P, 2>();       \
+    case 4: return batch_fn<M, P, 4>();       \
+    default: return batch_fn<M, P, 8>();      \
+  }
+#define FDTD_BATCH_POLES(M)                   \
+  switch (maxp) {                             \
+    case 0: FDTD_BATCH_ROWS(M, 0)             \
+    case -1: FDTD_BATCH_ROWS(M, -1)           \
+    case 1: FDTD_BATCH_ROWS(M, 1)             \
+    default: FDTD_BATCH_ROWS(M, 2)            \
+  }
+  if (mode == kTE) {
+    FDTD_BATCH_POLES(kTE)
+  }
+  FDTD_BATCH_POLES(kTM)
+#undef FDTD_BATCH_POLES
+#undef FDTD_BATCH_ROWS
+}
+
+}  // namespace fdtdb

@@ -129,6 +129,19 @@ int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaS
 
 __global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
 
+__global__ void batch_advance_kernel(Control* const* ctrls, int n, int nsteps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    ctrls[i]->t += nsteps;
+    ctrls[i]->dft_base = ctrls[i]->t;
+  }
+}
+
+int launch_batch_advance(Control* const* ctrls, int n, int nsteps, cudaStream_t s) {
+  batch_advance_kernel<<<(n + 127) / 128, 128, 0, s>>>(ctrls, n, nsteps);
+  return 1;
+}
+
 int launch_step_advance(Control* ctrl, cudaStream_t s) {
   step_advance_kernel<<<1, 1, 0, s>>>(ctrl);
   return 1;

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const __grid_constant__ Fu
     float undo0 = 0.f, undo1 = 0.f, undo2 = 0.f, add0 = 0.f, add1 = 0.f, add2 = 0.f;
     for (int s = 0; s < a.nsrc; s++) {
       const SourceDev& sr = a.src[s];
-      if (sr.cell != c) continue;
+      if (sr.target > 1 || sr.cell != c) continue;
       const double v = t < sr.nvals ? sr.vals[t] : 0.0;
       if (sr.target == 1) {
         const float dv = static_cast<float>(v * a.src_scale_d);
@@ -253,9 +253,28 @@ __global__ void __launch_bounds__(256) fused_h_kernel(const __grid_constant__ Fu
         }
       }
     }
-    if (hasH(MODE, 0)) a.H[0][c] -= dx_;
-    if (hasH(MODE, 1)) a.H[1][c] -= dy_;
-    if (hasH(MODE, 2)) a.H[2][c] -= dz_;
+    float add0 = 0.f, add1 = 0.f, add2 = 0.f, undo0 = 0.f, undo1 = 0.f, undo2 = 0.f;
+    for (int s = 0; s < a.nsrc; s++) {
+      const SourceDev& sr = a.src[s];
+      if (sr.target < 2 || sr.cell != c) continue;
+      const long long t = a.ctrl->t;
+      const double v = t < sr.nvals ? sr.vals[t] : 0.0;
+      if (sr.target == 3) {
+        const float dv = static_cast<float>(v * a.src_scale_b);
+        if (sr.comp == 0) dx_ -= dv;
+        else if (sr.comp == 1) dy_ -= dv;
+        else dz_ -= dv;
+      } else {
+        const float u = static_cast<float>(a.src_last[s] * a.src_scale_h), ad = static_cast<float>(v * a.src_scale_h);
+        if (sr.comp == 0) { undo0 += u; add0 += ad; }
+        else if (sr.comp == 1) { undo1 += u; add1 += ad; }
+        else { undo2 += u; add2 += ad; }
+        a.src_last[s] = v;
+      }
+    }
+    if (hasH(MODE, 0)) a.H[0][c] = a.H[0][c] - undo0 - dx_ + add0;
+    if (hasH(MODE, 1)) a.H[1][c] = a.H[1][c] - undo1 - dy_ + add1;
+    if (hasH(MODE, 2)) a.H[2][c] = a.H[2][c] - undo2 - dz_ + add2;
   }
 }
 

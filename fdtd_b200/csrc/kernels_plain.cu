@@ -230,6 +230,12 @@ __global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ Pl
       a.B.f[I][c] += -dt * tfsf_term<MODE>(p, ax, row, 1, I, idx, a.prof, a.dx);
     }
   }
+  // SoftSource on B
+  for (int s = 0; s < a.nsrc; s++) {
+    const SourceDev& sr = a.src[s];
+    if (sr.target != 3 || sr.cell != c) continue;
+    a.B.f[sr.comp][c] += t < sr.nvals ? sr.vals[t] : 0.0;
+  }
   // UpdatePML<Mode, Magnetic, J>
 #pragma unroll
   for (int J = 0; J < 3; J++) {
@@ -263,6 +269,12 @@ __global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ Pl
   for (int I = 2; I >= 0; I--) {
     if (!hasH(MODE, I)) continue;
     a.H.f[I][c] = a.B.f[I][c] / den;
+  }
+  // SoftSource on H
+  for (int s = 0; s < a.nsrc; s++) {
+    const SourceDev& sr = a.src[s];
+    if (sr.target != 2 || sr.cell != c) continue;
+    a.H.f[sr.comp][c] += t < sr.nvals ? sr.vals[t] : 0.0;
   }
 }
 

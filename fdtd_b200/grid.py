@@ -34,7 +34,8 @@ EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_ma
            "fdtd_set_material_blocks", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
-           "fdtd_last_error_string"]
+           "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_info",
+           "fdtd_batch_error_flags", "fdtd_last_error_string"]
 
 
 class FdtdError(RuntimeError):
@@ -91,6 +92,12 @@ def load_library(path: str = LIB_PATH):
         "fdtd_get_step": [vp, llp],
         "fdtd_launch_count": [vp, llp],
         "fdtd_memory_bytes": [vp, llp],
+        "fdtd_batch_create": [i, ctypes.POINTER(vp), ctypes.POINTER(vp)],
+        "fdtd_batch_destroy": [vp],
+        "fdtd_batch_tune": [vp, i],
+        "fdtd_batch_step": [vp, i, vp],
+        "fdtd_batch_info": [vp, ip, ip, ip, ctypes.POINTER(ctypes.c_float)],
+        "fdtd_batch_error_flags": [vp, ip],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -162,7 +169,7 @@ class Grid:
 
     def add_source(self, comp: int, pos, values, target: str = "E") -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)
-        _check(load_library().fdtd_add_source(self.h, comp, 0 if target == "E" else 1, *pos, _dp(v), len(v)))
+        _check(load_library().fdtd_add_source(self.h, comp, P.SOURCE_TARGETS[target], *pos, _dp(v), len(v)))
 
     def add_tfsf_plane(self, axis, orient, lo, hi, origin, k, pol_e, pol_h, aux_ncells, aux_values) -> None:
         av = np.ascontiguousarray(aux_values, dtype=np.float64)
@@ -278,6 +285,50 @@ class Grid:
     def close(self) -> None:
         if getattr(self, "h", None):
             load_library().fdtd_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent FP32 2D grids advanced together by one persistent kernel
+    launch per step() call (fdtd_batch_*)."""
+
+    def __init__(self, grids):
+        L = load_library()
+        self.grids = list(grids)
+        arr = (ctypes.c_void_p * len(self.grids))(*[g.h.value for g in self.grids])
+        h = ctypes.c_void_p()
+        _check(L.fdtd_batch_create(len(self.grids), arr, ctypes.byref(h)))
+        self.h = h
+
+    def tune(self, steps: int = 4) -> None:
+        _check(load_library().fdtd_batch_tune(self.h, steps))
+
+    def step(self, n: int, stream: Optional[int] = None) -> None:
+        _check(load_library().fdtd_batch_step(self.h, int(n), ctypes.c_void_p(stream) if stream else None))
+        for g in self.grids:
+            g._stepped_in_batch = True
+
+    def info(self) -> dict:
+        rows, blocks, items = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 4)()
+        _check(load_library().fdtd_batch_info(self.h, ctypes.byref(rows), ctypes.byref(blocks), ctypes.byref(items), ms))
+        return {"rows": rows.value, "blocks": blocks.value, "items": items.value,
+                "tune_ms_per_step": {r: float(m) for r, m in zip((1, 2, 4, 8), ms)}}
+
+    def error_flags(self) -> int:
+        v = ctypes.c_int()
+        _check(load_library().fdtd_batch_error_flags(self.h, ctypes.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            load_library().fdtd_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

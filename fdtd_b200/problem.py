@@ -30,6 +30,7 @@ TEM, TE, TM, THREED = 0, 1, 2, 3
 MODE_NAMES = {"TEM": TEM, "TE": TE, "TM": TM, "ThreeD": THREED, "3D": THREED}
 
 VACUUM, CONSTANT, DRUDE, LORENTZ = 0, 1, 2, 3
+SOURCE_TARGETS = {"E": 0, "D": 1, "H": 2, "B": 3}
 MAX_POLES = 4
 
 
@@ -80,8 +81,9 @@ class Material:
 @dataclass
 class Source:
     """Soft source (include/Source.hpp:183-261): values[t] added at step t to
-    component ``comp`` (0..2) of E (target 'E', after the constitutive update)
-    or of D (target 'D', before the CPML pass)."""
+    component ``comp`` (0..2) of E (target 'E', after the constitutive
+    update), D ('D', before the CPML pass), H ('H', after the magnetic
+    constitutive update) or B ('B', before the magnetic CPML pass)."""
 
     comp: int
     pos: Tuple[int, int, int]
@@ -275,6 +277,43 @@ def config2(n: int = 384, steps: int = 1000, npml: int = 12, radius: Optional[in
                 p.dfts.append(DFTRegion(3 + b, tuple(plo), tuple(phi), freqs))
     p.steps = steps
     return p
+
+
+def config3(nproblems: int = 64, steps: int = 3000, seed: int = 0, nmin: int = 128, nmax: int = 1024,
+            npml: int = 10, nrect: int = 10) -> List[Problem]:
+    """Batched 2D TE: `nproblems` grids with Nx, Ny uniform in [nmin, nmax]
+    from `seed`; each with `nrect` axis-aligned dielectric rectangles (eps_r
+    uniform in [1, 12], sides uniform in [8, 64]) placed inside the CPML-free
+    interior, a 10-cell CPML, and a Gaussian soft Hz source at a random
+    interior cell."""
+    dx = 1e-6
+    dt = courant_dt(dx, 0.99 / math.sqrt(2.0))
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(nproblems):
+        nx, ny = (int(v) for v in rng.integers(nmin, nmax + 1, size=2))
+        p = Problem(TE, (nx, ny, 1), dx, dt, name=f"te{nx}x{ny}_rects")
+        for a in (0, 1):
+            for s in (0, 1):
+                p.pml[(a, s)] = npml
+        lo = npml + 2
+        ids = np.zeros((1, ny, nx), np.uint8)
+        mats = [Material.vacuum()]
+        for r in range(nrect):
+            w, h = (int(v) for v in rng.integers(8, 65, size=2))
+            w = min(w, nx - 2 * lo - 1)
+            h = min(h, ny - 2 * lo - 1)
+            x0 = int(rng.integers(lo, nx - lo - w))
+            y0 = int(rng.integers(lo, ny - lo - h))
+            mats.append(Material.constant(float(rng.uniform(1.0, 12.0))))
+            ids[0, y0:y0 + h, x0:x0 + w] = len(mats) - 1
+        p.materials = mats
+        p.ids = ids
+        si, sj = int(rng.integers(lo, nx - lo)), int(rng.integers(lo, ny - lo))
+        p.sources.append(Source(2, (si, sj, 0), gaussian_pulse(steps), "H"))
+        p.steps = steps
+        out.append(p)
+    return out
 
 
 def config5(n: int = 768, steps: int = 500, npml: int = 16, block: int = 32, seed: int = 0,

@@ -111,9 +111,11 @@ int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids);
 /* Per-block ids: cell (i,j,k) takes ids[((k>>s)*nby + (j>>s))*nbx + (i>>s)]. */
 int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz);
 
-/* Soft source: vals[t] is added at step t (counted from grid creation) to
- * component comp (0..2) of E after the constitutive update (target 0, as
- * SoftSource<.., GetField<Ez>>), or of D before the CPML pass (target 1). */
+/* Soft source (SoftSource<Signal, Cell, GetField<F>>::apply): vals[t] is
+ * added at step t (counted from grid creation) to component comp (0..2) of
+ * E after the constitutive update (target 0), D before the CPML pass (1),
+ * H after the magnetic constitutive update (2) or B before the magnetic CPML
+ * pass (3). */
 int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals);
 
 /* One TFSF plane (TFSFPlane, Source.hpp:472-634): corrections on the cells
@@ -172,6 +174,25 @@ int fdtd_get_step(fdtd_grid* g, long long* step);
 int fdtd_launch_count(fdtd_grid* g, long long* count);
 /* Device bytes held by the grid. */
 int fdtd_memory_bytes(fdtd_grid* g, long long* bytes);
+
+/* ------------------------------------------------------------ batches
+ * Many independent FP32 2D grids (TE or TM, same mode and device, no TFSF or
+ * DFT, equal step counts), each set up with the calls above, advanced
+ * together by one persistent kernel launch per fdtd_batch_step (replayed
+ * from a CUDA graph). The grids stay usable on their own (download etc.). */
+typedef struct fdtd_batch fdtd_batch;
+int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out);
+int fdtd_batch_destroy(fdtd_batch* b);
+/* Autotuner: times each tile height (1, 2, 4, 8 rows of 128 cells) for
+ * `steps` steps on a snapshot of the grids' state, restores the state and
+ * keeps the fastest. */
+int fdtd_batch_tune(fdtd_batch* b, int steps);
+int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream);
+/* Tile height in use, CTAs of the persistent kernel, work items, and the
+ * tuner's ms per step for tile heights 1, 2, 4, 8 (0 if not tuned). */
+int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, float* tune_ms);
+/* Bit 0: a bounded grid-barrier wait expired and the kernel gave up. */
+int fdtd_batch_error_flags(fdtd_batch* b, int* flags);
 
 /* Last error of the calling thread ("" if none). */
 const char* fdtd_last_error_string(void);

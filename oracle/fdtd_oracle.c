@@ -15,8 +15,9 @@
  *   E half: YeeUpdate on every E flux, TFSF updateD, D-target sources,
  *           UpdatePML<Electric, X|Y|Z>, material update, E-target sources,
  *           DFT of E.
- *   H half: YeeUpdate on every B flux, TFSF updateB,
- *           UpdatePML<Magnetic, X|Y|Z>, material update, DFT of H.
+ *   H half: YeeUpdate on every B flux, TFSF updateB, B-target sources,
+ *           UpdatePML<Magnetic, X|Y|Z>, material update, H-target sources,
+ *           DFT of H.
  * Only interior cells (1..n-2 along each active axis) are updated; the outer
  * ring keeps its initial zeros, as in tests/testTM.cpp:33-40,103. */
 #include "fdtd_oracle.h"
@@ -229,7 +230,7 @@ int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids) {
 }
 
 int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {
-  if (comp < 0 || comp > 2 || target < 0 || target > 1) return -1;
+  if (comp < 0 || comp > 2 || target < 0 || target > 3) return -1;
   if (i < 0 || i >= g->n[0] || j < 0 || j >= g->n[1] || k < 0 || k >= g->n[2]) return -1;
   g->srcs = (src_t*)realloc(g->srcs, (g->nsrc + 1) * sizeof(src_t));
   src_t* s = &g->srcs[g->nsrc++];
@@ -560,6 +561,12 @@ static void step_one(oracle_grid* g) {
         }
       }
   tfsf_apply(g, 1);
+  for (int s = 0; s < g->nsrc; s++) {
+    src_t* sr = &g->srcs[s];
+    if (sr->target != 3 || !g->hasH[sr->comp]) continue;
+    size_t c = sr->k * sz + sr->j * sy + sr->i;
+    g->B[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
+  }
   for (int J = 0; J < 3; J++) {
     if (!pmlax[J]) continue;
     for (int k = k0; k <= k1; k++)
@@ -587,6 +594,12 @@ static void step_one(oracle_grid* g) {
           g->H[I][c] = g->B[I][c] / (m->mu_r * K_MU0);
         }
       }
+  for (int s = 0; s < g->nsrc; s++) {
+    src_t* sr = &g->srcs[s];
+    if (sr->target != 2 || !g->hasH[sr->comp]) continue;
+    size_t c = sr->k * sz + sr->j * sy + sr->i;
+    g->H[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
+  }
   dft_apply(g, 1, (double)g->t + 1.5);
   g->t++;
 }

@@ -39,7 +39,8 @@ int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells);
 int oracle_set_materials(oracle_grid* g, const oracle_material* m, int n);
 int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids);
 /* comp 0..2 = x,y,z; target 0 = E (after the constitutive update),
- * 1 = D (before it). vals[t] is added at step t. */
+ * 1 = D (before the CPML pass), 2 = H (after the magnetic constitutive
+ * update), 3 = B (before the magnetic CPML pass). vals[t] is added at step t. */
 int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k,
                       const double* vals, int nvals);
 /* One TFSF plane (include/Source.hpp:472-634) with its own Aux1D grid.

@@ -17,6 +17,8 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
+SOURCE_TARGETS = {"E": 0, "D": 1, "H": 2, "B": 3}
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 RUNNER_PATH = os.path.join(HERE, "_ref", "ref_runner")
@@ -120,7 +122,7 @@ class OracleGrid:
         self._keep = []
         for s in p.sources:
             v = np.ascontiguousarray(s.values, dtype=np.float64)
-            assert L.oracle_add_source(self.h, s.comp, 0 if s.target == "E" else 1, *s.pos, _dp(v), len(v)) == 0
+            assert L.oracle_add_source(self.h, s.comp, SOURCE_TARGETS[s.target], *s.pos, _dp(v), len(v)) == 0
         if p.tfsf is not None:
             t = p.tfsf
             av = np.ascontiguousarray(t.aux_values, dtype=np.float64)
@@ -221,7 +223,7 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
         for q, s in enumerate(p.sources):
             sp = os.path.join(td, f"src{q}.bin")
             np.ascontiguousarray(s.values, dtype=np.float64).tofile(sp)
-            lines.append(f"{s.comp} {0 if s.target == 'E' else 1} {s.pos[0]} {s.pos[1]} {s.pos[2]} {sp}")
+            lines.append(f"{s.comp} {SOURCE_TARGETS[s.target]} {s.pos[0]} {s.pos[1]} {s.pos[2]} {sp}")
         if p.tfsf is not None:
             t = p.tfsf
             ap = os.path.join(td, "aux.bin")

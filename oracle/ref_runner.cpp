@@ -25,7 +25,8 @@
 //   nmat M  then M lines: kind K delta freq gamma mu_r
 //        kind 0 vacuum, 1 constant, 2 drude, 3 lorentz
 //   matids <path|none>            uint8 per cell, index (k*ny+j)*nx+i
-//   nsrc S then S lines: comp target i j k path  (comp 0..2, target 0=E 1=D,
+//   nsrc S then S lines: comp target i j k path  (comp 0..2, target 0=E 1=D
+//        2=H 3=B,
 //        path: float64 per step, value added at step t)
 //   ntfsf T (T planes) then: aux_ncells aux_path origin_x origin_y origin_z
 //        kx ky kz set_pol pe_x pe_y pe_z ph_x ph_y ph_z, and T lines:
@@ -318,16 +319,24 @@ static int run(Scenario& s) {
     }
   }
 
-  std::vector<std::function<void(double)>> appliers, dappliers;
+  std::vector<std::function<void(double)>> appliers, dappliers, happliers, bappliers;
   for (auto& sr : s.srcs) {
     C& c = at(sr.i, sr.j, sr.k);
     StepSignal sig{&sr.vals};
-    auto& lst = sr.target == 0 ? appliers : dappliers;
+    auto& lst = sr.target == 0 ? appliers : sr.target == 1 ? dappliers : sr.target == 2 ? happliers : bappliers;
     auto add = [&](auto src) { lst.push_back([src](double t) mutable { src.apply(t); }); };
     if (sr.target == 0) {
       if (sr.comp == 0) { if constexpr (has_field<Mode, Ex>()) add(make_soft_source<Ex>(sig, c)); }
       if (sr.comp == 1) { if constexpr (has_field<Mode, Ey>()) add(make_soft_source<Ey>(sig, c)); }
       if (sr.comp == 2) { if constexpr (has_field<Mode, Ez>()) add(make_soft_source<Ez>(sig, c)); }
+    } else if (sr.target == 2) {
+      if (sr.comp == 0) { if constexpr (has_field<Mode, Hx>()) add(make_soft_source<Hx>(sig, c)); }
+      if (sr.comp == 1) { if constexpr (has_field<Mode, Hy>()) add(make_soft_source<Hy>(sig, c)); }
+      if (sr.comp == 2) { if constexpr (has_field<Mode, Hz>()) add(make_soft_source<Hz>(sig, c)); }
+    } else if (sr.target == 3) {
+      if (sr.comp == 0) { if constexpr (has_field<Mode, Hx>()) add(make_soft_source<Bx>(sig, c)); }
+      if (sr.comp == 1) { if constexpr (has_field<Mode, Hy>()) add(make_soft_source<By>(sig, c)); }
+      if (sr.comp == 2) { if constexpr (has_field<Mode, Hz>()) add(make_soft_source<Bz>(sig, c)); }
     } else {
       if (sr.comp == 0) { if constexpr (has_field<Mode, Ex>()) add(make_soft_source<Dx>(sig, c)); }
       if (sr.comp == 1) { if constexpr (has_field<Mode, Ey>()) add(make_soft_source<Dy>(sig, c)); }
@@ -352,10 +361,12 @@ static int run(Scenario& s) {
     for (C* c : interior) yee<Mode, By>(*c, dt, dx);
     for (C* c : interior) yee<Mode, Bz>(*c, dt, dx);
     for (auto& pl : planes) pl->updateB(dt, dx);
+    for (auto& ap : bappliers) ap(static_cast<double>(t));
     if (pmlax[0]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::X>(dt, dx)(*c);
     if (pmlax[1]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::Y>(dt, dx)(*c);
     if constexpr (Mode::dim == 3) { if (pmlax[2]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::Z>(dt, dx)(*c); }
     for (C* c : interior) hupd[matid(*c)](*c);
+    for (auto& ap : happliers) ap(static_cast<double>(t));
   }
 
   FILE* f = fopen(s.out.c_str(), "wb");

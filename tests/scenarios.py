@@ -144,7 +144,33 @@ def td_lorentz_two_pole_blocks() -> Problem:
     return p
 
 
+def te_h_sources() -> Problem:
+    """TE with soft sources on Hz after the magnetic update (H target, as
+    make_soft_source<Hz>) and on Bz before the magnetic CPML pass (B target)."""
+    p = Problem(TE, (44, 38, 1), DX, DT2, name="te_h_sources")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    p.sources.append(Source(2, (21, 19, 0), gaussian_pulse(70, 20, 6), "H"))
+    p.sources.append(Source(2, (12, 25, 0), 1e-6 * gaussian_pulse(70, 25, 6), "B"))
+    p.dfts.append(DFTRegion(5, (2, 19, 0), (41, 19, 0), [0.03]))
+    p.steps = 70
+    return p
+
+
+def td_h_sources() -> Problem:
+    nx, ny, nz = 16, 14, 15
+    p = Problem(THREED, (nx, ny, nz), DX, DT3, name="td_h_sources")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 3
+    p.sources.append(Source(0, (8, 7, 7), gaussian_pulse(40, 15, 5), "H"))
+    p.sources.append(Source(1, (6, 7, 8), 1e-6 * gaussian_pulse(40, 12, 5), "B"))
+    p.steps = 40
+    return p
+
+
 # scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
-                       te_tfsf_oblique, td_tfsf_box]
+                       te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]

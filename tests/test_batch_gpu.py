@@ -1,0 +1,89 @@
+"""Batched 2D grids (fdtd_batch_*): one persistent launch advances many
+independent grids of uneven sizes; each must match the oracle as if stepped
+alone, tuning must leave the state untouched, and the bounded grid barrier
+must never report an expiry in a normal run."""
+import numpy as np
+import pytest
+
+from fdtd_b200 import problem as P
+from helpers import mode_fields, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def small_te_batch(steps=60):
+    return P.config3(nproblems=5, steps=steps, seed=3, nmin=40, nmax=150, npml=6, nrect=4)
+
+
+def small_tm_batch(steps=50):
+    rng = np.random.default_rng(7)
+    out = []
+    for q in range(4):
+        nx, ny = (int(v) for v in rng.integers(36, 140, size=2))
+        dt = P.courant_dt(1e-6, 0.99 / np.sqrt(2.0))
+        p = P.Problem(P.TM, (nx, ny, 1), 1e-6, dt, name=f"tm{q}")
+        for a in (0, 1):
+            for s in (0, 1):
+                p.pml[(a, s)] = 5
+        p.materials = [P.Material.vacuum(), P.Material.drude(1.0, 0.3 / dt, 0.01 / dt),
+                       P.Material.lorentz(2.0, [(1.2, 0.1 / dt, 0.005 / dt), (0.5, 0.2 / dt, 0.01 / dt)])]
+        ids = np.zeros((1, ny, nx), np.uint8)
+        ids[0, 10:20, 12:22] = 1
+        ids[0, ny - 22:ny - 12, nx - 25:nx - 14] = 2
+        p.ids = ids
+        p.sources.append(P.Source(2, (nx // 2, ny // 2, 0), P.gaussian_pulse(steps, 20, 6), "E"))
+        p.sources.append(P.Source(0, (nx // 3, ny // 3, 0), 1e-3 * P.gaussian_pulse(steps, 25, 6), "H"))
+        p.steps = steps
+        out.append(p)
+    return out
+
+
+@pytest.mark.parametrize("make", [small_te_batch, small_tm_batch], ids=["te", "tm"])
+def test_batch_matches_oracle(fdtd, oracle, make):
+    probs = make()
+    grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+    b = fdtd.Batch(grids)
+    b.step(probs[0].steps - 7)
+    b.step(7)
+    assert b.error_flags() == 0
+    for p, g in zip(probs, grids):
+        o = oracle.run_oracle(p)
+        E, H, _, _ = mode_fields(p.mode)
+        for n in E + H:
+            r = rel_l2(g.get(n), o.get(n))
+            assert r <= 1e-4, (p.name, n, r)
+        assert g.step_count == p.steps
+
+
+def test_batch_tuning_preserves_state_and_results(fdtd):
+    probs = small_te_batch(40)
+    out = []
+    for tune in (False, True):
+        grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+        b = fdtd.Batch(grids)
+        if tune:
+            b.step(10)
+            b.tune(3)
+            info = b.info()
+            assert info["rows"] in (1, 2, 4, 8) and all(v > 0 for v in info["tune_ms_per_step"].values())
+            b.step(30)
+        else:
+            b.step(10)
+            b.step(30)
+        out.append([g.get("Hz") for g in grids])
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
+
+
+def test_batch_rejects_unsupported_grids(fdtd):
+    p = small_te_batch(10)[0]
+    g64 = fdtd.Grid.from_problem(p, "f64")
+    with pytest.raises(fdtd.FdtdError):
+        fdtd.Batch([g64])
+    g3 = fdtd.Grid(P.THREED, (16, 16, 16), 1e-6, 1e-15, "f32")
+    with pytest.raises(fdtd.FdtdError):
+        fdtd.Batch([g3])
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.add_dft(5, (2, 2, 0), (5, 5, 0), [0.1])
+    with pytest.raises(fdtd.FdtdError):
+        fdtd.Batch([g])
