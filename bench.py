@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="drude384", choices=["drude384", "lorentz768", "tm256"])
+    ap.add_argument("--workload", default="drude384", choices=["drude384", "lorentz768", "tm256", "batch64"])
     ap.add_argument("--n", type=int, default=0, help="override the grid size (same physics, scaled): for profiling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -188,12 +188,10 @@ def cpu_rate(problem, steps: int, kind: str):
     restatement ('port') on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    t0 = time.perf_counter()
     if kind == "reference":
-        pyoracle.run_reference(problem, steps)
+        dt = pyoracle.run_reference(problem, steps)["loop_seconds"]
     else:
-        pyoracle.run_oracle(problem, steps)
-    dt = time.perf_counter() - t0
+        dt = pyoracle.run_oracle(problem, steps).loop_seconds
     return problem.interior_cells * steps / dt, dt
 
 
@@ -217,9 +215,11 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    for _ in range(args.warmup and 1):
-        pass
-    cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)))
+    if args.workload == "batch64":
+        from fdtd_b200 import problem as P
+        cb = cpu_batch_baseline(P.config3(64, steps=args.steps + 16), budget_s=20.0)
+    else:
+        cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)))
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Gcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic", "scaling": "weak",
@@ -228,6 +228,129 @@ def run_reference_arm(args):
                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "vs_baseline": None}
     print(json.dumps(line), flush=True)
+
+
+def batch_alg_bytes(problems):
+    """Algorithmic bytes of one step of a batch of 2D TE grids: E (2 words)
+    and H (1 word) read and written once, material ids once, CPML psi over
+    the slab cells."""
+    total = 0.0
+    for p in problems:
+        nx, ny, _ = p.shape
+        cells = (nx - 2) * (ny - 2)
+        slab = 0
+        for a, ext, other in ((0, nx - 2, ny - 2), (1, ny - 2, nx - 2)):
+            w = sum(p.pml.get((a, s), 0) + 1 for s in (0, 1) if p.pml.get((a, s), 0) > 0)
+            slab += min(w, ext) * other
+        total += cells * (4 * 6 + 1) + slab * 4 * 2 * 2
+    return total
+
+
+def cpu_batch_baseline(problems, budget_s: float = 20.0):
+    """The reference's functors on the batch's problems, one process per
+    problem spread over all host cores, on a bounded number of steps."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    kind = "reference" if pyoracle.reference_available() else "port"
+    cores = os.cpu_count() or 1
+    cells = sum(p.interior_cells for p in problems)
+    ctx = mp.get_context("spawn")
+
+    def run(nsteps):
+        # time-loop seconds of every problem, run concurrently on the cores;
+        # the aggregate rate assumes perfect packing of the loops on the cores
+        with cf.ProcessPoolExecutor(max_workers=cores, mp_context=ctx) as ex:
+            return sum(ex.map(_cpu_one, [(p, nsteps, kind) for p in problems]))
+    steps = 2
+    loops = run(steps)
+    steps = max(2, int(steps * budget_s * cores / max(loops, 1e-3)))
+    loops = run(steps)
+    return {"value": cells * steps / (loops / cores) / 1e9, "unit": "Gcell-updates/s", "cores": cores, "kind": kind,
+            "sample": f"all {len(problems)} problems, {steps} steps each, one process per problem over {cores} cores; "
+                      f"rate = cells*steps / (sum of time-loop seconds / cores)"}
+
+
+def _cpu_one(job):
+    p, nsteps, kind = job
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if kind == "reference":
+        return pyoracle.run_reference(p, nsteps)["loop_seconds"]
+    return pyoracle.run_oracle(p, nsteps).loop_seconds
+
+
+def run_batch(args, torch, world, rank, local, stream):
+    from fdtd_b200 import grid as G, problem as P
+    probs = P.config3(64, steps=args.steps + args.warmup + 16)
+    grids = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
+    batch = G.Batch(grids)
+    batch.tune(4)
+    batch.step(args.warmup, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            batch.step(args.steps, stream=stream.cuda_stream)
+            end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    assert batch.error_flags() == 0
+    cells = sum(p.interior_cells for p in probs)
+    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    ab = batch_alg_bytes(probs)
+    peak, peak_kind = peaks()
+    ach = ab * args.steps / (ms / 1e3) / 1e9
+    info = batch.info()
+    batch.close()
+    for g in grids:
+        g.close()
+    # FP64 plain, one grid at a time (no batch kernel for the plain method)
+    n64 = max(3, min(50, args.steps))
+    g64 = [G.Grid.from_problem(p, "f64", device=local) for p in probs]
+    for g in g64:
+        g.step(2, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        for g in g64:
+            g.step(n64, stream=stream.cuda_stream)
+        end.record(stream)
+    torch.cuda.synchronize()
+    ms64 = start.elapsed_time(end)
+    for g in g64:
+        g.close()
+    # end to end: create the 64 grids from host arrays, run, read every Hz back
+    t0 = time.perf_counter()
+    ge = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
+    be = G.Batch(ge)
+    be.step(args.steps)
+    out = [g.get("Hz") for g in ge]
+    t_e2e = time.perf_counter() - t0
+    h2d = sum(p.ids.nbytes + sum(s.values.nbytes for s in p.sources) for p in probs)
+    d2h = sum(o.size * 8 for o in out)
+    be.close()
+    for g in ge:
+        g.close()
+    cpu = cpu_batch_baseline(probs) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    return {
+        "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch64_te_rects", "problems": len(probs), "interior_cells": cells, "seed": 0,
+                   "cpml": 10, "steps_in_config": 3000, "tile_rows": info["rows"], "ctas": info["blocks"],
+                   "tune_ms_per_step": info["tune_ms_per_step"],
+                   "l2": "state ~290 MB > L2; no flush", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "batch_kernel (persistent, all steps)", "achieved": ach, "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "alg_bytes_per_step": ab,
+                     "traffic": None},
+        "fp64_plain": {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "note": "grids stepped one by one"},
+        "e2e": {"value": cells * args.steps * world / t_e2e / 1e9, "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "wall_s": t_e2e},
+        "cpu_baseline": cpu, "gpu_launches": 2, "clocks": clk.summary(),
+    }
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -249,8 +372,16 @@ def main():
 
     from fdtd_b200 import grid as G
 
-    p = make_problem(args.workload, args.steps + args.warmup, args.n)
     stream = torch.cuda.Stream()
+    if args.workload == "batch64":
+        line = run_batch(args, torch, world, rank, local, stream)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    p = make_problem(args.workload, args.steps + args.warmup, args.n)
     g = G.Grid.from_problem(p, "f32", device=local)
     g.step(args.warmup, stream=stream.cuda_stream)
     torch.cuda.synchronize()

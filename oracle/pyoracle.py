@@ -186,8 +186,11 @@ class OracleGrid:
 
 
 def run_oracle(p, steps: Optional[int] = None) -> OracleGrid:
+    import time
     g = OracleGrid(p)
+    t0 = time.perf_counter()
     g.step(p.steps if steps is None else steps)
+    g.loop_seconds = time.perf_counter() - t0
     return g
 
 
@@ -239,6 +242,10 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
         sc = os.path.join(td, "scenario.txt")
         with open(sc, "w") as f:
             f.write("\n".join(lines) + "\n")
-        subprocess.run([RUNNER_PATH, sc], check=True)
+        res = subprocess.run([RUNNER_PATH, sc], check=True, capture_output=True, text=True)
         raw = np.fromfile(op, dtype=np.float64).reshape(len(ALL_NAMES), nz, ny, nx)
-    return {n: raw[q] for q, n in enumerate(ALL_NAMES)}
+    out = {n: raw[q] for q, n in enumerate(ALL_NAMES)}
+    for line in res.stdout.splitlines():
+        if line.startswith("loop_seconds"):
+            out["loop_seconds"] = float(line.split()[1])
+    return out

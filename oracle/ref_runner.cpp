@@ -36,7 +36,8 @@
 //   steps N
 //   out path
 // Output: float64 arrays in order D(3) E(3) B(3) H(3) P(3) J(3) and the CPML
-// integrators psi[ft][I][J] (18), each nx*ny*nz long.
+// integrators psi[ft][I][J] (18), each nx*ny*nz long. The wall time of the
+// time loop alone is printed as "loop_seconds <s>".
 #include <fdtd.h>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +47,7 @@
 #include <vector>
 #include <memory>
 #include <fstream>
+#include <chrono>
 
 namespace fdtd {
 template <typename U, typename F>
@@ -344,6 +346,7 @@ static int run(Scenario& s) {
     }
   }
 
+  const auto clock0 = std::chrono::steady_clock::now();
   for (int t = 0; t < s.steps; t++) {
     // ---- E half step: curl, TFSF, CPML per axis, material, sources
     for (C* c : interior) yee<Mode, Dx>(*c, dt, dx);
@@ -369,6 +372,8 @@ static int run(Scenario& s) {
     for (auto& ap : happliers) ap(static_cast<double>(t));
   }
 
+  const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - clock0).count();
+  printf("loop_seconds %.9f\n", loop_s);
   FILE* f = fopen(s.out.c_str(), "wb");
   if (!f) return 4;
   std::vector<double> buf(cells.size());
