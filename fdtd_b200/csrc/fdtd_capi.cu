@@ -147,6 +147,7 @@ struct fdtd_grid {
   Slab slab[3]{};
   uint8_t* d_ids = nullptr;
   uint16_t* d_bids = nullptr;
+  void* d_eps_map = nullptr;  // plain: double eps; fused: float 1/eps (pitch layout)
   int bshift = 0, nbx = 0, nby = 0, nbz = 0;
   void* d_mats = nullptr;
   int max_poles = 0;
@@ -543,6 +544,7 @@ PlainArgs plain_args(fdtd_grid* g) {
       a.prof[ft][x].G = static_cast<const double*>(g->d_prof[ft][x][3]);
     }
   a.mats = static_cast<const MatF64*>(g->d_mats);
+  a.eps_map = static_cast<const double*>(g->d_eps_map);
   a.dispersive = g->max_poles;
   return a;
 }
@@ -576,6 +578,7 @@ FusedArgs fused_args(fdtd_grid* g) {
       a.prof[ft][x].G = static_cast<const float*>(g->d_prof[ft][x][3]);
     }
   a.mats = static_cast<const MatF32*>(g->d_mats);
+  a.inv_eps_map = static_cast<const float*>(g->d_eps_map);
   a.max_poles = g->max_poles;
   a.all_dispersive = 1;
   for (auto& m : g->mats)
@@ -755,6 +758,28 @@ int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids,
   g->nby = nby;
   g->nbz = nbz;
   return upload_vec(g, reinterpret_cast<void**>(&g->d_bids), ids, nb * sizeof(uint16_t));
+}
+
+int fdtd_set_eps_map(fdtd_grid* g, const double* eps) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  CK(cudaSetDevice(g->d.device));
+  if (!eps) {
+    if (g->d_eps_map) dfree(g, g->d_eps_map);
+    g->d_eps_map = nullptr;
+    return FDTD_OK;
+  }
+  const long long nx = g->n[0], ny = g->n[1], nz = g->n[2], rl = rowlen(g);
+  std::vector<char> buf(field_elems(g) * elem(g), 0);
+  for (long long k = 0; k < nz; k++)
+    for (long long j = 0; j < ny; j++)
+      for (long long i = 0; i < nx; i++) {
+        const double e = eps[(k * ny + j) * nx + i];
+        if (!(e == e) || std::isinf(e)) return fail(FDTD_ERR_INVALID, "non-finite permittivity");
+        const long long q = (k * ny + j) * rl + i;
+        if (g->f32) reinterpret_cast<float*>(buf.data())[q] = e > 0 ? static_cast<float>(1.0 / e) : 0.0f;
+        else reinterpret_cast<double*>(buf.data())[q] = e > 0 ? e : 0.0;
+      }
+  return upload_vec(g, &g->d_eps_map, buf.data(), buf.size());
 }
 
 int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {

@@ -252,6 +252,13 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
       }
     }
   }
+  if (a.inv_eps_map) {
+    // per-cell permittivity of non-dispersive cells
+    const float4 v = ld4(a.inv_eps_map + c);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (el(v, e) > 0.f && a.mats[mids[e]].npoles == 0) set_el(ie, e, el(v, e));
+  }
   st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(exo, uX), dX, ie, g.ok, disp, g.uniform_mat, m0, mids, aX));
   st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(eyo, uY), dY, ie, g.ok, disp, g.uniform_mat, m0, mids, aY));
   st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(ezo, uZ), dZ, ie, g.ok, disp, g.uniform_mat, m0, mids, aZ));

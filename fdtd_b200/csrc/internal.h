@@ -118,6 +118,7 @@ struct PlainArgs {
   const uint16_t* bids;
   int bshift, nbx, nby;
   const MatF64* mats;
+  const double* eps_map;  // per-cell relative permittivity of non-dispersive cells (> 0), or null
   int dispersive;
   int nsrc;
   SourceDev src[kMaxSources];
@@ -143,6 +144,7 @@ struct FusedArgs {
   const uint16_t* bids;
   int bshift, nbx, nby;
   const MatF32* mats;
+  const float* inv_eps_map;  // per-cell 1/eps of non-dispersive cells (> 0), or null
   int max_poles;  // 0 none, -1 Drude only, 1..2 Lorentz
   int all_dispersive;  // every material of the table has poles
   int nsrc;

@@ -159,6 +159,12 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
     set_el(ie, e, a.mats[mid].inv_eps);
     if (MAXP != 0 && a.mats[mid].npoles != 0) disp = true;
   }
+  if (a.inv_eps_map) {
+    const float4 v = ld4(a.inv_eps_map + c);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (el(v, e) > 0.f && a.mats[mids[e]].npoles == 0) set_el(ie, e, el(v, e));
+  }
   if (MODE == kTE) {
     st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(ldcg4(a.E[0] + c), uX), dX, ie, ok, disp, uniform, m0, mids, aX));
     st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(ldcg4(a.E[1] + c), uY), dY, ie, ok, disp, uniform, m0, mids, aY));

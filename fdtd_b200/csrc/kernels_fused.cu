@@ -137,7 +137,11 @@ __global__ void __launch_bounds__(256) fused_e_kernel(const __grid_constant__ Fu
     if (a.ids) mid = a.ids[c];
     else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
     const MatF32& m = a.mats[mid];
-    const float ie = m.inv_eps;
+    float ie = m.inv_eps;
+    if (a.inv_eps_map && m.npoles == 0) {
+      const float v = a.inv_eps_map[c];
+      if (v > 0.f) ie = v;
+    }
     float d[3] = {dx_, dy_, dz_};
 #pragma unroll
     for (int I = 0; I < 3; I++) {

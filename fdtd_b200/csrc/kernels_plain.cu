@@ -149,7 +149,9 @@ __global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ Pl
     if (!hasE(MODE, I)) continue;
     const double D = a.D.f[I][c];
     if (m.kind <= 1) {
-      a.E.f[I][c] = D / m.den_e;
+      // a per-cell permittivity replaces the ConstantUpdate K of the cell
+      const double den = (a.eps_map && a.eps_map[c] > 0.0) ? a.eps_map[c] * kEps0 : m.den_e;
+      a.E.f[I][c] = D / den;
     } else if (m.kind == 2) {
       // drude::DrudeUpdate::implicit_update (DispersiveMaterials.hpp:979-998)
       double P = a.P[0].f[I][c], Jc = a.J[0].f[I][c];

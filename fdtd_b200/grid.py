@@ -31,7 +31,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
-           "fdtd_set_material_blocks", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
+           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_info",
@@ -75,6 +75,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_materials": [vp, ctypes.POINTER(MaterialC), i],
         "fdtd_set_material_ids": [vp, vp],
         "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
+        "fdtd_set_eps_map": [vp, dp],
         "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
         "fdtd_add_tfsf_plane": [vp, i, i, ip, ip, dp, dp, dp, dp, i, dp, i],
         "fdtd_add_dft": [vp, i, ip, ip, dp, i, ip],
@@ -166,6 +167,14 @@ class Grid:
         a = np.ascontiguousarray(bids, dtype=np.uint16)
         nbz, nby, nbx = a.shape
         _check(load_library().fdtd_set_material_blocks(self.h, shift, a.ctypes.data, nbx, nby, nbz))
+
+    def set_eps_map(self, eps: Optional[np.ndarray]) -> None:
+        if eps is None:
+            _check(load_library().fdtd_set_eps_map(self.h, None))
+            return
+        a = np.ascontiguousarray(eps, dtype=np.float64)
+        assert a.size == self.shape[0] * self.shape[1] * self.shape[2]
+        _check(load_library().fdtd_set_eps_map(self.h, _dp(a)))
 
     def add_source(self, comp: int, pos, values, target: str = "E") -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)

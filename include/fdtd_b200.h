@@ -111,6 +111,12 @@ int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids);
 /* Per-block ids: cell (i,j,k) takes ids[((k>>s)*nby + (j>>s))*nbx + (i>>s)]. */
 int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz);
 
+/* Per-cell relative permittivity (nx*ny*nz doubles, x fastest): a cell whose
+ * value is > 0 and whose material is vacuum or constant takes it in place of
+ * the material's eps_inf (a ConstantUpdate<Mode, Electric>(K) per cell);
+ * values <= 0 keep the material. NULL removes the map. */
+int fdtd_set_eps_map(fdtd_grid* g, const double* eps);
+
 /* Soft source (SoftSource<Signal, Cell, GetField<F>>::apply): vals[t] is
  * added at step t (counted from grid creation) to component comp (0..2) of
  * E after the constitutive update (target 0), D before the CPML pass (1),

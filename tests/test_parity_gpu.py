@@ -159,3 +159,44 @@ def test_check_finite_flags_nan(fdtd):
     with pytest.raises(fdtd.FdtdError) as e:
         g.check_finite()
     assert e.value.code == -5
+
+
+def _with_eps_map(p, seed):
+    """A per-cell permittivity map over the vacuum cells of `p`, and the same
+    problem restated for the oracle as one ConstantUpdate material per value."""
+    import copy
+    from fdtd_b200.problem import VACUUM, Material
+    nx, ny, nz = p.shape
+    rng = np.random.default_rng(seed)
+    levels = 1.0 + 3.0 * rng.random(8)
+    pick = rng.integers(0, len(levels), (nz, ny, nx))
+    base = p.cell_ids()
+    base = np.zeros((nz, ny, nx), np.uint8) if base is None else base
+    mats = list(p.materials) if p.materials else [Material.vacuum()]
+    vac = np.array([m.kind == VACUUM for m in mats])[base]
+    eps = np.where(vac, levels[pick], 0.0)
+    q = copy.deepcopy(p)
+    q.materials = mats + [Material.constant(float(v)) for v in levels]
+    q.ids = np.where(vac, len(mats) + pick, base).astype(np.uint8)
+    q.block_ids = None
+    return eps, q
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("make", [scenarios.tm_cpml_sources, scenarios.te_materials, scenarios.td_drude_lorentz],
+                         ids=lambda f: f.__name__)
+def test_eps_map_matches_per_cell_materials(fdtd, oracle, make, prec):
+    """fdtd_set_eps_map gives the same fields as one constant material per
+    cell (bit-identical E and H for the FP64 plain method)."""
+    p = make()
+    eps, q = _with_eps_map(p, 7)
+    o = oracle.run_oracle(q)
+    g = fdtd.Grid.from_problem(p, prec)
+    g.set_eps_map(eps)
+    g.step(p.steps)
+    g.synchronize()
+    E, H, _, _ = mode_fields(p.mode)
+    _compare(p, g, o, E + H, PLAIN_TOL if prec == "f64" else FUSED_TOL)
+    if prec == "f64":
+        for n in E + H:
+            assert np.array_equal(g.get(n), o.get(n)), n
