@@ -1,7 +1,7 @@
 """Benchmark of the FDTD time-step hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload drude384|lorentz768|tm256]
+                    [--workload drude384|lorentz768|tm256|batch64]
 
 Workload (default): the 3D FP32 Drude-sphere grid with TFSF and face DFTs --
 384^3 cells, 12-cell CPML, Drude sphere of radius 64 (eps_inf 1, wp*dt 0.3,
@@ -12,9 +12,12 @@ the whole grid. Metric: Gcell-updates/s over interior cells (the outer ring
 is never updated, as in the reference). Synthetic inputs; the state is ~1.4 GB
 of fields, far larger than L2, so no flush is needed between steps.
 
-Multi-GPU (torchrun, one process per GPU): every rank runs its own grid of
-the same size (independent replicas: the workload is one grid; sharding it by
-z slabs needs a halo exchange). value = cells of all ranks / max rank time;
+Multi-GPU (torchrun, one process per GPU): for the single-grid workloads
+every rank runs its own grid of the same size (independent replicas: the
+workload is one grid; sharding it by z slabs needs a halo exchange). For
+batch64, 64 problems per GPU are drawn from one seed and partitioned across
+the ranks by cost (fdtd_b200/shard.py); each rank steps only its share, with
+no exchange on the data path. value = cells of all ranks / max rank time;
 scaling "weak".
 
 --impl reference times the reference's own functors (oracle/_ref/ref_runner,
@@ -282,24 +285,43 @@ def _cpu_one(job):
 
 
 def run_batch(args, torch, world, rank, local, stream):
+    import torch.distributed as dist
     from fdtd_b200 import grid as G, problem as P
-    probs = P.config3(64, steps=args.steps + args.warmup + 16)
+    from fdtd_b200.shard import imbalance, partition_by_cost, problem_cost
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # 64 problems per GPU, drawn from one seed and partitioned by cost: each
+    # rank steps only its own share (no exchange on the data path)
+    allp = P.config3(64 * world, steps=args.steps + args.warmup + 16)
+    shares = partition_by_cost([problem_cost(p) for p in allp], world)
+    probs = [allp[q] for q in shares[rank]]
     grids = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
     batch = G.Batch(grids)
     batch.tune(4)
     batch.step(args.warmup, stream=stream.cuda_stream)
-    torch.cuda.synchronize()
+    barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         with torch.cuda.stream(stream):
             start.record(stream)
             batch.step(args.steps, stream=stream.cuda_stream)
             end.record(stream)
-        torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
+        barrier()
+    ms = max_over_ranks(start.elapsed_time(end))
     assert batch.error_flags() == 0
     cells = sum(p.interior_cells for p in probs)
-    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    total_cells = sum(p.interior_cells for p in allp)
+    value = total_cells * args.steps / (ms / 1e3) / 1e9
     ab = batch_alg_bytes(probs)
     peak, peak_kind = peaks()
     ach = ab * args.steps / (ms / 1e3) / 1e9
@@ -322,13 +344,14 @@ def run_batch(args, torch, world, rank, local, stream):
     ms64 = start.elapsed_time(end)
     for g in g64:
         g.close()
-    # end to end: create the 64 grids from host arrays, run, read every Hz back
+    # end to end: create this rank's grids from host arrays, run, read every Hz back
+    barrier()
     t0 = time.perf_counter()
     ge = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
     be = G.Batch(ge)
     be.step(args.steps)
     out = [g.get("Hz") for g in ge]
-    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
     h2d = sum(p.ids.nbytes + sum(s.values.nbytes for s in p.sources) for p in probs)
     d2h = sum(o.size * 8 for o in out)
     be.close()
@@ -339,15 +362,17 @@ def run_batch(args, torch, world, rank, local, stream):
         "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batch64_te_rects", "problems": len(probs), "interior_cells": cells, "seed": 0,
+        "config": {"workload": "batch64_te_rects", "problems": len(allp), "problems_per_gpu": 64,
+                   "interior_cells": total_cells, "seed": 0, "shard_imbalance": imbalance(
+                       [problem_cost(p) for p in allp], shares),
                    "cpml": 10, "steps_in_config": 3000, "tile_rows": info["rows"], "ctas": info["blocks"],
                    "tune_ms_per_step": info["tune_ms_per_step"],
-                   "l2": "state ~290 MB > L2; no flush", "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "l2": "state ~290 MB > L2; no flush", "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "kernel": "batch_kernel (persistent, all steps)", "achieved": ach, "peak": peak,
                      "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "alg_bytes_per_step": ab,
                      "traffic": None},
         "fp64_plain": {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "note": "grids stepped one by one"},
-        "e2e": {"value": cells * args.steps * world / t_e2e / 1e9, "unit": "Gcell-updates/s",
+        "e2e": {"value": total_cells * args.steps / t_e2e / 1e9, "unit": "Gcell-updates/s",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "wall_s": t_e2e},
         "cpu_baseline": cpu, "gpu_launches": 2, "clocks": clk.summary(),
     }
@@ -475,7 +500,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": p.name, "grid": list(p.shape), "interior_cells": cells, "cpml": 12,
                        "steps_in_config": 1000, "l2": "state (~1.4 GB) larger than L2; no flush",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                       "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": "fused_e_kernel (E sweep)", "achieved": e_ach, "peak": peak,
                          "unit": "GB/s", "frac": e_ach / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ab["e_sweep"], "launch_ms": prof["e_sweep"], "traffic": None},
