@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1563,3 +1564,119 @@ int fdtd_batch_error_flags(fdtd_batch* b, int* flags) {
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------
+// fdtd_step_static_scratch: the time step for callers that must not allocate
+// device memory once their grid is set up.
+//
+// The only scratch a step needs is the TFSF incident-field table: for every
+// plane, the aux grid's Ez and Hy after each step of the call, 2 (nsteps + 1) L
+// doubles. fdtd_step keeps it in a per-grid buffer that it grows with
+// cudaMalloc when a call asks for more steps than any call before. Here the
+// table lives in the fixed array below instead, so stepping allocates nothing:
+// no cudaMalloc, no cudaFree, no allocating library call, no graph. Steps run
+// as eagerly launched kernels, the same kernels and order as fdtd_step.
+//
+// * Size limit: kStaticAuxBytes (4 MiB) for the tables of all planes of one
+//   call, i.e. at most 4 MiB / (16 bytes x sum of the planes' L) - 1 steps per
+//   call; a larger call is refused with FDTD_ERR_INVALID and the limit in the
+//   message (split it into several calls).
+// * The device address of the array is looked up with cudaGetSymbolAddress
+//   once per device, on the first call there, and cached. That first lookup
+//   may make the runtime load this library's device code, so make the first
+//   call before any stream capture starts.
+// * Nothing in the array has to start at zero: the aux precompute kernel
+//   writes every row of every table before the sweeps of the call read it.
+// * The array is one per device, shared by every grid on it. Calls whose GPU
+//   work overlaps (different streams, different host threads) race on it;
+//   order them on one stream or synchronise between them.
+namespace {
+
+constexpr size_t kStaticAuxBytes = size_t(4) << 20;
+static __device__ __align__(256) double g_static_aux[kStaticAuxBytes / sizeof(double)];
+
+std::mutex g_static_aux_mu;
+double* g_static_aux_addr[64] = {};
+
+int static_aux_address(int device, double** out) {
+  if (device < 0 || device >= 64) return fail(FDTD_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_static_aux_mu);
+  if (!g_static_aux_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_aux);
+    if (e != cudaSuccess || !p)
+      return fail(FDTD_ERR_CUDA, std::string("cudaGetSymbolAddress(static TFSF table): ") + cudaGetErrorString(e));
+    g_static_aux_addr[device] = static_cast<double*>(p);
+  }
+  *out = g_static_aux_addr[device];
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
+  if (nsteps == 0) return FDTD_OK;
+  CK(cudaSetDevice(g->d.device));
+  double* base = nullptr;
+  int rc = static_aux_address(g->d.device, &base);
+  if (rc) return rc;
+  size_t row = 0;  // doubles per step over all planes' tables
+  for (auto& a : g->auxes) row += 2 * static_cast<size_t>(a.L);
+  const size_t cap = kStaticAuxBytes / sizeof(double);
+  if (row > 0 && row * (static_cast<size_t>(nsteps) + 1) > cap) {
+    const long long most = static_cast<long long>(cap / row) - 1;
+    return fail(FDTD_ERR_INVALID, "fdtd_step_static_scratch: " + std::to_string(nsteps) +
+                                      " steps need " + std::to_string(row * (nsteps + 1) * sizeof(double)) +
+                                      " bytes of TFSF table, more than the fixed " +
+                                      std::to_string(kStaticAuxBytes) + "; this grid takes at most " +
+                                      std::to_string(most < 0 ? 0 : most) + " steps per call");
+  }
+  if (g->dirty_dft) {
+    // laying out DFT regions allocates their sample buffers
+    if (!g->dfts.empty())
+      return fail(FDTD_ERR_INVALID,
+                  "fdtd_step_static_scratch: DFT regions were added since the last fdtd_step; one fdtd_step "
+                  "call (one step or more) lays out their buffers first");
+    rc = rebuild_dft(g);
+    if (rc) return rc;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  if (s != g->stream) CK(cudaStreamSynchronize(g->stream));  // set-up work on the grid's stream first
+  // point each plane's table at its slice of the fixed array for this call
+  double* saved_tab[kMaxPlanes];
+  long long saved_cap[kMaxPlanes];
+  const int naux = static_cast<int>(g->auxes.size());
+  double* p = base;
+  for (int q = 0; q < naux; q++) {
+    AuxH& a = g->auxes[q];
+    saved_tab[q] = a.d_tab;
+    saved_cap[q] = a.cap;
+    a.d_tab = p;
+    a.cap = nsteps + 1;
+    p += 2 * static_cast<size_t>(a.cap) * a.L;
+    double* st = a.d_state;
+    const int L = a.L;
+    g->launches += launch_aux_precompute(L, g->d.dt, g->d.dx, st, st + L, st + 2 * L, st + 3 * L, st + 4 * L,
+                                         st + 5 * L, a.d_coef, a.d_vals, static_cast<int>(a.vals.size()), g->t,
+                                         nsteps, a.d_tab, a.d_tab + a.cap * L, s);
+  }
+  if (naux > 0) {
+    Control c{};
+    c.t = g->t;
+    c.t0 = g->t;
+    cudaError_t e = cudaMemcpyAsync(g->ctrl, &c, sizeof(long long) * 2, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host value must outlive the copy
+    if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, std::string("step control upload: ") + cudaGetErrorString(e));
+  }
+  if (!rc) rc = enqueue_steps(g, nsteps, s, nullptr);
+  for (int q = 0; q < naux; q++) {
+    g->auxes[q].d_tab = saved_tab[q];
+    g->auxes[q].cap = saved_cap[q];
+  }
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  g->t += nsteps;
+  return FDTD_OK;
+}

@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_info",
            "fdtd_batch_error_flags", "fdtd_last_error_string"]
@@ -76,6 +76,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_material_ids": [vp, vp],
         "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
         "fdtd_set_eps_map": [vp, dp],
+        "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
         "fdtd_add_tfsf_plane": [vp, i, i, ip, ip, dp, dp, dp, dp, i, dp, i],
         "fdtd_add_dft": [vp, i, ip, ip, dp, i, ip],
@@ -216,6 +217,13 @@ class Grid:
     # ------------------------------------------------------------ run
     def step(self, n: int, stream: Optional[int] = None) -> None:
         _check(load_library().fdtd_step(self.h, int(n), ctypes.c_void_p(stream) if stream else None))
+
+    def step_static_scratch(self, n: int, stream: Optional[int] = None) -> None:
+        """step() that allocates no device memory: the TFSF table of the call
+        lives in a fixed 4 MiB device array shared by all grids of the device
+        (at most 4 MiB / (16 B x sum of the planes' aux lengths) - 1 steps per
+        call; calls that overlap on the GPU race on the array)."""
+        _check(load_library().fdtd_step_static_scratch(self.h, int(n), ctypes.c_void_p(stream) if stream else None))
 
     def profile_step(self, n: int, stream: Optional[int] = None) -> dict:
         """Mean per-step kernel times (ms) over n steps, from CUDA events

@@ -144,6 +144,22 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
 /* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
  * handle's stream). Returns once the work is enqueued. */
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
+/* fdtd_step for callers that cannot allocate device memory while stepping
+ * (no counterpart in the reference, whose steps run on the host). Same
+ * kernels, order and results as fdtd_step, launched eagerly; the per-call
+ * TFSF incident-field table goes into one fixed 4 MiB device array instead of
+ * a buffer that grows with cudaMalloc, so a call allocates nothing.
+ * - At most 4 MiB / (16 bytes x the sum of the planes' aux lengths L) - 1
+ *   steps per call (L = the plane's aux_ncells + 50); a larger call
+ *   returns FDTD_ERR_INVALID naming the limit. Without TFSF planes, no limit.
+ * - The array's address is looked up once per device on the first call, which
+ *   may load the library's device code: make that call before any stream
+ *   capture.
+ * - DFT regions added since the last fdtd_step need one fdtd_step call to lay
+ *   out their buffers; until then this returns FDTD_ERR_INVALID.
+ * - The array is shared by all grids of a device: calls whose GPU work
+ *   overlaps (other streams or host threads) race on it. */
+int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream);
 /* fdtd_step with CUDA events on the launching stream around each part of a
  * step: ms[0..4] receive the mean per-step time (milliseconds) of the E sweep,
  * the E-phase extras (TFSF kernel of the FP32 method, DFT gather), the H sweep,

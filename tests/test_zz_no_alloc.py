@@ -1,0 +1,63 @@
+"""fdtd_step_static_scratch (the step that allocates no device memory)
+against fdtd_step. Collected last on purpose: the entry point's fixed device
+array is shared by every grid of the device, so this file also checks that it
+still gives fdtd_step's results after all other tests have run."""
+import numpy as np
+import pytest
+
+import scenarios
+from helpers import mode_fields, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": 1e-12, "f32": 1e-4}
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("make", [scenarios.tm_tfsf_reference_polarisation, scenarios.td_tfsf_box],
+                         ids=lambda f: f.__name__)
+def test_static_scratch_step_matches_step(fdtd, make, prec):
+    """Two calls in a row of each entry point give the same fields and spectra."""
+    p = make()
+    ref = fdtd.Grid.from_problem(p, prec)
+    new = fdtd.Grid.from_problem(p, prec)
+    if p.dfts:
+        # one ordinary step lays out the DFT sample buffers of both grids
+        ref.step(1)
+        new.step(1)
+    E, H, _, _ = mode_fields(p.mode)
+    n = (p.steps - 1) // 2
+    for _ in range(2):
+        ref.step(n)
+        new.step_static_scratch(n)
+        assert new.step_count == ref.step_count
+        for name in E + H:
+            a, b = new.get(name), ref.get(name)
+            if np.any(b):
+                assert rel_l2(a, b) <= TOL[prec], name
+        for q in range(len(p.dfts)):
+            assert rel_l2(new.dft(q), ref.dft(q)) <= TOL[prec]
+    assert new.error_flags() == 0
+
+
+def test_static_scratch_step_refuses_oversize_calls(fdtd):
+    p = scenarios.td_tfsf_box()
+    p.dfts = []
+    g = fdtd.Grid.from_problem(p, "f32")
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.step_static_scratch(1 << 20)
+    assert e.value.code == -1
+    assert "steps per call" in str(e.value)
+    assert g.step_count == 0
+
+
+def test_static_scratch_step_needs_dft_layout(fdtd):
+    p = scenarios.td_tfsf_box()
+    assert p.dfts
+    g = fdtd.Grid.from_problem(p, "f32")
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.step_static_scratch(4)
+    assert e.value.code == -1
+    g.step(1)
+    g.step_static_scratch(4)
+    assert g.step_count == 5
