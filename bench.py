@@ -1,7 +1,7 @@
 """Benchmark of the FDTD time-step hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload drude384|lorentz768|tm256|batch64]
+                    [--workload drude384|lorentz768|tm256|batch64|adjoint512]
 
 Workload (default): the 3D FP32 Drude-sphere grid with TFSF and face DFTs --
 384^3 cells, 12-cell CPML, Drude sphere of radius 64 (eps_inf 1, wp*dt 0.3,
@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Gcell-updates/s (FP32 fused; FP64 plain alongside)"
+ADJ_METRIC = "inverse-design gradient: Gcell-updates/s of forward + adjoint (FP32 fused)"
 
 
 def parse():
@@ -48,7 +49,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="drude384", choices=["drude384", "lorentz768", "tm256", "batch64"])
+    ap.add_argument("--workload", default="drude384", choices=["drude384", "lorentz768", "tm256", "batch64",
+                                                                     "adjoint512"])
     ap.add_argument("--n", type=int, default=0, help="override the grid size (same physics, scaled): for profiling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -221,9 +223,12 @@ def run_reference_arm(args):
     if args.workload == "batch64":
         from fdtd_b200 import problem as P
         cb = cpu_batch_baseline(P.config3(64, steps=args.steps + 16), budget_s=20.0)
+    elif args.workload == "adjoint512":
+        cb = cpu_adjoint_baseline(budget_s=20.0)
     else:
         cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)))
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Gcell-updates/s",
+    metric = ADJ_METRIC if args.workload == "adjoint512" else METRIC
+    line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": "Gcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic", "scaling": "weak",
             "config": {"workload": args.workload, "reference_sample": cb["sample"]},
@@ -231,6 +236,89 @@ def run_reference_arm(args):
                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "vs_baseline": None}
     print(json.dumps(line), flush=True)
+
+
+def _adjoint_problem(n: int, steps: int):
+    from fdtd_b200 import problem as P
+    scale = n / 512
+    return P.config4(n=n, steps=steps, npml=max(6, int(16 * scale)), design=max(8, int(128 * scale)),
+                     nprobe=max(4, int(16 * scale)))
+
+
+def cpu_adjoint_baseline(budget_s: float = 20.0):
+    """The FP64 CPU adjoint (the oracle's restatement: the reference has no
+    adjoint) on a reduced inverse-design grid; value = gradient cell-steps/s
+    (forward + backward), one thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    n = 128
+
+    def run(steps):
+        p, s = _adjoint_problem(n, steps)
+        t0 = time.perf_counter()
+        pyoracle.adjoint_tm(p, steps, s.probe_lo[:2], s.probe_hi[:2], s.freq, s.design_lo[:2], s.design_hi[:2])
+        return time.perf_counter() - t0, p.interior_cells
+
+    dt0, cells = run(40)
+    steps = max(40, int(budget_s / dt0 * 40))
+    dt, cells = run(steps)
+    return {"value": cells * steps / dt / 1e9, "unit": "Gcell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{n}^2 inverse-design grid, {steps} steps forward + adjoint, {dt:.1f} s, single thread"}
+
+
+def run_adjoint(args, torch, world, rank, local):
+    """Inverse-design gradient, 2D TM FP32: one forward (checkpoints every 64
+    steps) and one backward of `steps` time steps on the 512^2 grid; value =
+    interior cells x steps / gradient time. Host clock around the synchronous
+    forward and backward calls (both end with a device synchronize)."""
+    import torch.distributed as dist
+    from fdtd_b200 import grid as G
+    steps = args.steps
+    p, spec = _adjoint_problem(args.n or 512, steps)
+    for _ in range(max(1, args.warmup // 10)):
+        pw, sw = _adjoint_problem(args.n or 512, 64)
+        gw = G.Grid.from_problem(pw, "f32", device=local)
+        aw = G.Adjoint(gw, sw.probe_lo[:2], sw.probe_hi[:2], sw.freq, sw.design_lo[:2], sw.design_hi[:2], 64)
+        aw.forward(64)
+        aw.backward()
+        aw.close()
+        gw.close()
+    g = G.Grid.from_problem(p, "f32", device=local)
+    adj = G.Adjoint(g, spec.probe_lo[:2], spec.probe_hi[:2], spec.freq, spec.design_lo[:2], spec.design_hi[:2],
+                    spec.ckpt_every)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = g.launch_count
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        J = adj.forward(steps)
+        t1 = time.perf_counter()
+        grad = adj.backward()
+        t2 = time.perf_counter()
+    launches = g.launch_count - l0
+    tt = torch.tensor([t2 - t0], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    wall = float(tt.item())
+    cells = p.interior_cells
+    cpu = cpu_adjoint_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    return {
+        "metric": ADJ_METRIC, "value":
+            cells * steps * world / wall / 1e9, "unit": "Gcell-updates/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": wall * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "adjoint512_tm_design128", "grid": list(p.shape), "interior_cells": cells,
+                   "design_box": [spec.design_lo[:2], spec.design_hi[:2]], "probes": 16, "freq": spec.freq,
+                   "ckpt_every": spec.ckpt_every, "l2": "512^2 state fits L2 (launch-bound)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "gradient_s": wall, "forward_s": t1 - t0, "backward_s": t2 - t1, "J": J,
+        "grad_abs_max": float(np.abs(grad).max()),
+        "e2e": {"value": cells * steps * world / wall / 1e9, "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": float(p.eps_map.nbytes) / steps, "d2h_bytes_per_step": float(grad.nbytes) / steps,
+                "note": "the forward and backward calls are the public API; eps map uploaded at grid creation"},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary(),
+    }
 
 
 def batch_alg_bytes(problems):
@@ -398,8 +486,11 @@ def main():
     from fdtd_b200 import grid as G
 
     stream = torch.cuda.Stream()
-    if args.workload == "batch64":
-        line = run_batch(args, torch, world, rank, local, stream)
+    if args.workload in ("batch64", "adjoint512"):
+        if args.workload == "batch64":
+            line = run_batch(args, torch, world, rank, local, stream)
+        else:
+            line = run_adjoint(args, torch, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:

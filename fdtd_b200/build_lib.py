@@ -32,6 +32,7 @@ SOURCES = {
     "kernels_tfsf.cu": [],
     "kernels_batch.cu": [],
     "kernels_common.cu": [],
+    "kernels_adjoint.cu": [],
     "fdtd_capi.cu": [],
 }
 HEADERS = ["internal.h", "fused3d_common.cuh", os.path.join("..", "..", "include", "fdtd_b200.h")]

@@ -96,6 +96,12 @@ struct SourceH {
   double* d_vals = nullptr;
 };
 
+struct BoxSourceH {
+  int comp, target, lo[3], hi[3];
+  double* d_vals = nullptr;
+  int nvals = 0;
+};
+
 struct AuxH {
   int ncells, L;
   std::vector<double> vals;
@@ -153,6 +159,7 @@ struct fdtd_grid {
   void* d_mats = nullptr;
   int max_poles = 0;
   std::vector<SourceH> srcs;
+  std::vector<BoxSourceH> boxes;
   double* d_src_last = nullptr;
   std::vector<PlaneH> planes;
   std::vector<AuxH> auxes;
@@ -807,6 +814,50 @@ int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, con
   return dalloc(g, reinterpret_cast<void**>(&g->d_src_last), kMaxSources * sizeof(double));
 }
 
+int fdtd_add_source_box(fdtd_grid* g, int comp, int target, const int* lo, const int* hi, const double* vals,
+                        int nvals) {
+  if (!g || !lo || !hi || (!vals && nvals > 0)) return fail(FDTD_ERR_INVALID, "null argument");
+  if (target == 1 || target == 3)
+    return fail(FDTD_ERR_UNSUPPORTED, "box sources add to E (target 0) or H (target 2); use point sources for D or B");
+  if (target != 0 && target != 2) return fail(FDTD_ERR_INVALID, "target must be 0 (E) or 2 (H)");
+  if (comp < 0 || comp > 2 || !(target == 0 ? hasE(g->d.mode, comp) : hasH(g->d.mode, comp)))
+    return fail(FDTD_ERR_INVALID, "component not in this mode");
+  if (nvals < 0) return fail(FDTD_ERR_INVALID, "nvals < 0");
+  for (int d = 0; d < 3; d++)
+    if (hi[d] < lo[d]) return fail(FDTD_ERR_INVALID, "empty source box");
+  if (!interior(g, lo[0], lo[1], lo[2]) || !interior(g, hi[0], hi[1], hi[2]))
+    return fail(FDTD_ERR_INVALID, "source box must lie in the interior cells");
+  CK(cudaSetDevice(g->d.device));
+  BoxSourceH b;
+  b.comp = comp;
+  b.target = target;
+  for (int d = 0; d < 3; d++) {
+    b.lo[d] = lo[d];
+    b.hi[d] = hi[d];
+  }
+  std::vector<double> v(vals, vals + nvals);
+  int rc = upload_vec(g, reinterpret_cast<void**>(&b.d_vals), v.data(), std::max<size_t>(1, v.size()) * sizeof(double));
+  if (rc) return rc;
+  b.nvals = nvals;
+  g->boxes.push_back(b);
+  g->version++;
+  return FDTD_OK;
+}
+
+// the box sources of one phase (0 = E, 1 = H): shift 0 adds this step's
+// value, shift -1 takes back the previous step's (fused method only)
+static int launch_boxes(fdtd_grid* g, int phase, int shift, cudaStream_t s) {
+  int n = 0;
+  for (const auto& b : g->boxes) {
+    if ((b.target == 0) != (phase == 0)) continue;
+    void* f = phase == 0 ? g->E[b.comp] : g->H[b.comp];
+    const double scale = (phase == 1 && g->f32 ? eta() : 1.0) * (shift < 0 ? -1.0 : 1.0);
+    n += launch_box_source(g->f32 ? 1 : 0, f, b.lo, b.hi, static_cast<int>(rowlen(g)), g->n[1], b.d_vals, b.nvals,
+                           scale, shift, g->ctrl, s);
+  }
+  return n;
+}
+
 int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const int* hi, const double* origin,
                         const double* k, const double* pol_e, const double* pol_h, int aux_ncells,
                         const double* aux_vals, int naux) {
@@ -973,8 +1024,10 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
   if (g->sweep_kind == FDTD_SWEEP_TMA && !use_tma)
     return fail(FDTD_ERR_UNSUPPORTED, "the TMA sweep is not available for this grid");
   const bool use_flat = use3d && !use_tma && (g->sweep_kind == FDTD_SWEEP_FLAT || g->sweep_kind == FDTD_SWEEP_AUTO);
+  const bool boxes = !g->boxes.empty();
   for (int q = 0; q < nsteps; q++) {
     if (prof) CK(cudaEventRecord(ev[0], s));
+    if (boxes && g->f32) g->launches += launch_boxes(g, 0, -1, s);
     if (g->f32) {
       g->launches += use_tma    ? launch_tma_e(fa, g->tma, s)
                      : use_flat ? launch_flat_e(fa, s)
@@ -984,9 +1037,11 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     else g->launches += launch_plain_e(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[1], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, g->d_plane_offs, g->plane_cells, s);
+    if (boxes) g->launches += launch_boxes(g, 0, 0, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[0], s);
     if (prof) CK(cudaEventRecord(ev[2], s));
+    if (boxes && g->f32) g->launches += launch_boxes(g, 1, -1, s);
     if (g->f32) {
       g->launches += use_tma    ? launch_tma_h(fa, g->tma, s)
                      : use_flat ? launch_flat_h(fa, s)
@@ -996,6 +1051,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     else g->launches += launch_plain_h(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[3], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, g->d_plane_offs, g->plane_cells, s);
+    if (boxes) g->launches += launch_boxes(g, 1, 0, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[1], s);
     if (prof) CK(cudaEventRecord(ev[4], s));
@@ -1387,6 +1443,7 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
     else if (g->d.mode != b->mode) why = "batched grids share one mode";
     else if (g->d.device != b->device) why = "batched grids share one device";
     else if (!g->planes.empty() || !g->dfts.empty()) why = "batched grids carry no TFSF planes or DFT regions";
+    else if (!g->boxes.empty()) why = "batched grids carry no box sources";
     else if (g->t != g0->t) why = "batched grids must have taken the same number of steps";
     else if (static_cast<long long>(g->pitch / 128) * g->n[1] >= (1 << 24)) why = "grid too large to batch";
     if (why) {
@@ -1680,3 +1737,266 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
   g->t += nsteps;
   return FDTD_OK;
 }
+
+// ----------------------------------------------------------------------------
+// Adjoint gradient d(objective)/d(eps_r) of a 2D TM FP32 fused grid.
+//
+// Objective: J = sum over a probe box of |X|^2, X the running DFT of Ez at
+// one frequency. Forward: the grid's own steps (graph-replayed), with a copy
+// of the whole time-stepped state (E, H, CPML integrators, source history,
+// step counter) every `ckpt_every` steps. Backward, per checkpoint segment
+// from the last: restore the checkpoint, recompute the segment's steps with
+// the same kernels (no DFT), keeping d_t of each design cell, then reverse
+// the segment's steps with the adjoint kernels of kernels_adjoint.cu. At the
+// end the grid is put back to its state after the forward.
+namespace {
+
+struct AdjBuf {
+  std::vector<void*> allocs;
+  ~AdjBuf() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+struct fdtd_adjoint {
+  fdtd_grid* g = nullptr;
+  int device = 0;
+  int plo[2], phi[2], dlo[2], dhi[2];
+  double freq = 0.0;
+  int ckpt_every = 64;
+  int dft = -1;
+  long long nsteps = 0;
+  bool forwarded = false;
+  std::vector<std::pair<void*, size_t>> state;
+  size_t state_bytes = 0;
+  int nckpt = 0;
+  AdjBuf buf;
+  char* d_ckpt = nullptr;
+  char* d_final = nullptr;
+  float* d_ie = nullptr;
+  float* adj[7] = {};   // aez, ahx, ahy, rxy, ryx, rzx, rzy
+  float* apsi[4] = {};  // apzx, apzy, apxy, apyx
+  size_t psi_elems[4] = {};
+  float* d_store = nullptr;
+  double* d_X = nullptr;
+  double* d_grad = nullptr;
+  double J = 0.0;
+};
+
+static int adj_alloc(fdtd_adjoint* a, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(FDTD_ERR_NOMEM, std::string("adjoint buffers: ") + cudaGetErrorString(e));
+  }
+  a->buf.allocs.push_back(*p);
+  return FDTD_OK;
+}
+
+static int adj_copy_state(fdtd_adjoint* a, char* base, bool save, cudaStream_t s) {
+  size_t off = 0;
+  for (auto& st : a->state) {
+    char* sp = base + off;
+    CK(cudaMemcpyAsync(save ? sp : st.first, save ? st.first : sp, st.second, cudaMemcpyDeviceToDevice, s));
+    off += (st.second + 255) / 256 * 256;
+  }
+  return FDTD_OK;
+}
+
+// one time step of the forward without DFT capture: the E/H sweeps and the
+// box sources of enqueue_steps, in its order (adjoint grids carry no TFSF)
+static int adj_recompute_step(fdtd_grid* g, const FusedArgs& fa, cudaStream_t s) {
+  const bool boxes = !g->boxes.empty();
+  if (boxes) g->launches += launch_boxes(g, 0, -1, s);
+  g->launches += launch_fused_e(g->d.mode, fa, s);
+  if (boxes) g->launches += launch_boxes(g, 0, 0, s);
+  if (boxes) g->launches += launch_boxes(g, 1, -1, s);
+  g->launches += launch_fused_h(g->d.mode, fa, s);
+  if (boxes) g->launches += launch_boxes(g, 1, 0, s);
+  g->launches += launch_step_advance(g->ctrl, s);
+  return FDTD_OK;
+}
+
+extern "C" {
+
+int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, double freq, const int* design_lo,
+                        const int* design_hi, int ckpt_every, fdtd_adjoint** out) {
+  if (!g || !probe_lo || !probe_hi || !design_lo || !design_hi || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  if (!g->f32 || g->d.mode != FDTD_TM)
+    return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes 2D TM grids of the FP32 fused method");
+  if (g->t != 0) return fail(FDTD_ERR_INVALID, "the adjoint starts from a grid that has not been stepped");
+  if (!g->planes.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes grids without TFSF planes");
+  if (g->max_poles != 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes non-dispersive materials");
+  if (ckpt_every < 1 || ckpt_every > 4096) return fail(FDTD_ERR_INVALID, "ckpt_every must be 1..4096");
+  if (!interior(g, probe_lo[0], probe_lo[1], 0) || !interior(g, probe_hi[0], probe_hi[1], 0) ||
+      probe_lo[0] > probe_hi[0] || probe_lo[1] > probe_hi[1])
+    return fail(FDTD_ERR_INVALID, "probe box must be a non-empty box of interior cells");
+  for (int d = 0; d < 2; d++) {
+    if (design_lo[d] > design_hi[d] || design_lo[d] < 1 || design_hi[d] > g->n[d] - 2)
+      return fail(FDTD_ERR_INVALID, "design box must be a non-empty box of interior cells");
+    for (int x = design_lo[d]; x <= design_hi[d]; x++)
+      if (slab_index(g->slab[d], x) >= 0) return fail(FDTD_ERR_UNSUPPORTED, "design box must lie outside the CPML");
+  }
+  for (const auto& sh : g->srcs)
+    if (sh.target == 1 && sh.i >= design_lo[0] && sh.i <= design_hi[0] && sh.j >= design_lo[1] &&
+        sh.j <= design_hi[1])
+      return fail(FDTD_ERR_UNSUPPORTED, "D-target sources inside the design box are not supported");
+  CK(cudaSetDevice(g->d.device));
+  const int lo3[3] = {probe_lo[0], probe_lo[1], 0}, hi3[3] = {probe_hi[0], probe_hi[1], 0};
+  int handle = -1;
+  int rc = fdtd_add_dft(g, 2, lo3, hi3, &freq, 1, &handle);
+  if (rc) return rc;
+  fdtd_adjoint* a = new fdtd_adjoint();
+  a->g = g;
+  a->device = g->d.device;
+  for (int d = 0; d < 2; d++) {
+    a->plo[d] = probe_lo[d];
+    a->phi[d] = probe_hi[d];
+    a->dlo[d] = design_lo[d];
+    a->dhi[d] = design_hi[d];
+  }
+  a->freq = freq;
+  a->ckpt_every = ckpt_every;
+  a->dft = handle;
+  *out = a;
+  return FDTD_OK;
+}
+
+int fdtd_adjoint_destroy(fdtd_adjoint* a) {
+  if (!a) return FDTD_OK;
+  cudaSetDevice(a->device);
+  cudaDeviceSynchronize();
+  delete a;
+  return FDTD_OK;
+}
+
+int fdtd_adjoint_forward(fdtd_adjoint* a, int nsteps, double* J) {
+  if (!a || !J) return fail(FDTD_ERR_INVALID, "null argument");
+  if (a->forwarded) return fail(FDTD_ERR_INVALID, "one forward per adjoint handle");
+  if (nsteps < 1) return fail(FDTD_ERR_INVALID, "nsteps < 1");
+  fdtd_grid* g = a->g;
+  if (g->t != 0) return fail(FDTD_ERR_INVALID, "the grid was stepped after the adjoint was created");
+  CK(cudaSetDevice(g->d.device));
+  if (g->dirty_dft) {
+    int rc = rebuild_dft(g);
+    if (rc) return rc;
+  }
+  cudaStream_t s = g->stream;
+  a->state = grid_state(g);
+  a->state_bytes = 0;
+  for (auto& st : a->state) a->state_bytes += (st.second + 255) / 256 * 256;
+  a->nckpt = (nsteps + a->ckpt_every - 1) / a->ckpt_every;
+  int rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_ckpt), a->state_bytes * a->nckpt);
+  if (!rc) rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_final), a->state_bytes);
+  if (rc) return rc;
+  for (int q = 0; q < a->nckpt; q++) {
+    rc = adj_copy_state(a, a->d_ckpt + a->state_bytes * q, true, s);
+    if (!rc) rc = step_impl(g, std::min(a->ckpt_every, nsteps - q * a->ckpt_every), nullptr, nullptr);
+    if (rc) return rc;
+  }
+  rc = adj_copy_state(a, a->d_final, true, s);
+  if (rc) return rc;
+  const DftH& r = g->dfts[a->dft];
+  rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_X), static_cast<size_t>(r.npts) * 2 * sizeof(double));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(a->d_X, r.d_acc, r.npts * 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  std::vector<double> X(static_cast<size_t>(r.npts) * 2);
+  CK(cudaMemcpyAsync(X.data(), r.d_acc, X.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double sum = 0.0;
+  for (long long p = 0; p < r.npts; p++) sum += X[2 * p] * X[2 * p] + X[2 * p + 1] * X[2 * p + 1];
+  a->J = sum;
+  a->nsteps = nsteps;
+  a->forwarded = true;
+  *J = sum;
+  return FDTD_OK;
+}
+
+int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad) {
+  if (!a || !grad) return fail(FDTD_ERR_INVALID, "null argument");
+  if (!a->forwarded) return fail(FDTD_ERR_INVALID, "run fdtd_adjoint_forward first");
+  fdtd_grid* g = a->g;
+  if (g->t != a->nsteps) return fail(FDTD_ERR_INVALID, "the grid was stepped after the adjoint forward");
+  CK(cudaSetDevice(g->d.device));
+  cudaStream_t s = g->stream;
+  const size_t fe = static_cast<size_t>(field_elems(g));
+  const int dw = a->dhi[0] - a->dlo[0] + 1, nd = dw * (a->dhi[1] - a->dlo[1] + 1);
+  int rc = FDTD_OK;
+  if (!a->d_ie) {
+    rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_ie), fe * sizeof(float));
+    for (int q = 0; q < 7 && !rc; q++) rc = adj_alloc(a, reinterpret_cast<void**>(&a->adj[q]), fe * sizeof(float));
+    // adjoint CPML integrators: the compact slabs of psi_zx, psi_zy (E) and psi_yx, psi_xy (H)
+    const size_t sx = static_cast<size_t>(g->n[1]) * g->slab[0].W, sy = static_cast<size_t>(g->slab[1].W) * rowlen(g);
+    const size_t sizes[4] = {sx, sy, sy, sx};
+    for (int q = 0; q < 4 && !rc; q++) {
+      a->psi_elems[q] = sizes[q];
+      rc = adj_alloc(a, reinterpret_cast<void**>(&a->apsi[q]), sizes[q] * sizeof(float));
+    }
+    if (!rc) rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_store), static_cast<size_t>(a->ckpt_every) * nd * sizeof(float));
+    if (!rc) rc = adj_alloc(a, reinterpret_cast<void**>(&a->d_grad), nd * sizeof(double));
+    if (rc) return rc;
+  }
+  FusedArgs fa = fused_args(g);
+  g->launches += launch_adjoint_inv_eps(fa, a->d_ie, s);
+  for (int q = 0; q < 7; q++) CK(cudaMemsetAsync(a->adj[q], 0, fe * sizeof(float), s));
+  for (int q = 0; q < 4; q++) CK(cudaMemsetAsync(a->apsi[q], 0, std::max<size_t>(a->psi_elems[q], 4) * sizeof(float), s));
+  CK(cudaMemsetAsync(a->d_grad, 0, nd * sizeof(double), s));
+  AdjArgs aa;
+  memset(&aa, 0, sizeof(aa));
+  aa.nx = g->n[0];
+  aa.ny = g->n[1];
+  aa.pitch = g->pitch;
+  for (int ft = 0; ft < 2; ft++)
+    for (int x = 0; x < 3; x++) aa.prof[ft][x] = fa.prof[ft][x];
+  for (int x = 0; x < 3; x++) {
+    aa.slab[x] = fa.slab[x];
+    aa.pml_axis[x] = fa.pml_axis[x];
+  }
+  aa.ie = a->d_ie;
+  aa.aez = a->adj[0];
+  aa.ahx = a->adj[1];
+  aa.ahy = a->adj[2];
+  aa.rxy = a->adj[3];
+  aa.ryx = a->adj[4];
+  aa.rzx = a->adj[5];
+  aa.rzy = a->adj[6];
+  aa.apzx = a->apsi[0];
+  aa.apzy = a->apsi[1];
+  aa.apxy = a->apsi[2];
+  aa.apyx = a->apsi[3];
+  for (int d = 0; d < 2; d++) {
+    aa.plo[d] = a->plo[d];
+    aa.phi[d] = a->phi[d];
+    aa.dlo[d] = a->dlo[d];
+    aa.dhi[d] = a->dhi[d];
+  }
+  aa.X = a->d_X;
+  aa.freq = a->freq;
+  aa.ndesign = nd;
+  aa.grad = a->d_grad;
+  const float* hx = static_cast<const float*>(g->H[0]);
+  const float* hy = static_cast<const float*>(g->H[1]);
+  for (int q = a->nckpt - 1; q >= 0 && !rc; q--) {
+    const long long t0 = static_cast<long long>(q) * a->ckpt_every;
+    const int len = static_cast<int>(std::min<long long>(a->ckpt_every, a->nsteps - t0));
+    rc = adj_copy_state(a, a->d_ckpt + a->state_bytes * q, false, s);
+    for (int k = 0; k < len && !rc; k++) {
+      g->launches += launch_adjoint_capture(aa, hx, hy, a->d_store + static_cast<size_t>(k) * nd, s);
+      rc = adj_recompute_step(g, fa, s);
+    }
+    for (int k = len - 1; k >= 0 && !rc; k--)
+      g->launches += launch_adjoint_step(aa, t0 + k + 1, a->d_store + static_cast<size_t>(k) * nd, s);
+  }
+  // the grid goes back to its state after the forward
+  if (!rc) rc = adj_copy_state(a, a->d_final, false, s);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(grad, a->d_grad, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return FDTD_OK;
+}
+
+}  // extern "C"

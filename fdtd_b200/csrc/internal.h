@@ -169,6 +169,25 @@ struct DftRegionDev {
   double* acc;  // [nf][npts][2]
 };
 
+// adjoint of the FP32 fused 2D TM step (kernels_adjoint.cu); all arrays in
+// the grid's pitch layout unless noted
+struct AdjArgs {
+  int nx, ny, pitch;
+  Prof<float> prof[2][3];
+  Slab slab[3];
+  int pml_axis[3];
+  const float* ie;                  // 1/eps per cell
+  float *aez, *ahx, *ahy;           // adjoint fields
+  float *apzx, *apzy, *apxy, *apyx; // adjoint CPML integrators (compact slabs)
+  float *rxy, *ryx, *rzx, *rzy;     // adjoints of the curl differences
+  int plo[2], phi[2];               // probe box (inclusive)
+  const double* X;                  // probe DFT (re, im), probe box order
+  double freq;                      // cycles per step
+  int dlo[2], dhi[2];               // design box (inclusive)
+  int ndesign;
+  double* grad;                     // dJ/deps_r, design box order
+};
+
 // kernel launchers (stream-ordered); each returns the number of launches
 int launch_plain_e(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
@@ -195,6 +214,11 @@ int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int 
 int launch_dft_rebase(Control* ctrl, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
+int launch_adjoint_inv_eps(const FusedArgs& fa, float* ie, cudaStream_t s);
+int launch_adjoint_capture(const AdjArgs& a, const float* hx, const float* hy, float* slot, cudaStream_t s);
+int launch_adjoint_step(const AdjArgs& a, long long n, const float* dslot, cudaStream_t s);
+int launch_box_source(int is_f32, void* field, const int* lo, const int* hi, int pitch, int ny, const double* vals,
+                      int nvals, double scale, int shift, const Control* ctrl, cudaStream_t s);
 // control block of a batch's persistent kernel (grid barrier + error flag)
 struct BatchCtl {
   unsigned count;  // CTAs arrived at the current barrier

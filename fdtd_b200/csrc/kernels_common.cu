@@ -129,6 +129,38 @@ int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaS
 
 __global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
 
+// A soft source on every cell of an inclusive box (a line source is a box one
+// cell wide): field += scale * vals[t + shift] on each cell, t the current
+// step; shift = -1 with a negative scale takes back the previous step's value
+// (the fused method stores E and H with their transient source included).
+template <typename T>
+__global__ void box_source_kernel(T* f, int lox, int loy, int loz, int ex, int ey, long long n, int pitch, int ny,
+                                  const double* vals, int nvals, double scale, int shift, const Control* ctrl) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long t = ctrl->t + shift;
+  if (q >= n || t < 0 || t >= nvals) return;
+  const int i = lox + static_cast<int>(q % ex);
+  const long long r = q / ex;
+  const int j = loy + static_cast<int>(r % ey);
+  const int k = loz + static_cast<int>(r / ey);
+  const long long c = (static_cast<long long>(k) * ny + j) * pitch + i;
+  f[c] = f[c] + static_cast<T>(scale * vals[t]);
+}
+
+int launch_box_source(int is_f32, void* field, const int* lo, const int* hi, int pitch, int ny, const double* vals,
+                      int nvals, double scale, int shift, const Control* ctrl, cudaStream_t s) {
+  const int ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
+  const long long n = static_cast<long long>(ex) * ey * ez;
+  const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+  if (is_f32)
+    box_source_kernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(field), lo[0], lo[1], lo[2], ex, ey, n, pitch,
+                                                    ny, vals, nvals, scale, shift, ctrl);
+  else
+    box_source_kernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(field), lo[0], lo[1], lo[2], ex, ey, n,
+                                                     pitch, ny, vals, nvals, scale, shift, ctrl);
+  return 1;
+}
+
 __global__ void batch_advance_kernel(Control* const* ctrls, int n, int nsteps) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {

@@ -83,7 +83,12 @@ __global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__
     if (a.ids) mid = a.ids[c];
     else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
     const MatF32& m = a.mats[mid];
-    const double sc = a.dt / kEps0 * m.inv_eps;
+    float ie = m.inv_eps;
+    if (a.inv_eps_map && m.npoles == 0) {
+      const float v = a.inv_eps_map[c];
+      if (v > 0.f) ie = v;
+    }
+    const double sc = a.dt / kEps0 * ie;
     for (int I = 0; I < 3; I++) {
       if (!hasE(MODE, I)) continue;
       const float dE = static_cast<float>(sc * corr[I]);

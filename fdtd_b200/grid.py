@@ -31,11 +31,12 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
-           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_tfsf_plane", "fdtd_add_dft",
+           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_info",
-           "fdtd_batch_error_flags", "fdtd_last_error_string"]
+           "fdtd_batch_error_flags", "fdtd_adjoint_create", "fdtd_adjoint_forward", "fdtd_adjoint_backward",
+           "fdtd_adjoint_destroy", "fdtd_last_error_string"]
 
 
 class FdtdError(RuntimeError):
@@ -78,6 +79,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_eps_map": [vp, dp],
         "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
+        "fdtd_add_source_box": [vp, i, i, ip, ip, dp, i],
         "fdtd_add_tfsf_plane": [vp, i, i, ip, ip, dp, dp, dp, dp, i, dp, i],
         "fdtd_add_dft": [vp, i, ip, ip, dp, i, ip],
         "fdtd_dft_npoints": [vp, i, llp],
@@ -100,6 +102,10 @@ def load_library(path: str = LIB_PATH):
         "fdtd_batch_step": [vp, i, vp],
         "fdtd_batch_info": [vp, ip, ip, ip, ctypes.POINTER(ctypes.c_float)],
         "fdtd_batch_error_flags": [vp, ip],
+        "fdtd_adjoint_create": [vp, ip, ip, ctypes.c_double, ip, ip, i, ctypes.POINTER(vp)],
+        "fdtd_adjoint_forward": [vp, i, dp],
+        "fdtd_adjoint_backward": [vp, dp],
+        "fdtd_adjoint_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -177,6 +183,11 @@ class Grid:
         assert a.size == self.shape[0] * self.shape[1] * self.shape[2]
         _check(load_library().fdtd_set_eps_map(self.h, _dp(a)))
 
+    def add_source_box(self, comp: int, lo, hi, values, target: str = "E") -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(load_library().fdtd_add_source_box(self.h, comp, P.SOURCE_TARGETS[target], _ip(lo), _ip(hi), _dp(v),
+                                                  len(v)))
+
     def add_source(self, comp: int, pos, values, target: str = "E") -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)
         _check(load_library().fdtd_add_source(self.h, comp, P.SOURCE_TARGETS[target], *pos, _dp(v), len(v)))
@@ -204,8 +215,13 @@ class Grid:
             g.set_material_ids(p.ids)
         elif p.block_ids is not None:
             g.set_material_blocks(p.block_shift, p.block_ids)
+        if p.eps_map is not None:
+            g.set_eps_map(p.eps_map)
         for s in p.sources:
-            g.add_source(s.comp, s.pos, s.values, s.target)
+            if s.hi is None:
+                g.add_source(s.comp, s.pos, s.values, s.target)
+            else:
+                g.add_source_box(s.comp, s.pos, s.hi, s.values, s.target)
         if p.tfsf is not None:
             t = p.tfsf
             for pl in t.planes:
@@ -346,6 +362,43 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "h", None):
             load_library().fdtd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """d(objective)/d(eps_r) of a 2D TM FP32 grid by the discrete adjoint
+    (fdtd_adjoint_*): J = sum over the probe box of |DFT_freq(Ez)|^2. The
+    grid must be unstepped; forward() steps it and returns J, backward()
+    returns dJ/deps_r over the design box as [ny_d, nx_d]."""
+
+    def __init__(self, grid: Grid, probe_lo, probe_hi, freq: float, design_lo, design_hi, ckpt_every: int = 64):
+        self.grid = grid
+        self.design = (tuple(design_lo), tuple(design_hi))
+        h = ctypes.c_void_p()
+        _check(load_library().fdtd_adjoint_create(grid.h, _ip(probe_lo), _ip(probe_hi), float(freq), _ip(design_lo),
+                                                  _ip(design_hi), int(ckpt_every), ctypes.byref(h)))
+        self.h = h
+
+    def forward(self, nsteps: int) -> float:
+        J = ctypes.c_double()
+        _check(load_library().fdtd_adjoint_forward(self.h, int(nsteps), ctypes.byref(J)))
+        return J.value
+
+    def backward(self) -> np.ndarray:
+        (x0, y0), (x1, y1) = self.design[0][:2], self.design[1][:2]
+        out = np.zeros((y1 - y0 + 1, x1 - x0 + 1))
+        _check(load_library().fdtd_adjoint_backward(self.h, _dp(out)))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            load_library().fdtd_adjoint_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -89,6 +89,9 @@ class Source:
     pos: Tuple[int, int, int]
     values: np.ndarray
     target: str = "E"
+    # with `hi`, the same source on every cell of the inclusive box pos..hi
+    # (a line source); E and H targets only
+    hi: Optional[Tuple[int, int, int]] = None
 
 
 @dataclass
@@ -137,6 +140,9 @@ class Problem:
     pml: dict = field(default_factory=dict)  # {(axis, side): ncells}
     materials: List[Material] = field(default_factory=lambda: [Material.vacuum()])
     ids: Optional[np.ndarray] = None  # uint8, shape (nz, ny, nx)
+    # per-cell relative permittivity of vacuum/constant cells (> 0 replaces
+    # the material's eps_inf), float64, shape (nz, ny, nx)
+    eps_map: Optional[np.ndarray] = None
     block_ids: Optional[np.ndarray] = None  # uint16, shape (nbz, nby, nbx)
     block_shift: int = 0
     sources: List[Source] = field(default_factory=list)
@@ -182,6 +188,29 @@ def gaussian_pulse(nsteps: int, t0: float = 60.0, spread: float = 20.0, offset: 
     """g(n) = exp(-((n + offset - t0)/spread)^2) for n = 0..nsteps-1."""
     n = np.arange(nsteps, dtype=np.float64) + offset
     return np.exp(-(((n - t0) / spread) ** 2))
+
+
+def sinusoid(nsteps: int, freq: float, phase: float = 0.0) -> np.ndarray:
+    """The reference's SinData / Sinusoid signal (include/Source.hpp:100-129)
+    sampled at t = n dt, with freq in cycles per step: angular frequency
+    w = 2 pi freq / dt, s(t) = tanh(t / tau) sin(w t + phase), tau = (10 / w)(pi / 2);
+    in steps, tau = 2.5 / freq."""
+    n = np.arange(nsteps, dtype=np.float64)
+    w = 2.0 * math.pi * freq
+    tau = 10.0 / w * math.pi / 2.0
+    return np.tanh(n / tau) * np.sin(w * n + phase)
+
+
+@dataclass
+class AdjointSpec:
+    """Objective J = sum over the probe box of |DFT_freq(Ez)|^2, gradient over
+    the design box (inclusive boxes, z = 0)."""
+    probe_lo: Tuple[int, int, int]
+    probe_hi: Tuple[int, int, int]
+    freq: float
+    design_lo: Tuple[int, int, int]
+    design_hi: Tuple[int, int, int]
+    ckpt_every: int = 64
 
 
 def ref_tm_polarisation(k):
@@ -314,6 +343,35 @@ def config3(nproblems: int = 64, steps: int = 3000, seed: int = 0, nmin: int = 1
         p.steps = steps
         out.append(p)
     return out
+
+
+def config4(n: int = 512, steps: int = 4000, npml: int = 16, design: int = 128, seed: int = 0, nprobe: int = 16,
+            freq: float = 0.05, ckpt_every: int = 64):
+    """Adjoint inverse design, 2D TM: 16-cell CPML, a central design box of
+    design^2 cells with eps_r uniform in [1, 12] from `seed`, a line source of
+    Ez (the Sinusoid signal at `freq` cycles per step) on column npml + 8
+    over every interior row, and the objective sum |DFT_freq(Ez)|^2 over
+    `nprobe` cells of column n - 1 - (npml + 8), centred. Returns (Problem,
+    AdjointSpec)."""
+    dx = 1e-6
+    dt = courant_dt(dx, 0.99 / math.sqrt(2.0))
+    p = Problem(TM, (n, n, 1), dx, dt, name=f"tm{n}_adjoint_design{design}")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = npml
+    rng = np.random.default_rng(seed)
+    d0 = (n - design) // 2
+    eps = np.zeros((1, n, n))
+    eps[0, d0:d0 + design, d0:d0 + design] = rng.uniform(1.0, 12.0, size=(design, design))
+    p.eps_map = eps
+    col = npml + 8
+    p.sources.append(Source(2, (col, 1, 0), sinusoid(steps, freq), "E", hi=(col, n - 2, 0)))
+    pc = n - 1 - (npml + 8)
+    j0 = n // 2 - nprobe // 2
+    spec = AdjointSpec((pc, j0, 0), (pc, j0 + nprobe - 1, 0), freq, (d0, d0, 0), (d0 + design - 1, d0 + design - 1, 0),
+                       ckpt_every)
+    p.steps = steps
+    return p, spec
 
 
 def config5(n: int = 768, steps: int = 500, npml: int = 16, block: int = 32, seed: int = 0,

@@ -123,6 +123,12 @@ int fdtd_set_eps_map(fdtd_grid* g, const double* eps);
  * H after the magnetic constitutive update (2) or B before the magnetic CPML
  * pass (3). */
 int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals);
+/* The same soft source on every interior cell of the inclusive box lo..hi
+ * (a line source is a box one cell wide): one SoftSource per cell in the
+ * reference, all driven by one signal. Targets E (0) or H (2) only; it is
+ * applied after the point sources of the same field. */
+int fdtd_add_source_box(fdtd_grid* g, int comp, int target, const int* lo, const int* hi, const double* vals,
+                        int nvals);
 
 /* One TFSF plane (TFSFPlane, Source.hpp:472-634): corrections on the cells
  * lo..hi (inclusive) with normal orient (0 = -axis, 1 = +axis), wave vector
@@ -217,6 +223,27 @@ int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, float* tu
 int fdtd_batch_error_flags(fdtd_batch* b, int* flags);
 
 /* Last error of the calling thread ("" if none). */
+/* ---- adjoint gradient (2D TM, FP32 fused method) ----
+ * d(objective)/d(eps_r) over a design box by the discrete adjoint of the
+ * time step. Objective J = sum over the probe box (inclusive, z = 0) of
+ * |X|^2, X the running DFT of Ez at `freq` (cycles per step, samples as
+ * fdtd_add_dft). The grid must be unstepped, without TFSF planes or
+ * dispersive materials; the design box must lie outside the CPML and hold no
+ * D-target source. create adds the probe DFT region to the grid. forward
+ * steps the grid nsteps times, checkpointing the state every ckpt_every
+ * steps, and returns J; backward recomputes each segment from its checkpoint,
+ * reverses it, leaves the grid in its post-forward state and writes
+ * dJ/deps_r of every design cell (x fastest) to the host array grad. One
+ * forward and one backward per handle; destroy it before its grid.
+ * The reference has no adjoint; its per-cell permittivity is the K of
+ * ConstantUpdate (DispersiveMaterials.hpp:354-359). */
+typedef struct fdtd_adjoint fdtd_adjoint;
+int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, double freq, const int* design_lo,
+                        const int* design_hi, int ckpt_every, fdtd_adjoint** out);
+int fdtd_adjoint_forward(fdtd_adjoint* a, int nsteps, double* J);
+int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad);
+int fdtd_adjoint_destroy(fdtd_adjoint* a);
+
 const char* fdtd_last_error_string(void);
 
 #ifdef __cplusplus

@@ -10,8 +10,9 @@
  * tests/golden/).
  *
  * Schedule of one step (the user loop of tests/testTM.cpp:102-113 and
- * include/Source.hpp:413-435, with TFSF and sources placed as documented in
- * DESIGN.md):
+ * include/Source.hpp:413-435; the reference fixes no place for TFSF planes and
+ * soft sources in a user loop, so they sit where this schedule puts them, and
+ * the GPU library follows the same schedule):
  *   E half: YeeUpdate on every E flux, TFSF updateD, D-target sources,
  *           UpdatePML<Electric, X|Y|Z>, material update, E-target sources,
  *           DFT of E.
@@ -65,6 +66,7 @@ typedef struct {
 
 typedef struct {
   int comp, target, i, j, k, nvals;
+  int i1, j1, k1; /* box sources: the inclusive upper corner */
   double* vals;
 } src_t;
 
@@ -87,6 +89,9 @@ struct oracle_grid {
   uint8_t* ids;
   src_t* srcs;
   int nsrc;
+  src_t* boxes;
+  int nbox;
+  double* eps_map; /* per-cell relative permittivity of vacuum/constant cells, or NULL */
   plane_t* planes;
   int nplanes;
   dft_t* dfts;
@@ -181,6 +186,9 @@ void oracle_destroy(oracle_grid* g) {
   free(g->ids);
   for (int s = 0; s < g->nsrc; s++) free(g->srcs[s].vals);
   free(g->srcs);
+  for (int s = 0; s < g->nbox; s++) free(g->boxes[s].vals);
+  free(g->boxes);
+  free(g->eps_map);
   for (int p = 0; p < g->nplanes; p++) {
     plane_t* pl = &g->planes[p];
     free(pl->Dz); free(pl->Ez); free(pl->By); free(pl->Hy); free(pl->psiE); free(pl->psiH); free(pl->vals);
@@ -237,6 +245,46 @@ int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k,
   s->comp = comp; s->target = target; s->i = i; s->j = j; s->k = k; s->nvals = nvals;
   s->vals = zalloc(nvals);
   memcpy(s->vals, vals, nvals * sizeof(double));
+  return 0;
+}
+
+int oracle_add_source_box(oracle_grid* g, int comp, int target, const int* lo, const int* hi, const double* vals,
+                          int nvals) {
+  if (comp < 0 || comp > 2 || (target != 0 && target != 2)) return -1;
+  for (int d = 0; d < 3; d++)
+    if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return -1;
+  g->boxes = (src_t*)realloc(g->boxes, (g->nbox + 1) * sizeof(src_t));
+  src_t* s = &g->boxes[g->nbox++];
+  s->comp = comp; s->target = target; s->nvals = nvals;
+  s->i = lo[0]; s->j = lo[1]; s->k = lo[2]; s->i1 = hi[0]; s->j1 = hi[1]; s->k1 = hi[2];
+  s->vals = zalloc(nvals);
+  memcpy(s->vals, vals, nvals * sizeof(double));
+  return 0;
+}
+
+/* every cell of each box source of `target` (0 = E, 2 = H) gets the value of
+ * step t, after the point sources of the same field */
+static void apply_boxes(oracle_grid* g, int target) {
+  const size_t sy = (size_t)g->n[0], sz = (size_t)g->n[0] * g->n[1];
+  for (int s = 0; s < g->nbox; s++) {
+    const src_t* b = &g->boxes[s];
+    if (b->target != target) continue;
+    const double v = g->t < b->nvals ? b->vals[g->t] : 0.0;
+    double* f = target == 0 ? g->E[b->comp] : g->H[b->comp];
+    for (int k = b->k; k <= b->k1; k++)
+      for (int j = b->j; j <= b->j1; j++)
+        for (int i = b->i; i <= b->i1; i++) f[k * sz + j * sy + i] += v;
+  }
+}
+
+int oracle_set_eps_map(oracle_grid* g, const double* eps) {
+  if (!eps) {
+    free(g->eps_map);
+    g->eps_map = NULL;
+    return 0;
+  }
+  if (!g->eps_map) g->eps_map = zalloc(g->ncell);
+  memcpy(g->eps_map, eps, g->ncell * sizeof(double));
   return 0;
 }
 
@@ -500,7 +548,10 @@ static void step_one(oracle_grid* g) {
           if (!g->hasE[I]) continue;
           double* D = &g->D[I][c];
           double* E = &g->E[I][c];
-          if (m->kind == OR_VACUUM) {
+          if (m->kind <= OR_CONSTANT && g->eps_map && g->eps_map[c] > 0.0) {
+            /* a per-cell ConstantUpdate<Mode, Electric>(K) */
+            *E = *D / (g->eps_map[c] * k_eps0);
+          } else if (m->kind == OR_VACUUM) {
             *E = *D / (1.0 * k_eps0);
           } else if (m->kind == OR_CONSTANT) {
             *E = *D / (m->eps_inf * k_eps0);
@@ -536,6 +587,7 @@ static void step_one(oracle_grid* g) {
     size_t c = sr->k * sz + sr->j * sy + sr->i;
     g->E[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
   }
+  apply_boxes(g, 0);
   dft_apply(g, 0, (double)(g->t + 1));
 
   /* ---------------- H half step ---------------- */
@@ -600,6 +652,7 @@ static void step_one(oracle_grid* g) {
     size_t c = sr->k * sz + sr->j * sy + sr->i;
     g->H[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
   }
+  apply_boxes(g, 2);
   dft_apply(g, 1, (double)g->t + 1.5);
   g->t++;
 }
@@ -634,5 +687,109 @@ int oracle_set(oracle_grid* g, int which, const double* in) {
   double* p = which_ptr(g, which);
   if (!p) return -1;
   memcpy(p, in, g->ncell * sizeof(double));
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * FP64 discrete adjoint of the TM step above (oracle_step), for
+ *   J = sum over the probe box of |X|^2,  X = the DFT of Ez at `freq`
+ *       (cycles per step; E samples at n = t + 1, as dft_apply),
+ * and its gradient with respect to the relative permittivity of every cell
+ * of the design box. It runs the forward itself from a fresh grid (t = 0),
+ * keeping D_z of the design cells after every step, then walks the steps
+ * backwards through the transpose of each update in reverse order:
+ *   H half:  B_x' = B_x - dt (F/dx diff_xy + G psi_xy),  psi_xy' = B psi_xy + C/dx diff_xy
+ *            (diff_xy = E_z[+y] - E_z), and likewise B_y with diff_yx = E_z[+x] - E_z
+ *            entering with the Levi-Civita sign -1; H = B / mu0.
+ *   E half:  D_z' = D_z + dt (F_x/dx diff_zx - F_y/dx diff_zy) + dt (G_x psi_zx + G_y psi_zy)
+ *            (old psi), psi_zx' = B_x psi_zx + C_x/dx diff_zx, psi_zy' = B_y psi_zy - C_y/dx diff_zy,
+ *            E_z = D_z' / (eps_r eps0)  =>  dJ/deps_r += lambda_E * (-D_z' / (eps_r^2 eps0)).
+ * Sources are affine in the state and drop out. Supported: TM, non-dispersive
+ * materials with mu_r = 1, no TFSF planes. Test infrastructure only. */
+int oracle_adjoint_tm(oracle_grid* g, int nsteps, const int* plo, const int* phi, double freq, const int* dlo,
+                      const int* dhi, double* J_out, double* grad) {
+  if (g->mode != TM || g->t != 0 || g->nplanes > 0 || nsteps < 1) return -1;
+  for (int m = 0; m < g->nmat; m++)
+    if (g->mats[m].kind > OR_CONSTANT || g->mats[m].mu_r != 1.0) return -1;
+  for (int d = 0; d < 2; d++)
+    if (dlo[d] < 1 || dhi[d] > g->n[d] - 2 || dlo[d] > dhi[d]) return -1;
+  const int nx = g->n[0], ny = g->n[1];
+  const size_t sy = (size_t)nx, nc = g->ncell;
+  const double dt = g->dt, dx = g->dx;
+  int lo3[3] = {plo[0], plo[1], 0}, hi3[3] = {phi[0], phi[1], 0};
+  const int h = oracle_add_dft(g, 2, lo3, hi3, &freq, 1);
+  if (h < 0) return -1;
+  const int dw = dhi[0] - dlo[0] + 1, nd = dw * (dhi[1] - dlo[1] + 1);
+  double* Dst = zalloc((size_t)nsteps * nd);
+  double* eps = zalloc(nd);
+  for (int q = 0; q < nd; q++) {
+    size_t c = (size_t)(dlo[1] + q / dw) * sy + dlo[0] + q % dw;
+    const oracle_material* m = &g->mats[g->ids ? g->ids[c] : 0];
+    eps[q] = (g->eps_map && g->eps_map[c] > 0.0) ? g->eps_map[c] : (m->kind == OR_VACUUM ? 1.0 : m->eps_inf);
+  }
+  for (int t = 0; t < nsteps; t++) {
+    step_one(g);
+    for (int q = 0; q < nd; q++) Dst[(size_t)t * nd + q] = g->D[2][(size_t)(dlo[1] + q / dw) * sy + dlo[0] + q % dw];
+  }
+  const dft_t* r = &g->dfts[h];
+  double J = 0.0;
+  for (int p = 0; p < r->npts; p++) J += r->acc[2 * p] * r->acc[2 * p] + r->acc[2 * p + 1] * r->acc[2 * p + 1];
+  *J_out = J;
+
+  double *lD = zalloc(nc), *lBx = zalloc(nc), *lBy = zalloc(nc), *lE = zalloc(nc);
+  double *lpzx = zalloc(nc), *lpzy = zalloc(nc), *lpxy = zalloc(nc), *lpyx = zalloc(nc);
+  double *qxy = zalloc(nc), *qyx = zalloc(nc), *qzx = zalloc(nc), *qzy = zalloc(nc);
+  const double *eF[2] = {g->cF[0][0], g->cF[0][1]}, *eG[2] = {g->cG[0][0], g->cG[0][1]};
+  const double *eB[2] = {g->cB[0][0], g->cB[0][1]}, *eC[2] = {g->cC[0][0], g->cC[0][1]};
+  const double *hF[2] = {g->cF[1][0], g->cF[1][1]}, *hG[2] = {g->cG[1][0], g->cG[1][1]};
+  const double *hB[2] = {g->cB[1][0], g->cB[1][1]}, *hC[2] = {g->cC[1][0], g->cC[1][1]};
+  for (int q = 0; q < nd; q++) grad[q] = 0.0;
+  for (int t = nsteps - 1; t >= 0; t--) {
+    /* H half, reversed: adjoints of diff_xy (qxy) and diff_yx (qyx) */
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = j * sy + i;
+        qxy[c] = -dt * hF[1][j] / dx * lBx[c] + hC[1][j] / dx * lpxy[c];
+        lpxy[c] = -dt * hG[1][j] * lBx[c] + hB[1][j] * lpxy[c];
+        qyx[c] = dt * hF[0][i] / dx * lBy[c] - hC[0][i] / dx * lpyx[c];
+        lpyx[c] = -dt * hG[0][i] * lBy[c] + hB[0][i] * lpyx[c];
+      }
+    const double ph = 2.0 * k_pi * freq * (double)(t + 1);
+    const double cs = cos(ph), sn = sin(ph);
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = j * sy + i;
+        double v = qxy[c - sy] - qxy[c] + qyx[c - 1] - qyx[c];
+        if (i >= plo[0] && i <= phi[0] && j >= plo[1] && j <= phi[1]) {
+          int p = (j - plo[1]) * (phi[0] - plo[0] + 1) + (i - plo[0]);
+          v += 2.0 * (r->acc[2 * p] * cs - r->acc[2 * p + 1] * sn);
+        }
+        lE[c] = v;
+      }
+    /* E half, reversed */
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = j * sy + i;
+        const oracle_material* m = &g->mats[g->ids ? g->ids[c] : 0];
+        double e = (g->eps_map && g->eps_map[c] > 0.0) ? g->eps_map[c] : (m->kind == OR_VACUUM ? 1.0 : m->eps_inf);
+        if (i >= dlo[0] && i <= dhi[0] && j >= dlo[1] && j <= dhi[1]) {
+          int q = (j - dlo[1]) * dw + (i - dlo[0]);
+          grad[q] += lE[c] * (-Dst[(size_t)t * nd + q] / (e * e * k_eps0));
+        }
+        lD[c] += lE[c] / (e * k_eps0);
+        qzx[c] = eC[0][i] / dx * lpzx[c] + dt * eF[0][i] / dx * lD[c];
+        lpzx[c] = dt * eG[0][i] * lD[c] + eB[0][i] * lpzx[c];
+        qzy[c] = -eC[1][j] / dx * lpzy[c] - dt * eF[1][j] / dx * lD[c];
+        lpzy[c] = dt * eG[1][j] * lD[c] + eB[1][j] * lpzy[c];
+      }
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = j * sy + i;
+        lBy[c] += (qzx[c] - qzx[c + 1]) / K_MU0;
+        lBx[c] += (qzy[c] - qzy[c + sy]) / K_MU0;
+      }
+  }
+  free(lD); free(lBx); free(lBy); free(lE); free(lpzx); free(lpzy); free(lpxy); free(lpyx);
+  free(qxy); free(qyx); free(qzx); free(qzy); free(Dst); free(eps);
   return 0;
 }

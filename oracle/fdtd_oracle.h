@@ -43,6 +43,13 @@ int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids);
  * update), 3 = B (before the magnetic CPML pass). vals[t] is added at step t. */
 int oracle_add_source(oracle_grid* g, int comp, int target, int i, int j, int k,
                       const double* vals, int nvals);
+/* the same source on every cell of the inclusive box lo..hi; target 0 (E) or
+ * 2 (H); applied after the point sources of the same field */
+int oracle_add_source_box(oracle_grid* g, int comp, int target, const int* lo, const int* hi, const double* vals,
+                          int nvals);
+/* per-cell relative permittivity (ncell doubles, x fastest): vacuum and
+ * constant cells with a value > 0 take it in place of eps_inf; NULL removes */
+int oracle_set_eps_map(oracle_grid* g, const double* eps);
 /* One TFSF plane (include/Source.hpp:472-634) with its own Aux1D grid.
  * axis/orient give the normal; lo/hi are inclusive cell ranges; origin (in
  * cells) and k define the location functor and wave vector; pol_e / pol_h are
@@ -65,6 +72,11 @@ int oracle_dft_npoints(const oracle_grid* g, int handle);
 /* the 1D CPML coefficient profile of one axis: out[4][n] = B, C, F, G */
 int oracle_pml_profile(const oracle_grid* g, int ft, int axis, double* out);
 double oracle_imp0(void);
+/* FP64 adjoint of a TM run from a fresh grid: runs nsteps, returns
+ * J = sum_probes |DFT_freq(Ez)|^2 and dJ/deps_r over the design box (x
+ * fastest). Non-dispersive materials with mu_r = 1, no TFSF planes. */
+int oracle_adjoint_tm(oracle_grid* g, int nsteps, const int* plo, const int* phi, double freq, const int* dlo,
+                      const int* dhi, double* J, double* grad);
 
 #ifdef __cplusplus
 }

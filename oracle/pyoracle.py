@@ -73,6 +73,9 @@ def lib():
         L.oracle_dft_npoints.argtypes = [vp, ctypes.c_int]
         L.oracle_pml_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.oracle_imp0.restype = ctypes.c_double
+        L.oracle_add_source_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, dp, ctypes.c_int]
+        L.oracle_set_eps_map.argtypes = [vp, dp]
+        L.oracle_adjoint_tm.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.c_double, ip, ip, dp, dp]
         _lib = L
     return _lib
 
@@ -122,7 +125,15 @@ class OracleGrid:
         self._keep = []
         for s in p.sources:
             v = np.ascontiguousarray(s.values, dtype=np.float64)
-            assert L.oracle_add_source(self.h, s.comp, SOURCE_TARGETS[s.target], *s.pos, _dp(v), len(v)) == 0
+            if s.hi is None:
+                assert L.oracle_add_source(self.h, s.comp, SOURCE_TARGETS[s.target], *s.pos, _dp(v), len(v)) == 0
+            else:
+                assert L.oracle_add_source_box(self.h, s.comp, SOURCE_TARGETS[s.target], _ip(s.pos), _ip(s.hi),
+                                               _dp(v), len(v)) == 0
+        if p.eps_map is not None:
+            self._eps = np.ascontiguousarray(p.eps_map, dtype=np.float64)
+            assert self._eps.size == nx * ny * nz
+            assert L.oracle_set_eps_map(self.h, _dp(self._eps)) == 0
         if p.tfsf is not None:
             t = p.tfsf
             av = np.ascontiguousarray(t.aux_values, dtype=np.float64)
@@ -222,11 +233,21 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
             lines.append(f"matids {ip}")
         else:
             lines.append("matids none")
-        lines.append(f"nsrc {len(p.sources)}")
-        for q, s in enumerate(p.sources):
-            sp = os.path.join(td, f"src{q}.bin")
-            np.ascontiguousarray(s.values, dtype=np.float64).tofile(sp)
-            lines.append(f"{s.comp} {SOURCE_TARGETS[s.target]} {s.pos[0]} {s.pos[1]} {s.pos[2]} {sp}")
+        if p.eps_map is not None:
+            raise ValueError("the reference runner takes per-cell material ids, not a permittivity map")
+        # a box source is one SoftSource per cell, applied after the point sources
+        pts = [(s, s.pos) for s in p.sources if s.hi is None]
+        for s in p.sources:
+            if s.hi is not None:
+                pts += [(s, (i, j, k)) for k in range(s.pos[2], s.hi[2] + 1) for j in range(s.pos[1], s.hi[1] + 1)
+                        for i in range(s.pos[0], s.hi[0] + 1)]
+        lines.append(f"nsrc {len(pts)}")
+        files = {}
+        for q, (s, pos) in enumerate(pts):
+            if id(s) not in files:
+                files[id(s)] = os.path.join(td, f"src{len(files)}.bin")
+                np.ascontiguousarray(s.values, dtype=np.float64).tofile(files[id(s)])
+            lines.append(f"{s.comp} {SOURCE_TARGETS[s.target]} {pos[0]} {pos[1]} {pos[2]} {files[id(s)]}")
         if p.tfsf is not None:
             t = p.tfsf
             ap = os.path.join(td, "aux.bin")
@@ -249,3 +270,17 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
         if line.startswith("loop_seconds"):
             out["loop_seconds"] = float(line.split()[1])
     return out
+
+
+def adjoint_tm(p, steps: int, probe_lo, probe_hi, freq: float, design_lo, design_hi):
+    """FP64 CPU adjoint (oracle_adjoint_tm) of a TM Problem from t = 0:
+    returns (J, dJ/deps_r over the design box as [ny_d, nx_d])."""
+    g = OracleGrid(p)
+    nd = (design_hi[0] - design_lo[0] + 1) * (design_hi[1] - design_lo[1] + 1)
+    grad = np.zeros(nd)
+    J = ctypes.c_double()
+    rc = lib().oracle_adjoint_tm(g.h, steps, _ip(probe_lo), _ip(probe_hi), freq, _ip(design_lo), _ip(design_hi),
+                                 ctypes.byref(J), _dp(grad))
+    if rc != 0:
+        raise ValueError("oracle_adjoint_tm rejected the problem")
+    return J.value, grad.reshape(design_hi[1] - design_lo[1] + 1, design_hi[0] - design_lo[0] + 1)

@@ -8,7 +8,7 @@ import math
 import numpy as np
 
 from fdtd_b200.problem import (TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion, courant_dt,
-                               gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, tfsf_box_planes)
+                               gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, sinusoid, tfsf_box_planes)
 
 DX = 1e-6
 DT2 = courant_dt(DX, 0.99 / math.sqrt(2.0))
@@ -170,7 +170,74 @@ def td_h_sources() -> Problem:
     return p
 
 
+def tm_line_source() -> Problem:
+    """TM with a line source (one Sinusoid-driven soft source per cell of a
+    column, E target), a point source on a cell of that line (point sources
+    apply first), and a box of soft sources on Hy (H target)."""
+    nx, ny = 42, 38
+    p = Problem(TM, (nx, ny, 1), DX, DT2, name="tm_line_source")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    p.sources.append(Source(2, (10, 18, 0), 0.5 * gaussian_pulse(90, 20, 6), "E"))
+    p.sources.append(Source(2, (10, 1, 0), sinusoid(90, 0.05), "E", hi=(10, ny - 2, 0)))
+    p.sources.append(Source(1, (20, 15, 0), 1e-3 * gaussian_pulse(90, 30, 8), "H", hi=(22, 17, 0)))
+    p.dfts.append(DFTRegion(2, (30, 1, 0), (30, ny - 2, 0), [0.05]))
+    p.steps = 90
+    return p
+
+
+def td_box_sources() -> Problem:
+    """3D box sources on Ez (E target) through a Drude block, and on Hx (H
+    target)."""
+    nx, ny, nz = 14, 15, 16
+    p = Problem(THREED, (nx, ny, nz), DX, DT3, name="td_box_sources")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 3
+    dt = DT3
+    p.materials = [Material.vacuum(), Material.drude(1.5, 0.3 / dt, 0.01 / dt)]
+    ids = np.zeros((nz, ny, nx), np.uint8)
+    ids[6:11, 5:10, 4:9] = 1
+    p.ids = ids
+    p.sources.append(Source(2, (6, 4, 5), gaussian_pulse(40, 15, 5), "E", hi=(6, 9, 8)))
+    p.sources.append(Source(0, (8, 7, 9), 1e-3 * gaussian_pulse(40, 12, 5), "H", hi=(9, 8, 9)))
+    p.dfts.append(DFTRegion(2, (1, 1, 8), (nx - 2, ny - 2, 8), [0.03]))
+    p.steps = 40
+    return p
+
+
+def tm_adjoint_small(n: int = 40, steps: int = 260, design: int = 8, seed: int = 1):
+    """The adjoint workload at a size the CPU oracle runs in well under a
+    second: TM, 6-cell CPML, a central design box of random eps_r in [1, 12],
+    an Ez line source (Sinusoid at 0.05 cycles/step), 4 probe cells on the
+    right. Returns (Problem, AdjointSpec)."""
+    from fdtd_b200.problem import AdjointSpec
+    p = Problem(TM, (n, n, 1), DX, DT2, name=f"tm{n}_adjoint_small")
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    rng = np.random.default_rng(seed)
+    d0 = (n - design) // 2
+    eps = np.zeros((1, n, n))
+    eps[0, d0:d0 + design, d0:d0 + design] = rng.uniform(1.0, 12.0, size=(design, design))
+    p.eps_map = eps
+    p.sources.append(Source(2, (8, 1, 0), sinusoid(steps, 0.05), "E", hi=(8, n - 2, 0)))
+    pc, j0 = n - 9, n // 2 - 2
+    spec = AdjointSpec((pc, j0, 0), (pc, j0 + 3, 0), 0.05, (d0, d0, 0), (d0 + design - 1, d0 + design - 1, 0), 32)
+    p.steps = steps
+    return p, spec
+
+
+def objective_problem(p, spec):
+    """`p` with the objective's DFT region as its only DFT region."""
+    import copy
+    q = copy.deepcopy(p)
+    q.dfts = [DFTRegion(2, spec.probe_lo, spec.probe_hi, [spec.freq])]
+    return q
+
+
 # scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
-                       te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources]
+                       te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]

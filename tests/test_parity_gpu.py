@@ -183,8 +183,8 @@ def _with_eps_map(p, seed):
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-@pytest.mark.parametrize("make", [scenarios.tm_cpml_sources, scenarios.te_materials, scenarios.td_drude_lorentz],
-                         ids=lambda f: f.__name__)
+@pytest.mark.parametrize("make", [scenarios.tm_cpml_sources, scenarios.te_materials, scenarios.td_drude_lorentz,
+                                  scenarios.td_tfsf_box, scenarios.tm_line_source], ids=lambda f: f.__name__)
 def test_eps_map_matches_per_cell_materials(fdtd, oracle, make, prec):
     """fdtd_set_eps_map gives the same fields as one constant material per
     cell (bit-identical E and H for the FP64 plain method)."""
