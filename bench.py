@@ -43,6 +43,16 @@ METRIC = "Gcell-updates/s (FP32 fused; FP64 plain alongside)"
 ADJ_METRIC = "inverse-design gradient: Gcell-updates/s of forward + adjoint (FP32 fused)"
 
 
+# steps of each workload's configuration (the bench times --steps of them)
+P_STEPS = {"drude384": 1000, "lorentz768": 500, "tm256": 2000}
+
+# per interior cell, from profiles/flat_sweeps_tfsf_drude256.md (256^3 capture)
+MEASURED_TRAFFIC = {
+    "drude384": {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
+                 "source": "ncu capture at 256^3 scaled by interior cells (profiles/flat_sweeps_tfsf_drude256.md)"},
+}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -532,8 +542,18 @@ def main():
     e_ach = ab["e_sweep"] / (prof["e_sweep"] / 1e3) / 1e9
     h_ach = ab["h_sweep"] / (prof["h_sweep"] / 1e3) / 1e9
     step_ach = ab["step"] * args.steps / (ms / 1e3) / 1e9
+    state_gb = g.memory_bytes / 1e9
     g.close()
     del g
+    three_d = p.mode == 3
+    e_name = "flat_e_kernel (E sweep)" if three_d else "fused_e_kernel (E sweep)"
+    h_name = "flat_h_kernel (H sweep)" if three_d else "fused_h_kernel (H sweep)"
+    # DRAM traffic per launch: dram__bytes_read.sum + dram__bytes_write.sum of
+    # one ncu capture of the same kernel on the same physics at a smaller size,
+    # scaled by interior cells (traffic grows with the cells swept)
+    tr = MEASURED_TRAFFIC.get(args.workload)
+    traffic_e = tr["e"] * cells if tr else None
+    traffic_h = tr["h"] * cells if tr else None
 
     # FP64 plain on the same grid and GPU (the metric's comparison)
     f64 = None
@@ -589,14 +609,17 @@ def main():
             "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": p.name, "grid": list(p.shape), "interior_cells": cells, "cpml": 12,
-                       "steps_in_config": 1000, "l2": "state (~1.4 GB) larger than L2; no flush",
-                       "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
-            "roofline": {"bound": "hbm", "kernel": "fused_e_kernel (E sweep)", "achieved": e_ach, "peak": peak,
+            "config": {"workload": p.name, "grid": list(p.shape), "interior_cells": cells,
+                       "cpml": max(p.pml.values()) if p.pml else 0, "steps_in_config": P_STEPS.get(args.workload),
+                       "l2": f"state {state_gb:.2f} GB on the device; "
+                             + ("larger than L2, no flush" if state_gb > 0.126 else "fits L2"),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": e_name, "achieved": e_ach, "peak": peak,
                          "unit": "GB/s", "frac": e_ach / peak, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": ab["e_sweep"], "launch_ms": prof["e_sweep"], "traffic": None},
-            "roofline_h": {"kernel": "fused_h_kernel (H sweep)", "achieved": h_ach, "frac": h_ach / peak,
-                           "alg_bytes_per_launch": ab["h_sweep"], "launch_ms": prof["h_sweep"]},
+                         "alg_bytes_per_launch": ab["e_sweep"], "launch_ms": prof["e_sweep"], "traffic": traffic_e,
+                         "traffic_source": tr["source"] if tr else None},
+            "roofline_h": {"kernel": h_name, "achieved": h_ach, "frac": h_ach / peak,
+                           "alg_bytes_per_launch": ab["h_sweep"], "launch_ms": prof["h_sweep"], "traffic": traffic_h},
             "roofline_step": {"alg_bytes_per_cell_step": ab["per_cell_step"], "achieved": step_ach,
                               "frac": step_ach / peak},
             "kernel_ms": prof,

@@ -1783,6 +1783,11 @@ struct fdtd_adjoint {
   double* d_X = nullptr;
   double* d_grad = nullptr;
   double J = 0.0;
+  std::map<int, cudaGraphExec_t> graphs;  // one replayable segment per length
+  std::map<int, long long> graph_launches;
+  ~fdtd_adjoint() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  }
 };
 
 static int adj_alloc(fdtd_adjoint* a, void** p, size_t bytes) {
@@ -1817,6 +1822,23 @@ static int adj_recompute_step(fdtd_grid* g, const FusedArgs& fa, cudaStream_t s)
   g->launches += launch_fused_h(g->d.mode, fa, s);
   if (boxes) g->launches += launch_boxes(g, 1, 0, s);
   g->launches += launch_step_advance(g->ctrl, s);
+  return FDTD_OK;
+}
+
+// recompute `len` steps from the restored checkpoint, keeping d_t of the
+// design cells, then reverse them
+static int adj_enqueue_segment(fdtd_adjoint* a, const FusedArgs& fa, const AdjArgs& aa, int len, cudaStream_t s) {
+  fdtd_grid* g = a->g;
+  const int nd = aa.ndesign;
+  const float* hx = static_cast<const float*>(g->H[0]);
+  const float* hy = static_cast<const float*>(g->H[1]);
+  for (int k = 0; k < len; k++) {
+    g->launches += launch_adjoint_capture(aa, hx, hy, a->d_store + static_cast<size_t>(k) * nd, s);
+    int rc = adj_recompute_step(g, fa, s);
+    if (rc) return rc;
+  }
+  for (int k = len - 1; k >= 0; k--)
+    g->launches += launch_adjoint_step(aa, len - 1 - k, a->d_store + static_cast<size_t>(k) * nd, s);
   return FDTD_OK;
 }
 
@@ -1977,18 +1999,38 @@ int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad) {
   aa.freq = a->freq;
   aa.ndesign = nd;
   aa.grad = a->d_grad;
-  const float* hx = static_cast<const float*>(g->H[0]);
-  const float* hy = static_cast<const float*>(g->H[1]);
+  aa.ctrl = g->ctrl;
+  // every segment of one length is the same launch sequence (the kernels read
+  // the step from the device counter the checkpoint restores): one captured
+  // graph per length, replayed; without graphs the launches go out one by one
   for (int q = a->nckpt - 1; q >= 0 && !rc; q--) {
     const long long t0 = static_cast<long long>(q) * a->ckpt_every;
     const int len = static_cast<int>(std::min<long long>(a->ckpt_every, a->nsteps - t0));
     rc = adj_copy_state(a, a->d_ckpt + a->state_bytes * q, false, s);
-    for (int k = 0; k < len && !rc; k++) {
-      g->launches += launch_adjoint_capture(aa, hx, hy, a->d_store + static_cast<size_t>(k) * nd, s);
-      rc = adj_recompute_step(g, fa, s);
+    if (rc) break;
+    if (!g->use_graphs) {
+      rc = adj_enqueue_segment(a, fa, aa, len, s);
+      continue;
     }
-    for (int k = len - 1; k >= 0 && !rc; k--)
-      g->launches += launch_adjoint_step(aa, t0 + k + 1, a->d_store + static_cast<size_t>(k) * nd, s);
+    auto it = a->graphs.find(len);
+    if (it == a->graphs.end()) {
+      const long long before = g->launches;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      rc = adj_enqueue_segment(a, fa, aa, len, s);
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamEndCapture(s, &graph);
+      a->graph_launches[len] = g->launches - before;
+      g->launches = before;
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("adjoint capture: ") + cudaGetErrorString(e));
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("adjoint instantiate: ") + cudaGetErrorString(e));
+      it = a->graphs.emplace(len, exec).first;
+    }
+    CK(cudaGraphLaunch(it->second, s));
+    g->launches += a->graph_launches[len];
   }
   // the grid goes back to its state after the forward
   if (!rc) rc = adj_copy_state(a, a->d_final, false, s);

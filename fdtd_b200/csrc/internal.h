@@ -186,6 +186,7 @@ struct AdjArgs {
   int dlo[2], dhi[2];               // design box (inclusive)
   int ndesign;
   double* grad;                     // dJ/deps_r, design box order
+  const Control* ctrl;              // the grid's step counter
 };
 
 // kernel launchers (stream-ordered); each returns the number of launches
@@ -216,7 +217,7 @@ int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaS
 int launch_step_advance(Control* ctrl, cudaStream_t s);
 int launch_adjoint_inv_eps(const FusedArgs& fa, float* ie, cudaStream_t s);
 int launch_adjoint_capture(const AdjArgs& a, const float* hx, const float* hy, float* slot, cudaStream_t s);
-int launch_adjoint_step(const AdjArgs& a, long long n, const float* dslot, cudaStream_t s);
+int launch_adjoint_step(const AdjArgs& a, int back, const float* dslot, cudaStream_t s);
 int launch_box_source(int is_f32, void* field, const int* lo, const int* hi, int pitch, int ny, const double* vals,
                       int nvals, double scale, int shift, const Control* ctrl, cudaStream_t s);
 // control block of a batch's persistent kernel (grid barrier + error flag)

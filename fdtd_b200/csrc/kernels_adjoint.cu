@@ -92,10 +92,13 @@ __global__ void __launch_bounds__(256) adj_h_kernel(const AdjArgs a) {
   a.ryx[c] = ryx;
 }
 
-__global__ void __launch_bounds__(256) adj_e_kernel(const AdjArgs a, long long n, const float* __restrict__ dslot) {
+// `back` counts the steps between this one and the last of the recomputed
+// segment, whose end the step counter holds: n = t + 1 = ctrl->t - back
+__global__ void __launch_bounds__(256) adj_e_kernel(const AdjArgs a, int back, const float* __restrict__ dslot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (!interior(a, i, j)) return;
   const long long c = static_cast<long long>(j) * a.pitch + i;
+  const long long n = a.ctrl->t - back;
   // A2
   float v = a.rxy[c - a.pitch] - a.rxy[c] - a.ryx[c - 1] + a.ryx[c];
   if (i >= a.plo[0] && i <= a.phi[0] && j >= a.plo[1] && j <= a.phi[1]) {
@@ -146,11 +149,12 @@ int launch_adjoint_capture(const AdjArgs& a, const float* hx, const float* hy, f
   return 1;
 }
 
-// the reverse of step t = n - 1 (n is the DFT sample index of its E half)
-int launch_adjoint_step(const AdjArgs& a, long long n, const float* dslot, cudaStream_t s) {
+// the reverse of the step `back` steps before the one that ends at the
+// device step counter
+int launch_adjoint_step(const AdjArgs& a, int back, const float* dslot, cudaStream_t s) {
   dim3 block(32, 8), grid((a.nx + 31) / 32, (a.ny + 7) / 8);
   adj_h_kernel<<<grid, block, 0, s>>>(a);
-  adj_e_kernel<<<grid, block, 0, s>>>(a, n, dslot);
+  adj_e_kernel<<<grid, block, 0, s>>>(a, back, dslot);
   return 2;
 }
 

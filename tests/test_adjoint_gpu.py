@@ -44,6 +44,17 @@ def test_checkpoint_spacing_does_not_change_the_gradient(fdtd):
     assert np.array_equal(a, b)
 
 
+def test_graph_replayed_backward_equals_eager(fdtd):
+    p, spec = scenarios.tm_adjoint_small()
+    _, a, _, _ = _gpu_gradient(fdtd, p, spec)
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.use_graphs(False)
+    adj = fdtd.Adjoint(g, spec.probe_lo[:2], spec.probe_hi[:2], spec.freq, spec.design_lo[:2], spec.design_hi[:2],
+                       spec.ckpt_every)
+    adj.forward(p.steps)
+    assert np.array_equal(adj.backward(), a)
+
+
 def test_backward_leaves_the_post_forward_state(fdtd):
     p, spec = scenarios.tm_adjoint_small()
     g = fdtd.Grid.from_problem(p, "f32")
