@@ -48,8 +48,9 @@ P_STEPS = {"drude384": 1000, "lorentz768": 500, "tm256": 2000}
 
 # per interior cell, from profiles/flat_sweeps_tfsf_drude256.md (256^3 capture)
 MEASURED_TRAFFIC = {
-    "drude384": {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
-                 "source": "ncu capture at 256^3 scaled by interior cells (profiles/flat_sweeps_tfsf_drude256.md)"},
+    ("drude384", "flat"): {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
+                           "source": "ncu capture at 256^3 scaled by interior cells "
+                                     "(profiles/flat_sweeps_tfsf_drude256.md)"},
 }
 
 
@@ -65,6 +66,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
+    ap.add_argument("--sweep", default="auto", choices=["auto", "regs", "tma", "flat", "staged"],
+                    help="3D FP32 sweep kernels (fdtd_set_sweep_kernel)")
     return ap.parse_args()
 
 
@@ -509,6 +512,8 @@ def main():
         return
     p = make_problem(args.workload, args.steps + args.warmup, args.n)
     g = G.Grid.from_problem(p, "f32", device=local)
+    if args.sweep != "auto":
+        g.set_sweep_kernel(args.sweep)
     g.step(args.warmup, stream=stream.cuda_stream)
     torch.cuda.synchronize()
     launches0 = g.launch_count
@@ -546,12 +551,13 @@ def main():
     g.close()
     del g
     three_d = p.mode == 3
-    e_name = "flat_e_kernel (E sweep)" if three_d else "fused_e_kernel (E sweep)"
-    h_name = "flat_h_kernel (H sweep)" if three_d else "fused_h_kernel (H sweep)"
+    kind = {"auto": "staged"}.get(args.sweep, args.sweep)
+    e_name = f"{kind}_e_kernel (E sweep)" if three_d else "fused_e_kernel (E sweep)"
+    h_name = f"{kind}_h_kernel (H sweep)" if three_d else "fused_h_kernel (H sweep)"
     # DRAM traffic per launch: dram__bytes_read.sum + dram__bytes_write.sum of
     # one ncu capture of the same kernel on the same physics at a smaller size,
     # scaled by interior cells (traffic grows with the cells swept)
-    tr = MEASURED_TRAFFIC.get(args.workload)
+    tr = MEASURED_TRAFFIC.get((args.workload, kind))
     traffic_e = tr["e"] * cells if tr else None
     traffic_h = tr["h"] * cells if tr else None
 

@@ -29,6 +29,7 @@ SOURCES = {
     "kernels_fused.cu": [],
     "kernels_fused3d.cu": [],
     "kernels_fused3d_tma.cu": [],
+    "kernels_fused3d_async.cu": [],
     "kernels_tfsf.cu": [],
     "kernels_batch.cu": [],
     "kernels_common.cu": [],

@@ -176,8 +176,6 @@ struct fdtd_grid {
   bool dirty_dft = true;
   int sweep_kind = FDTD_SWEEP_AUTO;
   TmaState* tma = nullptr;
-  long long* d_plane_offs = nullptr;  // prefix sums of TFSF plane cell counts
-  long long plane_cells = 0;
   long long version = 0;        // bumped by every change a captured graph would bake in
   long long graph_version = -1;
   cudaGraphExec_t graph = nullptr;
@@ -932,14 +930,8 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
   PlaneH ph;
   ph.dev = p;
   g->planes.push_back(ph);
-  std::vector<long long> offs(1, 0);
-  for (auto& q : g->planes) {
-    long long n = 1;
-    for (int d = 0; d < 3; d++) n *= q.dev.hi[d] - q.dev.lo[d] + 1;
-    offs.push_back(offs.back() + n);
-  }
-  g->plane_cells = offs.back();
-  return upload_vec(g, reinterpret_cast<void**>(&g->d_plane_offs), offs.data(), offs.size() * sizeof(long long));
+  g->version++;
+  return FDTD_OK;
 }
 
 int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) {
@@ -958,6 +950,7 @@ int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const dou
     r.hi[d] = hi[d];
     r.npts *= hi[d] - lo[d] + 1;
   }
+  if (r.npts >= (1LL << 31)) return fail(FDTD_ERR_UNSUPPORTED, "a DFT region holds at most 2^31 - 1 points");
   CK(cudaSetDevice(g->d.device));
   r.freqs.assign(freqs, freqs + nf);
   int rc = upload_vec(g, reinterpret_cast<void**>(&r.d_freqs), freqs, nf * sizeof(double));
@@ -1023,36 +1016,41 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
   const bool use_tma = use3d && g->sweep_kind == FDTD_SWEEP_TMA && tma_prepare(fa, &g->tma);
   if (g->sweep_kind == FDTD_SWEEP_TMA && !use_tma)
     return fail(FDTD_ERR_UNSUPPORTED, "the TMA sweep is not available for this grid");
-  const bool use_flat = use3d && !use_tma && (g->sweep_kind == FDTD_SWEEP_FLAT || g->sweep_kind == FDTD_SWEEP_AUTO);
+  // AUTO takes the staged sweeps, the fastest measured on B200
+  const bool use_staged =
+      use3d && (g->sweep_kind == FDTD_SWEEP_STAGED || g->sweep_kind == FDTD_SWEEP_AUTO);
+  const bool use_flat = use3d && !use_tma && !use_staged && g->sweep_kind == FDTD_SWEEP_FLAT;
   const bool boxes = !g->boxes.empty();
   for (int q = 0; q < nsteps; q++) {
     if (prof) CK(cudaEventRecord(ev[0], s));
     if (boxes && g->f32) g->launches += launch_boxes(g, 0, -1, s);
     if (g->f32) {
-      g->launches += use_tma    ? launch_tma_e(fa, g->tma, s)
-                     : use_flat ? launch_flat_e(fa, s)
+      g->launches += use_tma      ? launch_tma_e(fa, g->tma, s)
+                     : use_staged ? launch_staged_e(fa, s)
+                     : use_flat   ? launch_flat_e(fa, s)
                      : use3d    ? launch_fused3d_e(fa, s)
                                 : launch_fused_e(mode, fa, s);
     }
     else g->launches += launch_plain_e(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[1], s));
-    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, g->d_plane_offs, g->plane_cells, s);
+    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, s);
     if (boxes) g->launches += launch_boxes(g, 0, 0, s);
-    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], fE, g->n[1],
+    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], g->dft_maxpts[0], fE, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[0], s);
     if (prof) CK(cudaEventRecord(ev[2], s));
     if (boxes && g->f32) g->launches += launch_boxes(g, 1, -1, s);
     if (g->f32) {
-      g->launches += use_tma    ? launch_tma_h(fa, g->tma, s)
-                     : use_flat ? launch_flat_h(fa, s)
+      g->launches += use_tma      ? launch_tma_h(fa, g->tma, s)
+                     : use_staged ? launch_staged_h(fa, s)
+                     : use_flat   ? launch_flat_h(fa, s)
                      : use3d    ? launch_fused3d_h(fa, s)
                                 : launch_fused_h(mode, fa, s);
     }
     else g->launches += launch_plain_h(mode, pa, s);
     if (prof) CK(cudaEventRecord(ev[3], s));
-    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, g->d_plane_offs, g->plane_cells, s);
+    if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, s);
     if (boxes) g->launches += launch_boxes(g, 1, 0, s);
-    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], fH, g->n[1],
+    g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], g->dft_maxpts[1], fH, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[1], s);
     if (prof) CK(cudaEventRecord(ev[4], s));
     g->launches += launch_step_advance(g->ctrl, s);
@@ -1154,7 +1152,7 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
 
 int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
-  if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_FLAT) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
+  if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_STAGED) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
   g->sweep_kind = kind;
   g->version++;
   return FDTD_OK;

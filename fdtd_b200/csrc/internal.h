@@ -202,13 +202,15 @@ int launch_tma_e(const FusedArgs& a, const TmaState* st, cudaStream_t s);
 int launch_tma_h(const FusedArgs& a, const TmaState* st, cudaStream_t s);
 int launch_flat_e(const FusedArgs& a, cudaStream_t s);
 int launch_flat_h(const FusedArgs& a, cudaStream_t s);
-int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, const long long* d_offs, long long total, cudaStream_t s);
+int launch_staged_e(const FusedArgs& a, cudaStream_t s);
+int launch_staged_h(const FusedArgs& a, cudaStream_t s);
+int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, cudaStream_t s);
 int launch_fused3d_e(const FusedArgs& a, cudaStream_t s);
 int launch_fused3d_h(const FusedArgs& a, cudaStream_t s);
 int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, double* By, double* Hy,
                           double* psiE, double* psiH, const double* coef, const double* vals, int nvals,
                           long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);
-int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts,
+int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
                       const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s);
 int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
                      long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s);

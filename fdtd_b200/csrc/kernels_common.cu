@@ -14,21 +14,22 @@ namespace fdtdb {
 // folds the pending samples into the FP64 accumulators in one pass, with the
 // twiddles of the chunk computed once per block in shared memory. This reads
 // and writes each 16-byte accumulator once per chunk instead of once per step.
+// One grid row (blockIdx.y) per region: the region is uniform over the
+// block, and point indices within a region fit 32 bits.
 template <typename R>
-__global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, int nreg,
-                                                         long long total, const R* const* __restrict__ fields, int ny,
-                                                         int pitch, const Control* __restrict__ ctrl, R* buf) {
-  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= total) return;
-  int r = 0;
-  while (r + 1 < nreg && regions[r + 1].pt_off <= p) r++;
-  const DftRegionDev& g = regions[r];
-  const long long q = p - g.pt_off;
-  const int i = g.lo[0] + static_cast<int>(q % g.ext[0]);
-  const int j = g.lo[1] + static_cast<int>((q / g.ext[0]) % g.ext[1]);
-  const int k = g.lo[2] + static_cast<int>(q / (static_cast<long long>(g.ext[0]) * g.ext[1]));
+__global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, long long total,
+                                                         const R* const* __restrict__ fields, int ny, int pitch,
+                                                         const Control* __restrict__ ctrl, R* buf) {
+  const DftRegionDev& g = regions[blockIdx.y];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.npts) return;
+  const int ex = g.ext[0], ey = g.ext[1];
+  const int r = q / ex;
+  const int i = g.lo[0] + (q - r * ex);
+  const int j = g.lo[1] + r % ey;
+  const int k = g.lo[2] + r / ey;
   const long long slot = ctrl->t - ctrl->dft_base;
-  buf[slot * total + p] = fields[g.comp][(static_cast<long long>(k) * ny + j) * pitch + i];
+  buf[slot * total + g.pt_off + q] = fields[g.comp][(static_cast<long long>(k) * ny + j) * pitch + i];
 }
 
 template <typename R>
@@ -78,18 +79,16 @@ __global__ void __launch_bounds__(256) dft_flush_kernel(int phase, const DftRegi
 
 __global__ void dft_rebase_kernel(Control* ctrl) { ctrl->dft_base = ctrl->t; }
 
-int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts,
+int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
                       const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s) {
   if (nreg == 0 || total_pts == 0) return 0;
-  const unsigned blocks = static_cast<unsigned>((total_pts + 255) / 256);
+  const dim3 grid(static_cast<unsigned>((max_pts + 255) / 256), nreg);
   if (precision == 0)
-    dft_gather_kernel<double><<<blocks, 256, 0, s>>>(regions, nreg, total_pts,
-                                                     reinterpret_cast<const double* const*>(fields), ny, pitch, ctrl,
-                                                     static_cast<double*>(buf));
+    dft_gather_kernel<double><<<grid, 256, 0, s>>>(regions, total_pts, reinterpret_cast<const double* const*>(fields),
+                                                   ny, pitch, ctrl, static_cast<double*>(buf));
   else
-    dft_gather_kernel<float><<<blocks, 256, 0, s>>>(regions, nreg, total_pts,
-                                                    reinterpret_cast<const float* const*>(fields), ny, pitch, ctrl,
-                                                    static_cast<float*>(buf));
+    dft_gather_kernel<float><<<grid, 256, 0, s>>>(regions, total_pts, reinterpret_cast<const float* const*>(fields),
+                                                  ny, pitch, ctrl, static_cast<float*>(buf));
   return 1;
 }
 

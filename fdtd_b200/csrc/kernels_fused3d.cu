@@ -130,6 +130,9 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_e_kernel(const __grid_c
   const long long c0 = k0 * sz + jl * sy + x4;
   float4 hx[NZ + 1], hy[NZ + 1], hz[NZ], hx_ym[NZ], hz_ym[NZ], ex[NZ], ey[NZ], ez[NZ];
   unsigned ids[NZ];
+  // lane 0 takes its x-1 neighbours from the previous group's last cell: load
+  // them with the rest, so the warp waits for one round trip, not two
+  float hy_xm_l0[NZ], hz_xm_l0[NZ];
   hx[0] = ld4(a.H[0] + c0 - sz);
   hy[0] = ld4(a.H[1] + c0 - sz);
 #pragma unroll
@@ -138,6 +141,12 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_e_kernel(const __grid_c
     const long long c = c0 + q * sz;
     const bool in = k <= a.nz - 2;
     const long long cc = in ? c : c0;  // planes past the grid read a valid plane and are not computed
+    hy_xm_l0[q] = 0.f;
+    hz_xm_l0[q] = 0.f;
+    if (lane == 0) {
+      hy_xm_l0[q] = a.H[1][cc - 1];
+      hz_xm_l0[q] = a.H[2][cc - 1];
+    }
     hx[q + 1] = ld4(a.H[0] + cc);
     hy[q + 1] = ld4(a.H[1] + cc);
     hz[q] = ld4(a.H[2] + cc);
@@ -155,9 +164,8 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_e_kernel(const __grid_c
     float hz_xm0 = __shfl_up_sync(kFull, hz[q].w, 1);
     if (k > a.nz - 2) break;
     if (lane == 0) {
-      const long long c = c0 + q * sz;
-      hy_xm0 = a.H[1][c - 1];
-      hz_xm0 = a.H[2][c - 1];
+      hy_xm0 = hy_xm_l0[q];
+      hz_xm0 = hz_xm_l0[q];
     }
     e_group_update<MAXP>(a, g, k, hx[q + 1], hy[q + 1], hz[q], hx_ym[q], hz_ym[q], hx[q], hy[q], hy_xm0, hz_xm0, ex[q],
                          ey[q], ez[q], ids[q]);
@@ -177,12 +185,21 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_h_kernel(const __grid_c
   const long long ctop = ktop * sz + jl * sy + x4;
   // index q = 0 is plane ktop, q = 1 plane ktop-1, ...; ex/ey[q] hold plane ktop+1-q
   float4 ex[NZ + 1], ey[NZ + 1], ez[NZ], ex_yp[NZ], ez_yp[NZ], hx[NZ], hy[NZ], hz[NZ];
+  // lane 31 takes its x+1 neighbours from the next group's first cell: load
+  // them with the rest (one round trip per warp)
+  float ey_xp_l31[NZ], ez_xp_l31[NZ];
   ex[0] = ld4(a.E[0] + ctop + sz);
   ey[0] = ld4(a.E[1] + ctop + sz);
 #pragma unroll
   for (int q = 0; q < NZ; q++) {
     const int k = ktop - q;
     const long long cc = k >= 1 ? ctop - q * sz : ctop;
+    ey_xp_l31[q] = 0.f;
+    ez_xp_l31[q] = 0.f;
+    if (lane == 31) {
+      ey_xp_l31[q] = a.E[1][cc + 4];
+      ez_xp_l31[q] = a.E[2][cc + 4];
+    }
     ex[q + 1] = ld4(a.E[0] + cc);
     ey[q + 1] = ld4(a.E[1] + cc);
     ez[q] = ld4(a.E[2] + cc);
@@ -199,9 +216,8 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_h_kernel(const __grid_c
     float ez_xp3 = __shfl_down_sync(kFull, ez[q].x, 1);
     if (k < 1) break;
     if (lane == 31) {
-      const long long c = ctop - q * sz;
-      ey_xp3 = a.E[1][c + 4];
-      ez_xp3 = a.E[2][c + 4];
+      ey_xp3 = ey_xp_l31[q];
+      ez_xp3 = ez_xp_l31[q];
     }
     h_group_update(a, g, k, ex[q + 1], ey[q + 1], ez[q], ex_yp[q], ez_yp[q], ex[q], ey[q], ey_xp3, ez_xp3, hx[q],
                    hy[q], hz[q]);
@@ -246,7 +262,7 @@ int launch_fused3d_h(const FusedArgs& a, cudaStream_t s) {
 template <int MAXP>
 static void flat_e_dispatch(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRows - 1) / kRows, a.nz - 2), block(32, kRows, 1);
-  flat_e_kernel<MAXP, 1, (MAXP >= 2 ? 6 : 8)><<<grid, block, 0, s>>>(a);
+  flat_e_kernel<MAXP, 1, (MAXP >= 2 ? 6 : 7)><<<grid, block, 0, s>>>(a);
 }
 
 int launch_flat_e(const FusedArgs& a, cudaStream_t s) {

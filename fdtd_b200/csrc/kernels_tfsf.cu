@@ -12,6 +12,8 @@
 // A cell on several planes (box edges) is handled by the thread of the first
 // plane that contains it, which applies every plane's correction in plane
 // order; the result is deterministic.
+#include <algorithm>
+
 #include "fused3d_common.cuh"
 
 namespace fdtdb {
@@ -51,24 +53,36 @@ __device__ double plane_corr(const FusedArgs& a, const PlaneDev& p, long long ro
 
 }  // namespace
 
+// One grid row (blockIdx.y) per plane; cell indices within a plane fit 32 bits.
 template <int MODE>
-__global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__ FusedArgs a, int ft,
-                                                         const long long* __restrict__ offs) {
-  const long long gid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (gid >= offs[a.nplanes]) return;
-  int q = 0;
-  while (gid >= offs[q + 1]) q++;
+__global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__ FusedArgs a, int ft) {
+  const int q = blockIdx.y;
   const PlaneDev& p = a.planes[q];
-  const long long r = gid - offs[q];
-  const int ex = p.hi[0] - p.lo[0] + 1, ey = p.hi[1] - p.lo[1] + 1;
-  const int i = p.lo[0] + static_cast<int>(r % ex);
-  const int j = p.lo[1] + static_cast<int>((r / ex) % ey);
-  const int k = p.lo[2] + static_cast<int>(r / (static_cast<long long>(ex) * ey));
+  const int ex = p.hi[0] - p.lo[0] + 1, ey = p.hi[1] - p.lo[1] + 1, ez = p.hi[2] - p.lo[2] + 1;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ex * ey * ez) return;
+  const int rr = r / ex;
+  const int i = p.lo[0] + (r - rr * ex);
+  const int j = p.lo[1] + rr % ey;
+  const int k = p.lo[2] + rr / ey;
   for (int q0 = 0; q0 < q; q0++)
     if (in_plane(a.planes[q0], i, j, k)) return;  // an earlier plane's thread owns this cell
   const long long t = a.ctrl->t;
   const long long row = t - a.ctrl->t0 + (ft == 0 ? 0 : 1);
   const long long c = (static_cast<long long>(k) * a.ny + j) * a.pitch + i;
+  // the cell's fields (and material id) are read before the corrections are
+  // formed, so that their latency overlaps the aux-table lookups
+  float f0[3] = {0.f, 0.f, 0.f};
+  for (int I = 0; I < 3; I++) {
+    const bool has = ft == 0 ? hasE(MODE, I) : hasH(MODE, I);
+    if (has) f0[I] = ft == 0 ? a.E[I][c] : a.H[I][c];
+  }
+  int mid = 0;
+  if (ft == 0) {
+    if (a.ids) mid = a.ids[c];
+    else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  }
+  const float iemap = (ft == 0 && a.inv_eps_map) ? a.inv_eps_map[c] : 0.f;
   double corr[3] = {0.0, 0.0, 0.0};
   for (int q1 = q; q1 < a.nplanes; q1++) {
     const PlaneDev& pp = a.planes[q1];
@@ -79,37 +93,37 @@ __global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__
     }
   }
   if (ft == 0) {
-    int mid = 0;
-    if (a.ids) mid = a.ids[c];
-    else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
     const MatF32& m = a.mats[mid];
     float ie = m.inv_eps;
-    if (a.inv_eps_map && m.npoles == 0) {
-      const float v = a.inv_eps_map[c];
-      if (v > 0.f) ie = v;
-    }
+    if (m.npoles == 0 && iemap > 0.f) ie = iemap;
     const double sc = a.dt / kEps0 * ie;
     for (int I = 0; I < 3; I++) {
       if (!hasE(MODE, I)) continue;
       const float dE = static_cast<float>(sc * corr[I]);
-      a.E[I][c] += dE;
+      a.E[I][c] = f0[I] + dE;
       const int np = m.npoles < 0 ? 1 : m.npoles;
       for (int pq = 0; pq < np && pq < 2; pq++) a.J[pq][I][c] += m.b[pq] * dE;
     }
   } else {
     const double sc = a.eta * a.dt / kMu0;
     for (int I = 0; I < 3; I++)
-      if (hasH(MODE, I)) a.H[I][c] -= static_cast<float>(sc * corr[I]);
+      if (hasH(MODE, I)) a.H[I][c] = f0[I] - static_cast<float>(sc * corr[I]);
   }
 }
 
-int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, const long long* d_offs, long long total, cudaStream_t s) {
-  if (a.nplanes == 0 || total == 0) return 0;
-  const unsigned blocks = static_cast<unsigned>((total + 255) / 256);
+int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, cudaStream_t s) {
+  if (a.nplanes == 0) return 0;
+  long long most = 0;
+  for (int q = 0; q < a.nplanes; q++) {
+    const PlaneDev& p = a.planes[q];
+    most = std::max(most, static_cast<long long>(p.hi[0] - p.lo[0] + 1) * (p.hi[1] - p.lo[1] + 1) *
+                              (p.hi[2] - p.lo[2] + 1));
+  }
+  const dim3 grid(static_cast<unsigned>((most + 255) / 256), a.nplanes);
   switch (mode) {
-    case kTE: tfsf_fused_kernel<kTE><<<blocks, 256, 0, s>>>(a, ft, d_offs); break;
-    case kTM: tfsf_fused_kernel<kTM><<<blocks, 256, 0, s>>>(a, ft, d_offs); break;
-    default: tfsf_fused_kernel<kThreeD><<<blocks, 256, 0, s>>>(a, ft, d_offs); break;
+    case kTE: tfsf_fused_kernel<kTE><<<grid, 256, 0, s>>>(a, ft); break;
+    case kTM: tfsf_fused_kernel<kTM><<<grid, 256, 0, s>>>(a, ft); break;
+    default: tfsf_fused_kernel<kThreeD><<<grid, 256, 0, s>>>(a, ft); break;
   }
   return 1;
 }

@@ -173,11 +173,13 @@ int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream);
  * Synchronises after every step; for measurement, not production. */
 int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
 /* Which kernels carry the 3D FP32 fused sweeps: FDTD_SWEEP_AUTO (the
- * default: currently the flat sweeps, the fastest measured on B200), FDTD_SWEEP_REGS (z-marching, register prefetch),
+ * default: currently the staged sweeps, the fastest measured on B200), FDTD_SWEEP_REGS (z-marching, register prefetch),
  * FDTD_SWEEP_TMA (z-marching, TMA pipeline into shared memory; or
- * FDTD_ERR_UNSUPPORTED) or FDTD_SWEEP_FLAT (one thread per 4-cell group and
- * plane). All compute the same update. */
-enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3 };
+ * FDTD_ERR_UNSUPPORTED), FDTD_SWEEP_FLAT (one thread per 4-cell group and
+ * plane) or FDTD_SWEEP_STAGED (flat, with every operand of a thread copied
+ * into shared memory by cp.async at thread start). All compute the same
+ * update. */
+enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3, FDTD_SWEEP_STAGED = 4 };
 int fdtd_set_sweep_kernel(fdtd_grid* g, int kind);
 /* Replay a captured CUDA graph per 64 steps inside fdtd_step (default 1), or
  * launch every kernel from the host (0). Results are identical. */

@@ -73,7 +73,7 @@ def test_fused_f32_matches_oracle(fdtd, oracle, make):
     _compare(p, g, o, E + H, FUSED_TOL)
 
 
-@pytest.mark.parametrize("sweep", ["regs", "tma", "flat"])
+@pytest.mark.parametrize("sweep", ["regs", "tma", "flat", "staged"])
 @pytest.mark.parametrize("make", [m for m in scenarios.ALL_SCENARIOS if m().mode == 3], ids=lambda f: f.__name__)
 def test_fused_3d_sweep_kernels(fdtd, oracle, make, sweep):
     """Every 3D FP32 sweep implementation (register prefetch, TMA pipeline,
