@@ -46,8 +46,11 @@ ADJ_METRIC = "inverse-design gradient: Gcell-updates/s of forward + adjoint (FP3
 # steps of each workload's configuration (the bench times --steps of them)
 P_STEPS = {"drude384": 1000, "lorentz768": 500, "tm256": 2000}
 
-# per interior cell, from profiles/flat_sweeps_tfsf_drude256.md (256^3 capture)
+# DRAM bytes per interior cell of one sweep launch, from ncu captures at 256^3 (profiles/)
 MEASURED_TRAFFIC = {
+    ("drude384", "staged"): {"e": 663.850496e6 / 16387064, "h": 632.577024e6 / 16387064,
+                             "source": "ncu capture at 256^3 scaled by interior cells "
+                                       "(profiles/staged_sweeps_tfsf_gather_drude256.md)"},
     ("drude384", "flat"): {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
                            "source": "ncu capture at 256^3 scaled by interior cells "
                                      "(profiles/flat_sweeps_tfsf_drude256.md)"},
