@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--sweep", default="auto", choices=["auto", "regs", "tma", "flat", "staged"],
                     help="3D FP32 sweep kernels (fdtd_set_sweep_kernel)")
+    ap.add_argument("--batch-mode", default="tune", choices=["tune", "persistent", "per_phase"],
+                    help="batch64: autotune, or force a launch mode (with --batch-rows)")
+    ap.add_argument("--batch-rows", type=int, default=4, choices=[1, 2, 4, 8])
     return ap.parse_args()
 
 
@@ -411,7 +414,10 @@ def run_batch(args, torch, world, rank, local, stream):
     probs = [allp[q] for q in shares[rank]]
     grids = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
     batch = G.Batch(grids)
-    batch.tune(4)
+    if args.batch_mode == "tune":
+        batch.tune(4)
+    else:
+        batch.configure(args.batch_mode == "persistent", args.batch_rows)
     batch.step(args.warmup, stream=stream.cuda_stream)
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -434,33 +440,41 @@ def run_batch(args, torch, world, rank, local, stream):
     for g in grids:
         g.close()
     # FP64 plain, one grid at a time (no batch kernel for the plain method)
-    n64 = max(3, min(50, args.steps))
-    g64 = [G.Grid.from_problem(p, "f64", device=local) for p in probs]
-    for g in g64:
-        g.step(2, stream=stream.cuda_stream)
-    torch.cuda.synchronize()
-    with torch.cuda.stream(stream):
-        start.record(stream)
+    f64 = None
+    if not args.no_f64:
+        n64 = max(3, min(50, args.steps))
+        g64 = [G.Grid.from_problem(p, "f64", device=local) for p in probs]
         for g in g64:
-            g.step(n64, stream=stream.cuda_stream)
-        end.record(stream)
-    torch.cuda.synchronize()
-    ms64 = start.elapsed_time(end)
-    for g in g64:
-        g.close()
+            g.step(2, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for g in g64:
+                g.step(n64, stream=stream.cuda_stream)
+            end.record(stream)
+        torch.cuda.synchronize()
+        ms64 = start.elapsed_time(end)
+        for g in g64:
+            g.close()
+        f64 = {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "note": "grids stepped one by one"}
     # end to end: create this rank's grids from host arrays, run, read every Hz back
-    barrier()
-    t0 = time.perf_counter()
-    ge = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
-    be = G.Batch(ge)
-    be.step(args.steps)
-    out = [g.get("Hz") for g in ge]
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
-    h2d = sum(p.ids.nbytes + sum(s.values.nbytes for s in p.sources) for p in probs)
-    d2h = sum(o.size * 8 for o in out)
-    be.close()
-    for g in ge:
-        g.close()
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        ge = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
+        be = G.Batch(ge)
+        be.step(args.steps)
+        out = [g.get("Hz") for g in ge]
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        h2d = sum(p.ids.nbytes + sum(s.values.nbytes for s in p.sources) for p in probs)
+        d2h = sum(o.size * 8 for o in out)
+        be.close()
+        for g in ge:
+            g.close()
+        e2e = {"value": total_cells * args.steps / t_e2e / 1e9, "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "wall_s": t_e2e,
+               "note": "grid creation from host arrays, the steps without tuning, D2H of every Hz; host clock"}
     cpu = cpu_batch_baseline(probs) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     return {
         "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -470,15 +484,18 @@ def run_batch(args, torch, world, rank, local, stream):
                    "interior_cells": total_cells, "seed": 0, "shard_imbalance": imbalance(
                        [problem_cost(p) for p in allp], shares),
                    "cpml": 10, "steps_in_config": 3000, "tile_rows": info["rows"], "ctas": info["blocks"],
+                   "launch": info["launch"],
                    "tune_ms_per_step": info["tune_ms_per_step"],
                    "l2": "state ~290 MB > L2; no flush", "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "batch_kernel (persistent, all steps)", "achieved": ach, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": ("batch_kernel (persistent, all steps)" if info["launch"] == "persistent"
+                                                else "batch_phase_kernel (E and H launches of one step)"),
+                     "achieved": ach, "peak": peak,
                      "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "alg_bytes_per_step": ab,
                      "traffic": None},
-        "fp64_plain": {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "note": "grids stepped one by one"},
-        "e2e": {"value": total_cells * args.steps / t_e2e / 1e9, "unit": "Gcell-updates/s",
-                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "wall_s": t_e2e},
-        "cpu_baseline": cpu, "gpu_launches": 2, "clocks": clk.summary(),
+        "fp64_plain": f64,
+        "e2e": e2e,
+        "cpu_baseline": cpu, "gpu_launches": 2 if info["launch"] == "persistent" else 2 * args.steps + 1,
+        "clocks": clk.summary(),
     }
 
 

@@ -1346,9 +1346,11 @@ struct fdtd_batch {
   BatchCtl* d_ctl = nullptr;
   unsigned* d_items = nullptr;
   int nitems = 0, rows = 0, blocks = 0;
+  int persistent = 1;  // 1: one cooperative kernel for all steps; 0: one kernel per half step
   cudaStream_t stream = nullptr;
   std::map<int, cudaGraphExec_t> graphs;  // keyed by steps per launch
-  std::vector<float> tune_ms;            // measured ms per step of rows 1, 2, 4, 8
+  // measured ms per step: persistent with rows 1, 2, 4, 8, then per-phase with rows 1, 2, 4, 8
+  std::vector<float> tune_ms;
 };
 
 namespace {
@@ -1401,9 +1403,19 @@ int batch_items(fdtd_batch* b, int rows) {
 }
 
 int batch_launch(fdtd_batch* b, int nsteps, cudaStream_t s) {
-  void* fn = batch_kernel_ptr(b->mode, b->maxp, b->rows);
   const FusedArgs* args = b->d_args;
   const unsigned* items = b->d_items;
+  if (!b->persistent) {
+    void* fe = batch_phase_ptr(b->mode, b->maxp, b->rows, 0);
+    void* fh = batch_phase_ptr(b->mode, b->maxp, b->rows, 1);
+    for (int q = 0; q < nsteps; q++) {
+      void* params[] = {&args, &items, &q};
+      CK(cudaLaunchKernel(fe, dim3(b->nitems), dim3(32, b->rows), params, 0, s));
+      CK(cudaLaunchKernel(fh, dim3(b->nitems), dim3(32, b->rows), params, 0, s));
+    }
+    return FDTD_OK;
+  }
+  void* fn = batch_kernel_ptr(b->mode, b->maxp, b->rows);
   int nitems = b->nitems;
   BatchCtl* ctl = b->d_ctl;
   void* params[] = {&args, &items, &nitems, &ctl, &nsteps};
@@ -1517,15 +1529,18 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) {
     return FDTD_OK;
   };
   int rc = copy(true);
+  // candidates: the persistent kernel and the per-phase launches, each with
+  // tiles of 1, 2, 4 or 8 rows
   const int cand[4] = {1, 2, 4, 8};
   float best = 1e30f;
-  int best_rows = 4;
-  b->tune_ms.assign(4, 0.f);
+  int best_rows = 4, best_persistent = 1;
+  b->tune_ms.assign(8, 0.f);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  for (int q = 0; q < 4 && !rc; q++) {
-    rc = batch_items(b, cand[q]);
+  for (int q = 0; q < 8 && !rc; q++) {
+    b->persistent = q < 4 ? 1 : 0;
+    rc = batch_items(b, cand[q % 4]);
     if (!rc) rc = batch_launch(b, 1, b->stream);  // warm-up
     if (!rc) rc = copy(false);
     CK(cudaEventRecord(e0, b->stream));
@@ -1537,7 +1552,8 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) {
     b->tune_ms[q] = ms / steps;
     if (ms < best) {
       best = ms;
-      best_rows = cand[q];
+      best_rows = cand[q % 4];
+      best_persistent = b->persistent;
     }
     if (!rc) rc = copy(false);
   }
@@ -1551,7 +1567,19 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) {
   if (err) return fail(FDTD_ERR_TIMEOUT, "a batch grid barrier expired while tuning");
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  b->persistent = best_persistent;
   return batch_items(b, best_rows);
+}
+
+int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch");
+  if (rows != 1 && rows != 2 && rows != 4 && rows != 8) return fail(FDTD_ERR_INVALID, "rows must be 1, 2, 4 or 8");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  b->persistent = persistent ? 1 : 0;
+  return batch_items(b, rows);
 }
 
 int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
@@ -1588,7 +1616,7 @@ int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
   CK(cudaGraphLaunch(it->second, s));
   for (auto* g : b->grids) {
     g->t += nsteps;
-    g->launches += 2;
+    g->launches += b->persistent ? 2 : 2LL * nsteps + 1;
   }
   // later work on any member grid's own stream follows the batch
   cudaEvent_t ev;
@@ -1599,13 +1627,14 @@ int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
   return FDTD_OK;
 }
 
-int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, float* tune_ms) {
+int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, int* persistent, float* tune_ms) {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch");
   if (rows) *rows = b->rows;
-  if (blocks) *blocks = b->blocks;
+  if (blocks) *blocks = b->persistent ? b->blocks : b->nitems;
   if (items) *items = b->nitems;
+  if (persistent) *persistent = b->persistent;
   if (tune_ms)
-    for (int q = 0; q < 4; q++) tune_ms[q] = q < static_cast<int>(b->tune_ms.size()) ? b->tune_ms[q] : 0.f;
+    for (int q = 0; q < 8; q++) tune_ms[q] = q < static_cast<int>(b->tune_ms.size()) ? b->tune_ms[q] : 0.f;
   return FDTD_OK;
 }
 

@@ -230,6 +230,7 @@ struct BatchCtl {
   int pad;
 };
 void* batch_kernel_ptr(int mode, int maxp, int rows);
+void* batch_phase_ptr(int mode, int maxp, int rows, int phase);
 int launch_batch_advance(Control* const* ctrls, int n, int nsteps, cudaStream_t s);
 
 }  // namespace fdtdb

@@ -64,13 +64,21 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
 #pragma unroll
   for (int e = 0; e < 4; e++) ok[e] = row_ok && x4 + e >= 1 && x4 + e <= a.nx - 2;
   const long long c = static_cast<long long>(jl) * a.pitch + x4;
+  // every operand of the group is requested before any is used: one memory
+  // round trip per group (the lane-0 x neighbour and the old E included)
+  const int Ie0 = MODE == kTE ? 0 : 2;
+  const float4 eo0 = ldcg4(a.E[Ie0] + c);
+  const float4 eo1 = MODE == kTE ? ldcg4(a.E[1] + c) : eo0;
+  const unsigned ids4 = a.ids ? __ldcg(reinterpret_cast<const unsigned*>(a.ids + c)) : 0u;
+  const int Ih = MODE == kTE ? 2 : 1;
+  const float hxm_l0 = lane == 0 ? __ldcg(a.H[Ih] + c - 1) : 0.f;
   const float4 fsx = ld4(a.prof[0][0].F + x4);
   const float fsy = a.prof[0][1].F[jl];
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 hz = ldcg4(a.H[2] + c), hz_ym = ldcg4(a.H[2] + c - a.pitch);
     float hz_xm0 = __shfl_up_sync(0xffffffffu, hz.w, 1);
-    if (lane == 0) hz_xm0 = __ldcg(a.H[2] + c - 1);
+    if (lane == 0) hz_xm0 = hxm_l0;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       set_el(rxy, e, el(hz, e) - el(hz_ym, e));
@@ -81,7 +89,7 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   } else {
     const float4 hx = ldcg4(a.H[0] + c), hy = ldcg4(a.H[1] + c), hx_ym = ldcg4(a.H[0] + c - a.pitch);
     float hy_xm0 = __shfl_up_sync(0xffffffffu, hy.w, 1);
-    if (lane == 0) hy_xm0 = __ldcg(a.H[1] + c - 1);
+    if (lane == 0) hy_xm0 = hxm_l0;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       set_el(rzx, e, el(hy, e) - (e == 0 ? hy_xm0 : el(hy, e - 1)));
@@ -151,7 +159,6 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   float4 ie;
   int mids[4] = {0, 0, 0, 0};
   bool disp = false;
-  const unsigned ids4 = a.ids ? __ldcg(reinterpret_cast<const unsigned*>(a.ids + c)) : 0u;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const int mid = uniform ? 0 : static_cast<int>((ids4 >> (8 * e)) & 0xff);
@@ -166,10 +173,10 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
       if (el(v, e) > 0.f && a.mats[mids[e]].npoles == 0) set_el(ie, e, el(v, e));
   }
   if (MODE == kTE) {
-    st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(ldcg4(a.E[0] + c), uX), dX, ie, ok, disp, uniform, m0, mids, aX));
-    st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(ldcg4(a.E[1] + c), uY), dY, ie, ok, disp, uniform, m0, mids, aY));
+    st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(eo0, uX), dX, ie, ok, disp, uniform, m0, mids, aX));
+    st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(eo1, uY), dY, ie, ok, disp, uniform, m0, mids, aY));
   } else {
-    st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(ldcg4(a.E[2] + c), uZ), dZ, ie, ok, disp, uniform, m0, mids, aZ));
+    st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(eo0, uZ), dZ, ie, ok, disp, uniform, m0, mids, aZ));
   }
 }
 
@@ -182,13 +189,19 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
 #pragma unroll
   for (int e = 0; e < 4; e++) ok[e] = row_ok && x4 + e >= 1 && x4 + e <= a.nx - 2;
   const long long c = static_cast<long long>(jl) * a.pitch + x4;
+  // operands first, as in e_group_2d: the old H and the lane-31 x neighbour too
+  const int Ih0 = MODE == kTE ? 2 : 0;
+  const float4 ho0 = ldcg4(a.H[Ih0] + c);
+  const float4 ho1 = MODE == kTE ? ho0 : ldcg4(a.H[1] + c);
+  const int Ie = MODE == kTE ? 1 : 2;
+  const float exp_l31 = lane == 31 ? __ldcg(a.E[Ie] + c + 4) : 0.f;
   const float4 fsx = ld4(a.prof[1][0].F + x4);
   const float fsy = a.prof[1][1].F[jl];
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 ex = ldcg4(a.E[0] + c), ey = ldcg4(a.E[1] + c), ex_yp = ldcg4(a.E[0] + c + a.pitch);
     float ey_xp3 = __shfl_down_sync(0xffffffffu, ey.x, 1);
-    if (lane == 31) ey_xp3 = __ldcg(a.E[1] + c + 4);
+    if (lane == 31) ey_xp3 = exp_l31;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       set_el(rzx, e, (e == 3 ? ey_xp3 : el(ey, e + 1)) - el(ey, e));
@@ -198,7 +211,7 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   } else {
     const float4 ez = ldcg4(a.E[2] + c), ez_yp = ldcg4(a.E[2] + c + a.pitch);
     float ez_xp3 = __shfl_down_sync(0xffffffffu, ez.x, 1);
-    if (lane == 31) ez_xp3 = __ldcg(a.E[2] + c + 4);
+    if (lane == 31) ez_xp3 = exp_l31;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       set_el(rxy, e, el(ez_yp, e) - el(ez, e));
@@ -262,18 +275,17 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
       a.src_last[q] = v;
     }
   }
-  auto upd = [&](int I, float4 d, float4 u, float4 ad) {
-    float4 h = ldcg4(a.H[I] + c);
+  auto upd = [&](int I, float4 h, float4 d, float4 u, float4 ad) {
 #pragma unroll
     for (int e = 0; e < 4; e++)
       if (ok[e]) set_el(h, e, el(h, e) - el(u, e) - el(d, e) + el(ad, e));
     st4(a.H[I] + c, h);
   };
   if (MODE == kTE) {
-    upd(2, dZ, uZ, aZ);
+    upd(2, ho0, dZ, uZ, aZ);
   } else {
-    upd(0, dX, uX, aX);
-    upd(1, dY, uY, aY);
+    upd(0, ho0, dX, uX, aX);
+    upd(1, ho1, dY, uY, aY);
   }
 }
 
@@ -309,9 +321,54 @@ __global__ void __launch_bounds__(32 * ROWS) batch_kernel(const FusedArgs* __res
   }
 }
 
+// The same update, one CTA per item and one launch per half step (the batch's
+// "phase" launch mode): the hardware block scheduler keeps many items in
+// flight per SM where the persistent kernel walks its items one after
+// another. `s` is the step offset from the counters, which a separate kernel
+// advances after the last step of a launch sequence.
+template <int MODE, int MAXP, int ROWS, int PHASE>
+__global__ void __launch_bounds__(32 * ROWS) batch_phase_kernel(const FusedArgs* __restrict__ grids,
+                                                                const unsigned* __restrict__ items, int s) {
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const unsigned w = items[blockIdx.x];
+  const FusedArgs& a = grids[w >> 24];
+  const long long t = grids[0].ctrl->t + s;
+  const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
+  const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
+  if (PHASE == 0) e_group_2d<MODE, MAXP>(a, x4, j, lane, t);
+  else h_group_2d<MODE>(a, x4, j, lane, t);
+}
+
 template <int MODE, int MAXP, int ROWS>
 static void* batch_fn() {
   return reinterpret_cast<void*>(batch_kernel<MODE, MAXP, ROWS>);
+}
+
+template <int MODE, int MAXP, int ROWS>
+static void* phase_fn(int phase) {
+  return phase == 0 ? reinterpret_cast<void*>(batch_phase_kernel<MODE, MAXP, ROWS, 0>)
+                    : reinterpret_cast<void*>(batch_phase_kernel<MODE, MAXP, ROWS, 1>);
+}
+
+void* batch_phase_ptr(int mode, int maxp, int rows, int phase) {
+#define FDTD_PHASE_ROWS(M, P)                    \
+  switch (rows) {                                \
+    case 1: return phase_fn<M, P, 1>(phase);     \
+    case 2: return phase_fn<M, P, 2>(phase);     \
+    case 4: return phase_fn<M, P, 4>(phase);     \
+    default: return phase_fn<M, P, 8>(phase);    \
+  }
+#define FDTD_PHASE_POLES(M)                      \
+  switch (maxp) {                                \
+    case 0: FDTD_PHASE_ROWS(M, 0)                \
+    case -1: FDTD_PHASE_ROWS(M, -1)              \
+    case 1: FDTD_PHASE_ROWS(M, 1)                \
+    default: FDTD_PHASE_ROWS(M, 2)               \
+  }
+  if (mode == kTE) FDTD_PHASE_POLES(kTE)
+  FDTD_PHASE_POLES(kTM)
+#undef FDTD_PHASE_POLES
+#undef FDTD_PHASE_ROWS
 }
 
 void* batch_kernel_ptr(int mode, int maxp, int rows) {

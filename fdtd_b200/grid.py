@@ -34,7 +34,8 @@ EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_ma
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
-           "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_info",
+           "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
+           "fdtd_batch_info",
            "fdtd_batch_error_flags", "fdtd_adjoint_create", "fdtd_adjoint_forward", "fdtd_adjoint_backward",
            "fdtd_adjoint_destroy", "fdtd_last_error_string"]
 
@@ -100,7 +101,8 @@ def load_library(path: str = LIB_PATH):
         "fdtd_batch_destroy": [vp],
         "fdtd_batch_tune": [vp, i],
         "fdtd_batch_step": [vp, i, vp],
-        "fdtd_batch_info": [vp, ip, ip, ip, ctypes.POINTER(ctypes.c_float)],
+        "fdtd_batch_info": [vp, ip, ip, ip, ip, ctypes.POINTER(ctypes.c_float)],
+        "fdtd_batch_configure": [vp, i, i],
         "fdtd_batch_error_flags": [vp, ip],
         "fdtd_adjoint_create": [vp, ip, ip, ctypes.c_double, ip, ip, i, ctypes.POINTER(vp)],
         "fdtd_adjoint_forward": [vp, i, dp],
@@ -347,12 +349,18 @@ class Batch:
         for g in self.grids:
             g._stepped_in_batch = True
 
+    def configure(self, persistent: bool, rows: int) -> None:
+        _check(load_library().fdtd_batch_configure(self.h, 1 if persistent else 0, int(rows)))
+
     def info(self) -> dict:
-        rows, blocks, items = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        ms = (ctypes.c_float * 4)()
-        _check(load_library().fdtd_batch_info(self.h, ctypes.byref(rows), ctypes.byref(blocks), ctypes.byref(items), ms))
+        rows, blocks, items, pers = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 8)()
+        _check(load_library().fdtd_batch_info(self.h, ctypes.byref(rows), ctypes.byref(blocks), ctypes.byref(items),
+                                              ctypes.byref(pers), ms))
+        keys = [f"persistent_rows{r}" for r in (1, 2, 4, 8)] + [f"per_phase_rows{r}" for r in (1, 2, 4, 8)]
         return {"rows": rows.value, "blocks": blocks.value, "items": items.value,
-                "tune_ms_per_step": {r: float(m) for r, m in zip((1, 2, 4, 8), ms)}}
+                "launch": "persistent" if pers.value else "per_phase",
+                "tune_ms_per_step": {k: float(m) for k, m in zip(keys, ms)}}
 
     def error_flags(self) -> int:
         v = ctypes.c_int()

@@ -206,21 +206,28 @@ int fdtd_launch_count(fdtd_grid* g, long long* count);
 int fdtd_memory_bytes(fdtd_grid* g, long long* bytes);
 
 /* ------------------------------------------------------------ batches
- * Many independent FP32 2D grids (TE or TM, same mode and device, no TFSF or
- * DFT, equal step counts), each set up with the calls above, advanced
- * together by one persistent kernel launch per fdtd_batch_step (replayed
- * from a CUDA graph). The grids stay usable on their own (download etc.). */
+ * Many independent FP32 2D grids (TE or TM, same mode and device, no TFSF,
+ * DFT or box sources, equal step counts), each set up with the calls above,
+ * advanced together by fdtd_batch_step as one replayed CUDA graph: either one
+ * persistent cooperative kernel for all the steps (grid barriers between the
+ * half steps), or one kernel per half step over the tiles of every grid; the
+ * tuner picks. The grids stay usable on their own (download etc.). */
 typedef struct fdtd_batch fdtd_batch;
 int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out);
 int fdtd_batch_destroy(fdtd_batch* b);
-/* Autotuner: times each tile height (1, 2, 4, 8 rows of 128 cells) for
- * `steps` steps on a snapshot of the grids' state, restores the state and
- * keeps the fastest. */
+/* Autotuner: times both launch modes with each tile height (1, 2, 4, 8 rows
+ * of 128 cells) for `steps` steps on a snapshot of the grids' state, restores
+ * the state and keeps the fastest. */
 int fdtd_batch_tune(fdtd_batch* b, int steps);
+/* Choose the launch mode (1: persistent, 0: one kernel per half step) and
+ * the tile height (1, 2, 4 or 8) without tuning. */
+int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows);
 int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream);
-/* Tile height in use, CTAs of the persistent kernel, work items, and the
- * tuner's ms per step for tile heights 1, 2, 4, 8 (0 if not tuned). */
-int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, float* tune_ms);
+/* Tile height in use, CTAs per launch, work items, the launch mode (1:
+ * persistent, 0: per half step), and the tuner's ms per step (tune_ms[8]:
+ * persistent with tile heights 1, 2, 4, 8, then per half step with 1, 2, 4,
+ * 8; 0 if not tuned). Any output pointer may be NULL. */
+int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, int* persistent, float* tune_ms);
 /* Bit 0: a bounded grid-barrier wait expired and the kernel gave up. */
 int fdtd_batch_error_flags(fdtd_batch* b, int* flags);
 

@@ -1,5 +1,5 @@
-"""Batched 2D grids (fdtd_batch_*): one persistent launch advances many
-independent grids of uneven sizes; each must match the oracle as if stepped
+"""Batched 2D grids (fdtd_batch_*): one graph launch (a persistent kernel, or
+one kernel per half step) advances many independent grids of uneven sizes; each must match the oracle as if stepped
 alone, tuning must leave the state untouched, and the bounded grid barrier
 must never report an expiry in a normal run."""
 import numpy as np
@@ -73,6 +73,30 @@ def test_batch_tuning_preserves_state_and_results(fdtd):
         out.append([g.get("Hz") for g in grids])
     for a, c in zip(out[0], out[1]):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("make", [small_te_batch, small_tm_batch], ids=["te", "tm"])
+def test_batch_launch_modes_and_tiles_agree(fdtd, make):
+    """The persistent kernel and the per-half-step launches, with every tile
+    height, run the same update: bit-identical fields."""
+    probs = make()
+    ref = None
+    for persistent in (True, False):
+        for rows in (1, 2, 4, 8):
+            grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+            b = fdtd.Batch(grids)
+            b.configure(persistent, rows)
+            b.step(probs[0].steps)
+            assert b.error_flags() == 0
+            assert b.info()["launch"] == ("persistent" if persistent else "per_phase")
+            E, H, _, _ = mode_fields(probs[0].mode)
+            out = [g.get(n) for g in grids for n in E + H]
+            if ref is None:
+                ref = out
+            else:
+                for a, c in zip(ref, out):
+                    assert np.array_equal(a, c), (persistent, rows)
+            b.close()
 
 
 def test_batch_rejects_unsupported_grids(fdtd):
