@@ -122,7 +122,7 @@ template <int MAXP>
 __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCtx& g, int k, float4 hx, float4 hy,
                                                float4 hz, float4 hx_ym, float4 hz_ym, float4 hx_km, float4 hy_km,
                                                float hy_xm0, float hz_xm0, float4 exo, float4 eyo, float4 ezo,
-                                               unsigned ids4) {
+                                               unsigned ids4, const float* staged_px = nullptr) {
   if (!g.row_ok) return;
   const int j = g.j, x4 = g.x4;
   const long long c = (static_cast<long long>(k) * a.ny + j) * a.pitch + x4;
@@ -184,7 +184,10 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
       if (sx < 0) continue;
       const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + sx;
       const float B = a.prof[0][0].B[i], Cs = a.prof[0][0].C[i], G = a.prof[0][0].G[i];
-      const float py = a.psi[0][1][0][pi], pz = a.psi[0][2][0][pi];
+      // staged_px: the x-slab integrators of the group already copied to
+      // shared memory ([component y|z][cell])
+      const float py = staged_px ? staged_px[e] : a.psi[0][1][0][pi];
+      const float pz = staged_px ? staged_px[4 + e] : a.psi[0][2][0][pi];
       set_el(dY, e, el(dY, e) + py * G);
       set_el(dZ, e, el(dZ, e) + pz * G);
       a.psi[0][1][0][pi] = B * py + Cs * el(ryx, e);
@@ -268,7 +271,8 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
 // y+1, z+1 and the x+1 neighbour of the group's last cell) and the old H.
 __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCtx& g, int k, float4 ex, float4 ey,
                                                float4 ez, float4 ex_yp, float4 ez_yp, float4 ex_kp, float4 ey_kp,
-                                               float ey_xp3, float ez_xp3, float4 hx, float4 hy, float4 hz) {
+                                               float ey_xp3, float ez_xp3, float4 hx, float4 hy, float4 hz,
+                                               const float* staged_px = nullptr) {
   if (!g.row_ok) return;
   const int j = g.j, x4 = g.x4;
   const long long c = (static_cast<long long>(k) * a.ny + j) * a.pitch + x4;
@@ -329,7 +333,8 @@ __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCt
       if (sx < 0) continue;
       const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + sx;
       const float B = a.prof[1][0].B[i], Cs = a.prof[1][0].C[i], G = a.prof[1][0].G[i];
-      const float py = a.psi[1][1][0][pi], pz = a.psi[1][2][0][pi];
+      const float py = staged_px ? staged_px[e] : a.psi[1][1][0][pi];
+      const float pz = staged_px ? staged_px[4 + e] : a.psi[1][2][0][pi];
       set_el(dY, e, el(dY, e) + py * G);
       set_el(dZ, e, el(dZ, e) + pz * G);
       a.psi[1][1][0][pi] = B * py + Cs * el(ryx, e);

@@ -16,8 +16,8 @@ using namespace f3d;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kRowsA = 4;
 constexpr int kThreads = 32 * kRowsA;
-constexpr int kSlotsE = 10;  // hx_km, hy_km, hx, hy, hz, hx_ym, hz_ym, ex, ey, ez
-constexpr int kSlotsH = 10;  // ex_kp, ey_kp, ex, ey, ez, ex_yp, ez_yp, hx, hy, hz
+constexpr int kSlotsE = 12;  // hx_km, hy_km, hx, hy, hz, hx_ym, hz_ym, ex, ey, ez, x-slab psi (2)
+constexpr int kSlotsH = 12;  // ex_kp, ey_kp, ex, ey, ez, ex_yp, ez_yp, hx, hy, hz, x-slab psi (2)
 
 __device__ __forceinline__ void cp_async16(float4* dst, const float* src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -30,6 +30,20 @@ __device__ __forceinline__ void cp_async4(unsigned* dst, const void* src) {
 }
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// the x-slab CPML integrators of a group (two components) into slots
+// px[0..3], px[4..7]; only cells inside the slab are copied
+__device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx& g, int ft, int k, float* px) {
+  if (!g.pml_x) return;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int sx = g.ok[e] ? slab_index(a.slab[0], g.x4 + e) : -1;
+    if (sx < 0) continue;
+    const long long pi = (static_cast<long long>(k) * a.ny + g.j) * a.slab[0].W + sx;
+    cp_async4(reinterpret_cast<unsigned*>(px + e), a.psi[ft][1][0] + pi);
+    cp_async4(reinterpret_cast<unsigned*>(px + 4 + e), a.psi[ft][2][0] + pi);
+  }
+}
 
 }  // namespace
 
@@ -62,6 +76,9 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
     hz_xm0 = a.H[2][c - 1];
   }
   const GroupCtx g = make_ctx(a, 0, x4, j, lane, k, k + 1);
+  // slots 10 and 11 hold this thread's 8 x-slab floats
+  float* px = reinterpret_cast<float*>(sm + 10 * kThreads) + 8 * tid;
+  if (g.row_ok) stage_x_slab(a, g, 0, k, px);
   cp_async_wait_all();
   const float4 hy = s[3 * kThreads], hz = s[4 * kThreads];
   const float hy_sh = __shfl_up_sync(kFull, hy.w, 1);
@@ -71,7 +88,7 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
     hz_xm0 = hz_sh;
   }
   e_group_update<MAXP>(a, g, k, s[2 * kThreads], hy, hz, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads],
-                       hy_xm0, hz_xm0, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], a.ids ? *sid : 0u);
+                       hy_xm0, hz_xm0, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], a.ids ? *sid : 0u, px);
 }
 
 template <int MINB>
@@ -102,6 +119,8 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
     ez_xp3 = a.E[2][c + 4];
   }
   const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
+  float* px = reinterpret_cast<float*>(sm + 10 * kThreads) + 8 * tid;
+  if (g.row_ok) stage_x_slab(a, g, 1, k, px);
   cp_async_wait_all();
   const float4 ey = s[3 * kThreads], ez = s[4 * kThreads];
   const float ey_sh = __shfl_down_sync(kFull, ey.x, 1);
@@ -111,7 +130,7 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
     ez_xp3 = ez_sh;
   }
   h_group_update(a, g, k, s[2 * kThreads], ey, ez, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads], ey_xp3,
-                 ez_xp3, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads]);
+                 ez_xp3, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], px);
 }
 
 template <int MAXP>
