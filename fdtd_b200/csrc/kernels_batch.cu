@@ -74,6 +74,20 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const float hxm_l0 = lane == 0 ? __ldcg(a.H[Ih] + c - 1) : 0.f;
   const float4 fsx = ld4(a.prof[0][0].F + x4);
   const float fsy = a.prof[0][1].F[jl];
+  // CPML integrators of the group, requested with the fields
+  const int Ipy = MODE == kTE ? 0 : 2, Ipx = MODE == kTE ? 1 : 2;
+  const int sj = (row_ok && a.pml_axis[1]) ? slab_index(a.slab[1], j) : -1;
+  const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
+  float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sj >= 0) psy = ldcg4(a.psi[0][Ipy][1] + piy);
+  const bool xs = row_ok && a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
+  int sxe[4];
+  float psx[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    sxe[e] = (xs && ok[e]) ? slab_index(a.slab[0], x4 + e) : -1;
+    if (sxe[e] >= 0) psx[e] = __ldcg(a.psi[0][Ipx][0] + static_cast<long long>(j) * a.slab[0].W + sxe[e]);
+  }
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 hz = ldcg4(a.H[2] + c), hz_ym = ldcg4(a.H[2] + c - a.pitch);
@@ -99,39 +113,31 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   }
   if (!row_ok) return;
   // CPML: y slab rows share the field layout; x slab cells are compact
-  if (a.pml_axis[1]) {
-    const int sj = slab_index(a.slab[1], j);
-    if (sj >= 0) {
-      const long long pi = static_cast<long long>(sj) * a.pitch + x4;
-      const float B = a.prof[0][1].B[j], Cs = a.prof[0][1].C[j], G = a.prof[0][1].G[j];
-      const int I = MODE == kTE ? 0 : 2;
-      float4 ps = ldcg4(a.psi[0][I][1] + pi);
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        if (!ok[e]) continue;
-        const float raw = MODE == kTE ? el(rxy, e) : el(rzy, e);
-        if (MODE == kTE) set_el(dX, e, el(dX, e) + el(ps, e) * G);
-        else set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
-        set_el(ps, e, B * el(ps, e) + Cs * raw);
-      }
-      st4(a.psi[0][I][1] + pi, ps);
-    }
-  }
-  if (a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3)) {
+  if (sj >= 0) {
+    const float B = a.prof[0][1].B[j], Cs = a.prof[0][1].C[j], G = a.prof[0][1].G[j];
+    float4 ps = psy;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int i = x4 + e;
       if (!ok[e]) continue;
-      const int sx = slab_index(a.slab[0], i);
-      if (sx < 0) continue;
-      const long long pi = static_cast<long long>(j) * a.slab[0].W + sx;
+      const float raw = MODE == kTE ? el(rxy, e) : el(rzy, e);
+      if (MODE == kTE) set_el(dX, e, el(dX, e) + el(ps, e) * G);
+      else set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
+      set_el(ps, e, B * el(ps, e) + Cs * raw);
+    }
+    st4(a.psi[0][Ipy][1] + piy, ps);
+  }
+  if (xs) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      if (sxe[e] < 0) continue;
+      const int i = x4 + e;
+      const long long pi = static_cast<long long>(j) * a.slab[0].W + sxe[e];
       const float B = a.prof[0][0].B[i], Cs = a.prof[0][0].C[i], G = a.prof[0][0].G[i];
-      const int I = MODE == kTE ? 1 : 2;
-      const float ps = __ldcg(a.psi[0][I][0] + pi);
+      const float ps = psx[e];
       const float raw = MODE == kTE ? el(ryx, e) : el(rzx, e);
       if (MODE == kTE) set_el(dY, e, el(dY, e) + ps * G);
       else set_el(dZ, e, el(dZ, e) + ps * G);
-      a.psi[0][I][0][pi] = B * ps + Cs * raw;
+      a.psi[0][Ipx][0][pi] = B * ps + Cs * raw;
     }
   }
   // sources and material update (shared with the 3D sweeps)
@@ -197,6 +203,19 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const float exp_l31 = lane == 31 ? __ldcg(a.E[Ie] + c + 4) : 0.f;
   const float4 fsx = ld4(a.prof[1][0].F + x4);
   const float fsy = a.prof[1][1].F[jl];
+  const int Ipy = MODE == kTE ? 2 : 0, Ipx = MODE == kTE ? 2 : 1;
+  const int sj = (row_ok && a.pml_axis[1]) ? slab_index(a.slab[1], j) : -1;
+  const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
+  float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sj >= 0) psy = ldcg4(a.psi[1][Ipy][1] + piy);
+  const bool xs = row_ok && a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
+  int sxe[4];
+  float psx[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    sxe[e] = (xs && ok[e]) ? slab_index(a.slab[0], x4 + e) : -1;
+    if (sxe[e] >= 0) psx[e] = __ldcg(a.psi[1][Ipx][0] + static_cast<long long>(j) * a.slab[0].W + sxe[e]);
+  }
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 ex = ldcg4(a.E[0] + c), ey = ldcg4(a.E[1] + c), ex_yp = ldcg4(a.E[0] + c + a.pitch);
@@ -221,39 +240,31 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
     }
   }
   if (!row_ok) return;
-  if (a.pml_axis[1]) {
-    const int sj = slab_index(a.slab[1], j);
-    if (sj >= 0) {
-      const long long pi = static_cast<long long>(sj) * a.pitch + x4;
-      const float B = a.prof[1][1].B[j], Cs = a.prof[1][1].C[j], G = a.prof[1][1].G[j];
-      const int I = MODE == kTE ? 2 : 0;
-      float4 ps = ldcg4(a.psi[1][I][1] + pi);
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        if (!ok[e]) continue;
-        const float raw = MODE == kTE ? el(rzy, e) : el(rxy, e);
-        if (MODE == kTE) set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
-        else set_el(dX, e, el(dX, e) + el(ps, e) * G);
-        set_el(ps, e, B * el(ps, e) + Cs * raw);
-      }
-      st4(a.psi[1][I][1] + pi, ps);
-    }
-  }
-  if (a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3)) {
+  if (sj >= 0) {
+    const float B = a.prof[1][1].B[j], Cs = a.prof[1][1].C[j], G = a.prof[1][1].G[j];
+    float4 ps = psy;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int i = x4 + e;
       if (!ok[e]) continue;
-      const int sx = slab_index(a.slab[0], i);
-      if (sx < 0) continue;
-      const long long pi = static_cast<long long>(j) * a.slab[0].W + sx;
+      const float raw = MODE == kTE ? el(rzy, e) : el(rxy, e);
+      if (MODE == kTE) set_el(dZ, e, el(dZ, e) + el(ps, e) * G);
+      else set_el(dX, e, el(dX, e) + el(ps, e) * G);
+      set_el(ps, e, B * el(ps, e) + Cs * raw);
+    }
+    st4(a.psi[1][Ipy][1] + piy, ps);
+  }
+  if (xs) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      if (sxe[e] < 0) continue;
+      const int i = x4 + e;
+      const long long pi = static_cast<long long>(j) * a.slab[0].W + sxe[e];
       const float B = a.prof[1][0].B[i], Cs = a.prof[1][0].C[i], G = a.prof[1][0].G[i];
-      const int I = MODE == kTE ? 2 : 1;
-      const float ps = __ldcg(a.psi[1][I][0] + pi);
+      const float ps = psx[e];
       const float raw = MODE == kTE ? el(rzx, e) : el(ryx, e);
       if (MODE == kTE) set_el(dZ, e, el(dZ, e) + ps * G);
       else set_el(dY, e, el(dY, e) + ps * G);
-      a.psi[1][I][0][pi] = B * ps + Cs * raw;
+      a.psi[1][Ipx][0][pi] = B * ps + Cs * raw;
     }
   }
   float4 uX = make_float4(0.f, 0.f, 0.f, 0.f), uY = uX, uZ = uX, aX = uX, aY = uX, aZ = uX;
