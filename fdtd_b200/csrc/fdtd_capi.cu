@@ -174,6 +174,7 @@ struct fdtd_grid {
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
   bool dirty_dft = true;
+  int next_half = 0;  // fdtd_step_half: the phase expected next
   int sweep_kind = FDTD_SWEEP_AUTO;
   TmaState* tma = nullptr;
   long long version = 0;        // bumped by every change a captured graph would bake in
@@ -974,6 +975,7 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   if (!g || !out || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
     return fail(FDTD_ERR_INVALID, "bad DFT handle");
   CK(cudaSetDevice(g->d.device));
+  if (g->dft_pending > 0) g->launches += flush_dft(g, g->stream);  // samples left by fdtd_step_half
   const DftH& r = g->dfts[handle];
   const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
   CK(cudaStreamSynchronize(g->stream));
@@ -1073,6 +1075,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(g->d.device));
@@ -1155,6 +1158,89 @@ int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) {
   if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_STAGED) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
   g->sweep_kind = kind;
   g->version++;
+  return FDTD_OK;
+}
+
+// One half step, for callers that exchange data between the halves (the
+// ghost planes of a z-slab decomposition): the launches of one step of
+// enqueue_steps, split after the E-phase DFT gather; phase 0 also advances
+// the TFSF aux grids by one step. Launched eagerly, never from a graph.
+int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (phase != 0 && phase != 1) return fail(FDTD_ERR_INVALID, "phase must be 0 (E) or 1 (H)");
+  if (phase != g->next_half) return fail(FDTD_ERR_INVALID, "half steps alternate, the E half first");
+  CK(cudaSetDevice(g->d.device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  if (s != g->stream) CK(cudaStreamSynchronize(g->stream));
+  if (g->dirty_dft) {
+    int rc = rebuild_dft(g);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(g->stream));
+  }
+  const int mode = g->d.mode;
+  const bool boxes = !g->boxes.empty();
+  if (phase == 0) {
+    for (auto& a : g->auxes) {
+      if (a.cap < 2) {
+        if (a.d_tab) dfree(g, a.d_tab);
+        a.d_tab = nullptr;
+        int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(2) * a.L * sizeof(double));
+        if (rc) return rc;
+        a.cap = 2;
+        CK(cudaStreamSynchronize(g->stream));
+      }
+      double* st = a.d_state;
+      const int L = a.L;
+      g->launches += launch_aux_precompute(L, g->d.dt, g->d.dx, st, st + L, st + 2 * L, st + 3 * L, st + 4 * L,
+                                           st + 5 * L, a.d_coef, a.d_vals, static_cast<int>(a.vals.size()), g->t, 1,
+                                           a.d_tab, a.d_tab + a.cap * L, s);
+    }
+    if (!g->auxes.empty()) g->launches += launch_chunk_start(g->ctrl, s);
+  }
+  FusedArgs fa;
+  PlainArgs pa;
+  if (g->f32) fa = fused_args(g);
+  else pa = plain_args(g);
+  const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
+  const void* const* fields = reinterpret_cast<const void* const*>(g->d_fieldptrs) + (phase == 0 ? 0 : 3);
+  if (boxes && g->f32) g->launches += launch_boxes(g, phase, -1, s);
+  if (g->f32) {
+    if (phase == 0) g->launches += use3d ? launch_staged_e(fa, s) : launch_fused_e(mode, fa, s);
+    else g->launches += use3d ? launch_staged_h(fa, s) : launch_fused_h(mode, fa, s);
+    g->launches += launch_tfsf_fused(mode, fa, phase, s);
+  } else {
+    g->launches += phase == 0 ? launch_plain_e(mode, pa, s) : launch_plain_h(mode, pa, s);
+  }
+  if (boxes) g->launches += launch_boxes(g, phase, 0, s);
+  g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[phase], g->ndft[phase], g->dft_pts[phase],
+                                   g->dft_maxpts[phase], fields, g->n[1], static_cast<int>(rowlen(g)), g->ctrl,
+                                   g->d_dft_buf[phase], s);
+  if (phase == 1) {
+    g->launches += launch_step_advance(g->ctrl, s);
+    if (!g->dfts.empty() && ++g->dft_pending == kDftChunk) g->launches += flush_dft(g, s);
+    g->t += 1;
+  }
+  CK(cudaGetLastError());
+  g->next_half = 1 - phase;
+  return FDTD_OK;
+}
+
+// one z plane of a stored E or H component to or from a compact device
+// buffer (nx * ny values of the grid's precision, x fastest; H of the FP32
+// method is the stored eta * H)
+int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream) {
+  if (!g || !dev_buf) return fail(FDTD_ERR_INVALID, "null argument");
+  if (k < 0 || k >= g->n[2]) return fail(FDTD_ERR_INVALID, "plane index out of range");
+  void* f = nullptr;
+  if (which >= FDTD_EX && which <= FDTD_EZ) f = g->E[which - FDTD_EX];
+  else if (which >= FDTD_HX && which <= FDTD_HZ) f = g->H[which - FDTD_HX];
+  if (!f) return fail(FDTD_ERR_INVALID, "only the stored E and H components of the mode are copied");
+  CK(cudaSetDevice(g->d.device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  const size_t es = elem(g), row = static_cast<size_t>(rowlen(g)) * es, w = static_cast<size_t>(g->n[0]) * es;
+  char* plane = static_cast<char*>(f) + static_cast<size_t>(k) * g->n[1] * row;
+  if (to_grid) CK(cudaMemcpy2DAsync(plane, row, dev_buf, w, w, g->n[1], cudaMemcpyDeviceToDevice, s));
+  else CK(cudaMemcpy2DAsync(dev_buf, w, plane, row, w, g->n[1], cudaMemcpyDeviceToDevice, s));
   return FDTD_OK;
 }
 

@@ -217,6 +217,7 @@ int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int 
 int launch_dft_rebase(Control* ctrl, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
+int launch_chunk_start(Control* ctrl, cudaStream_t s);
 int launch_adjoint_inv_eps(const FusedArgs& fa, float* ie, cudaStream_t s);
 int launch_adjoint_capture(const AdjArgs& a, const float* hx, const float* hy, float* slot, cudaStream_t s);
 int launch_adjoint_step(const AdjArgs& a, int back, const float* dslot, cudaStream_t s);

@@ -128,6 +128,13 @@ int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaS
 
 __global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
 
+__global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }
+
+int launch_chunk_start(Control* ctrl, cudaStream_t s) {
+  chunk_start_kernel<<<1, 1, 0, s>>>(ctrl);
+  return 1;
+}
+
 // A soft source on every cell of an inclusive box (a line source is a box one
 // cell wide): field += scale * vals[t + shift] on each cell, t the current
 // step; shift = -1 with a negative scale takes back the previous step's value

@@ -150,6 +150,19 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
 /* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
  * handle's stream). Returns once the work is enqueued. */
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
+/* Half a time step: phase 0 = the E half (curl of H, CPML, materials,
+ * sources, TFSF, E-phase DFT sample; it also advances the TFSF aux grids one
+ * step), phase 1 = the H half, which completes the step. The halves must
+ * alternate, E first; fdtd_step refuses to run between them. For callers
+ * that exchange data between the halves, such as the ghost planes of a
+ * z-slab decomposition (the reference does the same between its E and H
+ * functors across MPI ranks, BoundaryUpdates.hpp:919-1051). Launched eagerly. */
+int fdtd_step_half(fdtd_grid* g, int phase, void* stream);
+/* Copy z plane k of a stored component (FDTD_EX..FDTD_EZ, FDTD_HX..FDTD_HZ)
+ * between the grid and a compact device buffer of nx*ny values of the grid's
+ * precision, x fastest (to_grid = 1: buffer to grid). The FP32 method stores
+ * eta*H, and that is what is copied. Stream-ordered on `stream`. */
+int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream);
 /* fdtd_step for callers that cannot allocate device memory while stepping
  * (no counterpart in the reference, whose steps run on the host). Same
  * kernels, order and results as fdtd_step, launched eagerly; the per-call

@@ -480,7 +480,8 @@ int oracle_dft_get(const oracle_grid* g, int handle, double* out) {
   return 0;
 }
 
-static void step_one(oracle_grid* g) {
+/* one half step: phase 0 = the E half, 1 = the H half (which ends the step) */
+static void step_half(oracle_grid* g, int phase) {
   const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
   const int three = g->mode == THREED;
   const double dt = g->dt, dx = g->dx;
@@ -490,6 +491,7 @@ static void step_one(oracle_grid* g) {
   int pmlax[3];
   for (int a = 0; a < 3; a++) pmlax[a] = g->pml[a][0] > 0 || g->pml[a][1] > 0;
 
+  if (phase == 1) goto h_half;
   /* ---------------- E half step ---------------- */
   for (int k = k0; k <= k1; k++)
     for (int j = 1; j <= ny - 2; j++)
@@ -589,7 +591,9 @@ static void step_one(oracle_grid* g) {
   }
   apply_boxes(g, 0);
   dft_apply(g, 0, (double)(g->t + 1));
+  return;
 
+h_half:
   /* ---------------- H half step ---------------- */
   for (int k = k0; k <= k1; k++)
     for (int j = 1; j <= ny - 2; j++)
@@ -657,8 +661,19 @@ static void step_one(oracle_grid* g) {
   g->t++;
 }
 
+static void step_one(oracle_grid* g) {
+  step_half(g, 0);
+  step_half(g, 1);
+}
+
 int oracle_step(oracle_grid* g, int nsteps) {
   for (int s = 0; s < nsteps; s++) step_one(g);
+  return 0;
+}
+
+int oracle_step_half(oracle_grid* g, int phase) {
+  if (phase != 0 && phase != 1) return -1;
+  step_half(g, phase);
   return 0;
 }
 

@@ -62,6 +62,9 @@ int oracle_add_tfsf_plane(oracle_grid* g, int axis, int orient, const int* lo, c
 int oracle_add_dft(oracle_grid* g, int comp, const int* lo, const int* hi,
                    const double* freqs, int nf);
 int oracle_step(oracle_grid* g, int nsteps);
+/* one half step: 0 = the E half, 1 = the H half (ends the step); the two
+ * must alternate, E first */
+int oracle_step_half(oracle_grid* g, int phase);
 /* which: 0..2 D, 3..5 E, 6..8 B, 9..11 H, 12..14 P(pole 0), 15..17 J(pole 0),
  * 18..35 psi[ft][I][J]; 36.. P/J of further poles (6 per pole). */
 int oracle_get(const oracle_grid* g, int which, double* out);

@@ -67,6 +67,7 @@ def lib():
                                             ctypes.c_int, dp, ctypes.c_int]
         L.oracle_add_dft.argtypes = [vp, ctypes.c_int, ip, ip, dp, ctypes.c_int]
         L.oracle_step.argtypes = [vp, ctypes.c_int]
+        L.oracle_step_half.argtypes = [vp, ctypes.c_int]
         L.oracle_get.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_set.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_dft_get.argtypes = [vp, ctypes.c_int, dp]
@@ -152,6 +153,17 @@ class OracleGrid:
 
     def step(self, n: int) -> None:
         lib().oracle_step(self.h, n)
+
+    def step_half(self, phase: int) -> None:
+        assert lib().oracle_step_half(self.h, phase) == 0
+
+    def get_plane(self, name: str, k: int) -> np.ndarray:
+        return self.get(name)[k].copy()
+
+    def set_plane(self, name: str, k: int, plane: np.ndarray) -> None:
+        a = self.get(name)
+        a[k] = plane
+        self.set(name, a)
 
     def get(self, name: str) -> np.ndarray:
         which = ALL_NAMES.index(name) if name in ALL_NAMES else int(name)

@@ -1,0 +1,132 @@
+"""Z-slab decomposition (fdtd_b200/zslab.py) on CPU: the partition and
+slicing rules, and the decomposed run with real ghost-plane exchanges between
+gloo ranks, each rank stepping its slab with the CPU oracle half step by half
+step. The gathered fields and spectra must equal the single-grid oracle bit
+for bit."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+import scenarios
+from fdtd_b200 import problem as P
+from fdtd_b200.zslab import ZSlabRank, local_problem, merge_dfts, partition_z
+
+CASES = [scenarios.td_tfsf_box, scenarios.td_drude_lorentz, scenarios.td_box_sources, scenarios.td_h_sources,
+         scenarios.td_lorentz_two_pole_blocks]
+
+
+@pytest.mark.parametrize("make", CASES, ids=lambda f: f.__name__)
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_partition_covers_the_interior_outside_the_cpml(make, world):
+    p = make()
+    nz = p.shape[2]
+    if make is scenarios.td_lorentz_two_pole_blocks and world == 3:
+        # 18 interior planes in 8-plane blocks with a 3-cell CPML: no room for
+        # two boundaries on block edges outside the CPML
+        with pytest.raises(ValueError):
+            partition_z(p, world)
+        return
+    ranges = partition_z(p, world)
+    assert ranges[0][0] == 1 and ranges[-1][1] == nz - 1
+    assert all(a[1] == b[0] and a[0] < a[1] for a, b in zip(ranges, ranges[1:]))
+    lo, hi = p.pml.get((2, 0), 0), p.pml.get((2, 1), 0)
+    for z0, z1 in ranges[1:]:
+        assert z0 > lo + 1 and z0 <= nz - 2 - hi
+        if p.block_ids is not None:
+            assert (z0 - 1) % (1 << p.block_shift) == 0
+
+
+def test_local_problem_moves_and_clips_everything_along_z():
+    p = scenarios.td_tfsf_box()
+    nz = p.shape[2]
+    ranges = partition_z(p, 3)
+    parts = [local_problem(p, z0, z1) for z0, z1 in ranges]
+    assert sum(q.shape[2] - 2 for q in parts) == nz - 2
+    assert (2, 0) in parts[0].pml and (2, 1) not in parts[0].pml
+    assert (2, 1) in parts[-1].pml and (2, 0) not in parts[-1].pml
+    assert all((2, s) not in parts[1].pml for s in (0, 1))
+    # every TFSF plane cell and DFT point lands on exactly one rank
+    n_tfsf = sum(np.prod([h - l + 1 for l, h in zip(pl.lo, pl.hi)]) for pl in p.tfsf.planes)
+    got = sum(np.prod([h - l + 1 for l, h in zip(pl.lo, pl.hi)]) for q in parts if q.tfsf for pl in q.tfsf.planes)
+    assert got == n_tfsf
+    for gi, r in enumerate(p.dfts):
+        n = np.prod([h - l + 1 for l, h in zip(r.lo, r.hi)])
+        m = sum(np.prod([h - l + 1 for l, h in zip(q.dfts[li].lo, q.dfts[li].hi)])
+                for q in parts for li, g in enumerate(q.dft_map) if g == gi)
+        assert m == n
+
+
+class OracleSlab:
+    """A rank's slab stepped by the CPU oracle, planes as torch CPU tensors."""
+
+    def __init__(self, q):
+        import pyoracle
+        self.g = pyoracle.OracleGrid(q)
+        self.nx, self.ny = q.shape[0], q.shape[1]
+
+    def empty_plane(self):
+        return torch.empty(self.nx * self.ny, dtype=torch.float64)
+
+    def read_plane(self, name, k):
+        return torch.from_numpy(np.ascontiguousarray(self.g.get_plane(name, k)).ravel())
+
+    def write_plane(self, name, k, t):
+        self.g.set_plane(name, k, t.numpy().reshape(self.ny, self.nx))
+
+    def step_half(self, phase):
+        self.g.step_half(phase)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, case, out_path):
+    import sys
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "oracle"))
+    import scenarios as sc
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        p = getattr(sc, case)()
+        z0, z1 = partition_z(p, world)[rank]
+        q = local_problem(p, z0, z1)
+        slab = OracleSlab(q)
+        ZSlabRank(slab, q.shape[2], rank, world).step(p.steps)
+        fields = {n: slab.g.get(n)[1:-1] for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
+        spectra = [slab.g.dft(li) for li in range(len(q.dfts))]
+        parts = [None] * world if rank == 0 else None
+        dist.gather_object((fields, q.dft_map, spectra), parts, dst=0)
+        if rank == 0:
+            merged = {n: np.concatenate([f[n] for f, _, _ in parts], axis=0) for n in fields}
+            dfts = merge_dfts(p, [(m, s) for _, m, s in parts])
+            np.savez(out_path, *dfts, **merged)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("make", CASES, ids=lambda f: f.__name__)
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_reproduce_the_single_grid(oracle, make, world, tmp_path):
+    if make is scenarios.td_lorentz_two_pole_blocks and world == 3:
+        pytest.skip("no block-aligned 3-way partition of this grid")
+    p = make()
+    out = str(tmp_path / "zslab.npz")
+    mp.start_processes(_rank_main, args=(world, _free_port(), make.__name__, out), nprocs=world, join=True,
+                       start_method="spawn")
+    got = np.load(out)
+    ref = oracle.run_oracle(p)
+    for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert np.array_equal(got[n], ref.get(n)[1:-1]), n
+    for q in range(len(p.dfts)):
+        assert np.array_equal(got[f"arr_{q}"], ref.dft(q)), q
