@@ -48,7 +48,7 @@ P_STEPS = {"drude384": 1000, "lorentz768": 500, "tm256": 2000}
 
 # DRAM bytes per interior cell of one sweep launch, from ncu captures at 256^3 (profiles/)
 MEASURED_TRAFFIC = {
-    ("drude384", "staged"): {"e": 663.850496e6 / 16387064, "h": 632.577024e6 / 16387064,
+    ("drude384", "staged"): {"e": 664.30848e6 / 16387064, "h": 629.359616e6 / 16387064,
                              "source": "ncu capture at 256^3 scaled by interior cells "
                                        "(profiles/staged_sweeps_tfsf_gather_drude256.md)"},
     ("drude384", "flat"): {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,

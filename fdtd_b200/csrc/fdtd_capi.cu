@@ -175,6 +175,7 @@ struct fdtd_grid {
   int* d_flag = nullptr;
   bool dirty_dft = true;
   int next_half = 0;  // fdtd_step_half: the phase expected next
+  BcFaces bcs{};      // faces with a boundary condition
   int sweep_kind = FDTD_SWEEP_AUTO;
   TmaState* tma = nullptr;
   long long version = 0;        // bumped by every change a captured graph would bake in
@@ -857,6 +858,28 @@ static int launch_boxes(fdtd_grid* g, int phase, int shift, cudaStream_t s) {
   return n;
 }
 
+// the boundary images of one half step (0: E, 1: H)
+static int launch_bc(fdtd_grid* g, int phase, cudaStream_t s) {
+  if (g->bcs.n == 0) return 0;
+  void* f[3];
+  for (int q = 0; q < 3; q++) f[q] = phase == 0 ? g->E[q] : g->H[q];
+  return launch_boundaries(g->bcs, phase, g->f32 ? 1 : 0, f, g->n[0], g->n[1], g->n[2], static_cast<int>(rowlen(g)),
+                           s);
+}
+
+int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (axis < 0 || axis >= dim_of(g) || side < 0 || side > 1) return fail(FDTD_ERR_INVALID, "bad axis or side");
+  if (kind < FDTD_BC_NONE || kind > FDTD_BC_PERIODIC) return fail(FDTD_ERR_INVALID, "bad boundary kind");
+  BcFaces nb{};
+  for (int q = 0; q < g->bcs.n; q++)
+    if (g->bcs.face[q].axis != axis || g->bcs.face[q].side != side) nb.face[nb.n++] = g->bcs.face[q];
+  if (kind != FDTD_BC_NONE) nb.face[nb.n++] = BcFace{axis, side, kind};
+  g->bcs = nb;
+  g->version++;
+  return FDTD_OK;
+}
+
 int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const int* hi, const double* origin,
                         const double* k, const double* pol_e, const double* pol_h, int aux_ncells,
                         const double* aux_vals, int naux) {
@@ -1037,6 +1060,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     if (prof) CK(cudaEventRecord(ev[1], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, s);
     if (boxes) g->launches += launch_boxes(g, 0, 0, s);
+    g->launches += launch_bc(g, 0, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], g->dft_maxpts[0], fE, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[0], s);
     if (prof) CK(cudaEventRecord(ev[2], s));
@@ -1052,6 +1076,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     if (prof) CK(cudaEventRecord(ev[3], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, s);
     if (boxes) g->launches += launch_boxes(g, 1, 0, s);
+    g->launches += launch_bc(g, 1, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], g->dft_maxpts[1], fH, g->n[1],
                                      static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[1], s);
     if (prof) CK(cudaEventRecord(ev[4], s));
@@ -1212,6 +1237,7 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
     g->launches += phase == 0 ? launch_plain_e(mode, pa, s) : launch_plain_h(mode, pa, s);
   }
   if (boxes) g->launches += launch_boxes(g, phase, 0, s);
+  g->launches += launch_bc(g, phase, s);
   g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[phase], g->ndft[phase], g->dft_pts[phase],
                                    g->dft_maxpts[phase], fields, g->n[1], static_cast<int>(rowlen(g)), g->ctrl,
                                    g->d_dft_buf[phase], s);
@@ -1540,6 +1566,7 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
     else if (g->d.device != b->device) why = "batched grids share one device";
     else if (!g->planes.empty() || !g->dfts.empty()) why = "batched grids carry no TFSF planes or DFT regions";
     else if (!g->boxes.empty()) why = "batched grids carry no box sources";
+    else if (g->bcs.n > 0) why = "batched grids carry no boundary conditions";
     else if (g->t != g0->t) why = "batched grids must have taken the same number of steps";
     else if (static_cast<long long>(g->pitch / 128) * g->n[1] >= (1 << 24)) why = "grid too large to batch";
     if (why) {
@@ -1965,6 +1992,7 @@ int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, 
   if (g->t != 0) return fail(FDTD_ERR_INVALID, "the adjoint starts from a grid that has not been stepped");
   if (!g->planes.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes grids without TFSF planes");
   if (g->max_poles != 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes non-dispersive materials");
+  if (g->bcs.n > 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes grids without boundary conditions");
   if (ckpt_every < 1 || ckpt_every > 4096) return fail(FDTD_ERR_INVALID, "ckpt_every must be 1..4096");
   if (!interior(g, probe_lo[0], probe_lo[1], 0) || !interior(g, probe_hi[0], probe_hi[1], 0) ||
       probe_lo[0] > probe_hi[0] || probe_lo[1] > probe_hi[1])

@@ -218,6 +218,17 @@ int launch_dft_rebase(Control* ctrl, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
 int launch_chunk_start(Control* ctrl, cudaStream_t s);
+// faces with a boundary condition (kind 1 PEC, 2 PMC, 3 symmetric,
+// 4 antisymmetric, 5 periodic)
+struct BcFace {
+  int axis, side, kind;
+};
+struct BcFaces {
+  int n;
+  BcFace face[6];
+};
+int launch_boundaries(const BcFaces& f, int ft, int is_f32, void* const* fields, int nx, int ny, int nz, int rowlen,
+                      cudaStream_t s);
 int launch_adjoint_inv_eps(const FusedArgs& fa, float* ie, cudaStream_t s);
 int launch_adjoint_capture(const AdjArgs& a, const float* hx, const float* hy, float* slot, cudaStream_t s);
 int launch_adjoint_step(const AdjArgs& a, int back, const float* dslot, cudaStream_t s);

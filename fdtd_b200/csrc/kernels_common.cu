@@ -130,6 +130,66 @@ __global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
 
 __global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }
 
+// Boundary conditions (include/BoundaryUpdates.hpp:230-760): on each face
+// with one, the outer cell takes the image of the interior cell next to the
+// face (periodic: of the interior cell at the far end of the axis), every
+// component of the half step's field times the sign of the condition. One
+// grid row (blockIdx.y) per face; cells of a face x fastest over the
+// interior range of the two other axes.
+__device__ __forceinline__ float bc_sign(int kind, int ft, int c, int axis) {
+  const bool normal = c == axis;
+  switch (kind) {
+    case 1: return ft == 0 ? (normal ? 1.f : -1.f) : (normal ? -1.f : 1.f);  // PEC
+    case 2: return ft == 0 ? (normal ? -1.f : 1.f) : (normal ? 1.f : -1.f);  // PMC
+    case 3: return normal ? -1.f : 1.f;                                      // symmetric
+    case 4: return normal ? 1.f : -1.f;                                      // antisymmetric
+    default: return 1.f;                                                     // periodic
+  }
+}
+
+template <typename T>
+__global__ void boundary_kernel(BcFaces f, int ft, T* f0, T* f1, T* f2, int nx, int ny, int nz, int rowlen) {
+  const BcFace& b = f.face[blockIdx.y];
+  int lo[3] = {1, 1, nz > 1 ? 1 : 0}, ext[3] = {nx - 2, ny - 2, nz > 1 ? nz - 2 : 1};
+  ext[b.axis] = 1;
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= static_cast<long long>(ext[0]) * ext[1] * ext[2]) return;
+  int idx[3];
+  idx[0] = lo[0] + static_cast<int>(q % ext[0]);
+  idx[1] = lo[1] + static_cast<int>((q / ext[0]) % ext[1]);
+  idx[2] = lo[2] + static_cast<int>(q / (static_cast<long long>(ext[0]) * ext[1]));
+  const int n[3] = {nx, ny, nz};
+  int src[3] = {idx[0], idx[1], idx[2]}, dst[3] = {idx[0], idx[1], idx[2]};
+  dst[b.axis] = b.side == 0 ? 0 : n[b.axis] - 1;
+  src[b.axis] = b.kind == 5 ? (b.side == 0 ? n[b.axis] - 2 : 1) : (b.side == 0 ? 1 : n[b.axis] - 2);
+  const long long cs = (static_cast<long long>(src[2]) * ny + src[1]) * rowlen + src[0];
+  const long long cd = (static_cast<long long>(dst[2]) * ny + dst[1]) * rowlen + dst[0];
+  T* fs[3] = {f0, f1, f2};
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (fs[c]) fs[c][cd] = static_cast<T>(bc_sign(b.kind, ft, c, b.axis)) * fs[c][cs];
+}
+
+int launch_boundaries(const BcFaces& f, int ft, int is_f32, void* const* fields, int nx, int ny, int nz, int rowlen,
+                      cudaStream_t s) {
+  if (f.n == 0) return 0;
+  long long most = 0;
+  for (int q = 0; q < f.n; q++) {
+    long long e[3] = {nx - 2, ny - 2, nz > 1 ? nz - 2 : 1};
+    e[f.face[q].axis] = 1;
+    most = e[0] * e[1] * e[2] > most ? e[0] * e[1] * e[2] : most;
+  }
+  const dim3 grid(static_cast<unsigned>((most + 255) / 256), f.n);
+  if (is_f32)
+    boundary_kernel<float><<<grid, 256, 0, s>>>(f, ft, static_cast<float*>(fields[0]), static_cast<float*>(fields[1]),
+                                                static_cast<float*>(fields[2]), nx, ny, nz, rowlen);
+  else
+    boundary_kernel<double><<<grid, 256, 0, s>>>(f, ft, static_cast<double*>(fields[0]),
+                                                 static_cast<double*>(fields[1]), static_cast<double*>(fields[2]), nx,
+                                                 ny, nz, rowlen);
+  return 1;
+}
+
 int launch_chunk_start(Control* ctrl, cudaStream_t s) {
   chunk_start_kernel<<<1, 1, 0, s>>>(ctrl);
   return 1;

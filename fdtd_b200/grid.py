@@ -31,7 +31,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
-           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
+           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
@@ -78,6 +78,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_material_ids": [vp, vp],
         "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
         "fdtd_set_eps_map": [vp, dp],
+        "fdtd_set_boundary": [vp, i, i, i],
         "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_step_half": [vp, i, vp],
         "fdtd_copy_plane": [vp, i, i, vp, i, vp],
@@ -179,6 +180,11 @@ class Grid:
         nbz, nby, nbx = a.shape
         _check(load_library().fdtd_set_material_blocks(self.h, shift, a.ctypes.data, nbx, nby, nbz))
 
+    def set_boundary(self, axis: int, side: int, kind: str) -> None:
+        """kind: 'none', 'pec', 'pmc', 'symmetric', 'antisymmetric' or 'periodic'."""
+        code = 0 if kind == "none" else P.BOUNDARY_KINDS[kind]
+        _check(load_library().fdtd_set_boundary(self.h, int(axis), int(side), code))
+
     def set_eps_map(self, eps: Optional[np.ndarray]) -> None:
         if eps is None:
             _check(load_library().fdtd_set_eps_map(self.h, None))
@@ -214,6 +220,8 @@ class Grid:
         g = cls(p.mode, p.shape, p.dx, p.dt, precision, device)
         for (a, s), n in sorted(p.pml.items()):
             g.set_pml(a, s, n)
+        for (a, s), kind in sorted(p.boundaries.items()):
+            g.set_boundary(a, s, kind)
         g.set_materials(p.materials)
         if p.ids is not None:
             g.set_material_ids(p.ids)

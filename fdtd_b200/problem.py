@@ -31,6 +31,10 @@ MODE_NAMES = {"TEM": TEM, "TE": TE, "TM": TM, "ThreeD": THREED, "3D": THREED}
 
 VACUUM, CONSTANT, DRUDE, LORENTZ = 0, 1, 2, 3
 SOURCE_TARGETS = {"E": 0, "D": 1, "H": 2, "B": 3}
+# boundary conditions of a face (include/BoundaryUpdates.hpp:18-27, 528-760):
+# the outer cell beyond the face takes a sign-masked image of the interior
+# cell next to the face, or (periodic) of the interior cell at the other end
+BOUNDARY_KINDS = {"pec": 1, "pmc": 2, "symmetric": 3, "antisymmetric": 4, "periodic": 5}
 MAX_POLES = 4
 
 
@@ -138,6 +142,7 @@ class Problem:
     dx: float
     dt: float
     pml: dict = field(default_factory=dict)  # {(axis, side): ncells}
+    boundaries: dict = field(default_factory=dict)  # {(axis, side): kind in BOUNDARY_KINDS}
     materials: List[Material] = field(default_factory=lambda: [Material.vacuum()])
     ids: Optional[np.ndarray] = None  # uint8, shape (nz, ny, nx)
     # per-cell relative permittivity of vacuum/constant cells (> 0 replaces

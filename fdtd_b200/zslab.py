@@ -14,8 +14,8 @@ ranks they are ghost planes, refilled every half step:
 
 This is the exchange of the reference's MPI boundary (BoundaryUpdates.hpp:
 919-1051), restated for SoA planes. Everything else is cut along z: material
-ids and the permittivity map are sliced; the z CPML stays with the first and
-last rank (range boundaries are kept out of the CPML slabs, and out of the
+ids and the permittivity map are sliced; the z CPML and z-face boundary
+conditions stay with the first and last rank (range boundaries are kept out of the CPML slabs, and out of the
 middle of material blocks); sources, TFSF planes (each rank replays the same
 aux grid) and DFT regions are clipped to each range and moved to local
 coordinates. Per cell the arithmetic is that of the single grid, so the
@@ -58,6 +58,8 @@ def partition_z(p: P.Problem, world: int) -> List[Tuple[int, int]]:
     interior = nz - 2
     if world < 1 or world > interior:
         raise ValueError("world must be 1..nz-2")
+    if world > 1 and "periodic" in (p.boundaries.get((2, 0)), p.boundaries.get((2, 1))):
+        raise ValueError("a periodic z boundary joins the first and last rank: not decomposed along z")
     last_lo, first_hi = _slab_planes(nz, p)
     align = (1 << p.block_shift) if (p.block_ids is not None and p.ids is None) else 1
     bounds = [1]
@@ -94,6 +96,11 @@ def local_problem(p: P.Problem, z0: int, z1: int) -> P.Problem:
         q.pml[(2, 0)] = p.pml[(2, 0)]
     if z1 == nz - 1 and p.pml.get((2, 1), 0) > 0:
         q.pml[(2, 1)] = p.pml[(2, 1)]
+    q.boundaries = {k: v for k, v in p.boundaries.items() if k[0] != 2}
+    if z0 == 1 and (2, 0) in p.boundaries:
+        q.boundaries[(2, 0)] = p.boundaries[(2, 0)]
+    if z1 == nz - 1 and (2, 1) in p.boundaries:
+        q.boundaries[(2, 1)] = p.boundaries[(2, 1)]
     q.ids = None if p.ids is None else np.ascontiguousarray(p.ids[off:off + nzl])
     q.block_ids = None
     if p.block_ids is not None and p.ids is None:

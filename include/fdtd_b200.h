@@ -117,6 +117,20 @@ int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids,
  * values <= 0 keep the material. NULL removes the map. */
 int fdtd_set_eps_map(fdtd_grid* g, const double* eps);
 
+/* Boundary condition of face (axis, side 0 = min, 1 = max), the
+ * make_pec/pmc/symmetric/antisymmetric/periodic_boundary of the reference
+ * (BoundaryUpdates.hpp:528-845) applied to the interior cells next to the
+ * face: after the sources of each half step, the outer cell beyond the face
+ * takes that cell's E (then H) times the condition's sign per component
+ * (PEC: E normal +, tangential -; H the opposite; PMC the reverse of PEC;
+ * symmetric: normal -, tangential +; antisymmetric the reverse), or, for
+ * periodic, the value of the interior cell at the far end of the axis.
+ * FDTD_BC_NONE (the default) leaves the outer cells at zero. Bloch-periodic
+ * is not offered: its complex factor has no meaning for the real fields. */
+enum { FDTD_BC_NONE = 0, FDTD_BC_PEC = 1, FDTD_BC_PMC = 2, FDTD_BC_SYMMETRIC = 3, FDTD_BC_ANTISYMMETRIC = 4,
+       FDTD_BC_PERIODIC = 5 };
+int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind);
+
 /* Soft source (SoftSource<Signal, Cell, GetField<F>>::apply): vals[t] is
  * added at step t (counted from grid creation) to component comp (0..2) of
  * E after the constitutive update (target 0), D before the CPML pass (1),

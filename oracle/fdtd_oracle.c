@@ -92,6 +92,7 @@ struct oracle_grid {
   src_t* boxes;
   int nbox;
   double* eps_map; /* per-cell relative permittivity of vacuum/constant cells, or NULL */
+  int bc[3][2];    /* boundary condition of each face: 0 none, 1..5 (oracle_set_boundary) */
   plane_t* planes;
   int nplanes;
   dft_t* dfts;
@@ -275,6 +276,54 @@ static void apply_boxes(oracle_grid* g, int target) {
       for (int j = b->j; j <= b->j1; j++)
         for (int i = b->i; i <= b->i1; i++) f[k * sz + j * sy + i] += v;
   }
+}
+
+int oracle_set_boundary(oracle_grid* g, int axis, int side, int kind) {
+  int dim = g->mode == THREED ? 3 : 2;
+  if (axis < 0 || axis >= dim || side < 0 || side > 1 || kind < 0 || kind > 5) return -1;
+  g->bc[axis][side] = kind;
+  return 0;
+}
+
+/* sign of the image of component c of field type ft (0 E, 1 H) across a face
+ * normal to `axis` (include/BoundaryUpdates.hpp:528-536, 612-618, 663-670,
+ * 716-723); periodic keeps the sign */
+static double bc_mask(int kind, int ft, int c, int axis) {
+  const int normal = c == axis;
+  switch (kind) {
+    case 1: return ft == 0 ? (normal ? 1.0 : -1.0) : (normal ? -1.0 : 1.0);  /* PEC */
+    case 2: return ft == 0 ? (normal ? -1.0 : 1.0) : (normal ? 1.0 : -1.0);  /* PMC */
+    case 3: return normal ? -1.0 : 1.0;                                       /* symmetric */
+    case 4: return normal ? 1.0 : -1.0;                                       /* antisymmetric */
+    default: return 1.0;                                                      /* periodic */
+  }
+}
+
+/* every face with a boundary condition: its outer cells take the masked
+ * image of the interior cells next to the face (periodic: of the interior
+ * cells at the far end of the axis), for E (ft 0) or H (ft 1) */
+static void apply_boundaries(oracle_grid* g, int ft) {
+  const int dim = g->mode == THREED ? 3 : 2;
+  const size_t sy = (size_t)g->n[0], sz = (size_t)g->n[0] * g->n[1];
+  for (int a = 0; a < dim; a++)
+    for (int side = 0; side < 2; side++) {
+      const int kind = g->bc[a][side];
+      if (!kind) continue;
+      int lo[3] = {1, 1, dim == 3 ? 1 : 0}, hi[3] = {g->n[0] - 2, g->n[1] - 2, dim == 3 ? g->n[2] - 2 : 0};
+      lo[a] = hi[a] = side == 0 ? 1 : g->n[a] - 2;
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            int src[3] = {i, j, k}, dst[3] = {i, j, k};
+            dst[a] = side == 0 ? 0 : g->n[a] - 1;
+            if (kind == 5) src[a] = side == 0 ? g->n[a] - 2 : 1;
+            const size_t cs = src[2] * sz + src[1] * sy + src[0], cd = dst[2] * sz + dst[1] * sy + dst[0];
+            for (int c = 0; c < 3; c++) {
+              if (ft == 0 && g->hasE[c]) g->E[c][cd] = bc_mask(kind, 0, c, a) * g->E[c][cs];
+              if (ft == 1 && g->hasH[c]) g->H[c][cd] = bc_mask(kind, 1, c, a) * g->H[c][cs];
+            }
+          }
+    }
 }
 
 int oracle_set_eps_map(oracle_grid* g, const double* eps) {
@@ -590,6 +639,7 @@ static void step_half(oracle_grid* g, int phase) {
     g->E[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
   }
   apply_boxes(g, 0);
+  apply_boundaries(g, 0);
   dft_apply(g, 0, (double)(g->t + 1));
   return;
 
@@ -657,6 +707,7 @@ h_half:
     g->H[sr->comp][c] += g->t < sr->nvals ? sr->vals[g->t] : 0.0;
   }
   apply_boxes(g, 2);
+  apply_boundaries(g, 1);
   dft_apply(g, 1, (double)g->t + 1.5);
   g->t++;
 }

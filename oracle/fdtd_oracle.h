@@ -50,6 +50,10 @@ int oracle_add_source_box(oracle_grid* g, int comp, int target, const int* lo, c
 /* per-cell relative permittivity (ncell doubles, x fastest): vacuum and
  * constant cells with a value > 0 take it in place of eps_inf; NULL removes */
 int oracle_set_eps_map(oracle_grid* g, const double* eps);
+/* boundary condition of face (axis, side): 0 none (the outer cells stay
+ * zero), 1 PEC, 2 PMC, 3 symmetric, 4 antisymmetric, 5 periodic; applied
+ * after the sources of each half step */
+int oracle_set_boundary(oracle_grid* g, int axis, int side, int kind);
 /* One TFSF plane (include/Source.hpp:472-634) with its own Aux1D grid.
  * axis/orient give the normal; lo/hi are inclusive cell ranges; origin (in
  * cells) and k define the location functor and wave vector; pol_e / pol_h are

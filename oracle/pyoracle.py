@@ -18,6 +18,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 SOURCE_TARGETS = {"E": 0, "D": 1, "H": 2, "B": 3}
+BOUNDARY_KINDS = {"pec": 1, "pmc": 2, "symmetric": 3, "antisymmetric": 4, "periodic": 5}
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
@@ -68,6 +69,7 @@ def lib():
         L.oracle_add_dft.argtypes = [vp, ctypes.c_int, ip, ip, dp, ctypes.c_int]
         L.oracle_step.argtypes = [vp, ctypes.c_int]
         L.oracle_step_half.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_boundary.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_get.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_set.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_dft_get.argtypes = [vp, ctypes.c_int, dp]
@@ -115,6 +117,8 @@ class OracleGrid:
             raise ValueError("oracle_create rejected the grid")
         for (a, s), n in sorted(p.pml.items()):
             assert L.oracle_set_pml(self.h, a, s, n) == 0
+        for (a, s), kind in sorted(p.boundaries.items()):
+            assert L.oracle_set_boundary(self.h, a, s, BOUNDARY_KINDS[kind]) == 0
         if len(p.materials) > 256:
             raise ValueError("the oracle takes at most 256 materials")
         mats = (OracleMaterial * len(p.materials))(*[_mat_struct(m) for m in p.materials])
@@ -269,6 +273,10 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
                          f"{t.pol_h[0]!r} {t.pol_h[1]!r} {t.pol_h[2]!r}")
             for pl in t.planes:
                 lines.append(f"{pl.axis} {pl.orient} {pl.lo[0]} {pl.hi[0]} {pl.lo[1]} {pl.hi[1]} {pl.lo[2]} {pl.hi[2]}")
+        if p.boundaries:
+            lines.append(f"nbc {len(p.boundaries)}")
+            for (a, sd), kind in sorted(p.boundaries.items()):
+                lines.append(f"{a} {sd} {BOUNDARY_KINDS[kind]}")
         lines.append(f"steps {steps}")
         op = os.path.join(td, "out.bin")
         lines.append(f"out {op}")

@@ -33,6 +33,11 @@
 //        axis orient i0 i1 j0 j1 k0 k1 (inclusive). set_pol 0 keeps the
 //        plane's own polarisation (TE/TM defaults), 1 sets pe/ph.
 //        aux_path: float64 per aux step (value for aux step s at index s-1)
+//   nbc B then B lines: axis side kind (optional; kind 1 PEC, 2 PMC,
+//        3 symmetric, 4 antisymmetric, 5 periodic), applied with the
+//        reference's make_*_boundary (include/BoundaryUpdates.hpp) to the
+//        interior cells next to the face, after the E sources (updateE) and
+//        after the H sources (updateH)
 //   steps N
 //   out path
 // Output: float64 arrays in order D(3) E(3) B(3) H(3) P(3) J(3) and the CPML
@@ -48,6 +53,8 @@
 #include <memory>
 #include <fstream>
 #include <chrono>
+#include <cstddef>
+#include <iterator>
 
 namespace fdtd {
 template <typename U, typename F>
@@ -98,6 +105,7 @@ static std::vector<double> read_f64(const std::string& path) {
 struct Mat { int kind; double K, delta, freq, gamma, mu; };
 struct Src { int comp, target, i, j, k; std::vector<double> vals; };
 struct PlaneSpec { int axis, orient, lo[3], hi[3]; };
+struct BcSpec { int axis, side, kind; };
 
 struct Scenario {
   int mode = 2, nx = 1, ny = 1, nz = 1;
@@ -109,6 +117,7 @@ struct Scenario {
   int aux_ncells = 0; std::vector<double> aux_vals; double origin[3] = {0, 0, 0}, kvec[3] = {1, 0, 0};
   int set_pol = 0; double pol_e[3] = {0, 0, 0}, pol_h[3] = {0, 0, 0};
   std::vector<PlaneSpec> planes;
+  std::vector<BcSpec> bcs;
   int steps = 0;
   std::string out;
 };
@@ -135,6 +144,32 @@ struct PtrIt {
   PtrIt operator++(int) { PtrIt t = *this; ++it; return t; }
   bool operator!=(const PtrIt& o) const { return it != o.it; }
   bool operator==(const PtrIt& o) const { return it == o.it; }
+};
+
+// Iterator over cell pointers with the iterator traits DerivedIterator
+// (include/BoundaryUpdates.hpp:415-478) reads.
+template <class C>
+struct BcIt {
+  typedef std::ptrdiff_t difference_type;
+  typedef C value_type;
+  typedef C& reference;
+  typedef C* pointer;
+  typedef std::forward_iterator_tag iterator_category;
+  typename std::vector<C*>::iterator it;
+  C& operator*() const { return **it; }
+  BcIt& operator++() { ++it; return *this; }
+  BcIt operator++(int) { BcIt t = *this; ++it; return t; }
+  bool operator!=(const BcIt& o) const { return it != o.it; }
+  bool operator==(const BcIt& o) const { return it == o.it; }
+};
+
+// the periodic partner of a boundary cell: the interior cell at the other
+// end of the axis (the Functor of make_periodic_boundary)
+template <class C>
+struct PartnerF {
+  std::vector<C*>* cells;
+  std::vector<C*>* partners;
+  C& operator()(BcIt<C> it) const { return *(*partners)[it.it - cells->begin()]; }
 };
 
 struct TableSignal {
@@ -346,6 +381,36 @@ static int run(Scenario& s) {
     }
   }
 
+  // boundary conditions on the faces (the boundary cells are the interior
+  // cells next to the face; their outer neighbours take the image)
+  std::vector<std::vector<C*>> bc_cells(s.bcs.size()), bc_partners(s.bcs.size());
+  std::vector<BoundaryData> bcs;
+  for (size_t q = 0; q < s.bcs.size(); q++) {
+    const BcSpec& b = s.bcs[q];
+    int lo[3] = {1, 1, dim == 3 ? 1 : 0}, hi[3] = {nx - 2, ny - 2, dim == 3 ? nz - 2 : 0};
+    lo[b.axis] = hi[b.axis] = b.side == 0 ? 1 : n[b.axis] - 2;
+    for (int k = lo[2]; k <= hi[2]; k++)
+      for (int j = lo[1]; j <= hi[1]; j++)
+        for (int i = lo[0]; i <= hi[0]; i++) {
+          bc_cells[q].push_back(&at(i, j, k));
+          int p[3] = {i, j, k};
+          p[b.axis] = b.side == 0 ? n[b.axis] - 2 : 1;
+          bc_partners[q].push_back(&at(p[0], p[1], p[2]));
+        }
+    BcIt<C> bb{bc_cells[q].begin()}, be{bc_cells[q].end()};
+    PartnerF<C> pf{&bc_cells[q], &bc_partners[q]};
+#define FDTD_BC(D, O)                                                                                      \
+  if (b.kind == 1) bcs.push_back(make_pec_boundary<Mode, D, O>(bb, be));                                 \
+  else if (b.kind == 2) bcs.push_back(make_pmc_boundary<Mode, D, O>(bb, be));                            \
+  else if (b.kind == 3) bcs.push_back(make_symmetric_boundary<Mode, D, O>(bb, be));                      \
+  else if (b.kind == 4) bcs.push_back(make_antisymmetric_boundary<Mode, D, O>(bb, be));                  \
+  else bcs.push_back(make_periodic_boundary<Mode, D, O>(bb, be, pf));
+    if (b.axis == 0) { if (b.side == 0) { FDTD_BC(Dir::X, Orientation::MIN) } else { FDTD_BC(Dir::X, Orientation::MAX) } }
+    else if (b.axis == 1) { if (b.side == 0) { FDTD_BC(Dir::Y, Orientation::MIN) } else { FDTD_BC(Dir::Y, Orientation::MAX) } }
+    else { if (b.side == 0) { FDTD_BC(Dir::Z, Orientation::MIN) } else { FDTD_BC(Dir::Z, Orientation::MAX) } }
+#undef FDTD_BC
+  }
+
   const auto clock0 = std::chrono::steady_clock::now();
   for (int t = 0; t < s.steps; t++) {
     // ---- E half step: curl, TFSF, CPML per axis, material, sources
@@ -359,6 +424,7 @@ static int run(Scenario& s) {
     if constexpr (Mode::dim == 3) { if (pmlax[2]) for (C* c : interior) UpdatePML<Mode, FieldType::Electric, Dir::Z>(dt, dx)(*c); }
     for (C* c : interior) eupd[matid(*c)](*c);
     for (auto& ap : appliers) ap(static_cast<double>(t));
+    for (auto& b : bcs) b.updateE();
     // ---- H half step
     for (C* c : interior) yee<Mode, Bx>(*c, dt, dx);
     for (C* c : interior) yee<Mode, By>(*c, dt, dx);
@@ -370,6 +436,7 @@ static int run(Scenario& s) {
     if constexpr (Mode::dim == 3) { if (pmlax[2]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::Z>(dt, dx)(*c); }
     for (C* c : interior) hupd[matid(*c)](*c);
     for (auto& ap : happliers) ap(static_cast<double>(t));
+    for (auto& b : bcs) b.updateH();
   }
 
   const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - clock0).count();
@@ -441,6 +508,10 @@ int main(int argc, char** argv) {
       if (m > 0) s.aux_vals = read_f64(p);
       s.planes.resize(m);
       for (auto& x : s.planes) in >> x.axis >> x.orient >> x.lo[0] >> x.hi[0] >> x.lo[1] >> x.hi[1] >> x.lo[2] >> x.hi[2];
+    } else if (key == "nbc") {
+      int m; in >> m;
+      s.bcs.resize(m);
+      for (auto& b : s.bcs) in >> b.axis >> b.side >> b.kind;
     } else if (key == "steps") in >> s.steps;
     else if (key == "out") in >> s.out;
     else { fprintf(stderr, "unknown key %s\n", key.c_str()); return 1; }

@@ -207,6 +207,56 @@ def td_box_sources() -> Problem:
     return p
 
 
+def tm_boundaries() -> Problem:
+    """TM with a PEC face (x min), a CPML face (x max) and periodic faces in y."""
+    nx, ny = 36, 30
+    p = Problem(TM, (nx, ny, 1), DX, DT2, name="tm_boundaries")
+    p.pml[(0, 1)] = 6
+    p.boundaries = {(0, 0): "pec", (1, 0): "periodic", (1, 1): "periodic"}
+    p.sources.append(Source(2, (10, 8, 0), gaussian_pulse(90, 20, 6), "E"))
+    p.sources.append(Source(0, (20, 22, 0), 1e-3 * gaussian_pulse(90, 25, 6), "H"))
+    p.dfts.append(DFTRegion(2, (1, 15, 0), (nx - 2, 15, 0), [0.04]))
+    p.steps = 90
+    return p
+
+
+def te_boundaries() -> Problem:
+    """TE with symmetric (x min), antisymmetric (y max) and PMC (y min)
+    faces and a CPML face (x max), through a constant-eps block."""
+    nx, ny = 34, 38
+    p = Problem(TE, (nx, ny, 1), DX, DT2, name="te_boundaries")
+    p.pml[(0, 1)] = 5
+    p.boundaries = {(0, 0): "symmetric", (1, 1): "antisymmetric", (1, 0): "pmc"}
+    p.materials = [Material.vacuum(), Material.constant(3.0)]
+    ids = np.zeros((1, ny, nx), np.uint8)
+    ids[0, 12:20, 6:14] = 1
+    p.ids = ids
+    p.sources.append(Source(2, (9, 18, 0), gaussian_pulse(80, 20, 6), "H"))
+    p.sources.append(Source(0, (15, 25, 0), gaussian_pulse(80, 25, 6), "E"))
+    p.dfts.append(DFTRegion(5, (1, 1, 0), (nx - 2, ny - 2, 0), [0.03]))
+    p.steps = 80
+    return p
+
+
+def td_boundaries() -> Problem:
+    """3D: periodic x, symmetric y min, PMC z min, PEC z max, CPML y max,
+    with a Drude block."""
+    nx, ny, nz = 14, 16, 15
+    p = Problem(THREED, (nx, ny, nz), DX, DT3, name="td_boundaries")
+    p.pml[(1, 1)] = 3
+    p.boundaries = {(0, 0): "periodic", (0, 1): "periodic", (1, 0): "symmetric", (2, 0): "pmc", (2, 1): "pec"}
+    dt = DT3
+    p.materials = [Material.vacuum(), Material.drude(1.0, 0.3 / dt, 0.01 / dt)]
+    ids = np.zeros((nz, ny, nx), np.uint8)
+    ids[5:9, 4:8, 3:7] = 1
+    p.ids = ids
+    p.sources.append(Source(2, (7, 8, 7), gaussian_pulse(40, 15, 5), "E"))
+    p.sources.append(Source(0, (4, 10, 9), 1e-3 * gaussian_pulse(40, 12, 5), "H"))
+    p.dfts.append(DFTRegion(1, (1, 1, 7), (nx - 2, ny - 2, 7), [0.03]))
+    p.steps = 40
+    return p
+
+
 def tm_adjoint_small(n: int = 40, steps: int = 260, design: int = 8, seed: int = 1):
     """The adjoint workload at a size the CPU oracle runs in well under a
     second: TM, 6-cell CPML, a central design box of random eps_r in [1, 12],
@@ -239,5 +289,6 @@ def objective_problem(p, spec):
 
 # scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
-                       te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources]
+                       te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources,
+                       tm_boundaries, te_boundaries, td_boundaries]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]

@@ -12,7 +12,7 @@ from fdtd_b200.zslab import ZSlabDomain
 pytestmark = pytest.mark.gpu
 
 CASES = [scenarios.td_tfsf_box, scenarios.td_drude_lorentz, scenarios.td_box_sources, scenarios.td_h_sources,
-         scenarios.td_lorentz_two_pole_blocks]
+         scenarios.td_lorentz_two_pole_blocks, scenarios.td_boundaries]
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
