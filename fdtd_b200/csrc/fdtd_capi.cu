@@ -176,6 +176,8 @@ struct fdtd_grid {
   bool dirty_dft = true;
   int next_half = 0;  // fdtd_step_half: the phase expected next
   BcFaces bcs{};      // faces with a boundary condition
+  int scheme = 1;     // time policy of the curl updates: 1 BD1, 3 BD3, 4 BD4
+  void* hist[2][3][3]{};  // FP64 flux history [D|B][level][comp] of BD3/BD4
   int sweep_kind = FDTD_SWEEP_AUTO;
   TmaState* tma = nullptr;
   long long version = 0;        // bumped by every change a captured graph would bake in
@@ -554,6 +556,26 @@ PlainArgs plain_args(fdtd_grid* g) {
   a.mats = static_cast<const MatF64*>(g->d_mats);
   a.eps_map = static_cast<const double*>(g->d_eps_map);
   a.dispersive = g->max_poles;
+  // TimePolicy constants (include/YeeUpdates.hpp:184-186, :205-215, :254-265),
+  // folded by the host compiler as the reference's constexpr divisions are
+  a.cc = 1.0;
+  if (g->scheme == 3) {
+    a.bd = 2;
+    a.cc = 24.0 / 23.0;
+    a.bdk[0] = 21.0 / 23.0;
+    a.bdk[1] = 3.0 / 23.0;
+    a.bdk[2] = 1.0 / 23.0;
+  } else if (g->scheme == 4) {
+    a.bd = 3;
+    a.cc = 24.0 / 22.0;
+    a.bdk[0] = 17.0 / 22.0;
+    a.bdk[1] = 9.0 / 22.0;
+    a.bdk[2] = 5.0 / 22.0;
+    a.bdk[3] = 1.0 / 22.0;
+  }
+  for (int ft = 0; ft < 2; ft++)
+    for (int l = 0; l < 3; l++)
+      for (int c = 0; c < 3; c++) a.hist[ft][l][c] = static_cast<double*>(g->hist[ft][l][c]);
   return a;
 }
 
@@ -876,6 +898,34 @@ int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) {
     if (g->bcs.face[q].axis != axis || g->bcs.face[q].side != side) nb.face[nb.n++] = g->bcs.face[q];
   if (kind != FDTD_BC_NONE) nb.face[nb.n++] = BcFace{axis, side, kind};
   g->bcs = nb;
+  g->version++;
+  return FDTD_OK;
+}
+
+int fdtd_set_time_scheme(fdtd_grid* g, int scheme) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (scheme != FDTD_BD1 && scheme != FDTD_BD3 && scheme != FDTD_BD4)
+    return fail(FDTD_ERR_INVALID, "time scheme must be FDTD_BD1, FDTD_BD3 or FDTD_BD4");
+  if (g->f32 && scheme != FDTD_BD1)
+    return fail(FDTD_ERR_UNSUPPORTED, "the FP32 fused method steps with the leapfrog (BD1) scheme only");
+  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "a half step is pending");
+  CK(cudaSetDevice(g->d.device));
+  for (int ft = 0; ft < 2; ft++)
+    for (int l = 0; l < 3; l++)
+      for (int c = 0; c < 3; c++)
+        if (g->hist[ft][l][c]) {
+          dfree(g, g->hist[ft][l][c]);
+          g->hist[ft][l][c] = nullptr;
+        }
+  const int levels = scheme == FDTD_BD1 ? 0 : scheme - 1;
+  for (int ft = 0; ft < 2; ft++)
+    for (int l = 0; l < levels; l++)
+      for (int c = 0; c < 3; c++) {
+        if (!(ft == 0 ? hasE(g->d.mode, c) : hasH(g->d.mode, c))) continue;
+        const int rc = dalloc(g, &g->hist[ft][l][c], static_cast<size_t>(field_elems(g)) * elem(g));
+        if (rc != FDTD_OK) return rc;
+      }
+  g->scheme = scheme;
   g->version++;
   return FDTD_OK;
 }

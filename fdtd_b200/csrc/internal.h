@@ -126,6 +126,13 @@ struct PlainArgs {
   PlaneDev planes[kMaxPlanes];
   AuxTab aux[kMaxPlanes];
   Control* ctrl;
+  // time policy of the curl updates (include/YeeUpdates.hpp:182-294): bd
+  // history levels (0 BD1, 2 BD3, 3 BD4), bdk the coefficients of
+  // TimePolicy::get, cc its curl_coeff; hist[D|B][level][comp]
+  int bd;
+  double bdk[4];
+  double cc;
+  double* hist[2][3][3];
 };
 
 struct FusedArgs {

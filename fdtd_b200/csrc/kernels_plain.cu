@@ -64,6 +64,32 @@ __device__ double tfsf_term(const PlaneDev& p, const AuxTab& aux, long long row,
   return terms[0] + terms[1];
 }
 
+// YeeUpdate::update_all (YeeUpdates.hpp:396-405) of flux F at cell c with the
+// summed curl terms: F = TimePolicy::get(F) + (Coeff*curl_coeff*dt) * curl,
+// then TimePolicy::increment moves the old flux into the history (BD3:
+// :209-213, :231-236; BD4: :258-263, :282-288). sdt = Coeff*curl_coeff*dt.
+__device__ __forceinline__ void time_policy_update(const PlainArgs& a, int ft, int I, long long c, double* F,
+                                                   double sdt, double curl) {
+  const double old = F[c];
+  if (a.bd == 0) {
+    F[c] = old + sdt * curl;
+    return;
+  }
+  double* h0 = a.hist[ft][0][I] + c;
+  double* h1 = a.hist[ft][1][I] + c;
+  if (a.bd == 2) {
+    const double get = a.bdk[0] * old + a.bdk[1] * *h0 - a.bdk[2] * *h1;
+    F[c] = get + sdt * curl;
+  } else {
+    double* h2 = a.hist[ft][2][I] + c;
+    const double get = a.bdk[0] * old + a.bdk[1] * *h0 - a.bdk[2] * *h1 + a.bdk[3] * *h2;
+    F[c] = get + sdt * curl;
+    *h2 = *h1;
+  }
+  *h1 = *h0;
+  *h0 = old;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ PlainArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -77,7 +103,7 @@ __global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ Pl
   const double dt = a.dt;
   const long long t = a.ctrl->t;
 
-  // YeeUpdate<Mode, D_I>: D = D + dt*(a<d1> + a<d2>), a = LC*F/dx*(H_K - H_K[-J])
+  // YeeUpdate<Mode, D_I, TimePolicy>: a = LC*F/dx*(H_K - H_K[-J])
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasE(MODE, I)) continue;
@@ -95,7 +121,7 @@ __global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ Pl
       const double fdx = a.prof[0][J].F[idx[J]];
       at[q] = (levi(I, J, K) == 1 ? fdx : -fdx) * diff;
     }
-    a.D.f[I][c] = a.D.f[I][c] + dt * (at[0] + at[1]);
+    time_policy_update(a, 0, I, c, a.D.f[I], a.cc * dt, at[0] + at[1]);
   }
   // TFSFPlane::updateD
   for (int q = 0; q < a.nplanes; q++) {
@@ -106,7 +132,7 @@ __global__ void __launch_bounds__(256) plain_e_kernel(const __grid_constant__ Pl
 #pragma unroll
     for (int I = 2; I >= 0; I--) {
       if (!hasE(MODE, I)) continue;
-      a.D.f[I][c] += dt * tfsf_term<MODE>(p, ax, row, 0, I, idx, a.prof, a.dx);
+      a.D.f[I][c] += a.cc * dt * tfsf_term<MODE>(p, ax, row, 0, I, idx, a.prof, a.dx);
     }
   }
   // SoftSource on D
@@ -200,7 +226,7 @@ __global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ Pl
   const double dt = a.dt;
   const long long t = a.ctrl->t;
 
-  // YeeUpdate<Mode, B_I>: B = B + (-dt)*(a<d1> + a<d2>), a = LC*F/dx*(E_K[+J] - E_K)
+  // YeeUpdate<Mode, B_I, TimePolicy>: a = LC*F/dx*(E_K[+J] - E_K)
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasH(MODE, I)) continue;
@@ -218,7 +244,7 @@ __global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ Pl
       const double fdx = a.prof[1][J].F[idx[J]];
       at[q] = (levi(I, J, K) == 1 ? fdx : -fdx) * diff;
     }
-    a.B.f[I][c] = a.B.f[I][c] + -dt * (at[0] + at[1]);
+    time_policy_update(a, 1, I, c, a.B.f[I], -a.cc * dt, at[0] + at[1]);
   }
   // TFSFPlane::updateB (the aux grid was advanced by updateD: row + 1)
   for (int q = 0; q < a.nplanes; q++) {
@@ -229,7 +255,7 @@ __global__ void __launch_bounds__(256) plain_h_kernel(const __grid_constant__ Pl
 #pragma unroll
     for (int I = 2; I >= 0; I--) {
       if (!hasH(MODE, I)) continue;
-      a.B.f[I][c] += -dt * tfsf_term<MODE>(p, ax, row, 1, I, idx, a.prof, a.dx);
+      a.B.f[I][c] += -a.cc * dt * tfsf_term<MODE>(p, ax, row, 1, I, idx, a.prof, a.dx);
     }
   }
   // SoftSource on B

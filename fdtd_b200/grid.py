@@ -31,7 +31,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
-           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
+           "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
@@ -79,6 +79,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
         "fdtd_set_eps_map": [vp, dp],
         "fdtd_set_boundary": [vp, i, i, i],
+        "fdtd_set_time_scheme": [vp, i],
         "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_step_half": [vp, i, vp],
         "fdtd_copy_plane": [vp, i, i, vp, i, vp],
@@ -185,6 +186,11 @@ class Grid:
         code = 0 if kind == "none" else P.BOUNDARY_KINDS[kind]
         _check(load_library().fdtd_set_boundary(self.h, int(axis), int(side), code))
 
+    def set_time_scheme(self, scheme: int) -> None:
+        """1 (BD1, leapfrog), 3 (BD3) or 4 (BD4): the TimePolicy of every
+        curl update and TFSF correction; FP64 grids only for 3 and 4."""
+        _check(load_library().fdtd_set_time_scheme(self.h, int(scheme)))
+
     def set_eps_map(self, eps: Optional[np.ndarray]) -> None:
         if eps is None:
             _check(load_library().fdtd_set_eps_map(self.h, None))
@@ -222,6 +228,8 @@ class Grid:
             g.set_pml(a, s, n)
         for (a, s), kind in sorted(p.boundaries.items()):
             g.set_boundary(a, s, kind)
+        if p.time_scheme != 1:
+            g.set_time_scheme(p.time_scheme)
         g.set_materials(p.materials)
         if p.ids is not None:
             g.set_material_ids(p.ids)

@@ -143,6 +143,9 @@ class Problem:
     dt: float
     pml: dict = field(default_factory=dict)  # {(axis, side): ncells}
     boundaries: dict = field(default_factory=dict)  # {(axis, side): kind in BOUNDARY_KINDS}
+    # time policy of the curl updates and TFSF corrections: 1 BD1 (leapfrog),
+    # 3 BD3, 4 BD4 (include/YeeUpdates.hpp:182-294)
+    time_scheme: int = 1
     materials: List[Material] = field(default_factory=lambda: [Material.vacuum()])
     ids: Optional[np.ndarray] = None  # uint8, shape (nz, ny, nx)
     # per-cell relative permittivity of vacuum/constant cells (> 0 replaces

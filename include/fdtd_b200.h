@@ -131,6 +131,18 @@ enum { FDTD_BC_NONE = 0, FDTD_BC_PEC = 1, FDTD_BC_PMC = 2, FDTD_BC_SYMMETRIC = 3
        FDTD_BC_PERIODIC = 5 };
 int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind);
 
+/* Time policy of every curl update and TFSF correction, the TimePolicy
+ * template argument of YeeUpdate and TFSFPlane (BD1, BD3, BD4 of
+ * include/YeeUpdates.hpp:182-294): the flux update becomes
+ * F = TimePolicy::get(F) + Coeff*curl_coeff*dt*curl with the flux history
+ * (F of the previous two or three steps, zero at first) moved on each step.
+ * BD3 and BD4 need a smaller time step than the leapfrog BD1 (they diverge at
+ * 0.99 of the Courant limit; 0.5 is stable). FP64 plain grids only: an FP32
+ * grid answers FDTD_ERR_UNSUPPORTED for BD3/BD4. Setting a scheme clears the
+ * history. */
+enum { FDTD_BD1 = 1, FDTD_BD3 = 3, FDTD_BD4 = 4 };
+int fdtd_set_time_scheme(fdtd_grid* g, int scheme);
+
 /* Soft source (SoftSource<Signal, Cell, GetField<F>>::apply): vals[t] is
  * added at step t (counted from grid creation) to component comp (0..2) of
  * E after the constitutive update (target 0), D before the CPML pass (1),

@@ -26,6 +26,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "fdtd_b200.h"
@@ -104,13 +105,14 @@ struct Ricker {
 
 // ------------------------------------------------------------ plan ops
 namespace detail {
-enum class OpKind { Yee, Pml, Material, Source, TfsfD, TfsfB };
+enum class OpKind { Yee, Pml, Material, Source, TfsfD, TfsfB, BoundaryE, BoundaryH };
 struct Op {
   OpKind kind;
   FieldType ft = FieldType::NONE;
   int comp = -1, axis = -1;
   fdtd_material mat{};
   int source = -1, plane = -1;
+  int scheme = FDTD_BD1;
 };
 inline fdtd_material blank_material(int kind) {
   fdtd_material m{};
@@ -121,16 +123,27 @@ inline fdtd_material blank_material(int kind) {
 }
 }  // namespace detail
 
-// YeeUpdate<Mode, Flux> (include/YeeUpdates.hpp:343-405); BD1 only
-template <class Mode, class Flux>
+// Time policies of the curl update (include/YeeUpdates.hpp:182-294). The
+// TFSF corrections of a grid follow the policy of its YeeUpdates, as a
+// TFSFPlane<..., TimePolicy> built with the same policy does.
+struct TemporalScheme {};
+struct BD1 : TemporalScheme { static constexpr int value = FDTD_BD1; };
+struct BD3 : TemporalScheme { static constexpr int value = FDTD_BD3; };
+struct BD4 : TemporalScheme { static constexpr int value = FDTD_BD4; };
+
+// YeeUpdate<Mode, Flux, TimePolicy> (include/YeeUpdates.hpp:343-405); BD3
+// and BD4 on FP64 grids only
+template <class Mode, class Flux, class TimePolicy = BD1>
 struct YeeUpdate {
   static_assert(Flux::flux, "YeeUpdate acts on a flux component (D or B)");
+  static_assert(std::is_base_of<TemporalScheme, TimePolicy>::value, "YeeUpdate needs a valid TemporalScheme");
   double dt, dx;
   YeeUpdate(double deltat, double deltax) : dt(deltat), dx(deltax) {}
   operator detail::Op() const {
     detail::Op o{detail::OpKind::Yee};
     o.ft = Flux::field_type;
     o.comp = Flux::comp;
+    o.scheme = TimePolicy::value;
     return o;
   }
 };
@@ -354,6 +367,51 @@ TFSFPlaneSpec make_tfsf_plane(std::array<int, 3> lo, std::array<int, 3> hi, std:
   return p;
 }
 
+// make_pec_boundary / make_pmc_boundary / make_symmetric_boundary /
+// make_antisymmetric_boundary / make_periodic_boundary<Mode, d, o>
+// (include/BoundaryUpdates.hpp:529-830) over the interior cells next to the
+// face (d, o); the periodic partner is the interior cell at the far end of
+// the axis. Added to a grid, the spec gives the plan ops of updateE() (after
+// the E sources) and updateH() (after the magnetic material update).
+struct BoundarySpec {
+  int axis, side, kind;
+  int index = -1;
+  struct E {
+    int index;
+    operator detail::Op() const {
+      detail::Op o{detail::OpKind::BoundaryE};
+      o.plane = index;
+      return o;
+    }
+  };
+  struct H {
+    int index;
+    operator detail::Op() const {
+      detail::Op o{detail::OpKind::BoundaryH};
+      o.plane = index;
+      return o;
+    }
+  };
+  E updateE() const { return E{index}; }
+  H updateH() const { return H{index}; }
+};
+template <class Mode, Dir d, Orientation o>
+BoundarySpec make_pec_boundary() { return {static_cast<int>(d), o == Orientation::MAX ? 1 : 0, FDTD_BC_PEC}; }
+template <class Mode, Dir d, Orientation o>
+BoundarySpec make_pmc_boundary() { return {static_cast<int>(d), o == Orientation::MAX ? 1 : 0, FDTD_BC_PMC}; }
+template <class Mode, Dir d, Orientation o>
+BoundarySpec make_symmetric_boundary() {
+  return {static_cast<int>(d), o == Orientation::MAX ? 1 : 0, FDTD_BC_SYMMETRIC};
+}
+template <class Mode, Dir d, Orientation o>
+BoundarySpec make_antisymmetric_boundary() {
+  return {static_cast<int>(d), o == Orientation::MAX ? 1 : 0, FDTD_BC_ANTISYMMETRIC};
+}
+template <class Mode, Dir d, Orientation o>
+BoundarySpec make_periodic_boundary() {
+  return {static_cast<int>(d), o == Orientation::MAX ? 1 : 0, FDTD_BC_PERIODIC};
+}
+
 namespace gpu {
 
 // A grid of Mode on one GPU; Real = double for the FP64 plain method, float
@@ -405,6 +463,11 @@ class Grid {
     s.index = nsrc_++;
     return s;
   }
+  BoundarySpec add(BoundarySpec b) {
+    check(fdtd_set_boundary(g_.get(), b.axis, b.side, b.kind));
+    b.index = nbc_++;
+    return b;
+  }
   TFSFPlaneSpec add(TFSFPlaneSpec p) {
     const std::vector<double> v = p.aux->table(max_steps_ + 1);
     check(fdtd_add_tfsf_plane(g_.get(), p.axis, p.orient, p.lo.data(), p.hi.data(), p.origin.data(), p.k.data(),
@@ -439,16 +502,20 @@ class Grid {
   };
 
   // E half: Yee on every E flux, TFSF D, D-target sources, CPML E per axis
-  // in X, Y, Z order, material E, E-target sources; H half: Yee on every B
-  // flux, TFSF B, CPML H, material H (tests/testTM.cpp:102-113).
+  // in X, Y, Z order, material E, E-target sources, boundary updateE; H half:
+  // Yee on every B flux, TFSF B, CPML H, material H, boundary updateH
+  // (tests/testTM.cpp:102-113). Every YeeUpdate takes one time policy.
   void validate() {
     size_t q = 0;
     auto fail = [](const std::string& m) { throw Error(FDTD_ERR_UNSUPPORTED, "plan: " + m); };
+    int scheme = -1;
     for (int half = 0; half < 2; half++) {
       const FieldType ft = half == 0 ? FieldType::Electric : FieldType::Magnetic;
       bool seen[3] = {false, false, false};
       while (q < plan_.size() && plan_[q].kind == detail::OpKind::Yee && plan_[q].ft == ft) {
         if (seen[plan_[q].comp]) fail("a YeeUpdate appears twice");
+        if (scheme >= 0 && plan_[q].scheme != scheme) fail("every YeeUpdate must take the same time policy");
+        scheme = plan_[q].scheme;
         seen[plan_[q].comp] = true;
         q++;
       }
@@ -480,8 +547,19 @@ class Grid {
       q++;
       if (half == 0)
         while (q < plan_.size() && plan_[q].kind == detail::OpKind::Source && plan_[q].axis == 0) q++;
+      const detail::OpKind bk = half == 0 ? detail::OpKind::BoundaryE : detail::OpKind::BoundaryH;
+      int nb = 0;
+      while (q < plan_.size() && plan_[q].kind == bk) {
+        nb++;
+        q++;
+      }
+      if (nb != nbc_) fail("every boundary must be updated once in each half step");
     }
-    if (q != plan_.size()) fail("operations after the magnetic material update");
+    if (q != plan_.size()) fail("operations after the magnetic boundary updates");
+    if (scheme != scheme_) {
+      check(fdtd_set_time_scheme(g_.get(), scheme));
+      scheme_ = scheme;
+    }
     if (!has_map_) {
       fdtd_material m = mat_e_;
       m.mu_r = mat_h_.mu_r;
@@ -493,7 +571,7 @@ class Grid {
   std::unique_ptr<fdtd_grid, Deleter> g_;
   std::array<int, 3> n_{};
   double dx_, dt_;
-  int max_steps_, steps_ = 0, nsrc_ = 0, nplanes_ = 0;
+  int max_steps_, steps_ = 0, nsrc_ = 0, nplanes_ = 0, nbc_ = 0, scheme_ = FDTD_BD1;
   bool pml_axes_[3] = {false, false, false};
   bool has_map_ = false, validated_ = false;
   std::vector<detail::Op> plan_;

@@ -93,6 +93,8 @@ struct oracle_grid {
   int nbox;
   double* eps_map; /* per-cell relative permittivity of vacuum/constant cells, or NULL */
   int bc[3][2];    /* boundary condition of each face: 0 none, 1..5 (oracle_set_boundary) */
+  int scheme;      /* time policy of the curl updates: 1 BD1, 3 BD3, 4 BD4 */
+  double* hist[2][3][3]; /* [D|B][level][comp]: the flux history BD(level) of BD3/BD4 */
   plane_t* planes;
   int nplanes;
   dft_t* dfts;
@@ -168,6 +170,7 @@ oracle_grid* oracle_create(int mode, int nx, int ny, int nz, double dx, double d
       g->cB[f][a] = zalloc(n); g->cC[f][a] = zalloc(n); g->cF[f][a] = zalloc(n); g->cG[f][a] = zalloc(n);
       for (int i = 0; i < n; i++) g->cF[f][a][i] = 1.0; /* NewPML defaults (PML.hpp:40-55) */
     }
+  g->scheme = 1;
   g->nmat = 1;
   memset(&g->mats[0], 0, sizeof(oracle_material));
   g->mats[0].kind = OR_VACUUM; g->mats[0].eps_inf = 1.0; g->mats[0].mu_r = 1.0;
@@ -190,6 +193,9 @@ void oracle_destroy(oracle_grid* g) {
   for (int s = 0; s < g->nbox; s++) free(g->boxes[s].vals);
   free(g->boxes);
   free(g->eps_map);
+  for (int f = 0; f < 2; f++)
+    for (int l = 0; l < 3; l++)
+      for (int c = 0; c < 3; c++) free(g->hist[f][l][c]);
   for (int p = 0; p < g->nplanes; p++) {
     plane_t* pl = &g->planes[p];
     free(pl->Dz); free(pl->Ez); free(pl->By); free(pl->Hy); free(pl->psiE); free(pl->psiH); free(pl->vals);
@@ -324,6 +330,51 @@ static void apply_boundaries(oracle_grid* g, int ft) {
             }
           }
     }
+}
+
+int oracle_set_time_scheme(oracle_grid* g, int scheme) {
+  if (scheme != 1 && scheme != 3 && scheme != 4) return -1;
+  int levels = scheme == 1 ? 0 : scheme - 1;
+  for (int f = 0; f < 2; f++)
+    for (int l = 0; l < 3; l++)
+      for (int c = 0; c < 3; c++) {
+        free(g->hist[f][l][c]);
+        g->hist[f][l][c] = l < levels ? zalloc(g->ncell) : NULL;
+      }
+  g->scheme = scheme;
+  return 0;
+}
+
+/* curl_coeff of the time policy (YeeUpdates.hpp:185, :206, :255) */
+static double curl_coeff(int scheme) { return scheme == 3 ? 24.0 / 23.0 : scheme == 4 ? 24.0 / 22.0 : 1.0; }
+
+/* YeeUpdate::update_all (YeeUpdates.hpp:396-405) for flux F[c] of field type
+ * ft with the summed curl terms `curl`: F = TimePolicy::get(F) + Coeff *
+ * curl_coeff * dt * curl, then TimePolicy::increment shifts the history
+ * (BD3: :209-213, :231-236; BD4: :258-263, :282-288). */
+static void yee_flux(oracle_grid* g, int ft, int I, size_t c, double curl) {
+  double* F = ft == 0 ? g->D[I] : g->B[I];
+  double coeff = ft == 0 ? 1.0 : -1.0;
+  double hold = F[c];
+  if (g->scheme == 1) {
+    F[c] = F[c] + coeff * 1.0 * g->dt * curl;
+    return;
+  }
+  double* h0 = g->hist[ft][0][I];
+  double* h1 = g->hist[ft][1][I];
+  if (g->scheme == 3) {
+    double get = 21.0 / 23.0 * F[c] + 3.0 / 23.0 * h0[c] - 1.0 / 23.0 * h1[c];
+    F[c] = get + coeff * (24.0 / 23.0) * g->dt * curl;
+    h1[c] = h0[c];
+    h0[c] = hold;
+  } else {
+    double* h2 = g->hist[ft][2][I];
+    double get = 17.0 / 22.0 * F[c] + 9.0 / 22.0 * h0[c] - 5.0 / 22.0 * h1[c] + 1.0 / 22.0 * h2[c];
+    F[c] = get + coeff * (24.0 / 22.0) * g->dt * curl;
+    h2[c] = h1[c];
+    h1[c] = h0[c];
+    h0[c] = hold;
+  }
 }
 
 int oracle_set_eps_map(oracle_grid* g, const double* eps) {
@@ -465,7 +516,7 @@ static void tfsf_cell(oracle_grid* g, plane_t* p, int ft, int I, int i, int j, i
   }
   double coeff = ft == 0 ? 1.0 : -1.0;
   double* F = ft == 0 ? g->D[I] : g->B[I];
-  F[c] += coeff * 1.0 * g->dt * (terms[0] + terms[1]);
+  F[c] += coeff * curl_coeff(g->scheme) * g->dt * (terms[0] + terms[1]);
 }
 
 static void tfsf_apply(oracle_grid* g, int ft) {
@@ -561,7 +612,7 @@ static void step_half(oracle_grid* g, int phase) {
             double diff = g->H[K][c] - g->H[K][c - str[J]];
             a[q] = lc(I, J, K) * g->cF[0][J][idx[J]] / (dx) * diff;
           }
-          g->D[I][c] = g->D[I][c] + 1.0 * 1.0 * dt * (a[0] + a[1]);
+          yee_flux(g, 0, I, c, a[0] + a[1]);
         }
       }
   tfsf_apply(g, 0);
@@ -663,7 +714,7 @@ h_half:
             double diff = g->E[K][c + str[J]] - g->E[K][c];
             a[q] = lc(I, J, K) * g->cF[1][J][idx[J]] / (dx) * diff;
           }
-          g->B[I][c] = g->B[I][c] + -1.0 * 1.0 * dt * (a[0] + a[1]);
+          yee_flux(g, 1, I, c, a[0] + a[1]);
         }
       }
   tfsf_apply(g, 1);
@@ -774,7 +825,7 @@ int oracle_set(oracle_grid* g, int which, const double* in) {
  * materials with mu_r = 1, no TFSF planes. Test infrastructure only. */
 int oracle_adjoint_tm(oracle_grid* g, int nsteps, const int* plo, const int* phi, double freq, const int* dlo,
                       const int* dhi, double* J_out, double* grad) {
-  if (g->mode != TM || g->t != 0 || g->nplanes > 0 || nsteps < 1) return -1;
+  if (g->mode != TM || g->t != 0 || g->nplanes > 0 || nsteps < 1 || g->scheme != 1) return -1;
   for (int m = 0; m < g->nmat; m++)
     if (g->mats[m].kind > OR_CONSTANT || g->mats[m].mu_r != 1.0) return -1;
   for (int d = 0; d < 2; d++)

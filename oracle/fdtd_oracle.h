@@ -54,6 +54,10 @@ int oracle_set_eps_map(oracle_grid* g, const double* eps);
  * zero), 1 PEC, 2 PMC, 3 symmetric, 4 antisymmetric, 5 periodic; applied
  * after the sources of each half step */
 int oracle_set_boundary(oracle_grid* g, int axis, int side, int kind);
+/* time policy of every curl update and TFSF correction
+ * (include/YeeUpdates.hpp:182-294): 1 BD1 (leapfrog, the default), 3 BD3,
+ * 4 BD4; the flux history starts at zero */
+int oracle_set_time_scheme(oracle_grid* g, int scheme);
 /* One TFSF plane (include/Source.hpp:472-634) with its own Aux1D grid.
  * axis/orient give the normal; lo/hi are inclusive cell ranges; origin (in
  * cells) and k define the location functor and wave vector; pol_e / pol_h are

@@ -70,6 +70,7 @@ def lib():
         L.oracle_step.argtypes = [vp, ctypes.c_int]
         L.oracle_step_half.argtypes = [vp, ctypes.c_int]
         L.oracle_set_boundary.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_set_time_scheme.argtypes = [vp, ctypes.c_int]
         L.oracle_get.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_set.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_dft_get.argtypes = [vp, ctypes.c_int, dp]
@@ -119,6 +120,8 @@ class OracleGrid:
             assert L.oracle_set_pml(self.h, a, s, n) == 0
         for (a, s), kind in sorted(p.boundaries.items()):
             assert L.oracle_set_boundary(self.h, a, s, BOUNDARY_KINDS[kind]) == 0
+        if p.time_scheme != 1:
+            assert L.oracle_set_time_scheme(self.h, p.time_scheme) == 0
         if len(p.materials) > 256:
             raise ValueError("the oracle takes at most 256 materials")
         mats = (OracleMaterial * len(p.materials))(*[_mat_struct(m) for m in p.materials])
@@ -154,6 +157,9 @@ class OracleGrid:
             hnd = L.oracle_add_dft(self.h, r.comp, _ip(r.lo), _ip(r.hi), _dp(fr), len(fr))
             assert hnd >= 0
             self.dft_handles.append(hnd)
+
+    def set_time_scheme(self, scheme: int) -> None:
+        assert lib().oracle_set_time_scheme(self.h, int(scheme)) == 0
 
     def step(self, n: int) -> None:
         lib().oracle_step(self.h, n)
@@ -277,6 +283,8 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
             lines.append(f"nbc {len(p.boundaries)}")
             for (a, sd), kind in sorted(p.boundaries.items()):
                 lines.append(f"{a} {sd} {BOUNDARY_KINDS[kind]}")
+        if p.time_scheme != 1:
+            lines.append(f"scheme {p.time_scheme}")
         lines.append(f"steps {steps}")
         op = os.path.join(td, "out.bin")
         lines.append(f"out {op}")

@@ -16,6 +16,10 @@
 //    argument order as :272-280.
 //  * `static constexpr double val` (:370, :745, :1047) is ODR-used; C++17
 //    makes it implicitly inline.
+//  * BD3::get and BD3::get_reverse (include/YeeUpdates.hpp:209-221) take the
+//    cell by const reference and call BD(i) on it, but BDFields
+//    (include/YeeFields.hpp:188-200) only has a non-const BD(i); the history
+//    mixin below is BDFields with a const BD(i) added.
 //
 // Scenario file (whitespace separated tokens, see oracle/pyoracle.py writer):
 //   mode <0 TEM|1 TE|2 TM|3 ThreeD>
@@ -33,6 +37,8 @@
 //        axis orient i0 i1 j0 j1 k0 k1 (inclusive). set_pol 0 keeps the
 //        plane's own polarisation (TE/TM defaults), 1 sets pe/ph.
 //        aux_path: float64 per aux step (value for aux step s at index s-1)
+//   scheme S (optional; 1 BD1 (default), 3 BD3, 4 BD4: the TimePolicy of
+//        every YeeUpdate and TFSFPlane, include/YeeUpdates.hpp:182-294)
 //   nbc B then B lines: axis side kind (optional; kind 1 PEC, 2 PMC,
 //        3 symmetric, 4 antisymmetric, 5 periodic), applied with the
 //        reference's make_*_boundary (include/BoundaryUpdates.hpp) to the
@@ -109,6 +115,7 @@ struct BcSpec { int axis, side, kind; };
 
 struct Scenario {
   int mode = 2, nx = 1, ny = 1, nz = 1;
+  int scheme = 1;
   double dx = 1, dt = 1;
   int pml[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   std::vector<Mat> mats;
@@ -122,11 +129,28 @@ struct Scenario {
   std::string out;
 };
 
+// History of the multi-step time policies: the reference's BDFields with a
+// const accessor (see the compile fixes above).
+template <int n, class Mode>
+struct History : public BDFields<n, Mode, double> {
+  typedef BDFields<n, Mode, double> Base;
+  using Base::BD;
+  const typename Base::Fields& BD(int i) const { return const_cast<History*>(this)->Base::BD(i); }
+};
+struct NoHistory {};
+template <class TP> struct Levels { static constexpr int n = 0; };
+template <> struct Levels<BD3> { static constexpr int n = 2; };
+template <> struct Levels<BD4> { static constexpr int n = 3; };
+template <class Mode, class TP>
+using HistoryOf = std::conditional_t<Levels<TP>::n == 0, NoHistory, History<(Levels<TP>::n > 0 ? Levels<TP>::n : 1), Mode>>;
+
 // The user-side cell: the reference's YeeCell mixins plus neighbour pointers
-// (the neighbour contract of include/DefaultInterfaces.hpp:66-79).
-template <class Mode>
+// (the neighbour contract of include/DefaultInterfaces.hpp:66-79), and the
+// field history when the time policy needs one.
+template <class Mode, class TP = BD1>
 struct Cell : public YeeCell<YeeFields<Mode, double, std::array>, DoublePolarization<double>,
-                             VacuumMagnetization<double>, NewPML<Mode, double>> {
+                             VacuumMagnetization<double>, NewPML<Mode, double>>,
+              public HistoryOf<Mode, TP> {
   Cell* nmin[3] = {nullptr, nullptr, nullptr};
   Cell* nmax[3] = {nullptr, nullptr, nullptr};
   int ci = 0, cj = 0, ck = 0;
@@ -191,20 +215,20 @@ struct StepSignal {
 };
 
 // Location functor of a TFSF plane: ((i,j,k) - origin) * dx.
-template <class Mode>
+template <class Mode, class TP>
 struct LocF {
   const double* origin;
   double dx;
-  std::array<double, Mode::dim> operator()(PtrIt<Cell<Mode>> it) const {
-    Cell<Mode>& c = *it;
+  std::array<double, Mode::dim> operator()(PtrIt<Cell<Mode, TP>> it) const {
+    Cell<Mode, TP>& c = *it;
     std::array<double, Mode::dim> pt;
     int idx[3] = {c.ci, c.cj, c.ck};
     for (int d = 0; d < Mode::dim; d++) pt[d] = (static_cast<double>(idx[d]) - origin[d]) * dx;
     return pt;
   }
 };
-template <class Mode>
-using PlaneOf = TFSFPlane<Mode, LocF<Mode>, PtrIt<Cell<Mode>>, Aux1D<double>>;
+template <class Mode, class TP>
+using PlaneOf = TFSFPlane<Mode, LocF<Mode, TP>, PtrIt<Cell<Mode, TP>>, Aux1D<double>, TP>;
 
 // TFSFPlane keeps its polarisation vectors private and, for ThreeD, leaves
 // them uninitialised (include/Source.hpp:572-584). The runner sets them
@@ -214,22 +238,23 @@ template <typename Tag, typename Tag::type M>
 struct Rob {
   friend typename Tag::type get(Tag) { return M; }
 };
-template <class Mode>
+template <class Mode, class TP>
 struct PolE {
-  typedef std::array<double, 3> PlaneOf<Mode>::*type;
+  typedef std::array<double, 3> PlaneOf<Mode, TP>::*type;
   friend type get(PolE);
 };
-template <class Mode>
+template <class Mode, class TP>
 struct PolH {
-  typedef std::array<double, 3> PlaneOf<Mode>::*type;
+  typedef std::array<double, 3> PlaneOf<Mode, TP>::*type;
   friend type get(PolH);
 };
-template struct Rob<PolE<TE>, &PlaneOf<TE>::mPolarization>;
-template struct Rob<PolH<TE>, &PlaneOf<TE>::mPolarizationH>;
-template struct Rob<PolE<TM>, &PlaneOf<TM>::mPolarization>;
-template struct Rob<PolH<TM>, &PlaneOf<TM>::mPolarizationH>;
-template struct Rob<PolE<ThreeD>, &PlaneOf<ThreeD>::mPolarization>;
-template struct Rob<PolH<ThreeD>, &PlaneOf<ThreeD>::mPolarizationH>;
+#define FDTD_ROB(M, TP)                                                       \
+  template struct Rob<PolE<M, TP>, &PlaneOf<M, TP>::mPolarization>;           \
+  template struct Rob<PolH<M, TP>, &PlaneOf<M, TP>::mPolarizationH>;
+FDTD_ROB(TE, BD1) FDTD_ROB(TM, BD1) FDTD_ROB(ThreeD, BD1)
+FDTD_ROB(TE, BD3) FDTD_ROB(TM, BD3) FDTD_ROB(ThreeD, BD3)
+FDTD_ROB(TE, BD4) FDTD_ROB(TM, BD4) FDTD_ROB(ThreeD, BD4)
+#undef FDTD_ROB
 
 template <class Mode, class F>
 constexpr bool has_field() {
@@ -252,15 +277,15 @@ double flux_or_zero(C& c) {
   else return 0.0;
 }
 
-template <class Mode, class Flux, class C> void yee(C& c, double dt, double dx) {
+template <class Mode, class Flux, class TP, class C> void yee(C& c, double dt, double dx) {
   if constexpr (Detail::tuple_contains_type<Flux, typename FieldComponents<Mode>::electric_flux>::value ||
                 Detail::tuple_contains_type<Flux, typename FieldComponents<Mode>::magnetic_flux>::value)
-    YeeUpdate<Mode, Flux>(dt, dx)(c);
+    YeeUpdate<Mode, Flux, TP>(dt, dx)(c);
 }
 
-template <class Mode>
+template <class Mode, class TP>
 static int run(Scenario& s) {
-  typedef Cell<Mode> C;
+  typedef Cell<Mode, TP> C;
   const int nx = s.nx, ny = s.ny, nz = s.nz;
   const int dim = Mode::dim;
   std::vector<C> cells((size_t)nx * ny * nz);
@@ -333,8 +358,8 @@ static int run(Scenario& s) {
   // TFSF planes over one shared 1D auxiliary grid (include/Source.hpp:280-634)
   typedef std::array<double, Mode::dim> PT;
   std::vector<std::vector<C*>> plane_cells(s.planes.size());
-  LocF<Mode> loc{s.origin, dx};
-  typedef PlaneOf<Mode> PlaneT;
+  LocF<Mode, TP> loc{s.origin, dx};
+  typedef PlaneOf<Mode, TP> PlaneT;
   std::vector<std::unique_ptr<PlaneT>> planes;
   if (!s.planes.empty()) {
     PT kv; for (int d = 0; d < Mode::dim; d++) kv[d] = s.kvec[d];
@@ -350,8 +375,8 @@ static int run(Scenario& s) {
       auto aux = std::make_shared<Aux1D<double>>(s.aux_ncells, dx, dt, TableSignal{&s.aux_vals, dt});
       planes.emplace_back(new PlaneT(kv, normal, loc, b, e, aux));
       if (s.set_pol) {
-        (*planes.back()).*get(PolE<Mode>()) = {s.pol_e[0], s.pol_e[1], s.pol_e[2]};
-        (*planes.back()).*get(PolH<Mode>()) = {s.pol_h[0], s.pol_h[1], s.pol_h[2]};
+        (*planes.back()).*get(PolE<Mode, TP>()) = {s.pol_e[0], s.pol_e[1], s.pol_e[2]};
+        (*planes.back()).*get(PolH<Mode, TP>()) = {s.pol_h[0], s.pol_h[1], s.pol_h[2]};
       }
     }
   }
@@ -414,9 +439,9 @@ static int run(Scenario& s) {
   const auto clock0 = std::chrono::steady_clock::now();
   for (int t = 0; t < s.steps; t++) {
     // ---- E half step: curl, TFSF, CPML per axis, material, sources
-    for (C* c : interior) yee<Mode, Dx>(*c, dt, dx);
-    for (C* c : interior) yee<Mode, Dy>(*c, dt, dx);
-    for (C* c : interior) yee<Mode, Dz>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Dx, TP>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Dy, TP>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Dz, TP>(*c, dt, dx);
     for (auto& pl : planes) pl->updateD(dt, dx);
     for (auto& ap : dappliers) ap(static_cast<double>(t));
     if (pmlax[0]) for (C* c : interior) UpdatePML<Mode, FieldType::Electric, Dir::X>(dt, dx)(*c);
@@ -426,9 +451,9 @@ static int run(Scenario& s) {
     for (auto& ap : appliers) ap(static_cast<double>(t));
     for (auto& b : bcs) b.updateE();
     // ---- H half step
-    for (C* c : interior) yee<Mode, Bx>(*c, dt, dx);
-    for (C* c : interior) yee<Mode, By>(*c, dt, dx);
-    for (C* c : interior) yee<Mode, Bz>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Bx, TP>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, By, TP>(*c, dt, dx);
+    for (C* c : interior) yee<Mode, Bz, TP>(*c, dt, dx);
     for (auto& pl : planes) pl->updateB(dt, dx);
     for (auto& ap : bappliers) ap(static_cast<double>(t));
     if (pmlax[0]) for (C* c : interior) UpdatePML<Mode, FieldType::Magnetic, Dir::X>(dt, dx)(*c);
@@ -512,14 +537,22 @@ int main(int argc, char** argv) {
       int m; in >> m;
       s.bcs.resize(m);
       for (auto& b : s.bcs) in >> b.axis >> b.side >> b.kind;
-    } else if (key == "steps") in >> s.steps;
+    } else if (key == "scheme") in >> s.scheme;
+    else if (key == "steps") in >> s.steps;
     else if (key == "out") in >> s.out;
     else { fprintf(stderr, "unknown key %s\n", key.c_str()); return 1; }
   }
-  switch (s.mode) {
-    case 1: return run<TE>(s);
-    case 2: return run<TM>(s);
-    case 3: return run<ThreeD>(s);
+  if (s.scheme != 1 && s.scheme != 3 && s.scheme != 4) { fprintf(stderr, "bad scheme\n"); return 1; }
+  switch (s.mode * 10 + s.scheme) {
+    case 11: return run<TE, BD1>(s);
+    case 13: return run<TE, BD3>(s);
+    case 14: return run<TE, BD4>(s);
+    case 21: return run<TM, BD1>(s);
+    case 23: return run<TM, BD3>(s);
+    case 24: return run<TM, BD4>(s);
+    case 31: return run<ThreeD, BD1>(s);
+    case 33: return run<ThreeD, BD3>(s);
+    case 34: return run<ThreeD, BD4>(s);
     default: fprintf(stderr, "mode %d not supported\n", s.mode); return 1;
   }
 }

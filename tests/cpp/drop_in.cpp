@@ -1,7 +1,9 @@
 // The reference's time loop written against fdtd_b200.hpp (the drop-in
-// layer), run on the GPU. Usage: drop_in <tm|td> <out.bin>
+// layer), run on the GPU. Usage: drop_in <tm|bd|td> <out.bin>
 //   tm: 2D TM, FP64 plain, 40 x 36, 6-cell CPML, Gaussian soft source on Ez
 //       (the user loop of tests/testTM.cpp with the reference's names);
+//   bd: 2D TM, FP64 plain, 36 x 30, BD3 time policy, PEC face at x min,
+//       CPML at x max, periodic faces in y;
 //   td: 3D, FP32 fused, 24^3, 4-cell CPML, Drude cube in a material map,
 //       x-propagating TFSF box (6 planes) with an Aux1D Gaussian.
 // Writes the listed fields (float64, x fastest) to out.bin.
@@ -50,6 +52,40 @@ int main(int argc, char** argv) {
       // a plan out of the fused order is refused
       try {
         grid.plan({VacuumUpdate<TM, FieldType::Electric>(), YeeUpdate<TM, Dz>(dt, dx)});
+        return 3;
+      } catch (const gpu::Error& e) {
+        if (e.code != FDTD_ERR_UNSUPPORTED) return 4;
+      }
+    } else if (!strcmp(argv[1], "bd")) {
+      const double dt = 0.5 / std::sqrt(2.0) * dx / c0;
+      const int steps = 90;
+      gpu::Grid<TM, double> grid(36, 30, 1, dx, dt, steps);
+      grid.set_pml(Dir::X, Orientation::MAX, 6);
+      auto pec = grid.add(make_pec_boundary<TM, Dir::X, Orientation::MIN>());
+      auto ylo = grid.add(make_periodic_boundary<TM, Dir::Y, Orientation::MIN>());
+      auto yhi = grid.add(make_periodic_boundary<TM, Dir::Y, Orientation::MAX>());
+      auto gauss = [dt](double t) { const double n = std::round(t / dt); return std::exp(-((n - 20.0) / 6.0) * ((n - 20.0) / 6.0)); };
+      auto src = grid.add(make_soft_source<Ez>(gauss, grid.cell(10, 8)));
+      grid.plan({YeeUpdate<TM, Dz, BD3>(dt, dx),
+                 UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Electric>(),
+                 src,
+                 pec.updateE(), ylo.updateE(), yhi.updateE(),
+                 YeeUpdate<TM, Bx, BD3>(dt, dx), YeeUpdate<TM, By, BD3>(dt, dx),
+                 UpdatePML<TM, FieldType::Magnetic, Dir::X>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Magnetic>(),
+                 pec.updateH(), ylo.updateH(), yhi.updateH()});
+      grid.step(steps);
+      dump(out, grid.get<Ez>());
+      dump(out, grid.get<Hx>());
+      dump(out, grid.get<Hy>());
+      // mixed time policies are refused
+      try {
+        grid.plan({YeeUpdate<TM, Dz, BD3>(dt, dx), UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx),
+                   VacuumUpdate<TM, FieldType::Electric>(), pec.updateE(), ylo.updateE(), yhi.updateE(),
+                   YeeUpdate<TM, Bx, BD4>(dt, dx), YeeUpdate<TM, By, BD4>(dt, dx),
+                   UpdatePML<TM, FieldType::Magnetic, Dir::X>(dt, dx), VacuumUpdate<TM, FieldType::Magnetic>(),
+                   pec.updateH(), ylo.updateH(), yhi.updateH()});
         return 3;
       } catch (const gpu::Error& e) {
         if (e.code != FDTD_ERR_UNSUPPORTED) return 4;

@@ -257,6 +257,35 @@ def td_boundaries() -> Problem:
     return p
 
 
+def _time_scheme(p: Problem, scheme: int, name: str) -> Problem:
+    """`p` stepped with the BD3/BD4 time policy at half the Courant limit
+    (both diverge near the limit); materials keep their rates."""
+    p.time_scheme = scheme
+    p.dt = courant_dt(p.dx, 0.5 / math.sqrt(p.dim))
+    p.name = name
+    return p
+
+
+def tm_bd3_tfsf() -> Problem:
+    """BD3 with a TFSF box, CPML and the reference's TM polarisation."""
+    return _time_scheme(tm_tfsf_reference_polarisation(), 3, "tm_bd3_tfsf")
+
+
+def te_bd4_materials() -> Problem:
+    """BD4 through constant, Drude and Lorentz cells with CPML."""
+    return _time_scheme(te_materials(), 4, "te_bd4_materials")
+
+
+def td_bd3_tfsf() -> Problem:
+    """3D BD3 with a TFSF box around a Drude cube."""
+    return _time_scheme(td_tfsf_box(), 3, "td_bd3_tfsf")
+
+
+def td_bd4_boundaries() -> Problem:
+    """3D BD4 with periodic, symmetric, PMC and PEC faces and H sources."""
+    return _time_scheme(td_boundaries(), 4, "td_bd4_boundaries")
+
+
 def tm_adjoint_small(n: int = 40, steps: int = 260, design: int = 8, seed: int = 1):
     """The adjoint workload at a size the CPU oracle runs in well under a
     second: TM, 6-cell CPML, a central design box of random eps_r in [1, 12],
@@ -290,5 +319,10 @@ def objective_problem(p, spec):
 # scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
                        te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources,
-                       tm_boundaries, te_boundaries, td_boundaries]
+                       tm_boundaries, te_boundaries, td_boundaries, tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf,
+                       td_bd4_boundaries]
+# scenarios on the BD3/BD4 time policies (FP64 plain method only)
+MULTISTEP_SCENARIOS = [tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf, td_bd4_boundaries]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]
+# scenarios the FP32 fused method runs (it steps with the leapfrog only)
+LEAPFROG_SCENARIOS = [m for m in ALL_SCENARIOS if m not in MULTISTEP_SCENARIOS]

@@ -51,3 +51,19 @@ def test_3d_fused_material_map_tfsf_through_templates(drop_in, oracle, tmp_path)
     got = run(drop_in, "td", tmp_path, 6, (24, 24, 24))
     for q, name in enumerate(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]):
         assert rel_l2(got[q], o.get(name)) <= 1e-4, name
+
+
+def test_tm_bd3_boundaries_through_templates(drop_in, oracle, tmp_path):
+    """YeeUpdate<TM, F, BD3> and make_pec/periodic_boundary through the C++
+    layer equal the oracle's BD3 step with the same faces."""
+    from fdtd_b200.problem import TM, Problem, Source, courant_dt
+    p = Problem(TM, (36, 30, 1), 1e-6, courant_dt(1e-6, 0.5 / math.sqrt(2.0)))
+    p.pml[(0, 1)] = 6
+    p.boundaries = {(0, 0): "pec", (1, 0): "periodic", (1, 1): "periodic"}
+    p.time_scheme = 3
+    n = np.arange(90, dtype=np.float64)
+    p.sources.append(Source(2, (10, 8, 0), np.exp(-(((n - 20.0) / 6.0) ** 2)), "E"))
+    o = oracle.run_oracle(p, 90)
+    got = run(drop_in, "bd", tmp_path, 3, (1, 30, 36))
+    for q, name in enumerate(["Ez", "Hx", "Hy"]):
+        assert rel_l2(got[q], o.get(name)) <= 1e-12, name

@@ -62,7 +62,7 @@ def test_plain_f64_bitwise_fields(fdtd, oracle, make):
         assert np.array_equal(g.get(n), o.get(n)), n
 
 
-@pytest.mark.parametrize("make", scenarios.ALL_SCENARIOS, ids=lambda f: f.__name__)
+@pytest.mark.parametrize("make", scenarios.LEAPFROG_SCENARIOS, ids=lambda f: f.__name__)
 def test_fused_f32_matches_oracle(fdtd, oracle, make):
     p = make()
     o = oracle.run_oracle(p)
@@ -74,7 +74,7 @@ def test_fused_f32_matches_oracle(fdtd, oracle, make):
 
 
 @pytest.mark.parametrize("sweep", ["regs", "tma", "flat", "staged"])
-@pytest.mark.parametrize("make", [m for m in scenarios.ALL_SCENARIOS if m().mode == 3], ids=lambda f: f.__name__)
+@pytest.mark.parametrize("make", [m for m in scenarios.LEAPFROG_SCENARIOS if m().mode == 3], ids=lambda f: f.__name__)
 def test_fused_3d_sweep_kernels(fdtd, oracle, make, sweep):
     """Every 3D FP32 sweep implementation (register prefetch, TMA pipeline,
     flat) meets the bar and reports no device-side error."""
@@ -87,6 +87,39 @@ def test_fused_3d_sweep_kernels(fdtd, oracle, make, sweep):
     assert g.error_flags() == 0
     E, H, _, _ = mode_fields(p.mode)
     _compare(p, g, o, E + H, FUSED_TOL)
+
+
+def test_multistep_schemes_are_fp64_only(fdtd):
+    p = scenarios.tm_bd3_tfsf()
+    with pytest.raises(fdtd.FdtdError):
+        fdtd.Grid.from_problem(p, "f32")
+    g = fdtd.Grid(p.mode, p.shape, p.dx, p.dt, "f32")
+    g.set_time_scheme(1)
+    with pytest.raises(fdtd.FdtdError):
+        g.set_time_scheme(2)
+
+
+def test_multistep_split_steps_and_reset(fdtd, oracle):
+    """BD4 history survives split fdtd_step calls and graph chunks; setting
+    the scheme again clears it, as on the oracle."""
+    p = scenarios.td_bd4_boundaries()
+    g1 = fdtd.Grid.from_problem(p, "f64")
+    g1.step(p.steps)
+    g2 = fdtd.Grid.from_problem(p, "f64")
+    g2.step(13)
+    g2.step(p.steps - 13)
+    for n in ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]:
+        assert np.array_equal(g1.get(n), g2.get(n)), n
+    o = oracle.OracleGrid(p)
+    o.step(9)
+    g3 = fdtd.Grid.from_problem(p, "f64")
+    g3.step(9)
+    o.set_time_scheme(3)
+    g3.set_time_scheme(3)
+    o.step(11)
+    g3.step(11)
+    for n in ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]:
+        assert np.array_equal(g3.get(n), o.get(n)), n
 
 
 def test_split_steps_equal_one_call(fdtd, oracle):

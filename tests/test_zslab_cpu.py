@@ -16,7 +16,7 @@ from fdtd_b200 import problem as P
 from fdtd_b200.zslab import ZSlabRank, local_problem, merge_dfts, partition_z
 
 CASES = [scenarios.td_tfsf_box, scenarios.td_drude_lorentz, scenarios.td_box_sources, scenarios.td_h_sources,
-         scenarios.td_lorentz_two_pole_blocks, scenarios.td_boundaries]
+         scenarios.td_lorentz_two_pole_blocks, scenarios.td_boundaries, scenarios.td_bd4_boundaries]
 
 
 @pytest.mark.parametrize("make", CASES, ids=lambda f: f.__name__)
