@@ -442,19 +442,62 @@ int build_aux(fdtd_grid* g, AuxH& a) {
                     std::max<size_t>(1, a.vals.size()) * sizeof(double));
 }
 
+// Quantities by code (fdtd_add_dft, fdtd_read_quantity): 0..2 E, 3..5 H,
+// 6..8 Je, 9..11 Jh, 12 rho. Phase 0 samples after the E half (E, Jh, rho),
+// phase 1 after the H half (H, Je).
+int quantity_phase(int q) { return (q >= 3 && q < 9) ? 1 : 0; }
+
+bool quantity_in_mode(const fdtd_grid* g, int q) {
+  const int m = g->d.mode;
+  if (q < 0 || q > 12) return false;
+  if (q < 3) return hasE(m, q);
+  if (q < 6) return hasH(m, q - 3);
+  if (q < 9) return hasE(m, q - 6);
+  if (q < 12) return hasH(m, q - 9);
+  return m != FDTD_TM;
+}
+
+int quantity_check(const fdtd_grid* g, int q, const int* lo, const int* hi) {
+  if (q < 0 || q > 12) return fail(FDTD_ERR_INVALID, "quantity must be 0..12");
+  if (!quantity_in_mode(g, q)) return fail(FDTD_ERR_INVALID, "quantity not in this mode");
+  const int dim = dim_of(g);
+  for (int d = 0; d < 3; d++) {
+    if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return fail(FDTD_ERR_INVALID, "box outside the grid");
+    if (q >= 6 && d < dim && (lo[d] < 1 || hi[d] > g->n[d] - 2))
+      return fail(FDTD_ERR_INVALID, "surface quantities are defined on interior cells only");
+  }
+  return FDTD_OK;
+}
+
+// the device description of quantity q over lo..hi
+DftRegionDev quantity_region(const fdtd_grid* g, int q, const int* lo, const int* hi) {
+  DftRegionDev o{};
+  o.mode = g->d.mode;
+  o.kind = q < 6 ? 0 : q < 9 ? 1 : q < 12 ? 2 : 3;
+  o.comp = q < 12 ? q % 3 : 0;
+  const double dx = g->d.dx;
+  // SurfaceQuantities.hpp:211, :265, :324: 1.0/dx, -1.0/dx, eps0/dx; the
+  // FP32 method stores eta*H, so Je takes a further 1/eta
+  if (o.kind == 1) o.scale = g->f32 ? 1.0 / dx / eta() : 1.0 / dx;
+  else if (o.kind == 2) o.scale = -1.0 / dx;
+  else if (o.kind == 3) o.scale = kEps0 / dx;
+  o.npts = 1;
+  for (int d = 0; d < 3; d++) {
+    o.lo[d] = lo[d];
+    o.ext[d] = hi[d] - lo[d] + 1;
+    o.npts *= o.ext[d];
+  }
+  return o;
+}
+
 int rebuild_dft(fdtd_grid* g) {
   for (int ph = 0; ph < 2; ph++) {
     std::vector<DftRegionDev> v;
     long long off = 0;
     for (auto& r : g->dfts) {
-      if ((r.comp < 3) != (ph == 0)) continue;
-      DftRegionDev o{};
-      o.comp = r.comp % 3;
+      if (quantity_phase(r.comp) != ph) continue;
+      DftRegionDev o = quantity_region(g, r.comp, r.lo, r.hi);
       o.nf = r.nf;
-      for (int d = 0; d < 3; d++) {
-        o.lo[d] = r.lo[d];
-        o.ext[d] = r.hi[d] - r.lo[d] + 1;
-      }
       o.npts = r.npts;
       o.pt_off = off;
       o.freqs = r.d_freqs;
@@ -1010,9 +1053,8 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
 
 int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) {
   if (!g || !lo || !hi || !freqs || !handle) return fail(FDTD_ERR_INVALID, "null argument");
-  if (comp < 0 || comp > 5) return fail(FDTD_ERR_INVALID, "comp must be 0..5");
-  if (comp < 3 ? !hasE(g->d.mode, comp) : !hasH(g->d.mode, comp - 3))
-    return fail(FDTD_ERR_INVALID, "component not in this mode");
+  const int qc = quantity_check(g, comp, lo, hi);
+  if (qc != FDTD_OK) return qc;
   if (nf < 1) return fail(FDTD_ERR_INVALID, "nf must be >= 1");
   DftH r;
   r.comp = comp;
@@ -1053,7 +1095,7 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
   CK(cudaStreamSynchronize(g->stream));
   CK(cudaMemcpy(out, r.d_acc, n * sizeof(double), cudaMemcpyDeviceToHost));
-  if (g->f32 && r.comp >= 3) {
+  if (g->f32 && r.comp >= 3 && r.comp < 6) {
     const double s = 1.0 / eta();  // stored H is eta*H
     for (size_t q = 0; q < n; q++) out[q] *= s;
   }
@@ -1378,6 +1420,37 @@ static int locate(fdtd_grid* g, int which, void** p, double* scale, int* psi_axi
     *psi_axis = J;
     if (g->f32) *scale = ft == 0 ? eps0 / dt : kMu0 / (eta() * dt);
   }
+  return FDTD_OK;
+}
+
+int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double* host) {
+  if (!g || !lo || !hi || !host) return fail(FDTD_ERR_INVALID, "null argument");
+  const int qc = quantity_check(g, q, lo, hi);
+  if (qc != FDTD_OK) return qc;
+  CK(cudaSetDevice(g->d.device));
+  const DftRegionDev r = quantity_region(g, q, lo, hi);
+  if (r.npts >= (1LL << 31)) return fail(FDTD_ERR_UNSUPPORTED, "a box holds at most 2^31 - 1 cells");
+  if (!g->d_fieldptrs) return fail(FDTD_ERR_INVALID, "grid has no fields");
+  // a scratch of its own: the grid's tracked allocations would invalidate
+  // its captured step graphs
+  void* buf = nullptr;
+  cudaError_t ae = cudaMalloc(&buf, static_cast<size_t>(r.npts) * elem(g));
+  if (ae != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ae == cudaErrorMemoryAllocation ? FDTD_ERR_NOMEM : FDTD_ERR_CUDA, cudaGetErrorString(ae));
+  }
+  const void* const* fields = reinterpret_cast<const void* const*>(g->d_fieldptrs) + (quantity_phase(q) == 0 ? 0 : 3);
+  g->launches += launch_quantity_read(g->f32 ? 1 : 0, r, fields, g->n[1], static_cast<int>(rowlen(g)), buf, g->stream);
+  std::vector<char> h(static_cast<size_t>(r.npts) * elem(g));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), buf, h.size(), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
+  const double hs = (g->f32 && q >= 3 && q < 6) ? 1.0 / eta() : 1.0;  // stored H is eta*H
+  for (long long p = 0; p < r.npts; p++)
+    host[p] = g->f32 ? static_cast<double>(reinterpret_cast<float*>(h.data())[p]) * hs
+                     : reinterpret_cast<double*>(h.data())[p];
   return FDTD_OK;
 }
 

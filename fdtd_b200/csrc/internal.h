@@ -170,6 +170,11 @@ struct FusedArgs {
 
 struct DftRegionDev {
   int comp, nf;
+  // quantity: kind 0 a field component (comp of the phase's E or H), 1 the
+  // surface current Je, 2 Jh, 3 the surface charge density rho (comp 0);
+  // mode the grid's EM mode; scale the factor of the derived quantities
+  int kind, mode;
+  double scale;
   int lo[3], ext[3];
   long long npts, pt_off;
   const double* freqs;
@@ -219,6 +224,9 @@ int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, d
                           long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);
 int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
                       const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s);
+// one quantity over a box into out (npts values of the field precision)
+int launch_quantity_read(int precision, const DftRegionDev& r, const void* const* fields, int ny, int pitch,
+                         void* out, cudaStream_t s);
 int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
                      long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s);
 int launch_dft_rebase(Control* ctrl, cudaStream_t s);

@@ -16,6 +16,55 @@ namespace fdtdb {
 // and writes each 16-byte accumulator once per chunk instead of once per step.
 // One grid row (blockIdx.y) per region: the region is uniform over the
 // block, and point indices within a region fit 32 bits.
+// One quantity of cell c. f holds the phase's three field arrays (E for
+// kinds 0, 2, 3 of the E phase; H for kinds 0, 1 of the H phase). The
+// surface current Je (UpdateSurfaceCurrentE, SurfaceQuantities.hpp:256-296)
+// reads H at the cell and its lower neighbours, Jh (UpdateSurfaceCurrentH,
+// :315-356) E at the cell and its upper neighbours, rho
+// (UpdateSurfaceChargeDensity, :203-242) E at the cell and its lower
+// neighbours; each sum is formed in the reference's order and multiplied by
+// scale (1/dx, -1/dx, eps0/dx; with 1/eta folded in for the stored eta*H of
+// the FP32 method). The host keeps the boxes of derived kinds in the interior.
+template <typename R>
+__device__ __forceinline__ R quantity_sample(const DftRegionDev& g, const R* const* f, long long c, long long sy,
+                                             long long sz) {
+  const R s = static_cast<R>(g.scale);
+  switch (g.kind) {
+    case 0:
+      return f[g.comp][c];
+    case 1:
+      if (g.mode == kTE) {
+        if (g.comp == 0) return s * (f[2][c] - f[2][c - sy]);
+        return s * (-f[2][c] + f[2][c - 1]);
+      }
+      if (g.comp == 0) return s * (f[2][c] - f[2][c - sy] - f[1][c] + f[1][c - sz]);
+      if (g.comp == 1) return s * (f[0][c] - f[0][c - sz] - f[2][c] + f[2][c - 1]);
+      return s * (f[1][c] - f[1][c - 1] - f[0][c] + f[0][c - sy]);
+    case 2:
+      if (g.mode == kTM) {
+        if (g.comp == 0) return s * (f[2][c + sy] - f[2][c]);
+        return s * (-f[2][c + 1] + f[2][c]);
+      }
+      if (g.comp == 0) return s * (f[2][c + sy] - f[2][c] - f[1][c + sz] + f[1][c]);
+      if (g.comp == 1) return s * (f[0][c + sz] - f[0][c] - f[2][c + 1] + f[2][c]);
+      return s * (f[1][c + 1] - f[1][c] - f[0][c + sy] + f[0][c]);
+    default:
+      if (g.mode == kTE) return s * (f[0][c] + f[1][c] - f[0][c - 1] - f[1][c - sy]);
+      return s * (f[0][c] + f[1][c] + f[2][c] - f[0][c - 1] - f[1][c - sy] - f[2][c - sz]);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ R quantity_at_point(const DftRegionDev& g, const R* const* f, int ny, int pitch, int q) {
+  const int ex = g.ext[0], ey = g.ext[1];
+  const int r = q / ex;
+  const int i = g.lo[0] + (q - r * ex);
+  const int j = g.lo[1] + r % ey;
+  const int k = g.lo[2] + r / ey;
+  const long long sz = static_cast<long long>(ny) * pitch;
+  return quantity_sample(g, f, k * sz + static_cast<long long>(j) * pitch + i, pitch, sz);
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, long long total,
                                                          const R* const* __restrict__ fields, int ny, int pitch,
@@ -23,13 +72,29 @@ __global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __r
   const DftRegionDev& g = regions[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.npts) return;
-  const int ex = g.ext[0], ey = g.ext[1];
-  const int r = q / ex;
-  const int i = g.lo[0] + (q - r * ex);
-  const int j = g.lo[1] + r % ey;
-  const int k = g.lo[2] + r / ey;
   const long long slot = ctrl->t - ctrl->dft_base;
-  buf[slot * total + g.pt_off + q] = fields[g.comp][(static_cast<long long>(k) * ny + j) * pitch + i];
+  buf[slot * total + g.pt_off + q] = quantity_at_point(g, fields, ny, pitch, q);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) quantity_read_kernel(const DftRegionDev g, const R* const* __restrict__ fields,
+                                                            int ny, int pitch, R* out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.npts) return;
+  out[q] = quantity_at_point(g, fields, ny, pitch, q);
+}
+
+int launch_quantity_read(int precision, const DftRegionDev& r, const void* const* fields, int ny, int pitch,
+                         void* out, cudaStream_t s) {
+  if (r.npts == 0) return 0;
+  const unsigned grid = static_cast<unsigned>((r.npts + 255) / 256);
+  if (precision == 0)
+    quantity_read_kernel<double><<<grid, 256, 0, s>>>(r, reinterpret_cast<const double* const*>(fields), ny, pitch,
+                                                      static_cast<double*>(out));
+  else
+    quantity_read_kernel<float><<<grid, 256, 0, s>>>(r, reinterpret_cast<const float* const*>(fields), ny, pitch,
+                                                     static_cast<float*>(out));
+  return 1;
 }
 
 template <typename R>

@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_step", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
            "fdtd_batch_info",
@@ -89,6 +89,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_add_dft": [vp, i, ip, ip, dp, i, ip],
         "fdtd_dft_npoints": [vp, i, llp],
         "fdtd_dft_read": [vp, i, dp],
+        "fdtd_read_quantity": [vp, i, ip, ip, dp],
         "fdtd_step": [vp, i, vp],
         "fdtd_profile_step": [vp, i, vp, dp],
         "fdtd_set_sweep_kernel": [vp, i],
@@ -295,7 +296,30 @@ class Grid:
         _check(load_library().fdtd_synchronize(self.h))
 
     # ------------------------------------------------------------ read back
+    def read_quantity(self, q: int, lo, hi) -> np.ndarray:
+        """Quantity q (P.QUANTITIES: E, H, the surface currents Je, Jh and the
+        surface charge density rho) over the inclusive box lo..hi from the
+        current fields, shape (nz_b, ny_b, nx_b)."""
+        n = [h - l + 1 for l, h in zip(lo, hi)]
+        out = np.empty(n[0] * n[1] * n[2], dtype=np.float64)
+        _check(load_library().fdtd_read_quantity(self.h, int(q), _ip(lo), _ip(hi), _dp(out)))
+        return out.reshape(n[2], n[1], n[0])
+
+    def surface(self, name: str) -> np.ndarray:
+        """Surface quantity `name` (rho, Jex, .., Jhz) on every interior cell,
+        zero elsewhere and where the mode has none."""
+        nx, ny, nz = self.shape
+        out = np.zeros((nz, ny, nx))
+        q = P.QUANTITIES[name]
+        three = self.mode == P.THREED
+        lo, hi = (1, 1, 1 if three else 0), (nx - 2, ny - 2, nz - 2 if three else 0)
+        if P.quantity_in_mode(self.mode, q):
+            out[lo[2]:hi[2] + 1, 1:ny - 1, 1:nx - 1] = self.read_quantity(q, lo, hi)
+        return out
+
     def get(self, name: str) -> np.ndarray:
+        if isinstance(name, str) and name in P.SURFACE_NAMES:
+            return self.surface(name)
         which = ALL_NAMES.index(name) if isinstance(name, str) and name in ALL_NAMES else int(name)
         nx, ny, nz = self.shape
         out = np.empty(nx * ny * nz, dtype=np.float64)

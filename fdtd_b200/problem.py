@@ -124,15 +124,39 @@ class TFSF:
 
 @dataclass
 class DFTRegion:
-    """Running DFT of component comp (0..2 E, 3..5 H) over the inclusive box
-    lo..hi at frequencies freqs (cycles/step). E sampled at the end of the E
-    half of step t carries time index t+1, H at the end of the H half t+1.5;
-    X_f = sum_n x[n] * exp(-2*pi*i*f*n)."""
+    """Running DFT of quantity comp (QUANTITIES: 0..2 E, 3..5 H, 6..8 Je,
+    9..11 Jh, 12 rho) over the inclusive box lo..hi at frequencies freqs
+    (cycles/step). The quantities of E (E, Jh, rho), sampled at the end of
+    the E half of step t, carry time index t+1; those of H (H, Je) t+1.5;
+    X_f = sum_n x[n] * exp(-2*pi*i*f*n). Boxes of surface quantities lie in
+    the interior."""
 
     comp: int
     lo: Tuple[int, int, int]
     hi: Tuple[int, int, int]
     freqs: Sequence[float]
+
+
+# quantity codes of the C ABI (FDTD_Q_*): fields, then the surface quantities
+# of include/SurfaceQuantities.hpp (Je from H, Jh from E, rho from E)
+QUANTITIES = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5, "Jex": 6, "Jey": 7, "Jez": 8,
+              "Jhx": 9, "Jhy": 10, "Jhz": 11, "rho": 12}
+SURFACE_NAMES = ["rho", "Jex", "Jey", "Jez", "Jhx", "Jhy", "Jhz"]
+
+
+def quantity_in_mode(mode: int, q: int) -> bool:
+    """Whether quantity q exists in `mode` (rho: TE and ThreeD)."""
+    has_e = [mode == THREED or (mode == TE and c < 2) or (mode == TM and c == 2) for c in range(3)]
+    has_h = [mode == THREED or (mode == TE and c == 2) or (mode == TM and c < 2) for c in range(3)]
+    if q < 3:
+        return has_e[q]
+    if q < 6:
+        return has_h[q - 3]
+    if q < 9:
+        return has_e[q - 6]
+    if q < 12:
+        return has_h[q - 9]
+    return q == 12 and mode != TM
 
 
 @dataclass

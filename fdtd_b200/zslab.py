@@ -136,6 +136,14 @@ def local_problem(p: P.Problem, z0: int, z1: int) -> P.Problem:
     for gi, r in enumerate(p.dfts):
         c = _clip_box(r.lo, r.hi, z0, z1)
         if c is not None:
+            # Je_x, Je_y and rho read the plane below, Jh_x and Jh_y the plane
+            # above; at a slab boundary that plane is a ghost whose exchange
+            # comes after the half step's DFT sample
+            lo_z, hi_z = c[0][2] + off, c[1][2] + off
+            if r.comp in (6, 7, 12) and z0 > 1 and lo_z == z0:
+                raise ValueError(f"DFT region {gi} of quantity {r.comp} reads the plane below slab boundary {z0}")
+            if r.comp in (9, 10) and z1 < nz - 1 and hi_z == z1 - 1:
+                raise ValueError(f"DFT region {gi} of quantity {r.comp} reads the plane above slab boundary {z1}")
             q.dfts.append(P.DFTRegion(r.comp, c[0], c[1], list(r.freqs)))
             q.dft_map.append(gi)
     return q

@@ -25,6 +25,9 @@
  *     YeeUpdate<Mode,B*>, UpdatePML<Mode,Magnetic,d>,
  *     material H (YeeUpdates.hpp:343-405, PML.hpp:296-355)
  *   reading cell.Ez() etc.                                   fdtd_download / fdtd_upload
+ *   UpdateSurfaceCurrentE/H, UpdateSurfaceChargeDensity      fdtd_read_quantity, and
+ *     on cells, then cell.Jez() etc.                         fdtd_add_dft of FDTD_Q_J*,
+ *     (SurfaceQuantities.hpp:169-356)                        FDTD_Q_RHO
  *
  * Ownership: the grid handle owns all device memory; host pointers passed in
  * are read during the call only. Errors: every call returns FDTD_OK (0) or a
@@ -165,10 +168,34 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
                         const double* origin, const double* k, const double* pol_e, const double* pol_h,
                         int aux_ncells, const double* aux_vals, int naux);
 
-/* Running DFT of comp (0..2 E, 3..5 H) over the inclusive box lo..hi at nf
- * frequencies (cycles per step). X_f = sum_n x[n] exp(-2 pi i f n), with
- * n = t+1 for E at the end of step t's E half and t+1.5 for H. */
+/* Quantities of a cell: the fields and the surface quantities of
+ * SurfaceQuantities<Mode> (include/SurfaceQuantities.hpp:169-356). */
+enum {
+  FDTD_Q_EX = 0, FDTD_Q_EY, FDTD_Q_EZ, FDTD_Q_HX, FDTD_Q_HY, FDTD_Q_HZ,
+  /* UpdateSurfaceCurrentE: Je = curl H / dx on the cell and its lower
+   * neighbours (components of E present in the mode) */
+  FDTD_Q_JEX = 6, FDTD_Q_JEY, FDTD_Q_JEZ,
+  /* UpdateSurfaceCurrentH: Jh = -curl E / dx on the cell and its upper
+   * neighbours (components of H present in the mode) */
+  FDTD_Q_JHX = 9, FDTD_Q_JHY, FDTD_Q_JHZ,
+  /* UpdateSurfaceChargeDensity: rho = eps0 div E / dx (TE and ThreeD; the
+   * reference's TM functor does nothing) */
+  FDTD_Q_RHO = 12
+};
+
+/* Running DFT of quantity comp (FDTD_Q_*) over the inclusive box lo..hi at
+ * nf frequencies (cycles per step). X_f = sum_n x[n] exp(-2 pi i f n), with
+ * n = t+1 for the quantities of E (E, Jh, rho) sampled at the end of step
+ * t's E half and t+1.5 for those of H (H, Je). Boxes of surface quantities
+ * lie in the interior. */
 int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle);
+
+/* Quantity q (FDTD_Q_*) on every cell of the inclusive box lo..hi from the
+ * current fields, x fastest, into host (FP64): the snapshot of applying the
+ * reference's UpdateSurfaceCurrentE / UpdateSurfaceCurrentH /
+ * UpdateSurfaceChargeDensity functors to those cells and reading them back.
+ * Synchronises the grid's stream. */
+int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double* host);
 int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints);
 /* host out: [nf][npoints][2] doubles (re, im), points x fastest */
 int fdtd_dft_read(fdtd_grid* g, int handle, double* out);

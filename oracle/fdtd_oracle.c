@@ -533,11 +533,82 @@ static void tfsf_apply(oracle_grid* g, int ft) {
   }
 }
 
+/* Quantities of a cell, by code: 0..2 E, 3..5 H, 6..8 the surface current
+ * Je (UpdateSurfaceCurrentE, SurfaceQuantities.hpp:256-296), 9..11 Jh
+ * (UpdateSurfaceCurrentH, :315-356), 12 the surface charge density rho
+ * (UpdateSurfaceChargeDensity, :203-242), each in the reference's operation
+ * order. Je reads H at the cell and its lower neighbours, Jh reads E at the
+ * cell and its upper neighbours, rho reads E at the cell and its lower
+ * neighbours. */
+static int quantity_present(const oracle_grid* g, int q) {
+  if (q < 0 || q > 12) return 0;
+  if (q < 3) return g->hasE[q];
+  if (q < 6) return g->hasH[q - 3];
+  if (q < 9) return g->hasE[q - 6];
+  if (q < 12) return g->hasH[q - 9];
+  return g->mode != TM;
+}
+
+static double quantity_at(const oracle_grid* g, int q, size_t c) {
+  const size_t sy = (size_t)g->n[0], sz = (size_t)g->n[0] * g->n[1];
+  const double dx = g->dx;
+  double* const* E = g->E;
+  double* const* H = g->H;
+  if (q < 3) return E[q][c];
+  if (q < 6) return H[q - 3][c];
+  if (q < 9) {
+    if (g->mode == TE) {
+      if (q == 6) return 1.0 / dx * (H[2][c] - H[2][c - sy]);
+      return 1.0 / dx * (-H[2][c] + H[2][c - 1]);
+    }
+    if (q == 6) return 1.0 / dx * (H[2][c] - H[2][c - sy] - H[1][c] + H[1][c - sz]);
+    if (q == 7) return 1.0 / dx * (H[0][c] - H[0][c - sz] - H[2][c] + H[2][c - 1]);
+    return 1.0 / dx * (H[1][c] - H[1][c - 1] - H[0][c] + H[0][c - sy]);
+  }
+  if (q < 12) {
+    if (g->mode == TM) {
+      if (q == 9) return -1.0 / dx * (E[2][c + sy] - E[2][c]);
+      return -1.0 / dx * (-E[2][c + 1] + E[2][c]);
+    }
+    if (q == 9) return -1.0 / dx * (E[2][c + sy] - E[2][c] - E[1][c + sz] + E[1][c]);
+    if (q == 10) return -1.0 / dx * (E[0][c + sz] - E[0][c] - E[2][c + 1] + E[2][c]);
+    return -1.0 / dx * (E[1][c + 1] - E[1][c] - E[0][c + sy] + E[0][c]);
+  }
+  if (g->mode == TE) return k_eps0 / dx * (E[0][c] + E[1][c] - E[0][c - 1] - E[1][c - sy]);
+  return k_eps0 / dx * (E[0][c] + E[1][c] + E[2][c] - E[0][c - 1] - E[1][c - sy] - E[2][c - sz]);
+}
+
+/* the box must lie in the interior (the quantities read +-1 neighbours) */
+static int quantity_box_ok(const oracle_grid* g, int q, const int* lo, const int* hi) {
+  int dim = g->mode == THREED ? 3 : 2;
+  for (int d = 0; d < 3; d++) {
+    if (lo[d] > hi[d]) return 0;
+    if (q < 6) {
+      if (lo[d] < 0 || hi[d] >= g->n[d]) return 0;
+    } else if (d < dim) {
+      if (lo[d] < 1 || hi[d] > g->n[d] - 2) return 0;
+    } else if (lo[d] != 0 || hi[d] != 0) return 0;
+  }
+  return quantity_present(g, q);
+}
+
+int oracle_read_quantity(const oracle_grid* g, int q, const int* lo, const int* hi, double* out) {
+  if (!quantity_box_ok(g, q, lo, hi)) return -1;
+  size_t p = 0;
+  for (int k = lo[2]; k <= hi[2]; k++)
+    for (int j = lo[1]; j <= hi[1]; j++)
+      for (int i = lo[0]; i <= hi[0]; i++) out[p++] = quantity_at(g, q, ((size_t)k * g->n[1] + j) * g->n[0] + i);
+  return 0;
+}
+
+/* phase of a quantity's samples: 0 (after the E half: E, Jh, rho) or 1 (after
+ * the H half: H, Je) */
+static int quantity_phase(int q) { return (q >= 3 && q < 9) ? 1 : 0; }
+
 static void dft_apply(oracle_grid* g, int ft, double n) {
   for (int d = 0; d < g->ndft; d++) {
     dft_t* r = &g->dfts[d];
-    if ((r->comp < 3) != (ft == 0)) continue;
-    const double* x = r->comp < 3 ? g->E[r->comp] : g->H[r->comp - 3];
+    if (quantity_phase(r->comp) != ft) continue;
     for (int f = 0; f < r->nf; f++) {
       double ph = 2.0 * k_pi * r->freqs[f] * n;
       double wr = cos(ph), wi = -sin(ph);
@@ -545,7 +616,7 @@ static void dft_apply(oracle_grid* g, int ft, double n) {
       for (int k = r->lo[2]; k <= r->hi[2]; k++)
         for (int j = r->lo[1]; j <= r->hi[1]; j++)
           for (int i = r->lo[0]; i <= r->hi[0]; i++, p++) {
-            double v = x[((size_t)k * g->n[1] + j) * g->n[0] + i];
+            double v = quantity_at(g, r->comp, ((size_t)k * g->n[1] + j) * g->n[0] + i);
             r->acc[((size_t)f * r->npts + p) * 2] += v * wr;
             r->acc[((size_t)f * r->npts + p) * 2 + 1] += v * wi;
           }
@@ -554,9 +625,11 @@ static void dft_apply(oracle_grid* g, int ft, double n) {
 }
 
 int oracle_add_dft(oracle_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf) {
-  if (comp < 0 || comp > 5 || nf < 1) return -1;
-  for (int d = 0; d < 3; d++)
-    if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return -1;
+  if (comp < 0 || comp > 12 || nf < 1) return -1;
+  if (comp < 6) {
+    for (int d = 0; d < 3; d++)
+      if (lo[d] < 0 || hi[d] >= g->n[d] || lo[d] > hi[d]) return -1;
+  } else if (!quantity_box_ok(g, comp, lo, hi)) return -1;
   g->dfts = (dft_t*)realloc(g->dfts, (g->ndft + 1) * sizeof(dft_t));
   dft_t* r = &g->dfts[g->ndft];
   r->comp = comp; r->nf = nf;

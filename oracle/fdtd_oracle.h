@@ -66,9 +66,15 @@ int oracle_set_time_scheme(oracle_grid* g, int scheme);
 int oracle_add_tfsf_plane(oracle_grid* g, int axis, int orient, const int* lo, const int* hi,
                           const double* origin, const double* kvec, const double* pol_e,
                           const double* pol_h, int aux_ncells, const double* aux_vals, int naux);
-/* Running DFT of one component (0..2 E, 3..5 H) over an inclusive box. */
+/* Running DFT of one quantity over an inclusive box: 0..2 E, 3..5 H, 6..8
+ * the surface current Je (from H, sampled after the H half), 9..11 Jh (from
+ * E), 12 the surface charge density rho (from E; not in TM). */
 int oracle_add_dft(oracle_grid* g, int comp, const int* lo, const int* hi,
                    const double* freqs, int nf);
+/* the quantity (codes as for oracle_add_dft) on every cell of the inclusive
+ * box lo..hi, x fastest, from the current fields; boxes of quantities 6..12
+ * lie in the interior */
+int oracle_read_quantity(const oracle_grid* g, int q, const int* lo, const int* hi, double* out);
 int oracle_step(oracle_grid* g, int nsteps);
 /* one half step: 0 = the E half, 1 = the H half (ends the step); the two
  * must alternate, E first */

@@ -28,7 +28,11 @@ RUNNER_PATH = os.path.join(HERE, "_ref", "ref_runner")
 NAMES = ["Dx", "Dy", "Dz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Hx", "Hy", "Hz",
          "Px", "Py", "Pz", "Jx", "Jy", "Jz"]
 PSI_NAMES = [f"psi{'EH'[f]}{'xyz'[i]}{'xyz'[j]}" for f in range(2) for i in range(3) for j in range(3)]
-ALL_NAMES = NAMES + PSI_NAMES
+# surface quantities (include/SurfaceQuantities.hpp) on every interior cell,
+# by quantity code (oracle_read_quantity): rho 12, Je 6..8, Jh 9..11
+SURFACE_NAMES = ["rho", "Jex", "Jey", "Jez", "Jhx", "Jhy", "Jhz"]
+SURFACE_CODES = {"rho": 12, "Jex": 6, "Jey": 7, "Jez": 8, "Jhx": 9, "Jhy": 10, "Jhz": 11}
+ALL_NAMES = NAMES + PSI_NAMES + SURFACE_NAMES
 
 
 class OracleMaterial(ctypes.Structure):
@@ -80,6 +84,7 @@ def lib():
         L.oracle_add_source_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, dp, ctypes.c_int]
         L.oracle_set_eps_map.argtypes = [vp, dp]
         L.oracle_adjoint_tm.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.c_double, ip, ip, dp, dp]
+        L.oracle_read_quantity.argtypes = [vp, ctypes.c_int, ip, ip, dp]
         _lib = L
     return _lib
 
@@ -175,7 +180,33 @@ class OracleGrid:
         a[k] = plane
         self.set(name, a)
 
+    def read_quantity(self, code: int, lo, hi) -> np.ndarray:
+        """A quantity (0..5 E/H, 6..8 Je, 9..11 Jh, 12 rho) over an inclusive
+        box, shape (nz_b, ny_b, nx_b)."""
+        n = [h - l + 1 for l, h in zip(lo, hi)]
+        out = np.empty(n[0] * n[1] * n[2], dtype=np.float64)
+        rc = lib().oracle_read_quantity(self.h, int(code), _ip(lo), _ip(hi), _dp(out))
+        if rc != 0:
+            raise ValueError("quantity not in this mode or box outside the interior")
+        return out.reshape(n[2], n[1], n[0])
+
+    def surface(self, name: str) -> np.ndarray:
+        """A surface quantity on every interior cell (zero elsewhere, and
+        zero where the mode has none), as the reference runner dumps it."""
+        nx, ny, nz = self.p.shape
+        out = np.zeros((nz, ny, nx))
+        code = SURFACE_CODES[name]
+        three = self.p.mode == 3
+        lo, hi = (1, 1, 1 if three else 0), (nx - 2, ny - 2, nz - 2 if three else 0)
+        try:
+            out[lo[2]:hi[2] + 1, 1:ny - 1, 1:nx - 1] = self.read_quantity(code, lo, hi)
+        except ValueError:
+            pass
+        return out
+
     def get(self, name: str) -> np.ndarray:
+        if name in SURFACE_CODES:
+            return self.surface(name)
         which = ALL_NAMES.index(name) if name in ALL_NAMES else int(name)
         nx, ny, nz = self.p.shape
         out = np.empty(nx * ny * nz, dtype=np.float64)

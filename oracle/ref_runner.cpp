@@ -46,9 +46,13 @@
 //        after the H sources (updateH)
 //   steps N
 //   out path
-// Output: float64 arrays in order D(3) E(3) B(3) H(3) P(3) J(3) and the CPML
-// integrators psi[ft][I][J] (18), each nx*ny*nz long. The wall time of the
-// time loop alone is printed as "loop_seconds <s>".
+// Output: float64 arrays in order D(3) E(3) B(3) H(3) P(3) J(3), the CPML
+// integrators psi[ft][I][J] (18), and the surface quantities rho, Je(3),
+// Jh(3) that UpdateSurfaceChargeDensity, UpdateSurfaceCurrentE and
+// UpdateSurfaceCurrentH (include/SurfaceQuantities.hpp:203-356) give on every
+// interior cell after the last step (zero where the mode has none), each
+// nx*ny*nz long. The wall time of the time loop alone is printed as
+// "loop_seconds <s>".
 #include <fdtd.h>
 #include <cstdio>
 #include <cstdlib>
@@ -150,7 +154,7 @@ using HistoryOf = std::conditional_t<Levels<TP>::n == 0, NoHistory, History<(Lev
 template <class Mode, class TP = BD1>
 struct Cell : public YeeCell<YeeFields<Mode, double, std::array>, DoublePolarization<double>,
                              VacuumMagnetization<double>, NewPML<Mode, double>>,
-              public HistoryOf<Mode, TP> {
+              public HistoryOf<Mode, TP>, public SurfaceQuantities<Mode> {
   Cell* nmin[3] = {nullptr, nullptr, nullptr};
   Cell* nmax[3] = {nullptr, nullptr, nullptr};
   int ci = 0, cj = 0, ck = 0;
@@ -261,6 +265,15 @@ constexpr bool has_field() {
   return Detail::tuple_contains_type<F, typename FieldComponents<Mode>::electric>::value ||
          Detail::tuple_contains_type<F, typename FieldComponents<Mode>::magnetic>::value;
 }
+
+// a surface quantity of the cell, or 0 where SurfaceQuantities<Mode> has none
+#define FDTD_SQ(name)                                                  \
+  template <class C> auto sq_##name(C& c, int) -> decltype(c.name()) { \
+    return c.name();                                                   \
+  }                                                                    \
+  template <class C> double sq_##name(C&, long) { return 0.0; }
+FDTD_SQ(rho) FDTD_SQ(Jex) FDTD_SQ(Jey) FDTD_SQ(Jez) FDTD_SQ(Jhx) FDTD_SQ(Jhy) FDTD_SQ(Jhz)
+#undef FDTD_SQ
 
 template <class Mode, class F, class C>
 double field_or_zero(C& c) {
@@ -466,6 +479,16 @@ static int run(Scenario& s) {
 
   const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - clock0).count();
   printf("loop_seconds %.9f\n", loop_s);
+  {
+    UpdateSurfaceChargeDensity<Mode> rho(dx);
+    UpdateSurfaceCurrentE<Mode> je(dx);
+    UpdateSurfaceCurrentH<Mode> jh(dx);
+    for (C* c : interior) {
+      rho(*c);
+      je(*c);
+      jh(*c);
+    }
+  }
   FILE* f = fopen(s.out.c_str(), "wb");
   if (!f) return 4;
   std::vector<double> buf(cells.size());
@@ -498,6 +521,13 @@ static int run(Scenario& s) {
   PSI(Magnetic, X, X) PSI(Magnetic, X, Y) PSI(Magnetic, X, Z)
   PSI(Magnetic, Y, X) PSI(Magnetic, Y, Y) PSI(Magnetic, Y, Z)
   PSI(Magnetic, Z, X) PSI(Magnetic, Z, Y) PSI(Magnetic, Z, Z)
+  dump([](C& c) { return static_cast<double>(sq_rho(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jex(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jey(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jez(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jhx(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jhy(c, 0)); });
+  dump([](C& c) { return static_cast<double>(sq_Jhz(c, 0)); });
   fclose(f);
   return 0;
 }

@@ -28,7 +28,7 @@ def main():
     for make in scenarios.REFERENCE_SCENARIOS:
         p = make()
         ref = pyoracle.run_reference(p)
-        arrays = {k: ref[k] for k in KEEP + pyoracle.PSI_NAMES if np.any(ref[k] != 0)}
+        arrays = {k: ref[k] for k in KEEP + pyoracle.PSI_NAMES + pyoracle.SURFACE_NAMES if np.any(ref[k] != 0)}
         np.savez_compressed(os.path.join(out_dir, p.name + ".npz"), steps=p.steps, **arrays)
         print(p.name, sorted(arrays))
 

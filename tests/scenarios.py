@@ -24,6 +24,9 @@ def tm_cpml_sources() -> Problem:
     p.sources.append(Source(2, (12, 10, 0), 1e-12 * gaussian_pulse(80, 25, 6), "D"))
     p.dfts.append(DFTRegion(2, (0, 18, 0), (39, 18, 0), [0.02, 0.05]))
     p.dfts.append(DFTRegion(3, (5, 5, 0), (9, 8, 0), [0.03]))
+    # surface current Je_z and Jh_x (SurfaceQuantities.hpp) on boxes
+    p.dfts.append(DFTRegion(8, (8, 6, 0), (31, 28, 0), [0.03]))
+    p.dfts.append(DFTRegion(9, (1, 1, 0), (38, 34, 0), [0.02, 0.05]))
     p.steps = 80
     return p
 
@@ -44,6 +47,10 @@ def te_materials() -> Problem:
     p.sources.append(Source(0, (16, 20, 0), gaussian_pulse(60, 20, 6), "E"))
     p.sources.append(Source(1, (16, 21, 0), gaussian_pulse(60, 20, 6), "E"))
     p.dfts.append(DFTRegion(5, (3, 3, 0), (29, 37, 0), [0.04]))
+    # surface charge density and currents (SurfaceQuantities.hpp)
+    p.dfts.append(DFTRegion(12, (2, 2, 0), (30, 38, 0), [0.04]))
+    p.dfts.append(DFTRegion(7, (6, 6, 0), (26, 34, 0), [0.03]))
+    p.dfts.append(DFTRegion(11, (1, 1, 0), (31, 39, 0), [0.04]))
     p.steps = 60
     return p
 
@@ -118,6 +125,19 @@ def td_tfsf_box() -> Problem:
         p.dfts.append(DFTRegion((a + 1) % 3, tuple(lo), tuple(hi), [0.03, 0.06]))
         p.dfts.append(DFTRegion(3 + (a + 2) % 3, tuple(lo), tuple(hi), [0.03, 0.06]))
     p.steps = 50
+    return p
+
+
+def td_surface_dft() -> Problem:
+    """3D running DFTs of every surface quantity (rho, Je, Jh of
+    SurfaceQuantities.hpp) on boxes through a Drude cube and a Lorentz slab."""
+    p = td_drude_lorentz()
+    p.name = "td_surface_dft"
+    nx, ny, nz = p.shape
+    for q in range(6, 13):
+        lo = (1 + q % 2, 2, 1 + q % 3)
+        hi = (nx - 2, ny - 3 + q % 2, nz - 2 - q % 2)
+        p.dfts.append(DFTRegion(q, lo, hi, [0.03, 0.05]))
     return p
 
 
@@ -323,6 +343,6 @@ REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_
                        td_bd4_boundaries]
 # scenarios on the BD3/BD4 time policies (FP64 plain method only)
 MULTISTEP_SCENARIOS = [tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf, td_bd4_boundaries]
-ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks]
+ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks, td_surface_dft]
 # scenarios the FP32 fused method runs (it steps with the leapfrog only)
 LEAPFROG_SCENARIOS = [m for m in ALL_SCENARIOS if m not in MULTISTEP_SCENARIOS]

@@ -6,6 +6,9 @@ oracle on the same seeded inputs.
   reference's operation order without FMA contraction, so in practice the
   fields come out bit-identical; the tolerance is the stated bar).
 * FP32 fused method: <= 1e-4 relative L2 on E, H, P, J and the DFTs.
+* Surface quantities (rho, Je, Jh of include/SurfaceQuantities.hpp, read
+  with fdtd_read_quantity): bit-identical in FP64; in FP32 they are
+  differences of neighbouring fields, so the bar is 1e-3 relative L2.
 """
 import numpy as np
 import pytest
@@ -17,6 +20,7 @@ pytestmark = pytest.mark.gpu
 
 PLAIN_TOL = 1e-12
 FUSED_TOL = 1e-4
+SURFACE_F32_TOL = 1e-3
 
 
 def _compare(p, g, o, names, tol):
@@ -58,7 +62,7 @@ def test_plain_f64_bitwise_fields(fdtd, oracle, make):
     g = fdtd.Grid.from_problem(p, "f64")
     g.step(p.steps)
     E, H, _, _ = mode_fields(p.mode)
-    for n in E + H:
+    for n in E + H + oracle.SURFACE_NAMES:
         assert np.array_equal(g.get(n), o.get(n)), n
 
 
@@ -71,6 +75,31 @@ def test_fused_f32_matches_oracle(fdtd, oracle, make):
     g.synchronize()
     E, H, _, _ = mode_fields(p.mode)
     _compare(p, g, o, E + H, FUSED_TOL)
+    for n in oracle.SURFACE_NAMES:
+        ref = o.get(n)
+        if np.any(ref):
+            assert rel_l2(g.get(n), ref) <= SURFACE_F32_TOL, n
+
+
+def test_read_quantity_boxes_and_errors(fdtd, oracle):
+    """fdtd_read_quantity on sub-boxes equals the oracle's, and refuses
+    quantities outside the mode and boxes that leave the interior."""
+    p = scenarios.td_drude_lorentz()
+    o = oracle.OracleGrid(p)
+    o.step(p.steps)
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    for q, lo, hi in [(12, (1, 2, 3), (12, 9, 14)), (6, (4, 1, 1), (9, 13, 5)), (11, (2, 2, 2), (2, 13, 14)),
+                      (2, (0, 0, 0), (13, 14, 15)), (4, (3, 3, 3), (8, 8, 8))]:
+        assert np.array_equal(g.read_quantity(q, lo, hi), o.read_quantity(q, lo, hi)), q
+    with pytest.raises(fdtd.FdtdError):
+        g.read_quantity(6, (0, 1, 1), (5, 5, 5))
+    t = scenarios.tm_cpml_sources()
+    gt = fdtd.Grid.from_problem(t, "f32")
+    with pytest.raises(fdtd.FdtdError):
+        gt.read_quantity(12, (1, 1, 0), (5, 5, 0))  # rho: the TM functor does nothing
+    with pytest.raises(fdtd.FdtdError):
+        gt.read_quantity(6, (1, 1, 0), (5, 5, 0))  # Je_x: no Ex in TM
 
 
 @pytest.mark.parametrize("sweep", ["regs", "tma", "flat", "staged"])

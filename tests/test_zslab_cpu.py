@@ -60,6 +60,18 @@ def test_local_problem_moves_and_clips_everything_along_z():
         assert m == n
 
 
+def test_surface_dfts_that_read_a_ghost_plane_are_refused():
+    p = scenarios.td_surface_dft()
+    ranges = partition_z(p, 2)
+    with pytest.raises(ValueError):
+        [local_problem(p, z0, z1) for z0, z1 in ranges]
+    # a Je_z region needs no z neighbour and splits freely
+    q = scenarios.td_drude_lorentz()
+    q.dfts = [P.DFTRegion(8, (1, 1, 1), (12, 13, 14), [0.03])]
+    parts = [local_problem(q, z0, z1) for z0, z1 in partition_z(q, 2)]
+    assert sum(len(x.dfts) for x in parts) == 2
+
+
 class OracleSlab:
     """A rank's slab stepped by the CPU oracle, planes as torch CPU tensors."""
 
