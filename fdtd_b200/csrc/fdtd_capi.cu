@@ -8,6 +8,7 @@
 // launches per step: E sweep, E-phase DFT, H sweep, H-phase DFT, step counter.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -334,6 +335,7 @@ int build_materials(fdtd_grid* g) {
       MatF32& o = v[q];
       memset(&o, 0, sizeof(o));
       o.inv_eps = static_cast<float>(m.kind == FDTD_VACUUM ? 1.0 : 1.0 / m.eps_inf);
+      o.inv_mu = static_cast<float>(1.0 / m.mu_r);
       if (m.kind == FDTD_DRUDE) {
         const double bb = m.gamma[0] * dt * 0.5, w = dt * m.freq[0];
         o.npoles = -1;
@@ -654,8 +656,11 @@ FusedArgs fused_args(fdtd_grid* g) {
   a.inv_eps_map = static_cast<const float*>(g->d_eps_map);
   a.max_poles = g->max_poles;
   a.all_dispersive = 1;
-  for (auto& m : g->mats)
+  a.has_mu = 0;
+  for (auto& m : g->mats) {
     if (m.kind != FDTD_DRUDE && m.kind != FDTD_LORENTZ) a.all_dispersive = 0;
+    if (m.mu_r != 1.0) a.has_mu = 1;
+  }
   a.src_scale_d = static_cast<float>(1.0 / kEps0);
   a.src_scale_b = static_cast<float>(eta() / kMu0);
   a.src_scale_h = static_cast<float>(eta());
@@ -787,7 +792,6 @@ int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
       return fail(FDTD_ERR_INVALID, "Lorentz takes 1..4 poles");
     if (m.kind != FDTD_VACUUM && !(m.eps_inf > 0)) return fail(FDTD_ERR_INVALID, "eps_inf must be positive");
     if (!(m.mu_r > 0)) return fail(FDTD_ERR_INVALID, "mu_r must be positive");
-    if (g->f32 && m.mu_r != 1.0) return fail(FDTD_ERR_UNSUPPORTED, "the FP32 fused method takes mu_r = 1");
   }
   CK(cudaSetDevice(g->d.device));
   g->mats.assign(mats, mats + n);
@@ -1690,6 +1694,8 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
     else if (!g->planes.empty() || !g->dfts.empty()) why = "batched grids carry no TFSF planes or DFT regions";
     else if (!g->boxes.empty()) why = "batched grids carry no box sources";
     else if (g->bcs.n > 0) why = "batched grids carry no boundary conditions";
+    else if (std::any_of(g->mats.begin(), g->mats.end(), [](const fdtd_material& m) { return m.mu_r != 1.0; }))
+      why = "batched grids take mu_r = 1";
     else if (g->t != g0->t) why = "batched grids must have taken the same number of steps";
     else if (static_cast<long long>(g->pitch / 128) * g->n[1] >= (1 << 24)) why = "grid too large to batch";
     if (why) {
@@ -2116,6 +2122,8 @@ int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, 
   if (!g->planes.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes grids without TFSF planes");
   if (g->max_poles != 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes non-dispersive materials");
   if (g->bcs.n > 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes grids without boundary conditions");
+  for (auto& m : g->mats)
+    if (m.mu_r != 1.0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes mu_r = 1");
   if (ckpt_every < 1 || ckpt_every > 4096) return fail(FDTD_ERR_INVALID, "ckpt_every must be 1..4096");
   if (!interior(g, probe_lo[0], probe_lo[1], 0) || !interior(g, probe_hi[0], probe_hi[1], 0) ||
       probe_lo[0] > probe_hi[0] || probe_lo[1] > probe_hi[1])

@@ -267,8 +267,34 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
   st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(ezo, uZ), dZ, ie, g.ok, disp, g.uniform_mat, m0, mids, aZ));
 }
 
+// 1/mu_r of the group's 4 cells: H = B/(mu_r mu0) (the magnetic
+// ConstantUpdate, DispersiveMaterials.hpp:354-359), so the flux change of the
+// step is scaled per cell before it is added to the stored eta*H.
+__device__ __forceinline__ float4 group_inv_mu(const FusedArgs& a, const GroupCtx& g, int k, long long c) {
+  float4 r;
+  if (g.uniform_mat) {
+    const float m = a.mats[0].inv_mu;
+    return make_float4(m, m, m, m);
+  }
+  if (a.ids) {
+    const unsigned w = *reinterpret_cast<const unsigned*>(a.ids + c);
+#pragma unroll
+    for (int e = 0; e < 4; e++) set_el(r, e, a.mats[(w >> (8 * e)) & 0xff].inv_mu);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      set_el(r, e,
+             a.mats[a.bids[((k >> a.bshift) * a.nby + (g.j >> a.bshift)) * a.nbx + (min(g.x4 + e, a.nx - 1) >> a.bshift)]]
+                 .inv_mu);
+  }
+  return r;
+}
+
 // The H update of one group at plane k from the E values around it (own,
 // y+1, z+1 and the x+1 neighbour of the group's last cell) and the old H.
+// MU: some material has mu_r != 1 (a separate instantiation, so that the
+// common case keeps its registers).
+template <bool MU>
 __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCtx& g, int k, float4 ex, float4 ey,
                                                float4 ez, float4 ex_yp, float4 ez_yp, float4 ex_kp, float4 ey_kp,
                                                float ey_xp3, float ez_xp3, float4 hx, float4 hy, float4 hz,
@@ -369,6 +395,15 @@ __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCt
         }
         a.src_last[q] = v;
       }
+    }
+  }
+  if (MU) {
+    const float4 im = group_inv_mu(a, g, k, c);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      set_el(dX, e, el(dX, e) * el(im, e));
+      set_el(dY, e, el(dY, e) * el(im, e));
+      set_el(dZ, e, el(dZ, e) * el(im, e));
     }
   }
 #pragma unroll

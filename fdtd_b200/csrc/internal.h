@@ -69,6 +69,7 @@ struct MatF32 {
   float inv_eps;  // 1/eps_inf
   int npoles;     // 0: non-dispersive; Drude: -1 (one J only)
   float a[2], b[2], c[2];
+  float inv_mu;   // 1/mu_r (magnetic ConstantUpdate K; 1 for VacuumUpdate)
   // Drude: Jt' = a*Jt + b*E
   // Lorentz pole: Pt' = Pt + Jt; Jt' = a*Jt + b*E - c*Pt'
 };
@@ -154,6 +155,7 @@ struct FusedArgs {
   const float* inv_eps_map;  // per-cell 1/eps of non-dispersive cells (> 0), or null
   int max_poles;  // 0 none, -1 Drude only, 1..2 Lorentz
   int all_dispersive;  // every material of the table has poles
+  int has_mu;          // some material has mu_r != 1: the H updates scale by 1/mu_r
   int nsrc;
   SourceDev src[kMaxSources];
   float src_scale_d;  // 1/eps0 for D-target sources

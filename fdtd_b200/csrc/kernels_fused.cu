@@ -276,6 +276,16 @@ __global__ void __launch_bounds__(256) fused_h_kernel(const __grid_constant__ Fu
         a.src_last[s] = v;
       }
     }
+    if (a.has_mu) {
+      // H = B/(mu_r mu0): the step's flux change scales by 1/mu_r
+      int mid = 0;
+      if (a.ids) mid = a.ids[c];
+      else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+      const float im = a.mats[mid].inv_mu;
+      dx_ *= im;
+      dy_ *= im;
+      dz_ *= im;
+    }
     if (hasH(MODE, 0)) a.H[0][c] = a.H[0][c] - undo0 - dx_ + add0;
     if (hasH(MODE, 1)) a.H[1][c] = a.H[1][c] - undo1 - dy_ + add1;
     if (hasH(MODE, 2)) a.H[2][c] = a.H[2][c] - undo2 - dz_ + add2;

@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(32 * kRows) fused3d_e_kernel(const __grid_cons
   }
 }
 
+template <bool MU>
 __global__ void __launch_bounds__(32 * kRows) fused3d_h_kernel(const __grid_constant__ FusedArgs a, int kchunk) {
   const int lane = threadIdx.x;
   const int x4 = blockIdx.x * 128 + lane * 4;
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(32 * kRows) fused3d_h_kernel(const __grid_cons
       ey_xp3 = a.E[1][c + 4];
       ez_xp3 = a.E[2][c + 4];
     }
-    h_group_update(a, g, k, cex, cey, cez, cex_yp, cez_yp, ex_kp, ey_kp, ey_xp3, ez_xp3, chx, chy, chz);
+    h_group_update<MU>(a, g, k, cex, cey, cez, cex_yp, cez_yp, ex_kp, ey_kp, ey_xp3, ez_xp3, chx, chy, chz);
     ex_kp = cex;
     ey_kp = cey;
   }
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_e_kernel(const __grid_c
   }
 }
 
-template <int NZ, int MINB>
+template <int NZ, int MINB, bool MU>
 __global__ void __launch_bounds__(32 * kRows, MINB) flat_h_kernel(const __grid_constant__ FusedArgs a) {
   const int lane = threadIdx.x;
   const int x4 = blockIdx.x * 128 + lane * 4;
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(32 * kRows, MINB) flat_h_kernel(const __grid_c
       ey_xp3 = ey_xp_l31[q];
       ez_xp3 = ez_xp_l31[q];
     }
-    h_group_update(a, g, k, ex[q + 1], ey[q + 1], ez[q], ex_yp[q], ez_yp[q], ex[q], ey[q], ey_xp3, ez_xp3, hx[q],
+    h_group_update<MU>(a, g, k, ex[q + 1], ey[q + 1], ez[q], ex_yp[q], ez_yp[q], ex[q], ey[q], ey_xp3, ez_xp3, hx[q],
                    hy[q], hz[q]);
   }
 }
@@ -252,7 +253,8 @@ int launch_fused3d_h(const FusedArgs& a, cudaStream_t s) {
   const int bx = a.pitch / 128, by = (a.ny - 2 + kRows - 1) / kRows;
   const int kchunk = kchunk3d(a.nz, bx * by);
   const int bz = (a.nz - 2 + kchunk - 1) / kchunk;
-  fused3d_h_kernel<<<dim3(bx, by, bz), dim3(32, kRows, 1), 0, s>>>(a, kchunk);
+  if (a.has_mu) fused3d_h_kernel<true><<<dim3(bx, by, bz), dim3(32, kRows, 1), 0, s>>>(a, kchunk);
+  else fused3d_h_kernel<false><<<dim3(bx, by, bz), dim3(32, kRows, 1), 0, s>>>(a, kchunk);
   return 1;
 }
 
@@ -277,7 +279,8 @@ int launch_flat_e(const FusedArgs& a, cudaStream_t s) {
 
 int launch_flat_h(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRows - 1) / kRows, a.nz - 2), block(32, kRows, 1);
-  flat_h_kernel<1, 8><<<grid, block, 0, s>>>(a);
+  if (a.has_mu) flat_h_kernel<1, 8, true><<<grid, block, 0, s>>>(a);
+  else flat_h_kernel<1, 8, false><<<grid, block, 0, s>>>(a);
   return 1;
 }
 

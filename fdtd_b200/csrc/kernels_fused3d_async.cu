@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
                        hy_xm0, hz_xm0, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], a.ids ? *sid : 0u, px);
 }
 
-template <int MINB>
+template <int MINB, bool MU>
 __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
     ey_xp3 = ey_sh;
     ez_xp3 = ez_sh;
   }
-  h_group_update(a, g, k, s[2 * kThreads], ey, ez, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads], ey_xp3,
+  h_group_update<MU>(a, g, k, s[2 * kThreads], ey, ez, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads], ey_xp3,
                  ez_xp3, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], px);
 }
 
@@ -156,16 +156,22 @@ int launch_staged_e(const FusedArgs& a, cudaStream_t s) {
   return 1;
 }
 
-int launch_staged_h(const FusedArgs& a, cudaStream_t s) {
+template <bool MU>
+static void staged_h_dispatch(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.nz - 2), block(32, kRowsA, 1);
   const size_t smem = kSlotsH * kThreads * sizeof(float4);
   static bool carveout = false;
   if (!carveout) {
-    cudaFuncSetAttribute(staged_h_kernel<8>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(staged_h_kernel<8, MU>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
     carveout = true;
   }
-  staged_h_kernel<8><<<grid, block, smem, s>>>(a);
+  staged_h_kernel<8, MU><<<grid, block, smem, s>>>(a);
+}
+
+int launch_staged_h(const FusedArgs& a, cudaStream_t s) {
+  if (a.has_mu) staged_h_dispatch<true>(a, s);
+  else staged_h_dispatch<false>(a, s);
   return 1;
 }
 

@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(32 * kTY, 2) tma_e_kernel(const __grid_constan
   }
 }
 
+template <bool MU>
 __global__ void __launch_bounds__(32 * kTY, 2) tma_h_kernel(const __grid_constant__ FusedArgs a,
                                                           const __grid_constant__ TmaMapsH m, int kchunk) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(32 * kTY, 2) tma_h_kernel(const __grid_constan
       }
       const int ho = ty * 128 + 4 * lane;
       const float4 hx = lds4(sH + ho), hy = lds4(sH + kTY * 128 + ho), hz = lds4(sH + 2 * kTY * 128 + ho);
-      h_group_update(a, g, k, ex, ey, ez, ex_yp, ez_yp, ex_kp, ey_kp, ey_xp3, ez_xp3, hx, hy, hz);
+      h_group_update<MU>(a, g, k, ex, ey, ez, ex_yp, ez_yp, ex_kp, ey_kp, ey_xp3, ez_xp3, hx, hy, hz);
       ex_kp = ex;
       ey_kp = ey;
     }
@@ -301,7 +302,8 @@ bool tma_prepare(const FusedArgs& a, TmaState** state) {
          cudaFuncSetAttribute(tma_e_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, se) == cudaSuccess &&
          cudaFuncSetAttribute(tma_e_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, se) == cudaSuccess &&
          cudaFuncSetAttribute(tma_e_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, se) == cudaSuccess &&
-         cudaFuncSetAttribute(tma_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sh) == cudaSuccess;
+         cudaFuncSetAttribute(tma_h_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh) == cudaSuccess &&
+         cudaFuncSetAttribute(tma_h_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh) == cudaSuccess;
     if (!ok) return false;
     attr = true;
   }
@@ -339,7 +341,8 @@ int launch_tma_h(const FusedArgs& a, const TmaState* st, cudaStream_t s) {
   int bz;
   const int kchunk = tma_kchunk(a, &bz);
   dim3 grid(a.pitch / 128, (a.ny - 2 + kTY - 1) / kTY, bz), block(32, kTY, 1);
-  tma_h_kernel<<<grid, block, 128 + kStages * kStageH, s>>>(a, st->h, kchunk);
+  if (a.has_mu) tma_h_kernel<true><<<grid, block, 128 + kStages * kStageH, s>>>(a, st->h, kchunk);
+  else tma_h_kernel<false><<<grid, block, 128 + kStages * kStageH, s>>>(a, st->h, kchunk);
   return 1;
 }
 

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__
     if (has) f0[I] = ft == 0 ? a.E[I][c] : a.H[I][c];
   }
   int mid = 0;
-  if (ft == 0) {
+  if (ft == 0 || a.has_mu) {
     if (a.ids) mid = a.ids[c];
     else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
   }
@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(256) tfsf_fused_kernel(const __grid_constant__
       for (int pq = 0; pq < np && pq < 2; pq++) a.J[pq][I][c] += m.b[pq] * dE;
     }
   } else {
-    const double sc = a.eta * a.dt / kMu0;
+    // the correction goes to B; H = B/(mu_r mu0)
+    const double sc = a.eta * a.dt / kMu0 * (a.has_mu ? static_cast<double>(a.mats[mid].inv_mu) : 1.0);
     for (int I = 0; I < 3; I++)
       if (hasH(MODE, I)) a.H[I][c] = f0[I] - static_cast<float>(sc * corr[I]);
   }

@@ -11,9 +11,9 @@
 // touching the reference:
 //  * DispersiveAtomicUpdate (include/DispersiveMaterials.hpp:260-282) puts
 //    enable_if on a class template parameter, which g++13 rejects when any
-//    material functor is instantiated; the partial specialisations below
-//    forward to UpdateStruct::implicit_update / explicit_update with the same
-//    argument order as :272-280.
+//    material functor is instantiated; ref_compile_fixes.hpp holds partial
+//    specialisations that forward to UpdateStruct::implicit_update /
+//    explicit_update with the same argument order as :272-280.
 //  * `static constexpr double val` (:370, :745, :1047) is ODR-used; C++17
 //    makes it implicitly inline.
 //  * BD3::get and BD3::get_reverse (include/YeeUpdates.hpp:209-221) take the
@@ -54,6 +54,7 @@
 // nx*ny*nz long. The wall time of the time loop alone is printed as
 // "loop_seconds <s>".
 #include <fdtd.h>
+#include "ref_compile_fixes.hpp"
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -66,38 +67,6 @@
 #include <cstddef>
 #include <iterator>
 
-namespace fdtd {
-template <typename U, typename F>
-struct DispersiveAtomicUpdate<U, true, F> {
-  static constexpr Dir d = FieldDir<F>::value;
-  static constexpr FieldType ft = F::field_type;
-  typedef typename FluxComponent<ft, d>::type DType;
-  typedef typename FieldComponent<ft, d>::type EType;
-  typedef typename CurrentComponent<ft, d>::type JType;
-  typedef typename PolarizationComponent<ft, d>::type PType;
-  template <typename T, typename... Args>
-  static void get(T&& f, Args&&... args) {
-    U::implicit_update(GetField<DType>::get(f), GetField<EType>::get(f),
-                       GetField<PType>::get(f), GetField<JType>::get(f),
-                       std::forward<Args>(args)...);
-  }
-};
-template <typename U, typename F>
-struct DispersiveAtomicUpdate<U, false, F> {
-  static constexpr Dir d = FieldDir<F>::value;
-  static constexpr FieldType ft = F::field_type;
-  typedef typename FluxComponent<ft, d>::type DType;
-  typedef typename FieldComponent<ft, d>::type EType;
-  typedef typename CurrentComponent<ft, d>::type JType;
-  typedef typename PolarizationComponent<ft, d>::type PType;
-  template <typename T, typename... Args>
-  static void get(T&& f, Args&&... args) {
-    U::explicit_update(GetField<DType>::get(f), GetField<EType>::get(f),
-                       GetField<PType>::get(f), GetField<JType>::get(f),
-                       std::forward<Args>(args)...);
-  }
-};
-}  // namespace fdtd
 
 using namespace fdtd;
 

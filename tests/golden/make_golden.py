@@ -5,7 +5,11 @@ oracle/_ref/ref_runner -- the reference's own update functors compiled from
 its headers (oracle/Makefile) -- and the final fields are stored as
 <name>.npz. Run from the repository root, where the reference tree exists:
 
-    make -C oracle _ref/ref_runner && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py
+
+It also writes config_*.xml: the reference's own XML writers (print_summary
+of MaterialMap, PMLOptions, BoundaryOptions) run on config_spec.txt by
+oracle/_ref/ref_xml, the fixtures of the config loaders.
 """
 import os
 import sys
@@ -23,8 +27,29 @@ import scenarios  # noqa: E402
 KEEP = ["Dx", "Dy", "Dz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Hx", "Hy", "Hz", "Px", "Py", "Pz", "Jx", "Jy", "Jz"]
 
 
+def write_config_fixtures(out_dir):
+    """config_{materials,pml,boundaries}.xml: the reference's own
+    print_summary writers (oracle/_ref/ref_xml) on config_spec.txt."""
+    import subprocess
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_xml")
+    text = subprocess.run([exe, os.path.join(out_dir, "config_spec.txt")], check=True, capture_output=True,
+                          text=True).stdout
+    sections, cur = {}, None
+    for line in text.splitlines():
+        if line.startswith("=== "):
+            cur = line[4:]
+            sections[cur] = []
+        else:
+            sections[cur].append(line)
+    for name, lines in sections.items():
+        with open(os.path.join(out_dir, f"config_{name}.xml"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+        print("config", name)
+
+
 def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    write_config_fixtures(out_dir)
     for make in scenarios.REFERENCE_SCENARIOS:
         p = make()
         ref = pyoracle.run_reference(p)

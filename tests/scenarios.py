@@ -7,7 +7,7 @@ import math
 
 import numpy as np
 
-from fdtd_b200.problem import (TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion, courant_dt,
+from fdtd_b200.problem import (CONSTANT, DRUDE, TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion, courant_dt,
                                gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, sinusoid, tfsf_box_planes)
 
 DX = 1e-6
@@ -138,6 +138,43 @@ def td_surface_dft() -> Problem:
         lo = (1 + q % 2, 2, 1 + q % 3)
         hi = (nx - 2, ny - 3 + q % 2, nz - 2 - q % 2)
         p.dfts.append(DFTRegion(q, lo, hi, [0.03, 0.05]))
+    return p
+
+
+def tm_magnetic_tfsf() -> Problem:
+    """TM TFSF box around magnetic cells: a constant block (eps 2, mu 1.7)
+    and a Drude block with mu 1.3 (ConstantUpdate<Mode, Magnetic>), with a
+    B-target source inside the magnetic block."""
+    p = tm_tfsf_reference_polarisation()
+    p.name = "tm_magnetic_tfsf"
+    n = p.shape[0]
+    dt = p.dt
+    p.materials = [Material.vacuum(), Material(CONSTANT, 2.0, 1.7, []),
+                   Material(DRUDE, 1.0, 1.3, [(1.0, 0.3 / dt, 0.01 / dt)])]
+    ids = np.zeros((1, n, n), np.uint8)
+    ids[0, 24:32, 22:30] = 1
+    ids[0, 30:38, 33:40] = 2
+    p.ids = ids
+    p.sources.append(Source(0, (25, 27, 0), 1e-9 * gaussian_pulse(100, 30, 8), "B"))
+    p.dfts.append(DFTRegion(4, (20, 30, 0), (39, 30, 0), [0.03]))
+    return p
+
+
+def td_magnetic_tfsf() -> Problem:
+    """3D TFSF box with a magnetic cube (eps 1.5, mu 2.2), a magnetic Drude
+    slab (mu 1.4) and H- and B-target sources in them."""
+    p = td_tfsf_box()
+    p.name = "td_magnetic_tfsf"
+    n = p.shape[0]
+    dt = p.dt
+    p.materials = [Material.vacuum(), Material(CONSTANT, 1.5, 2.2, []),
+                   Material(DRUDE, 1.0, 1.4, [(1.0, 0.3 / dt, 0.01 / dt)])]
+    ids = np.zeros((n, n, n), np.uint8)
+    ids[9:13, 10:14, 9:15] = 1
+    ids[13:16, 8:16, 11:13] = 2
+    p.ids = ids
+    p.sources.append(Source(1, (11, 12, 10), 1e-3 * gaussian_pulse(50, 15, 5), "H"))
+    p.sources.append(Source(2, (12, 10, 14), 1e-9 * gaussian_pulse(50, 18, 5), "B"))
     return p
 
 
@@ -340,7 +377,7 @@ def objective_problem(p, spec):
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
                        te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources,
                        tm_boundaries, te_boundaries, td_boundaries, tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf,
-                       td_bd4_boundaries]
+                       td_bd4_boundaries, tm_magnetic_tfsf, td_magnetic_tfsf]
 # scenarios on the BD3/BD4 time policies (FP64 plain method only)
 MULTISTEP_SCENARIOS = [tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf, td_bd4_boundaries]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks, td_surface_dft]
