@@ -74,26 +74,63 @@ def parse():
     ap.add_argument("--batch-mode", default="tune", choices=["tune", "persistent", "per_phase"],
                     help="batch64: autotune, or force a launch mode (with --batch-rows)")
     ap.add_argument("--batch-rows", type=int, default=4, choices=[1, 2, 4, 8])
+    ap.add_argument("--variant", default="none", choices=list(VARIANTS),
+                    help="3D/2D grid workloads: measure a feature beside the hot path (see VARIANTS)")
     return ap.parse_args()
 
 
-def make_problem(workload: str, steps: int, n: int = 0):
-    from fdtd_b200 import problem as P
-    if workload == "drude384":
-        return P.config2(n=n or 384, steps=steps)
-    if workload == "lorentz768":
-        return P.config5(n=n or 768, steps=steps)
-    return P.config1(n=n or 256, steps=steps)
+# Variants of the grid workloads that exercise the features around the hot
+# path; each keeps the workload's grid, materials and sources.
+VARIANTS = {
+    "none": "the workload as configured",
+    "pec_backed": "a PEC boundary condition on all six faces behind the CPML (boundary image kernel each half step)",
+    "surface_dft": "the face DFTs capture the surface currents instead of the fields: Jh in place of each E "
+                   "component, Je in place of each H component",
+    "bd3": "the FP64 plain leg steps with the BD3 time policy (flux history) at Courant 0.5",
+    "bd4": "the FP64 plain leg steps with the BD4 time policy (flux history) at Courant 0.5",
+}
 
 
-def small_problem(workload: str, steps: int):
-    """Same physics on a grid the CPU finishes in seconds."""
+def apply_variant(p, variant: str, fp64: bool = False):
+    """The problem p changed for `variant` (in place); bd3/bd4 change only the
+    FP64 plain problem (the FP32 method steps with the leapfrog)."""
+    if variant == "pec_backed":
+        for a in range(p.dim):
+            for s in (0, 1):
+                p.boundaries[(a, s)] = "pec"
+    elif variant == "surface_dft":
+        for r in p.dfts:
+            r.comp = r.comp + 9 if r.comp < 3 else r.comp + 3
+    elif variant in ("bd3", "bd4") and fp64:
+        p.time_scheme = 3 if variant == "bd3" else 4
+        p.dt = p.dt * 0.5 / 0.99
+    return p
+
+
+def make_problem(workload: str, steps: int, n: int = 0, variant: str = "none", fp64: bool = False):
     from fdtd_b200 import problem as P
     if workload == "drude384":
-        return P.config2(n=64, steps=steps), "64^3 grid (sphere, CPML, insets scaled by 64/384)"
-    if workload == "lorentz768":
-        return P.config5(n=64, steps=steps, block=16), "64^3 grid, 16^3 eps blocks"
-    return P.config1(n=256, steps=steps), "256^2 grid"
+        p = P.config2(n=n or 384, steps=steps)
+    elif workload == "lorentz768":
+        p = P.config5(n=n or 768, steps=steps)
+    else:
+        p = P.config1(n=n or 256, steps=steps)
+    return apply_variant(p, variant, fp64)
+
+
+def small_problem(workload: str, steps: int, variant: str = "none"):
+    """Same physics on a grid the CPU finishes in seconds (the CPU path is
+    the FP64 one: bd3/bd4 apply)."""
+    from fdtd_b200 import problem as P
+    if workload == "drude384":
+        p, d = P.config2(n=64, steps=steps), "64^3 grid (sphere, CPML, insets scaled by 64/384)"
+    elif workload == "lorentz768":
+        p, d = P.config5(n=64, steps=steps, block=16), "64^3 grid, 16^3 eps blocks"
+    else:
+        p, d = P.config1(n=256, steps=steps), "256^2 grid"
+    if variant != "none":
+        d += f", variant {variant}"
+    return apply_variant(p, variant, fp64=True), d
 
 
 # ------------------------------------------------------------------ clocks
@@ -191,8 +228,10 @@ def alg_bytes(p, word: int):
         h_sweep = cells * word * (nh * 2 + ne) + psi_h
         step_min = cells * word * (ne + nh) * 2 + psi_e + psi_h + disp + id_bytes
     else:  # plain FP64 keeps D, E, B, H: flux read+write, field write, curl read
-        e_sweep = cells * word * (ne * 3 + nh) + psi_e + disp + id_bytes
-        h_sweep = cells * word * (nh * 3 + ne) + psi_h + id_bytes
+        # BD3/BD4 keep 2/3 past fluxes per component, each read and written
+        hist = {3: 2, 4: 3}.get(getattr(p, "time_scheme", 1), 0) * 2
+        e_sweep = cells * word * (ne * (3 + hist) + nh) + psi_e + disp + id_bytes
+        h_sweep = cells * word * (nh * (3 + hist) + ne) + psi_h + id_bytes
         step_min = e_sweep + h_sweep
     return {"e_sweep": float(e_sweep), "h_sweep": float(h_sweep), "step": float(step_min),
             "per_cell_step": float(step_min) / cells}
@@ -219,17 +258,17 @@ def cpu_rate(problem, steps: int, kind: str):
     return problem.interior_cells * steps / dt, dt
 
 
-def cpu_baseline(workload: str, budget_s: float = 15.0):
+def cpu_baseline(workload: str, budget_s: float = 15.0, variant: str = "none"):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     kind = "reference" if pyoracle.reference_available() else "port"
-    p, desc = small_problem(workload, 10)
+    p, desc = small_problem(workload, 10, variant)
     if kind == "reference" and p.materials and max(len(m.poles) for m in p.materials) > 1:
         kind = "port"  # the reference holds one pole per cell
     # calibrate on a few steps, then run a sample of about budget_s
-    rate0, _ = cpu_rate(small_problem(workload, 4)[0], 4, kind)
+    rate0, _ = cpu_rate(small_problem(workload, 4, variant)[0], 4, kind)
     steps = max(4, int(budget_s * rate0 / p.interior_cells))
-    p, desc = small_problem(workload, steps)
+    p, desc = small_problem(workload, steps, variant)
     rate, dt = cpu_rate(p, steps, kind)
     return {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": 1, "kind": kind,
             "sample": f"{desc}, {steps} steps, {dt:.1f} s, single thread"}
@@ -245,7 +284,8 @@ def run_reference_arm(args):
     elif args.workload == "adjoint512":
         cb = cpu_adjoint_baseline(budget_s=20.0)
     else:
-        cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)))
+        cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)),
+                          variant=args.variant)
     metric = ADJ_METRIC if args.workload == "adjoint512" else METRIC
     line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": "Gcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
@@ -417,7 +457,7 @@ def run_batch(args, torch, world, rank, local, stream):
     if args.batch_mode == "tune":
         batch.tune(4)
     else:
-        batch.configure(args.batch_mode == "persistent", args.batch_rows)
+        batch.configure(args.batch_mode, args.batch_rows)
     batch.step(args.warmup, stream=stream.cuda_stream)
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -530,7 +570,7 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    p = make_problem(args.workload, args.steps + args.warmup, args.n)
+    p = make_problem(args.workload, args.steps + args.warmup, args.n, args.variant)
     g = G.Grid.from_problem(p, "f32", device=local)
     if args.sweep != "auto":
         g.set_sweep_kernel(args.sweep)
@@ -584,7 +624,7 @@ def main():
     # FP64 plain on the same grid and GPU (the metric's comparison)
     f64 = None
     if not args.no_f64:
-        p64 = make_problem(args.workload, args.steps + args.warmup, args.n)
+        p64 = make_problem(args.workload, args.steps + args.warmup, args.n, args.variant, fp64=True)
         g64 = G.Grid.from_problem(p64, "f64", device=local)
         n64 = max(3, min(args.steps, 200))
         g64.step(args.warmup, stream=stream.cuda_stream)
@@ -595,7 +635,17 @@ def main():
             end.record(stream)
         barrier()
         ms64 = start.elapsed_time(end)
-        f64 = {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "ms_per_step": ms64 / n64}
+        prof64 = g64.profile_step(min(10, n64), stream=stream.cuda_stream)
+        ab64 = alg_bytes(p64, 8)
+        e64 = ab64["e_sweep"] / (prof64["e_sweep"] / 1e3) / 1e9
+        h64 = ab64["h_sweep"] / (prof64["h_sweep"] / 1e3) / 1e9
+        f64 = {"value": cells * n64 / (ms64 / 1e3) / 1e9, "steps": n64, "ms_per_step": ms64 / n64,
+               "time_scheme": p64.time_scheme, "kernel_ms": prof64,
+               "roofline": {"bound": "hbm", "kernel": "plain_e_kernel (E sweep)", "achieved": e64, "peak": peak,
+                            "unit": "GB/s", "frac": e64 / peak, "alg_bytes_per_launch": ab64["e_sweep"],
+                            "launch_ms": prof64["e_sweep"]},
+               "roofline_h": {"kernel": "plain_h_kernel (H sweep)", "achieved": h64, "frac": h64 / peak,
+                              "alg_bytes_per_launch": ab64["h_sweep"], "launch_ms": prof64["h_sweep"]}}
         g64.close()
         del g64
 
@@ -603,7 +653,7 @@ def main():
     # (material ids, source and aux tables), run, read every DFT spectrum back
     e2e = None
     if not args.no_e2e:
-        pe = make_problem(args.workload, args.steps, args.n)  # the user's host-side description
+        pe = make_problem(args.workload, args.steps, args.n, args.variant)  # the user's host-side description
         barrier()
         t0 = time.perf_counter()
         ge = G.Grid.from_problem(pe, "f32", device=local)
@@ -628,14 +678,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.workload)
+        cpu = cpu_baseline(args.workload, variant=args.variant)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": p.name, "grid": list(p.shape), "interior_cells": cells,
+            "config": {"workload": p.name, "variant": args.variant, "grid": list(p.shape), "interior_cells": cells,
                        "cpml": max(p.pml.values()) if p.pml else 0, "steps_in_config": P_STEPS.get(args.workload),
                        "l2": f"state {state_gb:.2f} GB on the device; "
                              + ("larger than L2, no flush" if state_gb > 0.126 else "fits L2"),

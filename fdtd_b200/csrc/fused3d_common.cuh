@@ -34,18 +34,22 @@ __device__ __forceinline__ float4 sub4(float4 a, float4 b) {
 
 // Material update of one E component for the 4 cells of a group: returns the
 // new E (plus this step's E-target source values), updating P/J in place.
+// spj: the group's J (then P) values already staged in shared memory, slot
+// (q*3 + I) for J and (NP*3 + q*3 + I) for P, `stride` float4 apart; null
+// reads them from global memory.
 template <int MAXP>
 __device__ __forceinline__ float4 e_comp(const FusedArgs& a, int I, long long c, float4 eo, float4 d, float4 ie,
                                          const bool ok[4], bool disp, bool uniform, const MatF32& m0,
-                                         const int mids[4], float4 add) {
+                                         const int mids[4], float4 add, const float4* spj = nullptr,
+                                         int stride = 0) {
   float4 en;
   if (MAXP != 0 && disp) {
     constexpr int NP = MAXP <= 0 ? 1 : MAXP;
     float4 jt[NP], pt[NP];
 #pragma unroll
     for (int q = 0; q < NP; q++) {
-      jt[q] = ld4(a.J[q][I] + c);
-      if (MAXP > 0) pt[q] = ld4(a.P[q][I] + c);
+      jt[q] = spj ? spj[(q * 3 + I) * stride] : ld4(a.J[q][I] + c);
+      if (MAXP > 0) pt[q] = spj ? spj[(NP * 3 + q * 3 + I) * stride] : ld4(a.P[q][I] + c);
     }
 #pragma unroll
     for (int e = 0; e < 4; e++) {
@@ -122,7 +126,8 @@ template <int MAXP>
 __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCtx& g, int k, float4 hx, float4 hy,
                                                float4 hz, float4 hx_ym, float4 hz_ym, float4 hx_km, float4 hy_km,
                                                float hy_xm0, float hz_xm0, float4 exo, float4 eyo, float4 ezo,
-                                               unsigned ids4, const float* staged_px = nullptr) {
+                                               unsigned ids4, const float* staged_px = nullptr,
+                                               const float4* spj = nullptr, int pj_stride = 0) {
   if (!g.row_ok) return;
   const int j = g.j, x4 = g.x4;
   const long long c = (static_cast<long long>(k) * a.ny + j) * a.pitch + x4;
@@ -262,9 +267,12 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
     for (int e = 0; e < 4; e++)
       if (el(v, e) > 0.f && a.mats[mids[e]].npoles == 0) set_el(ie, e, el(v, e));
   }
-  st4(a.E[0] + c, e_comp<MAXP>(a, 0, c, sub4(exo, uX), dX, ie, g.ok, disp, g.uniform_mat, m0, mids, aX));
-  st4(a.E[1] + c, e_comp<MAXP>(a, 1, c, sub4(eyo, uY), dY, ie, g.ok, disp, g.uniform_mat, m0, mids, aY));
-  st4(a.E[2] + c, e_comp<MAXP>(a, 2, c, sub4(ezo, uZ), dZ, ie, g.ok, disp, g.uniform_mat, m0, mids, aZ));
+  st4(a.E[0] + c,
+      e_comp<MAXP>(a, 0, c, sub4(exo, uX), dX, ie, g.ok, disp, g.uniform_mat, m0, mids, aX, spj, pj_stride));
+  st4(a.E[1] + c,
+      e_comp<MAXP>(a, 1, c, sub4(eyo, uY), dY, ie, g.ok, disp, g.uniform_mat, m0, mids, aY, spj, pj_stride));
+  st4(a.E[2] + c,
+      e_comp<MAXP>(a, 2, c, sub4(ezo, uZ), dZ, ie, g.ok, disp, g.uniform_mat, m0, mids, aZ, spj, pj_stride));
 }
 
 // 1/mu_r of the group's 4 cells: H = B/(mu_r mu0) (the magnetic

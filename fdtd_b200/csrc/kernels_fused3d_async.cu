@@ -6,6 +6,8 @@
 // after cp.async.wait_all the thread reads its slots back (each thread reads
 // only what it copied itself, so no CTA barrier is needed) and runs the same
 // update as the other sweeps (fused3d_common.cuh).
+#include <algorithm>
+
 #include "fused3d_common.cuh"
 
 namespace fdtdb {
@@ -17,6 +19,12 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kRowsA = 4;
 constexpr int kThreads = 32 * kRowsA;
 constexpr int kSlotsE = 12;  // hx_km, hy_km, hx, hy, hz, hx_ym, hz_ym, ex, ey, ez, x-slab psi (2)
+// with every material dispersive, the ADE state follows: J (then P) of each
+// pole and component
+template <int MAXP>
+constexpr int pj_slots() {
+  return MAXP == 0 ? 0 : (MAXP < 0 ? 3 : 6 * MAXP);
+}
 constexpr int kSlotsH = 12;  // ex_kp, ey_kp, ex, ey, ez, ex_yp, ez_yp, hx, hy, hz, x-slab psi (2)
 
 __device__ __forceinline__ void cp_async16(float4* dst, const float* src) {
@@ -47,9 +55,13 @@ __device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx&
 
 }  // namespace
 
-template <int MAXP, int MINB>
+// PJ: every material of the grid is dispersive, so the group's J (and P)
+// are staged with the fields and all of the thread's loads are in flight at
+// once (they are otherwise read per component, after the fields arrive)
+template <int MAXP, int MINB, bool PJ>
 __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
+  constexpr int kPJ = PJ ? pj_slots<MAXP>() : 0;
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
   const int x4 = blockIdx.x * 128 + lane * 4;
   const int j = 1 + blockIdx.y * kRowsA + threadIdx.y;
@@ -58,7 +70,7 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
   const long long c = k * sz + jl * sy + x4;
   float4* s = sm + tid;
-  unsigned* sid = reinterpret_cast<unsigned*>(sm + kSlotsE * kThreads) + tid;
+  unsigned* sid = reinterpret_cast<unsigned*>(sm + (kSlotsE + kPJ) * kThreads) + tid;
   cp_async16(s + 0 * kThreads, a.H[0] + c - sz);
   cp_async16(s + 1 * kThreads, a.H[1] + c - sz);
   cp_async16(s + 2 * kThreads, a.H[0] + c);
@@ -70,6 +82,16 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
   cp_async16(s + 8 * kThreads, a.E[1] + c);
   cp_async16(s + 9 * kThreads, a.E[2] + c);
   if (a.ids) cp_async4(sid, a.ids + c);
+  if (PJ) {
+    constexpr int NP = MAXP < 0 ? 1 : MAXP;
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+#pragma unroll
+      for (int I = 0; I < 3; I++) {
+        cp_async16(s + (kSlotsE + q * 3 + I) * kThreads, a.J[q][I] + c);
+        if (MAXP > 0) cp_async16(s + (kSlotsE + NP * 3 + q * 3 + I) * kThreads, a.P[q][I] + c);
+      }
+  }
   float hy_xm0 = 0.f, hz_xm0 = 0.f;
   if (lane == 0) {
     hy_xm0 = a.H[1][c - 1];
@@ -88,7 +110,8 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
     hz_xm0 = hz_sh;
   }
   e_group_update<MAXP>(a, g, k, s[2 * kThreads], hy, hz, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads],
-                       hy_xm0, hz_xm0, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], a.ids ? *sid : 0u, px);
+                       hy_xm0, hz_xm0, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], a.ids ? *sid : 0u, px,
+                       PJ ? s + kSlotsE * kThreads : nullptr, kThreads);
 }
 
 template <int MINB, bool MU>
@@ -133,17 +156,46 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
                  ez_xp3, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], px);
 }
 
-template <int MAXP>
-static void staged_e_dispatch(const FusedArgs& a, cudaStream_t s) {
+// The shared-memory carveout (percent of the largest) that holds `ctas` CTAs
+// of `smem` bytes each (plus the 1 KB the runtime reserves per CTA): asking
+// for no more leaves the rest of the SM's 256 KB to L1, which holds the
+// sweeps' register spills.
+static int carveout_for(int ctas, size_t smem) {
+  int dev = 0, max_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (max_sm <= 0) return cudaSharedmemCarveoutMaxShared;
+  const size_t need = static_cast<size_t>(ctas) * (smem + 1024);
+  return static_cast<int>(std::min<size_t>(100, (need * 100 + max_sm - 1) / max_sm));
+}
+
+// CTAs per SM: 7 (6 for two poles) with the ADE state read per component;
+// with it staged, as many as the shared memory holds (two poles: 4 x 49.7 KB)
+template <int MAXP, bool PJ>
+static void staged_e_launch(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.nz - 2), block(32, kRowsA, 1);
-  const size_t smem = kSlotsE * kThreads * sizeof(float4) + kThreads * sizeof(unsigned);
-  auto fn = staged_e_kernel<MAXP, (MAXP >= 2 ? 6 : 7)>;
-  static bool carveout = false;  // ask for the largest shared-memory split once
-  if (!carveout) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    carveout = true;
+  constexpr int slots = kSlotsE + (PJ ? pj_slots<MAXP>() : 0);
+  constexpr int minb = !PJ ? (MAXP >= 2 ? 6 : 7) : (MAXP >= 2 ? 4 : (MAXP == 1 ? 6 : 7));
+  const size_t smem = slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned);
+  auto fn = staged_e_kernel<MAXP, minb, PJ>;
+  static bool attrs = false;  // once: the shared-memory split that holds minb CTAs, the rest as L1
+  if (!attrs) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_for(minb, smem));
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    attrs = true;
   }
   fn<<<grid, block, smem, s>>>(a);
+}
+
+template <int MAXP>
+static void staged_e_dispatch(const FusedArgs& a, cudaStream_t s) {
+  if constexpr (MAXP != 0) {
+    if (a.all_dispersive) {
+      staged_e_launch<MAXP, true>(a, s);
+      return;
+    }
+  }
+  staged_e_launch<MAXP, false>(a, s);
 }
 
 int launch_staged_e(const FusedArgs& a, cudaStream_t s) {
@@ -163,7 +215,7 @@ static void staged_h_dispatch(const FusedArgs& a, cudaStream_t s) {
   static bool carveout = false;
   if (!carveout) {
     cudaFuncSetAttribute(staged_h_kernel<8, MU>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
+                         carveout_for(8, smem));
     carveout = true;
   }
   staged_h_kernel<8, MU><<<grid, block, smem, s>>>(a);

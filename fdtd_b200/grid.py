@@ -401,7 +401,11 @@ class Batch:
         for g in self.grids:
             g._stepped_in_batch = True
 
-    def configure(self, persistent: bool, rows: int) -> None:
+    def configure(self, persistent, rows: int) -> None:
+        """persistent: True or 'persistent' for the cooperative kernel,
+        False or 'per_phase' for one launch per half step."""
+        if isinstance(persistent, str):
+            persistent = persistent == "persistent"
         _check(load_library().fdtd_batch_configure(self.h, 1 if persistent else 0, int(rows)))
 
     def info(self) -> dict:

@@ -20,7 +20,9 @@
 
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstdint>
+#include <algorithm>
 #include <functional>
 #include <initializer_list>
 #include <memory>
@@ -496,6 +498,36 @@ class Grid {
     return v;
   }
 
+  // A quantity (FDTD_Q_*) on the cells lo..hi, x fastest: a field, or what
+  // UpdateSurfaceCurrentE / UpdateSurfaceCurrentH / UpdateSurfaceChargeDensity
+  // (include/SurfaceQuantities.hpp:203-356) would leave in those cells now.
+  std::vector<double> read(int quantity, std::array<int, 3> lo, std::array<int, 3> hi) const {
+    size_t n = 1;
+    for (int d = 0; d < 3; d++) n *= static_cast<size_t>(std::max(0, hi[d] - lo[d] + 1));
+    std::vector<double> v(n);
+    check(fdtd_read_quantity(g_.get(), quantity, lo.data(), hi.data(), v.data()));
+    return v;
+  }
+
+  // Running DFT of a quantity (FDTD_Q_*) over lo..hi at freqs (cycles per
+  // step), from the next step on; the reference's DataCapture has no Fourier
+  // capture. dft(handle) returns [nf][points].
+  int add_dft(int quantity, std::array<int, 3> lo, std::array<int, 3> hi, const std::vector<double>& freqs) {
+    int h = -1;
+    check(fdtd_add_dft(g_.get(), quantity, lo.data(), hi.data(), freqs.data(), static_cast<int>(freqs.size()), &h));
+    dft_nf_.push_back(static_cast<int>(freqs.size()));
+    return h;
+  }
+  std::vector<std::complex<double>> dft(int handle) const {
+    long long np = 0;
+    check(fdtd_dft_npoints(g_.get(), handle, &np));
+    std::vector<double> raw(static_cast<size_t>(dft_nf_.at(handle)) * np * 2);
+    check(fdtd_dft_read(g_.get(), handle, raw.data()));
+    std::vector<std::complex<double>> out(raw.size() / 2);
+    for (size_t q = 0; q < out.size(); q++) out[q] = {raw[2 * q], raw[2 * q + 1]};
+    return out;
+  }
+
  private:
   struct Deleter {
     void operator()(fdtd_grid* g) const { fdtd_grid_destroy(g); }
@@ -575,6 +607,7 @@ class Grid {
   bool pml_axes_[3] = {false, false, false};
   bool has_map_ = false, validated_ = false;
   std::vector<detail::Op> plan_;
+  std::vector<int> dft_nf_;
   fdtd_material mat_e_{}, mat_h_{};
 };
 

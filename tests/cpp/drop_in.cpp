@@ -3,7 +3,8 @@
 //   tm: 2D TM, FP64 plain, 40 x 36, 6-cell CPML, Gaussian soft source on Ez
 //       (the user loop of tests/testTM.cpp with the reference's names);
 //   bd: 2D TM, FP64 plain, 36 x 30, BD3 time policy, PEC face at x min,
-//       CPML at x max, periodic faces in y;
+//       CPML at x max, periodic faces in y; also writes the surface current
+//       Jh_x on the interior and the running DFT of Je_z on a box;
 //   td: 3D, FP32 fused, 24^3, 4-cell CPML, Drude cube in a material map,
 //       x-propagating TFSF box (6 planes) with an Aux1D Gaussian.
 // Writes the listed fields (float64, x fastest) to out.bin.
@@ -75,10 +76,19 @@ int main(int argc, char** argv) {
                  UpdatePML<TM, FieldType::Magnetic, Dir::X>(dt, dx),
                  VacuumUpdate<TM, FieldType::Magnetic>(),
                  pec.updateH(), ylo.updateH(), yhi.updateH()});
+      const int hd = grid.add_dft(FDTD_Q_JEZ, {2, 2, 0}, {33, 27, 0}, {0.03, 0.05});
       grid.step(steps);
       dump(out, grid.get<Ez>());
       dump(out, grid.get<Hx>());
       dump(out, grid.get<Hy>());
+      // surface current Jh_x on the interior, and the Je_z spectrum
+      dump(out, grid.read(FDTD_Q_JHX, {1, 1, 0}, {34, 28, 0}));
+      std::vector<double> spec;
+      for (auto& z : grid.dft(hd)) {
+        spec.push_back(z.real());
+        spec.push_back(z.imag());
+      }
+      dump(out, spec);
       // mixed time policies are refused
       try {
         grid.plan({YeeUpdate<TM, Dz, BD3>(dt, dx), UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx),

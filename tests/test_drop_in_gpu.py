@@ -63,7 +63,18 @@ def test_tm_bd3_boundaries_through_templates(drop_in, oracle, tmp_path):
     p.time_scheme = 3
     n = np.arange(90, dtype=np.float64)
     p.sources.append(Source(2, (10, 8, 0), np.exp(-(((n - 20.0) / 6.0) ** 2)), "E"))
+    from fdtd_b200.problem import DFTRegion
+    p.dfts.append(DFTRegion(8, (2, 2, 0), (33, 27, 0), [0.03, 0.05]))
     o = oracle.run_oracle(p, 90)
-    got = run(drop_in, "bd", tmp_path, 3, (1, 30, 36))
+    out = str(tmp_path / "bd.bin")
+    subprocess.run([drop_in, "bd", out], check=True)
+    raw = np.fromfile(out, dtype=np.float64)
+    n = 30 * 36
     for q, name in enumerate(["Ez", "Hx", "Hy"]):
-        assert rel_l2(got[q], o.get(name)) <= 1e-12, name
+        assert rel_l2(raw[q * n:(q + 1) * n].reshape(1, 30, 36), o.get(name)) <= 1e-12, name
+    jh = raw[3 * n:3 * n + 34 * 28]
+    assert rel_l2(jh, o.read_quantity(9, (1, 1, 0), (34, 28, 0)).ravel()) <= 1e-12
+    spec = raw[3 * n + 34 * 28:]
+    ref = o.dft(0).ravel()
+    got = spec[0::2] + 1j * spec[1::2]
+    assert rel_l2(got, ref) <= 1e-12

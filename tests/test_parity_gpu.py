@@ -118,6 +118,40 @@ def test_fused_3d_sweep_kernels(fdtd, oracle, make, sweep):
     _compare(p, g, o, E + H, FUSED_TOL)
 
 
+def _all_dispersive(kind):
+    """td_drude_lorentz with a material table that holds dispersive
+    materials only (the sweeps then stage the ADE state with the fields)."""
+    from fdtd_b200.problem import Material
+    p = scenarios.td_drude_lorentz()
+    dt = p.dt
+    drude = Material.drude(1.0, 0.3 / dt, 0.01 / dt)
+    if kind == "drude":
+        p.materials, p.ids = [drude], None
+    elif kind == "drude_lorentz1":
+        p.materials = [drude, Material.lorentz(2.0, [(1.0, 0.1 / dt, 0.005 / dt)])]
+        p.ids = (p.ids == 2).astype(np.uint8)
+    else:
+        p.materials = [Material.lorentz(2.0, [(1.5, 0.1 / dt, 0.005 / dt), (0.8, 0.25 / dt, 0.02 / dt)]),
+                       Material.lorentz(3.0, [(1.0, 0.12 / dt, 0.01 / dt), (0.5, 0.2 / dt, 0.03 / dt)])]
+        p.ids = (p.ids == 1).astype(np.uint8)
+    p.name = f"td_all_{kind}"
+    return p
+
+
+@pytest.mark.parametrize("sweep", ["regs", "tma", "flat", "staged"])
+@pytest.mark.parametrize("kind", ["drude", "drude_lorentz1", "lorentz2"])
+def test_all_dispersive_tables_every_sweep(fdtd, oracle, kind, sweep):
+    p = _all_dispersive(kind)
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.set_sweep_kernel(sweep)
+    g.step(p.steps)
+    g.synchronize()
+    assert g.error_flags() == 0
+    E, H, _, _ = mode_fields(p.mode)
+    _compare(p, g, o, E + H, FUSED_TOL)
+
+
 def test_multistep_schemes_are_fp64_only(fdtd):
     p = scenarios.tm_bd3_tfsf()
     with pytest.raises(fdtd.FdtdError):
