@@ -657,10 +657,15 @@ def main():
         barrier()
         t0 = time.perf_counter()
         ge = G.Grid.from_problem(pe, "f32", device=local)
+        ge.synchronize()
+        t1 = time.perf_counter()
         ge.step(args.steps)
+        ge.synchronize()
+        t2 = time.perf_counter()
         spectra = [ge.dft(q) for q in range(len(pe.dfts))]
         ge.synchronize()
         t_e2e = time.perf_counter() - t0
+        parts = {"create_s": t1 - t0, "steps_s": t2 - t1, "read_s": t_e2e - (t2 - t0)}
         h2d = (pe.ids.nbytes if pe.ids is not None else 0) + sum(s.values.nbytes for s in pe.sources)
         if pe.tfsf is not None:
             h2d += pe.tfsf.aux_values.nbytes
@@ -670,7 +675,7 @@ def main():
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e = {"value": cells * args.steps * world / float(tt.item()) / 1e9, "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "wall_s": float(tt.item()),
+               "wall_s": float(tt.item()), "parts": parts,
                "note": "grid creation through the C ABI, H2D of material ids/source/aux tables, the steps and D2H "
                        "of all DFT spectra, timed by the host clock (the synthetic problem is built before)"}
         ge.close()

@@ -943,7 +943,12 @@ int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) {
   BcFaces nb{};
   for (int q = 0; q < g->bcs.n; q++)
     if (g->bcs.face[q].axis != axis || g->bcs.face[q].side != side) nb.face[nb.n++] = g->bcs.face[q];
-  if (kind != FDTD_BC_NONE) nb.face[nb.n++] = BcFace{axis, side, kind};
+  if (kind != FDTD_BC_NONE) {
+    BcFace fc{axis, side, kind, {}};
+    for (int ft = 0; ft < 2; ft++)
+      for (int c = 0; c < 3; c++) fc.sgn[ft][c] = bc_sign(kind, ft, c, axis);
+    nb.face[nb.n++] = fc;
+  }
   g->bcs = nb;
   g->version++;
   return FDTD_OK;

@@ -239,7 +239,10 @@ int launch_chunk_start(Control* ctrl, cudaStream_t s);
 // 4 antisymmetric, 5 periodic)
 struct BcFace {
   int axis, side, kind;
+  float sgn[2][3];  // the condition's sign per component, E (0) and H (1) half
 };
+// the sign of component c of field type ft for a face of `kind` normal to axis
+__host__ __device__ float bc_sign(int kind, int ft, int c, int axis);
 struct BcFaces {
   int n;
   BcFace face[6];

@@ -5,6 +5,8 @@
 // include/DataCapture.hpp:61-191; this capture is defined here):
 //   X_f += x[n] * exp(-2 pi i f n), n = t+1 for E, t+1.5 for H,
 // accumulated in FP64 whatever the field precision.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace fdtdb {
@@ -198,10 +200,11 @@ __global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }
 // Boundary conditions (include/BoundaryUpdates.hpp:230-760): on each face
 // with one, the outer cell takes the image of the interior cell next to the
 // face (periodic: of the interior cell at the far end of the axis), every
-// component of the half step's field times the sign of the condition. One
-// grid row (blockIdx.y) per face; cells of a face x fastest over the
-// interior range of the two other axes.
-__device__ __forceinline__ float bc_sign(int kind, int ft, int c, int axis) {
+// component of the half step's field times the sign of the condition.
+// Launch: blockIdx.z = face; the 2D thread grid spans the face's two
+// transverse axes (u, v) = (y, z) for x faces, (x, z) for y faces and (x, y)
+// for z faces, so y and z faces are read and written along x, coalesced.
+__host__ __device__ float bc_sign(int kind, int ft, int c, int axis) {
   const bool normal = c == axis;
   switch (kind) {
     case 1: return ft == 0 ? (normal ? 1.f : -1.f) : (normal ? -1.f : 1.f);  // PEC
@@ -213,45 +216,53 @@ __device__ __forceinline__ float bc_sign(int kind, int ft, int c, int axis) {
 }
 
 template <typename T>
-__global__ void boundary_kernel(BcFaces f, int ft, T* f0, T* f1, T* f2, int nx, int ny, int nz, int rowlen) {
-  const BcFace& b = f.face[blockIdx.y];
-  int lo[3] = {1, 1, nz > 1 ? 1 : 0}, ext[3] = {nx - 2, ny - 2, nz > 1 ? nz - 2 : 1};
-  ext[b.axis] = 1;
-  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (q >= static_cast<long long>(ext[0]) * ext[1] * ext[2]) return;
-  int idx[3];
-  idx[0] = lo[0] + static_cast<int>(q % ext[0]);
-  idx[1] = lo[1] + static_cast<int>((q / ext[0]) % ext[1]);
-  idx[2] = lo[2] + static_cast<int>(q / (static_cast<long long>(ext[0]) * ext[1]));
+__global__ void __launch_bounds__(256) boundary_kernel(BcFaces f, int ft, T* f0, T* f1, T* f2, int nx, int ny,
+                                                       int nz, int rowlen) {
+  const BcFace& b = f.face[blockIdx.z];
+  const int ua = b.axis == 0 ? 1 : 0, va = b.axis == 2 ? 1 : 2;  // transverse axes
   const int n[3] = {nx, ny, nz};
-  int src[3] = {idx[0], idx[1], idx[2]}, dst[3] = {idx[0], idx[1], idx[2]};
-  dst[b.axis] = b.side == 0 ? 0 : n[b.axis] - 1;
-  src[b.axis] = b.kind == 5 ? (b.side == 0 ? n[b.axis] - 2 : 1) : (b.side == 0 ? 1 : n[b.axis] - 2);
+  const int three = nz > 1;
+  const int u = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = (va < 2 || three) ? 1 + static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y)
+                                  : static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+  if (u > n[ua] - 2) return;
+  if (va == 2 && !three ? v != 0 : v > n[va] - 2) return;
+  int dst[3], src[3];
+  dst[ua] = src[ua] = u;
+  dst[va] = src[va] = v;
+  const int na = n[b.axis];
+  dst[b.axis] = b.side == 0 ? 0 : na - 1;
+  src[b.axis] = b.kind == 5 ? (b.side == 0 ? na - 2 : 1) : (b.side == 0 ? 1 : na - 2);
   const long long cs = (static_cast<long long>(src[2]) * ny + src[1]) * rowlen + src[0];
   const long long cd = (static_cast<long long>(dst[2]) * ny + dst[1]) * rowlen + dst[0];
-  T* fs[3] = {f0, f1, f2};
-#pragma unroll
-  for (int c = 0; c < 3; c++)
-    if (fs[c]) fs[c][cd] = static_cast<T>(bc_sign(b.kind, ft, c, b.axis)) * fs[c][cs];
+  const T s0 = static_cast<T>(b.sgn[ft][0]), s1 = static_cast<T>(b.sgn[ft][1]), s2 = static_cast<T>(b.sgn[ft][2]);
+  const T v0 = f0 ? f0[cs] : T(0), v1 = f1 ? f1[cs] : T(0), v2 = f2 ? f2[cs] : T(0);
+  if (f0) f0[cd] = s0 * v0;
+  if (f1) f1[cd] = s1 * v1;
+  if (f2) f2[cd] = s2 * v2;
 }
 
 int launch_boundaries(const BcFaces& f, int ft, int is_f32, void* const* fields, int nx, int ny, int nz, int rowlen,
                       cudaStream_t s) {
   if (f.n == 0) return 0;
-  long long most = 0;
+  // the largest transverse extents over the faces
+  int mu = 1, mv = 1;
+  const int n[3] = {nx, ny, nz};
   for (int q = 0; q < f.n; q++) {
-    long long e[3] = {nx - 2, ny - 2, nz > 1 ? nz - 2 : 1};
-    e[f.face[q].axis] = 1;
-    most = e[0] * e[1] * e[2] > most ? e[0] * e[1] * e[2] : most;
+    const int ax = f.face[q].axis;
+    const int ua = ax == 0 ? 1 : 0, va = ax == 2 ? 1 : 2;
+    mu = std::max(mu, n[ua] - 2);
+    mv = std::max(mv, va == 2 && nz == 1 ? 1 : n[va] - 2);
   }
-  const dim3 grid(static_cast<unsigned>((most + 255) / 256), f.n);
+  const dim3 block(32, 8, 1);
+  const dim3 grid(static_cast<unsigned>((mu + 31) / 32), static_cast<unsigned>((mv + 7) / 8), f.n);
   if (is_f32)
-    boundary_kernel<float><<<grid, 256, 0, s>>>(f, ft, static_cast<float*>(fields[0]), static_cast<float*>(fields[1]),
-                                                static_cast<float*>(fields[2]), nx, ny, nz, rowlen);
+    boundary_kernel<float><<<grid, block, 0, s>>>(f, ft, static_cast<float*>(fields[0]), static_cast<float*>(fields[1]),
+                                                  static_cast<float*>(fields[2]), nx, ny, nz, rowlen);
   else
-    boundary_kernel<double><<<grid, 256, 0, s>>>(f, ft, static_cast<double*>(fields[0]),
-                                                 static_cast<double*>(fields[1]), static_cast<double*>(fields[2]), nx,
-                                                 ny, nz, rowlen);
+    boundary_kernel<double><<<grid, block, 0, s>>>(f, ft, static_cast<double*>(fields[0]),
+                                                   static_cast<double*>(fields[1]), static_cast<double*>(fields[2]),
+                                                   nx, ny, nz, rowlen);
   return 1;
 }
 
