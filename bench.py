@@ -54,6 +54,9 @@ MEASURED_TRAFFIC = {
     ("drude384", "flat"): {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
                            "source": "ncu capture at 256^3 scaled by interior cells "
                                      "(profiles/flat_sweeps_tfsf_drude256.md)"},
+    ("lorentz768", "staged"): {"e": 7581.576e6 / 55742968, "h": 2209.036e6 / 55742968,
+                               "source": "ncu capture at 384^3 scaled by interior cells "
+                                         "(profiles/staged_sweeps_lorentz384.md)"},
 }
 
 
