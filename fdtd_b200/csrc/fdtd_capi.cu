@@ -175,6 +175,7 @@ struct fdtd_grid {
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
   bool dirty_dft = true;
+  bool dirty_pml = false;  // host CPML profiles changed: device profiles and slabs follow before use
   int next_half = 0;  // fdtd_step_half: the phase expected next
   BcFaces bcs{};      // faces with a boundary condition
   int scheme = 1;     // time policy of the curl updates: 1 BD1, 3 BD3, 4 BD4
@@ -278,6 +279,20 @@ int upload_profiles(fdtd_grid* g) {
         }
       }
     }
+  return FDTD_OK;
+}
+
+int alloc_psi(fdtd_grid* g);
+
+// fdtd_set_pml regrades the host profiles only; the device profiles and the
+// CPML integrator slabs (zeroed) follow here, once, before anything reads them
+int ensure_pml(fdtd_grid* g) {
+  if (!g->dirty_pml) return FDTD_OK;
+  int rc = upload_profiles(g);
+  if (rc) return rc;
+  rc = alloc_psi(g);
+  if (rc) return rc;
+  g->dirty_pml = false;
   return FDTD_OK;
 }
 
@@ -776,9 +791,9 @@ int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) {
   for (int s = 0; s < 2; s++)
     if (g->pml[axis][s] > 0)
       grade(g->d.dx, g->d.dt, g->n[axis], g->pml[axis][s], s, g->prof[0][axis], g->prof[1][axis]);
-  int rc = upload_profiles(g);
-  if (rc) return rc;
-  return alloc_psi(g);
+  g->dirty_pml = true;
+  g->version++;
+  return FDTD_OK;
 }
 
 int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
@@ -801,12 +816,13 @@ int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
 int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) {
   if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
   const long long n = static_cast<long long>(g->n[0]) * g->n[1] * g->n[2];
+  // range check in one pass, then the rows copied into the padded layout
+  uint8_t top = 0;
+  for (long long c = 0; c < n; c++) top = ids[c] > top ? ids[c] : top;
+  if (top >= g->mats.size()) return fail(FDTD_ERR_INVALID, "material id out of range of the material table");
   std::vector<uint8_t> v(static_cast<size_t>(field_elems(g)), 0);
-  for (long long c = 0; c < n; c++) {
-    if (ids[c] >= g->mats.size()) return fail(FDTD_ERR_INVALID, "material id out of range of the material table");
-    const long long i = c % g->n[0], j = (c / g->n[0]) % g->n[1], k = c / (static_cast<long long>(g->n[0]) * g->n[1]);
-    v[(k * g->n[1] + j) * rowlen(g) + i] = ids[c];
-  }
+  const long long rows = static_cast<long long>(g->n[1]) * g->n[2], rl = rowlen(g);
+  for (long long r = 0; r < rows; r++) memcpy(v.data() + r * rl, ids + r * g->n[0], static_cast<size_t>(g->n[0]));
   CK(cudaSetDevice(g->d.device));
   if (g->d_bids) {
     dfree(g, g->d_bids);
@@ -1116,6 +1132,19 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
 
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream) { return step_impl(g, nsteps, stream, nullptr); }
 
+int fdtd_prepare(fdtd_grid* g) {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  CK(cudaSetDevice(g->d.device));
+  int rc = ensure_pml(g);
+  if (rc) return rc;
+  if (g->dirty_dft) {
+    rc = rebuild_dft(g);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(g->stream));
+  return FDTD_OK;
+}
+
 int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms) {
   if (!ms) return fail(FDTD_ERR_INVALID, "null argument");
   return step_impl(g, nsteps, stream, ms);
@@ -1205,6 +1234,11 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(g->d.device));
+  {
+    // before any graph capture: the CPML set-up synchronises its stream
+    const int prc = ensure_pml(g);
+    if (prc) return prc;
+  }
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
   if (s != g->stream) {
     // order the caller's stream after any set-up work on ours
@@ -1323,6 +1357,10 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
     }
     if (!g->auxes.empty()) g->launches += launch_chunk_start(g->ctrl, s);
   }
+  {
+    const int prc = ensure_pml(g);
+    if (prc) return prc;
+  }
   FusedArgs fa;
   PlainArgs pa;
   if (g->f32) fa = fused_args(g);
@@ -1398,6 +1436,10 @@ int fdtd_synchronize(fdtd_grid* g) {
 // which -> (device pointer, scale to SI, element layout)
 static int locate(fdtd_grid* g, int which, void** p, double* scale, int* psi_axis) {
   *p = nullptr;
+  if (which >= 18 && which < 36) {
+    const int prc = ensure_pml(g);
+    if (prc) return prc;
+  }
   *scale = 1.0;
   *psi_axis = -1;
   const double eps0 = kEps0, dt = g->d.dt;
@@ -1720,6 +1762,8 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
   std::vector<FusedArgs> args;
   std::vector<Control*> ctrls;
   for (auto* g : b->grids) {
+    const int prc = ensure_pml(g);
+    if (prc) return prc;
     CK(cudaStreamSynchronize(g->stream));
     args.push_back(fused_args(g));
     ctrls.push_back(g->ctrl);
@@ -1964,12 +2008,16 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
                                       std::to_string(kStaticAuxBytes) + "; this grid takes at most " +
                                       std::to_string(most < 0 ? 0 : most) + " steps per call");
   }
+  if (g->dirty_pml)
+    return fail(FDTD_ERR_INVALID,
+                "fdtd_step_static_scratch: the CPML changed since the last fdtd_step; fdtd_prepare (or one "
+                "fdtd_step) lays out its integrator slabs first");
   if (g->dirty_dft) {
     // laying out DFT regions allocates their sample buffers
     if (!g->dfts.empty())
       return fail(FDTD_ERR_INVALID,
-                  "fdtd_step_static_scratch: DFT regions were added since the last fdtd_step; one fdtd_step "
-                  "call (one step or more) lays out their buffers first");
+                  "fdtd_step_static_scratch: DFT regions were added since the last fdtd_step; fdtd_prepare (or "
+                  "one fdtd_step) lays out their buffers first");
     rc = rebuild_dft(g);
     if (rc) return rc;
   }
@@ -2130,6 +2178,10 @@ int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, 
   for (auto& m : g->mats)
     if (m.mu_r != 1.0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes mu_r = 1");
   if (ckpt_every < 1 || ckpt_every > 4096) return fail(FDTD_ERR_INVALID, "ckpt_every must be 1..4096");
+  {
+    const int prc = ensure_pml(g);
+    if (prc) return prc;
+  }
   if (!interior(g, probe_lo[0], probe_lo[1], 0) || !interior(g, probe_hi[0], probe_hi[1], 0) ||
       probe_lo[0] > probe_hi[0] || probe_lo[1] > probe_hi[1])
     return fail(FDTD_ERR_INVALID, "probe box must be a non-empty box of interior cells");

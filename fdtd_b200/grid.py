@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
            "fdtd_batch_info",
@@ -80,6 +80,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_set_eps_map": [vp, dp],
         "fdtd_set_boundary": [vp, i, i, i],
         "fdtd_set_time_scheme": [vp, i],
+        "fdtd_prepare": [vp],
         "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_step_half": [vp, i, vp],
         "fdtd_copy_plane": [vp, i, i, vp, i, vp],
@@ -186,6 +187,10 @@ class Grid:
         """kind: 'none', 'pec', 'pmc', 'symmetric', 'antisymmetric' or 'periodic'."""
         code = 0 if kind == "none" else P.BOUNDARY_KINDS[kind]
         _check(load_library().fdtd_set_boundary(self.h, int(axis), int(side), code))
+
+    def prepare(self) -> None:
+        """Lay out the deferred device state (CPML slabs, DFT buffers) now."""
+        _check(load_library().fdtd_prepare(self.h))
 
     def set_time_scheme(self, scheme: int) -> None:
         """1 (BD1, leapfrog), 3 (BD3) or 4 (BD4): the TimePolicy of every
@@ -343,10 +348,10 @@ class Grid:
         n = ctypes.c_longlong()
         _check(L.fdtd_dft_npoints(self.h, handle, ctypes.byref(n)))
         nf = self.dft_meta[handle]
-        out = np.empty(nf * n.value * 2, dtype=np.float64)
-        _check(L.fdtd_dft_read(self.h, handle, _dp(out)))
-        out = out.reshape(nf, n.value, 2)
-        return out[..., 0] + 1j * out[..., 1]
+        # (re, im) pairs as written by the C ABI are complex128 in memory
+        out = np.empty((nf, n.value), dtype=np.complex128)
+        _check(L.fdtd_dft_read(self.h, handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     def check_finite(self) -> None:
         _check(load_library().fdtd_check_finite(self.h))

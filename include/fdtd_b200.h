@@ -216,6 +216,13 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream);
  * precision, x fastest (to_grid = 1: buffer to grid). The FP32 method stores
  * eta*H, and that is what is copied. Stream-ordered on `stream`. */
 int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream);
+/* Lays out the device state that the set-up calls defer: the CPML
+ * coefficient profiles and integrator slabs (fdtd_set_pml regrades on the
+ * host only) and the DFT sample buffers. fdtd_step and fdtd_step_half do it
+ * themselves; call it before the first fdtd_step_static_scratch of a grid
+ * that has not stepped, which allocates nothing. No counterpart in the
+ * reference (its cells carry their CPML state from construction). */
+int fdtd_prepare(fdtd_grid* g);
 /* fdtd_step for callers that cannot allocate device memory while stepping
  * (no counterpart in the reference, whose steps run on the host). Same
  * kernels, order and results as fdtd_step, launched eagerly; the per-call

@@ -21,12 +21,11 @@ def test_static_scratch_step_matches_step(fdtd, make, prec):
     p = make()
     ref = fdtd.Grid.from_problem(p, prec)
     new = fdtd.Grid.from_problem(p, prec)
-    if p.dfts:
-        # one ordinary step lays out the DFT sample buffers of both grids
-        ref.step(1)
-        new.step(1)
+    # lay out what set-up deferred (CPML slabs, DFT buffers) before the
+    # first no-allocation step
+    new.prepare()
     E, H, _, _ = mode_fields(p.mode)
-    n = (p.steps - 1) // 2
+    n = p.steps // 2
     for _ in range(2):
         ref.step(n)
         new.step_static_scratch(n)
@@ -61,3 +60,19 @@ def test_static_scratch_step_needs_dft_layout(fdtd):
     g.step(1)
     g.step_static_scratch(4)
     assert g.step_count == 5
+
+
+def test_static_scratch_step_after_prepare(fdtd):
+    """fdtd_prepare lays out the CPML slabs and DFT buffers, after which the
+    no-allocation step runs on a grid that never took an ordinary step."""
+    p = scenarios.td_tfsf_box()
+    ref = fdtd.Grid.from_problem(p, "f32")
+    new = fdtd.Grid.from_problem(p, "f32")
+    with pytest.raises(fdtd.FdtdError):
+        new.step_static_scratch(4)  # CPML and DFT layout pending
+    new.prepare()
+    ref.step(20)
+    new.step_static_scratch(20)
+    for name in ("Ex", "Ez", "Hy"):
+        assert rel_l2(new.get(name), ref.get(name)) <= TOL["f32"], name
+    assert rel_l2(new.dft(0), ref.dft(0)) <= TOL["f32"]
