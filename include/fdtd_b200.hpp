@@ -19,6 +19,8 @@
 #pragma once
 
 #include <array>
+#include <cctype>
+#include <map>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -450,6 +452,12 @@ class Grid {
   // A per-cell material map: ids index `mats` (the role of MaterialMap,
   // include/MaterialMap.hpp:204-284). The plan's material op must then be
   // MaterialMapUpdate.
+  // the same from C-ABI material rows (e.g. xml::read_material_map's values)
+  void set_material_map(const std::vector<fdtd_material>& mats, const std::vector<uint8_t>& ids) {
+    check(fdtd_set_materials(g_.get(), mats.data(), static_cast<int>(mats.size())));
+    check(fdtd_set_material_ids(g_.get(), ids.data()));
+    has_map_ = true;
+  }
   void set_material_map(const std::vector<detail::Op>& mats, const std::vector<uint8_t>& ids) {
     std::vector<fdtd_material> m;
     for (auto& o : mats) m.push_back(o.mat);
@@ -623,4 +631,228 @@ struct MaterialMapUpdate {
 };
 
 }  // namespace gpu
+
+// ------------------------------------------------------------ configuration files
+// Readers of the reference's XML configuration: MaterialMap::readXML
+// (include/MaterialMap.hpp:236-282) with MaterialPair::readXML (:134-181) and
+// the storages' readXML (DispersiveMaterials.hpp:411-427, :466-471,
+// :822-865, :1117-1147); PMLOptions::readXML (PML.hpp:215-281);
+// BoundaryOptions::readXML (BoundaryUpdates.hpp:163-223). The reference reads
+// them with tinyxml2; this is a small element-tree parser of its own (tags
+// and text; declarations, comments and attributes are skipped). Unknown
+// names throw, as MapNameTo does (FDTDConstants.hpp:107-124); dispersions and
+// boundaries the GPU path does not implement throw Error(FDTD_ERR_UNSUPPORTED).
+namespace xml {
+
+struct Node {
+  std::string tag, text;
+  std::vector<Node> kids;
+  const Node* child(const std::string& t) const {
+    for (auto& k : kids)
+      if (k.tag == t) return &k;
+    return nullptr;
+  }
+};
+
+namespace detail {
+inline void skip_ws(const std::string& s, size_t& p) {
+  while (p < s.size() && std::isspace(static_cast<unsigned char>(s[p]))) p++;
+}
+inline std::string trim(const std::string& t) {
+  size_t a = 0, b = t.size();
+  while (a < b && std::isspace(static_cast<unsigned char>(t[a]))) a++;
+  while (b > a && std::isspace(static_cast<unsigned char>(t[b - 1]))) b--;
+  return t.substr(a, b - a);
+}
+inline void skip_misc(const std::string& s, size_t& p) {
+  for (;;) {
+    skip_ws(s, p);
+    if (s.compare(p, 4, "<!--") == 0) {
+      const size_t e = s.find("-->", p);
+      p = e == std::string::npos ? s.size() : e + 3;
+    } else if (s.compare(p, 2, "<?") == 0) {
+      const size_t e = s.find("?>", p);
+      p = e == std::string::npos ? s.size() : e + 2;
+    } else {
+      return;
+    }
+  }
+}
+inline Node parse_element(const std::string& s, size_t& p) {
+  if (p >= s.size() || s[p] != '<') throw std::runtime_error("xml: element expected");
+  const size_t e = s.find('>', p);
+  if (e == std::string::npos) throw std::runtime_error("xml: unterminated tag");
+  std::string head = s.substr(p + 1, e - p - 1);
+  p = e + 1;
+  const bool empty = !head.empty() && head.back() == '/';
+  if (empty) head.pop_back();
+  Node n;
+  n.tag = head.substr(0, head.find_first_of(" \t\r\n"));
+  if (empty) return n;
+  for (;;) {
+    const size_t lt = s.find('<', p);
+    if (lt == std::string::npos) throw std::runtime_error("xml: unterminated element " + n.tag);
+    n.text += s.substr(p, lt - p);
+    p = lt;
+    if (s.compare(p, 4, "<!--") == 0 || s.compare(p, 2, "<?") == 0) {
+      skip_misc(s, p);
+      continue;
+    }
+    if (s.compare(p, 2, "</") == 0) {
+      const size_t ce = s.find('>', p);
+      if (ce == std::string::npos || trim(s.substr(p + 2, ce - p - 2)) != n.tag)
+        throw std::runtime_error("xml: mismatched closing tag for " + n.tag);
+      p = ce + 1;
+      n.text = trim(n.text);
+      return n;
+    }
+    n.kids.push_back(parse_element(s, p));
+  }
+}
+inline double number(const Node* n) {
+  if (!n) throw std::runtime_error("xml: value missing");
+  return std::stod(n->text);
+}
+}  // namespace detail
+
+// the document element of an XML text
+inline Node parse(const std::string& text) {
+  size_t p = 0;
+  detail::skip_misc(text, p);
+  return detail::parse_element(text, p);
+}
+
+// One material of a map: the C-ABI row (kind, eps_inf, mu_r, poles). Electric
+// Vacuum/Constant/Drude/Lorentz and magnetic Vacuum/Constant are supported;
+// a Lorentz <Delta> is read but, as in the reference's update, not used.
+inline fdtd_material material_pair(const Node& pair) {
+  const Node* el = pair.child("Electric");
+  const Node* mg = pair.child("Magnetic");
+  if (!el || !mg || el->kids.empty() || mg->kids.empty())
+    throw std::runtime_error("xml: a MaterialPair needs <Electric> and <Magnetic>");
+  static const char* known[] = {"Vacuum", "Constant", "Conductive", "Drude", "FluidDrude", "Lorentz",
+                                "MagnetizedDrude", "SelfMagnetizedDrude", "MagnetizedFluidDrude",
+                                "SelfMagnetizedFluidDrude", "MultiCoefficient", "Anisotropic"};
+  auto check_name = [&](const std::string& t) {
+    for (auto* k : known)
+      if (t == k) return;
+    throw std::runtime_error("xml: unknown dispersion " + t);
+  };
+  const Node& e = el->kids[0];
+  const Node& m = mg->kids[0];
+  check_name(e.tag);
+  check_name(m.tag);
+  fdtd_material r = ::fdtd::detail::blank_material(FDTD_VACUUM);
+  if (m.tag == "Constant") r.mu_r = detail::number(m.child("Constant"));
+  else if (m.tag != "Vacuum")
+    throw gpu::Error(FDTD_ERR_UNSUPPORTED, "magnetic dispersion " + m.tag + " is not implemented on the GPU path");
+  if (e.tag == "Vacuum") return r;
+  r.eps_inf = detail::number(e.child("Constant"));
+  if (e.tag == "Constant") {
+    r.kind = FDTD_CONSTANT;
+  } else if (e.tag == "Drude" || e.tag == "Lorentz") {
+    r.kind = e.tag == "Drude" ? FDTD_DRUDE : FDTD_LORENTZ;
+    r.npoles = 1;
+    r.delta_eps[0] = 1.0;
+    r.freq[0] = detail::number(e.child("Freq"));
+    r.gamma[0] = detail::number(e.child("Gamma"));
+  } else {
+    throw gpu::Error(FDTD_ERR_UNSUPPORTED, "electric dispersion " + e.tag + " is not implemented on the GPU path");
+  }
+  return r;
+}
+
+// identifier -> material; the first of repeated identifiers is kept, as
+// std::map::insert does
+inline std::map<std::string, fdtd_material> read_material_map(const std::string& text) {
+  const Node root = parse(text);
+  std::map<std::string, fdtd_material> out;
+  for (auto& item : root.kids) {
+    if (item.tag != "Item") continue;
+    const Node* id = item.child("Identifier");
+    const Node* pair = item.child("MaterialPair");
+    if (!id || !pair) throw std::runtime_error("xml: an <Item> needs <Identifier> and <MaterialPair>");
+    out.emplace(id->text, material_pair(*pair));
+  }
+  return out;
+}
+
+// PMLOptions: N (default 10) and a 0/1 flag per face (default off)
+struct PMLOptions {
+  int N = 10;
+  bool face[3][2] = {{false, false}, {false, false}, {false, false}};
+};
+inline PMLOptions read_pml_options(const std::string& text) {
+  const Node root = parse(text);
+  PMLOptions o;
+  static const char* axes[3] = {"X", "Y", "Z"};
+  for (auto& c : root.kids) {
+    if (c.tag == "N") o.N = static_cast<int>(detail::number(&c));
+    for (int a = 0; a < 3; a++) {
+      if (c.tag != axes[a]) continue;
+      for (auto& m : c.kids) {
+        const int side = m.tag == "MIN" ? 0 : m.tag == "MAX" ? 1 : -1;
+        if (side < 0) continue;
+        if (m.text != "0" && m.text != "1") throw std::runtime_error("xml: a 0/1 flag is expected in <" + m.tag + ">");
+        o.face[a][side] = m.text == "1";
+      }
+    }
+  }
+  return o;
+}
+
+// BoundaryOptions: a boundary name per face (default PEC)
+struct BoundaryOptions {
+  std::string face[3][2] = {{"PEC", "PEC"}, {"PEC", "PEC"}, {"PEC", "PEC"}};
+  // the specs of the faces of a dim-dimensional grid that carry a condition
+  // (NONE and Parallel faces get none; BlochPeriodic is not implemented)
+  std::vector<BoundarySpec> specs(int dim) const {
+    std::vector<BoundarySpec> v;
+    for (int a = 0; a < dim; a++)
+      for (int s = 0; s < 2; s++) {
+        const std::string& f = face[a][s];
+        int kind = -1;
+        if (f == "PEC") kind = FDTD_BC_PEC;
+        else if (f == "PMC") kind = FDTD_BC_PMC;
+        else if (f == "Symmetric") kind = FDTD_BC_SYMMETRIC;
+        else if (f == "Antisymmetric") kind = FDTD_BC_ANTISYMMETRIC;
+        else if (f == "Periodic") kind = FDTD_BC_PERIODIC;
+        else if (f == "BlochPeriodic")
+          throw gpu::Error(FDTD_ERR_UNSUPPORTED, "BlochPeriodic boundaries are not implemented on the GPU path");
+        if (kind >= 0) v.push_back(BoundarySpec{a, s, kind});
+      }
+    return v;
+  }
+};
+// the CPML of the flagged faces on a grid's axes
+template <class Grid>
+void apply(Grid& grid, const PMLOptions& o, int dim) {
+  for (int a = 0; a < dim; a++)
+    for (int s = 0; s < 2; s++)
+      if (o.face[a][s]) grid.set_pml(static_cast<Dir>(a), s == 0 ? Orientation::MIN : Orientation::MAX, o.N);
+}
+
+inline BoundaryOptions read_boundary_options(const std::string& text) {
+  const Node root = parse(text);
+  BoundaryOptions o;
+  static const char* axes[3] = {"X", "Y", "Z"};
+  static const char* names[] = {"Periodic", "BlochPeriodic", "PEC", "PMC", "Symmetric", "Antisymmetric",
+                                "Parallel", "NONE"};
+  for (auto& c : root.kids)
+    for (int a = 0; a < 3; a++) {
+      if (c.tag != axes[a]) continue;
+      for (auto& m : c.kids) {
+        const int side = m.tag == "MIN" ? 0 : m.tag == "MAX" ? 1 : -1;
+        if (side < 0) continue;
+        const std::string name = m.kids.empty() ? m.text : m.kids[0].tag;
+        bool ok = false;
+        for (auto* n : names) ok = ok || name == n;
+        if (!ok) throw std::runtime_error("xml: unknown boundary " + name);
+        o.face[a][side] = name;
+      }
+    }
+  return o;
+}
+
+}  // namespace xml
 }  // namespace fdtd

@@ -178,3 +178,29 @@ def test_loaded_config_runs_like_the_hand_built_problem(oracle):
     ga, gb = oracle.run_oracle(a), oracle.run_oracle(b)
     for n in ("Ex", "Ey", "Hz"):
         assert np.array_equal(ga.get(n), gb.get(n)), n
+
+
+def test_cpp_readers_match_the_spec(tmp_path):
+    """The C++ layer's readers (fdtd::xml in include/fdtd_b200.hpp) on the
+    same golden documents give the same values; tests/cpp/config_xml.cpp also
+    checks their errors. Compiled and run on the host, no GPU needed."""
+    exe = str(tmp_path / "config_xml")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(HERE, "cpp", "config_xml.cpp"), "-o", exe], check=True)
+    out = subprocess.run([exe] + [os.path.join(GOLDEN, f"config_{n}.xml") for n in ("materials", "pml", "boundaries")],
+                         check=True, capture_output=True, text=True).stdout.splitlines()
+    mats, pml, bc = _spec(os.path.join(GOLDEN, "config_spec.txt"))
+    got = {}
+    for line in out:
+        f = line.split()
+        if f[0] == "mat":
+            got[f[1]] = P.Material(int(f[2]), float(f[3]), float(f[4]),
+                                   [(1.0, float(f[6]), float(f[7]))] if int(f[5]) else [])
+    assert sorted(got) == sorted(r[0] for r in mats)
+    for row in mats:
+        assert got[row[0]] == _expected(row), row[0]
+    pml_line = [l for l in out if l.startswith("pml ")][0].split()
+    assert int(pml_line[1]) == pml[0] and [int(x) for x in pml_line[2:]] == pml[1]
+    bc_line = [l for l in out if l.startswith("bc ")][0].split()
+    assert bc_line[1:] == [C.BOUNDARIES[k] for k in bc]
+    assert [l for l in out if l.startswith("errors ")] == ["errors 31"]
