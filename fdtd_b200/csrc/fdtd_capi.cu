@@ -170,7 +170,7 @@ struct fdtd_grid {
   long long dft_pts[2]{};
   long long dft_maxpts[2]{};
   void* d_dft_buf[2]{};   // [kDftChunk][points] samples per phase
-  int dft_pending = 0;    // samples in the buffers (host mirror of t - dft_base)
+  int dft_pending = 0;    // samples in the buffers: the slot of the next one
   void** d_fieldptrs = nullptr;  // [E0,E1,E2,H0,H1,H2]
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
@@ -507,7 +507,24 @@ DftRegionDev quantity_region(const fdtd_grid* g, int q, const int* lo, const int
   return o;
 }
 
+// fold the buffered DFT samples of both phases into the accumulators
+int flush_dft(fdtd_grid* g, cudaStream_t s) {
+  int n = 0;
+  for (int ph = 0; ph < 2; ph++)
+    n += launch_dft_flush(ph, g->f32 ? 1 : 0, g->d_dft[ph], g->ndft[ph], g->dft_maxpts[ph], g->dft_pts[ph],
+                          g->d_dft_buf[ph], g->ctrl, g->dft_pending, s);
+  if (g->dft_pending > 0) n += launch_dft_rebase(g->ctrl, g->dft_pending, s);
+  g->dft_pending = 0;
+  return n;
+}
+
 int rebuild_dft(fdtd_grid* g) {
+  if (g->dft_pending > 0) {
+    // samples that fdtd_step_half left in the old layout's buffers
+    CK(cudaDeviceSynchronize());
+    g->launches += flush_dft(g, g->stream);
+    CK(cudaStreamSynchronize(g->stream));
+  }
   for (int ph = 0; ph < 2; ph++) {
     std::vector<DftRegionDev> v;
     long long off = 0;
@@ -534,19 +551,12 @@ int rebuild_dft(fdtd_grid* g) {
       if (rc) return rc;
     }
   }
+  if (!g->dfts.empty()) {
+    // the first sample of the new layout is that of the next step
+    g->launches += launch_dft_set_base(g->ctrl, g->t, g->stream);
+  }
   g->dirty_dft = false;
   return FDTD_OK;
-}
-
-// fold the buffered DFT samples of both phases into the accumulators
-int flush_dft(fdtd_grid* g, cudaStream_t s) {
-  int n = 0;
-  for (int ph = 0; ph < 2; ph++)
-    n += launch_dft_flush(ph, g->f32 ? 1 : 0, g->d_dft[ph], g->ndft[ph], g->dft_maxpts[ph], g->dft_pts[ph],
-                          g->d_dft_buf[ph], g->ctrl, s);
-  n += launch_dft_rebase(g->ctrl, s);
-  g->dft_pending = 0;
-  return n;
 }
 
 template <typename Args>
@@ -1081,6 +1091,7 @@ int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const dou
   const int qc = quantity_check(g, comp, lo, hi);
   if (qc != FDTD_OK) return qc;
   if (nf < 1) return fail(FDTD_ERR_INVALID, "nf must be >= 1");
+  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "DFT regions are added between whole steps");
   DftH r;
   r.comp = comp;
   r.nf = nf;
@@ -1192,7 +1203,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     if (boxes) g->launches += launch_boxes(g, 0, 0, s);
     g->launches += launch_bc(g, 0, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[0], g->ndft[0], g->dft_pts[0], g->dft_maxpts[0], fE, g->n[1],
-                                     static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[0], s);
+                                     static_cast<int>(rowlen(g)), g->dft_pending, g->d_dft_buf[0], s);
     if (prof) CK(cudaEventRecord(ev[2], s));
     if (boxes && g->f32) g->launches += launch_boxes(g, 1, -1, s);
     if (g->f32) {
@@ -1208,7 +1219,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
     if (boxes) g->launches += launch_boxes(g, 1, 0, s);
     g->launches += launch_bc(g, 1, s);
     g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[1], g->ndft[1], g->dft_pts[1], g->dft_maxpts[1], fH, g->n[1],
-                                     static_cast<int>(rowlen(g)), g->ctrl, g->d_dft_buf[1], s);
+                                     static_cast<int>(rowlen(g)), g->dft_pending, g->d_dft_buf[1], s);
     if (prof) CK(cudaEventRecord(ev[4], s));
     g->launches += launch_step_advance(g->ctrl, s);
     if (!g->dfts.empty() && ++g->dft_pending == kDftChunk) g->launches += flush_dft(g, s);
@@ -1276,6 +1287,8 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
     CK(cudaMemcpyAsync(g->ctrl, &c, sizeof(long long) * 2, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));  // the host value must outlive the copy
   }
+  // a captured graph takes its samples from slot 0 on
+  if (g->dft_pending > 0) g->launches += flush_dft(g, s);
   // one graph replay = kGraphSteps steps (and, with DFT regions, one flush)
   const bool graphs = !prof && g->use_graphs && nsteps >= kGraphSteps;
   int done = 0;
@@ -1378,8 +1391,8 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
   if (boxes) g->launches += launch_boxes(g, phase, 0, s);
   g->launches += launch_bc(g, phase, s);
   g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[phase], g->ndft[phase], g->dft_pts[phase],
-                                   g->dft_maxpts[phase], fields, g->n[1], static_cast<int>(rowlen(g)), g->ctrl,
-                                   g->d_dft_buf[phase], s);
+                                   g->dft_maxpts[phase], fields, g->n[1], static_cast<int>(rowlen(g)),
+                                   g->dft_pending, g->d_dft_buf[phase], s);
   if (phase == 1) {
     g->launches += launch_step_advance(g->ctrl, s);
     if (!g->dfts.empty() && ++g->dft_pending == kDftChunk) g->launches += flush_dft(g, s);
@@ -2049,6 +2062,8 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host value must outlive the copy
     if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, std::string("step control upload: ") + cudaGetErrorString(e));
   }
+  // a caller that captures this call replays its samples from slot 0 on
+  if (!rc && g->dft_pending > 0) g->launches += flush_dft(g, s);
   if (!rc) rc = enqueue_steps(g, nsteps, s, nullptr);
   for (int q = 0; q < naux; q++) {
     g->auxes[q].d_tab = saved_tab[q];

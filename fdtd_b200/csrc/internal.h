@@ -225,13 +225,14 @@ int launch_aux_precompute(int L, double dt, double dx, double* Dz, double* Ez, d
                           double* psiE, double* psiH, const double* coef, const double* vals, int nvals,
                           long long s0, int nsteps, double* Etab, double* Htab, cudaStream_t s);
 int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
-                      const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s);
+                      const void* const* fields, int ny, int pitch, int slot, void* buf, cudaStream_t s);
 // one quantity over a box into out (npts values of the field precision)
 int launch_quantity_read(int precision, const DftRegionDev& r, const void* const* fields, int ny, int pitch,
                          void* out, cudaStream_t s);
 int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
-                     long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s);
-int launch_dft_rebase(Control* ctrl, cudaStream_t s);
+                     long long total_pts, const void* buf, const Control* ctrl, int nsamp, cudaStream_t s);
+int launch_dft_rebase(Control* ctrl, int nsamp, cudaStream_t s);
+int launch_dft_set_base(Control* ctrl, long long base, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
 int launch_chunk_start(Control* ctrl, cudaStream_t s);

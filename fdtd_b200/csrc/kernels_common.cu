@@ -12,7 +12,8 @@
 namespace fdtdb {
 
 // The capture is chunked: every half step a gather copies the region values
-// into slot (t - dft_base) of a ring of kDftChunk samples per point; a flush
+// into slot `slot` (the samples taken since the last flush, counted on the
+// host) of a ring of kDftChunk samples per point; a flush
 // folds the pending samples into the FP64 accumulators in one pass, with the
 // twiddles of the chunk computed once per block in shared memory. This reads
 // and writes each 16-byte accumulator once per chunk instead of once per step.
@@ -70,11 +71,10 @@ __device__ __forceinline__ R quantity_at_point(const DftRegionDev& g, const R* c
 template <typename R>
 __global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, long long total,
                                                          const R* const* __restrict__ fields, int ny, int pitch,
-                                                         const Control* __restrict__ ctrl, R* buf) {
+                                                         long long slot, R* buf) {
   const DftRegionDev& g = regions[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.npts) return;
-  const long long slot = ctrl->t - ctrl->dft_base;
   buf[slot * total + g.pt_off + q] = quantity_at_point(g, fields, ny, pitch, q);
 }
 
@@ -102,12 +102,11 @@ int launch_quantity_read(int precision, const DftRegionDev& r, const void* const
 template <typename R>
 __global__ void __launch_bounds__(256) dft_flush_kernel(int phase, const DftRegionDev* __restrict__ regions,
                                                         long long total, const R* __restrict__ buf,
-                                                        const Control* __restrict__ ctrl) {
+                                                        const Control* __restrict__ ctrl, int nsamp) {
   __shared__ double2 tw[kDftChunk * 8];
   const DftRegionDev& g = regions[blockIdx.y];
   const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (static_cast<long long>(blockIdx.x) * blockDim.x >= g.npts) return;  // block-uniform
-  const int nsamp = static_cast<int>(ctrl->t - ctrl->dft_base);
   if (nsamp <= 0) return;
   const double nbase = static_cast<double>(ctrl->dft_base) + (phase == 0 ? 1.0 : 1.5);
   for (int f0 = 0; f0 < g.nf; f0 += 8) {
@@ -144,34 +143,42 @@ __global__ void __launch_bounds__(256) dft_flush_kernel(int phase, const DftRegi
   }
 }
 
-__global__ void dft_rebase_kernel(Control* ctrl) { ctrl->dft_base = ctrl->t; }
+// after a flush of nsamp samples the next sample is nsamp steps later
+__global__ void dft_rebase_kernel(Control* ctrl, int nsamp) { ctrl->dft_base += nsamp; }
+
+__global__ void dft_set_base_kernel(Control* ctrl, long long base) { ctrl->dft_base = base; }
 
 int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
-                      const void* const* fields, int ny, int pitch, const Control* ctrl, void* buf, cudaStream_t s) {
+                      const void* const* fields, int ny, int pitch, int slot, void* buf, cudaStream_t s) {
   if (nreg == 0 || total_pts == 0) return 0;
   const dim3 grid(static_cast<unsigned>((max_pts + 255) / 256), nreg);
   if (precision == 0)
     dft_gather_kernel<double><<<grid, 256, 0, s>>>(regions, total_pts, reinterpret_cast<const double* const*>(fields),
-                                                   ny, pitch, ctrl, static_cast<double*>(buf));
+                                                   ny, pitch, slot, static_cast<double*>(buf));
   else
     dft_gather_kernel<float><<<grid, 256, 0, s>>>(regions, total_pts, reinterpret_cast<const float* const*>(fields),
-                                                  ny, pitch, ctrl, static_cast<float*>(buf));
+                                                  ny, pitch, slot, static_cast<float*>(buf));
   return 1;
 }
 
 int launch_dft_flush(int phase, int precision, const DftRegionDev* regions, int nreg, long long max_pts,
-                     long long total_pts, const void* buf, const Control* ctrl, cudaStream_t s) {
-  if (nreg == 0 || total_pts == 0) return 0;
+                     long long total_pts, const void* buf, const Control* ctrl, int nsamp, cudaStream_t s) {
+  if (nreg == 0 || total_pts == 0 || nsamp <= 0) return 0;
   dim3 grid(static_cast<unsigned>((max_pts + 255) / 256), nreg);
   if (precision == 0)
-    dft_flush_kernel<double><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const double*>(buf), ctrl);
+    dft_flush_kernel<double><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const double*>(buf), ctrl, nsamp);
   else
-    dft_flush_kernel<float><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const float*>(buf), ctrl);
+    dft_flush_kernel<float><<<grid, 256, 0, s>>>(phase, regions, total_pts, static_cast<const float*>(buf), ctrl, nsamp);
   return 1;
 }
 
-int launch_dft_rebase(Control* ctrl, cudaStream_t s) {
-  dft_rebase_kernel<<<1, 1, 0, s>>>(ctrl);
+int launch_dft_rebase(Control* ctrl, int nsamp, cudaStream_t s) {
+  dft_rebase_kernel<<<1, 1, 0, s>>>(ctrl, nsamp);
+  return 1;
+}
+
+int launch_dft_set_base(Control* ctrl, long long base, cudaStream_t s) {
+  dft_set_base_kernel<<<1, 1, 0, s>>>(ctrl, base);
   return 1;
 }
 

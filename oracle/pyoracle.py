@@ -156,12 +156,19 @@ class OracleGrid:
                                              _dp(np.array(t.pol_e, float)), _dp(np.array(t.pol_h, float)),
                                              t.aux_ncells, _dp(av), len(av))
                 assert rc == 0
-        self.dft_handles = []
+        self.dft_handles, self.dft_nf = [], []
         for r in p.dfts:
-            fr = np.array(r.freqs, dtype=np.float64)
-            hnd = L.oracle_add_dft(self.h, r.comp, _ip(r.lo), _ip(r.hi), _dp(fr), len(fr))
-            assert hnd >= 0
-            self.dft_handles.append(hnd)
+            self.add_dft(r.comp, r.lo, r.hi, r.freqs)
+
+    def add_dft(self, comp: int, lo, hi, freqs) -> int:
+        """A running DFT region (also after steps were taken: its samples
+        start with the next step); returns its index for dft()."""
+        fr = np.array(freqs, dtype=np.float64)
+        hnd = lib().oracle_add_dft(self.h, comp, _ip(lo), _ip(hi), _dp(fr), len(fr))
+        assert hnd >= 0
+        self.dft_handles.append(hnd)
+        self.dft_nf.append(len(fr))
+        return len(self.dft_handles) - 1
 
     def set_time_scheme(self, scheme: int) -> None:
         assert lib().oracle_set_time_scheme(self.h, int(scheme)) == 0
@@ -228,7 +235,7 @@ class OracleGrid:
         """[nf][npoints] complex"""
         L = lib()
         n = L.oracle_dft_npoints(self.h, self.dft_handles[q])
-        nf = len(self.p.dfts[q].freqs)
+        nf = self.dft_nf[q]
         out = np.empty(nf * n * 2, dtype=np.float64)
         assert L.oracle_dft_get(self.h, self.dft_handles[q], _dp(out)) == 0
         out = out.reshape(nf, n, 2)

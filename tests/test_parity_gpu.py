@@ -296,3 +296,42 @@ def test_eps_map_matches_per_cell_materials(fdtd, oracle, make, prec):
     if prec == "f64":
         for n in E + H:
             assert np.array_equal(g.get(n), o.get(n)), n
+
+
+@pytest.mark.parametrize("make", [scenarios.tm_cpml_sources, scenarios.td_surface_dft, scenarios.td_tfsf_box],
+                         ids=lambda f: f.__name__)
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_dft_regions_added_mid_run(fdtd, oracle, make, precision):
+    """DFT regions added after steps were taken sample from the next step on,
+    as the reference's running DFT does: the first half of the regions after
+    70 whole steps (one captured graph and a remainder), the rest after three
+    half-step pairs that left samples in the buffers of the old layout."""
+    p = make()
+    regions, p.dfts = p.dfts, []
+    first, rest = regions[: max(1, len(regions) // 2)], regions[max(1, len(regions) // 2):]
+    o = oracle.OracleGrid(p)
+    g = fdtd.Grid.from_problem(p, precision)
+    o.step(70)
+    g.step(70)
+    for r in first:
+        o.add_dft(r.comp, r.lo, r.hi, r.freqs)
+        g.add_dft(r.comp, r.lo, r.hi, r.freqs)
+    o.step(75)
+    g.step(75)
+    for _ in range(3):
+        for ph in (0, 1):
+            o.step_half(ph)
+            g.step_half(ph)
+    g.step_half(0)
+    with pytest.raises(fdtd.FdtdError):
+        g.add_dft(regions[0].comp, regions[0].lo, regions[0].hi, regions[0].freqs)
+    g.step_half(1)
+    o.step(1)
+    for r in rest:
+        o.add_dft(r.comp, r.lo, r.hi, r.freqs)
+        g.add_dft(r.comp, r.lo, r.hi, r.freqs)
+    o.step(40)
+    g.step(40)
+    tol = PLAIN_TOL if precision == "f64" else FUSED_TOL
+    for q in range(len(regions)):
+        assert rel_l2(g.dft(q), o.dft(q)) <= tol, (q, regions[q].comp)
