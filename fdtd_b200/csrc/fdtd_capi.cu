@@ -534,6 +534,8 @@ int rebuild_dft(fdtd_grid* g) {
       o.nf = r.nf;
       o.npts = r.npts;
       o.pt_off = off;
+      // spectra of H in SI units: the FP32 method stores eta*H
+      o.acc_scale = g->f32 && r.comp >= 3 && r.comp < 6 ? 1.0 / eta() : 1.0;
       o.freqs = r.d_freqs;
       o.acc = r.d_acc;
       off += r.npts;
@@ -1131,10 +1133,6 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
   CK(cudaStreamSynchronize(g->stream));
   CK(cudaMemcpy(out, r.d_acc, n * sizeof(double), cudaMemcpyDeviceToHost));
-  if (g->f32 && r.comp >= 3 && r.comp < 6) {
-    const double s = 1.0 / eta();  // stored H is eta*H
-    for (size_t q = 0; q < n; q++) out[q] *= s;
-  }
   return FDTD_OK;
 }
 

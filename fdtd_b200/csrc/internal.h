@@ -177,6 +177,7 @@ struct DftRegionDev {
   // mode the grid's EM mode; scale the factor of the derived quantities
   int kind, mode;
   double scale;
+  double acc_scale;  // factor of every sample as the flush folds it (1/eta for stored eta*H)
   int lo[3], ext[3];
   long long npts, pt_off;
   const double* freqs;

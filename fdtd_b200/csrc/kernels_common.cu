@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) dft_flush_kernel(int phase, const DftRegi
     if (q >= g.npts) continue;
     double re[8] = {0, 0, 0, 0, 0, 0, 0, 0}, im[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int m = 0; m < nsamp; m++) {
-      const double x = static_cast<double>(buf[static_cast<long long>(m) * total + g.pt_off + q]);
+      const double x = static_cast<double>(buf[static_cast<long long>(m) * total + g.pt_off + q]) * g.acc_scale;
 #pragma unroll
       for (int f = 0; f < 8; f++) {
         if (f < nfb) {

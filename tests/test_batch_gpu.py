@@ -111,3 +111,30 @@ def test_batch_rejects_unsupported_grids(fdtd):
     g.add_dft(5, (2, 2, 0), (5, 5, 0), [0.1])
     with pytest.raises(fdtd.FdtdError):
         fdtd.Batch([g])
+
+
+def _single_vs_batch_problems():
+    import scenarios
+    tm, _ = scenarios.tm_adjoint_small(n=56, steps=90)
+    tm.sources = [P.Source(2, (9, 20, 0), P.sinusoid(90, 0.05), "E"),
+                  P.Source(2, (30, 33, 0), 1e-2 * P.gaussian_pulse(90, 30, 8), "D")]
+    te = small_te_batch(90)[1]
+    return [tm, te]
+
+
+@pytest.mark.parametrize("which", [0, 1], ids=["tm_eps_map", "te_rects"])
+def test_batch_of_one_matches_the_single_grid(fdtd, which):
+    """A grid advanced in a batch equals the same grid advanced alone up to
+    float rounding (the batch's 128-bit group updates and the single-grid
+    sweeps may contract different products into FMAs); the adjoint's
+    persistent recompute is built on the same group updates."""
+    p = _single_vs_batch_problems()[which]
+    a = fdtd.Grid.from_problem(p, "f32")
+    a.step(p.steps)
+    g = fdtd.Grid.from_problem(p, "f32")
+    b = fdtd.Batch([g])
+    b.step(p.steps)
+    assert b.error_flags() == 0
+    E, H, _, _ = mode_fields(p.mode)
+    for n in E + H:
+        assert rel_l2(g.get(n), a.get(n)) <= 1e-6, n
