@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
@@ -174,6 +175,8 @@ struct fdtd_grid {
   void** d_fieldptrs = nullptr;  // [E0,E1,E2,H0,H1,H2]
   Control* ctrl = nullptr;
   int* d_flag = nullptr;
+  char* h_stage = nullptr;  // two pinned chunks of kStageChunk bytes for large reads
+  cudaEvent_t stage_ev[2]{};
   bool dirty_dft = true;
   bool dirty_pml = false;  // host CPML profiles changed: device profiles and slabs follow before use
   int next_half = 0;  // fdtd_step_half: the phase expected next
@@ -192,6 +195,29 @@ struct fdtd_grid {
 namespace {
 
 size_t elem(const fdtd_grid* g) { return g->f32 ? 4 : 8; }
+
+// Copies `bytes` from pinned `src` into a host buffer with several threads.
+// A fresh pageable buffer's first touch costs a page fault per 4 KB, which one
+// thread takes one after another; the kernel serves faults of different
+// threads in parallel. Each thread takes at least 1 MB.
+void parallel_host_copy(char* dst, const char* src, size_t bytes) {
+  constexpr size_t kPerThread = size_t(1) << 20;
+  const size_t most = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const size_t nt = std::max<size_t>(1, std::min(most, bytes / kPerThread));
+  if (nt == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t per = (bytes + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (size_t q = 0; q < nt; q++) {
+    const size_t lo = q * per, hi = std::min(bytes, lo + per);
+    if (lo >= hi) break;
+    th.emplace_back([=] { std::memcpy(dst + lo, src + lo, hi - lo); });
+  }
+  for (auto& t : th) t.join();
+}
+
 long long rowlen(const fdtd_grid* g) { return g->f32 ? g->pitch : g->n[0]; }
 long long field_elems(const fdtd_grid* g) { return rowlen(g) * g->n[1] * g->n[2]; }
 
@@ -782,6 +808,9 @@ int fdtd_grid_destroy(fdtd_grid* g) {
   cudaSetDevice(g->d.device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   for (void* p : g->allocs) cudaFree(p);
+  if (g->h_stage) cudaFreeHost(g->h_stage);
+  for (auto& e : g->stage_ev)
+    if (e) cudaEventDestroy(e);
   if (g->stream) cudaStreamDestroy(g->stream);
   tma_release(g->tma);
   if (g->graph) cudaGraphExecDestroy(g->graph);
@@ -1124,6 +1153,46 @@ int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints) {
   return FDTD_OK;
 }
 
+}  // extern "C"
+
+// Reads `bytes` of device memory into a pageable host buffer. Large reads go
+// through the grid's two pinned chunks: the copy engine fills one at full
+// link speed while host threads move the other into `out`, instead of the
+// driver's own staging with a single-threaded copy and page faults.
+static int read_to_host(fdtd_grid* g, void* out, const void* src, size_t bytes) {
+  constexpr size_t kStageChunk = size_t(8) << 20;
+  if (bytes < kStageChunk) {
+    CK(cudaStreamSynchronize(g->stream));
+    CK(cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost));
+    return FDTD_OK;
+  }
+  if (!g->h_stage) {
+    CK(cudaHostAlloc(reinterpret_cast<void**>(&g->h_stage), 2 * kStageChunk, cudaHostAllocDefault));
+    for (auto& e : g->stage_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const char* d = static_cast<const char*>(src);
+  char* h = static_cast<char*>(out);
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  auto issue = [&](size_t c) -> cudaError_t {
+    const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    cudaError_t e = cudaMemcpyAsync(g->h_stage + (c % 2) * kStageChunk, d + off, len, cudaMemcpyDeviceToHost,
+                                    g->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(g->stage_ev[c % 2], g->stream);
+    return e;
+  };
+  CK(issue(0));
+  for (size_t c = 0; c < nch; c++) {
+    // the other chunk's previous contents were copied out in the last pass
+    if (c + 1 < nch) CK(issue(c + 1));
+    CK(cudaEventSynchronize(g->stage_ev[c % 2]));
+    const size_t off = c * kStageChunk;
+    parallel_host_copy(h + off, g->h_stage + (c % 2) * kStageChunk, std::min(kStageChunk, bytes - off));
+  }
+  return FDTD_OK;
+}
+
+extern "C" {
+
 int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   if (!g || !out || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
     return fail(FDTD_ERR_INVALID, "bad DFT handle");
@@ -1132,8 +1201,7 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   const DftH& r = g->dfts[handle];
   const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
   CK(cudaStreamSynchronize(g->stream));
-  CK(cudaMemcpy(out, r.d_acc, n * sizeof(double), cudaMemcpyDeviceToHost));
-  return FDTD_OK;
+  return read_to_host(g, out, r.d_acc, n * sizeof(double));
 }
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof);

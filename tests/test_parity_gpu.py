@@ -335,3 +335,32 @@ def test_dft_regions_added_mid_run(fdtd, oracle, make, precision):
     tol = PLAIN_TOL if precision == "f64" else FUSED_TOL
     for q in range(len(regions)):
         assert rel_l2(g.dft(q), o.dft(q)) <= tol, (q, regions[q].comp)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_large_spectrum_read_equals_its_parts(fdtd, precision):
+    """A spectrum of more than 8 MB is read through pinned staging chunks and
+    several host threads; it must equal, bit for bit, the same points taken
+    as four smaller regions (read with one plain copy each)."""
+    from fdtd_b200 import problem as P
+    n = 38
+    p = P.Problem(P.THREED, (n, n, n), 1e-6, P.courant_dt(1e-6, 0.99 / np.sqrt(3.0)), name="large_spectrum")
+    for a in range(3):
+        for s in (0, 1):
+            p.pml[(a, s)] = 4
+    p.sources.append(P.Source(1, (n // 2, n // 2, n // 2), P.gaussian_pulse(30, 12, 4), "E"))
+    p.steps = 30
+    nx, ny, nz = p.shape
+    lo, hi = (1, 1, 1), (nx - 2, ny - 2, nz - 2)
+    freqs = [0.01 * (q + 1) for q in range(32)]
+    g = fdtd.Grid.from_problem(p, precision)
+    whole = g.add_dft(1, lo, hi, freqs)
+    cuts = np.linspace(lo[2], hi[2] + 1, 5).astype(int)
+    parts = [g.add_dft(1, (lo[0], lo[1], int(a)), (hi[0], hi[1], int(b) - 1), freqs) for a, b in zip(cuts, cuts[1:])]
+    g.step(p.steps)
+    w = g.dft(whole)
+    assert w.nbytes > 8 << 20
+    ex, ey = hi[0] - lo[0] + 1, hi[1] - lo[1] + 1
+    got = np.concatenate([g.dft(h).reshape(len(freqs), -1, ey, ex) for h in parts], axis=1)
+    assert np.any(w != 0)
+    assert np.array_equal(got.reshape(w.shape), w)
