@@ -197,7 +197,10 @@ int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const dou
  * Synchronises the grid's stream. */
 int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double* host);
 int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints);
-/* host out: [nf][npoints][2] doubles (re, im), points x fastest */
+/* host out: [nf][npoints][2] doubles (re, im), points x fastest. Blocks
+ * until the spectrum is in `out`. Spectra of 8 MB and more pass through two
+ * pinned 8 MB chunks that the grid allocates at its first such read and
+ * keeps until fdtd_grid_destroy; several host threads copy them into `out`. */
 int fdtd_dft_read(fdtd_grid* g, int handle, double* out);
 
 /* Advance nsteps full time steps on `stream` (a cudaStream_t, or NULL for the
