@@ -213,7 +213,13 @@ void parallel_host_copy(char* dst, const char* src, size_t bytes) {
   for (size_t q = 0; q < nt; q++) {
     const size_t lo = q * per, hi = std::min(bytes, lo + per);
     if (lo >= hi) break;
-    th.emplace_back([=] { std::memcpy(dst + lo, src + lo, hi - lo); });
+    try {
+      th.emplace_back([=] { std::memcpy(dst + lo, src + lo, hi - lo); });
+    } catch (...) {
+      // no thread to be had (resource limits): this thread copies the slice;
+      // nothing may throw across the C ABI
+      std::memcpy(dst + lo, src + lo, hi - lo);
+    }
   }
   for (auto& t : th) t.join();
 }
