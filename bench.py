@@ -22,7 +22,9 @@ scaling "weak".
 
 --impl reference times the reference's own functors (oracle/_ref/ref_runner,
 compiled from the reference headers) on the host cores, on a reduced grid of
-the same physics, and prints its line; ranks other than 0 exit at once.
+the same physics, and prints its line; ranks other than 0 exit at once. The
+reference steps a grid on one thread, so the arm runs one copy of the sample
+per host core at once and reports their combined rate ("cores").
 """
 from __future__ import annotations
 
@@ -261,7 +263,22 @@ def cpu_rate(problem, steps: int, kind: str):
     return problem.interior_cells * steps / dt, dt
 
 
-def cpu_baseline(workload: str, budget_s: float = 15.0, variant: str = "none"):
+def host_cores() -> int:
+    """The CPUs this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(workload: str, budget_s: float = 15.0, variant: str = "none", replicas: int = 1):
+    """The reference's functors (or the C restatement) on a bounded sample of
+    the workload. The reference steps one grid on one thread (it has no
+    threading of its own), so with replicas > 1 that many copies of the
+    sample run at once, one process each, and the rate is their combined
+    cell-updates over the slowest copy's time loop."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     kind = "reference" if pyoracle.reference_available() else "port"
@@ -272,9 +289,18 @@ def cpu_baseline(workload: str, budget_s: float = 15.0, variant: str = "none"):
     rate0, _ = cpu_rate(small_problem(workload, 4, variant)[0], 4, kind)
     steps = max(4, int(budget_s * rate0 / p.interior_cells))
     p, desc = small_problem(workload, steps, variant)
-    rate, dt = cpu_rate(p, steps, kind)
-    return {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": 1, "kind": kind,
-            "sample": f"{desc}, {steps} steps, {dt:.1f} s, single thread"}
+    if replicas <= 1:
+        rate, dt = cpu_rate(p, steps, kind)
+        return {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": 1, "kind": kind,
+                "sample": f"{desc}, {steps} steps, {dt:.1f} s, single thread"}
+    with cf.ProcessPoolExecutor(max_workers=replicas, mp_context=mp.get_context("spawn")) as ex:
+        loops = list(ex.map(_cpu_one, [(p, steps, kind)] * replicas))
+    slow = max(loops)
+    return {"value": p.interior_cells * steps * replicas / slow / 1e9, "unit": "Gcell-updates/s", "cores": replicas,
+            "kind": kind,
+            "sample": f"{desc}, {steps} steps, {replicas} copies at once (one process and thread each: the "
+                      f"reference steps a grid on one thread), slowest time loop {slow:.1f} s; rate = copies x "
+                      f"cells x steps / slowest time loop"}
 
 
 def run_reference_arm(args):
@@ -288,7 +314,7 @@ def run_reference_arm(args):
         cb = cpu_adjoint_baseline(budget_s=20.0)
     else:
         cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)),
-                          variant=args.variant)
+                          variant=args.variant, replicas=min(256, host_cores()))
     metric = ADJ_METRIC if args.workload == "adjoint512" else METRIC
     line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": "Gcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
@@ -407,7 +433,7 @@ def cpu_batch_baseline(problems, budget_s: float = 20.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     kind = "reference" if pyoracle.reference_available() else "port"
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     cells = sum(p.interior_cells for p in problems)
     ctx = mp.get_context("spawn")
 

@@ -39,3 +39,13 @@ def test_plain_bytes_count_the_flux_history():
     assert a4["h_sweep"] - a1["h_sweep"] == pytest.approx(cells * 8 * 3 * 6)
     # FP32 bytes ignore the scheme (the fused method is leapfrog only)
     assert bench.alg_bytes(p1, 4) == bench.alg_bytes(bench.make_problem("drude384", 10, 32), 4)
+
+
+def test_reference_arm_copies_run_at_once():
+    """The reference arm's sample runs as concurrent single-thread copies:
+    the reported cores are the copies, the rate their combined cell-updates."""
+    one = bench.cpu_baseline("drude384", budget_s=0.3)
+    two = bench.cpu_baseline("drude384", budget_s=0.3, replicas=2)
+    assert one["cores"] == 1 and two["cores"] == 2
+    assert two["kind"] == one["kind"] and two["value"] > 0
+    assert "2 copies at once" in two["sample"]
