@@ -311,10 +311,10 @@ def run_reference_arm(args):
         from fdtd_b200 import problem as P
         cb = cpu_batch_baseline(P.config3(64, steps=args.steps + 16), budget_s=20.0)
     elif args.workload == "adjoint512":
-        cb = cpu_adjoint_baseline(budget_s=20.0, replicas=min(256, host_cores()))
+        cb = cpu_adjoint_baseline(budget_s=20.0, replicas=min(128, host_cores()))
     else:
         cb = cpu_baseline(args.workload, budget_s=max(5.0, min(30.0, 3.0 * max(1, args.steps) / 100)),
-                          variant=args.variant, replicas=min(256, host_cores()))
+                          variant=args.variant, replicas=min(128, host_cores()))
     metric = ADJ_METRIC if args.workload == "adjoint512" else METRIC
     line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": "Gcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
