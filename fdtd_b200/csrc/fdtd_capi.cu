@@ -10,8 +10,10 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -35,6 +37,26 @@ static int fail(int code, const std::string& msg) {
   } while (0)
 
 extern "C" const char* fdtd_last_error_string(void) { return g_err.c_str(); }
+
+// No C++ exception may leave the C ABI: each entry point is a function-try-
+// block whose handler turns a host allocation failure (std::bad_alloc from a
+// container, say) or any other exception into an error code.
+static int host_failure() {
+  try {
+    throw;
+  } catch (const std::bad_alloc&) {
+    g_err = "host memory allocation failed";
+    return FDTD_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    try {
+      g_err = std::string("host error: ") + e.what();
+    } catch (...) {
+    }
+    return FDTD_ERR_INVALID;
+  } catch (...) {
+    return FDTD_ERR_INVALID;
+  }
+}
 
 namespace {
 
@@ -734,7 +756,7 @@ FusedArgs fused_args(fdtd_grid* g) {
 
 extern "C" {
 
-int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out) {
+int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out) try {
   if (!desc || !out) return fail(FDTD_ERR_INVALID, "null argument");
   *out = nullptr;
   const fdtd_grid_desc& d = *desc;
@@ -807,9 +829,11 @@ int fdtd_grid_create(const fdtd_grid_desc* desc, fdtd_grid** out) {
   }
   *out = g;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_grid_destroy(fdtd_grid* g) {
+int fdtd_grid_destroy(fdtd_grid* g) try {
   if (!g) return FDTD_OK;
   cudaSetDevice(g->d.device);
   if (g->stream) cudaStreamSynchronize(g->stream);
@@ -822,9 +846,11 @@ int fdtd_grid_destroy(fdtd_grid* g) {
   if (g->graph) cudaGraphExecDestroy(g->graph);
   delete g;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) {
+int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (axis < 0 || axis >= dim_of(g) || side < 0 || side > 1) return fail(FDTD_ERR_INVALID, "bad axis or side");
   if (ncells < 1) return fail(FDTD_ERR_INVALID, "ncells must be >= 1");
@@ -841,9 +867,11 @@ int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) {
   g->dirty_pml = true;
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
+int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) try {
   if (!g || !mats) return fail(FDTD_ERR_INVALID, "null argument");
   if (n < 1 || n > 65536) return fail(FDTD_ERR_INVALID, "material count must be 1..65536");
   for (int q = 0; q < n; q++) {
@@ -858,9 +886,11 @@ int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) {
   CK(cudaSetDevice(g->d.device));
   g->mats.assign(mats, mats + n);
   return build_materials(g);
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) {
+int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) try {
   if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
   const long long n = static_cast<long long>(g->n[0]) * g->n[1] * g->n[2];
   // range check in one pass, then the rows copied into the padded layout
@@ -876,9 +906,11 @@ int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) {
     g->d_bids = nullptr;
   }
   return upload_vec(g, reinterpret_cast<void**>(&g->d_ids), v.data(), v.size());
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz) {
+int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids, int nbx, int nby, int nbz) try {
   if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
   if (block_shift < 0 || block_shift > 16) return fail(FDTD_ERR_INVALID, "bad block_shift");
   for (int a = 0; a < 3; a++) {
@@ -898,9 +930,11 @@ int fdtd_set_material_blocks(fdtd_grid* g, int block_shift, const uint16_t* ids,
   g->nby = nby;
   g->nbz = nbz;
   return upload_vec(g, reinterpret_cast<void**>(&g->d_bids), ids, nb * sizeof(uint16_t));
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_eps_map(fdtd_grid* g, const double* eps) {
+int fdtd_set_eps_map(fdtd_grid* g, const double* eps) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   CK(cudaSetDevice(g->d.device));
   if (!eps) {
@@ -920,9 +954,11 @@ int fdtd_set_eps_map(fdtd_grid* g, const double* eps) {
         else reinterpret_cast<double*>(buf.data())[q] = e > 0 ? e : 0.0;
       }
   return upload_vec(g, &g->d_eps_map, buf.data(), buf.size());
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) {
+int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, const double* vals, int nvals) try {
   if (!g || (!vals && nvals > 0)) return fail(FDTD_ERR_INVALID, "null argument");
   if (target < 0 || target > 3) return fail(FDTD_ERR_INVALID, "target must be 0 (E), 1 (D), 2 (H) or 3 (B)");
   if (comp < 0 || comp > 2 || !(target < 2 ? hasE(g->d.mode, comp) : hasH(g->d.mode, comp)))
@@ -944,10 +980,12 @@ int fdtd_add_source(fdtd_grid* g, int comp, int target, int i, int j, int k, con
   g->srcs.push_back(s);
   if (g->d_src_last) dfree(g, g->d_src_last);
   return dalloc(g, reinterpret_cast<void**>(&g->d_src_last), kMaxSources * sizeof(double));
+} catch (...) {
+  return host_failure();
 }
 
 int fdtd_add_source_box(fdtd_grid* g, int comp, int target, const int* lo, const int* hi, const double* vals,
-                        int nvals) {
+                        int nvals) try {
   if (!g || !lo || !hi || (!vals && nvals > 0)) return fail(FDTD_ERR_INVALID, "null argument");
   if (target == 1 || target == 3)
     return fail(FDTD_ERR_UNSUPPORTED, "box sources add to E (target 0) or H (target 2); use point sources for D or B");
@@ -974,6 +1012,8 @@ int fdtd_add_source_box(fdtd_grid* g, int comp, int target, const int* lo, const
   g->boxes.push_back(b);
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // the box sources of one phase (0 = E, 1 = H): shift 0 adds this step's
@@ -999,7 +1039,7 @@ static int launch_bc(fdtd_grid* g, int phase, cudaStream_t s) {
                            s);
 }
 
-int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) {
+int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (axis < 0 || axis >= dim_of(g) || side < 0 || side > 1) return fail(FDTD_ERR_INVALID, "bad axis or side");
   if (kind < FDTD_BC_NONE || kind > FDTD_BC_PERIODIC) return fail(FDTD_ERR_INVALID, "bad boundary kind");
@@ -1015,9 +1055,11 @@ int fdtd_set_boundary(fdtd_grid* g, int axis, int side, int kind) {
   g->bcs = nb;
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_set_time_scheme(fdtd_grid* g, int scheme) {
+int fdtd_set_time_scheme(fdtd_grid* g, int scheme) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (scheme != FDTD_BD1 && scheme != FDTD_BD3 && scheme != FDTD_BD4)
     return fail(FDTD_ERR_INVALID, "time scheme must be FDTD_BD1, FDTD_BD3 or FDTD_BD4");
@@ -1043,11 +1085,13 @@ int fdtd_set_time_scheme(fdtd_grid* g, int scheme) {
   g->scheme = scheme;
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const int* hi, const double* origin,
                         const double* k, const double* pol_e, const double* pol_h, int aux_ncells,
-                        const double* aux_vals, int naux) {
+                        const double* aux_vals, int naux) try {
   if (!g || !lo || !hi || !origin || !k || !pol_e || !pol_h || (!aux_vals && naux > 0))
     return fail(FDTD_ERR_INVALID, "null argument");
   const int dim = dim_of(g);
@@ -1121,9 +1165,11 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
   g->planes.push_back(ph);
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) {
+int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const double* freqs, int nf, int* handle) try {
   if (!g || !lo || !hi || !freqs || !handle) return fail(FDTD_ERR_INVALID, "null argument");
   const int qc = quantity_check(g, comp, lo, hi);
   if (qc != FDTD_OK) return qc;
@@ -1150,13 +1196,17 @@ int fdtd_add_dft(fdtd_grid* g, int comp, const int* lo, const int* hi, const dou
   *handle = static_cast<int>(g->dfts.size()) - 1;
   g->dirty_dft = true;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints) {
+int fdtd_dft_npoints(fdtd_grid* g, int handle, long long* npoints) try {
   if (!g || !npoints || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
     return fail(FDTD_ERR_INVALID, "bad DFT handle");
   *npoints = g->dfts[handle].npts;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 }  // extern "C"
@@ -1199,7 +1249,7 @@ static int read_to_host(fdtd_grid* g, void* out, const void* src, size_t bytes) 
 
 extern "C" {
 
-int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
+int fdtd_dft_read(fdtd_grid* g, int handle, double* out) try {
   if (!g || !out || handle < 0 || handle >= static_cast<int>(g->dfts.size()))
     return fail(FDTD_ERR_INVALID, "bad DFT handle");
   CK(cudaSetDevice(g->d.device));
@@ -1208,14 +1258,20 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) {
   const size_t n = static_cast<size_t>(r.nf) * r.npts * 2;
   CK(cudaStreamSynchronize(g->stream));
   return read_to_host(g, out, r.d_acc, n * sizeof(double));
+} catch (...) {
+  return host_failure();
 }
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof);
 static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof);
 
-int fdtd_step(fdtd_grid* g, int nsteps, void* stream) { return step_impl(g, nsteps, stream, nullptr); }
+int fdtd_step(fdtd_grid* g, int nsteps, void* stream) try {
+  return step_impl(g, nsteps, stream, nullptr);
+} catch (...) {
+  return host_failure();
+}
 
-int fdtd_prepare(fdtd_grid* g) {
+int fdtd_prepare(fdtd_grid* g) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   CK(cudaSetDevice(g->d.device));
   int rc = ensure_pml(g);
@@ -1226,11 +1282,15 @@ int fdtd_prepare(fdtd_grid* g) {
   }
   CK(cudaStreamSynchronize(g->stream));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms) {
+int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms) try {
   if (!ms) return fail(FDTD_ERR_INVALID, "null argument");
   return step_impl(g, nsteps, stream, ms);
+} catch (...) {
+  return host_failure();
 }
 
 // Enqueues nsteps steps on s (kernels only, so it can run under stream
@@ -1398,19 +1458,21 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   return FDTD_OK;
 }
 
-int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) {
+int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_STAGED) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
   g->sweep_kind = kind;
   g->version++;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // One half step, for callers that exchange data between the halves (the
 // ghost planes of a z-slab decomposition): the launches of one step of
 // enqueue_steps, split after the E-phase DFT gather; phase 0 also advances
 // the TFSF aux grids by one step. Launched eagerly, never from a graph.
-int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
+int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (phase != 0 && phase != 1) return fail(FDTD_ERR_INVALID, "phase must be 0 (E) or 1 (H)");
   if (phase != g->next_half) return fail(FDTD_ERR_INVALID, "half steps alternate, the E half first");
@@ -1473,12 +1535,14 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) {
   CK(cudaGetLastError());
   g->next_half = 1 - phase;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // one z plane of a stored E or H component to or from a compact device
 // buffer (nx * ny values of the grid's precision, x fastest; H of the FP32
 // method is the stored eta * H)
-int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream) {
+int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream) try {
   if (!g || !dev_buf) return fail(FDTD_ERR_INVALID, "null argument");
   if (k < 0 || k >= g->n[2]) return fail(FDTD_ERR_INVALID, "plane index out of range");
   void* f = nullptr;
@@ -1492,15 +1556,19 @@ int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, 
   if (to_grid) CK(cudaMemcpy2DAsync(plane, row, dev_buf, w, w, g->n[1], cudaMemcpyDeviceToDevice, s));
   else CK(cudaMemcpy2DAsync(dev_buf, w, plane, row, w, g->n[1], cudaMemcpyDeviceToDevice, s));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_use_graphs(fdtd_grid* g, int enable) {
+int fdtd_use_graphs(fdtd_grid* g, int enable) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   g->use_graphs = enable != 0;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_error_flags(fdtd_grid* g, int* flags) {
+int fdtd_error_flags(fdtd_grid* g, int* flags) try {
   if (!g || !flags) return fail(FDTD_ERR_INVALID, "null argument");
   CK(cudaSetDevice(g->d.device));
   Control c;
@@ -1508,14 +1576,18 @@ int fdtd_error_flags(fdtd_grid* g, int* flags) {
   CK(cudaMemcpy(&c, g->ctrl, sizeof(c), cudaMemcpyDeviceToHost));
   *flags = c.error;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_synchronize(fdtd_grid* g) {
+int fdtd_synchronize(fdtd_grid* g) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   CK(cudaSetDevice(g->d.device));
   CK(cudaStreamSynchronize(g->stream));
   CK(cudaDeviceSynchronize());
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // which -> (device pointer, scale to SI, element layout)
@@ -1559,7 +1631,7 @@ static int locate(fdtd_grid* g, int which, void** p, double* scale, int* psi_axi
   return FDTD_OK;
 }
 
-int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double* host) {
+int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double* host) try {
   if (!g || !lo || !hi || !host) return fail(FDTD_ERR_INVALID, "null argument");
   const int qc = quantity_check(g, q, lo, hi);
   if (qc != FDTD_OK) return qc;
@@ -1588,9 +1660,11 @@ int fdtd_read_quantity(fdtd_grid* g, int q, const int* lo, const int* hi, double
     host[p] = g->f32 ? static_cast<double>(reinterpret_cast<float*>(h.data())[p]) * hs
                      : reinterpret_cast<double*>(h.data())[p];
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_download(fdtd_grid* g, int which, double* host) {
+int fdtd_download(fdtd_grid* g, int which, double* host) try {
   if (!g || !host) return fail(FDTD_ERR_INVALID, "null argument");
   void* p;
   double scale;
@@ -1640,9 +1714,11 @@ int fdtd_download(fdtd_grid* g, int which, double* host) {
         }
       }
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_upload(fdtd_grid* g, int which, const double* host) {
+int fdtd_upload(fdtd_grid* g, int which, const double* host) try {
   if (!g || !host) return fail(FDTD_ERR_INVALID, "null argument");
   void* p;
   double scale;
@@ -1665,9 +1741,11 @@ int fdtd_upload(fdtd_grid* g, int which, const double* host) {
       }
   CK(cudaMemcpy(p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_check_finite(fdtd_grid* g) {
+int fdtd_check_finite(fdtd_grid* g) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   CK(cudaSetDevice(g->d.device));
   CK(cudaMemsetAsync(g->d_flag, 0, sizeof(int), g->stream));
@@ -1685,24 +1763,32 @@ int fdtd_check_finite(fdtd_grid* g) {
   CK(cudaStreamSynchronize(g->stream));
   if (flag) return fail(FDTD_ERR_NONFINITE, "a field holds NaN or Inf");
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_get_step(fdtd_grid* g, long long* step) {
+int fdtd_get_step(fdtd_grid* g, long long* step) try {
   if (!g || !step) return fail(FDTD_ERR_INVALID, "null argument");
   *step = g->t;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_launch_count(fdtd_grid* g, long long* count) {
+int fdtd_launch_count(fdtd_grid* g, long long* count) try {
   if (!g || !count) return fail(FDTD_ERR_INVALID, "null argument");
   *count = g->launches;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_memory_bytes(fdtd_grid* g, long long* bytes) {
+int fdtd_memory_bytes(fdtd_grid* g, long long* bytes) try {
   if (!g || !bytes) return fail(FDTD_ERR_INVALID, "null argument");
   *bytes = g->bytes;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 }  // extern "C"
@@ -1807,7 +1893,7 @@ int batch_launch(fdtd_batch* b, int nsteps, cudaStream_t s) {
 
 extern "C" {
 
-int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
+int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) try {
   if (!grids || !out || n < 1) return fail(FDTD_ERR_INVALID, "need at least one grid");
   if (n > 255) return fail(FDTD_ERR_UNSUPPORTED, "at most 255 grids per batch");
   *out = nullptr;
@@ -1866,9 +1952,11 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) {
   }
   *out = b;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_batch_destroy(fdtd_batch* b) {
+int fdtd_batch_destroy(fdtd_batch* b) try {
   if (!b) return FDTD_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
@@ -1880,11 +1968,13 @@ int fdtd_batch_destroy(fdtd_batch* b) {
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // Times every tile height on a copy of the state (restored afterwards) and
 // keeps the fastest.
-int fdtd_batch_tune(fdtd_batch* b, int steps) {
+int fdtd_batch_tune(fdtd_batch* b, int steps) try {
   if (!b || steps < 1) return fail(FDTD_ERR_INVALID, "bad argument");
   CK(cudaSetDevice(b->device));
   CK(cudaDeviceSynchronize());
@@ -1945,9 +2035,11 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) {
   b->graphs.clear();
   b->persistent = best_persistent;
   return batch_items(b, best_rows);
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) {
+int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) try {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch");
   if (rows != 1 && rows != 2 && rows != 4 && rows != 8) return fail(FDTD_ERR_INVALID, "rows must be 1, 2, 4 or 8");
   CK(cudaSetDevice(b->device));
@@ -1956,9 +2048,11 @@ int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) {
   b->graphs.clear();
   b->persistent = persistent ? 1 : 0;
   return batch_items(b, rows);
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
+int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) try {
   if (!b || nsteps < 0) return fail(FDTD_ERR_INVALID, "bad argument");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(b->device));
@@ -2001,9 +2095,11 @@ int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) {
   for (auto* g : b->grids) CK(cudaStreamWaitEvent(g->stream, ev, 0));
   CK(cudaEventDestroy(ev));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, int* persistent, float* tune_ms) {
+int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, int* persistent, float* tune_ms) try {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch");
   if (rows) *rows = b->rows;
   if (blocks) *blocks = b->persistent ? b->blocks : b->nitems;
@@ -2012,15 +2108,19 @@ int fdtd_batch_info(fdtd_batch* b, int* rows, int* blocks, int* items, int* pers
   if (tune_ms)
     for (int q = 0; q < 8; q++) tune_ms[q] = q < static_cast<int>(b->tune_ms.size()) ? b->tune_ms[q] : 0.f;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_batch_error_flags(fdtd_batch* b, int* flags) {
+int fdtd_batch_error_flags(fdtd_batch* b, int* flags) try {
   if (!b || !flags) return fail(FDTD_ERR_INVALID, "null argument");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpy(flags, &b->d_ctl->error, sizeof(int), cudaMemcpyDeviceToHost));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 }  // extern "C"
@@ -2254,7 +2354,7 @@ static int adj_enqueue_segment(fdtd_adjoint* a, const FusedArgs& fa, const AdjAr
 extern "C" {
 
 int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, double freq, const int* design_lo,
-                        const int* design_hi, int ckpt_every, fdtd_adjoint** out) {
+                        const int* design_hi, int ckpt_every, fdtd_adjoint** out) try {
   if (!g || !probe_lo || !probe_hi || !design_lo || !design_hi || !out) return fail(FDTD_ERR_INVALID, "null argument");
   if (!g->f32 || g->d.mode != FDTD_TM)
     return fail(FDTD_ERR_UNSUPPORTED, "the adjoint takes 2D TM grids of the FP32 fused method");
@@ -2301,17 +2401,21 @@ int fdtd_adjoint_create(fdtd_grid* g, const int* probe_lo, const int* probe_hi, 
   a->dft = handle;
   *out = a;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_adjoint_destroy(fdtd_adjoint* a) {
+int fdtd_adjoint_destroy(fdtd_adjoint* a) try {
   if (!a) return FDTD_OK;
   cudaSetDevice(a->device);
   cudaDeviceSynchronize();
   delete a;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_adjoint_forward(fdtd_adjoint* a, int nsteps, double* J) {
+int fdtd_adjoint_forward(fdtd_adjoint* a, int nsteps, double* J) try {
   if (!a || !J) return fail(FDTD_ERR_INVALID, "null argument");
   if (a->forwarded) return fail(FDTD_ERR_INVALID, "one forward per adjoint handle");
   if (nsteps < 1) return fail(FDTD_ERR_INVALID, "nsteps < 1");
@@ -2351,9 +2455,11 @@ int fdtd_adjoint_forward(fdtd_adjoint* a, int nsteps, double* J) {
   a->forwarded = true;
   *J = sum;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
-int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad) {
+int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad) try {
   if (!a || !grad) return fail(FDTD_ERR_INVALID, "null argument");
   if (!a->forwarded) return fail(FDTD_ERR_INVALID, "run fdtd_adjoint_forward first");
   fdtd_grid* g = a->g;
@@ -2455,6 +2561,8 @@ int fdtd_adjoint_backward(fdtd_adjoint* a, double* grad) {
   CK(cudaMemcpyAsync(grad, a->d_grad, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 }  // extern "C"

@@ -59,7 +59,7 @@ enum {
   FDTD_ERR_INVALID = -1,     /* bad argument or state */
   FDTD_ERR_CUDA = -2,        /* a CUDA call failed */
   FDTD_ERR_UNSUPPORTED = -3, /* valid, but not supported by this method */
-  FDTD_ERR_NOMEM = -4,       /* device allocation failed */
+  FDTD_ERR_NOMEM = -4,       /* a device or host allocation failed */
   FDTD_ERR_NONFINITE = -5,   /* a field went non-finite (fdtd_check_finite) */
   FDTD_ERR_TIMEOUT = -6      /* a bounded device wait gave up */
 };
