@@ -68,14 +68,29 @@ __device__ __forceinline__ R quantity_at_point(const DftRegionDev& g, const R* c
   return quantity_sample(g, f, k * sz + static_cast<long long>(j) * pitch + i, pitch, sz);
 }
 
+// points per thread of the gather: all their loads are issued before any
+// store, so that more of the (often one-per-sector) field reads are in flight
+constexpr int kGatherPts = 4;
+
 template <typename R>
 __global__ void __launch_bounds__(256) dft_gather_kernel(const DftRegionDev* __restrict__ regions, long long total,
                                                          const R* const* __restrict__ fields, int ny, int pitch,
                                                          long long slot, R* buf) {
   const DftRegionDev& g = regions[blockIdx.y];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= g.npts) return;
-  buf[slot * total + g.pt_off + q] = quantity_at_point(g, fields, ny, pitch, q);
+  const int q0 = blockIdx.x * (256 * kGatherPts) + threadIdx.x;
+  if (q0 >= g.npts) return;
+  R v[kGatherPts];
+#pragma unroll
+  for (int u = 0; u < kGatherPts; u++) {
+    const int q = q0 + u * 256;
+    if (q < g.npts) v[u] = quantity_at_point(g, fields, ny, pitch, q);
+  }
+  R* out = buf + slot * total + g.pt_off;
+#pragma unroll
+  for (int u = 0; u < kGatherPts; u++) {
+    const int q = q0 + u * 256;
+    if (q < g.npts) out[q] = v[u];
+  }
 }
 
 template <typename R>
@@ -151,7 +166,7 @@ __global__ void dft_set_base_kernel(Control* ctrl, long long base) { ctrl->dft_b
 int launch_dft_gather(int precision, const DftRegionDev* regions, int nreg, long long total_pts, long long max_pts,
                       const void* const* fields, int ny, int pitch, int slot, void* buf, cudaStream_t s) {
   if (nreg == 0 || total_pts == 0) return 0;
-  const dim3 grid(static_cast<unsigned>((max_pts + 255) / 256), nreg);
+  const dim3 grid(static_cast<unsigned>((max_pts + 256 * kGatherPts - 1) / (256 * kGatherPts)), nreg);
   if (precision == 0)
     dft_gather_kernel<double><<<grid, 256, 0, s>>>(regions, total_pts, reinterpret_cast<const double* const*>(fields),
                                                    ny, pitch, slot, static_cast<double*>(buf));
