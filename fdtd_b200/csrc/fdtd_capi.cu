@@ -1767,6 +1767,46 @@ int fdtd_check_finite(fdtd_grid* g) try {
   return host_failure();
 }
 
+int fdtd_field_error(fdtd_grid* g, fdtd_grid* ref, int which, double* err_sq, double* ref_sq) try {
+  if (!g || !ref || !err_sq || !ref_sq) return fail(FDTD_ERR_INVALID, "null argument");
+  if (g->d.device != ref->d.device) return fail(FDTD_ERR_INVALID, "the two grids live on different devices");
+  for (int d = 0; d < 3; d++)
+    if (g->n[d] != ref->n[d]) return fail(FDTD_ERR_INVALID, "the two grids differ in shape");
+  if (which >= 18 && which < 36) return fail(FDTD_ERR_UNSUPPORTED, "CPML integrators are not compared");
+  void *pa, *pb;
+  double sa, sb;
+  int ja, jb;
+  int rc = locate(g, which, &pa, &sa, &ja);
+  if (rc) return rc;
+  rc = locate(ref, which, &pb, &sb, &jb);
+  if (rc) return rc;
+  if (!pa || !pb) return fail(FDTD_ERR_UNSUPPORTED, "field not stored by one of the grids");
+  CK(cudaSetDevice(g->d.device));
+  CK(cudaStreamSynchronize(ref->stream));
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, 2 * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? FDTD_ERR_NOMEM : FDTD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  double h[2] = {0.0, 0.0};
+  e = cudaMemsetAsync(out, 0, 2 * sizeof(double), g->stream);
+  if (e == cudaSuccess) {
+    g->launches += launch_field_diff(pa, g->f32 ? 1 : 0, rowlen(g), sa, pb, ref->f32 ? 1 : 0, rowlen(ref), sb,
+                                     g->n[0], static_cast<long long>(g->n[1]) * g->n[2], out, g->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(out);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
+  *err_sq = h[0];
+  *ref_sq = h[1];
+  return FDTD_OK;
+} catch (...) {
+  return host_failure();
+}
+
 int fdtd_get_step(fdtd_grid* g, long long* step) try {
   if (!g || !step) return fail(FDTD_ERR_INVALID, "null argument");
   *step = g->t;
@@ -2174,8 +2214,9 @@ int static_aux_address(int device, double** out) {
 
 }  // namespace
 
-extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) {
+extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(g->d.device));
@@ -2207,6 +2248,16 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
     if (rc) return rc;
   }
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  if (!g->auxes.empty()) {
+    // the TFSF step counter goes up from a host value, and the call waits
+    // for that copy: neither is possible while the stream is being captured
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(FDTD_ERR_UNSUPPORTED,
+                  "fdtd_step_static_scratch: a grid with TFSF planes uploads its step counter and synchronises "
+                  "the stream, which a stream under capture cannot do");
+  }
   if (s != g->stream) CK(cudaStreamSynchronize(g->stream));  // set-up work on the grid's stream first
   // point each plane's table at its slice of the fixed array for this call
   double* saved_tab[kMaxPlanes];
@@ -2234,7 +2285,8 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host value must outlive the copy
     if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, std::string("step control upload: ") + cudaGetErrorString(e));
   }
-  // a caller that captures this call replays its samples from slot 0 on
+  // as in fdtd_step: pending DFT samples are folded first, so the call's
+  // samples fill the ring from slot 0 on
   if (!rc && g->dft_pending > 0) g->launches += flush_dft(g, s);
   if (!rc) rc = enqueue_steps(g, nsteps, s, nullptr);
   for (int q = 0; q < naux; q++) {
@@ -2245,6 +2297,8 @@ extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) 
   CK(cudaGetLastError());
   g->t += nsteps;
   return FDTD_OK;
+} catch (...) {
+  return host_failure();
 }
 
 // ----------------------------------------------------------------------------

@@ -236,6 +236,9 @@ int launch_dft_rebase(Control* ctrl, int nsamp, cudaStream_t s);
 int launch_dft_set_base(Control* ctrl, long long base, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
+// out[0] += sum over rows of (a*sa - b*sb)^2, out[1] += sum (b*sb)^2 (FP64)
+int launch_field_diff(const void* a, int a_f32, long long rla, double sa, const void* b, int b_f32, long long rlb,
+                      double sb, int nx, long long nrows, double* out, cudaStream_t s);
 int launch_chunk_start(Control* ctrl, cudaStream_t s);
 // faces with a boundary condition (kind 1 PEC, 2 PMC, 3 symmetric,
 // 4 antisymmetric, 5 periodic)

@@ -215,6 +215,64 @@ int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaS
   return 1;
 }
 
+// Squared difference of two stored fields of equal extent, each scaled to SI
+// units, and the squared reference: out[0] += sum (a sa - b sb)^2,
+// out[1] += sum (b sb)^2 over the nx cells of every row (j, k); the rows of a
+// and b are rla and rlb values long (FP32 rows are padded). FP64 sums.
+template <typename RA, typename RB>
+__global__ void __launch_bounds__(256) field_diff_kernel(const RA* __restrict__ a, long long rla, double sa,
+                                                         const RB* __restrict__ b, long long rlb, double sb, int nx,
+                                                         long long nrows, double* out) {
+  double d2 = 0.0, r2 = 0.0;
+  for (long long row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const RA* pa = a + row * rla;
+    const RB* pb = b + row * rlb;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      const double va = static_cast<double>(pa[i]) * sa, vb = static_cast<double>(pb[i]) * sb;
+      d2 += (va - vb) * (va - vb);
+      r2 += vb * vb;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 += __shfl_down_sync(0xffffffffu, d2, o);
+    r2 += __shfl_down_sync(0xffffffffu, r2, o);
+  }
+  __shared__ double part[2][8];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    part[0][w] = d2;
+    part[1][w] = r2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (blockDim.x >> 5); q++) {
+      d2 += part[0][q];
+      r2 += part[1][q];
+    }
+    atomicAdd(out, d2);
+    atomicAdd(out + 1, r2);
+  }
+}
+
+int launch_field_diff(const void* a, int a_f32, long long rla, double sa, const void* b, int b_f32, long long rlb,
+                      double sb, int nx, long long nrows, double* out, cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>(std::min<long long>(nrows, 148LL * 8));
+  if (blocks == 0) return 0;
+  if (a_f32 && b_f32)
+    field_diff_kernel<float, float><<<blocks, 256, 0, s>>>(static_cast<const float*>(a), rla, sa,
+                                                            static_cast<const float*>(b), rlb, sb, nx, nrows, out);
+  else if (a_f32)
+    field_diff_kernel<float, double><<<blocks, 256, 0, s>>>(static_cast<const float*>(a), rla, sa,
+                                                             static_cast<const double*>(b), rlb, sb, nx, nrows, out);
+  else if (b_f32)
+    field_diff_kernel<double, float><<<blocks, 256, 0, s>>>(static_cast<const double*>(a), rla, sa,
+                                                             static_cast<const float*>(b), rlb, sb, nx, nrows, out);
+  else
+    field_diff_kernel<double, double><<<blocks, 256, 0, s>>>(static_cast<const double*>(a), rla, sa,
+                                                              static_cast<const double*>(b), rlb, sb, nx, nrows, out);
+  return 1;
+}
+
 __global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
 
 __global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }

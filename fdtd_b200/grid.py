@@ -33,7 +33,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
-           "fdtd_check_finite", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
+           "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
            "fdtd_batch_info",
            "fdtd_batch_error_flags", "fdtd_adjoint_create", "fdtd_adjoint_forward", "fdtd_adjoint_backward",
@@ -100,6 +100,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_download": [vp, i, dp],
         "fdtd_upload": [vp, i, dp],
         "fdtd_check_finite": [vp],
+        "fdtd_field_error": [vp, vp, i, dp, dp],
         "fdtd_get_step": [vp, llp],
         "fdtd_launch_count": [vp, llp],
         "fdtd_memory_bytes": [vp, llp],
@@ -355,6 +356,15 @@ class Grid:
 
     def check_finite(self) -> None:
         _check(load_library().fdtd_check_finite(self.h))
+
+    def field_error(self, ref: "Grid", name: str) -> float:
+        """Relative L2 error of field `name` of this grid against the same
+        field of grid `ref` (same shape and device), computed on the device
+        in FP64 over every cell (fdtd_field_error)."""
+        which = ALL_NAMES.index(name)
+        e2, r2 = ctypes.c_double(), ctypes.c_double()
+        _check(load_library().fdtd_field_error(self.h, ref.h, which, ctypes.byref(e2), ctypes.byref(r2)))
+        return float(np.sqrt(e2.value / r2.value)) if r2.value > 0 else float(np.sqrt(e2.value))
 
     @property
     def step_count(self) -> int:

@@ -297,41 +297,46 @@ def config1(n: int = 256, steps: int = 2000, npml: int = 16) -> Problem:
 
 
 def config2(n: int = 384, steps: int = 1000, npml: int = 12, radius: Optional[int] = None,
-            tfsf_inset: Optional[int] = None, dft_inset: Optional[int] = None, nfreq: int = 8) -> Problem:
+            tfsf_inset: Optional[int] = None, dft_inset: Optional[int] = None, nfreq: int = 8,
+            shape: Optional[Tuple[int, int, int]] = None) -> Problem:
     """3D, 12-cell CPML, Drude sphere (eps_inf 1, wp*dt 0.3, gamma*dt 0.01) of
     radius 64 at the centre, TFSF box inset 24 with an x-propagating
     z-polarised Gaussian plane wave, DFT at 8 frequencies of the 4 tangential
     components on the 6 faces of the box inset 20. Smaller n scales radius
-    and insets by n/384."""
-    scale = n / 384.0
+    and insets by n/384. `shape` (nx, ny, nz) replaces the cube n^3; the
+    radius and insets then scale with its smallest extent."""
+    shape = tuple(shape) if shape is not None else (n, n, n)
+    nmin = min(shape)
+    scale = nmin / 384.0
     radius = radius if radius is not None else max(2, int(round(64 * scale)))
     tfsf_inset = tfsf_inset if tfsf_inset is not None else max(npml + 3, int(round(24 * scale)))
     dft_inset = dft_inset if dft_inset is not None else max(npml + 2, tfsf_inset - max(1, int(round(4 * scale))))
     dx = 1e-6
     dt = courant_dt(dx, 0.99 / math.sqrt(3.0))
-    p = Problem(THREED, (n, n, n), dx, dt, name=f"3d{n}_drude_sphere_tfsf_dft")
+    name = f"3d{n}_drude_sphere_tfsf_dft" if shape == (n, n, n) else \
+        f"3d{shape[0]}x{shape[1]}x{shape[2]}_drude_sphere_tfsf_dft"
+    p = Problem(THREED, shape, dx, dt, name=name)
     for a in range(3):
         for s in (0, 1):
             p.pml[(a, s)] = npml
     p.materials = [Material.vacuum(), Material.drude(1.0, 0.3 / dt, 0.01 / dt)]
-    c = n // 2
-    ax = np.arange(n) - c
-    r2 = ax[:, None, None] ** 2 + ax[None, :, None] ** 2 + ax[None, None, :] ** 2
+    cx, cy, cz = (v // 2 for v in shape)
+    r2 = ((np.arange(shape[2]) - cz)[:, None, None] ** 2 + (np.arange(shape[1]) - cy)[None, :, None] ** 2
+          + (np.arange(shape[0]) - cx)[None, None, :] ** 2)
     p.ids = (r2 <= radius * radius).astype(np.uint8)
     lo = (tfsf_inset,) * 3
-    hi = (n - 1 - tfsf_inset,) * 3
+    hi = tuple(v - 1 - tfsf_inset for v in shape)
     k = (1.0, 0.0, 0.0)
     # E along z, H along y: the aux Hy already carries the sign of the
     # incident Hy, so the H polarisation multiplying it is +y.
-    p.tfsf = TFSF(aux_ncells=n, aux_values=gaussian_pulse(steps, offset=1.0), origin=(c, c, c), k=k,
+    p.tfsf = TFSF(aux_ncells=max(shape), aux_values=gaussian_pulse(steps, offset=1.0), origin=(cx, cy, cz), k=k,
                   pol_e=(0.0, 0.0, 1.0), pol_h=(0.0, 1.0, 0.0), planes=tfsf_box_planes(THREED, lo, hi))
     freqs = [0.01 * (q + 1) for q in range(nfreq)]
-    a0, a1 = dft_inset, n - 1 - dft_inset
     for a in range(3):
         for side in (0, 1):
-            plo = [a0, a0, a0]
-            phi = [a1, a1, a1]
-            plo[a] = phi[a] = a0 if side == 0 else a1
+            plo = [dft_inset] * 3
+            phi = [v - 1 - dft_inset for v in shape]
+            plo[a] = phi[a] = dft_inset if side == 0 else shape[a] - 1 - dft_inset
             tang = [b for b in range(3) if b != a]
             for b in tang:
                 p.dfts.append(DFTRegion(b, tuple(plo), tuple(phi), freqs))
@@ -407,29 +412,33 @@ def config4(n: int = 512, steps: int = 4000, npml: int = 16, design: int = 128, 
 
 
 def config5(n: int = 768, steps: int = 500, npml: int = 16, block: int = 32, seed: int = 0,
-            nfreq: int = 4) -> Problem:
+            nfreq: int = 4, shape: Optional[Tuple[int, int, int]] = None) -> Problem:
     """3D, 16-cell CPML, two-pole Lorentz everywhere (delta_eps 1.5, w0*dt
     0.1, delta*dt 0.005 and 0.8, 0.25, 0.02), eps_inf per 32^3 block uniform
     in [1,6] from `seed`, soft Ez dipole at the centre, DFT of Ez at 4
-    frequencies on the central z plane."""
+    frequencies on the central z plane. `shape` (nx, ny, nz) replaces the
+    cube n^3."""
+    shape = tuple(shape) if shape is not None else (n, n, n)
     dx = 1e-6
     dt = courant_dt(dx, 0.99 / math.sqrt(3.0))
-    p = Problem(THREED, (n, n, n), dx, dt, name=f"3d{n}_lorentz2_blocks{block}")
+    name = f"3d{n}_lorentz2_blocks{block}" if shape == (n, n, n) else \
+        f"3d{shape[0]}x{shape[1]}x{shape[2]}_lorentz2_blocks{block}"
+    p = Problem(THREED, shape, dx, dt, name=name)
     for a in range(3):
         for s in (0, 1):
             p.pml[(a, s)] = npml
     shift = int(round(math.log2(block)))
     assert 1 << shift == block
-    nb = (n + block - 1) // block
+    nb = [(v + block - 1) // block for v in shape]
     rng = np.random.default_rng(seed)
-    eps = rng.uniform(1.0, 6.0, size=nb ** 3)
+    eps = rng.uniform(1.0, 6.0, size=nb[0] * nb[1] * nb[2])
     poles = [(1.5, 0.1 / dt, 0.005 / dt), (0.8, 0.25 / dt, 0.02 / dt)]
     p.materials = [Material.lorentz(float(e), poles) for e in eps]
-    p.block_ids = np.arange(nb ** 3, dtype=np.uint16).reshape(nb, nb, nb)
+    p.block_ids = np.arange(eps.size, dtype=np.uint16).reshape(nb[2], nb[1], nb[0])
     p.block_shift = shift
-    c = n // 2
-    p.sources.append(Source(2, (c, c, c), gaussian_pulse(steps), "E"))
+    cx, cy, cz = (v // 2 for v in shape)
+    p.sources.append(Source(2, (cx, cy, cz), gaussian_pulse(steps), "E"))
     freqs = [0.01 * (q + 1) for q in range(nfreq)]
-    p.dfts.append(DFTRegion(2, (0, 0, c), (n - 1, n - 1, c), freqs))
+    p.dfts.append(DFTRegion(2, (0, 0, cz), (shape[0] - 1, shape[1] - 1, cz), freqs))
     p.steps = steps
     return p

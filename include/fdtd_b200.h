@@ -237,8 +237,12 @@ int fdtd_prepare(fdtd_grid* g);
  * - The array's address is looked up once per device on the first call, which
  *   may load the library's device code: make that call before any stream
  *   capture.
- * - DFT regions added since the last fdtd_step need one fdtd_step call to lay
- *   out their buffers; until then this returns FDTD_ERR_INVALID.
+ * - DFT regions added (or a CPML set) since the last step need fdtd_prepare
+ *   (or one fdtd_step) to lay out their buffers; until then this returns
+ *   FDTD_ERR_INVALID. So does a call between the halves of fdtd_step_half.
+ * - With TFSF planes the call uploads the step counter from the host and
+ *   waits for that copy; on a stream under capture it returns
+ *   FDTD_ERR_UNSUPPORTED.
  * - The array is shared by all grids of a device: calls whose GPU work
  *   overlaps (other streams or host threads) race on it. */
 int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream);
@@ -274,6 +278,17 @@ int fdtd_upload(fdtd_grid* g, int which, const double* host);
 
 /* Checks every stored field for NaN/Inf; FDTD_ERR_NONFINITE if any. */
 int fdtd_check_finite(fdtd_grid* g);
+
+/* Relative-L2 error of one field of grid g against the same field of grid
+ * ref (same shape and device, either precision), computed on the device in
+ * FP64 and in SI units over every cell: err_sq = sum (g - ref)^2, ref_sq =
+ * sum ref^2, so the relative L2 error is sqrt(err_sq / ref_sq). `which` is a
+ * field selector of fdtd_download (E, H, and D, B, P, J where both grids
+ * store them; not the CPML integrators). Waits for both grids' streams. The
+ * reference keeps no second copy of its fields to compare against; this
+ * states the FP32 method's error against an FP64 plain grid at sizes where
+ * downloading both would not fit host memory. */
+int fdtd_field_error(fdtd_grid* g, fdtd_grid* ref, int which, double* err_sq, double* ref_sq);
 
 /* Steps taken so far, and kernels this handle launched so far. */
 int fdtd_get_step(fdtd_grid* g, long long* step);

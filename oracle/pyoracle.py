@@ -21,6 +21,14 @@ SOURCE_TARGETS = {"E": 0, "D": 1, "H": 2, "B": 3}
 BOUNDARY_KINDS = {"pec": 1, "pmc": 2, "symmetric": 3, "antisymmetric": 4, "periodic": 5}
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference tree (pederson/fdtd) lies: FDTD_REFERENCE_DIR, or the
+# container's read-only copy. The reference runner and the XML writers are
+# compiled from its headers there; without it the golden fixtures stand in.
+REFERENCE_DIR = os.environ.get("FDTD_REFERENCE_DIR") or "/root/reference"
+
+
+def reference_tree_present() -> bool:
+    return os.path.isfile(os.path.join(REFERENCE_DIR, "include", "YeeUpdates.hpp"))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 RUNNER_PATH = os.path.join(HERE, "_ref", "ref_runner")
 
@@ -49,8 +57,8 @@ def build(quiet: bool = True) -> None:
     is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", HERE, "_ref/ref_runner"], check=True,
+    if reference_tree_present():
+        subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_DIR}", "_ref/ref_runner"], check=True,
                        stdout=subprocess.DEVNULL if quiet else None)
 
 

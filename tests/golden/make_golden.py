@@ -5,7 +5,7 @@ oracle/_ref/ref_runner -- the reference's own update functors compiled from
 its headers (oracle/Makefile) -- and the final fields are stored as
 <name>.npz. Run from the repository root, where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle REF=$FDTD_REFERENCE_DIR ref && python tests/golden/make_golden.py
 
 It also writes config_*.xml: the reference's own XML writers (print_summary
 of MaterialMap, PMLOptions, BoundaryOptions) run on config_spec.txt by

@@ -15,6 +15,8 @@ import subprocess
 import numpy as np
 import pytest
 
+import pyoracle
+
 import scenarios
 from fdtd_b200 import config_xml as C
 from fdtd_b200 import problem as P
@@ -80,9 +82,10 @@ def test_golden_reference_writer_output_reads_back():
            os.path.join(GOLDEN, "config_pml.xml"), os.path.join(GOLDEN, "config_boundaries.xml"))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not present")
+@pytest.mark.skipif(not pyoracle.reference_tree_present(), reason="reference tree not present")
 def test_reference_writer_live_random_values(tmp_path):
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "_ref/ref_xml"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={pyoracle.REFERENCE_DIR}", "_ref/ref_xml"],
+                   check=True)
     rng = np.random.default_rng(7)
     six = lambda v: float(f"{v:.6g}")  # the writer's default stream precision
     lines = ["nmat 8"]

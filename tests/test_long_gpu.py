@@ -1,0 +1,116 @@
+"""GPU parity at the configurations' own lengths, against the CPU oracle.
+
+The scenario tests run 40-100 steps; these run the step counts of the
+benchmark configurations, so FP32 round-off accumulated over hundreds of
+steps, the DFT over thousands of samples (many 64-sample flushes) and the
+staged 3D sweeps at a row pitch above 128 cells (CPML lanes at both row
+ends) are covered:
+
+* 2D TM vacuum 256^2, 2000 steps, FP64 plain (the configuration itself):
+  <= 1e-12 relative L2 on fields, CPML integrators and the row DFT.
+* 3D Drude sphere with TFSF box and face DFTs (132x44x44, 1000 steps): FP64
+  plain <= 1e-12, FP32 fused <= 1e-4 on E, H and every DFT spectrum.
+* 3D two-pole Lorentz in every cell, eps per 16^3 block, central-plane DFT
+  (132x48x48, 500 steps): FP64 <= 1e-12, FP32 <= 1e-4.
+* The four smallest batched 2D TE problems of the 64 (seed 0) at their 3000
+  steps, stepped together by the batch kernel: FP32 <= 1e-4 on E, H.
+
+The CPU oracle runs in spawned worker processes (one per problem, started
+before any GPU work of this module) while the GPU grids step.
+"""
+import concurrent.futures as cf
+import multiprocessing as mp
+
+import numpy as np
+import pytest
+
+from helpers import batch_subset, long_problem, mode_fields, oracle_job, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_TOL = 1e-12
+FUSED_TOL = 1e-4
+
+PSI = [f"psi{'EH'[f]}{'xyz'[i]}{'xyz'[j]}" for f in range(2) for i in range(3) for j in range(3)]
+JOBS = {
+    "tm256_2000": ["Ez", "Hx", "Hy", "Dz", "Bx", "By"] + PSI,
+    "drude132x44x44_1000": ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz", "Jx", "Jy", "Jz"],
+    "lorentz132x48x48_500": ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"],
+}
+for _q in range(4):
+    JOBS[f"batch3000_{_q}"] = ["Ex", "Ey", "Hz"]
+
+
+@pytest.fixture(scope="module")
+def long_oracle():
+    """The oracle's results of every long problem, computed concurrently."""
+    ctx = mp.get_context("spawn")
+    ex = cf.ProcessPoolExecutor(max_workers=len(JOBS), mp_context=ctx)
+    futs = {name: ex.submit(oracle_job, (name, names)) for name, names in JOBS.items()}
+    cache = {}
+
+    def get(name):
+        if name not in cache:
+            cache[name] = futs[name].result()
+        return cache[name]
+
+    yield get
+    ex.shutdown(wait=True)
+
+
+def _check(p, g, ref, names, tol):
+    fields, dfts, _ = ref
+    worst = {}
+    for n in names:
+        r = fields[n]
+        if np.any(r):
+            worst[n] = rel_l2(g.get(n), r)
+    for q, r in enumerate(dfts):
+        worst[f"dft{q}"] = rel_l2(g.dft(q), r)
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, f"{p.name}: {bad}"
+    return worst
+
+
+def test_config1_full_length_f64(fdtd, long_oracle):
+    """2D TM 256^2 vacuum, 16-cell CPML, Gaussian Ez source, row DFT at three
+    frequencies, 2000 steps: the configuration itself, FP64 <= 1e-12."""
+    p = long_problem("tm256_2000")
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    g.synchronize()
+    _check(p, g, long_oracle("tm256_2000"), JOBS["tm256_2000"], PLAIN_TOL)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["drude132x44x44_1000", "lorentz132x48x48_500"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_3d_config_length(fdtd, long_oracle, name, prec):
+    p = long_problem(name)
+    assert p.shape[0] > 128  # FP32 rows padded to a 256-cell pitch
+    g = fdtd.Grid.from_problem(p, prec)
+    g.step(p.steps)
+    g.synchronize()
+    assert g.error_flags() == 0
+    names = JOBS[name] if prec == "f64" else ["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"]
+    worst = _check(p, g, long_oracle(name), names, PLAIN_TOL if prec == "f64" else FUSED_TOL)
+    g.close()
+    print(name, prec, max(worst.values()))
+
+
+def test_batch_config_length(fdtd, long_oracle):
+    """Four batched TE problems of different sizes, 3000 steps in one
+    persistent launch per call (graph-replayed), FP32 <= 1e-4."""
+    probs = batch_subset()
+    assert len({p.shape for p in probs}) == 4
+    grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+    b = fdtd.Batch(grids)
+    b.configure("persistent", 4)
+    b.step(3000)
+    assert b.error_flags() == 0
+    for q, (p, g) in enumerate(zip(probs, grids)):
+        E, H, _, _ = mode_fields(p.mode)
+        _check(p, g, long_oracle(f"batch3000_{q}"), E + H, FUSED_TOL)
+    b.close()
+    for g in grids:
+        g.close()

@@ -15,6 +15,8 @@ import os
 import numpy as np
 import pytest
 
+import pyoracle
+
 import scenarios
 from helpers import rel_l2
 
@@ -38,7 +40,7 @@ def test_oracle_matches_golden_bitwise(oracle, make):
             assert not np.any(g.get(n)), f"{p.name}:{n} should be zero"
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not present")
+@pytest.mark.skipif(not pyoracle.reference_tree_present(), reason="reference tree not present")
 def test_oracle_matches_reference_runner_live(oracle):
     import subprocess
     subprocess.run(["make", "-s", "-C", os.path.dirname(oracle.__file__), "_ref/ref_runner"], check=True)

@@ -76,3 +76,70 @@ def test_static_scratch_step_after_prepare(fdtd):
     for name in ("Ex", "Ez", "Hy"):
         assert rel_l2(new.get(name), ref.get(name)) <= TOL["f32"], name
     assert rel_l2(new.dft(0), ref.dft(0)) <= TOL["f32"]
+
+
+def test_static_scratch_step_on_caller_stream(fdtd):
+    """A stream of the caller (not the grid's own) gives fdtd_step's results;
+    the grid's set-up work is ordered before it."""
+    import torch
+    p = scenarios.td_tfsf_box()
+    ref = fdtd.Grid.from_problem(p, "f32")
+    new = fdtd.Grid.from_problem(p, "f32")
+    new.prepare()
+    s = torch.cuda.Stream()
+    n = p.steps // 2
+    for _ in range(2):
+        ref.step(n)
+        new.step_static_scratch(n, stream=s.cuda_stream)
+    s.synchronize()
+    for name in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert rel_l2(new.get(name), ref.get(name)) <= TOL["f32"], name
+    for q in range(len(p.dfts)):
+        assert rel_l2(new.dft(q), ref.dft(q)) <= TOL["f32"]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_static_scratch_step_refuses_between_halves(fdtd, prec):
+    p = scenarios.td_tfsf_box()
+    g = fdtd.Grid.from_problem(p, prec)
+    g.prepare()
+    g.step_half(0)
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.step_static_scratch(2)
+    assert e.value.code == -1
+    assert "half" in str(e.value)
+    g.step_half(1)
+    g.step_static_scratch(2)
+    assert g.step_count == 3
+
+
+def test_static_scratch_step_refuses_oversize_calls_f64(fdtd):
+    p = scenarios.td_tfsf_box()
+    p.dfts = []
+    g = fdtd.Grid.from_problem(p, "f64")
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.step_static_scratch(1 << 20)
+    assert e.value.code == -1
+    assert "steps per call" in str(e.value)
+    assert g.step_count == 0
+
+
+def test_static_scratch_step_allocates_nothing(fdtd):
+    """Free device memory (cudaMemGetInfo) is the same before and after a
+    call that takes more steps than any call before it (fdtd_step would grow
+    its TFSF table with cudaMalloc there)."""
+    import torch
+    p = scenarios.td_tfsf_box()
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.prepare()
+    # the first call on a device looks up the array's address, and the
+    # runtime may load kernels on their first use: one call of every kernel
+    # this test runs comes first
+    g.step_static_scratch(p.steps)
+    g.synchronize()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    g.step_static_scratch(p.steps + 8)
+    g.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
