@@ -89,7 +89,7 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=-1,
                     help="steps at which the FP32 error against FP64 is measured (-1: the configuration's length, "
                          "0: skip)")
-    ap.add_argument("--sweep", default="auto", choices=["auto", "regs", "tma", "flat", "staged"],
+    ap.add_argument("--sweep", default="auto", choices=["auto", "regs", "tma", "flat", "staged", "eh"],
                     help="3D FP32 sweep kernels (fdtd_set_sweep_kernel)")
     ap.add_argument("--batch-mode", default="tune", choices=["tune", "persistent", "per_phase"],
                     help="batch64: autotune, or force a launch mode (with --batch-rows)")
@@ -756,14 +756,21 @@ def run_grid(args, torch, world, rank, local, stream):
     prof = g.profile_step(nprof, stream=stream.cuda_stream)
     ab = alg_bytes(p, 4)
     peak, peak_kind = peaks()
-    e_ach = ab["e_sweep"] / (prof["e_sweep"] / 1e3) / 1e9
-    h_ach = ab["h_sweep"] / (prof["h_sweep"] / 1e3) / 1e9
-    step_ach = ab["step"] * args.steps / (ms / 1e3) / 1e9
     state_gb = g.memory_bytes / 1e9
     three_d = p.mode == 3
     kind = {"auto": "staged"}.get(args.sweep, args.sweep)
-    e_name = f"{kind}_e_kernel (E sweep)" if three_d else "fused_e_kernel (E sweep)"
-    h_name = f"{kind}_h_kernel (H sweep)" if three_d else "fused_h_kernel (H sweep)"
+    one_launch = kind == "eh" and three_d
+    if one_launch:
+        # E and H of the whole step in one launch: its bytes are the step's
+        ab = dict(ab, e_sweep=ab["step"], h_sweep=0.0)
+    e_ach = ab["e_sweep"] / (prof["e_sweep"] / 1e3) / 1e9
+    h_ach = ab["h_sweep"] / (prof["h_sweep"] / 1e3) / 1e9 if prof["h_sweep"] > 0 else None
+    step_ach = ab["step"] * args.steps / (ms / 1e3) / 1e9
+    if one_launch:
+        e_name, h_name = "staged_eh_kernel (E and H sweeps of a step, one launch)", None
+    else:
+        e_name = f"{kind}_e_kernel (E sweep)" if three_d else "fused_e_kernel (E sweep)"
+        h_name = f"{kind}_h_kernel (H sweep)" if three_d else "fused_h_kernel (H sweep)"
     # DRAM traffic per launch: dram__bytes_read.sum + dram__bytes_write.sum of
     # one ncu capture of the same kernel on the same physics at a smaller size,
     # scaled by interior cells (traffic grows with the cells swept)
@@ -856,7 +863,8 @@ def run_grid(args, torch, world, rank, local, stream):
                          + ("larger than L2, no flush" if state_gb > 0.126 else "fits L2"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         # the whole step against the minimal formulation's bytes per cell-step
-        "roofline": {"bound": "hbm", "scope": "whole step (all kernels of a step)", "kernel": f"{e_name} + {h_name} + extras",
+        "roofline": {"bound": "hbm", "scope": "whole step (all kernels of a step)",
+                     "kernel": f"{e_name} + extras" if h_name is None else f"{e_name} + {h_name} + extras",
                      "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
                      "peak_kind": peak_kind, "alg_bytes_per_cell_step": ab["per_cell_step"],
                      "alg_bytes_per_step": ab["step"], "step_ms": ms / args.steps,
@@ -864,8 +872,9 @@ def run_grid(args, torch, world, rank, local, stream):
                      "traffic_source": tr["source"] if tr else None},
         "roofline_e": {"kernel": e_name, "achieved": e_ach, "frac": e_ach / peak,
                        "alg_bytes_per_launch": ab["e_sweep"], "launch_ms": prof["e_sweep"], "traffic": traffic_e},
-        "roofline_h": {"kernel": h_name, "achieved": h_ach, "frac": h_ach / peak,
-                       "alg_bytes_per_launch": ab["h_sweep"], "launch_ms": prof["h_sweep"], "traffic": traffic_h},
+        "roofline_h": None if h_name is None else {
+            "kernel": h_name, "achieved": h_ach, "frac": h_ach / peak, "alg_bytes_per_launch": ab["h_sweep"],
+            "launch_ms": prof["h_sweep"], "traffic": traffic_h},
         "kernel_ms": prof,
         "fp64_plain": f64,
         "fp32_over_fp64": (value / world / f64["value"]) if f64 else None,

@@ -207,6 +207,8 @@ struct fdtd_grid {
   void* hist[2][3][3]{};  // FP64 flux history [D|B][level][comp] of BD3/BD4
   int sweep_kind = FDTD_SWEEP_AUTO;
   TmaState* tma = nullptr;
+  unsigned* d_eh = nullptr;  // one-launch step: [0] epoch, then the E tile flags
+  long long eh_words = 0;
   long long version = 0;        // bumped by every change a captured graph would bake in
   long long graph_version = -1;
   cudaGraphExec_t graph = nullptr;
@@ -348,6 +350,20 @@ int ensure_pml(fdtd_grid* g) {
   if (rc) return rc;
   g->dirty_pml = false;
   return FDTD_OK;
+}
+
+// The one-launch 3D FP32 step keeps an epoch and one flag per E tile of
+// every plane (zeroed); laid out once, before any step that may use it.
+bool eh_wanted(const fdtd_grid* g) {
+  return g->f32 && g->d.mode == kThreeD && (g->sweep_kind == FDTD_SWEEP_EH || g->sweep_kind == FDTD_SWEEP_AUTO);
+}
+
+int ensure_eh(fdtd_grid* g) {
+  if (!eh_wanted(g) || g->d_eh) return FDTD_OK;
+  const long long nbx = g->pitch / 128, nby = (g->n[1] - 2 + 3) / 4, np = g->n[2] - 2;
+  if (nbx <= 0 || nby <= 0 || np <= 0) return FDTD_OK;
+  g->eh_words = 1 + nbx * nby * np;
+  return dalloc(g, reinterpret_cast<void**>(&g->d_eh), static_cast<size_t>(g->eh_words) * sizeof(unsigned));
 }
 
 int alloc_psi(fdtd_grid* g) {
@@ -1276,6 +1292,8 @@ int fdtd_prepare(fdtd_grid* g) try {
   CK(cudaSetDevice(g->d.device));
   int rc = ensure_pml(g);
   if (rc) return rc;
+  rc = ensure_eh(g);
+  if (rc) return rc;
   if (g->dirty_dft) {
     rc = rebuild_dft(g);
     if (rc) return rc;
@@ -1319,8 +1337,48 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
       use3d && (g->sweep_kind == FDTD_SWEEP_STAGED || g->sweep_kind == FDTD_SWEEP_AUTO);
   const bool use_flat = use3d && !use_tma && !use_staged && g->sweep_kind == FDTD_SWEEP_FLAT;
   const bool boxes = !g->boxes.empty();
+  // the whole step in one launch: 3D FP32 grids without TFSF planes, box
+  // sources, boundary conditions or mu_r != 1 (whose extra kernels run
+  // between the two sweeps)
+  EhSched eh{};
+  int eh_blocks = 0;
+  const bool use_eh = use3d && !use_tma && eh_wanted(g) && g->d_eh && !boxes && g->bcs.n == 0 &&
+                      g->sweep_kind == FDTD_SWEEP_EH && staged_eh_plan(fa, &eh, &eh_blocks);
+  if (g->sweep_kind == FDTD_SWEEP_EH && !use_eh)
+    return fail(FDTD_ERR_UNSUPPORTED,
+                "the one-launch step needs a 3D FP32 grid without TFSF planes, box sources, boundary conditions "
+                "or mu_r != 1");
+  if (use_eh) {
+    eh.epoch = g->d_eh;
+    eh.flags = g->d_eh + 1;
+  }
   for (int q = 0; q < nsteps; q++) {
     if (prof) CK(cudaEventRecord(ev[0], s));
+    if (use_eh) {
+      g->launches += launch_staged_eh(fa, eh, eh_blocks, s);
+      if (prof) CK(cudaEventRecord(ev[1], s));
+      g->launches += launch_dft_gather(1, g->d_dft[0], g->ndft[0], g->dft_pts[0], g->dft_maxpts[0], fE, g->n[1],
+                                       static_cast<int>(rowlen(g)), g->dft_pending, g->d_dft_buf[0], s);
+      if (prof) {
+        CK(cudaEventRecord(ev[2], s));
+        CK(cudaEventRecord(ev[3], s));
+      }
+      g->launches += launch_dft_gather(1, g->d_dft[1], g->ndft[1], g->dft_pts[1], g->dft_maxpts[1], fH, g->n[1],
+                                       static_cast<int>(rowlen(g)), g->dft_pending, g->d_dft_buf[1], s);
+      if (prof) CK(cudaEventRecord(ev[4], s));
+      g->launches += launch_step_advance(g->ctrl, g->d_eh, s);
+      if (!g->dfts.empty() && ++g->dft_pending == kDftChunk) g->launches += flush_dft(g, s);
+      if (prof) {
+        CK(cudaEventRecord(ev[5], s));
+        CK(cudaEventSynchronize(ev[5]));
+        for (int k = 0; k < 5; k++) {
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+          prof[k] += ms / nsteps;
+        }
+      }
+      continue;
+    }
     if (boxes && g->f32) g->launches += launch_boxes(g, 0, -1, s);
     if (g->f32) {
       g->launches += use_tma      ? launch_tma_e(fa, g->tma, s)
@@ -1379,7 +1437,9 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   CK(cudaSetDevice(g->d.device));
   {
     // before any graph capture: the CPML set-up synchronises its stream
-    const int prc = ensure_pml(g);
+    int prc = ensure_pml(g);
+    if (prc) return prc;
+    prc = ensure_eh(g);
     if (prc) return prc;
   }
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
@@ -1460,7 +1520,7 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
 
 int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
-  if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_STAGED) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
+  if (kind < FDTD_SWEEP_AUTO || kind > FDTD_SWEEP_EH) return fail(FDTD_ERR_INVALID, "bad sweep kernel kind");
   g->sweep_kind = kind;
   g->version++;
   return FDTD_OK;

@@ -1,6 +1,10 @@
 // Internal declarations shared by the fdtd_b200 CUDA sources.
 #pragma once
 #include <cstdint>
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace fdtdb {
@@ -12,6 +16,20 @@ constexpr int kMaxSources = 16;
 constexpr int kAuxNpml = 15;  // Aux1D::mNPML (include/Source.hpp:362)
 constexpr int kDftChunk = 64;  // samples buffered per DFT point before a flush
 constexpr int kGraphSteps = kDftChunk;  // steps per captured CUDA graph
+
+// Runs set(), once per (current device, key) in the process, under a lock:
+// for kernel attributes (dynamic shared memory limit, carveout), which belong
+// to a device's context, so that grids on several devices and several host
+// threads each see them set before their first launch.
+template <typename F>
+inline void once_per_device(const void* key, F set) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.insert({dev, key}).second) set();
+}
 
 // include/FDTDConstants.hpp:394-398
 constexpr double kPi = 3.14159265358979323846264338327950288;
@@ -219,6 +237,24 @@ int launch_flat_e(const FusedArgs& a, cudaStream_t s);
 int launch_flat_h(const FusedArgs& a, cudaStream_t s);
 int launch_staged_e(const FusedArgs& a, cudaStream_t s);
 int launch_staged_h(const FusedArgs& a, cudaStream_t s);
+// The whole 3D FP32 step (E and H sweeps) in one persistent launch: work
+// items are tiles of one plane (128 cells x 4 rows) of the E or the H sweep,
+// ordered E(1..lag), then E(k), H(k - lag) for k = lag+1..np, then the last
+// H planes; the CTAs take items round-robin, and an H tile first waits for
+// the E tiles it reads (flags holding the launch's epoch).
+struct EhSched {
+  int nbx, nby;           // tiles per plane: x blocks of 128 cells, y blocks of 4 rows
+  int np;                 // interior planes (nz - 2)
+  int lag;                // H of plane k - lag follows E of plane k
+  long long nitems;       // 2 * np * nbx * nby
+  unsigned* flags;        // [np][nbx * nby]: epoch at which E of (plane, tile) was stored
+  const unsigned* epoch;  // steps launched so far; this launch's epoch is *epoch + 1
+};
+// Plans the one-launch step of grid `a` on the current device: the tiles,
+// the resident CTAs (`blocks`) and the lag. false if the grid needs the two
+// sweeps (or the kernel cannot be resident).
+bool staged_eh_plan(const FusedArgs& a, EhSched* s, int* blocks);
+int launch_staged_eh(const FusedArgs& a, const EhSched& s, int blocks, cudaStream_t st);
 int launch_tfsf_fused(int mode, const FusedArgs& a, int ft, cudaStream_t s);
 int launch_fused3d_e(const FusedArgs& a, cudaStream_t s);
 int launch_fused3d_h(const FusedArgs& a, cudaStream_t s);
@@ -236,6 +272,8 @@ int launch_dft_rebase(Control* ctrl, int nsamp, cudaStream_t s);
 int launch_dft_set_base(Control* ctrl, long long base, cudaStream_t s);
 int launch_finite_check(const void* p, long long n, int is_f32, int* flag, cudaStream_t s);
 int launch_step_advance(Control* ctrl, cudaStream_t s);
+// advances the step counter and, if non-null, the one-launch step's epoch
+int launch_step_advance(Control* ctrl, unsigned* epoch, cudaStream_t s);
 // out[0] += sum over rows of (a*sa - b*sb)^2, out[1] += sum (b*sb)^2 (FP64)
 int launch_field_diff(const void* a, int a_f32, long long rla, double sa, const void* b, int b_f32, long long rlb,
                       double sb, int nx, long long nrows, double* out, cudaStream_t s);

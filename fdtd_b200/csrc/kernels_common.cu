@@ -273,7 +273,10 @@ int launch_field_diff(const void* a, int a_f32, long long rla, double sa, const 
   return 1;
 }
 
-__global__ void step_advance_kernel(Control* ctrl) { ctrl->t += 1; }
+__global__ void step_advance_kernel(Control* ctrl, unsigned* epoch) {
+  ctrl->t += 1;
+  if (epoch) *epoch += 1u;
+}
 
 __global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }
 
@@ -396,8 +399,10 @@ int launch_batch_advance(Control* const* ctrls, int n, int nsteps, cudaStream_t 
   return 1;
 }
 
-int launch_step_advance(Control* ctrl, cudaStream_t s) {
-  step_advance_kernel<<<1, 1, 0, s>>>(ctrl);
+int launch_step_advance(Control* ctrl, cudaStream_t s) { return launch_step_advance(ctrl, nullptr, s); }
+
+int launch_step_advance(Control* ctrl, unsigned* epoch, cudaStream_t s) {
+  step_advance_kernel<<<1, 1, 0, s>>>(ctrl, epoch);
   return 1;
 }
 

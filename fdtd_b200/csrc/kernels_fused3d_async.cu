@@ -55,18 +55,18 @@ __device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx&
 
 }  // namespace
 
+// The E update of one tile: the 4-cell groups of x block bx (128 cells),
+// rows 1 + 4 by .. 4 + 4 by, plane k; one group per thread of the CTA's 128.
 // PJ: every material of the grid is dispersive, so the group's J (and P)
 // are staged with the fields and all of the thread's loads are in flight at
 // once (they are otherwise read per component, after the fields arrive)
-template <int MAXP, int MINB, bool PJ>
-__global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_constant__ FusedArgs a) {
-  extern __shared__ float4 sm[];
+template <int MAXP, bool PJ>
+__device__ __forceinline__ void e_tile(const FusedArgs& a, int bx, int by, int k, float4* sm) {
   constexpr int kPJ = PJ ? pj_slots<MAXP>() : 0;
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
-  const int x4 = blockIdx.x * 128 + lane * 4;
-  const int j = 1 + blockIdx.y * kRowsA + threadIdx.y;
+  const int x4 = bx * 128 + lane * 4;
+  const int j = 1 + by * kRowsA + threadIdx.y;
   const int jl = min(j, a.ny - 2);
-  const int k = 1 + blockIdx.z;
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
   const long long c = k * sz + jl * sy + x4;
   float4* s = sm + tid;
@@ -114,15 +114,21 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
                        PJ ? s + kSlotsE * kThreads : nullptr, kThreads);
 }
 
-template <int MINB, bool MU>
-__global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_constant__ FusedArgs a) {
+template <int MAXP, int MINB, bool PJ>
+__global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
+  e_tile<MAXP, PJ>(a, blockIdx.x, blockIdx.y, 1 + blockIdx.z, sm);
+}
+
+// The H update of one tile (as e_tile). CG: the E values of the x+1
+// neighbour tile are read through L2 only (ld.global.cg), for a kernel in
+// which another CTA wrote them earlier in the same launch.
+template <bool MU, bool CG>
+__device__ __forceinline__ void h_tile(const FusedArgs& a, int bx, int by, int k, float4* sm) {
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
-  const int x4 = blockIdx.x * 128 + lane * 4;
-  const int j = 1 + blockIdx.y * kRowsA + threadIdx.y;
+  const int x4 = bx * 128 + lane * 4;
+  const int j = 1 + by * kRowsA + threadIdx.y;
   const int jl = min(j, a.ny - 2);
-  // planes from the top down, as the flat H sweep
-  const int k = a.nz - 2 - blockIdx.z;
   const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
   const long long c = k * sz + jl * sy + x4;
   float4* s = sm + tid;
@@ -138,8 +144,13 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
   cp_async16(s + 9 * kThreads, a.H[2] + c);
   float ey_xp3 = 0.f, ez_xp3 = 0.f;
   if (lane == 31) {
-    ey_xp3 = a.E[1][c + 4];
-    ez_xp3 = a.E[2][c + 4];
+    if (CG) {
+      ey_xp3 = __ldcg(a.E[1] + c + 4);
+      ez_xp3 = __ldcg(a.E[2] + c + 4);
+    } else {
+      ey_xp3 = a.E[1][c + 4];
+      ez_xp3 = a.E[2][c + 4];
+    }
   }
   const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
   float* px = reinterpret_cast<float*>(sm + 10 * kThreads) + 8 * tid;
@@ -154,6 +165,13 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_c
   }
   h_group_update<MU>(a, g, k, s[2 * kThreads], ey, ez, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads], ey_xp3,
                  ez_xp3, s[7 * kThreads], s[8 * kThreads], s[9 * kThreads], px);
+}
+
+template <int MINB, bool MU>
+__global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_constant__ FusedArgs a) {
+  extern __shared__ float4 sm[];
+  // planes from the top down, as the flat H sweep
+  h_tile<MU, false>(a, blockIdx.x, blockIdx.y, a.nz - 2 - blockIdx.z, sm);
 }
 
 // The shared-memory carveout (percent of the largest) that holds `ctas` CTAs
@@ -178,12 +196,11 @@ static void staged_e_launch(const FusedArgs& a, cudaStream_t s) {
   constexpr int minb = !PJ ? (MAXP >= 2 ? 6 : 7) : (MAXP >= 2 ? 4 : (MAXP == 1 ? 6 : 7));
   const size_t smem = slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned);
   auto fn = staged_e_kernel<MAXP, minb, PJ>;
-  static bool attrs = false;  // once: the shared-memory split that holds minb CTAs, the rest as L1
-  if (!attrs) {
+  // once per device: the shared-memory split that holds minb CTAs, the rest as L1
+  once_per_device(reinterpret_cast<const void*>(fn), [&] {
     cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_for(minb, smem));
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    attrs = true;
-  }
+  });
   fn<<<grid, block, smem, s>>>(a);
 }
 
@@ -212,18 +229,197 @@ template <bool MU>
 static void staged_h_dispatch(const FusedArgs& a, cudaStream_t s) {
   dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.nz - 2), block(32, kRowsA, 1);
   const size_t smem = kSlotsH * kThreads * sizeof(float4);
-  static bool carveout = false;
-  if (!carveout) {
-    cudaFuncSetAttribute(staged_h_kernel<8, MU>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         carveout_for(8, smem));
-    carveout = true;
-  }
+  once_per_device(reinterpret_cast<const void*>(staged_h_kernel<8, MU>), [&] {
+    cudaFuncSetAttribute(staged_h_kernel<8, MU>, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_for(8, smem));
+  });
   staged_h_kernel<8, MU><<<grid, block, smem, s>>>(a);
 }
 
 int launch_staged_h(const FusedArgs& a, cudaStream_t s) {
   if (a.has_mu) staged_h_dispatch<true>(a, s);
   else staged_h_dispatch<false>(a, s);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// The whole step in one launch (staged_eh_kernel).
+//
+// The two sweeps read each E and H word twice per step: the E sweep reads H
+// and E, the H sweep E and H again. Here one persistent launch runs both, in
+// an order that keeps what the H tiles read in L2: work items are tiles of one
+// plane of one sweep, taken round-robin by the resident CTAs in the order
+//   E(1) .. E(lag),  E(lag+1) H(1),  E(lag+2) H(2),  ..,  E(np) H(np-lag),
+//   H(np-lag+1) .. H(np)
+// (each a batch of every tile of the plane), so H of plane k runs about lag
+// planes after E of plane k has stored the E it reads, and the E and H of the
+// planes in between are still in L2.
+//
+// Dependences. E of tile t at plane k reads H at planes k and k-1 of t, and
+// at plane k of t's x-1 and y-1 neighbours; H of tile t at plane k reads E at
+// planes k and k+1 of t and at plane k of the x+1 and y+1 neighbours, and
+// overwrites the H that the E tiles at (k, t), (k, t+x), (k, t+y) and
+// (k+1, t) read. So H(k, t) runs once those four E tiles are done: each E
+// tile publishes its epoch in flags[k][t] (release, after a CTA barrier), and
+// the first thread of an H tile acquires the flags of the four before the
+// CTA reads anything. Every dependence points to an earlier item, and every
+// CTA is resident (cooperative launch), so the earliest unfinished item can
+// always run: no cycle of waits. Each wait is bounded; on expiry the kernel
+// sets bit 1 of the grid's error flags and goes on (the step's result is
+// then wrong, but the launch ends). E values that another CTA wrote in this
+// launch are read through L2 only (cp.async.cg, ld.global.cg).
+//
+// The epoch is read from device memory at launch and advanced by the step
+// counter's kernel after it, never reset, so flags of an earlier launch
+// never satisfy a later one.
+namespace {
+
+constexpr int kDepPolls = 1 << 18;  // a few tenths of a second with the back-off below
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// waits (bounded) until *p has reached `target`; false if it gave up, or
+// if another wait of the launch gave up before (bit 1 of *err): after the
+// first expiry no tile waits any more, so the launch ends soon whatever the
+// cause
+__device__ __forceinline__ bool wait_epoch(const unsigned* p, unsigned target, const int* err) {
+  for (int it = 0; it < kDepPolls; it++) {
+    if (static_cast<int>(ld_acquire_u32(p) - target) >= 0) return true;
+    if ((it & 63) == 63 && (*reinterpret_cast<const volatile int*>(err) & 2)) return false;
+    __nanosleep(it < 32 ? 32 : 256);
+  }
+  return false;
+}
+
+}  // namespace
+
+template <int MAXP, int MINB, bool PJ>
+__global__ void __launch_bounds__(kThreads, MINB)
+    staged_eh_kernel(const __grid_constant__ FusedArgs a, const __grid_constant__ EhSched s) {
+  extern __shared__ float4 sm[];
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  const unsigned target = *s.epoch + 1u;
+  const int T = s.nbx * s.nby, L = s.lag, NP = s.np;
+  for (long long it = blockIdx.x; it < s.nitems; it += gridDim.x) {
+    const int b = static_cast<int>(it / T);
+    const int tile = static_cast<int>(it - static_cast<long long>(b) * T);
+    bool e_phase;
+    int k;
+    if (b < L) {
+      e_phase = true;
+      k = 1 + b;
+    } else if (b < 2 * NP - L) {
+      const int m = b - L;
+      e_phase = (m & 1) == 0;
+      k = e_phase ? L + 1 + (m >> 1) : 1 + (m >> 1);
+    } else {
+      e_phase = false;
+      k = NP - L + 1 + (b - (2 * NP - L));
+    }
+    const int bx = tile % s.nbx, by = tile / s.nbx;
+    unsigned* f = s.flags + static_cast<long long>(k - 1) * T + tile;
+    if (e_phase) {
+      e_tile<MAXP, PJ>(a, bx, by, k, sm);
+      __syncthreads();
+      if (lead) {
+        __threadfence();
+        st_release_u32(f, target);
+      }
+    } else {
+      if (lead) {
+        const int* err = &a.ctrl->error;
+        bool ok = wait_epoch(f, target, err);
+        if (ok && bx + 1 < s.nbx) ok = wait_epoch(f + 1, target, err);
+        if (ok && by + 1 < s.nby) ok = wait_epoch(f + s.nbx, target, err);
+        if (ok && k < NP) ok = wait_epoch(f + T, target, err);
+        if (!ok) atomicOr(&a.ctrl->error, 2);
+      }
+      __syncthreads();
+      h_tile<false, true>(a, bx, by, k, sm);
+    }
+  }
+}
+
+namespace {
+
+// the kernel and its dynamic shared memory for a grid's materials
+struct EhKernel {
+  const void* fn;
+  size_t smem;
+  int minb;
+};
+
+template <int MAXP, bool PJ>
+EhKernel eh_kernel() {
+  constexpr int slots = kSlotsE + (PJ ? pj_slots<MAXP>() : 0);
+  constexpr int minb = !PJ ? (MAXP >= 2 ? 6 : 7) : (MAXP >= 2 ? 4 : (MAXP == 1 ? 6 : 7));
+  return {reinterpret_cast<const void*>(staged_eh_kernel<MAXP, minb, PJ>),
+          slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned), minb};
+}
+
+EhKernel eh_select(const FusedArgs& a) {
+  const bool pj = a.all_dispersive != 0;
+  switch (a.max_poles) {
+    case 0: return eh_kernel<0, false>();
+    case -1: return pj ? eh_kernel<-1, true>() : eh_kernel<-1, false>();
+    case 1: return pj ? eh_kernel<1, true>() : eh_kernel<1, false>();
+    default: return pj ? eh_kernel<2, true>() : eh_kernel<2, false>();
+  }
+}
+
+}  // namespace
+
+bool staged_eh_plan(const FusedArgs& a, EhSched* s, int* blocks) {
+  if (a.pitch % 128 != 0 || a.has_mu || a.nplanes > 0 || a.nz < 3) return false;
+  const EhKernel k = eh_select(a);
+  once_per_device(k.fn, [&] {
+    cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_for(k.minb, k.smem));
+    cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(k.smem));
+  });
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kThreads, k.smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (per_sm <= 0 || sms <= 0) return false;
+  s->nbx = a.pitch / 128;
+  s->nby = (a.ny - 2 + kRowsA - 1) / kRowsA;
+  s->np = a.nz - 2;
+  const long long T = static_cast<long long>(s->nbx) * s->nby;
+  if (T * s->np >= (1LL << 31)) return false;
+  *blocks = per_sm * sms;
+  // H of plane k waits for E of plane k+1, (2 lag - 1) batches earlier: with
+  // lag >= blocks / T + 1 that is at least two rounds of the resident CTAs
+  s->lag = static_cast<int>(std::min<long long>(s->np, (*blocks + T - 1) / T + 1));
+  s->nitems = 2 * T * s->np;
+  return true;
+}
+
+int launch_staged_eh(const FusedArgs& a, const EhSched& s, int blocks, cudaStream_t st) {
+  const EhKernel k = eh_select(a);
+  FusedArgs args = a;
+  EhSched sched = s;
+  void* params[] = {&args, &sched};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(32, kRowsA, 1);
+  cfg.dynamicSmemBytes = k.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeCooperative;
+  attr.val.cooperative = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelExC(&cfg, k.fn, params);
   return 1;
 }
 

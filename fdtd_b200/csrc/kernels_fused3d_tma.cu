@@ -295,8 +295,9 @@ bool tma_prepare(const FusedArgs& a, TmaState** state) {
   else
     st.e.ids = st.e.E[0];
   if (!ok) return false;
-  static bool attr = false;
-  if (!attr) {
+  {
+    // the attributes belong to the current device's context: set on every
+    // preparation (a host call), so each device has them before its launches
     const int se = 128 + kStages * kStageE, sh = 128 + kStages * kStageH;
     ok = cudaFuncSetAttribute(tma_e_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, se) == cudaSuccess &&
          cudaFuncSetAttribute(tma_e_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, se) == cudaSuccess &&
@@ -305,7 +306,6 @@ bool tma_prepare(const FusedArgs& a, TmaState** state) {
          cudaFuncSetAttribute(tma_h_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh) == cudaSuccess &&
          cudaFuncSetAttribute(tma_h_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh) == cudaSuccess;
     if (!ok) return false;
-    attr = true;
   }
   st.ok = true;
   return true;

@@ -285,7 +285,7 @@ class Grid:
         _check(load_library().fdtd_profile_step(self.h, int(n), ctypes.c_void_p(stream) if stream else None, _dp(ms)))
         return dict(zip(["e_sweep", "e_extra", "h_sweep", "h_extra", "advance_flush"], ms.tolist()))
 
-    SWEEP_KINDS = {"auto": 0, "regs": 1, "tma": 2, "flat": 3, "staged": 4}
+    SWEEP_KINDS = {"auto": 0, "regs": 1, "tma": 2, "flat": 3, "staged": 4, "eh": 5}
 
     def set_sweep_kernel(self, kind: str) -> None:
         _check(load_library().fdtd_set_sweep_kernel(self.h, self.SWEEP_KINDS[kind]))

@@ -256,16 +256,23 @@ int fdtd_profile_step(fdtd_grid* g, int nsteps, void* stream, double* ms);
  * default: currently the staged sweeps, the fastest measured on B200), FDTD_SWEEP_REGS (z-marching, register prefetch),
  * FDTD_SWEEP_TMA (z-marching, TMA pipeline into shared memory; or
  * FDTD_ERR_UNSUPPORTED), FDTD_SWEEP_FLAT (one thread per 4-cell group and
- * plane) or FDTD_SWEEP_STAGED (flat, with every operand of a thread copied
- * into shared memory by cp.async at thread start). All compute the same
- * update. */
-enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3, FDTD_SWEEP_STAGED = 4 };
+ * plane), FDTD_SWEEP_STAGED (flat, with every operand of a thread copied
+ * into shared memory by cp.async at thread start) or FDTD_SWEEP_EH (the
+ * staged E and H updates of a whole step in one persistent launch, H tiles
+ * following the E tiles they read by a few planes so that E and H are read
+ * from HBM about once per step; grids without TFSF planes, box sources,
+ * boundary conditions or mu_r != 1, else FDTD_ERR_UNSUPPORTED at the step).
+ * All compute the same update, cell for cell. */
+enum { FDTD_SWEEP_AUTO = 0, FDTD_SWEEP_REGS = 1, FDTD_SWEEP_TMA = 2, FDTD_SWEEP_FLAT = 3, FDTD_SWEEP_STAGED = 4,
+       FDTD_SWEEP_EH = 5 };
 int fdtd_set_sweep_kernel(fdtd_grid* g, int kind);
 /* Replay a captured CUDA graph per 64 steps inside fdtd_step (default 1), or
  * launch every kernel from the host (0). Results are identical. */
 int fdtd_use_graphs(fdtd_grid* g, int enable);
 /* Device-side error flags accumulated by the kernels (0 = none; bit 0: a
- * bounded wait on a TMA stage expired and the sweep was abandoned). */
+ * bounded wait on a TMA stage expired and the sweep was abandoned; bit 1: in
+ * the one-launch step an H tile's bounded wait for the E tiles it reads
+ * expired, so that step's result is not valid). */
 int fdtd_error_flags(fdtd_grid* g, int* flags);
 /* Wait for all work on the handle's streams. */
 int fdtd_synchronize(fdtd_grid* g);
