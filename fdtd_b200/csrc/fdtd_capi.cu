@@ -72,10 +72,13 @@ double ref_sqrt(double x) {
 }
 double imp0() { return ref_sqrt(kMu0 / kEps0); }
 
-// PMLParameterModel(dx) (include/PML.hpp:368-393)
+// PMLParameterModel(dx) and PMLParameterModel(m, ma, sMax, kMax, aMax)
+// (include/PML.hpp:368-393)
 struct PmlModel {
   double m, ma, smax, kmax, amax;
   explicit PmlModel(double dx) : m(3), ma(1), smax(0.8 * (m + 1) / (imp0() * dx)), kmax(5), amax(0.05) {}
+  PmlModel(double m_, double ma_, double smax_, double kmax_, double amax_)
+      : m(m_), ma(ma_), smax(smax_), kmax(kmax_), amax(amax_) {}
   double K(double x) const { if (x < 0.0) return 1.0; return x > 1.0 ? 1.0 : 1.0 + pow(x, m) * (kmax - 1.0); }
   double S(double x) const { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(x, m) * smax; }
   double A(double x) const { if (x < 0.0) return 0.0; return x > 1.0 ? 0.0 : pow(1.0 - x, ma) * amax; }
@@ -102,8 +105,7 @@ struct Profile {  // one (field type, axis)
 };
 
 // grading loop of tests/testTM.cpp:44-71 for one side of one axis
-void grade(double dx, double dt, int n, int np, int side, Profile& e, Profile& h) {
-  PmlModel p(dx);
+void grade(const PmlModel& p, double dt, int n, int np, int side, Profile& e, Profile& h) {
   for (int i = 1; i < np + 2; i++) {
     double x = static_cast<double>(np - i + 1) / static_cast<double>(np);
     double xm = x - 0.5 / static_cast<double>(np);
@@ -163,6 +165,10 @@ struct fdtd_grid {
   long long launches = 0;
   long long t = 0;
   int pml[3][2]{};
+  // the grading of each CPML side: PMLParameterModel(dx) unless
+  // fdtd_set_pml_model gave the model's five parameters
+  bool pml_custom[3][2]{};
+  double pml_model[3][2][5]{};
   Profile prof[2][3];
   std::vector<fdtd_material> mats;
   // device state
@@ -866,23 +872,46 @@ int fdtd_grid_destroy(fdtd_grid* g) try {
   return host_failure();
 }
 
-int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) try {
+static int set_pml_side(fdtd_grid* g, int axis, int side, int ncells, const double* model) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (axis < 0 || axis >= dim_of(g) || side < 0 || side > 1) return fail(FDTD_ERR_INVALID, "bad axis or side");
   if (ncells < 1) return fail(FDTD_ERR_INVALID, "ncells must be >= 1");
+  if (model) {
+    for (int q = 0; q < 5; q++)
+      if (!std::isfinite(model[q])) return fail(FDTD_ERR_INVALID, "CPML model parameters must be finite");
+    if (model[3] < 1.0) return fail(FDTD_ERR_INVALID, "kappa_max must be >= 1 (kappa grows from 1 in the layer)");
+    if (model[2] < 0.0 || model[4] < 0.0) return fail(FDTD_ERR_INVALID, "sigma_max and alpha_max must be >= 0");
+  }
   const int other = g->pml[axis][1 - side];
   const int w = (ncells + 1) + (other > 0 ? other + 1 : 0);
   if (w > g->n[axis] - 2) return fail(FDTD_ERR_INVALID, "CPML slabs overlap: grid too small for the widths");
   CK(cudaSetDevice(g->d.device));
   g->pml[axis][side] = ncells;
+  g->pml_custom[axis][side] = model != nullptr;
+  for (int q = 0; q < 5; q++) g->pml_model[axis][side][q] = model ? model[q] : 0.0;
   // regrade the whole axis in side order (min first), as the user loop would
   for (int ft = 0; ft < 2; ft++) g->prof[ft][axis].reset(g->n[axis]);
-  for (int s = 0; s < 2; s++)
-    if (g->pml[axis][s] > 0)
-      grade(g->d.dx, g->d.dt, g->n[axis], g->pml[axis][s], s, g->prof[0][axis], g->prof[1][axis]);
+  for (int s = 0; s < 2; s++) {
+    if (g->pml[axis][s] <= 0) continue;
+    const double* pm = g->pml_model[axis][s];
+    const PmlModel p = g->pml_custom[axis][s] ? PmlModel(pm[0], pm[1], pm[2], pm[3], pm[4]) : PmlModel(g->d.dx);
+    grade(p, g->d.dt, g->n[axis], g->pml[axis][s], s, g->prof[0][axis], g->prof[1][axis]);
+  }
   g->dirty_pml = true;
   g->version++;
   return FDTD_OK;
+}
+
+int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells) try {
+  return set_pml_side(g, axis, side, ncells, nullptr);
+} catch (...) {
+  return host_failure();
+}
+
+int fdtd_set_pml_model(fdtd_grid* g, int axis, int side, int ncells, double m, double ma, double sigma_max,
+                       double kappa_max, double alpha_max) try {
+  const double model[5] = {m, ma, sigma_max, kappa_max, alpha_max};
+  return set_pml_side(g, axis, side, ncells, model);
 } catch (...) {
   return host_failure();
 }

@@ -30,7 +30,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
           -4: "FDTD_ERR_NOMEM", -5: "FDTD_ERR_NONFINITE", -6: "FDTD_ERR_TIMEOUT"}
 
 # every symbol include/fdtd_b200.h declares
-EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_materials", "fdtd_set_material_ids",
+EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_pml_model", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
@@ -74,6 +74,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_grid_create": [ctypes.POINTER(GridDesc), ctypes.POINTER(vp)],
         "fdtd_grid_destroy": [vp],
         "fdtd_set_pml": [vp, i, i, i],
+        "fdtd_set_pml_model": [vp, i, i, i] + [ctypes.c_double] * 5,
         "fdtd_set_materials": [vp, ctypes.POINTER(MaterialC), i],
         "fdtd_set_material_ids": [vp, vp],
         "fdtd_set_material_blocks": [vp, i, vp, i, i, i],
@@ -170,6 +171,12 @@ class Grid:
     def set_pml(self, axis: int, side: int, ncells: int) -> None:
         _check(load_library().fdtd_set_pml(self.h, axis, side, ncells))
 
+    def set_pml_model(self, axis: int, side: int, ncells: int, m: float, ma: float, sigma_max: float,
+                      kappa_max: float, alpha_max: float) -> None:
+        """CPML graded with PMLParameterModel(m, ma, sMax, kMax, aMax)."""
+        _check(load_library().fdtd_set_pml_model(self.h, axis, side, ncells, float(m), float(ma), float(sigma_max),
+                                                 float(kappa_max), float(alpha_max)))
+
     def set_materials(self, mats) -> None:
         arr = (MaterialC * len(mats))(*[material_struct(m) for m in mats])
         _check(load_library().fdtd_set_materials(self.h, arr, len(mats)))
@@ -232,7 +239,10 @@ class Grid:
     def from_problem(cls, p: P.Problem, precision="f64", device: int = 0) -> "Grid":
         g = cls(p.mode, p.shape, p.dx, p.dt, precision, device)
         for (a, s), n in sorted(p.pml.items()):
-            g.set_pml(a, s, n)
+            if (a, s) in p.pml_models:
+                g.set_pml_model(a, s, n, *p.pml_models[(a, s)])
+            else:
+                g.set_pml(a, s, n)
         for (a, s), kind in sorted(p.boundaries.items()):
             g.set_boundary(a, s, kind)
         if p.time_scheme != 1:

@@ -166,6 +166,9 @@ class Problem:
     dx: float
     dt: float
     pml: dict = field(default_factory=dict)  # {(axis, side): ncells}
+    # {(axis, side): (m, ma, sigma_max, kappa_max, alpha_max)}: sides graded
+    # with PMLParameterModel(m, ma, sMax, kMax, aMax) instead of (dx)
+    pml_models: dict = field(default_factory=dict)
     boundaries: dict = field(default_factory=dict)  # {(axis, side): kind in BOUNDARY_KINDS}
     # time policy of the curl updates and TFSF corrections: 1 BD1 (leapfrog),
     # 3 BD3, 4 BD4 (include/YeeUpdates.hpp:182-294)

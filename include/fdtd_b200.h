@@ -106,6 +106,14 @@ int fdtd_grid_destroy(fdtd_grid* g);
  * PMLParameterModel(dx) (m=3, m_a=1, sigma_max=0.8(m+1)/(imp0 dx), kappa_max=5,
  * alpha_max=0.05) and placed as in tests/testTM.cpp:44-71. */
 int fdtd_set_pml(fdtd_grid* g, int axis, int side, int ncells);
+/* The same CPML graded with the five-parameter PMLParameterModel(m, ma,
+ * sMax, kMax, aMax) (include/PML.hpp:376-377): kappa = 1 + x^m (kappa_max -
+ * 1), sigma = x^m sigma_max, alpha = (1 - x)^ma alpha_max at depth x into the
+ * layer, and the coefficients of NewPML::setPMLParameters (PML.hpp:84-102)
+ * from them, in FP64 on the host. fdtd_set_pml returns a side to the
+ * default model. kappa_max >= 1; sigma_max, alpha_max >= 0. */
+int fdtd_set_pml_model(fdtd_grid* g, int axis, int side, int ncells, double m, double ma, double sigma_max,
+                       double kappa_max, double alpha_max);
 
 /* Material table (n <= 65536 entries; per-cell ids address the first 256). */
 int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n);

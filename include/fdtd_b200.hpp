@@ -251,6 +251,8 @@ struct LorentzPoles {
 struct PMLParameterModel {
   double mM, mMa, msMax, mkMax, maMax;
   explicit PMLParameterModel(double dx) : mM(3), mMa(1), msMax(0.8 * (3 + 1) / (imp0 * dx)), mkMax(5), maMax(0.05) {}
+  PMLParameterModel(double m, double ma, double sMax, double kMax, double aMax)
+      : mM(m), mMa(ma), msMax(sMax), mkMax(kMax), maMax(aMax) {}
   double K(double x) const { return x < 0.0 ? 1.0 : (x > 1.0 ? 1.0 : 1.0 + std::pow(x, mM) * (mkMax - 1.0)); }
   double S(double x) const { return x < 0.0 ? 0.0 : (x > 1.0 ? 0.0 : std::pow(x, mM) * msMax); }
   double A(double x) const { return x < 0.0 ? 0.0 : (x > 1.0 ? 0.0 : std::pow(1.0 - x, mMa) * maMax); }
@@ -447,6 +449,13 @@ class Grid {
   void set_pml(Dir d, int n) {
     set_pml(d, Orientation::MIN, n);
     set_pml(d, Orientation::MAX, n);
+  }
+  // the same, graded with a PMLParameterModel of the caller's parameters
+  // (the loop of tests/testTM.cpp:44-71 with another model)
+  void set_pml(Dir d, Orientation o, int n, const PMLParameterModel& m) {
+    check(fdtd_set_pml_model(g_.get(), static_cast<int>(d), o == Orientation::MAX ? 1 : 0, n, m.mM, m.mMa, m.msMax,
+                             m.mkMax, m.maMax));
+    pml_axes_[static_cast<int>(d)] = true;
   }
 
   // A per-cell material map: ids index `mats` (the role of MaterialMap,

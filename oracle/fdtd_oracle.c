@@ -132,9 +132,10 @@ static void set_params(double K, double S, double A, double dt, double* B, doubl
   *G = (nu == 0) ? 0.0 : 1.0 / dt * (1.0 - *B) / nu;
 }
 
-/* grading loop of tests/testTM.cpp:44-71 for one side of one axis */
-static void grade(double dx, double dt, int n, int np, int side, double* B[2], double* C[2], double* F[2], double* G[2]) {
-  pml_model p = model_for(dx);
+/* grading loop of tests/testTM.cpp:44-71 for one side of one axis, with
+   the model of PMLParameterModel(dx) or PMLParameterModel(m, ma, sMax,
+   kMax, aMax) (include/PML.hpp:370-377) */
+static void grade(pml_model p, double dt, int n, int np, int side, double* B[2], double* C[2], double* F[2], double* G[2]) {
   for (int i = 1; i < np + 2; i++) {
     double x = (double)(np - i + 1) / (double)np;
     double xm = x - 0.5 / (double)np;
@@ -207,7 +208,7 @@ void oracle_destroy(oracle_grid* g) {
   free(g);
 }
 
-int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells) {
+static int set_pml_side(oracle_grid* g, int axis, int side, int ncells, pml_model p) {
   int dim = g->mode == THREED ? 3 : 2;
   if (axis < 0 || axis >= dim || side < 0 || side > 1 || ncells < 1) return -1;
   g->pml[axis][side] = ncells;
@@ -215,8 +216,19 @@ int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells) {
   double* C[2] = {g->cC[0][axis], g->cC[1][axis]};
   double* F[2] = {g->cF[0][axis], g->cF[1][axis]};
   double* G[2] = {g->cG[0][axis], g->cG[1][axis]};
-  grade(g->dx, g->dt, g->n[axis], ncells, side, B, C, F, G);
+  grade(p, g->dt, g->n[axis], ncells, side, B, C, F, G);
   return 0;
+}
+
+int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells) {
+  return set_pml_side(g, axis, side, ncells, model_for(g->dx));
+}
+
+int oracle_set_pml_model(oracle_grid* g, int axis, int side, int ncells, double m, double ma, double smax,
+                         double kmax, double amax) {
+  pml_model p;
+  p.m = m; p.ma = ma; p.smax = smax; p.kmax = kmax; p.amax = amax;
+  return set_pml_side(g, axis, side, ncells, p);
 }
 
 int oracle_pml_profile(const oracle_grid* g, int ft, int axis, double* out) {

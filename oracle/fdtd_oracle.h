@@ -36,6 +36,9 @@ void oracle_destroy(oracle_grid* g);
 /* CPML of `ncells` on one side (0 = min, 1 = max) of `axis`, graded with
  * PMLParameterModel(dx) (include/PML.hpp:368-393). */
 int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells);
+/* the same side graded with PMLParameterModel(m, ma, sMax, kMax, aMax) */
+int oracle_set_pml_model(oracle_grid* g, int axis, int side, int ncells, double m, double ma, double smax,
+                         double kmax, double amax);
 int oracle_set_materials(oracle_grid* g, const oracle_material* m, int n);
 int oracle_set_material_ids(oracle_grid* g, const uint8_t* ids);
 /* comp 0..2 = x,y,z; target 0 = E (after the constitutive update),

@@ -73,6 +73,7 @@ def lib():
         L.oracle_create.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 2
         L.oracle_destroy.argtypes = [vp]
         L.oracle_set_pml.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_set_pml_model.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 5
         L.oracle_set_materials.argtypes = [vp, ctypes.POINTER(OracleMaterial), ctypes.c_int]
         L.oracle_set_material_ids.argtypes = [vp, ctypes.c_void_p]
         L.oracle_add_source.argtypes = [vp] + [ctypes.c_int] * 5 + [dp, ctypes.c_int]
@@ -130,7 +131,10 @@ class OracleGrid:
         if not self.h:
             raise ValueError("oracle_create rejected the grid")
         for (a, s), n in sorted(p.pml.items()):
-            assert L.oracle_set_pml(self.h, a, s, n) == 0
+            if (a, s) in getattr(p, "pml_models", {}):
+                assert L.oracle_set_pml_model(self.h, a, s, n, *[float(v) for v in p.pml_models[(a, s)]]) == 0
+            else:
+                assert L.oracle_set_pml(self.h, a, s, n) == 0
         for (a, s), kind in sorted(p.boundaries.items()):
             assert L.oracle_set_boundary(self.h, a, s, BOUNDARY_KINDS[kind]) == 0
         if p.time_scheme != 1:
@@ -288,6 +292,8 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
         lines = [f"mode {p.mode}", f"dims {nx} {ny} {nz}", f"dxdt {p.dx!r} {p.dt!r}"]
         pm = [p.pml.get((a, s), 0) for a in range(3) for s in range(2)]
         lines.append("pml " + " ".join(str(x) for x in pm))
+        for (a, sd), mp in sorted(getattr(p, "pml_models", {}).items()):
+            lines.append(f"pmlmodel {a} {sd} " + " ".join(repr(float(v)) for v in mp))
         lines.append(f"nmat {len(p.materials)}")
         for m in p.materials:
             if len(m.poles) > 1:

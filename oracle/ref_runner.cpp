@@ -26,6 +26,8 @@
 //   dims nx ny nz
 //   dxdt dx dt
 //   pml nlo_x nhi_x nlo_y nhi_y nlo_z nhi_z
+//   pmlmodel axis side m ma sMax kMax aMax   (optional, per side: grade it with
+//                                 PMLParameterModel(m, ma, sMax, kMax, aMax))
 //   nmat M  then M lines: kind K delta freq gamma mu_r
 //        kind 0 vacuum, 1 constant, 2 drude, 3 lorentz
 //   matids <path|none>            uint8 per cell, index (k*ny+j)*nx+i
@@ -91,6 +93,9 @@ struct Scenario {
   int scheme = 1;
   double dx = 1, dt = 1;
   int pml[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  // per side: 0 = PMLParameterModel(dx), 1 = PMLParameterModel(m, ma, sMax, kMax, aMax)
+  int pml_custom[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  double pml_model[3][2][5] = {};
   std::vector<Mat> mats;
   std::vector<uint8_t> ids;
   std::vector<Src> srcs;
@@ -291,12 +296,15 @@ static int run(Scenario& s) {
         }
         interior.push_back(&c);
       }
-  // CPML profile, following tests/testTM.cpp:44-71 per axis and side
-  PMLParameterModel p(s.dx);
+  // CPML profile, following tests/testTM.cpp:44-71 per axis and side, with
+  // the reference's own PMLParameterModel constructors (include/PML.hpp:372-377)
   for (int a = 0; a < dim; a++) {
     for (int side = 0; side < 2; side++) {
       int np = s.pml[a][side];
       if (np <= 0) continue;
+      const double* pm = s.pml_model[a][side];
+      const PMLParameterModel p = s.pml_custom[a][side] ? PMLParameterModel(pm[0], pm[1], pm[2], pm[3], pm[4])
+                                                        : PMLParameterModel(s.dx);
       for (int i = 1; i < np + 2; i++) {
         double x = static_cast<double>(np - i + 1) / static_cast<double>(np);
         double xm = x - 0.5 / static_cast<double>(np);
@@ -511,6 +519,12 @@ int main(int argc, char** argv) {
     else if (key == "dims") in >> s.nx >> s.ny >> s.nz;
     else if (key == "dxdt") in >> s.dx >> s.dt;
     else if (key == "pml") for (int a = 0; a < 3; a++) in >> s.pml[a][0] >> s.pml[a][1];
+    else if (key == "pmlmodel") {
+      int a, sd;
+      in >> a >> sd;
+      s.pml_custom[a][sd] = 1;
+      for (int q = 0; q < 5; q++) in >> s.pml_model[a][sd][q];
+    }
     else if (key == "nmat") {
       int m; in >> m; s.mats.resize(m);
       for (auto& x : s.mats) in >> x.kind >> x.K >> x.delta >> x.freq >> x.gamma >> x.mu;

@@ -6,7 +6,9 @@
 //       CPML at x max, periodic faces in y; also writes the surface current
 //       Jh_x on the interior and the running DFT of Je_z on a box;
 //   td: 3D, FP32 fused, 24^3, 4-cell CPML, Drude cube in a material map,
-//       x-propagating TFSF box (6 planes) with an Aux1D Gaussian.
+//       x-propagating TFSF box (6 planes) with an Aux1D Gaussian;
+//   pm: the tm loop with the x-min and y-max CPML graded by
+//       PMLParameterModel(m, ma, sMax, kMax, aMax) of the caller's values.
 // Writes the listed fields (float64, x fastest) to out.bin.
 #include <cmath>
 #include <cstdio>
@@ -57,6 +59,30 @@ int main(int argc, char** argv) {
       } catch (const gpu::Error& e) {
         if (e.code != FDTD_ERR_UNSUPPORTED) return 4;
       }
+    } else if (!strcmp(argv[1], "pm")) {
+      const double dt = 0.99 / std::sqrt(2.0) * dx / c0;
+      const int steps = 80;
+      const double s0 = 0.8 * 4 / (imp0 * dx);
+      gpu::Grid<TM, double> grid(40, 36, 1, dx, dt, steps);
+      grid.set_pml(Dir::X, Orientation::MIN, 6, PMLParameterModel(4.0, 2.0, 1.3 * s0, 8.0, 0.1));
+      grid.set_pml(Dir::X, Orientation::MAX, 6);
+      grid.set_pml(Dir::Y, Orientation::MIN, 6);
+      grid.set_pml(Dir::Y, Orientation::MAX, 6, PMLParameterModel(3.5, 1.5, 2.0 * s0, 3.0, 0.2));
+      auto gauss = [dt](double t) { const double n = t / dt; return std::exp(-((n - 20.0) / 6.0) * ((n - 20.0) / 6.0)); };
+      auto src = grid.add(make_soft_source<Ez>(gauss, grid.cell(20, 18)));
+      grid.plan({YeeUpdate<TM, Dz>(dt, dx),
+                 UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx),
+                 UpdatePML<TM, FieldType::Electric, Dir::Y>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Electric>(),
+                 src,
+                 YeeUpdate<TM, Bx>(dt, dx), YeeUpdate<TM, By>(dt, dx),
+                 UpdatePML<TM, FieldType::Magnetic, Dir::X>(dt, dx),
+                 UpdatePML<TM, FieldType::Magnetic, Dir::Y>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Magnetic>()});
+      grid.step(steps);
+      dump(out, grid.get<Ez>());
+      dump(out, grid.get<Hx>());
+      dump(out, grid.get<Hy>());
     } else if (!strcmp(argv[1], "bd")) {
       const double dt = 0.5 / std::sqrt(2.0) * dx / c0;
       const int steps = 90;

@@ -5,7 +5,9 @@ oracle/_ref/ref_runner -- the reference's own update functors compiled from
 its headers (oracle/Makefile) -- and the final fields are stored as
 <name>.npz. Run from the repository root, where the reference tree exists:
 
-    make -C oracle REF=$FDTD_REFERENCE_DIR ref && python tests/golden/make_golden.py
+    make -C oracle REF=$FDTD_REFERENCE_DIR ref && python tests/golden/make_golden.py [scenario ...]
+
+(with scenario names, only those scenarios' fixtures are rewritten)
 
 It also writes config_*.xml: the reference's own XML writers (print_summary
 of MaterialMap, PMLOptions, BoundaryOptions) run on config_spec.txt by
@@ -47,10 +49,14 @@ def write_config_fixtures(out_dir):
         print("config", name)
 
 
-def main():
+def main(names=None):
+    """All fixtures, or (names given) only those scenarios' .npz files."""
     out_dir = os.path.dirname(os.path.abspath(__file__))
-    write_config_fixtures(out_dir)
+    if not names:
+        write_config_fixtures(out_dir)
     for make in scenarios.REFERENCE_SCENARIOS:
+        if names and make.__name__ not in names:
+            continue
         p = make()
         ref = pyoracle.run_reference(p)
         arrays = {k: ref[k] for k in KEEP + pyoracle.PSI_NAMES + pyoracle.SURFACE_NAMES if np.any(ref[k] != 0)}
@@ -59,4 +65,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

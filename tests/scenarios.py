@@ -7,8 +7,9 @@ import math
 
 import numpy as np
 
-from fdtd_b200.problem import (CONSTANT, DRUDE, TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion, courant_dt,
-                               gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, sinusoid, tfsf_box_planes)
+from fdtd_b200.problem import (CONSTANT, DRUDE, IMP0, TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion,
+                               courant_dt, gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, sinusoid,
+                               tfsf_box_planes)
 
 DX = 1e-6
 DT2 = courant_dt(DX, 0.99 / math.sqrt(2.0))
@@ -373,11 +374,36 @@ def objective_problem(p, spec):
     return q
 
 
+def tm_cpml_model() -> Problem:
+    """TM with CPML sides graded by their own PMLParameterModel(m, ma, sMax,
+    kMax, aMax) (include/PML.hpp:376-377): a steeper, stronger layer, a
+    kappa-free quadratic one, a third shape, and one default side."""
+    p = tm_cpml_sources()
+    p.name = "tm_cpml_model"
+    s0 = 0.8 * 4 / (IMP0 * DX)
+    p.pml_models[(0, 0)] = (4.0, 2.0, 1.3 * s0, 8.0, 0.1)
+    p.pml_models[(0, 1)] = (2.0, 1.0, 0.6 * s0, 1.0, 0.0)
+    p.pml_models[(1, 1)] = (3.5, 1.5, 2.0 * s0, 3.0, 0.2)
+    return p
+
+
+def td_cpml_model() -> Problem:
+    """3D dispersive cells with the z and x-max CPML sides graded by
+    PMLParameterModel(m, ma, sMax, kMax, aMax)."""
+    p = td_drude_lorentz()
+    p.name = "td_cpml_model"
+    s0 = 0.8 * 4 / (IMP0 * DX)
+    p.pml_models[(2, 0)] = (2.5, 1.0, 1.5 * s0, 6.0, 0.08)
+    p.pml_models[(2, 1)] = (4.0, 3.0, 0.9 * s0, 2.0, 0.01)
+    p.pml_models[(0, 1)] = (3.0, 2.0, 1.1 * s0, 11.0, 0.15)
+    return p
+
+
 # scenarios the reference itself can run (one pole per cell)
 REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_reference_polarisation,
                        te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources,
                        tm_boundaries, te_boundaries, td_boundaries, tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf,
-                       td_bd4_boundaries, tm_magnetic_tfsf, td_magnetic_tfsf]
+                       td_bd4_boundaries, tm_magnetic_tfsf, td_magnetic_tfsf, tm_cpml_model, td_cpml_model]
 # scenarios on the BD3/BD4 time policies (FP64 plain method only)
 MULTISTEP_SCENARIOS = [tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf, td_bd4_boundaries]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks, td_surface_dft]

@@ -45,6 +45,28 @@ def test_tm_plain_through_templates(drop_in, oracle, tmp_path):
         assert rel_l2(got[q], o.get(name)) <= 1e-12, name
 
 
+def test_tm_custom_cpml_model_through_templates(drop_in, oracle, tmp_path):
+    """grid.set_pml(d, o, n, PMLParameterModel(m, ma, sMax, kMax, aMax)):
+    the user's grading reaches the GPU profiles (FP64 <= 1e-12)."""
+    from fdtd_b200.problem import IMP0, TM, Problem, Source, courant_dt
+    p = Problem(TM, (40, 36, 1), 1e-6, courant_dt(1e-6, 0.99 / math.sqrt(2.0)))
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    s0 = 0.8 * 4 / (IMP0 * 1e-6)
+    p.pml_models[(0, 0)] = (4.0, 2.0, 1.3 * s0, 8.0, 0.1)
+    p.pml_models[(1, 1)] = (3.5, 1.5, 2.0 * s0, 3.0, 0.2)
+    n = np.arange(80, dtype=np.float64)
+    p.sources.append(Source(2, (20, 18, 0), np.exp(-(((n - 20.0) / 6.0) ** 2)), "E"))
+    o = oracle.run_oracle(p, 80)
+    got = run(drop_in, "pm", tmp_path, 3, (1, 36, 40))
+    for q, name in enumerate(["Ez", "Hx", "Hy"]):
+        assert rel_l2(got[q], o.get(name)) <= 1e-12, name
+    # and the grading is not the default one
+    p.pml_models = {}
+    assert rel_l2(got[0], oracle.run_oracle(p, 80).get("Ez")) > 1e-9
+
+
 def test_3d_fused_material_map_tfsf_through_templates(drop_in, oracle, tmp_path):
     p = scenarios.td_tfsf_box()
     o = oracle.run_oracle(p)
