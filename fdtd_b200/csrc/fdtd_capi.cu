@@ -366,7 +366,7 @@ bool eh_wanted(const fdtd_grid* g) {
 
 int ensure_eh(fdtd_grid* g) {
   if (!eh_wanted(g) || g->d_eh) return FDTD_OK;
-  const long long nbx = g->pitch / 128, nby = (g->n[1] - 2 + 3) / 4, np = g->n[2] - 2;
+  const long long nbx = g->pitch / 128, nby = (g->n[1] - 2 + 7) / 8, np = g->n[2] - 2;  // tiles of 128 x 8
   if (nbx <= 0 || nby <= 0 || np <= 0) return FDTD_OK;
   g->eh_words = 1 + nbx * nby * np;
   return dalloc(g, reinterpret_cast<void**>(&g->d_eh), static_cast<size_t>(g->eh_words) * sizeof(unsigned));

@@ -60,8 +60,14 @@ __device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx&
 // PJ: every material of the grid is dispersive, so the group's J (and P)
 // are staged with the fields and all of the thread's loads are in flight at
 // once (they are otherwise read per component, after the fields arrive)
-template <int MAXP, bool PJ>
-__device__ __forceinline__ void e_tile(const FusedArgs& a, int bx, int by, int k, float4* sm) {
+struct NoHook {
+  __device__ void operator()() const {}
+};
+
+// hook() runs after every copy of the tile has been requested, before the
+// wait for them (the one-launch kernel does its bookkeeping there).
+template <int MAXP, bool PJ, class Hook = NoHook>
+__device__ __forceinline__ void e_tile(const FusedArgs& a, int bx, int by, int k, float4* sm, Hook hook = Hook()) {
   constexpr int kPJ = PJ ? pj_slots<MAXP>() : 0;
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
   const int x4 = bx * 128 + lane * 4;
@@ -101,6 +107,7 @@ __device__ __forceinline__ void e_tile(const FusedArgs& a, int bx, int by, int k
   // slots 10 and 11 hold this thread's 8 x-slab floats
   float* px = reinterpret_cast<float*>(sm + 10 * kThreads) + 8 * tid;
   if (g.row_ok) stage_x_slab(a, g, 0, k, px);
+  hook();
   cp_async_wait_all();
   const float4 hy = s[3 * kThreads], hz = s[4 * kThreads];
   const float hy_sh = __shfl_up_sync(kFull, hy.w, 1);
@@ -120,10 +127,8 @@ __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_c
   e_tile<MAXP, PJ>(a, blockIdx.x, blockIdx.y, 1 + blockIdx.z, sm);
 }
 
-// The H update of one tile (as e_tile). CG: the E values of the x+1
-// neighbour tile are read through L2 only (ld.global.cg), for a kernel in
-// which another CTA wrote them earlier in the same launch.
-template <bool MU, bool CG>
+// The H update of one tile (as e_tile).
+template <bool MU>
 __device__ __forceinline__ void h_tile(const FusedArgs& a, int bx, int by, int k, float4* sm) {
   const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
   const int x4 = bx * 128 + lane * 4;
@@ -144,13 +149,8 @@ __device__ __forceinline__ void h_tile(const FusedArgs& a, int bx, int by, int k
   cp_async16(s + 9 * kThreads, a.H[2] + c);
   float ey_xp3 = 0.f, ez_xp3 = 0.f;
   if (lane == 31) {
-    if (CG) {
-      ey_xp3 = __ldcg(a.E[1] + c + 4);
-      ez_xp3 = __ldcg(a.E[2] + c + 4);
-    } else {
-      ey_xp3 = a.E[1][c + 4];
-      ez_xp3 = a.E[2][c + 4];
-    }
+    ey_xp3 = a.E[1][c + 4];
+    ez_xp3 = a.E[2][c + 4];
   }
   const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
   float* px = reinterpret_cast<float*>(sm + 10 * kThreads) + 8 * tid;
@@ -171,7 +171,7 @@ template <int MINB, bool MU>
 __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
   // planes from the top down, as the flat H sweep
-  h_tile<MU, false>(a, blockIdx.x, blockIdx.y, a.nz - 2 - blockIdx.z, sm);
+  h_tile<MU>(a, blockIdx.x, blockIdx.y, a.nz - 2 - blockIdx.z, sm);
 }
 
 // The shared-memory carveout (percent of the largest) that holds `ctas` CTAs
@@ -246,104 +246,263 @@ int launch_staged_h(const FusedArgs& a, cudaStream_t s) {
 //
 // The two sweeps read each E and H word twice per step: the E sweep reads H
 // and E, the H sweep E and H again. Here one persistent launch runs both, in
-// an order that keeps what the H tiles read in L2: work items are tiles of one
-// plane of one sweep, taken round-robin by the resident CTAs in the order
+// an order that keeps what the H items read in L2: work items are tiles of
+// one plane (128 cells x 8 rows) of one sweep, taken round-robin by the
+// resident CTAs in the order
 //   E(1) .. E(lag),  E(lag+1) H(1),  E(lag+2) H(2),  ..,  E(np) H(np-lag),
 //   H(np-lag+1) .. H(np)
 // (each a batch of every tile of the plane), so H of plane k runs about lag
-// planes after E of plane k has stored the E it reads, and the E and H of the
-// planes in between are still in L2.
+// planes after E of plane k has stored the E it reads, and the E and H of
+// the planes in between are still in L2. An E item updates its two 4-row
+// halves one after the other (the E update stages 24 operands per group,
+// which is what the shared memory holds); an H item stages both halves at
+// once (12 operands per group each), so the H updates keep as many copies in
+// flight per SM as the standalone H sweep does with twice the CTAs.
 //
 // Dependences. E of tile t at plane k reads H at planes k and k-1 of t, and
 // at plane k of t's x-1 and y-1 neighbours; H of tile t at plane k reads E at
 // planes k and k+1 of t and at plane k of the x+1 and y+1 neighbours, and
 // overwrites the H that the E tiles at (k, t), (k, t+x), (k, t+y) and
 // (k+1, t) read. So H(k, t) runs once those four E tiles are done: each E
-// tile publishes its epoch in flags[k][t] (release, after a CTA barrier), and
-// the first thread of an H tile acquires the flags of the four before the
-// CTA reads anything. Every dependence points to an earlier item, and every
-// CTA is resident (cooperative launch), so the earliest unfinished item can
-// always run: no cycle of waits. Each wait is bounded; on expiry the kernel
-// sets bit 1 of the grid's error flags and goes on (the step's result is
-// then wrong, but the launch ends). E values that another CTA wrote in this
+// tile publishes the launch's epoch in flags[k][t], and an H tile starts
+// reading E only once its four flags hold it. Every dependence points to an
+// earlier item, and every CTA is resident (cooperative launch), so the
+// earliest unfinished item can always run: no cycle of waits. Each wait is
+// bounded; on expiry the kernel sets bit 1 of the grid's error flags and
+// stops waiting for the rest of the launch (the step's result is then
+// wrong, but the launch ends). E values that another CTA wrote in this
 // launch are read through L2 only (cp.async.cg, ld.global.cg).
+//
+// The bookkeeping is the CTA's first thread's, off the copies' path:
+// * an E tile's flag is stored (release: fence, then a relaxed store) during
+//   the CTA's next item, once that item's copies are in flight, so the
+//   fence's wait for the E tile's stores overlaps the next loads; it is
+//   always published before the CTA waits for anything, and at the end, so
+//   no CTA waits while holding an unpublished flag;
+// * when the CTA's next item is an H tile, its four flags are read (relaxed
+//   loads, then the fence: an acquire) during the current item; if all hold
+//   the epoch, that H tile starts its E copies without a wait (flags only
+//   move forward). The outcome reaches the CTA through shared memory and
+//   the barrier that ends every item.
 //
 // The epoch is read from device memory at launch and advanced by the step
 // counter's kernel after it, never reset, so flags of an earlier launch
 // never satisfy a later one.
 namespace {
 
-constexpr int kDepPolls = 1 << 18;  // a few tenths of a second with the back-off below
+constexpr int kRowsEH = 2 * kRowsA;  // rows of an item's tile: two 4-row halves
+constexpr int kDepPolls = 1 << 18;   // a few tenths of a second with the back-off below
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// waits (bounded) until *p has reached `target`; false if it gave up, or
-// if another wait of the launch gave up before (bit 1 of *err): after the
-// first expiry no tile waits any more, so the launch ends soon whatever the
-// cause
-__device__ __forceinline__ bool wait_epoch(const unsigned* p, unsigned target, const int* err) {
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+__device__ __forceinline__ bool reached(unsigned v, unsigned target) { return static_cast<int>(v - target) >= 0; }
+
+// Waits (bounded) until the flags f[0], f[o1], f[o2], f[o3] have all
+// reached `target` (an offset of 0 stands for a dependence the tile does not
+// have), reading the four together with relaxed loads; the fence after the
+// last poll makes the wait an acquire. false if it gave up, or if another
+// wait of the launch gave up before (bit 1 of *err).
+__device__ __forceinline__ bool wait_epochs(const unsigned* f, long long o1, long long o2, long long o3,
+                                            unsigned target, const int* err) {
+  bool ok = false;
   for (int it = 0; it < kDepPolls; it++) {
-    if (static_cast<int>(ld_acquire_u32(p) - target) >= 0) return true;
-    if ((it & 63) == 63 && (*reinterpret_cast<const volatile int*>(err) & 2)) return false;
+    const unsigned v0 = ld_relaxed_u32(f), v1 = ld_relaxed_u32(f + o1), v2 = ld_relaxed_u32(f + o2),
+                   v3 = ld_relaxed_u32(f + o3);
+    ok = reached(v0, target) && reached(v1, target) && reached(v2, target) && reached(v3, target);
+    if (ok) break;
+    if ((it & 63) == 63 && (*reinterpret_cast<const volatile int*>(err) & 2)) break;
     __nanosleep(it < 32 ? 32 : 256);
   }
-  return false;
+  fence_acq_rel_gpu();
+  return ok;
+}
+
+// item -> (E or H, plane k, tile) in the schedule's order
+struct EhItem {
+  bool e;
+  int k, tile;
+};
+
+__device__ __forceinline__ EhItem eh_decode(const EhSched& s, int T, long long it) {
+  const int L = s.lag, NP = s.np;
+  const int b = static_cast<int>(it / T);
+  EhItem r;
+  r.tile = static_cast<int>(it - static_cast<long long>(b) * T);
+  if (b < L) {
+    r.e = true;
+    r.k = 1 + b;
+  } else if (b < 2 * NP - L) {
+    const int m = b - L;
+    r.e = (m & 1) == 0;
+    r.k = r.e ? L + 1 + (m >> 1) : 1 + (m >> 1);
+  } else {
+    r.e = false;
+    r.k = NP - L + 1 + (b - (2 * NP - L));
+  }
+  return r;
+}
+
+// offsets (from an H tile's own flag) of the E tiles it reads: x+1, y+1 and
+// the plane above; 0 where the tile has no such neighbour
+__device__ __forceinline__ void eh_deps(const EhSched& s, int T, const EhItem& q, long long& ox, long long& oy,
+                                        long long& oz) {
+  const int bx = q.tile % s.nbx, by = q.tile / s.nbx;
+  ox = bx + 1 < s.nbx ? 1 : 0;
+  oy = by + 1 < s.nby ? s.nbx : 0;
+  oz = q.k < s.np ? T : 0;
 }
 
 }  // namespace
+
+// The H update of both 4-row halves of an 8-row tile at once: half h stages
+// its 12 operands per group in slots 12 h .. 12 h + 11. The tile's own H and
+// CPML integrators are requested first, then dep() (the wait for the E tiles
+// it reads, when one is needed), then E; hook() runs once every copy is in
+// flight.
+template <class Dep, class Hook>
+__device__ __forceinline__ void h_pair(const FusedArgs& a, int bx, int by8, int k, float4* sm, Dep dep, Hook hook) {
+  const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
+  const int x4 = bx * 128 + lane * 4;
+  const long long sy = a.pitch, sz = static_cast<long long>(a.pitch) * a.ny;
+  long long c[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int j = 1 + (2 * by8 + h) * kRowsA + threadIdx.y;
+    c[h] = k * sz + min(j, a.ny - 2) * sy + x4;
+    float4* s = sm + tid + h * 12 * kThreads;
+    cp_async16(s + 7 * kThreads, a.H[0] + c[h]);
+    cp_async16(s + 8 * kThreads, a.H[1] + c[h]);
+    cp_async16(s + 9 * kThreads, a.H[2] + c[h]);
+    const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
+    if (g.row_ok) stage_x_slab(a, g, 1, k, reinterpret_cast<float*>(sm + (h * 12 + 10) * kThreads) + 8 * tid);
+  }
+  dep();
+  float ey_xp3[2] = {0.f, 0.f}, ez_xp3[2] = {0.f, 0.f};
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    float4* s = sm + tid + h * 12 * kThreads;
+    cp_async16(s + 0 * kThreads, a.E[0] + c[h] + sz);
+    cp_async16(s + 1 * kThreads, a.E[1] + c[h] + sz);
+    cp_async16(s + 2 * kThreads, a.E[0] + c[h]);
+    cp_async16(s + 3 * kThreads, a.E[1] + c[h]);
+    cp_async16(s + 4 * kThreads, a.E[2] + c[h]);
+    cp_async16(s + 5 * kThreads, a.E[0] + c[h] + sy);
+    cp_async16(s + 6 * kThreads, a.E[2] + c[h] + sy);
+    if (lane == 31) {
+      ey_xp3[h] = __ldcg(a.E[1] + c[h] + 4);
+      ez_xp3[h] = __ldcg(a.E[2] + c[h] + 4);
+    }
+  }
+  hook();
+  cp_async_wait_all();
+  // one copy of the update's code for both halves (the kernel's code is
+  // large enough that instruction fetch stalls it)
+#pragma unroll 1
+  for (int h = 0; h < 2; h++) {
+    const int j = 1 + (2 * by8 + h) * kRowsA + threadIdx.y;
+    const float4* s = sm + tid + h * 12 * kThreads;
+    const GroupCtx g = make_ctx(a, 1, x4, j, lane, k, k + 1);
+    const float4 ey = s[3 * kThreads], ez = s[4 * kThreads];
+    const float ey_sh = __shfl_down_sync(kFull, ey.x, 1);
+    const float ez_sh = __shfl_down_sync(kFull, ez.x, 1);
+    h_group_update<false>(a, g, k, s[2 * kThreads], ey, ez, s[5 * kThreads], s[6 * kThreads], s[0], s[1 * kThreads],
+                          lane != 31 ? ey_sh : ey_xp3[h], lane != 31 ? ez_sh : ez_xp3[h], s[7 * kThreads],
+                          s[8 * kThreads], s[9 * kThreads],
+                          reinterpret_cast<const float*>(sm + (h * 12 + 10) * kThreads) + 8 * tid);
+  }
+}
 
 template <int MAXP, int MINB, bool PJ>
 __global__ void __launch_bounds__(kThreads, MINB)
     staged_eh_kernel(const __grid_constant__ FusedArgs a, const __grid_constant__ EhSched s) {
   extern __shared__ float4 sm[];
+  __shared__ int s_ready[2];  // by item parity: the item's E dependences were seen reached
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
   const unsigned target = *s.epoch + 1u;
-  const int T = s.nbx * s.nby, L = s.lag, NP = s.np;
-  for (long long it = blockIdx.x; it < s.nitems; it += gridDim.x) {
-    const int b = static_cast<int>(it / T);
-    const int tile = static_cast<int>(it - static_cast<long long>(b) * T);
-    bool e_phase;
-    int k;
-    if (b < L) {
-      e_phase = true;
-      k = 1 + b;
-    } else if (b < 2 * NP - L) {
-      const int m = b - L;
-      e_phase = (m & 1) == 0;
-      k = e_phase ? L + 1 + (m >> 1) : 1 + (m >> 1);
-    } else {
-      e_phase = false;
-      k = NP - L + 1 + (b - (2 * NP - L));
-    }
-    const int bx = tile % s.nbx, by = tile / s.nbx;
-    unsigned* f = s.flags + static_cast<long long>(k - 1) * T + tile;
-    if (e_phase) {
-      e_tile<MAXP, PJ>(a, bx, by, k, sm);
-      __syncthreads();
-      if (lead) {
-        __threadfence();
-        st_release_u32(f, target);
+  const int T = s.nbx * s.nby;
+  const int halves4 = (a.ny - 2 + kRowsA - 1) / kRowsA;  // 4-row halves with rows to update
+  if (lead) s_ready[0] = 0;
+  __syncthreads();
+  unsigned* pending = nullptr;  // lead: the E flag still to be published
+  int par = 0;
+  for (long long it = blockIdx.x; it < s.nitems; it += gridDim.x, par ^= 1) {
+    const EhItem q = eh_decode(s, T, it);
+    const int bx = q.tile % s.nbx, by8 = q.tile / s.nbx;
+    unsigned* f = s.flags + static_cast<long long>(q.k - 1) * T + q.tile;
+    const bool ready = s_ready[par] != 0;
+    auto publish = [&] {
+      if (pending) {
+        fence_acq_rel_gpu();
+        st_relaxed_u32(pending, target);
+        pending = nullptr;
       }
-    } else {
-      if (lead) {
-        const int* err = &a.ctrl->error;
-        bool ok = wait_epoch(f, target, err);
-        if (ok && bx + 1 < s.nbx) ok = wait_epoch(f + 1, target, err);
-        if (ok && by + 1 < s.nby) ok = wait_epoch(f + s.nbx, target, err);
-        if (ok && k < NP) ok = wait_epoch(f + T, target, err);
-        if (!ok) atomicOr(&a.ctrl->error, 2);
+    };
+    // once every copy of the item is in flight: publish, and look at the
+    // next item's dependences
+    auto hook = [&] {
+      if (!lead) return;
+      bool next = false;
+      const long long nx = it + gridDim.x;
+      if (nx < s.nitems) {
+        const EhItem n = eh_decode(s, T, nx);
+        if (!n.e) {
+          long long ox, oy, oz;
+          eh_deps(s, T, n, ox, oy, oz);
+          const unsigned* g = s.flags + static_cast<long long>(n.k - 1) * T + n.tile;
+          const unsigned v0 = ld_relaxed_u32(g), v1 = ld_relaxed_u32(g + ox), v2 = ld_relaxed_u32(g + oy),
+                         v3 = ld_relaxed_u32(g + oz);
+          next = reached(v0, target) && reached(v1, target) && reached(v2, target) && reached(v3, target);
+        }
       }
+      // one fence: the acquire of those loads and the release of the flag
+      fence_acq_rel_gpu();
+      if (pending) {
+        st_relaxed_u32(pending, target);
+        pending = nullptr;
+      }
+      s_ready[par ^ 1] = next ? 1 : 0;
+    };
+    if (q.e) {
+      // the two halves in turn, through one copy of the E update's code; the
+      // bookkeeping runs with the first half's copies in flight
+      const int nh = 2 * by8 + 1 < halves4 ? 2 : 1;
+#pragma unroll 1
+      for (int h = 0; h < nh; h++) {
+        auto hook_h = [&] {
+          if (h == 0) hook();
+        };
+        e_tile<MAXP, PJ>(a, bx, 2 * by8 + h, q.k, sm, hook_h);
+      }
+      __syncthreads();  // every thread's stores are issued before the flag is published
+      if (lead) pending = f;
+    } else {
+      auto dep = [&] {
+        if (ready) return;
+        if (lead) {
+          publish();
+          long long ox, oy, oz;
+          eh_deps(s, T, q, ox, oy, oz);
+          if (!wait_epochs(f, ox, oy, oz, target, &a.ctrl->error)) atomicOr(&a.ctrl->error, 2);
+        }
+        __syncthreads();
+      };
+      h_pair(a, bx, by8, q.k, sm, dep, hook);
       __syncthreads();
-      h_tile<false, true>(a, bx, by, k, sm);
     }
+  }
+  if (lead && pending) {
+    fence_acq_rel_gpu();
+    st_relaxed_u32(pending, target);
   }
 }
 
@@ -356,12 +515,16 @@ struct EhKernel {
   int minb;
 };
 
+// shared memory: the larger of an E item's slots (with its material ids) and
+// an H item's two halves of 12 slots; 4 CTAs per SM at 49-50 KB each
 template <int MAXP, bool PJ>
 EhKernel eh_kernel() {
   constexpr int slots = kSlotsE + (PJ ? pj_slots<MAXP>() : 0);
-  constexpr int minb = !PJ ? (MAXP >= 2 ? 6 : 7) : (MAXP >= 2 ? 4 : (MAXP == 1 ? 6 : 7));
-  return {reinterpret_cast<const void*>(staged_eh_kernel<MAXP, minb, PJ>),
-          slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned), minb};
+  constexpr size_t e_bytes = slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned);
+  constexpr size_t h_bytes = 2 * kSlotsH * kThreads * sizeof(float4);
+  constexpr int minb = 4;
+  return {reinterpret_cast<const void*>(staged_eh_kernel<MAXP, minb, PJ>), e_bytes > h_bytes ? e_bytes : h_bytes,
+          minb};
 }
 
 EhKernel eh_select(const FusedArgs& a) {
@@ -392,7 +555,7 @@ bool staged_eh_plan(const FusedArgs& a, EhSched* s, int* blocks) {
   }
   if (per_sm <= 0 || sms <= 0) return false;
   s->nbx = a.pitch / 128;
-  s->nby = (a.ny - 2 + kRowsA - 1) / kRowsA;
+  s->nby = (a.ny - 2 + kRowsEH - 1) / kRowsEH;
   s->np = a.nz - 2;
   const long long T = static_cast<long long>(s->nbx) * s->nby;
   if (T * s->np >= (1LL << 31)) return false;

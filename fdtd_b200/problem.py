@@ -302,8 +302,8 @@ def config1(n: int = 256, steps: int = 2000, npml: int = 16) -> Problem:
 def config2(n: int = 384, steps: int = 1000, npml: int = 12, radius: Optional[int] = None,
             tfsf_inset: Optional[int] = None, dft_inset: Optional[int] = None, nfreq: int = 8,
             shape: Optional[Tuple[int, int, int]] = None) -> Problem:
-    """3D, 12-cell CPML, Drude sphere (eps_inf 1, wp*dt 0.3, gamma*dt 0.01) of
-    radius 64 at the centre, TFSF box inset 24 with an x-propagating
+    """3D, 12-cell CPML, Courant 0.98/sqrt(3), Drude sphere (eps_inf 1, wp*dt
+    0.3, gamma*dt 0.01) of radius 64 at the centre, TFSF box inset 24 with an x-propagating
     z-polarised Gaussian plane wave, DFT at 8 frequencies of the 4 tangential
     components on the 6 faces of the box inset 20. Smaller n scales radius
     and insets by n/384. `shape` (nx, ny, nz) replaces the cube n^3; the
@@ -315,7 +315,11 @@ def config2(n: int = 384, steps: int = 1000, npml: int = 12, radius: Optional[in
     tfsf_inset = tfsf_inset if tfsf_inset is not None else max(npml + 3, int(round(24 * scale)))
     dft_inset = dft_inset if dft_inset is not None else max(npml + 2, tfsf_inset - max(1, int(round(4 * scale))))
     dx = 1e-6
-    dt = courant_dt(dx, 0.99 / math.sqrt(3.0))
+    # Courant 0.98/sqrt(3): the reference's Drude update (DispersiveMaterials.hpp
+    # :979-998) with wp*dt = 0.3 is stable only while 4 S^2 + (wp dt)^2 <= 4,
+    # S = c dt sqrt(3)/dx, i.e. S <= 0.9887; at 0.99 the highest Yee mode in
+    # the sphere grows by ~1.1 per step (tests/test_stability_cpu.py)
+    dt = courant_dt(dx, 0.98 / math.sqrt(3.0))
     name = f"3d{n}_drude_sphere_tfsf_dft" if shape == (n, n, n) else \
         f"3d{shape[0]}x{shape[1]}x{shape[2]}_drude_sphere_tfsf_dft"
     p = Problem(THREED, shape, dx, dt, name=name)
