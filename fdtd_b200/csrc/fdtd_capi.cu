@@ -704,6 +704,9 @@ PlainArgs plain_args(fdtd_grid* g) {
   a.mats = static_cast<const MatF64*>(g->d_mats);
   a.eps_map = static_cast<const double*>(g->d_eps_map);
   a.dispersive = g->max_poles;
+  a.all_dispersive = g->mats.empty() ? 0 : 1;
+  for (auto& m : g->mats)
+    if (m.kind != FDTD_DRUDE && m.kind != FDTD_LORENTZ) a.all_dispersive = 0;
   // TimePolicy constants (include/YeeUpdates.hpp:184-186, :205-215, :254-265),
   // folded by the host compiler as the reference's constexpr divisions are
   a.cc = 1.0;

@@ -138,7 +138,8 @@ struct PlainArgs {
   int bshift, nbx, nby;
   const MatF64* mats;
   const double* eps_map;  // per-cell relative permittivity of non-dispersive cells (> 0), or null
-  int dispersive;
+  int dispersive;      // most poles of any material (Drude: 1)
+  int all_dispersive;  // every material has poles: P and J are read with the fields
   int nsrc;
   SourceDev src[kMaxSources];
   int nplanes;

@@ -48,14 +48,24 @@ def batch_subset():
 
 
 def oracle_job(job):
-    """(problem name, field names) -> ({name: array}, [spectra], seconds) of
-    the CPU oracle after the problem's steps (runs in a worker process)."""
+    """(problem name, field names) -> ({name: array}, [spectra], seconds,
+    {name: largest L2 norm over the run}) of the CPU oracle after the
+    problem's steps; the norms are sampled every 50 steps (runs in a worker
+    process)."""
     import time
     import pyoracle
     name, names = job
     p = long_problem(name)
     t0 = time.perf_counter()
-    o = pyoracle.run_oracle(p)
+    o = pyoracle.OracleGrid(p)
+    peak = {n: 0.0 for n in names}
+    done = 0
+    while done < p.steps:
+        n_ = min(50, p.steps - done)
+        o.step(n_)
+        done += n_
+        for n in names:
+            peak[n] = max(peak[n], float(np.linalg.norm(o.get(n))))
     fields = {n: o.get(n) for n in names}
     dfts = [o.dft(q) for q in range(len(p.dfts))]
-    return fields, dfts, time.perf_counter() - t0
+    return fields, dfts, time.perf_counter() - t0, peak
