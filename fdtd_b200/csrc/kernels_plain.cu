@@ -73,104 +73,74 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// shared-memory slots (one double per thread each) of the plain kernels:
-// E half: H at the cell and its curl neighbours, D, the CPML integrators,
-// and P, J of NP poles; H half: E and its neighbours, B, the integrators
-__host__ __device__ constexpr int plain_e_slots(int mode, int np) {
+// Shared-memory slots (one double per thread each) of the plain kernels,
+// numbered once for the copies and the reads: E half: H at the cell and at
+// its curl neighbours, D, the CPML integrators and P, J of NP poles; H half:
+// E at the cell and its neighbours, B and the integrators.
+struct PlainSlots {
+  int own[3];     // H (E half) or E (H half) at the cell
+  int nb[3][3];   // [K][J]: component K at the neighbour along J
+  int flux[3];    // D or B
+  int psi[3][3];  // [I][J]
+  int p[2][3], j[2][3];
+  int n;
+};
+
+__host__ __device__ constexpr PlainSlots plain_slots(int mode, int ft, int np) {
+  PlainSlots s{};
   int n = 0;
-  for (int K = 0; K < 3; K++) n += hasH(mode, K) ? 1 : 0;
+  // ft 0: the E half (fluxes of E, curl of H); 1: the H half
+  for (int K = 0; K < 3; K++)
+    if (ft == 0 ? hasH(mode, K) : hasE(mode, K)) s.own[K] = n++;
   for (int I = 0; I < 3; I++)
-    for (int J = 0; J < 3; J++)
-      if (I != J && hasE(mode, I) && hasH(mode, third(I, J))) n++;
-  for (int I = 0; I < 3; I++) n += hasE(mode, I) ? 1 : 0;
+    for (int J = 0; J < 3; J++) {
+      if (I == J || !(ft == 0 ? hasE(mode, I) : hasH(mode, I))) continue;
+      const int K = third(I, J);
+      if (ft == 0 ? hasH(mode, K) : hasE(mode, K)) s.nb[K][J] = n++;
+    }
+  for (int I = 0; I < 3; I++)
+    if (ft == 0 ? hasE(mode, I) : hasH(mode, I)) s.flux[I] = n++;
   for (int J = 0; J < 3; J++)
     for (int I = 0; I < 3; I++)
-      if (hasE(mode, I) && I != J && !(mode != kThreeD && J == 2)) n++;
-  for (int I = 0; I < 3; I++) n += hasE(mode, I) ? 2 * np : 0;
-  return n;
-}
-
-__host__ __device__ constexpr int plain_h_slots(int mode) {
-  int n = 0;
-  for (int K = 0; K < 3; K++) n += hasE(mode, K) ? 1 : 0;
-  for (int I = 0; I < 3; I++)
-    for (int J = 0; J < 3; J++)
-      if (I != J && hasH(mode, I) && hasE(mode, third(I, J))) n++;
-  for (int I = 0; I < 3; I++) n += hasH(mode, I) ? 1 : 0;
-  for (int J = 0; J < 3; J++)
+      if ((ft == 0 ? hasE(mode, I) : hasH(mode, I)) && I != J && !(mode != kThreeD && J == 2)) s.psi[I][J] = n++;
+  for (int q = 0; q < np; q++)
     for (int I = 0; I < 3; I++)
-      if (hasH(mode, I) && I != J && !(mode != kThreeD && J == 2)) n++;
-  return n;
+      if (hasE(mode, I)) {
+        s.p[q][I] = n++;
+        s.j[q][I] = n++;
+      }
+  s.n = n;
+  return s;
 }
 
-// YeeUpdate::update_all (YeeUpdates.hpp:396-405) of flux F at cell c with the
-// summed curl terms: F = TimePolicy::get(F) + (Coeff*curl_coeff*dt) * curl,
-// then TimePolicy::increment moves the old flux into the history (BD3:
-// :209-213, :231-236; BD4: :258-263, :282-288). sdt = Coeff*curl_coeff*dt.
-__device__ __forceinline__ void time_policy_update(const PlainArgs& a, int ft, int I, long long c, double* F,
-                                                   double sdt, double curl) {
-  const double old = F[c];
-  if (a.bd == 0) {
-    F[c] = old + sdt * curl;
-    return;
-  }
-  double* h0 = a.hist[ft][0][I] + c;
-  double* h1 = a.hist[ft][1][I] + c;
-  if (a.bd == 2) {
-    const double get = a.bdk[0] * old + a.bdk[1] * *h0 - a.bdk[2] * *h1;
-    F[c] = get + sdt * curl;
-  } else {
-    double* h2 = a.hist[ft][2][I] + c;
-    const double get = a.bdk[0] * old + a.bdk[1] * *h0 - a.bdk[2] * *h1 + a.bdk[3] * *h2;
-    F[c] = get + sdt * curl;
-    *h2 = *h1;
-  }
-  *h1 = *h0;
-  *h0 = old;
-}
-
-// Both kernels first request every operand of their cell -- the H (E)
-// values of the curl, the flux, the CPML integrators and, with every
-// material dispersive, P and J -- with cp.async into the thread's own
-// shared-memory slots (copies in flight hold no registers), read them back,
-// apply the passes above to registers in the reference's order, and store
-// the results at the end. The arrays may alias as far as the compiler knows,
-// so reading each pass's operands after the previous pass's stores would
-// make a cell wait for one memory round trip per pass; here all the reads
-// are in flight together. The arithmetic, and so every result, is the same.
+// Each thread takes ZC cells along z (planes k0 .. k0 + ZC - 1 of its (i, j)):
+// it requests every operand of all of them -- the H (E) values of the curl,
+// the flux, the CPML integrators and, with every material dispersive, P and
+// J -- with cp.async into its own shared-memory slots (copies in flight hold
+// no registers), then, cell by cell, reads them back, applies the passes
+// above to registers in the reference's order and stores the results. The
+// arrays may alias as far as the compiler knows, so reading each pass's
+// operands after the previous pass's stores would make a cell wait for one
+// memory round trip per pass; here all the reads of ZC cells are in flight
+// together. The arithmetic, and so every result, is the same.
 //
 // NP: poles of P and J read with the fields (0: read after the material id,
 // for the cells whose material has poles). HIST: the BD3/BD4 time policy's
 // flux history is read and moved (a separate instantiation, so that the
 // leapfrog's kernels keep their registers).
-template <int MODE, int NP, bool HIST>
-__global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_constant__ PlainArgs a) {
-  extern __shared__ double smd[];
-  constexpr int NPS = NP > 0 ? NP : 1;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = MODE == kThreeD ? blockIdx.z + 1 : 0;
-  if (i > a.nx - 2 || j > a.ny - 2) return;
+
+// the copies of one cell of the E half; sets the CPML integrator indices
+template <int MODE, int NP>
+__device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, int k, double* slot,
+                                              long long (&pidx)[3]) {
+  constexpr PlainSlots S = plain_slots(MODE, 0, NP);
   const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
   const long long c = k * sz + j * sy + i;
   const long long str[3] = {1, sy, sz};
   const int idx[3] = {i, j, k};
-  const double dt = a.dt;
-  const long long t = a.ctrl->t;
-
-  // ---- every read of the cell, copied into the thread's shared-memory slots
-  // (cp.async: in flight together without holding registers), then read
-  // back; the CPML integrators only where the cell lies in a slab
-  double* slot = smd + tid;
-  int ns = 0;
-  int s_hc[3] = {}, s_hn[3][3] = {}, s_d[3] = {}, s_ps[3][3] = {}, s_p[NPS][3] = {}, s_j[NPS][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasH(MODE, K)) {
-      s_hc[K] = ns++;
-      cp_async8(slot + s_hc[K] * kPlainThreads, a.H.f[K] + c);
-    }
+    if (hasH(MODE, K)) cp_async8(slot + S.own[K] * kPlainThreads, a.H.f[K] + c);
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasE(MODE, I)) continue;
@@ -178,92 +148,89 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
     for (int J = 0; J < 3; J++) {
       if (J == I) continue;
       const int K = third(I, J);
-      if (!hasH(MODE, K)) continue;
-      s_hn[K][J] = ns++;
-      cp_async8(slot + s_hn[K][J] * kPlainThreads, a.H.f[K] + c - str[J]);
+      if (hasH(MODE, K)) cp_async8(slot + S.nb[K][J] * kPlainThreads, a.H.f[K] + c - str[J]);
     }
   }
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasE(MODE, I)) {
-      s_d[I] = ns++;
-      cp_async8(slot + s_d[I] * kPlainThreads, a.D.f[I] + c);
-    }
-  long long pidx[3] = {-1, -1, -1};
+    if (hasE(MODE, I)) cp_async8(slot + S.flux[I] * kPlainThreads, a.D.f[I] + c);
 #pragma unroll
   for (int J = 0; J < 3; J++) {
+    pidx[J] = -1;
     const int s = a.pml_axis[J] ? slab_index(a.slab[J], idx[J]) : -1;
-    if (s >= 0) {
-      if (J == 0) pidx[J] = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
-      else if (J == 1) pidx[J] = (static_cast<long long>(k) * a.slab[1].W + s) * a.nx + i;
-      else pidx[J] = (static_cast<long long>(s) * a.ny + j) * a.nx + i;
-    }
-#pragma unroll
-    for (int I = 0; I < 3; I++) {
-      if (!hasE(MODE, I) || I == J || (MODE != kThreeD && J == 2)) continue;
-      s_ps[I][J] = ns++;
-      if (pidx[J] >= 0) cp_async8(slot + s_ps[I][J] * kPlainThreads, a.psi[0][I][J] + pidx[J]);
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < NP; q++)
+    if (s < 0) continue;
+    if (J == 0) pidx[J] = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
+    else if (J == 1) pidx[J] = (static_cast<long long>(k) * a.slab[1].W + s) * a.nx + i;
+    else pidx[J] = (static_cast<long long>(s) * a.ny + j) * a.nx + i;
 #pragma unroll
     for (int I = 0; I < 3; I++)
-      if (hasE(MODE, I)) {
-        s_p[q][I] = ns++;
-        s_j[q][I] = ns++;
-        if (q < a.dispersive) {
-          cp_async8(slot + s_p[q][I] * kPlainThreads, a.P[q].f[I] + c);
-          cp_async8(slot + s_j[q][I] * kPlainThreads, a.J[q].f[I] + c);
-        }
-      }
-  double h0[3] = {}, h1[3] = {}, h2[3] = {};
-#pragma unroll
-  for (int I = 0; I < 3; I++) {
-    if (!hasE(MODE, I)) continue;
-    if (HIST) {
-      h0[I] = a.hist[0][0][I][c];
-      h1[I] = a.hist[0][1][I][c];
-      if (a.bd == 3) h2[I] = a.hist[0][2][I][c];
-    }
+      if (hasE(MODE, I) && I != J && !(MODE != kThreeD && J == 2))
+        cp_async8(slot + S.psi[I][J] * kPlainThreads, a.psi[0][I][J] + pidx[J]);
   }
-  int mid = 0;
-  if (a.ids) mid = a.ids[c];
-  else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
-  cp_async_wait_all();
-  double hc[3] = {0.0, 0.0, 0.0}, hn[3][3] = {}, d[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
-  double pp[NPS][3] = {}, jj[NPS][3] = {};
-#pragma unroll
-  for (int K = 0; K < 3; K++)
-    if (hasH(MODE, K)) hc[K] = slot[s_hc[K] * kPlainThreads];
-#pragma unroll
-  for (int K = 0; K < 3; K++)
-#pragma unroll
-    for (int J = 0; J < 3; J++)
-      if (J != K && hasH(MODE, K)) {
-        const int I = third(J, K);
-        if (hasE(MODE, I)) hn[K][J] = slot[s_hn[K][J] * kPlainThreads];
-      }
-#pragma unroll
-  for (int I = 0; I < 3; I++)
-    if (hasE(MODE, I)) d[I] = slot[s_d[I] * kPlainThreads];
-#pragma unroll
-  for (int J = 0; J < 3; J++)
-#pragma unroll
-    for (int I = 0; I < 3; I++)
-      if (hasE(MODE, I) && I != J && !(MODE != kThreeD && J == 2) && pidx[J] >= 0)
-        ps[I][J] = slot[s_ps[I][J] * kPlainThreads];
 #pragma unroll
   for (int q = 0; q < NP; q++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && q < a.dispersive) {
-        pp[q][I] = slot[s_p[q][I] * kPlainThreads];
-        jj[q][I] = slot[s_j[q][I] * kPlainThreads];
+        cp_async8(slot + S.p[q][I] * kPlainThreads, a.P[q].f[I] + c);
+        cp_async8(slot + S.j[q][I] * kPlainThreads, a.J[q].f[I] + c);
       }
-  const double eps_cell = a.eps_map ? a.eps_map[c] : 0.0;
+}
 
-  // ---- YeeUpdate<Mode, D_I, TimePolicy>: a = LC*F/dx*(H_K - H_K[-J])
+// the reference's E half of one cell from its slots
+template <int MODE, int NP, bool HIST>
+__device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
+                                             const long long (&pidx)[3]) {
+  constexpr PlainSlots S = plain_slots(MODE, 0, NP);
+  constexpr int NPS = NP > 0 ? NP : 1;
+  const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
+  const long long c = k * sz + j * sy + i;
+  const int idx[3] = {i, j, k};
+  const double dt = a.dt;
+  const long long t = a.ctrl->t;
+  double h0[3] = {}, h1[3] = {}, h2[3] = {};
+#pragma unroll
+  for (int I = 0; I < 3; I++) {
+    if (!hasE(MODE, I) || !HIST) continue;
+    h0[I] = a.hist[0][0][I][c];
+    h1[I] = a.hist[0][1][I][c];
+    if (a.bd == 3) h2[I] = a.hist[0][2][I][c];
+  }
+  int mid = 0;
+  if (a.ids) mid = a.ids[c];
+  else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  const double eps_cell = a.eps_map ? a.eps_map[c] : 0.0;
+  double hc[3] = {0.0, 0.0, 0.0}, hn[3][3] = {}, d[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
+  double pp[NPS][3] = {}, jj[NPS][3] = {};
+#pragma unroll
+  for (int K = 0; K < 3; K++)
+    if (hasH(MODE, K)) hc[K] = slot[S.own[K] * kPlainThreads];
+#pragma unroll
+  for (int K = 0; K < 3; K++)
+#pragma unroll
+    for (int J = 0; J < 3; J++)
+      if (J != K && hasH(MODE, K) && hasE(MODE, third(J, K))) hn[K][J] = slot[S.nb[K][J] * kPlainThreads];
+#pragma unroll
+  for (int I = 0; I < 3; I++)
+    if (hasE(MODE, I)) d[I] = slot[S.flux[I] * kPlainThreads];
+#pragma unroll
+  for (int J = 0; J < 3; J++)
+#pragma unroll
+    for (int I = 0; I < 3; I++)
+      if (hasE(MODE, I) && I != J && !(MODE != kThreeD && J == 2) && pidx[J] >= 0)
+        ps[I][J] = slot[S.psi[I][J] * kPlainThreads];
+#pragma unroll
+  for (int q = 0; q < NP; q++)
+#pragma unroll
+    for (int I = 0; I < 3; I++)
+      if (hasE(MODE, I) && q < a.dispersive) {
+        pp[q][I] = slot[S.p[q][I] * kPlainThreads];
+        jj[q][I] = slot[S.j[q][I] * kPlainThreads];
+      }
+
+  // YeeUpdate<Mode, D_I, TimePolicy>: a = LC*F/dx*(H_K - H_K[-J]), then
+  // F = TimePolicy::get(F) + (Coeff*curl_coeff*dt) * curl and the history
+  // moves on (YeeUpdates.hpp:182-294, :396-405)
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasE(MODE, I)) continue;
@@ -281,7 +248,6 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
       const double fdx = a.prof[0][J].F[idx[J]];
       at[q] = (levi(I, J, K) == 1 ? fdx : -fdx) * diff;
     }
-    // TimePolicy::get + increment (YeeUpdates.hpp:182-294), as time_policy_update
     const double old = d[I], sdt = a.cc * dt, curl = at[0] + at[1];
     if (!HIST) {
       d[I] = old + sdt * curl;
@@ -339,13 +305,12 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
   // material update
   const MatF64& m = a.mats[mid];
   if (NP == 0 && m.kind >= 2) {
-    for (int q = 0; q < NPS; q++)  // NP == 0: NPS == 1, pole 0 here, further poles below
 #pragma unroll
-      for (int I = 0; I < 3; I++)
-        if (hasE(MODE, I)) {
-          pp[q][I] = a.P[q].f[I][c];
-          jj[q][I] = a.J[q].f[I][c];
-        }
+    for (int I = 0; I < 3; I++)
+      if (hasE(MODE, I)) {
+        pp[0][I] = a.P[0].f[I][c];
+        jj[0][I] = a.J[0].f[I][c];
+      }
   }
   double e[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -410,8 +375,7 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
     for (int I = 0; I < 3; I++)
       if (sr.comp == I) e[I] += v;
   }
-
-  // ---- every write of the cell
+  // every write of the cell
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasE(MODE, I)) continue;
@@ -446,31 +410,39 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
   }
 }
 
-template <int MODE, bool HIST>
-__global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_constant__ PlainArgs a) {
+template <int MODE, int NP, bool HIST, int ZC>
+__global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_constant__ PlainArgs a) {
   extern __shared__ double smd[];
+  constexpr int NS = plain_slots(MODE, 0, NP).n;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = MODE == kThreeD ? blockIdx.z + 1 : 0;
+  const int k0 = MODE == kThreeD ? blockIdx.z * ZC + 1 : 0;
   if (i > a.nx - 2 || j > a.ny - 2) return;
+  long long pidx[ZC][3];
+#pragma unroll
+  for (int z = 0; z < ZC; z++)
+    if (z == 0 || k0 + z <= a.nz - 2)
+      plain_e_stage<MODE, NP>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
+  cp_async_wait_all();
+#pragma unroll 1
+  for (int z = 0; z < ZC; z++)
+    if (z == 0 || k0 + z <= a.nz - 2)
+      plain_e_cell<MODE, NP, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
+}
+
+// the copies of one cell of the H half
+template <int MODE>
+__device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, int k, double* slot,
+                                              long long (&pidx)[3]) {
+  constexpr PlainSlots S = plain_slots(MODE, 1, 0);
   const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
   const long long c = k * sz + j * sy + i;
   const long long str[3] = {1, sy, sz};
   const int idx[3] = {i, j, k};
-  const double dt = a.dt;
-  const long long t = a.ctrl->t;
-
-  // ---- every read of the cell, through the thread's shared-memory slots
-  double* slot = smd + tid;
-  int ns = 0;
-  int s_ec[3] = {}, s_en[3][3] = {}, s_b[3] = {}, s_ps[3][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasE(MODE, K)) {
-      s_ec[K] = ns++;
-      cp_async8(slot + s_ec[K] * kPlainThreads, a.E.f[K] + c);
-    }
+    if (hasE(MODE, K)) cp_async8(slot + S.own[K] * kPlainThreads, a.E.f[K] + c);
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasH(MODE, I)) continue;
@@ -478,70 +450,68 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
     for (int J = 0; J < 3; J++) {
       if (J == I) continue;
       const int K = third(I, J);
-      if (!hasE(MODE, K)) continue;
-      s_en[K][J] = ns++;
-      cp_async8(slot + s_en[K][J] * kPlainThreads, a.E.f[K] + c + str[J]);
+      if (hasE(MODE, K)) cp_async8(slot + S.nb[K][J] * kPlainThreads, a.E.f[K] + c + str[J]);
     }
   }
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasH(MODE, I)) {
-      s_b[I] = ns++;
-      cp_async8(slot + s_b[I] * kPlainThreads, a.B.f[I] + c);
-    }
-  long long pidx[3] = {-1, -1, -1};
+    if (hasH(MODE, I)) cp_async8(slot + S.flux[I] * kPlainThreads, a.B.f[I] + c);
 #pragma unroll
   for (int J = 0; J < 3; J++) {
+    pidx[J] = -1;
     const int s = a.pml_axis[J] ? slab_index(a.slab[J], idx[J]) : -1;
-    if (s >= 0) {
-      if (J == 0) pidx[J] = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
-      else if (J == 1) pidx[J] = (static_cast<long long>(k) * a.slab[1].W + s) * a.nx + i;
-      else pidx[J] = (static_cast<long long>(s) * a.ny + j) * a.nx + i;
-    }
+    if (s < 0) continue;
+    if (J == 0) pidx[J] = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
+    else if (J == 1) pidx[J] = (static_cast<long long>(k) * a.slab[1].W + s) * a.nx + i;
+    else pidx[J] = (static_cast<long long>(s) * a.ny + j) * a.nx + i;
 #pragma unroll
-    for (int I = 0; I < 3; I++) {
-      if (!hasH(MODE, I) || I == J || (MODE != kThreeD && J == 2)) continue;
-      s_ps[I][J] = ns++;
-      if (pidx[J] >= 0) cp_async8(slot + s_ps[I][J] * kPlainThreads, a.psi[1][I][J] + pidx[J]);
-    }
+    for (int I = 0; I < 3; I++)
+      if (hasH(MODE, I) && I != J && !(MODE != kThreeD && J == 2))
+        cp_async8(slot + S.psi[I][J] * kPlainThreads, a.psi[1][I][J] + pidx[J]);
   }
+}
+
+// the reference's H half of one cell from its slots
+template <int MODE, bool HIST>
+__device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
+                                             const long long (&pidx)[3]) {
+  constexpr PlainSlots S = plain_slots(MODE, 1, 0);
+  const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
+  const long long c = k * sz + j * sy + i;
+  const int idx[3] = {i, j, k};
+  const double dt = a.dt;
+  const long long t = a.ctrl->t;
   double h0[3] = {}, h1[3] = {}, h2[3] = {};
 #pragma unroll
   for (int I = 0; I < 3; I++) {
-    if (!hasH(MODE, I)) continue;
-    if (HIST) {
-      h0[I] = a.hist[1][0][I][c];
-      h1[I] = a.hist[1][1][I][c];
-      if (a.bd == 3) h2[I] = a.hist[1][2][I][c];
-    }
+    if (!hasH(MODE, I) || !HIST) continue;
+    h0[I] = a.hist[1][0][I][c];
+    h1[I] = a.hist[1][1][I][c];
+    if (a.bd == 3) h2[I] = a.hist[1][2][I][c];
   }
   int mid = 0;
   if (a.ids) mid = a.ids[c];
   else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
-  cp_async_wait_all();
   double ec[3] = {0.0, 0.0, 0.0}, en[3][3] = {}, b[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasE(MODE, K)) ec[K] = slot[s_ec[K] * kPlainThreads];
+    if (hasE(MODE, K)) ec[K] = slot[S.own[K] * kPlainThreads];
 #pragma unroll
   for (int K = 0; K < 3; K++)
 #pragma unroll
     for (int J = 0; J < 3; J++)
-      if (J != K && hasE(MODE, K)) {
-        const int I = third(J, K);
-        if (hasH(MODE, I)) en[K][J] = slot[s_en[K][J] * kPlainThreads];
-      }
+      if (J != K && hasE(MODE, K) && hasH(MODE, third(J, K))) en[K][J] = slot[S.nb[K][J] * kPlainThreads];
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasH(MODE, I)) b[I] = slot[s_b[I] * kPlainThreads];
+    if (hasH(MODE, I)) b[I] = slot[S.flux[I] * kPlainThreads];
 #pragma unroll
   for (int J = 0; J < 3; J++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasH(MODE, I) && I != J && !(MODE != kThreeD && J == 2) && pidx[J] >= 0)
-        ps[I][J] = slot[s_ps[I][J] * kPlainThreads];
+        ps[I][J] = slot[S.psi[I][J] * kPlainThreads];
 
-  // ---- YeeUpdate<Mode, B_I, TimePolicy>: a = LC*F/dx*(E_K[+J] - E_K)
+  // YeeUpdate<Mode, B_I, TimePolicy>: a = LC*F/dx*(E_K[+J] - E_K)
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasH(MODE, I)) continue;
@@ -630,8 +600,7 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
     for (int I = 0; I < 3; I++)
       if (sr.comp == I) h[I] += v;
   }
-
-  // ---- every write of the cell
+  // every write of the cell
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasH(MODE, I)) continue;
@@ -650,6 +619,27 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
     for (int I = 0; I < 3; I++)
       if (hasH(MODE, I) && I != J) a.psi[1][I][J][pidx[J]] = ps[I][J];
   }
+}
+
+template <int MODE, bool HIST, int ZC>
+__global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_constant__ PlainArgs a) {
+  extern __shared__ double smd[];
+  constexpr int NS = plain_slots(MODE, 1, 0).n;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k0 = MODE == kThreeD ? blockIdx.z * ZC + 1 : 0;
+  if (i > a.nx - 2 || j > a.ny - 2) return;
+  long long pidx[ZC][3];
+#pragma unroll
+  for (int z = 0; z < ZC; z++)
+    if (z == 0 || k0 + z <= a.nz - 2)
+      plain_h_stage<MODE>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
+  cp_async_wait_all();
+#pragma unroll 1
+  for (int z = 0; z < ZC; z++)
+    if (z == 0 || k0 + z <= a.nz - 2)
+      plain_h_cell<MODE, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
 }
 
 // the shared-memory carveout that holds the two CTAs per SM that the
@@ -674,25 +664,31 @@ static void plain_launch(F fn, size_t smem, const dim3& grid, const dim3& block,
   fn<<<grid, block, smem, s>>>(a);
 }
 
+// 3D grids: two cells along z per thread for the sweeps with few slots
+// (twice the copies in flight at the same occupancy), one for the two-pole E
+// sweep, whose 30 slots a thread fill shared memory at two CTAs per SM
 template <int MODE>
 static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
-  dim3 block(32, kPlainThreads / 32, 1);
-  dim3 grid((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y, MODE == kThreeD ? a.nz - 2 : 1);
-  constexpr size_t sh = plain_h_slots(MODE) * kPlainThreads * sizeof(double);
-  constexpr size_t s0 = plain_e_slots(MODE, 0) * kPlainThreads * sizeof(double);
-  constexpr size_t s1 = plain_e_slots(MODE, 1) * kPlainThreads * sizeof(double);
-  constexpr size_t s2 = plain_e_slots(MODE, 2) * kPlainThreads * sizeof(double);
+  constexpr int ZC = MODE == kThreeD ? 2 : 1;
+  const dim3 block(32, kPlainThreads / 32, 1);
+  auto grid = [&](int zc) {
+    return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y,
+                MODE == kThreeD ? (a.nz - 2 + zc - 1) / zc : 1);
+  };
+  auto bytes = [](int ft, int np, int zc) {
+    return static_cast<size_t>(plain_slots(MODE, ft, np).n) * zc * kPlainThreads * sizeof(double);
+  };
   if (!e) {
-    if (a.bd) plain_launch(plain_h_kernel<MODE, true>, sh, grid, block, a, s);
-    else plain_launch(plain_h_kernel<MODE, false>, sh, grid, block, a, s);
+    if (a.bd) plain_launch(plain_h_kernel<MODE, true, ZC>, bytes(1, 0, ZC), grid(ZC), block, a, s);
+    else plain_launch(plain_h_kernel<MODE, false, ZC>, bytes(1, 0, ZC), grid(ZC), block, a, s);
   } else if (a.bd) {
-    plain_launch(plain_e_kernel<MODE, 0, true>, s0, grid, block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, true, ZC>, bytes(0, 0, ZC), grid(ZC), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 1) {
-    plain_launch(plain_e_kernel<MODE, 1, false>, s1, grid, block, a, s);
+    plain_launch(plain_e_kernel<MODE, 1, false, ZC>, bytes(0, 1, ZC), grid(ZC), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 2) {
-    plain_launch(plain_e_kernel<MODE, 2, false>, s2, grid, block, a, s);
+    plain_launch(plain_e_kernel<MODE, 2, false, 1>, bytes(0, 2, 1), grid(1), block, a, s);
   } else {
-    plain_launch(plain_e_kernel<MODE, 0, false>, s0, grid, block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, false, ZC>, bytes(0, 0, ZC), grid(ZC), block, a, s);
   }
   return 1;
 }
