@@ -644,7 +644,8 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
 
 // the shared-memory carveout that holds the two CTAs per SM that the
 // kernels' registers allow (plus the 1 KB the runtime reserves per CTA); the
-// rest of the SM's memory stays L1, which serves the neighbour reads
+// rest of the SM's memory stays L1, which serves the neighbour reads (a
+// larger carveout slowed the sweeps measurably)
 static int plain_carveout(size_t smem) {
   int dev = 0, max_sm = 0;
   cudaGetDevice(&dev);
@@ -664,12 +665,14 @@ static void plain_launch(F fn, size_t smem, const dim3& grid, const dim3& block,
   fn<<<grid, block, smem, s>>>(a);
 }
 
-// 3D grids: two cells along z per thread for the sweeps with few slots
-// (twice the copies in flight at the same occupancy), one for the two-pole E
-// sweep, whose 30 slots a thread fill shared memory at two CTAs per SM
+// One cell per thread (ZC = 1). Two cells along z per thread, both staged
+// before either is computed, measured no faster on B200 (the sweeps are
+// bound by the latency of their FP64 arithmetic -- the reference's IEEE
+// divisions among it -- at the two CTAs per SM their registers allow, not by
+// the copies in flight), nor did three CTAs per SM at 80 registers (spills).
 template <int MODE>
 static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
-  constexpr int ZC = MODE == kThreeD ? 2 : 1;
+  constexpr int ZC = 1;
   const dim3 block(32, kPlainThreads / 32, 1);
   auto grid = [&](int zc) {
     return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y,
@@ -684,7 +687,7 @@ static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
   } else if (a.bd) {
     plain_launch(plain_e_kernel<MODE, 0, true, ZC>, bytes(0, 0, ZC), grid(ZC), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 1) {
-    plain_launch(plain_e_kernel<MODE, 1, false, ZC>, bytes(0, 1, ZC), grid(ZC), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 1, false, 1>, bytes(0, 1, 1), grid(1), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 2) {
     plain_launch(plain_e_kernel<MODE, 2, false, 1>, bytes(0, 2, 1), grid(1), block, a, s);
   } else {
