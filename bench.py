@@ -582,6 +582,16 @@ def run_batch(args, torch, world, rank, local, stream):
     peak, peak_kind = peaks()
     ach = ab * args.steps / (ms / 1e3) / 1e9
     info = batch.info()
+    ir = batch.item_rows()
+    classes = {}
+    for p_, r_, c_ in zip(probs, ir["rows"], ir["size_class"]):
+        e = classes.setdefault(str(c_), {"problems": 0, "cells_min": None, "cells_max": 0, "item_rows": set()})
+        e["problems"] += 1
+        e["cells_min"] = p_.interior_cells if e["cells_min"] is None else min(e["cells_min"], p_.interior_cells)
+        e["cells_max"] = max(e["cells_max"], p_.interior_cells)
+        e["item_rows"].add(r_)
+    for e in classes.values():
+        e["item_rows"] = sorted(e["item_rows"])
     batch.close()
     for g in grids:
         g.close()
@@ -632,6 +642,7 @@ def run_batch(args, torch, world, rank, local, stream):
                    "cpml": 10, "steps_in_config": 3000, "tile_rows": info["rows"], "ctas": info["blocks"],
                    "launch": info["launch"],
                    "tune_ms_per_step": info["tune_ms_per_step"],
+                   "size_classes": classes, "tuned_ms_per_step": ir["tuned_ms_per_step"],
                    "l2": "state ~290 MB > L2; no flush", "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "kernel": ("batch_kernel (persistent, all steps)" if info["launch"] == "persistent"
                                                 else "batch_phase_kernel (E and H launches of one step)"),

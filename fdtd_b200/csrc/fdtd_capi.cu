@@ -1936,10 +1936,14 @@ struct fdtd_batch {
   unsigned* d_items = nullptr;
   int nitems = 0, rows = 0, blocks = 0;
   int persistent = 1;  // 1: one cooperative kernel for all steps; 0: one kernel per half step
+  std::vector<FusedArgs> h_args;  // host copy of d_args
+  std::vector<int> mult;          // per grid: work-item rows = rows * mult
+  std::vector<int> cls;           // per grid: its size class (quartile of cell counts), for the tuner
   cudaStream_t stream = nullptr;
   std::map<int, cudaGraphExec_t> graphs;  // keyed by steps per launch
   // measured ms per step: persistent with rows 1, 2, 4, 8, then per-phase with rows 1, 2, 4, 8
   std::vector<float> tune_ms;
+  float tune_best_ms = 0.f;  // with the per-class item heights
 };
 
 namespace {
@@ -1967,13 +1971,18 @@ std::vector<std::pair<void*, size_t>> grid_state(fdtd_grid* g) {
   return out;
 }
 
+// the work list of kernel tile height `rows`, each grid's items `rows *
+// b->mult[grid]` rows high (the grids' arguments are re-uploaded with it)
 int batch_items(fdtd_batch* b, int rows) {
   std::vector<unsigned> items;
   for (size_t q = 0; q < b->grids.size(); q++) {
     const fdtd_grid* g = b->grids[q];
-    const int tx = g->pitch / 128, ty = (g->n[1] - 2 + rows - 1) / rows;
+    const int R = rows * b->mult[q];
+    b->h_args[q].item_rows = R;
+    const int tx = g->pitch / 128, ty = (g->n[1] - 2 + R - 1) / R;
     for (int t = 0; t < tx * ty; t++) items.push_back(static_cast<unsigned>(q) << 24 | static_cast<unsigned>(t));
   }
+  CK(cudaMemcpy(b->d_args, b->h_args.data(), b->h_args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice));
   // consecutive items (tiles of one grid) go to consecutive CTAs
   b->nitems = static_cast<int>(items.size());
   if (b->d_items) cudaFree(b->d_items);
@@ -2073,6 +2082,18 @@ int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out) try {
   }
   CK(cudaMalloc(&b->d_args, args.size() * sizeof(FusedArgs)));
   CK(cudaMemcpy(b->d_args, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice));
+  b->h_args = args;
+  b->mult.assign(b->grids.size(), 1);
+  {
+    // size classes: quartiles of the grids' cell counts
+    std::vector<int> order(b->grids.size());
+    for (size_t q = 0; q < order.size(); q++) order[q] = static_cast<int>(q);
+    auto cells = [&](int q) { return static_cast<long long>(b->grids[q]->n[0]) * b->grids[q]->n[1]; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) < cells(y); });
+    b->cls.assign(b->grids.size(), 0);
+    const int nc = std::min<int>(4, static_cast<int>(order.size()));
+    for (size_t r = 0; r < order.size(); r++) b->cls[order[r]] = static_cast<int>(r * nc / order.size());
+  }
   CK(cudaMalloc(&b->d_ctrls, ctrls.size() * sizeof(Control*)));
   CK(cudaMemcpy(b->d_ctrls, ctrls.data(), ctrls.size() * sizeof(Control*), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&b->d_ctl, sizeof(BatchCtl)));
@@ -2130,6 +2151,7 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
   // candidates: the persistent kernel and the per-phase launches, each with
   // tiles of 1, 2, 4 or 8 rows
   const int cand[4] = {1, 2, 4, 8};
+  b->mult.assign(b->grids.size(), 1);
   float best = 1e30f;
   int best_rows = 4, best_persistent = 1;
   b->tune_ms.assign(8, 0.f);
@@ -2155,6 +2177,38 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
     }
     if (!rc) rc = copy(false);
   }
+  // per size class: the work-item height, in multiples 1, 2, 4, 8 of the
+  // chosen kernel tile height, one class after the other (largest grids
+  // first), the others held at their best so far
+  b->persistent = best_persistent;
+  const int ncls = b->cls.empty() ? 0 : 1 + *std::max_element(b->cls.begin(), b->cls.end());
+  for (int c = ncls - 1; c >= 0 && !rc; c--) {
+    int keep = 1;
+    for (int m : {2, 4, 8}) {
+      std::vector<int> old = b->mult;
+      for (size_t q = 0; q < b->grids.size(); q++)
+        if (b->cls[q] == c) b->mult[q] = m;
+      rc = batch_items(b, best_rows);
+      if (!rc) rc = batch_launch(b, 1, b->stream);
+      if (!rc) rc = copy(false);
+      CK(cudaEventRecord(e0, b->stream));
+      if (!rc) rc = batch_launch(b, steps, b->stream);
+      CK(cudaEventRecord(e1, b->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (!rc) rc = copy(false);
+      if (ms < best) {
+        best = ms;
+        keep = m;
+      } else {
+        b->mult = old;
+      }
+    }
+    for (size_t q = 0; q < b->grids.size(); q++)
+      if (b->cls[q] == c) b->mult[q] = keep;
+  }
+  b->tune_best_ms = best / steps;
   CK(cudaStreamSynchronize(b->stream));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2179,7 +2233,39 @@ int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) try {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
   b->persistent = persistent ? 1 : 0;
+  b->mult.assign(b->grids.size(), 1);
   return batch_items(b, rows);
+} catch (...) {
+  return host_failure();
+}
+
+int fdtd_batch_set_item_rows(fdtd_batch* b, const int* rows_per_grid) try {
+  if (!b || !rows_per_grid) return fail(FDTD_ERR_INVALID, "null argument");
+  std::vector<int> m(b->grids.size());
+  for (size_t q = 0; q < b->grids.size(); q++) {
+    const int r = rows_per_grid[q];
+    if (r < b->rows || r % b->rows != 0 || (r / b->rows & (r / b->rows - 1)) != 0 || r / b->rows > 8)
+      return fail(FDTD_ERR_INVALID, "item rows must be the tile height times 1, 2, 4 or 8");
+    m[q] = r / b->rows;
+  }
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  b->mult = m;
+  return batch_items(b, b->rows);
+} catch (...) {
+  return host_failure();
+}
+
+int fdtd_batch_item_rows(fdtd_batch* b, int* rows_per_grid, int* size_class, float* tuned_ms) try {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch");
+  for (size_t q = 0; q < b->grids.size(); q++) {
+    if (rows_per_grid) rows_per_grid[q] = b->rows * b->mult[q];
+    if (size_class) size_class[q] = b->cls[q];
+  }
+  if (tuned_ms) *tuned_ms = b->tune_best_ms;
+  return FDTD_OK;
 } catch (...) {
   return host_failure();
 }

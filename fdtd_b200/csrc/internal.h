@@ -187,6 +187,7 @@ struct FusedArgs {
   double dx, dt;
   double eta;
   Control* ctrl;
+  int item_rows;  // batches: rows of one work item of this grid (a multiple of the kernel's rows; 0: the kernel's)
 };
 
 struct DftRegionDev {

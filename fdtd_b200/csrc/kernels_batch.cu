@@ -2,8 +2,10 @@
 //
 // Many independent TE/TM grids of uneven sizes (each an fdtd_grid set up with
 // the ordinary calls) are advanced together by ONE cooperative kernel that
-// runs every requested step: the work list holds (grid, 128 x ROWS tile)
-// items; each CTA takes items round-robin; the E phase of all grids, a grid
+// runs every requested step: the work list holds (grid, tile) items, a tile
+// being 128 cells x the grid's item rows (a multiple of the CTA's ROWS, set
+// per grid by the tuner from the grid's size); each CTA takes items
+// round-robin; the E phase of all grids, a grid
 // barrier, the H phase, a barrier, next step. The update per 4-cell group is
 // the fused E/H form of kernels_fused.cu restated for 2D with 128-bit access.
 //
@@ -317,16 +319,18 @@ __global__ void __launch_bounds__(32 * ROWS) batch_kernel(const FusedArgs* __res
       const unsigned w = items[it];
       const FusedArgs& a = grids[w >> 24];
       const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
-      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
-      e_group_2d<MODE, MAXP>(a, x4, j, lane, t);
+      const int R = a.item_rows > 0 ? a.item_rows : ROWS;
+      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
+      for (int r = 0; r < R; r += ROWS) e_group_2d<MODE, MAXP>(a, x4, j + r, lane, t);
     }
     if (!grid_barrier(ctl, gridDim.x)) return;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
       const unsigned w = items[it];
       const FusedArgs& a = grids[w >> 24];
       const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
-      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
-      h_group_2d<MODE>(a, x4, j, lane, t);
+      const int R = a.item_rows > 0 ? a.item_rows : ROWS;
+      const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
+      for (int r = 0; r < R; r += ROWS) h_group_2d<MODE>(a, x4, j + r, lane, t);
     }
     if (!grid_barrier(ctl, gridDim.x)) return;
   }
@@ -345,9 +349,12 @@ __global__ void __launch_bounds__(32 * ROWS) batch_phase_kernel(const FusedArgs*
   const FusedArgs& a = grids[w >> 24];
   const long long t = grids[0].ctrl->t + s;
   const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
-  const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * ROWS + ty;
-  if (PHASE == 0) e_group_2d<MODE, MAXP>(a, x4, j, lane, t);
-  else h_group_2d<MODE>(a, x4, j, lane, t);
+  const int R = a.item_rows > 0 ? a.item_rows : ROWS;
+  const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
+  for (int r = 0; r < R; r += ROWS) {
+    if (PHASE == 0) e_group_2d<MODE, MAXP>(a, x4, j + r, lane, t);
+    else h_group_2d<MODE>(a, x4, j + r, lane, t);
+  }
 }
 
 template <int MODE, int MAXP, int ROWS>

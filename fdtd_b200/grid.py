@@ -35,7 +35,7 @@ EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_pm
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
-           "fdtd_batch_info",
+           "fdtd_batch_info", "fdtd_batch_item_rows", "fdtd_batch_set_item_rows",
            "fdtd_batch_error_flags", "fdtd_adjoint_create", "fdtd_adjoint_forward", "fdtd_adjoint_backward",
            "fdtd_adjoint_destroy", "fdtd_last_error_string"]
 
@@ -110,6 +110,8 @@ def load_library(path: str = LIB_PATH):
         "fdtd_batch_tune": [vp, i],
         "fdtd_batch_step": [vp, i, vp],
         "fdtd_batch_info": [vp, ip, ip, ip, ip, ctypes.POINTER(ctypes.c_float)],
+        "fdtd_batch_item_rows": [vp, ip, ip, ctypes.POINTER(ctypes.c_float)],
+        "fdtd_batch_set_item_rows": [vp, ip],
         "fdtd_batch_configure": [vp, i, i],
         "fdtd_batch_error_flags": [vp, ip],
         "fdtd_adjoint_create": [vp, ip, ip, ctypes.c_double, ip, ip, i, ctypes.POINTER(vp)],
@@ -442,6 +444,17 @@ class Batch:
         return {"rows": rows.value, "blocks": blocks.value, "items": items.value,
                 "launch": "persistent" if pers.value else "per_phase",
                 "tune_ms_per_step": {k: float(m) for k, m in zip(keys, ms)}}
+
+    def item_rows(self) -> dict:
+        """Per grid: the rows of its work items and its size class; and the
+        tuner's ms per step with them."""
+        n = len(self.grids)
+        rows, cls, ms = (ctypes.c_int * n)(), (ctypes.c_int * n)(), ctypes.c_float()
+        _check(load_library().fdtd_batch_item_rows(self.h, rows, cls, ctypes.byref(ms)))
+        return {"rows": list(rows), "size_class": list(cls), "tuned_ms_per_step": float(ms.value)}
+
+    def set_item_rows(self, rows_per_grid) -> None:
+        _check(load_library().fdtd_batch_set_item_rows(self.h, _ip(rows_per_grid)))
 
     def error_flags(self) -> int:
         v = ctypes.c_int()

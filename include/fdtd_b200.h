@@ -322,12 +322,23 @@ typedef struct fdtd_batch fdtd_batch;
 int fdtd_batch_create(int n, fdtd_grid* const* grids, fdtd_batch** out);
 int fdtd_batch_destroy(fdtd_batch* b);
 /* Autotuner: times both launch modes with each tile height (1, 2, 4, 8 rows
- * of 128 cells) for `steps` steps on a snapshot of the grids' state, restores
- * the state and keeps the fastest. */
+ * of 128 cells) for `steps` steps on a snapshot of the grids' state; then,
+ * for the fastest, each size class of grids (quartiles of the cell counts,
+ * largest first) in turn with work items 1, 2, 4 or 8 times that height;
+ * restores the state and keeps the fastest. */
 int fdtd_batch_tune(fdtd_batch* b, int steps);
 /* Choose the launch mode (1: persistent, 0: one kernel per half step) and
- * the tile height (1, 2, 4 or 8) without tuning. */
+ * the tile height (1, 2, 4 or 8) without tuning; every grid's work items are
+ * one tile high. */
 int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows);
+/* Per grid of the batch (in creation order): the rows of its work items and
+ * its size class (0 = the quarter of the grids with the fewest cells .. 3);
+ * the tuner's ms per step with those heights (0 if not tuned). Any output
+ * pointer may be NULL. */
+int fdtd_batch_item_rows(fdtd_batch* b, int* rows_per_grid, int* size_class, float* tuned_ms);
+/* Set the work-item rows of every grid (in creation order): the tile height
+ * in use times 1, 2, 4 or 8. The tuner's choice, by hand. */
+int fdtd_batch_set_item_rows(fdtd_batch* b, const int* rows_per_grid);
 int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream);
 /* Tile height in use, CTAs per launch, work items, the launch mode (1:
  * persistent, 0: per half step), and the tuner's ms per step (tune_ms[8]:

@@ -66,6 +66,13 @@ def test_batch_tuning_preserves_state_and_results(fdtd):
             b.tune(3)
             info = b.info()
             assert info["rows"] in (1, 2, 4, 8) and all(v > 0 for v in info["tune_ms_per_step"].values())
+            # work-item heights per size class: 1, 2, 4 or 8 tiles, one height per class
+            ir = b.item_rows()
+            assert ir["tuned_ms_per_step"] > 0
+            assert set(ir["size_class"]) == set(range(min(4, len(grids))))
+            for r, c in zip(ir["rows"], ir["size_class"]):
+                assert r in (info["rows"], 2 * info["rows"], 4 * info["rows"], 8 * info["rows"])
+                assert len({r2 for r2, c2 in zip(ir["rows"], ir["size_class"]) if c2 == c}) == 1
             b.step(30)
         else:
             b.step(10)
@@ -73,6 +80,32 @@ def test_batch_tuning_preserves_state_and_results(fdtd):
         out.append([g.get("Hz") for g in grids])
     for a, c in zip(out[0], out[1]):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_batch_item_heights_per_grid_agree(fdtd, persistent):
+    """Work items 1, 2, 4 and 8 tiles high, mixed per grid (as the tuner sets
+    them per size class), give the one-tile result bit for bit."""
+    probs = small_te_batch(30)
+    out = []
+    for mixed in (False, True):
+        grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+        b = fdtd.Batch(grids)
+        b.configure(persistent, 2)
+        if mixed:
+            b.set_item_rows([2 * (1 << (q % 4)) for q in range(len(grids))])
+            assert b.item_rows()["rows"] == [2 * (1 << (q % 4)) for q in range(len(grids))]
+        b.step(30)
+        assert b.error_flags() == 0
+        out.append([g.get("Hz") for g in grids] + [g.get("Ex") for g in grids])
+        b.close()
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
+    grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+    b = fdtd.Batch(grids)
+    b.configure(True, 2)
+    with pytest.raises(fdtd.FdtdError):
+        b.set_item_rows([3] * len(grids))
 
 
 @pytest.mark.parametrize("make", [small_te_batch, small_tm_batch], ids=["te", "tm"])
