@@ -208,6 +208,7 @@ struct fdtd_grid {
   bool dirty_dft = true;
   bool dirty_pml = false;  // host CPML profiles changed: device profiles and slabs follow before use
   int next_half = 0;  // fdtd_step_half: the phase expected next
+  bool half_split = false;  // fdtd_step_half_part: part 0 of the half step ran, part 1 is due
   BcFaces bcs{};      // faces with a boundary condition
   int scheme = 1;     // time policy of the curl updates: 1 BD1, 3 BD3, 4 BD4
   void* hist[2][3][3]{};  // FP64 flux history [D|B][level][comp] of BD3/BD4
@@ -727,6 +728,8 @@ PlainArgs plain_args(fdtd_grid* g) {
   for (int ft = 0; ft < 2; ft++)
     for (int l = 0; l < 3; l++)
       for (int c = 0; c < 3; c++) a.hist[ft][l][c] = static_cast<double*>(g->hist[ft][l][c]);
+  a.kbeg = 1;
+  a.kend = g->n[2] - 1;
   return a;
 }
 
@@ -774,6 +777,8 @@ FusedArgs fused_args(fdtd_grid* g) {
   a.dx = g->d.dx;
   a.dt = g->d.dt;
   a.eta = eta();
+  a.kbeg = 1;
+  a.kend = g->n[2] - 1;
   return a;
 }
 
@@ -1463,7 +1468,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
 
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
-  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
+  if (g->next_half != 0 || g->half_split) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(g->d.device));
@@ -1564,21 +1569,34 @@ int fdtd_set_sweep_kernel(fdtd_grid* g, int kind) try {
 // ghost planes of a z-slab decomposition): the launches of one step of
 // enqueue_steps, split after the E-phase DFT gather; phase 0 also advances
 // the TFSF aux grids by one step. Launched eagerly, never from a graph.
-int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
+//
+// part -1 runs the whole half step. Parts 0 and 1 split it so that a ghost
+// plane's transfer can overlap the sweep: part 0 runs what comes before the
+// sweep and sweeps every plane whose update reads no ghost plane (E half:
+// planes 2 .. nz-2; plane 1 differences H along z with plane 0. H half:
+// planes 1 .. nz-3; plane nz-2 reads E of plane nz-1); part 1 sweeps the
+// remaining plane and runs everything after the sweep. Per cell the updates
+// are those of the whole sweep, so the results are identical.
+static int half_step_impl(fdtd_grid* g, int phase, int part, void* stream) {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   if (phase != 0 && phase != 1) return fail(FDTD_ERR_INVALID, "phase must be 0 (E) or 1 (H)");
+  if (part < -1 || part > 1) return fail(FDTD_ERR_INVALID, "part must be -1 (whole), 0 or 1");
   if (phase != g->next_half) return fail(FDTD_ERR_INVALID, "half steps alternate, the E half first");
+  if (part == 1 && !g->half_split) return fail(FDTD_ERR_INVALID, "part 1 of a half step comes after its part 0");
+  if (part != 1 && g->half_split) return fail(FDTD_ERR_INVALID, "part 0 of this half step is waiting for its part 1");
+  const int mode = g->d.mode;
+  if (part >= 0 && (mode != kThreeD || g->n[2] < 4))
+    return fail(FDTD_ERR_UNSUPPORTED, "a half step splits along z on 3D grids of 2 or more interior planes");
   CK(cudaSetDevice(g->d.device));
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
-  if (s != g->stream) CK(cudaStreamSynchronize(g->stream));
-  if (g->dirty_dft) {
+  if (s != g->stream && part != 1) CK(cudaStreamSynchronize(g->stream));
+  if (part != 1 && g->dirty_dft) {
     int rc = rebuild_dft(g);
     if (rc) return rc;
     CK(cudaStreamSynchronize(g->stream));
   }
-  const int mode = g->d.mode;
   const bool boxes = !g->boxes.empty();
-  if (phase == 0) {
+  if (part != 1 && phase == 0) {
     for (auto& a : g->auxes) {
       if (a.cap < 2) {
         if (a.d_tab) dfree(g, a.d_tab);
@@ -1605,15 +1623,32 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
   if (g->f32) fa = fused_args(g);
   else pa = plain_args(g);
   const bool use3d = g->f32 && mode == kThreeD && fused3d_supported(fa);
+  if (part >= 0 && g->f32 && !use3d)
+    return fail(FDTD_ERR_UNSUPPORTED, "the split half step needs the staged 3D sweeps (row pitch a multiple of 128)");
+  // the planes of this part: E half part 0 = 2 .. nz-2, part 1 = 1; H half
+  // part 0 = 1 .. nz-3, part 1 = nz-2
+  if (part >= 0) {
+    const int nz = g->n[2];
+    const int kb = phase == 0 ? (part == 0 ? 2 : 1) : (part == 0 ? 1 : nz - 2);
+    const int ke = phase == 0 ? (part == 0 ? nz - 1 : 2) : (part == 0 ? nz - 2 : nz - 1);
+    fa.kbeg = pa.kbeg = kb;
+    fa.kend = pa.kend = ke;
+  }
   const void* const* fields = reinterpret_cast<const void* const*>(g->d_fieldptrs) + (phase == 0 ? 0 : 3);
-  if (boxes && g->f32) g->launches += launch_boxes(g, phase, -1, s);
+  if (part != 1 && boxes && g->f32) g->launches += launch_boxes(g, phase, -1, s);
   if (g->f32) {
     if (phase == 0) g->launches += use3d ? launch_staged_e(fa, s) : launch_fused_e(mode, fa, s);
     else g->launches += use3d ? launch_staged_h(fa, s) : launch_fused_h(mode, fa, s);
-    g->launches += launch_tfsf_fused(mode, fa, phase, s);
   } else {
     g->launches += phase == 0 ? launch_plain_e(mode, pa, s) : launch_plain_h(mode, pa, s);
   }
+  if (part == 0) {
+    CK(cudaGetLastError());
+    g->half_split = true;
+    return FDTD_OK;
+  }
+  g->half_split = false;
+  if (g->f32) g->launches += launch_tfsf_fused(mode, fa, phase, s);
   if (boxes) g->launches += launch_boxes(g, phase, 0, s);
   g->launches += launch_bc(g, phase, s);
   g->launches += launch_dft_gather(g->f32 ? 1 : 0, g->d_dft[phase], g->ndft[phase], g->dft_pts[phase],
@@ -1627,6 +1662,18 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
   CK(cudaGetLastError());
   g->next_half = 1 - phase;
   return FDTD_OK;
+}
+
+int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
+  if (g && g->half_split) return fail(FDTD_ERR_INVALID, "part 0 of this half step is waiting for its part 1");
+  return half_step_impl(g, phase, -1, stream);
+} catch (...) {
+  return host_failure();
+}
+
+int fdtd_step_half_part(fdtd_grid* g, int phase, int part, void* stream) try {
+  if (part != 0 && part != 1) return fail(FDTD_ERR_INVALID, "part must be 0 or 1");
+  return half_step_impl(g, phase, part, stream);
 } catch (...) {
   return host_failure();
 }
@@ -2394,7 +2441,7 @@ int static_aux_address(int device, double** out) {
 
 extern "C" int fdtd_step_static_scratch(fdtd_grid* g, int nsteps, void* stream) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
-  if (g->next_half != 0) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
+  if (g->next_half != 0 || g->half_split) return fail(FDTD_ERR_INVALID, "an E half step was taken without its H half");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "nsteps < 0");
   if (nsteps == 0) return FDTD_OK;
   CK(cudaSetDevice(g->d.device));

@@ -153,6 +153,7 @@ struct PlainArgs {
   double bdk[4];
   double cc;
   double* hist[2][3][3];
+  int kbeg, kend;  // 3D: the sweeps update planes kbeg .. kend-1 (all interior planes: 1 .. nz-2)
 };
 
 struct FusedArgs {
@@ -188,6 +189,7 @@ struct FusedArgs {
   double eta;
   Control* ctrl;
   int item_rows;  // batches: rows of one work item of this grid (a multiple of the kernel's rows; 0: the kernel's)
+  int kbeg, kend;  // the staged 3D sweeps update planes kbeg .. kend-1 (all interior planes: 1 .. nz-2)
 };
 
 struct DftRegionDev {

@@ -124,7 +124,7 @@ __device__ __forceinline__ void e_tile(const FusedArgs& a, int bx, int by, int k
 template <int MAXP, int MINB, bool PJ>
 __global__ void __launch_bounds__(kThreads, MINB) staged_e_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
-  e_tile<MAXP, PJ>(a, blockIdx.x, blockIdx.y, 1 + blockIdx.z, sm);
+  e_tile<MAXP, PJ>(a, blockIdx.x, blockIdx.y, a.kbeg + blockIdx.z, sm);
 }
 
 // The H update of one tile (as e_tile).
@@ -171,7 +171,7 @@ template <int MINB, bool MU>
 __global__ void __launch_bounds__(kThreads, MINB) staged_h_kernel(const __grid_constant__ FusedArgs a) {
   extern __shared__ float4 sm[];
   // planes from the top down, as the flat H sweep
-  h_tile<MU>(a, blockIdx.x, blockIdx.y, a.nz - 2 - blockIdx.z, sm);
+  h_tile<MU>(a, blockIdx.x, blockIdx.y, a.kend - 1 - blockIdx.z, sm);
 }
 
 // The shared-memory carveout (percent of the largest) that holds `ctas` CTAs
@@ -191,7 +191,7 @@ static int carveout_for(int ctas, size_t smem) {
 // with it staged, as many as the shared memory holds (two poles: 4 x 49.7 KB)
 template <int MAXP, bool PJ>
 static void staged_e_launch(const FusedArgs& a, cudaStream_t s) {
-  dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.nz - 2), block(32, kRowsA, 1);
+  dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.kend - a.kbeg), block(32, kRowsA, 1);
   constexpr int slots = kSlotsE + (PJ ? pj_slots<MAXP>() : 0);
   constexpr int minb = !PJ ? (MAXP >= 2 ? 6 : 7) : (MAXP >= 2 ? 4 : (MAXP == 1 ? 6 : 7));
   const size_t smem = slots * kThreads * sizeof(float4) + kThreads * sizeof(unsigned);
@@ -227,7 +227,7 @@ int launch_staged_e(const FusedArgs& a, cudaStream_t s) {
 
 template <bool MU>
 static void staged_h_dispatch(const FusedArgs& a, cudaStream_t s) {
-  dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.nz - 2), block(32, kRowsA, 1);
+  dim3 grid(a.pitch / 128, (a.ny - 2 + kRowsA - 1) / kRowsA, a.kend - a.kbeg), block(32, kRowsA, 1);
   const size_t smem = kSlotsH * kThreads * sizeof(float4);
   once_per_device(reinterpret_cast<const void*>(staged_h_kernel<8, MU>), [&] {
     cudaFuncSetAttribute(staged_h_kernel<8, MU>, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_for(8, smem));

@@ -417,17 +417,17 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k0 = MODE == kThreeD ? blockIdx.z * ZC + 1 : 0;
+  const int k0 = MODE == kThreeD ? a.kbeg + blockIdx.z * ZC : 0;
   if (i > a.nx - 2 || j > a.ny - 2) return;
   long long pidx[ZC][3];
 #pragma unroll
   for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z <= a.nz - 2)
+    if (z == 0 || k0 + z < a.kend)
       plain_e_stage<MODE, NP>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
   cp_async_wait_all();
 #pragma unroll 1
   for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z <= a.nz - 2)
+    if (z == 0 || k0 + z < a.kend)
       plain_e_cell<MODE, NP, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
 }
 
@@ -628,17 +628,17 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k0 = MODE == kThreeD ? blockIdx.z * ZC + 1 : 0;
+  const int k0 = MODE == kThreeD ? a.kbeg + blockIdx.z * ZC : 0;
   if (i > a.nx - 2 || j > a.ny - 2) return;
   long long pidx[ZC][3];
 #pragma unroll
   for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z <= a.nz - 2)
+    if (z == 0 || k0 + z < a.kend)
       plain_h_stage<MODE>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
   cp_async_wait_all();
 #pragma unroll 1
   for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z <= a.nz - 2)
+    if (z == 0 || k0 + z < a.kend)
       plain_h_cell<MODE, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
 }
 
@@ -676,7 +676,7 @@ static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
   const dim3 block(32, kPlainThreads / 32, 1);
   auto grid = [&](int zc) {
     return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y,
-                MODE == kThreeD ? (a.nz - 2 + zc - 1) / zc : 1);
+                MODE == kThreeD ? (a.kend - a.kbeg + zc - 1) / zc : 1);
   };
   auto bytes = [](int ft, int np, int zc) {
     return static_cast<size_t>(plain_slots(MODE, ft, np).n) * zc * kPlainThreads * sizeof(double);

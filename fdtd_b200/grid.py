@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_pml_model", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_step_half_part", "fdtd_copy_plane", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
            "fdtd_batch_info", "fdtd_batch_item_rows", "fdtd_batch_set_item_rows",
@@ -84,6 +84,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_prepare": [vp],
         "fdtd_step_static_scratch": [vp, i, vp],
         "fdtd_step_half": [vp, i, vp],
+        "fdtd_step_half_part": [vp, i, i, vp],
         "fdtd_copy_plane": [vp, i, i, vp, i, vp],
         "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
         "fdtd_add_source_box": [vp, i, i, ip, ip, dp, i],
@@ -275,6 +276,12 @@ class Grid:
 
     def step_half(self, phase: int, stream: Optional[int] = None) -> None:
         _check(load_library().fdtd_step_half(self.h, int(phase), ctypes.c_void_p(stream) if stream else None))
+
+    def step_half_part(self, phase: int, part: int, stream: Optional[int] = None) -> None:
+        """Part 0 or 1 of half step `phase`: the planes that read no ghost
+        plane, then the ghost-adjacent plane and the rest of the half step."""
+        _check(load_library().fdtd_step_half_part(self.h, int(phase), int(part),
+                                                  ctypes.c_void_p(stream) if stream else None))
 
     def copy_plane(self, name: str, k: int, dev_ptr: int, to_grid: bool, stream: Optional[int] = None) -> None:
         """Copy z plane k of component `name` ('Ex'..'Hz') between the grid and

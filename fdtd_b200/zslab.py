@@ -22,9 +22,15 @@ coordinates. Per cell the arithmetic is that of the single grid, so the
 decomposed run reproduces it to the last bit.
 
 Two drivers share the slicing: `ZSlabDomain` keeps every range in one process
-(on one device, halos copied in stream order, no kernel ever waits on
-another), and `ZSlabRank` is one range per process, with the ghost planes
-sent over torch.distributed (NCCL between GPUs, gloo on CPU).
+(on one device; no kernel ever waits on another), and `ZSlabRank` is one range
+per process, with the ghost planes sent over torch.distributed (NCCL between
+GPUs, gloo on CPU).
+
+Both overlap the transfer of a ghost plane with the sweep, through the split
+half step of the C ABI (fdtd_step_half_part): part 0 of a half step sweeps
+every plane whose update reads no ghost plane while the planes travel; once
+they have landed, part 1 sweeps the plane next to the ghost and finishes the
+half step. Per cell the arithmetic is unchanged.
 """
 from __future__ import annotations
 
@@ -163,7 +169,10 @@ def merge_dfts(p: P.Problem, parts: Sequence[Tuple[List[int], List[np.ndarray]]]
 class ZSlabDomain:
     """Every z range of one grid in this process, on one device: the
     decomposed run on a single GPU (or as a check of the decomposition). The
-    ghost planes are copied between the ranges' grids in stream order."""
+    sweeps run on one stream and the ghost-plane copies on a second one, so
+    that each half step's copies overlap the slabs' interior sweeps (part 0);
+    events order the copies after the half step that produced their planes
+    and the ghost-adjacent sweeps (part 1) after the copies."""
 
     def __init__(self, p: P.Problem, world: int, precision: str = "f32", device: int = 0):
         import torch
@@ -175,34 +184,45 @@ class ZSlabDomain:
         nx, ny, _ = p.shape
         dtype = torch.float32 if precision in ("f32", "fused") else torch.float64
         self.torch = torch
-        self.buf = torch.empty(nx * ny, dtype=dtype, device=f"cuda:{device}")
-        # one stream for every slab's kernels and every ghost-plane copy, so
-        # that they run in the order issued (a grid given no stream would use
-        # its own)
+        # one buffer per slab boundary and component, so that copies of one
+        # half step never wait for one another
+        nb = max(0, len(self.grids) - 1) * 2
+        self.bufs = [torch.empty(nx * ny, dtype=dtype, device=f"cuda:{device}") for _ in range(max(1, nb))]
         self.stream_obj = torch.cuda.Stream(device)
+        self.copy_obj = torch.cuda.Stream(device)
         self.stream = self.stream_obj.cuda_stream
+        self.copy_stream = self.copy_obj.cuda_stream
         self.stream_obj.wait_stream(torch.cuda.current_stream(device))
+        self.copy_obj.wait_stream(torch.cuda.current_stream(device))
 
     def _halo(self, names, up: bool):
+        """The ghost-plane copies of one half step on the copy stream."""
         n = len(self.grids)
         for r in range(n - 1):
             lower, upper = self.grids[r], self.grids[r + 1]
-            for name in names:
+            for c, name in enumerate(names):
+                buf = self.bufs[2 * r + c].data_ptr()
                 if up:  # lower's top owned plane -> upper's ghost plane 0
-                    lower.copy_plane(name, lower.shape[2] - 2, self.buf.data_ptr(), False, self.stream)
-                    upper.copy_plane(name, 0, self.buf.data_ptr(), True, self.stream)
+                    lower.copy_plane(name, lower.shape[2] - 2, buf, False, self.copy_stream)
+                    upper.copy_plane(name, 0, buf, True, self.copy_stream)
                 else:  # upper's first owned plane -> lower's top ghost plane
-                    upper.copy_plane(name, 1, self.buf.data_ptr(), False, self.stream)
-                    lower.copy_plane(name, lower.shape[2] - 1, self.buf.data_ptr(), True, self.stream)
+                    upper.copy_plane(name, 1, buf, False, self.copy_stream)
+                    lower.copy_plane(name, lower.shape[2] - 1, buf, True, self.copy_stream)
+
+    def _half(self, phase: int, names, up: bool):
+        # the planes to send are final once the previous half step has run
+        self.copy_obj.wait_stream(self.stream_obj)
+        self._halo(names, up)
+        for g in self.grids:
+            g.step_half_part(phase, 0, self.stream)
+        self.stream_obj.wait_stream(self.copy_obj)
+        for g in self.grids:
+            g.step_half_part(phase, 1, self.stream)
 
     def step(self, n: int) -> None:
         for _ in range(n):
-            self._halo(H_HALO, up=True)
-            for g in self.grids:
-                g.step_half(0, self.stream)
-            self._halo(E_HALO, up=False)
-            for g in self.grids:
-                g.step_half(1, self.stream)
+            self._half(0, H_HALO, up=True)
+            self._half(1, E_HALO, up=False)
 
     def get(self, name: str) -> np.ndarray:
         """The global field assembled from the ranges' owned planes."""
@@ -218,16 +238,20 @@ class ZSlabDomain:
 class ZSlabRank:
     """One z range per process (one process per GPU): this rank's grid and
     the exchange of its ghost planes with the ranks above and below over
-    torch.distributed (NCCL between GPUs; gloo with CPU tensors). `grid` is
-    anything with step_half(phase), read_plane(name, k) -> tensor and
-    write_plane(name, k, tensor) and the local problem's shape."""
+    torch.distributed (NCCL between GPUs; gloo with CPU tensors). Each half
+    step posts the plane transfers, runs the interior part of the sweep,
+    waits for the transfers, writes the ghost plane and runs the rest. `grid`
+    is anything with step_half_part(phase, part), read_plane(name, k) ->
+    tensor, write_plane(name, k, tensor) and empty_plane()."""
 
     def __init__(self, grid, nz_local: int, rank: int, world: int, group=None):
         self.g = grid
         self.nzl = nz_local
         self.rank, self.world, self.group = rank, world, group
 
-    def _exchange(self, names, up: bool):
+    def _post(self, names, up: bool):
+        """Send this rank's planes of `names` and request the neighbour's:
+        the transfers run while the interior sweep does."""
         import torch.distributed as dist
         peer_send = self.rank + 1 if up else self.rank - 1
         peer_recv = self.rank - 1 if up else self.rank + 1
@@ -241,20 +265,30 @@ class ZSlabRank:
                 buf = self.g.empty_plane()
                 reqs.append(dist.irecv(buf, peer_recv, group=self.group))
                 recvd.append((name, buf))
+        return reqs, recvd, k_recv
+
+    def _land(self, pending):
+        """Wait for the transfers and write the received planes into the
+        ghost plane."""
+        reqs, recvd, k_recv = pending
         for r in reqs:
             r.wait()
         for name, buf in recvd:
             self.g.write_plane(name, k_recv, buf)
+
+    def _half(self, phase: int, names, up: bool):
+        pending = self._post(names, up)
+        self.g.step_half_part(phase, 0)
+        self._land(pending)
+        self.g.step_half_part(phase, 1)
 
     def step(self, n: int) -> None:
         import contextlib
         ctx = self.g.stream_context() if hasattr(self.g, "stream_context") else contextlib.nullcontext()
         with ctx:
             for _ in range(n):
-                self._exchange(H_HALO, up=True)
-                self.g.step_half(0)
-                self._exchange(E_HALO, up=False)
-                self.g.step_half(1)
+                self._half(0, H_HALO, up=True)
+                self._half(1, E_HALO, up=False)
 
 
 class GpuSlab:
@@ -295,3 +329,6 @@ class GpuSlab:
 
     def step_half(self, phase):
         self.grid.step_half(phase, self._stream())
+
+    def step_half_part(self, phase, part):
+        self.grid.step_half_part(phase, part, self._stream())

@@ -222,6 +222,16 @@ int fdtd_step(fdtd_grid* g, int nsteps, void* stream);
  * z-slab decomposition (the reference does the same between its E and H
  * functors across MPI ranks, BoundaryUpdates.hpp:919-1051). Launched eagerly. */
 int fdtd_step_half(fdtd_grid* g, int phase, void* stream);
+/* The half step `phase` in two parts (3D grids), so that a ghost plane can
+ * travel while the sweep runs: part 0 sweeps every plane whose update reads
+ * no ghost plane -- for the E half planes 2 .. nz-2 (plane 1 reads H of plane
+ * 0), for the H half planes 1 .. nz-3 (plane nz-2 reads E of plane nz-1) --
+ * and part 1, called once plane 0 (E half) or plane nz-1 (H half) holds the
+ * neighbour's values, sweeps the remaining plane and runs the rest of the
+ * half step. Parts 0 then 1 give exactly fdtd_step_half's results; other
+ * calls on the grid between them are refused. FP32 grids need the staged
+ * sweeps (FDTD_SWEEP_AUTO or FDTD_SWEEP_STAGED). Launched eagerly. */
+int fdtd_step_half_part(fdtd_grid* g, int phase, int part, void* stream);
 /* Copy z plane k of a stored component (FDTD_EX..FDTD_EZ, FDTD_HX..FDTD_HZ)
  * between the grid and a compact device buffer of nx*ny values of the grid's
  * precision, x fastest (to_grid = 1: buffer to grid). The FP32 method stores

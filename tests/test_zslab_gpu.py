@@ -1,8 +1,10 @@
 """Z-slab decomposition on the GPU: every slab of the grid in this process on
-one device (ZSlabDomain: fdtd_step_half for the halves, fdtd_copy_plane for
-the ghost planes, all in one stream, so no kernel ever waits on another). The
+one device (ZSlabDomain: fdtd_step_half_part for the halves, the ghost planes
+copied with fdtd_copy_plane on a second stream while the interior parts of
+the sweeps run; events order them, no kernel ever waits on another). The
 assembled fields and spectra must equal those of the single grid stepped with
-fdtd_step, bit for bit, for both methods."""
+fdtd_step, bit for bit, for both methods; so must a single grid stepped in
+split half steps."""
 import numpy as np
 import pytest
 
@@ -45,3 +47,44 @@ def test_half_steps_must_alternate(fdtd):
     g.step_half(1)
     g.step(3)
     assert g.step_count == 4
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("make", [scenarios.td_tfsf_box, scenarios.td_box_sources, scenarios.td_boundaries,
+                                  scenarios.td_lorentz_two_pole_blocks], ids=lambda f: f.__name__)
+def test_split_half_steps_equal_the_step(fdtd, make, prec):
+    """fdtd_step_half_part: part 0 (planes that read no ghost plane) then
+    part 1 (the plane next to it, and the rest of the half step) of both
+    halves give fdtd_step's fields and spectra bit for bit."""
+    p = make()
+    ref = fdtd.Grid.from_problem(p, prec)
+    ref.step(p.steps)
+    g = fdtd.Grid.from_problem(p, prec)
+    for _ in range(p.steps):
+        for phase in (0, 1):
+            g.step_half_part(phase, 0)
+            g.step_half_part(phase, 1)
+    assert g.step_count == p.steps
+    for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert np.array_equal(g.get(n), ref.get(n)), n
+    for q in range(len(p.dfts)):
+        assert np.array_equal(g.dft(q), ref.dft(q)), q
+
+
+def test_split_half_steps_are_ordered(fdtd):
+    p = scenarios.td_tfsf_box()
+    g = fdtd.Grid.from_problem(p, "f32")
+    with pytest.raises(fdtd.FdtdError):
+        g.step_half_part(0, 1)  # part 1 before part 0
+    g.step_half_part(0, 0)
+    for bad in (lambda: g.step_half(0), lambda: g.step(1), lambda: g.step_half_part(0, 0),
+                lambda: g.step_half_part(1, 0)):
+        with pytest.raises(fdtd.FdtdError):
+            bad()
+    g.step_half_part(0, 1)
+    g.step_half(1)
+    assert g.step_count == 1
+    tm = fdtd.Grid.from_problem(scenarios.tm_cpml_sources(), "f32")
+    with pytest.raises(fdtd.FdtdError) as e:
+        tm.step_half_part(0, 0)  # 2D grids have no z planes to split
+    assert e.value.code == -3
