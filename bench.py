@@ -94,6 +94,10 @@ def parse():
     ap.add_argument("--batch-mode", default="tune", choices=["tune", "persistent", "per_phase"],
                     help="batch64: autotune, or force a launch mode (with --batch-rows)")
     ap.add_argument("--batch-rows", type=int, default=4, choices=[1, 2, 4, 8])
+    ap.add_argument("--decompose", default="replicas", choices=["replicas", "zslab"],
+                    help="single-grid workloads on N GPUs: independent replicas (weak scaling), or one grid cut "
+                         "into z slabs, one per rank, ghost planes over NCCL overlapped with the interior sweep "
+                         "(strong scaling)")
     ap.add_argument("--variant", default="none", choices=list(VARIANTS),
                     help="3D/2D grid workloads: measure a feature beside the hot path (see VARIANTS)")
     return ap.parse_args()
@@ -687,7 +691,8 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    line = run_grid(args, torch, world, rank, local, stream)
+    line = run_zslab(args, torch, world, rank, local) if args.decompose == "zslab" else \
+        run_grid(args, torch, world, rank, local, stream)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -720,6 +725,59 @@ def accuracy(g, g64, p, steps: int) -> dict:
             "fields_rel_l2": fields, "dft_rel_l2_max": max(dfts) if dfts else None,
             "dft_rel_l2": dfts if len(dfts) <= 8 else None, "worst": worst, "bound": 1e-4,
             "within_bound": bool(worst <= 1e-4)}
+
+
+def run_zslab(args, torch, world, rank, local):
+    """One grid of the workload cut into `world` z slabs, one per rank
+    (fdtd_b200/zslab.py): each half step sends the ghost planes over NCCL
+    while the interior part of the sweep runs (fdtd_step_half_part). value =
+    the global grid's interior cell-updates / max rank time; scaling strong."""
+    import torch.distributed as dist
+    from fdtd_b200.zslab import GpuSlab, ZSlabRank, local_problem, partition_z
+    p = make_problem(args.workload, args.steps + args.warmup, args.n, args.variant)
+    z0, z1 = partition_z(p, world)[rank]
+    q = local_problem(p, z0, z1)
+    slab = GpuSlab(q, "f32", device=local)
+    drv = ZSlabRank(slab, q.shape[2], rank, world)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    drv.step(args.warmup)
+    slab.synchronize()
+    barrier()
+    launches0 = slab.grid.launch_count
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(slab.stream)
+        drv.step(args.steps)
+        end.record(slab.stream)
+        slab.synchronize()
+        barrier()
+    ms = start.elapsed_time(end)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = p.interior_cells
+    ab = alg_bytes(p, 4)
+    peak, peak_kind = peaks()
+    step_ach = ab["step"] * args.steps / (ms_max / 1e3) / 1e9
+    return {
+        "metric": METRIC, "value": cells * args.steps / (ms_max / 1e3) / 1e9, "unit": "Gcell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": p.name, "grid": list(p.shape), "interior_cells": cells,
+                   "parallelism": f"z slabs x{world}", "slab_planes": [list(r) for r in partition_z(p, world)],
+                   "l2": "state larger than L2, no flush"},
+        "roofline": {"bound": "hbm", "scope": "whole step, all GPUs", "achieved": step_ach, "peak": peak * world,
+                     "unit": "GB/s", "frac": step_ach / (peak * world), "peak_kind": peak_kind,
+                     "alg_bytes_per_cell_step": ab["per_cell_step"], "traffic": None},
+        "e2e": None, "cpu_baseline": None, "gpu_launches": slab.grid.launch_count - launches0,
+        "clocks": clk.summary(),
+    }
 
 
 def run_grid(args, torch, world, rank, local, stream):
