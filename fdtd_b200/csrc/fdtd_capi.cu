@@ -1699,6 +1699,33 @@ int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, 
   return host_failure();
 }
 
+int fdtd_copy_plane_between(fdtd_grid* src, int which, int k_src, fdtd_grid* dst, int k_dst, void* stream) try {
+  if (!src || !dst) return fail(FDTD_ERR_INVALID, "null grid");
+  if (src->f32 != dst->f32 || src->d.mode != dst->d.mode || src->n[0] != dst->n[0] || src->n[1] != dst->n[1])
+    return fail(FDTD_ERR_INVALID, "the two grids differ in precision, mode or plane extent");
+  if (k_src < 0 || k_src >= src->n[2] || k_dst < 0 || k_dst >= dst->n[2])
+    return fail(FDTD_ERR_INVALID, "plane index out of range");
+  auto field = [&](fdtd_grid* g) -> void* {
+    if (which >= FDTD_EX && which <= FDTD_EZ) return g->E[which - FDTD_EX];
+    if (which >= FDTD_HX && which <= FDTD_HZ) return g->H[which - FDTD_HX];
+    return nullptr;
+  };
+  void* fs = field(src);
+  void* fd = field(dst);
+  if (!fs || !fd) return fail(FDTD_ERR_INVALID, "only the stored E and H components of the mode are copied");
+  CK(cudaSetDevice(dst->d.device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : dst->stream;
+  const size_t es = elem(src), row = static_cast<size_t>(rowlen(src)) * es, w = static_cast<size_t>(src->n[0]) * es;
+  const char* ps = static_cast<const char*>(fs) + static_cast<size_t>(k_src) * src->n[1] * row;
+  char* pd = static_cast<char*>(fd) + static_cast<size_t>(k_dst) * dst->n[1] * row;
+  // one strided copy; between devices the runtime routes it over the peer
+  // link (unified addressing), within one device it is a device copy
+  CK(cudaMemcpy2DAsync(pd, row, ps, row, w, src->n[1], cudaMemcpyDefault, s));
+  return FDTD_OK;
+} catch (...) {
+  return host_failure();
+}
+
 int fdtd_use_graphs(fdtd_grid* g, int enable) try {
   if (!g) return fail(FDTD_ERR_INVALID, "null grid");
   g->use_graphs = enable != 0;

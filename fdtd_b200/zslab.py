@@ -181,13 +181,7 @@ class ZSlabDomain:
         self.ranges = partition_z(p, world)
         self.parts = [local_problem(p, z0, z1) for z0, z1 in self.ranges]
         self.grids = [Grid.from_problem(q, precision, device=device) for q in self.parts]
-        nx, ny, _ = p.shape
-        dtype = torch.float32 if precision in ("f32", "fused") else torch.float64
         self.torch = torch
-        # one buffer per slab boundary and component, so that copies of one
-        # half step never wait for one another
-        nb = max(0, len(self.grids) - 1) * 2
-        self.bufs = [torch.empty(nx * ny, dtype=dtype, device=f"cuda:{device}") for _ in range(max(1, nb))]
         self.stream_obj = torch.cuda.Stream(device)
         self.copy_obj = torch.cuda.Stream(device)
         self.stream = self.stream_obj.cuda_stream
@@ -196,18 +190,16 @@ class ZSlabDomain:
         self.copy_obj.wait_stream(torch.cuda.current_stream(device))
 
     def _halo(self, names, up: bool):
-        """The ghost-plane copies of one half step on the copy stream."""
+        """The ghost-plane copies of one half step on the copy stream, plane
+        to plane (fdtd_copy_plane_between)."""
         n = len(self.grids)
         for r in range(n - 1):
             lower, upper = self.grids[r], self.grids[r + 1]
-            for c, name in enumerate(names):
-                buf = self.bufs[2 * r + c].data_ptr()
+            for name in names:
                 if up:  # lower's top owned plane -> upper's ghost plane 0
-                    lower.copy_plane(name, lower.shape[2] - 2, buf, False, self.copy_stream)
-                    upper.copy_plane(name, 0, buf, True, self.copy_stream)
+                    lower.copy_plane_to(name, lower.shape[2] - 2, upper, 0, self.copy_stream)
                 else:  # upper's first owned plane -> lower's top ghost plane
-                    upper.copy_plane(name, 1, buf, False, self.copy_stream)
-                    lower.copy_plane(name, lower.shape[2] - 1, buf, True, self.copy_stream)
+                    upper.copy_plane_to(name, 1, lower, lower.shape[2] - 1, self.copy_stream)
 
     def _half(self, phase: int, names, up: bool):
         # the planes to send are final once the previous half step has run

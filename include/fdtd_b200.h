@@ -237,6 +237,14 @@ int fdtd_step_half_part(fdtd_grid* g, int phase, int part, void* stream);
  * precision, x fastest (to_grid = 1: buffer to grid). The FP32 method stores
  * eta*H, and that is what is copied. Stream-ordered on `stream`. */
 int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, void* stream);
+/* Copy z plane k_src of a stored component of grid src straight into z plane
+ * k_dst of the same component of grid dst (same precision, mode and x-y
+ * extent; the same or another device, a peer copy then), on `stream` (NULL =
+ * dst's stream) -- a ghost-plane exchange between two slabs held by one
+ * process, with no staging buffer (the reference's MPI boundary exchange,
+ * BoundaryUpdates.hpp:919-1051, between two ranks). The caller orders it after
+ * the half step that wrote the source plane. */
+int fdtd_copy_plane_between(fdtd_grid* src, int which, int k_src, fdtd_grid* dst, int k_dst, void* stream);
 /* Lays out the device state that the set-up calls defer: the CPML
  * coefficient profiles and integrator slabs (fdtd_set_pml regrades on the
  * host only) and the DFT sample buffers. fdtd_step and fdtd_step_half do it

@@ -1,6 +1,6 @@
 """Z-slab decomposition on the GPU: every slab of the grid in this process on
 one device (ZSlabDomain: fdtd_step_half_part for the halves, the ghost planes
-copied with fdtd_copy_plane on a second stream while the interior parts of
+copied plane to plane with fdtd_copy_plane_between on a second stream while the interior parts of
 the sweeps run; events order them, no kernel ever waits on another). The
 assembled fields and spectra must equal those of the single grid stepped with
 fdtd_step, bit for bit, for both methods; so must a single grid stepped in
@@ -88,3 +88,25 @@ def test_split_half_steps_are_ordered(fdtd):
     with pytest.raises(fdtd.FdtdError) as e:
         tm.step_half_part(0, 0)  # 2D grids have no z planes to split
     assert e.value.code == -3
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_plane_copy_between_grids(fdtd, prec):
+    """fdtd_copy_plane_between moves exactly one z plane of one component."""
+    p = scenarios.td_tfsf_box()
+    a = fdtd.Grid.from_problem(p, prec)
+    b = fdtd.Grid.from_problem(p, prec)
+    a.step(7)
+    a.synchronize()
+    a.copy_plane_to("Hy", 5, b, 9)
+    b.synchronize()
+    got, src = b.get("Hy"), a.get("Hy")
+    assert np.array_equal(got[9], src[5])
+    got[9] = 0.0
+    assert not np.any(got)
+    assert not np.any(b.get("Hx"))
+    c = fdtd.Grid.from_problem(scenarios.td_drude_lorentz(), prec)  # another x-y extent
+    with pytest.raises(fdtd.FdtdError):
+        a.copy_plane_to("Hy", 5, c, 3)
+    with pytest.raises(fdtd.FdtdError):
+        a.copy_plane_to("Hy", 99, b, 3)
