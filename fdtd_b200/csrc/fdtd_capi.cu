@@ -461,6 +461,10 @@ int build_materials(fdtd_grid* g) {
       // VacuumStorage K = 1 (DispersiveMaterials.hpp:446-457)
       o.den_e = (m.kind == FDTD_VACUUM ? 1.0 : m.eps_inf) * kEps0;
       o.den_h = m.mu_r * kMu0;
+      for (int p = 0; p < o.npoles; p++) {
+        o.freq[p] = m.freq[p];
+        o.gamma[p] = m.gamma[p];
+      }
       if (m.kind == FDTD_DRUDE) {
         // drude::DrudeUpdate::implicit_update (DispersiveMaterials.hpp:986-996)
         const double b = m.gamma[0] * dt * 0.5;
@@ -1674,6 +1678,30 @@ int fdtd_step_half(fdtd_grid* g, int phase, void* stream) try {
 int fdtd_step_half_part(fdtd_grid* g, int phase, int part, void* stream) try {
   if (part != 0 && part != 1) return fail(FDTD_ERR_INVALID, "part must be 0 or 1");
   return half_step_impl(g, phase, part, stream);
+} catch (...) {
+  return host_failure();
+}
+
+// The reference's forward (explicit) material updates, XUpdate<Mode, ft,
+// forward = true> (DispersiveMaterials.hpp:345-349, :922-934): the flux (and
+// the Drude P and J) from the field, on every interior cell. Only the FP64
+// plain method stores D and B; the reference's explicit Lorentz update is a
+// static_assert (:697-706), so grids with a Lorentz material refuse ft 0.
+int fdtd_material_explicit(fdtd_grid* g, int ft, void* stream) try {
+  if (!g) return fail(FDTD_ERR_INVALID, "null grid");
+  if (ft != 0 && ft != 1) return fail(FDTD_ERR_INVALID, "ft must be 0 (electric) or 1 (magnetic)");
+  if (g->f32) return fail(FDTD_ERR_UNSUPPORTED, "the FP32 fused method stores no D or B");
+  if (g->half_split) return fail(FDTD_ERR_INVALID, "part 0 of this half step is waiting for its part 1");
+  if (ft == 0)
+    for (const fdtd_material& m : g->mats)
+      if (m.kind == FDTD_LORENTZ) return fail(FDTD_ERR_UNSUPPORTED, "the reference has no explicit Lorentz update");
+  CK(cudaSetDevice(g->d.device));
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  if (s != g->stream) CK(cudaStreamSynchronize(g->stream));
+  const PlainArgs pa = plain_args(g);
+  g->launches += launch_material_explicit(g->d.mode, pa, ft, s);
+  CK(cudaGetLastError());
+  return FDTD_OK;
 } catch (...) {
   return host_failure();
 }

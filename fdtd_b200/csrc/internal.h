@@ -80,6 +80,8 @@ struct MatF64 {
   // Drude: c1 = 1-b, c2 = 1+b, c3 = ((w*w)/dt)*eps0
   // Lorentz: c1 = bm/b, c2 = ((q*delta)*eps0), c3 = q = (freq*w)/b
   double c1[kMaxPoles], c2[kMaxPoles], c3[kMaxPoles];
+  // the storage's own values, for the forward (explicit) updates
+  double freq[kMaxPoles], gamma[kMaxPoles];
 };
 
 // Material coefficients for the FP32 fused method (scaled variables)
@@ -229,6 +231,8 @@ struct AdjArgs {
 // kernel launchers (stream-ordered); each returns the number of launches
 int launch_plain_e(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
+// the forward material updates of field type ft on every interior cell
+int launch_material_explicit(int mode, const PlainArgs& a, int ft, cudaStream_t s);
 int launch_fused_e(int mode, const FusedArgs& a, cudaStream_t s);
 int launch_fused_h(int mode, const FusedArgs& a, cudaStream_t s);
 bool fused3d_supported(const FusedArgs& a);

@@ -712,6 +712,62 @@ int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s) {
 }
 
 // ----------------------------------------------------------------------------
+// The forward (explicit) material updates, XUpdate<Mode, ft, forward = true>:
+// the flux from the field on every interior cell. Electric: ConstantUpdate
+// and VacuumUpdate D = (K*eps0)*E (DispersiveMaterials.hpp:345-349), Drude
+// P = (-dt*J + (1+b)*P)/(1+b), J = (J - c*E)/(1+b), D = (K*eps0)*E + P with
+// b = gamma*dt and c = ((dt*w)*w)*eps0 (:922-934). Magnetic: B = (mu_r*mu0)*H.
+// Components in the order nested_for_each_tuple_type visits them (z, y, x).
+template <int MODE>
+__global__ void material_explicit_kernel(const __grid_constant__ PlainArgs a, int ft) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = MODE == kThreeD ? 1 + static_cast<int>(blockIdx.z) : 0;
+  if (i > a.nx - 2 || j > a.ny - 2) return;
+  const long long c = (static_cast<long long>(k) * a.ny + j) * a.nx + i;
+  int mid = 0;
+  if (a.ids) mid = a.ids[c];
+  else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  const MatF64& m = a.mats[mid];
+  if (ft == 1) {
+#pragma unroll
+    for (int I = 2; I >= 0; I--)
+      if (hasH(MODE, I)) a.B.f[I][c] = m.den_h * a.H.f[I][c];
+    return;
+  }
+  const double eps_cell = a.eps_map ? a.eps_map[c] : 0.0;
+  const double dt = a.dt;
+#pragma unroll
+  for (int I = 2; I >= 0; I--) {
+    if (!hasE(MODE, I)) continue;
+    const double E = a.E.f[I][c];
+    if (m.kind <= 1) {
+      const double den = (a.eps_map && eps_cell > 0.0) ? eps_cell * kEps0 : m.den_e;
+      a.D.f[I][c] = den * E;
+    } else {
+      const double b = m.gamma[0] * dt;
+      const double cc = dt * m.freq[0] * m.freq[0] * kEps0;
+      const double P = a.P[0].f[I][c], Jc = a.J[0].f[I][c];
+      const double Pn = (-dt * Jc + (1.0 + b) * P) / (1.0 + b);
+      a.P[0].f[I][c] = Pn;
+      a.J[0].f[I][c] = (Jc - cc * E) / (1.0 + b);
+      a.D.f[I][c] = m.den_e * E + Pn;
+    }
+  }
+}
+
+int launch_material_explicit(int mode, const PlainArgs& a, int ft, cudaStream_t s) {
+  const dim3 block(32, 8, 1);
+  const dim3 grid((a.nx - 2 + 31) / 32, (a.ny - 2 + 7) / 8, mode == kThreeD ? a.nz - 2 : 1);
+  switch (mode) {
+    case kTE: material_explicit_kernel<kTE><<<grid, block, 0, s>>>(a, ft); break;
+    case kTM: material_explicit_kernel<kTM><<<grid, block, 0, s>>>(a, ft); break;
+    default: material_explicit_kernel<kThreeD><<<grid, block, 0, s>>>(a, ft); break;
+  }
+  return 1;
+}
+
+// ----------------------------------------------------------------------------
 // Aux1D::time_step (include/Source.hpp:413-435) advanced nsteps times by one
 // CTA, writing Ez and Hy after every step into the tables (row 0 = the state
 // on entry). coef holds the aux CPML profile: [ft][B,Cdx,Fdx,G][L].

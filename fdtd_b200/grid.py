@@ -32,7 +32,7 @@ STATUS = {0: "FDTD_OK", -1: "FDTD_ERR_INVALID", -2: "FDTD_ERR_CUDA", -3: "FDTD_E
 # every symbol include/fdtd_b200.h declares
 EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_pml_model", "fdtd_set_materials", "fdtd_set_material_ids",
            "fdtd_set_material_blocks", "fdtd_set_eps_map", "fdtd_set_boundary", "fdtd_set_time_scheme", "fdtd_add_source", "fdtd_add_source_box", "fdtd_add_tfsf_plane", "fdtd_add_dft",
-           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_step_half_part", "fdtd_copy_plane", "fdtd_copy_plane_between", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
+           "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_step_half_part", "fdtd_copy_plane", "fdtd_copy_plane_between", "fdtd_material_explicit", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
            "fdtd_batch_info", "fdtd_batch_item_rows", "fdtd_batch_set_item_rows",
@@ -87,6 +87,7 @@ def load_library(path: str = LIB_PATH):
         "fdtd_step_half_part": [vp, i, i, vp],
         "fdtd_copy_plane": [vp, i, i, vp, i, vp],
         "fdtd_copy_plane_between": [vp, i, i, vp, i, vp],
+        "fdtd_material_explicit": [vp, i, vp],
         "fdtd_add_source": [vp, i, i, i, i, i, dp, i],
         "fdtd_add_source_box": [vp, i, i, ip, ip, dp, i],
         "fdtd_add_tfsf_plane": [vp, i, i, ip, ip, dp, dp, dp, dp, i, dp, i],
@@ -296,6 +297,11 @@ class Grid:
         which = FIELD_NAMES.index(name)
         _check(load_library().fdtd_copy_plane_between(self.h, which, int(k), dst.h, int(k_dst),
                                                       ctypes.c_void_p(stream) if stream else None))
+
+    def material_explicit(self, ft: int, stream: Optional[int] = None) -> None:
+        """The forward material updates of field type ft (0 electric: D, and
+        the Drude P and J, from E; 1 magnetic: B from H). FP64 grids."""
+        _check(load_library().fdtd_material_explicit(self.h, int(ft), ctypes.c_void_p(stream) if stream else None))
 
     def step_static_scratch(self, n: int, stream: Optional[int] = None) -> None:
         """step() that allocates no device memory: the TFSF table of the call

@@ -245,6 +245,15 @@ int fdtd_copy_plane(fdtd_grid* g, int which, int k, void* dev_buf, int to_grid, 
  * BoundaryUpdates.hpp:919-1051, between two ranks). The caller orders it after
  * the half step that wrote the source plane. */
 int fdtd_copy_plane_between(fdtd_grid* src, int which, int k_src, fdtd_grid* dst, int k_dst, void* stream);
+/* The reference's forward (explicit) material updates of field type ft
+ * (0 electric, 1 magnetic) on every interior cell, XUpdate<Mode, ft,
+ * forward = true> (DispersiveMaterials.hpp:345-349, :922-934): D = eps*E
+ * (VacuumUpdate, ConstantUpdate, the eps map), for Drude cells P and J
+ * advanced explicitly and D = eps_inf*eps0*E + P; B = mu_r*mu0*H. FP64 grids
+ * only (FDTD_ERR_UNSUPPORTED on FP32, which stores no D or B); grids with a
+ * Lorentz material refuse ft 0, as the reference's explicit Lorentz update is
+ * a static_assert (:697-706). Stream-ordered on `stream` (NULL = the grid's). */
+int fdtd_material_explicit(fdtd_grid* g, int ft, void* stream);
 /* Lays out the device state that the set-up calls defer: the CPML
  * coefficient profiles and integrator slabs (fdtd_set_pml regrades on the
  * host only) and the DFT sample buffers. fdtd_step and fdtd_step_half do it

@@ -168,7 +168,7 @@ struct UpdatePML {
 // Material updates (include/DispersiveMaterials.hpp:489-497, :881-884, :1208-1211)
 template <class Mode, FieldType ft, bool forward = false>
 struct VacuumUpdate {
-  static_assert(!forward, "only the implicit (forward = false) update is on the GPU path");
+  static_assert(!forward, "a plan takes the implicit updates; Grid::apply_forward_materials runs the forward ones");
   operator detail::Op() const {
     detail::Op o{detail::OpKind::Material};
     o.ft = ft;
@@ -178,7 +178,7 @@ struct VacuumUpdate {
 };
 template <class Mode, FieldType ft, bool forward = false>
 struct ConstantUpdate {
-  static_assert(!forward, "only the implicit (forward = false) update is on the GPU path");
+  static_assert(!forward, "a plan takes the implicit updates; Grid::apply_forward_materials runs the forward ones");
   double K;
   explicit ConstantUpdate(double k) : K(k) {}
   operator detail::Op() const {
@@ -192,7 +192,8 @@ struct ConstantUpdate {
 };
 template <class Mode, FieldType ft, bool forward = false>
 struct DrudeUpdate {
-  static_assert(ft == FieldType::Electric && !forward, "Drude acts on the electric field, implicitly");
+  static_assert(ft == FieldType::Electric && !forward,
+                "Drude acts on the electric field, implicitly in a plan (Grid::apply_forward_materials runs the forward one)");
   double K, Freq, Gamma;
   DrudeUpdate(double k, double freq, double gamma, double /*dt*/ = 0) : K(k), Freq(freq), Gamma(gamma) {}
   operator detail::Op() const {
@@ -506,6 +507,14 @@ class Grid {
     if (steps_ + n > max_steps_) throw Error(FDTD_ERR_INVALID, "more steps than the grid was created for");
     check(fdtd_step(g_.get(), n, nullptr));
     steps_ += n;
+  }
+
+  // The forward (explicit) material updates, XUpdate<Mode, ft, forward = true>
+  // (include/DispersiveMaterials.hpp:345-349, :922-934), of the grid's
+  // material table on every interior cell: D (and the Drude P, J) from E, or
+  // B from H. FP64 grids; no Lorentz material for FieldType::Electric.
+  void apply_forward_materials(FieldType ft) {
+    check(fdtd_material_explicit(g_.get(), static_cast<int>(ft), nullptr));
   }
 
   template <class F>

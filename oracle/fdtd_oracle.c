@@ -858,6 +858,49 @@ int oracle_step(oracle_grid* g, int nsteps) {
   return 0;
 }
 
+/* The forward (explicit) material updates, XUpdate<Mode, ft, forward = true>
+   (DispersiveMaterials.hpp:345-349 constant and vacuum, :922-934 Drude): the
+   flux -- and the Drude P and J -- from the field, on every interior cell.
+   The reference's Lorentz explicit update is a static_assert (:697-706):
+   grids with a Lorentz material are refused (-2). */
+int oracle_material_explicit(oracle_grid* g, int ft) {
+  if (ft != 0 && ft != 1) return -1;
+  for (int q = 0; q < g->nmat; q++)
+    if (ft == 0 && g->mats[q].kind == OR_LORENTZ) return -2;
+  const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const int k0 = g->mode == THREED ? 1 : 0, k1 = g->mode == THREED ? nz - 2 : 0;
+  const double dt = g->dt;
+  for (int k = k0; k <= k1; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        size_t c = k * sz + j * sy + i;
+        const oracle_material* m = &g->mats[g->ids ? g->ids[c] : 0];
+        for (int I = 2; I >= 0; I--) {
+          if (ft == 1) {
+            if (g->hasH[I]) g->B[I][c] = m->mu_r * K_MU0 * g->H[I][c];
+            continue;
+          }
+          if (!g->hasE[I]) continue;
+          const double E = g->E[I][c];
+          if (m->kind <= OR_CONSTANT) {
+            const double K = (g->eps_map && g->eps_map[c] > 0.0) ? g->eps_map[c]
+                             : (m->kind == OR_VACUUM ? 1.0 : m->eps_inf);
+            g->D[I][c] = K * k_eps0 * E;
+          } else { /* Drude */
+            double* P = &g->P[0][I][c];
+            double* Jc = &g->J[0][I][c];
+            double b = m->gamma[0] * dt;
+            double cc = dt * m->freq[0] * m->freq[0] * k_eps0;
+            *P = (-dt * *Jc + (1.0 + b) * *P) / (1.0 + b);
+            *Jc = (*Jc - cc * E) / (1.0 + b);
+            g->D[I][c] = m->eps_inf * k_eps0 * E + *P;
+          }
+        }
+      }
+  return 0;
+}
+
 int oracle_step_half(oracle_grid* g, int phase) {
   if (phase != 0 && phase != 1) return -1;
   step_half(g, phase);

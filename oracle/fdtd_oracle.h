@@ -36,6 +36,9 @@ void oracle_destroy(oracle_grid* g);
 /* CPML of `ncells` on one side (0 = min, 1 = max) of `axis`, graded with
  * PMLParameterModel(dx) (include/PML.hpp:368-393). */
 int oracle_set_pml(oracle_grid* g, int axis, int side, int ncells);
+/* the forward (explicit) material updates of field type ft (0 electric, 1
+   magnetic) on every interior cell; -2 with a Lorentz material */
+int oracle_material_explicit(oracle_grid* g, int ft);
 /* the same side graded with PMLParameterModel(m, ma, sMax, kMax, aMax) */
 int oracle_set_pml_model(oracle_grid* g, int axis, int side, int ncells, double m, double ma, double smax,
                          double kmax, double amax);

@@ -82,6 +82,7 @@ def lib():
         L.oracle_add_dft.argtypes = [vp, ctypes.c_int, ip, ip, dp, ctypes.c_int]
         L.oracle_step.argtypes = [vp, ctypes.c_int]
         L.oracle_step_half.argtypes = [vp, ctypes.c_int]
+        L.oracle_material_explicit.argtypes = [vp, ctypes.c_int]
         L.oracle_set_boundary.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_set_time_scheme.argtypes = [vp, ctypes.c_int]
         L.oracle_get.argtypes = [vp, ctypes.c_int, dp]
@@ -191,6 +192,12 @@ class OracleGrid:
     def step_half(self, phase: int) -> None:
         assert lib().oracle_step_half(self.h, phase) == 0
 
+    def material_explicit(self, ft: int) -> None:
+        """The forward material updates (flux from field) of field type ft."""
+        rc = lib().oracle_material_explicit(self.h, int(ft))
+        if rc != 0:
+            raise ValueError("no forward material update for this grid (a Lorentz material)")
+
     def get_plane(self, name: str, k: int) -> np.ndarray:
         return self.get(name)[k].copy()
 
@@ -281,9 +288,11 @@ def reference_available() -> bool:
     return os.path.exists(RUNNER_PATH)
 
 
-def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
+def run_reference(p, steps: Optional[int] = None, explicit: bool = False) -> Dict[str, np.ndarray]:
     """Run the reference's own functors on the same Problem; returns every
-    output array by name (shape (nz, ny, nx))."""
+    output array by name (shape (nz, ny, nx)). explicit: after the steps, the
+    reference's forward material updates (XUpdate<Mode, ft, true>) of the
+    electric and then the magnetic field on every interior cell."""
     if not reference_available():
         raise RuntimeError("oracle/_ref/ref_runner is not built")
     steps = p.steps if steps is None else steps
@@ -337,6 +346,8 @@ def run_reference(p, steps: Optional[int] = None) -> Dict[str, np.ndarray]:
                 lines.append(f"{a} {sd} {BOUNDARY_KINDS[kind]}")
         if p.time_scheme != 1:
             lines.append(f"scheme {p.time_scheme}")
+        if explicit:
+            lines.append("explicit 1")
         lines.append(f"steps {steps}")
         op = os.path.join(td, "out.bin")
         lines.append(f"out {op}")

@@ -26,6 +26,8 @@
 //   dims nx ny nz
 //   dxdt dx dt
 //   pml nlo_x nhi_x nlo_y nhi_y nlo_z nhi_z
+//   explicit 1                    (optional: after the steps, the forward material
+//                                 updates XUpdate<Mode, ft, true>, E then H)
 //   pmlmodel axis side m ma sMax kMax aMax   (optional, per side: grade it with
 //                                 PMLParameterModel(m, ma, sMax, kMax, aMax))
 //   nmat M  then M lines: kind K delta freq gamma mu_r
@@ -94,6 +96,7 @@ struct Scenario {
   double dx = 1, dt = 1;
   int pml[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   // per side: 0 = PMLParameterModel(dx), 1 = PMLParameterModel(m, ma, sMax, kMax, aMax)
+  int explicit_after = 0;  // after the steps, the forward material updates (flux from field)
   int pml_custom[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   double pml_model[3][2][5] = {};
   std::vector<Mat> mats;
@@ -456,6 +459,23 @@ static int run(Scenario& s) {
 
   const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - clock0).count();
   printf("loop_seconds %.9f\n", loop_s);
+  if (s.explicit_after) {
+    // the reference's forward material functors, XUpdate<Mode, ft, true>
+    // (DispersiveMaterials.hpp:489-497, :1208-1211): flux from field
+    std::vector<std::function<void(C&)>> eexp, hexp;
+    for (auto& m : s.mats) {
+      switch (m.kind) {
+        case 0: { VacuumUpdate<Mode, FieldType::Electric, true> u; eexp.push_back([u](C& c) mutable { u(c); }); break; }
+        case 1: { ConstantUpdate<Mode, FieldType::Electric, true> u(m.K); eexp.push_back([u](C& c) mutable { u(c); }); break; }
+        case 2: { DrudeUpdate<Mode, FieldType::Electric, true> u(m.K, m.freq, m.gamma, dt); eexp.push_back([u](C& c) mutable { u(c); }); break; }
+        default: fprintf(stderr, "no forward update for this material kind\n"); return 5;
+      }
+      if (m.mu == 1.0) { VacuumUpdate<Mode, FieldType::Magnetic, true> u; hexp.push_back([u](C& c) mutable { u(c); }); }
+      else { ConstantUpdate<Mode, FieldType::Magnetic, true> u(m.mu); hexp.push_back([u](C& c) mutable { u(c); }); }
+    }
+    for (C* c : interior) eexp[matid(*c)](*c);
+    for (C* c : interior) hexp[matid(*c)](*c);
+  }
   {
     UpdateSurfaceChargeDensity<Mode> rho(dx);
     UpdateSurfaceCurrentE<Mode> je(dx);
@@ -519,6 +539,7 @@ int main(int argc, char** argv) {
     else if (key == "dims") in >> s.nx >> s.ny >> s.nz;
     else if (key == "dxdt") in >> s.dx >> s.dt;
     else if (key == "pml") for (int a = 0; a < 3; a++) in >> s.pml[a][0] >> s.pml[a][1];
+    else if (key == "explicit") in >> s.explicit_after;
     else if (key == "pmlmodel") {
       int a, sd;
       in >> a >> sd;

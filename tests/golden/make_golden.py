@@ -9,6 +9,11 @@ its headers (oracle/Makefile) -- and the final fields are stored as
 
 (with scenario names, only those scenarios' fixtures are rewritten)
 
+Each scenario of FORWARD_SCENARIOS, with its Lorentz materials replaced
+(scenarios.forward_materials), is run the same way and then the reference's
+forward material updates (XUpdate<Mode, ft, true>) of E and of H are applied
+to every interior cell: <name>_fwd.npz.
+
 It also writes config_*.xml: the reference's own XML writers (print_summary
 of MaterialMap, PMLOptions, BoundaryOptions) run on config_spec.txt by
 oracle/_ref/ref_xml, the fixtures of the config loaders.
@@ -60,6 +65,14 @@ def main(names=None):
         p = make()
         ref = pyoracle.run_reference(p)
         arrays = {k: ref[k] for k in KEEP + pyoracle.PSI_NAMES + pyoracle.SURFACE_NAMES if np.any(ref[k] != 0)}
+        np.savez_compressed(os.path.join(out_dir, p.name + ".npz"), steps=p.steps, **arrays)
+        print(p.name, sorted(arrays))
+    for make in scenarios.FORWARD_SCENARIOS:
+        p = scenarios.forward_materials(make)
+        if names and p.name not in names:
+            continue
+        ref = pyoracle.run_reference(p, explicit=True)
+        arrays = {k: ref[k] for k in KEEP + pyoracle.PSI_NAMES if np.any(ref[k] != 0)}
         np.savez_compressed(os.path.join(out_dir, p.name + ".npz"), steps=p.steps, **arrays)
         print(p.name, sorted(arrays))
 

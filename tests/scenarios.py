@@ -7,7 +7,7 @@ import math
 
 import numpy as np
 
-from fdtd_b200.problem import (CONSTANT, DRUDE, IMP0, TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion,
+from fdtd_b200.problem import (CONSTANT, DRUDE, IMP0, LORENTZ, TE, TM, THREED, TFSF, Material, Problem, Source, DFTRegion,
                                courant_dt, gaussian_pulse, ref_te_polarisation, ref_tm_polarisation, sinusoid,
                                tfsf_box_planes)
 
@@ -404,6 +404,22 @@ REFERENCE_SCENARIOS = [tm_cpml_sources, te_materials, td_drude_lorentz, tm_tfsf_
                        te_tfsf_oblique, td_tfsf_box, te_h_sources, td_h_sources, tm_line_source, td_box_sources,
                        tm_boundaries, te_boundaries, td_boundaries, tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf,
                        td_bd4_boundaries, tm_magnetic_tfsf, td_magnetic_tfsf, tm_cpml_model, td_cpml_model]
+# scenarios whose every material has a forward (explicit) update in the
+# reference, run with those updates applied after the steps
+# (forward_materials): each Lorentz material becomes a magnetic constant one
+FORWARD_SCENARIOS = [te_materials, td_drude_lorentz, tm_cpml_sources]
+
+
+def forward_materials(make) -> Problem:
+    """Scenario `make` with each Lorentz material replaced by a constant one of
+    the same eps_inf and mu_r 1.6 (the reference's explicit Lorentz update is a
+    static_assert), named <name>_fwd."""
+    p = make()
+    p.materials = [Material.constant(m.eps_inf, 1.6) if m.kind == LORENTZ else m for m in p.materials]
+    p.name += "_fwd"
+    return p
+
+
 # scenarios on the BD3/BD4 time policies (FP64 plain method only)
 MULTISTEP_SCENARIOS = [tm_bd3_tfsf, te_bd4_materials, td_bd3_tfsf, td_bd4_boundaries]
 ALL_SCENARIOS = REFERENCE_SCENARIOS + [td_lorentz_two_pole_blocks, td_surface_dft]

@@ -53,6 +53,40 @@ def test_oracle_matches_reference_runner_live(oracle):
             assert np.array_equal(g.get(n), ref[n]), f"{p.name}:{n}"
 
 
+@pytest.mark.parametrize("make", scenarios.FORWARD_SCENARIOS, ids=lambda f: f.__name__)
+def test_forward_material_updates_match_golden(oracle, make):
+    """The steps, then the forward (explicit) material updates of E and of H:
+    bit for bit the reference's XUpdate<Mode, ft, true> (<name>_fwd.npz)."""
+    p = scenarios.forward_materials(make)
+    gold = np.load(os.path.join(GOLDEN, p.name + ".npz"))
+    g = oracle.run_oracle(p)
+    g.material_explicit(0)
+    g.material_explicit(1)
+    for n in oracle.NAMES + oracle.PSI_NAMES:
+        want = gold[n] if n in gold.files else np.zeros_like(g.get(n))
+        assert np.array_equal(g.get(n), want), f"{p.name}:{n}"
+
+
+def test_forward_lorentz_update_is_refused(oracle):
+    g = oracle.run_oracle(scenarios.td_drude_lorentz(), 2)
+    with pytest.raises(ValueError):
+        g.material_explicit(0)
+    g.material_explicit(1)  # the magnetic side has no Lorentz material
+
+
+@pytest.mark.skipif(not pyoracle.reference_tree_present(), reason="reference tree not present")
+def test_forward_material_updates_match_reference_runner_live(oracle):
+    for make in scenarios.FORWARD_SCENARIOS:
+        p = scenarios.forward_materials(make)
+        p.steps = p.steps // 2 + 5
+        ref = oracle.run_reference(p, explicit=True)
+        g = oracle.run_oracle(p)
+        g.material_explicit(0)
+        g.material_explicit(1)
+        for n in oracle.NAMES + oracle.PSI_NAMES:
+            assert np.array_equal(g.get(n), ref[n]), f"{p.name}:{n}"
+
+
 def test_constants_match_reference():
     from fdtd_b200 import problem as P
     assert P.EPS0 == 8.854e-12

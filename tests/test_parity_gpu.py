@@ -364,3 +364,35 @@ def test_large_spectrum_read_equals_its_parts(fdtd, precision):
     got = np.concatenate([g.dft(h).reshape(len(freqs), -1, ey, ex) for h in parts], axis=1)
     assert np.any(w != 0)
     assert np.array_equal(got.reshape(w.shape), w)
+
+
+@pytest.mark.parametrize("make", scenarios.FORWARD_SCENARIOS, ids=lambda f: f.__name__)
+def test_forward_material_updates_match_oracle(fdtd, oracle, make):
+    """fdtd_material_explicit (the reference's XUpdate<Mode, ft, true>) after
+    the steps: every stored array bit for bit the oracle's, which reproduces
+    the reference's <name>_fwd fixtures."""
+    p = scenarios.forward_materials(make)
+    o = oracle.run_oracle(p)
+    o.material_explicit(0)
+    o.material_explicit(1)
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    g.material_explicit(0)
+    g.material_explicit(1)
+    g.synchronize()
+    for n in oracle.NAMES + oracle.PSI_NAMES:
+        assert np.array_equal(g.get(n), o.get(n)), f"{p.name}:{n}"
+
+
+def test_forward_material_updates_refusals(fdtd):
+    g = fdtd.Grid.from_problem(scenarios.td_drude_lorentz(), "f64")
+    with pytest.raises(fdtd.FdtdError) as e:
+        g.material_explicit(0)  # a Lorentz material: no explicit update in the reference
+    assert e.value.code == -3
+    g.material_explicit(1)
+    f32 = fdtd.Grid.from_problem(scenarios.forward_materials(scenarios.te_materials), "f32")
+    with pytest.raises(fdtd.FdtdError) as e:
+        f32.material_explicit(1)  # the FP32 method stores no D or B
+    assert e.value.code == -3
+    with pytest.raises(fdtd.FdtdError):
+        g.material_explicit(2)
