@@ -29,7 +29,8 @@ __device__ __forceinline__ double interp_aux(const double* row, int L, double lo
 // TFSFPlane::field_update::dir_update (Source.hpp:506-531) for flux I of type
 // ft at cell idx, summed over d1, d2 as in field_update::get (:542-553).
 template <int MODE>
-__device__ double tfsf_term(const PlaneDev& p, const AuxTab& aux, long long row, int ft, int I, const int idx[3],
+__device__ __forceinline__ double tfsf_term(const PlaneDev& p, const AuxTab& aux, long long row, int ft, int I,
+                                            const int (&idx)[3],
                             const Prof<double> (&prof)[2][3], double dx) {
   constexpr int dim = MODE == kThreeD ? 3 : 2;
   const int d1 = dir1(I);
@@ -66,12 +67,27 @@ __device__ double tfsf_term(const PlaneDev& p, const AuxTab& aux, long long row,
 
 constexpr int kPlainThreads = 256;  // 32 x 8 cells per CTA
 
+// f[comp] += v with comp known only at run time, as selects: indexing the
+// array with comp would put it (a cell's whole D, E, B or H) in local memory
+__device__ __forceinline__ void add_to_component(double (&f)[3], int comp, double v) {
+#pragma unroll
+  for (int I = 0; I < 3; I++) {
+    const double sum = f[I] + v;
+    f[I] = comp == I ? sum : f[I];
+  }
+}
+
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
 }
 
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Shared-memory slots (one double per thread each) of the plain kernels,
 // numbered once for the copies and the reads: E half: H at the cell and at
@@ -129,6 +145,65 @@ __host__ __device__ constexpr PlainSlots plain_slots(int mode, int ft, int np) {
 // flux history is read and moved (a separate instantiation, so that the
 // leapfrog's kernels keep their registers).
 
+// What a cell reads besides its staged operands, loaded before the wait for
+// the copies so that these loads are in flight with them: the step count,
+// the cell's material id and eps-map value, and the curl's F profile values.
+struct PlainPre {
+  long long t;
+  int mid;
+  double eps_cell;
+  double fdx[3];
+  unsigned planes, srcs;  // the TFSF planes and sources whose boxes meet the CTA's cells
+};
+
+// The TFSF planes and soft sources that can touch the cells of this CTA
+// (columns i0..i0+31, rows j0..j0+7, planes k0..k1): the same for every
+// thread of the CTA, so the per-cell loops over them are uniform and skip
+// the planes and sources elsewhere in the grid.
+__device__ __forceinline__ void plain_masks(const PlainArgs& a, int i0, int j0, int k0, int k1, PlainPre& r) {
+  const int i1 = i0 + 31, j1 = j0 + 7;
+  r.planes = 0;
+  for (int q = 0; q < a.nplanes; q++) {
+    const PlaneDev& p = a.planes[q];
+    if (p.lo[0] <= i1 && p.hi[0] >= i0 && p.lo[1] <= j1 && p.hi[1] >= j0 && p.lo[2] <= k1 && p.hi[2] >= k0)
+      r.planes |= 1u << q;
+  }
+  r.srcs = 0;
+  for (int q = 0; q < a.nsrc; q++) {
+    const SourceDev& sr = a.src[q];
+    if (sr.i >= i0 && sr.i <= i1 && sr.j >= j0 && sr.j <= j1 && sr.k >= k0 && sr.k <= k1) r.srcs |= 1u << q;
+  }
+}
+
+// the per-cell part of it for plane k; t and the x and y profile values
+// come from `base` (the same for every plane of the thread's column)
+template <int MODE>
+__device__ __forceinline__ PlainPre plain_pre_at(const PlainArgs& a, int ft, int i, int j, int k, long long c,
+                                                 const PlainPre& base) {
+  PlainPre r;
+  r.t = base.t;
+  r.mid = 0;
+  if (a.ids) r.mid = a.ids[c];
+  else if (a.bids) r.mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  r.eps_cell = (ft == 0 && a.eps_map) ? a.eps_map[c] : 0.0;
+  r.fdx[0] = base.fdx[0];
+  r.fdx[1] = base.fdx[1];
+  r.fdx[2] = MODE != kThreeD ? 1.0 : a.prof[ft][2].F[k];
+  r.planes = base.planes;
+  r.srcs = base.srcs;
+  return r;
+}
+
+template <int MODE>
+__device__ __forceinline__ PlainPre plain_pre(const PlainArgs& a, int ft, int i, int j, int k, long long c, int nz) {
+  PlainPre base;
+  base.t = a.ctrl->t;
+  base.fdx[0] = a.prof[ft][0].F[i];
+  base.fdx[1] = a.prof[ft][1].F[j];
+  plain_masks(a, blockIdx.x * 32 + 1, blockIdx.y * 8 + 1, k, k + nz - 1, base);
+  return plain_pre_at<MODE>(a, ft, i, j, k, c, base);
+}
+
 // the copies of one cell of the E half; sets the CPML integrator indices
 template <int MODE, int NP>
 __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, int k, double* slot,
@@ -180,14 +255,14 @@ __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, 
 // the reference's E half of one cell from its slots
 template <int MODE, int NP, bool HIST>
 __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
-                                             const long long (&pidx)[3]) {
+                                             const long long (&pidx)[3], const PlainPre& pre) {
   constexpr PlainSlots S = plain_slots(MODE, 0, NP);
   constexpr int NPS = NP > 0 ? NP : 1;
   const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
   const long long c = k * sz + j * sy + i;
   const int idx[3] = {i, j, k};
   const double dt = a.dt;
-  const long long t = a.ctrl->t;
+  const long long t = pre.t;
   double h0[3] = {}, h1[3] = {}, h2[3] = {};
 #pragma unroll
   for (int I = 0; I < 3; I++) {
@@ -196,10 +271,8 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
     h1[I] = a.hist[0][1][I][c];
     if (a.bd == 3) h2[I] = a.hist[0][2][I][c];
   }
-  int mid = 0;
-  if (a.ids) mid = a.ids[c];
-  else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
-  const double eps_cell = a.eps_map ? a.eps_map[c] : 0.0;
+  const int mid = pre.mid;
+  const double eps_cell = pre.eps_cell;
   double hc[3] = {0.0, 0.0, 0.0}, hn[3][3] = {}, d[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
   double pp[NPS][3] = {}, jj[NPS][3] = {};
 #pragma unroll
@@ -245,7 +318,7 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
         continue;
       }
       const double diff = hc[K] - hn[K][J];
-      const double fdx = a.prof[0][J].F[idx[J]];
+      const double fdx = pre.fdx[J];
       at[q] = (levi(I, J, K) == 1 ? fdx : -fdx) * diff;
     }
     const double old = d[I], sdt = a.cc * dt, curl = at[0] + at[1];
@@ -265,7 +338,8 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
     }
   }
   // TFSFPlane::updateD
-  for (int q = 0; q < a.nplanes; q++) {
+  for (unsigned mq = pre.planes; mq; mq &= mq - 1) {
+    const int q = __ffs(mq) - 1;
     const PlaneDev& p = a.planes[q];
     if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
     const AuxTab& ax = a.aux[p.aux];
@@ -277,13 +351,11 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
     }
   }
   // SoftSource on D
-  for (int s = 0; s < a.nsrc; s++) {
-    const SourceDev& sr = a.src[s];
+  for (unsigned ms = pre.srcs; ms; ms &= ms - 1) {
+    const SourceDev& sr = a.src[__ffs(ms) - 1];
     if (sr.target != 1 || sr.cell != c) continue;
     const double v = t < sr.nvals ? sr.vals[t] : 0.0;
-#pragma unroll
-    for (int I = 0; I < 3; I++)
-      if (sr.comp == I) d[I] += v;
+    add_to_component(d, sr.comp, v);
   }
   // UpdatePML<Mode, Electric, J>, J = X, Y, Z in that order
 #pragma unroll
@@ -367,13 +439,11 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
     }
   }
   // SoftSource on E
-  for (int s = 0; s < a.nsrc; s++) {
-    const SourceDev& sr = a.src[s];
+  for (unsigned ms = pre.srcs; ms; ms &= ms - 1) {
+    const SourceDev& sr = a.src[__ffs(ms) - 1];
     if (sr.target != 0 || sr.cell != c) continue;
     const double v = t < sr.nvals ? sr.vals[t] : 0.0;
-#pragma unroll
-    for (int I = 0; I < 3; I++)
-      if (sr.comp == I) e[I] += v;
+    add_to_component(e, sr.comp, v);
   }
   // every write of the cell
 #pragma unroll
@@ -419,16 +489,28 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k0 = MODE == kThreeD ? a.kbeg + blockIdx.z * ZC : 0;
   if (i > a.nx - 2 || j > a.ny - 2) return;
-  long long pidx[ZC][3];
-#pragma unroll
-  for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z < a.kend)
-      plain_e_stage<MODE, NP>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
-  cp_async_wait_all();
+  const long long sz = static_cast<long long>(a.nx) * a.ny, cij = static_cast<long long>(j) * a.nx + i;
+  const int nz = MODE == kThreeD ? min(ZC, a.kend - k0) : 1;
+  long long pc[3], pn[3];
+  plain_e_stage<MODE, NP>(a, i, j, k0, smd + tid, pc);
+  PlainPre rc = plain_pre<MODE>(a, 0, i, j, k0, k0 * sz + cij, nz), rn = rc;
+  cp_async_commit();
 #pragma unroll 1
-  for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z < a.kend)
-      plain_e_cell<MODE, NP, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
+  for (int z = 0; z < nz; z++) {
+    double* cur = smd + tid + (z & 1) * NS * kPlainThreads;
+    if (z + 1 < nz) {
+      plain_e_stage<MODE, NP>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * kPlainThreads, pn);
+      rn = plain_pre_at<MODE>(a, 0, i, j, k0 + z + 1, (k0 + z + 1) * sz + cij, rc);
+      cp_async_commit();
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
+    plain_e_cell<MODE, NP, HIST>(a, i, j, k0 + z, cur, pc, rc);
+#pragma unroll
+    for (int J = 0; J < 3; J++) pc[J] = pn[J];
+    rc = rn;
+  }
 }
 
 // the copies of one cell of the H half
@@ -474,13 +556,13 @@ __device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, 
 // the reference's H half of one cell from its slots
 template <int MODE, bool HIST>
 __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
-                                             const long long (&pidx)[3]) {
+                                             const long long (&pidx)[3], const PlainPre& pre) {
   constexpr PlainSlots S = plain_slots(MODE, 1, 0);
   const long long sy = a.nx, sz = static_cast<long long>(a.nx) * a.ny;
   const long long c = k * sz + j * sy + i;
   const int idx[3] = {i, j, k};
   const double dt = a.dt;
-  const long long t = a.ctrl->t;
+  const long long t = pre.t;
   double h0[3] = {}, h1[3] = {}, h2[3] = {};
 #pragma unroll
   for (int I = 0; I < 3; I++) {
@@ -489,9 +571,7 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
     h1[I] = a.hist[1][1][I][c];
     if (a.bd == 3) h2[I] = a.hist[1][2][I][c];
   }
-  int mid = 0;
-  if (a.ids) mid = a.ids[c];
-  else if (a.bids) mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  const int mid = pre.mid;
   double ec[3] = {0.0, 0.0, 0.0}, en[3][3] = {}, b[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
@@ -526,7 +606,7 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
         continue;
       }
       const double diff = en[K][J] - ec[K];
-      const double fdx = a.prof[1][J].F[idx[J]];
+      const double fdx = pre.fdx[J];
       at[q] = (levi(I, J, K) == 1 ? fdx : -fdx) * diff;
     }
     const double old = b[I], sdt = -a.cc * dt, curl = at[0] + at[1];
@@ -546,7 +626,8 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
     }
   }
   // TFSFPlane::updateB (the aux grid was advanced by updateD: row + 1)
-  for (int q = 0; q < a.nplanes; q++) {
+  for (unsigned mq = pre.planes; mq; mq &= mq - 1) {
+    const int q = __ffs(mq) - 1;
     const PlaneDev& p = a.planes[q];
     if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
     const AuxTab& ax = a.aux[p.aux];
@@ -558,13 +639,11 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
     }
   }
   // SoftSource on B
-  for (int s = 0; s < a.nsrc; s++) {
-    const SourceDev& sr = a.src[s];
+  for (unsigned ms = pre.srcs; ms; ms &= ms - 1) {
+    const SourceDev& sr = a.src[__ffs(ms) - 1];
     if (sr.target != 3 || sr.cell != c) continue;
     const double v = t < sr.nvals ? sr.vals[t] : 0.0;
-#pragma unroll
-    for (int I = 0; I < 3; I++)
-      if (sr.comp == I) b[I] += v;
+    add_to_component(b, sr.comp, v);
   }
   // UpdatePML<Mode, Magnetic, J>
 #pragma unroll
@@ -592,13 +671,11 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
     h[I] = b[I] / den;
   }
   // SoftSource on H
-  for (int s = 0; s < a.nsrc; s++) {
-    const SourceDev& sr = a.src[s];
+  for (unsigned ms = pre.srcs; ms; ms &= ms - 1) {
+    const SourceDev& sr = a.src[__ffs(ms) - 1];
     if (sr.target != 2 || sr.cell != c) continue;
     const double v = t < sr.nvals ? sr.vals[t] : 0.0;
-#pragma unroll
-    for (int I = 0; I < 3; I++)
-      if (sr.comp == I) h[I] += v;
+    add_to_component(h, sr.comp, v);
   }
   // every write of the cell
 #pragma unroll
@@ -630,16 +707,28 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k0 = MODE == kThreeD ? a.kbeg + blockIdx.z * ZC : 0;
   if (i > a.nx - 2 || j > a.ny - 2) return;
-  long long pidx[ZC][3];
-#pragma unroll
-  for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z < a.kend)
-      plain_h_stage<MODE>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
-  cp_async_wait_all();
+  const long long sz = static_cast<long long>(a.nx) * a.ny, cij = static_cast<long long>(j) * a.nx + i;
+  const int nz = MODE == kThreeD ? min(ZC, a.kend - k0) : 1;
+  long long pc[3], pn[3];
+  plain_h_stage<MODE>(a, i, j, k0, smd + tid, pc);
+  PlainPre rc = plain_pre<MODE>(a, 1, i, j, k0, k0 * sz + cij, nz), rn = rc;
+  cp_async_commit();
 #pragma unroll 1
-  for (int z = 0; z < ZC; z++)
-    if (z == 0 || k0 + z < a.kend)
-      plain_h_cell<MODE, HIST>(a, i, j, k0 + z, smd + tid + z * NS * kPlainThreads, pidx[z]);
+  for (int z = 0; z < nz; z++) {
+    double* cur = smd + tid + (z & 1) * NS * kPlainThreads;
+    if (z + 1 < nz) {
+      plain_h_stage<MODE>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * kPlainThreads, pn);
+      rn = plain_pre_at<MODE>(a, 1, i, j, k0 + z + 1, (k0 + z + 1) * sz + cij, rc);
+      cp_async_commit();
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
+    plain_h_cell<MODE, HIST>(a, i, j, k0 + z, cur, pc, rc);
+#pragma unroll
+    for (int J = 0; J < 3; J++) pc[J] = pn[J];
+    rc = rn;
+  }
 }
 
 // the shared-memory carveout that holds the two CTAs per SM that the
@@ -665,33 +754,35 @@ static void plain_launch(F fn, size_t smem, const dim3& grid, const dim3& block,
   fn<<<grid, block, smem, s>>>(a);
 }
 
-// One cell per thread (ZC = 1). Two cells along z per thread, both staged
-// before either is computed, measured no faster on B200 (the sweeps are
-// bound by the latency of their FP64 arithmetic -- the reference's IEEE
-// divisions among it -- at the two CTAs per SM their registers allow, not by
-// the copies in flight), nor did three CTAs per SM at 80 registers (spills).
+// ZC planes per thread along z (3D): the copies of plane z + 1 go into the
+// second set of slots while plane z is computed from the first, so the
+// copies of the next cell overlap the FP64 arithmetic of this one (with one
+// plane per thread the copies and the arithmetic of a thread alternate, and
+// two CTAs per SM cannot fill the gaps). Two-pole grids, whose slots would
+// not leave room for two CTAs per SM twice over, and the BD3/BD4 kernels
+// take one plane per thread.
 template <int MODE>
 static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
-  constexpr int ZC = 1;
+  constexpr int ZP = MODE == kThreeD ? 8 : 1;
   const dim3 block(32, kPlainThreads / 32, 1);
   auto grid = [&](int zc) {
     return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y,
                 MODE == kThreeD ? (a.kend - a.kbeg + zc - 1) / zc : 1);
   };
   auto bytes = [](int ft, int np, int zc) {
-    return static_cast<size_t>(plain_slots(MODE, ft, np).n) * zc * kPlainThreads * sizeof(double);
+    return static_cast<size_t>(plain_slots(MODE, ft, np).n) * (zc > 1 ? 2 : 1) * kPlainThreads * sizeof(double);
   };
   if (!e) {
-    if (a.bd) plain_launch(plain_h_kernel<MODE, true, ZC>, bytes(1, 0, ZC), grid(ZC), block, a, s);
-    else plain_launch(plain_h_kernel<MODE, false, ZC>, bytes(1, 0, ZC), grid(ZC), block, a, s);
+    if (a.bd) plain_launch(plain_h_kernel<MODE, true, 1>, bytes(1, 0, 1), grid(1), block, a, s);
+    else plain_launch(plain_h_kernel<MODE, false, ZP>, bytes(1, 0, ZP), grid(ZP), block, a, s);
   } else if (a.bd) {
-    plain_launch(plain_e_kernel<MODE, 0, true, ZC>, bytes(0, 0, ZC), grid(ZC), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, true, 1>, bytes(0, 0, 1), grid(1), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 1) {
-    plain_launch(plain_e_kernel<MODE, 1, false, 1>, bytes(0, 1, 1), grid(1), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 1, false, ZP>, bytes(0, 1, ZP), grid(ZP), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 2) {
     plain_launch(plain_e_kernel<MODE, 2, false, 1>, bytes(0, 2, 1), grid(1), block, a, s);
   } else {
-    plain_launch(plain_e_kernel<MODE, 0, false, ZC>, bytes(0, 0, ZC), grid(ZC), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, false, ZP>, bytes(0, 0, ZP), grid(ZP), block, a, s);
   }
   return 1;
 }
