@@ -65,7 +65,7 @@ __device__ __forceinline__ double tfsf_term(const PlaneDev& p, const AuxTab& aux
   return terms[0] + terms[1];
 }
 
-constexpr int kPlainThreads = 256;  // 32 x 8 cells per CTA
+constexpr int kPlainThreads = 256;  // 32 x 8 cells per CTA (two-pole E sweep: 32 x 4)
 
 // f[comp] += v with comp known only at run time, as selects: indexing the
 // array with comp would put it (a cell's whole D, E, B or H) in local memory
@@ -157,11 +157,12 @@ struct PlainPre {
 };
 
 // The TFSF planes and soft sources that can touch the cells of this CTA
-// (columns i0..i0+31, rows j0..j0+7, planes k0..k1): the same for every
+// (columns i0..i0+31, rows j0..j1, planes k0..k1): the same for every
 // thread of the CTA, so the per-cell loops over them are uniform and skip
 // the planes and sources elsewhere in the grid.
-__device__ __forceinline__ void plain_masks(const PlainArgs& a, int i0, int j0, int k0, int k1, PlainPre& r) {
-  const int i1 = i0 + 31, j1 = j0 + 7;
+__device__ __forceinline__ void plain_masks(const PlainArgs& a, int i0, int j0, int j1, int k0, int k1,
+                                            PlainPre& r) {
+  const int i1 = i0 + 31;
   r.planes = 0;
   for (int q = 0; q < a.nplanes; q++) {
     const PlaneDev& p = a.planes[q];
@@ -200,12 +201,13 @@ __device__ __forceinline__ PlainPre plain_pre(const PlainArgs& a, int ft, int i,
   base.t = a.ctrl->t;
   base.fdx[0] = a.prof[ft][0].F[i];
   base.fdx[1] = a.prof[ft][1].F[j];
-  plain_masks(a, blockIdx.x * 32 + 1, blockIdx.y * 8 + 1, k, k + nz - 1, base);
+  const int j0 = blockIdx.y * blockDim.y + 1;
+  plain_masks(a, blockIdx.x * 32 + 1, j0, j0 + blockDim.y - 1, k, k + nz - 1, base);
   return plain_pre_at<MODE>(a, ft, i, j, k, c, base);
 }
 
 // the copies of one cell of the E half; sets the CPML integrator indices
-template <int MODE, int NP>
+template <int MODE, int NP, int T>
 __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, int k, double* slot,
                                               long long (&pidx)[3]) {
   constexpr PlainSlots S = plain_slots(MODE, 0, NP);
@@ -215,7 +217,7 @@ __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, 
   const int idx[3] = {i, j, k};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasH(MODE, K)) cp_async8(slot + S.own[K] * kPlainThreads, a.H.f[K] + c);
+    if (hasH(MODE, K)) cp_async8(slot + S.own[K] * T, a.H.f[K] + c);
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasE(MODE, I)) continue;
@@ -223,12 +225,12 @@ __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, 
     for (int J = 0; J < 3; J++) {
       if (J == I) continue;
       const int K = third(I, J);
-      if (hasH(MODE, K)) cp_async8(slot + S.nb[K][J] * kPlainThreads, a.H.f[K] + c - str[J]);
+      if (hasH(MODE, K)) cp_async8(slot + S.nb[K][J] * T, a.H.f[K] + c - str[J]);
     }
   }
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasE(MODE, I)) cp_async8(slot + S.flux[I] * kPlainThreads, a.D.f[I] + c);
+    if (hasE(MODE, I)) cp_async8(slot + S.flux[I] * T, a.D.f[I] + c);
 #pragma unroll
   for (int J = 0; J < 3; J++) {
     pidx[J] = -1;
@@ -240,20 +242,20 @@ __device__ __forceinline__ void plain_e_stage(const PlainArgs& a, int i, int j, 
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && I != J && !(MODE != kThreeD && J == 2))
-        cp_async8(slot + S.psi[I][J] * kPlainThreads, a.psi[0][I][J] + pidx[J]);
+        cp_async8(slot + S.psi[I][J] * T, a.psi[0][I][J] + pidx[J]);
   }
 #pragma unroll
   for (int q = 0; q < NP; q++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && q < a.dispersive) {
-        cp_async8(slot + S.p[q][I] * kPlainThreads, a.P[q].f[I] + c);
-        cp_async8(slot + S.j[q][I] * kPlainThreads, a.J[q].f[I] + c);
+        cp_async8(slot + S.p[q][I] * T, a.P[q].f[I] + c);
+        cp_async8(slot + S.j[q][I] * T, a.J[q].f[I] + c);
       }
 }
 
 // the reference's E half of one cell from its slots
-template <int MODE, int NP, bool HIST>
+template <int MODE, int NP, bool HIST, int T>
 __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
                                              const long long (&pidx)[3], const PlainPre& pre) {
   constexpr PlainSlots S = plain_slots(MODE, 0, NP);
@@ -277,28 +279,28 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
   double pp[NPS][3] = {}, jj[NPS][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasH(MODE, K)) hc[K] = slot[S.own[K] * kPlainThreads];
+    if (hasH(MODE, K)) hc[K] = slot[S.own[K] * T];
 #pragma unroll
   for (int K = 0; K < 3; K++)
 #pragma unroll
     for (int J = 0; J < 3; J++)
-      if (J != K && hasH(MODE, K) && hasE(MODE, third(J, K))) hn[K][J] = slot[S.nb[K][J] * kPlainThreads];
+      if (J != K && hasH(MODE, K) && hasE(MODE, third(J, K))) hn[K][J] = slot[S.nb[K][J] * T];
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasE(MODE, I)) d[I] = slot[S.flux[I] * kPlainThreads];
+    if (hasE(MODE, I)) d[I] = slot[S.flux[I] * T];
 #pragma unroll
   for (int J = 0; J < 3; J++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && I != J && !(MODE != kThreeD && J == 2) && pidx[J] >= 0)
-        ps[I][J] = slot[S.psi[I][J] * kPlainThreads];
+        ps[I][J] = slot[S.psi[I][J] * T];
 #pragma unroll
   for (int q = 0; q < NP; q++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && q < a.dispersive) {
-        pp[q][I] = slot[S.p[q][I] * kPlainThreads];
-        jj[q][I] = slot[S.j[q][I] * kPlainThreads];
+        pp[q][I] = slot[S.p[q][I] * T];
+        jj[q][I] = slot[S.j[q][I] * T];
       }
 
   // YeeUpdate<Mode, D_I, TimePolicy>: a = LC*F/dx*(H_K - H_K[-J]), then
@@ -480,8 +482,8 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
   }
 }
 
-template <int MODE, int NP, bool HIST, int ZC>
-__global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_constant__ PlainArgs a) {
+template <int MODE, int NP, bool HIST, int ZC, int T>
+__global__ void __launch_bounds__(T, T == 256 ? 2 : 3) plain_e_kernel(const __grid_constant__ PlainArgs a) {
   extern __shared__ double smd[];
   constexpr int NS = plain_slots(MODE, 0, NP).n;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -492,21 +494,21 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
   const long long sz = static_cast<long long>(a.nx) * a.ny, cij = static_cast<long long>(j) * a.nx + i;
   const int nz = MODE == kThreeD ? min(ZC, a.kend - k0) : 1;
   long long pc[3], pn[3];
-  plain_e_stage<MODE, NP>(a, i, j, k0, smd + tid, pc);
+  plain_e_stage<MODE, NP, T>(a, i, j, k0, smd + tid, pc);
   PlainPre rc = plain_pre<MODE>(a, 0, i, j, k0, k0 * sz + cij, nz), rn = rc;
   cp_async_commit();
 #pragma unroll 1
   for (int z = 0; z < nz; z++) {
-    double* cur = smd + tid + (z & 1) * NS * kPlainThreads;
+    double* cur = smd + tid + (z & 1) * NS * T;
     if (z + 1 < nz) {
-      plain_e_stage<MODE, NP>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * kPlainThreads, pn);
+      plain_e_stage<MODE, NP, T>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * T, pn);
       rn = plain_pre_at<MODE>(a, 0, i, j, k0 + z + 1, (k0 + z + 1) * sz + cij, rc);
       cp_async_commit();
       cp_async_wait_group<1>();
     } else {
       cp_async_wait_group<0>();
     }
-    plain_e_cell<MODE, NP, HIST>(a, i, j, k0 + z, cur, pc, rc);
+    plain_e_cell<MODE, NP, HIST, T>(a, i, j, k0 + z, cur, pc, rc);
 #pragma unroll
     for (int J = 0; J < 3; J++) pc[J] = pn[J];
     rc = rn;
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_e_kernel(const __grid_
 }
 
 // the copies of one cell of the H half
-template <int MODE>
+template <int MODE, int T>
 __device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, int k, double* slot,
                                               long long (&pidx)[3]) {
   constexpr PlainSlots S = plain_slots(MODE, 1, 0);
@@ -524,7 +526,7 @@ __device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, 
   const int idx[3] = {i, j, k};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasE(MODE, K)) cp_async8(slot + S.own[K] * kPlainThreads, a.E.f[K] + c);
+    if (hasE(MODE, K)) cp_async8(slot + S.own[K] * T, a.E.f[K] + c);
 #pragma unroll
   for (int I = 0; I < 3; I++) {
     if (!hasH(MODE, I)) continue;
@@ -532,12 +534,12 @@ __device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, 
     for (int J = 0; J < 3; J++) {
       if (J == I) continue;
       const int K = third(I, J);
-      if (hasE(MODE, K)) cp_async8(slot + S.nb[K][J] * kPlainThreads, a.E.f[K] + c + str[J]);
+      if (hasE(MODE, K)) cp_async8(slot + S.nb[K][J] * T, a.E.f[K] + c + str[J]);
     }
   }
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasH(MODE, I)) cp_async8(slot + S.flux[I] * kPlainThreads, a.B.f[I] + c);
+    if (hasH(MODE, I)) cp_async8(slot + S.flux[I] * T, a.B.f[I] + c);
 #pragma unroll
   for (int J = 0; J < 3; J++) {
     pidx[J] = -1;
@@ -549,12 +551,12 @@ __device__ __forceinline__ void plain_h_stage(const PlainArgs& a, int i, int j, 
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasH(MODE, I) && I != J && !(MODE != kThreeD && J == 2))
-        cp_async8(slot + S.psi[I][J] * kPlainThreads, a.psi[1][I][J] + pidx[J]);
+        cp_async8(slot + S.psi[I][J] * T, a.psi[1][I][J] + pidx[J]);
   }
 }
 
 // the reference's H half of one cell from its slots
-template <int MODE, bool HIST>
+template <int MODE, bool HIST, int T>
 __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, int k, const double* slot,
                                              const long long (&pidx)[3], const PlainPre& pre) {
   constexpr PlainSlots S = plain_slots(MODE, 1, 0);
@@ -575,21 +577,21 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
   double ec[3] = {0.0, 0.0, 0.0}, en[3][3] = {}, b[3] = {0.0, 0.0, 0.0}, ps[3][3] = {};
 #pragma unroll
   for (int K = 0; K < 3; K++)
-    if (hasE(MODE, K)) ec[K] = slot[S.own[K] * kPlainThreads];
+    if (hasE(MODE, K)) ec[K] = slot[S.own[K] * T];
 #pragma unroll
   for (int K = 0; K < 3; K++)
 #pragma unroll
     for (int J = 0; J < 3; J++)
-      if (J != K && hasE(MODE, K) && hasH(MODE, third(J, K))) en[K][J] = slot[S.nb[K][J] * kPlainThreads];
+      if (J != K && hasE(MODE, K) && hasH(MODE, third(J, K))) en[K][J] = slot[S.nb[K][J] * T];
 #pragma unroll
   for (int I = 0; I < 3; I++)
-    if (hasH(MODE, I)) b[I] = slot[S.flux[I] * kPlainThreads];
+    if (hasH(MODE, I)) b[I] = slot[S.flux[I] * T];
 #pragma unroll
   for (int J = 0; J < 3; J++)
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasH(MODE, I) && I != J && !(MODE != kThreeD && J == 2) && pidx[J] >= 0)
-        ps[I][J] = slot[S.psi[I][J] * kPlainThreads];
+        ps[I][J] = slot[S.psi[I][J] * T];
 
   // YeeUpdate<Mode, B_I, TimePolicy>: a = LC*F/dx*(E_K[+J] - E_K)
 #pragma unroll
@@ -698,8 +700,8 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
   }
 }
 
-template <int MODE, bool HIST, int ZC>
-__global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_constant__ PlainArgs a) {
+template <int MODE, bool HIST, int ZC, int T>
+__global__ void __launch_bounds__(T, T == 256 ? 2 : 3) plain_h_kernel(const __grid_constant__ PlainArgs a) {
   extern __shared__ double smd[];
   constexpr int NS = plain_slots(MODE, 1, 0).n;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -710,21 +712,21 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
   const long long sz = static_cast<long long>(a.nx) * a.ny, cij = static_cast<long long>(j) * a.nx + i;
   const int nz = MODE == kThreeD ? min(ZC, a.kend - k0) : 1;
   long long pc[3], pn[3];
-  plain_h_stage<MODE>(a, i, j, k0, smd + tid, pc);
+  plain_h_stage<MODE, T>(a, i, j, k0, smd + tid, pc);
   PlainPre rc = plain_pre<MODE>(a, 1, i, j, k0, k0 * sz + cij, nz), rn = rc;
   cp_async_commit();
 #pragma unroll 1
   for (int z = 0; z < nz; z++) {
-    double* cur = smd + tid + (z & 1) * NS * kPlainThreads;
+    double* cur = smd + tid + (z & 1) * NS * T;
     if (z + 1 < nz) {
-      plain_h_stage<MODE>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * kPlainThreads, pn);
+      plain_h_stage<MODE, T>(a, i, j, k0 + z + 1, smd + tid + ((z & 1) ^ 1) * NS * T, pn);
       rn = plain_pre_at<MODE>(a, 1, i, j, k0 + z + 1, (k0 + z + 1) * sz + cij, rc);
       cp_async_commit();
       cp_async_wait_group<1>();
     } else {
       cp_async_wait_group<0>();
     }
-    plain_h_cell<MODE, HIST>(a, i, j, k0 + z, cur, pc, rc);
+    plain_h_cell<MODE, HIST, T>(a, i, j, k0 + z, cur, pc, rc);
 #pragma unroll
     for (int J = 0; J < 3; J++) pc[J] = pn[J];
     rc = rn;
@@ -735,21 +737,22 @@ __global__ void __launch_bounds__(kPlainThreads, 2) plain_h_kernel(const __grid_
 // kernels' registers allow (plus the 1 KB the runtime reserves per CTA); the
 // rest of the SM's memory stays L1, which serves the neighbour reads (a
 // larger carveout slowed the sweeps measurably)
-static int plain_carveout(size_t smem) {
+static int plain_carveout(size_t smem, int ctas) {
   int dev = 0, max_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (max_sm <= 0) return cudaSharedmemCarveoutMaxShared;
-  const size_t need = 2 * (smem + 1024);
+  const size_t need = ctas * (smem + 1024);
   return static_cast<int>(need * 100 / max_sm + 1 > 100 ? 100 : need * 100 / max_sm + 1);
 }
 
 template <class F>
 static void plain_launch(F fn, size_t smem, const dim3& grid, const dim3& block, const PlainArgs& a,
                          cudaStream_t s) {
+  const int ctas = block.x * block.y == 256 ? 2 : 3;
   once_per_device(reinterpret_cast<const void*>(fn), [&] {
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, plain_carveout(smem));
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, plain_carveout(smem, ctas));
   });
   fn<<<grid, block, smem, s>>>(a);
 }
@@ -758,31 +761,33 @@ static void plain_launch(F fn, size_t smem, const dim3& grid, const dim3& block,
 // second set of slots while plane z is computed from the first, so the
 // copies of the next cell overlap the FP64 arithmetic of this one (with one
 // plane per thread the copies and the arithmetic of a thread alternate, and
-// two CTAs per SM cannot fill the gaps). Two-pole grids, whose slots would
-// not leave room for two CTAs per SM twice over, and the BD3/BD4 kernels
-// take one plane per thread.
+// two CTAs per SM cannot fill the gaps). Two-pole grids, whose 30 slots per
+// cell doubled would leave one 256-thread CTA per SM, take CTAs of 32 x 4
+// threads, three per SM. BD3/BD4 kernels take one plane per thread.
 template <int MODE>
 static int launch_plain(const PlainArgs& a, cudaStream_t s, bool e) {
   constexpr int ZP = MODE == kThreeD ? 8 : 1;
-  const dim3 block(32, kPlainThreads / 32, 1);
-  auto grid = [&](int zc) {
-    return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + block.y - 1) / block.y,
+  constexpr int T2 = MODE == kThreeD ? 128 : kPlainThreads;
+  auto grid = [&](int zc, int t) {
+    return dim3((a.nx - 2 + 31) / 32, (a.ny - 2 + t / 32 - 1) / (t / 32),
                 MODE == kThreeD ? (a.kend - a.kbeg + zc - 1) / zc : 1);
   };
-  auto bytes = [](int ft, int np, int zc) {
-    return static_cast<size_t>(plain_slots(MODE, ft, np).n) * (zc > 1 ? 2 : 1) * kPlainThreads * sizeof(double);
+  auto bytes = [](int ft, int np, int zc, int t) {
+    return static_cast<size_t>(plain_slots(MODE, ft, np).n) * (zc > 1 ? 2 : 1) * t * sizeof(double);
   };
+  constexpr int T = kPlainThreads;
+  const dim3 block(32, T / 32, 1), block2(32, T2 / 32, 1);
   if (!e) {
-    if (a.bd) plain_launch(plain_h_kernel<MODE, true, 1>, bytes(1, 0, 1), grid(1), block, a, s);
-    else plain_launch(plain_h_kernel<MODE, false, ZP>, bytes(1, 0, ZP), grid(ZP), block, a, s);
+    if (a.bd) plain_launch(plain_h_kernel<MODE, true, 1, T>, bytes(1, 0, 1, T), grid(1, T), block, a, s);
+    else plain_launch(plain_h_kernel<MODE, false, ZP, T>, bytes(1, 0, ZP, T), grid(ZP, T), block, a, s);
   } else if (a.bd) {
-    plain_launch(plain_e_kernel<MODE, 0, true, 1>, bytes(0, 0, 1), grid(1), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, true, 1, T>, bytes(0, 0, 1, T), grid(1, T), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 1) {
-    plain_launch(plain_e_kernel<MODE, 1, false, ZP>, bytes(0, 1, ZP), grid(ZP), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 1, false, ZP, T>, bytes(0, 1, ZP, T), grid(ZP, T), block, a, s);
   } else if (a.all_dispersive && a.dispersive == 2) {
-    plain_launch(plain_e_kernel<MODE, 2, false, 1>, bytes(0, 2, 1), grid(1), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 2, false, ZP, T2>, bytes(0, 2, ZP, T2), grid(ZP, T2), block2, a, s);
   } else {
-    plain_launch(plain_e_kernel<MODE, 0, false, ZP>, bytes(0, 0, ZP), grid(ZP), block, a, s);
+    plain_launch(plain_e_kernel<MODE, 0, false, ZP, T>, bytes(0, 0, ZP, T), grid(ZP, T), block, a, s);
   }
   return 1;
 }

@@ -152,6 +152,24 @@ def test_all_dispersive_tables_every_sweep(fdtd, oracle, kind, sweep):
     _compare(p, g, o, E + H, FUSED_TOL)
 
 
+@pytest.mark.parametrize("kind", ["drude", "drude_lorentz1", "lorentz2"])
+def test_all_dispersive_tables_f64_bitwise(fdtd, oracle, kind):
+    """The FP64 sweeps that stage P and J with the fields (one pole: 256
+    threads per CTA; two poles: 128) give the oracle's every stored array bit
+    for bit, the grid's z extent not a multiple of their 8 planes per thread."""
+    p = _all_dispersive(kind)
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f64")
+    g.step(p.steps)
+    g.synchronize()
+    assert (p.shape[2] - 2) % 8 != 0
+    for n in oracle.NAMES + oracle.PSI_NAMES:
+        assert np.array_equal(g.get(n), o.get(n)), n
+    for pole in range(1, max(len(m.poles) for m in p.materials)):
+        for n in ["Px", "Py", "Pz", "Jx", "Jy", "Jz"]:
+            assert np.array_equal(g.get_pole(pole, n), o.get_pole(pole, n)), (pole, n)
+
+
 def test_multistep_schemes_are_fp64_only(fdtd):
     p = scenarios.tm_bd3_tfsf()
     with pytest.raises(fdtd.FdtdError):
