@@ -373,6 +373,10 @@ int ensure_eh(fdtd_grid* g) {
   return dalloc(g, reinterpret_cast<void**>(&g->d_eh), static_cast<size_t>(g->eh_words) * sizeof(unsigned));
 }
 
+// the 3D FP32 method keeps its x slabs in the aligned layout (Slab::lo4)
+static bool xslab_aligned(const fdtd_grid* g) { return g->f32 && g->d.mode == kThreeD; }
+static long long xslab_row(const fdtd_grid* g) { return xslab_aligned(g) ? g->slab[0].W4 : g->slab[0].W; }
+
 int alloc_psi(fdtd_grid* g) {
   for (int ft = 0; ft < 2; ft++)
     for (int I = 0; I < 3; I++)
@@ -388,6 +392,11 @@ int alloc_psi(fdtd_grid* g) {
     g->slab[a].wlo = wlo;
     g->slab[a].hi0 = g->n[a] - 1 - whi;
     g->slab[a].W = wlo + whi;
+    const int lo4 = wlo > 0 ? (wlo + 1 + 3) / 4 * 4 : 0;
+    const int hb = whi > 0 ? std::max(lo4, g->slab[a].hi0 / 4 * 4) : g->n[a] + 4;
+    g->slab[a].lo4 = lo4;
+    g->slab[a].hb = hb;
+    g->slab[a].W4 = lo4 + (whi > 0 ? (g->n[a] + 3) / 4 * 4 - hb : 0);
   }
   for (int ft = 0; ft < 2; ft++)
     for (int I = 0; I < 3; I++) {
@@ -396,7 +405,7 @@ int alloc_psi(fdtd_grid* g) {
       for (int J = 0; J < 3; J++) {
         if (J == I || g->slab[J].W == 0) continue;
         long long cnt;
-        if (J == 0) cnt = static_cast<long long>(g->n[2]) * g->n[1] * g->slab[0].W;
+        if (J == 0) cnt = static_cast<long long>(g->n[2]) * g->n[1] * xslab_row(g);
         else if (J == 1) cnt = static_cast<long long>(g->n[2]) * g->slab[1].W * rowlen(g);
         else cnt = static_cast<long long>(g->slab[2].W) * g->n[1] * rowlen(g);
         int rc = dalloc(g, &g->psi[ft][I][J], cnt * elem(g));
@@ -1875,7 +1884,7 @@ int fdtd_download(fdtd_grid* g, int which, double* host) try {
   }
   long long cnt = field_elems(g);
   if (J >= 0) {
-    if (J == 0) cnt = nz * ny * g->slab[0].W;
+    if (J == 0) cnt = nz * ny * xslab_row(g);
     else if (J == 1) cnt = nz * g->slab[1].W * rowlen(g);
     else cnt = static_cast<long long>(g->slab[2].W) * ny * rowlen(g);
   }
@@ -1901,7 +1910,7 @@ int fdtd_download(fdtd_grid* g, int which, double* host) try {
             continue;
           }
           long long q;
-          if (J == 0) q = (k * ny + j) * g->slab[0].W + s;
+          if (J == 0) q = (k * ny + j) * xslab_row(g) + (xslab_aligned(g) ? slab_index4(g->slab[0], idx[0]) : s);
           else if (J == 1) q = (k * g->slab[1].W + s) * rl + i;
           else q = (static_cast<long long>(s) * ny + j) * rl + i;
           host[o] = val(q) * scale;

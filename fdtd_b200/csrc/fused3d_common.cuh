@@ -91,7 +91,8 @@ __device__ __forceinline__ float4 e_comp(const FusedArgs& a, int I, long long c,
 struct GroupCtx {
   int x4, j, lane;
   bool ok[4];
-  bool row_ok, pml_x, pml_y, src_here, uniform_mat;
+  bool row_ok, pml_y, src_here, uniform_mat;
+  int sx4;  // the group's first position in the aligned x-slab rows, or -1 (no x-slab cell)
   float4 fsx;
   float fsy;
   long long t;
@@ -105,7 +106,7 @@ __device__ __forceinline__ GroupCtx make_ctx(const FusedArgs& a, int ft, int x4,
   g.row_ok = j <= a.ny - 2;
 #pragma unroll
   for (int e = 0; e < 4; e++) g.ok[e] = g.row_ok && x4 + e >= 1 && x4 + e <= a.nx - 2;
-  g.pml_x = a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
+  g.sx4 = a.pml_axis[0] ? slab_group4(a.slab[0], x4) : -1;
   g.pml_y = a.pml_axis[1] && slab_index(a.slab[1], min(j, a.ny - 2)) >= 0;
   g.src_here = false;
   for (int s = 0; s < a.nsrc; s++)
@@ -180,24 +181,25 @@ __device__ __forceinline__ void e_group_update(const FusedArgs& a, const GroupCt
     st4(a.psi[0][0][2] + pi, px);
     st4(a.psi[0][1][2] + pi, py);
   }
-  if (g.pml_x) {
+  if (g.sx4 >= 0) {
+    // the group's x-slab integrators as one aligned float4 per component;
+    // cells outside the slab have zero coefficients and keep zero, cells
+    // not updated keep theirs
+    const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W4 + g.sx4;
+    const float4 B = ld4(a.prof[0][0].B + x4), Cs = ld4(a.prof[0][0].C + x4), G = ld4(a.prof[0][0].G + x4);
+    float4 py = staged_px ? reinterpret_cast<const float4*>(staged_px)[0] : ld4(a.psi[0][1][0] + pi);
+    float4 pz = staged_px ? reinterpret_cast<const float4*>(staged_px)[1] : ld4(a.psi[0][2][0] + pi);
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int i = x4 + e;
       if (!g.ok[e]) continue;
-      const int sx = slab_index(a.slab[0], i);
-      if (sx < 0) continue;
-      const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + sx;
-      const float B = a.prof[0][0].B[i], Cs = a.prof[0][0].C[i], G = a.prof[0][0].G[i];
-      // staged_px: the x-slab integrators of the group already copied to
-      // shared memory ([component y|z][cell])
-      const float py = staged_px ? staged_px[e] : a.psi[0][1][0][pi];
-      const float pz = staged_px ? staged_px[4 + e] : a.psi[0][2][0][pi];
-      set_el(dY, e, el(dY, e) + py * G);
-      set_el(dZ, e, el(dZ, e) + pz * G);
-      a.psi[0][1][0][pi] = B * py + Cs * el(ryx, e);
-      a.psi[0][2][0][pi] = B * pz + Cs * el(rzx, e);
+      const float y = el(py, e), z = el(pz, e);
+      set_el(dY, e, el(dY, e) + y * el(G, e));
+      set_el(dZ, e, el(dZ, e) + z * el(G, e));
+      set_el(py, e, el(B, e) * y + el(Cs, e) * el(ryx, e));
+      set_el(pz, e, el(B, e) * z + el(Cs, e) * el(rzx, e));
     }
+    st4(a.psi[0][1][0] + pi, py);
+    st4(a.psi[0][2][0] + pi, pz);
   }
   // sources: D-target adds to the flux; E-target undoes last step's value
   // (kept in E by the previous step) and adds this step's after the update
@@ -358,22 +360,25 @@ __device__ __forceinline__ void h_group_update(const FusedArgs& a, const GroupCt
     st4(a.psi[1][0][2] + pi, px);
     st4(a.psi[1][1][2] + pi, py);
   }
-  if (g.pml_x) {
+  if (g.sx4 >= 0) {
+    // the group's x-slab integrators as one aligned float4 per component;
+    // cells outside the slab have zero coefficients and keep zero, cells
+    // not updated keep theirs
+    const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W4 + g.sx4;
+    const float4 B = ld4(a.prof[1][0].B + x4), Cs = ld4(a.prof[1][0].C + x4), G = ld4(a.prof[1][0].G + x4);
+    float4 py = staged_px ? reinterpret_cast<const float4*>(staged_px)[0] : ld4(a.psi[1][1][0] + pi);
+    float4 pz = staged_px ? reinterpret_cast<const float4*>(staged_px)[1] : ld4(a.psi[1][2][0] + pi);
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int i = x4 + e;
       if (!g.ok[e]) continue;
-      const int sx = slab_index(a.slab[0], i);
-      if (sx < 0) continue;
-      const long long pi = (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + sx;
-      const float B = a.prof[1][0].B[i], Cs = a.prof[1][0].C[i], G = a.prof[1][0].G[i];
-      const float py = staged_px ? staged_px[e] : a.psi[1][1][0][pi];
-      const float pz = staged_px ? staged_px[4 + e] : a.psi[1][2][0][pi];
-      set_el(dY, e, el(dY, e) + py * G);
-      set_el(dZ, e, el(dZ, e) + pz * G);
-      a.psi[1][1][0][pi] = B * py + Cs * el(ryx, e);
-      a.psi[1][2][0][pi] = B * pz + Cs * el(rzx, e);
+      const float y = el(py, e), z = el(pz, e);
+      set_el(dY, e, el(dY, e) + y * el(G, e));
+      set_el(dZ, e, el(dZ, e) + z * el(G, e));
+      set_el(py, e, el(B, e) * y + el(Cs, e) * el(ryx, e));
+      set_el(pz, e, el(B, e) * z + el(Cs, e) * el(rzx, e));
     }
+    st4(a.psi[1][1][0] + pi, py);
+    st4(a.psi[1][2][0] + pi, pz);
   }
   // sources: B-target adds to the flux; H-target undoes last step's value
   // and adds this step's after the update (H is stored as eta*H)

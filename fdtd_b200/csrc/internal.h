@@ -56,10 +56,23 @@ __host__ __device__ constexpr int dir1(int I) { return I == 0 ? 1 : (I == 1 ? 2 
 // CPML slab of one axis: lo slab = cells 1..wlo, hi slab = hi0..hi0+whi-1
 struct Slab {
   int wlo, hi0, W;
+  // The x slab of the 3D FP32 method in rows of W4 floats: cell i < lo4 at
+  // i, cell i >= hb at lo4 + i - hb (lo4, hb, W4 multiples of 4), so that
+  // each 4-cell group that touches the slab is one aligned float4; the
+  // padding cells have zero CPML coefficients and keep zero integrators.
+  int lo4, hb, W4;
 };
 __host__ __device__ inline int slab_index(const Slab& s, int i) {
   if (i <= s.wlo) return i - 1;
   if (i >= s.hi0) return s.wlo + (i - s.hi0);
+  return -1;
+}
+// position of slab cell i (slab_index(s, i) >= 0) in the aligned x layout
+__host__ __device__ inline int slab_index4(const Slab& s, int i) { return i < s.lo4 ? i : s.lo4 + (i - s.hb); }
+// first position of the 4-cell group at x4 in the aligned x layout, or -1
+__host__ __device__ inline int slab_group4(const Slab& s, int x4) {
+  if (x4 < s.lo4) return x4;
+  if (x4 >= s.hb && x4 < s.hb + (s.W4 - s.lo4)) return s.lo4 + (x4 - s.hb);
   return -1;
 }
 

@@ -42,15 +42,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the x-slab CPML integrators of a group (two components) into slots
 // px[0..3], px[4..7]; only cells inside the slab are copied
 __device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx& g, int ft, int k, float* px) {
-  if (!g.pml_x) return;
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    const int sx = g.ok[e] ? slab_index(a.slab[0], g.x4 + e) : -1;
-    if (sx < 0) continue;
-    const long long pi = (static_cast<long long>(k) * a.ny + g.j) * a.slab[0].W + sx;
-    cp_async4(reinterpret_cast<unsigned*>(px + e), a.psi[ft][1][0] + pi);
-    cp_async4(reinterpret_cast<unsigned*>(px + 4 + e), a.psi[ft][2][0] + pi);
-  }
+  if (g.sx4 < 0) return;
+  const long long pi = (static_cast<long long>(k) * a.ny + g.j) * a.slab[0].W4 + g.sx4;
+  cp_async16(reinterpret_cast<float4*>(px), a.psi[ft][1][0] + pi);
+  cp_async16(reinterpret_cast<float4*>(px + 4), a.psi[ft][2][0] + pi);
 }
 
 }  // namespace
