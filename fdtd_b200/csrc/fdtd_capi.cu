@@ -373,8 +373,8 @@ int ensure_eh(fdtd_grid* g) {
   return dalloc(g, reinterpret_cast<void**>(&g->d_eh), static_cast<size_t>(g->eh_words) * sizeof(unsigned));
 }
 
-// the 3D FP32 method keeps its x slabs in the aligned layout (Slab::lo4)
-static bool xslab_aligned(const fdtd_grid* g) { return g->f32 && g->d.mode == kThreeD; }
+// the FP32 method keeps its x slabs in the aligned layout (Slab::lo4)
+static bool xslab_aligned(const fdtd_grid* g) { return g->f32; }
 static long long xslab_row(const fdtd_grid* g) { return xslab_aligned(g) ? g->slab[0].W4 : g->slab[0].W; }
 
 int alloc_psi(fdtd_grid* g) {

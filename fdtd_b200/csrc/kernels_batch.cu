@@ -82,14 +82,11 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
   float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
   if (sj >= 0) psy = ldcg4(a.psi[0][Ipy][1] + piy);
-  const bool xs = row_ok && a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
-  int sxe[4];
-  float psx[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    sxe[e] = (xs && ok[e]) ? slab_index(a.slab[0], x4 + e) : -1;
-    if (sxe[e] >= 0) psx[e] = __ldcg(a.psi[0][Ipx][0] + static_cast<long long>(j) * a.slab[0].W + sxe[e]);
-  }
+  // the x-slab integrators of the group: one aligned float4 (Slab::lo4)
+  const int sx4 = (row_ok && a.pml_axis[0]) ? slab_group4(a.slab[0], x4) : -1;
+  const long long pix = static_cast<long long>(j) * a.slab[0].W4 + max(sx4, 0);
+  float4 psx = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sx4 >= 0) psx = ldcg4(a.psi[0][Ipx][0] + pix);
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 hz = ldcg4(a.H[2] + c), hz_ym = ldcg4(a.H[2] + c - a.pitch);
@@ -128,19 +125,20 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
     }
     st4(a.psi[0][Ipy][1] + piy, ps);
   }
-  if (xs) {
+  if (sx4 >= 0) {
+    // cells outside the slab have zero coefficients and keep zero
+    const float4 B = ld4(a.prof[0][0].B + x4), Cs = ld4(a.prof[0][0].C + x4), G = ld4(a.prof[0][0].G + x4);
+    float4 ps = psx;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      if (sxe[e] < 0) continue;
-      const int i = x4 + e;
-      const long long pi = static_cast<long long>(j) * a.slab[0].W + sxe[e];
-      const float B = a.prof[0][0].B[i], Cs = a.prof[0][0].C[i], G = a.prof[0][0].G[i];
-      const float ps = psx[e];
+      if (!ok[e]) continue;
+      const float p = el(psx, e);
       const float raw = MODE == kTE ? el(ryx, e) : el(rzx, e);
-      if (MODE == kTE) set_el(dY, e, el(dY, e) + ps * G);
-      else set_el(dZ, e, el(dZ, e) + ps * G);
-      a.psi[0][Ipx][0][pi] = B * ps + Cs * raw;
+      if (MODE == kTE) set_el(dY, e, el(dY, e) + p * el(G, e));
+      else set_el(dZ, e, el(dZ, e) + p * el(G, e));
+      set_el(ps, e, el(B, e) * p + el(Cs, e) * raw);
     }
+    st4(a.psi[0][Ipx][0] + pix, ps);
   }
   // sources and material update (shared with the 3D sweeps)
   float4 uX = make_float4(0.f, 0.f, 0.f, 0.f), uY = uX, uZ = uX, aX = uX, aY = uX, aZ = uX;
@@ -210,14 +208,11 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
   float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
   if (sj >= 0) psy = ldcg4(a.psi[1][Ipy][1] + piy);
-  const bool xs = row_ok && a.pml_axis[0] && hits_slab(a.slab[0], x4, x4 + 3);
-  int sxe[4];
-  float psx[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    sxe[e] = (xs && ok[e]) ? slab_index(a.slab[0], x4 + e) : -1;
-    if (sxe[e] >= 0) psx[e] = __ldcg(a.psi[1][Ipx][0] + static_cast<long long>(j) * a.slab[0].W + sxe[e]);
-  }
+  // the x-slab integrators of the group: one aligned float4 (Slab::lo4)
+  const int sx4 = (row_ok && a.pml_axis[0]) ? slab_group4(a.slab[0], x4) : -1;
+  const long long pix = static_cast<long long>(j) * a.slab[0].W4 + max(sx4, 0);
+  float4 psx = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sx4 >= 0) psx = ldcg4(a.psi[1][Ipx][0] + pix);
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
     const float4 ex = ldcg4(a.E[0] + c), ey = ldcg4(a.E[1] + c), ex_yp = ldcg4(a.E[0] + c + a.pitch);
@@ -255,19 +250,19 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
     }
     st4(a.psi[1][Ipy][1] + piy, ps);
   }
-  if (xs) {
+  if (sx4 >= 0) {
+    const float4 B = ld4(a.prof[1][0].B + x4), Cs = ld4(a.prof[1][0].C + x4), G = ld4(a.prof[1][0].G + x4);
+    float4 ps = psx;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      if (sxe[e] < 0) continue;
-      const int i = x4 + e;
-      const long long pi = static_cast<long long>(j) * a.slab[0].W + sxe[e];
-      const float B = a.prof[1][0].B[i], Cs = a.prof[1][0].C[i], G = a.prof[1][0].G[i];
-      const float ps = psx[e];
+      if (!ok[e]) continue;
+      const float p = el(psx, e);
       const float raw = MODE == kTE ? el(rzx, e) : el(ryx, e);
-      if (MODE == kTE) set_el(dZ, e, el(dZ, e) + ps * G);
-      else set_el(dY, e, el(dY, e) + ps * G);
-      a.psi[1][Ipx][0][pi] = B * ps + Cs * raw;
+      if (MODE == kTE) set_el(dZ, e, el(dZ, e) + p * el(G, e));
+      else set_el(dY, e, el(dY, e) + p * el(G, e));
+      set_el(ps, e, el(B, e) * p + el(Cs, e) * raw);
     }
+    st4(a.psi[1][Ipx][0] + pix, ps);
   }
   float4 uX = make_float4(0.f, 0.f, 0.f, 0.f), uY = uX, uZ = uX, aX = uX, aY = uX, aZ = uX;
   for (int q = 0; q < a.nsrc; q++) {

@@ -26,10 +26,9 @@ namespace fdtdb {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBY = 8;
 
-// the x slab of a 3D grid is in the aligned layout of the 3D sweeps (Slab::lo4)
+// the x slab of the FP32 method is in the aligned layout (Slab::lo4)
 __device__ __forceinline__ long long psi_index(const FusedArgs& a, int J, int s, int i, int j, int k) {
-  if (J == 0 && a.nz > 1) return (static_cast<long long>(k) * a.ny + j) * a.slab[0].W4 + slab_index4(a.slab[0], i);
-  if (J == 0) return (static_cast<long long>(k) * a.ny + j) * a.slab[0].W + s;
+  if (J == 0) return (static_cast<long long>(k) * a.ny + j) * a.slab[0].W4 + slab_index4(a.slab[0], i);
   if (J == 1) return (static_cast<long long>(k) * a.slab[1].W + s) * a.pitch + i;
   return (static_cast<long long>(s) * a.ny + j) * a.pitch + i;
 }
