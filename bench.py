@@ -802,6 +802,7 @@ def run_grid(args, torch, world, rank, local, stream):
     g = G.Grid.from_problem(p, "f32", device=local)
     if args.sweep != "auto":
         g.set_sweep_kernel(args.sweep)
+    g.prepare()  # set-up: CPML slabs, DFT buffers, TFSF tables and the captured step graph
     g.step(args.warmup, stream=stream.cuda_stream)
     torch.cuda.synchronize()
     launches0 = g.launch_count
@@ -893,6 +894,7 @@ def run_grid(args, torch, world, rank, local, stream):
         p64 = make_problem(args.workload, nsig, args.n, args.variant, fp64=True)
         g64 = G.Grid.from_problem(p64, "f64", device=local)
         n64 = max(3, min(args.steps, 200))
+        g64.prepare()
         g64.step(args.warmup, stream=stream.cuda_stream)
         barrier()
         with torch.cuda.stream(stream):

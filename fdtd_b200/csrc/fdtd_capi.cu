@@ -1331,6 +1331,48 @@ int fdtd_dft_read(fdtd_grid* g, int handle, double* out) try {
 static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof);
 static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof);
 
+// The TFSF aux tables for a call of nsteps steps: at least 257 rows, so that
+// calls of up to 256 steps keep them (and the step graph, whose launches hold
+// their addresses); new tables make the graph stale.
+static int ensure_aux_tables(fdtd_grid* g, int nsteps) {
+  for (auto& a : g->auxes) {
+    if (a.cap >= nsteps + 1) continue;
+    if (a.d_tab) dfree(g, a.d_tab);
+    a.d_tab = nullptr;
+    const long long cap = std::max<long long>(nsteps + 1, 257);
+    int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(cap) * a.L * sizeof(double));
+    if (rc) return rc;
+    a.cap = cap;
+    g->version++;
+    CK(cudaStreamSynchronize(g->stream));
+  }
+  return FDTD_OK;
+}
+
+// The captured graph of kGraphSteps steps, captured again when anything it
+// holds changed (g->version). Pending DFT samples must have been folded.
+static int ensure_step_graph(fdtd_grid* g, cudaStream_t s) {
+  if (g->graph && g->graph_version == g->version) return FDTD_OK;
+  if (g->graph) {
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  const long long before = g->launches;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_steps(g, kGraphSteps, s, nullptr);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&g->graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  g->graph_launches = g->launches - before;
+  g->launches = before;
+  g->graph_version = g->version;
+  return FDTD_OK;
+}
+
 int fdtd_step(fdtd_grid* g, int nsteps, void* stream) try {
   return step_impl(g, nsteps, stream, nullptr);
 } catch (...) {
@@ -1346,6 +1388,15 @@ int fdtd_prepare(fdtd_grid* g) try {
   if (rc) return rc;
   if (g->dirty_dft) {
     rc = rebuild_dft(g);
+    if (rc) return rc;
+  }
+  // the step graph too (its capture launches nothing), so that the first
+  // call of kGraphSteps or more steps replays it at once
+  if (g->use_graphs && g->next_half == 0 && !g->half_split) {
+    rc = ensure_aux_tables(g, kGraphSteps);
+    if (rc) return rc;
+    if (g->dft_pending > 0) g->launches += flush_dft(g, g->stream);
+    rc = ensure_step_graph(g, g->stream);
     if (rc) return rc;
   }
   CK(cudaStreamSynchronize(g->stream));
@@ -1507,53 +1558,27 @@ static int step_impl(fdtd_grid* g, int nsteps, void* stream, double* prof) {
     CK(cudaStreamSynchronize(g->stream));
   }
   // TFSF: precompute the aux grids' Ez/Hy for this chunk of steps
+  {
+    const int rc = ensure_aux_tables(g, nsteps);
+    if (rc) return rc;
+  }
   for (auto& a : g->auxes) {
-    if (a.cap < nsteps + 1) {
-      if (a.d_tab) dfree(g, a.d_tab);
-      a.d_tab = nullptr;
-      int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(nsteps + 1) * a.L * sizeof(double));
-      if (rc) return rc;
-      a.cap = nsteps + 1;
-      CK(cudaStreamSynchronize(g->stream));
-    }
     double* st = a.d_state;
     const int L = a.L;
     g->launches += launch_aux_precompute(L, g->d.dt, g->d.dx, st, st + L, st + 2 * L, st + 3 * L, st + 4 * L,
                                          st + 5 * L, a.d_coef, a.d_vals, static_cast<int>(a.vals.size()), g->t,
                                          nsteps, a.d_tab, a.d_tab + a.cap * L, s);
   }
-  if (!g->auxes.empty()) {
-    Control c{};
-    c.t = g->t;
-    c.t0 = g->t;
-    CK(cudaMemcpyAsync(g->ctrl, &c, sizeof(long long) * 2, cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));  // the host value must outlive the copy
-  }
+  // the tables' first row is this step (set on the stream: no host wait)
+  if (!g->auxes.empty()) g->launches += launch_set_step(g->ctrl, g->t, s);
   // a captured graph takes its samples from slot 0 on
   if (g->dft_pending > 0) g->launches += flush_dft(g, s);
   // one graph replay = kGraphSteps steps (and, with DFT regions, one flush)
   const bool graphs = !prof && g->use_graphs && nsteps >= kGraphSteps;
   int done = 0;
   if (graphs) {
-    if (!g->graph || g->graph_version != g->version) {
-      if (g->graph) {
-        cudaGraphExecDestroy(g->graph);
-        g->graph = nullptr;
-      }
-      const long long before = g->launches;
-      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue_steps(g, kGraphSteps, s, nullptr);
-      cudaGraph_t graph = nullptr;
-      cudaError_t e = cudaStreamEndCapture(s, &graph);
-      if (rc) return rc;
-      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
-      e = cudaGraphInstantiate(&g->graph, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-      g->graph_launches = g->launches - before;
-      g->launches = before;
-      g->graph_version = g->version;
-    }
+    const int rc = ensure_step_graph(g, s);
+    if (rc) return rc;
     for (; done + kGraphSteps <= nsteps; done += kGraphSteps) {
       CK(cudaGraphLaunch(g->graph, s));
       g->launches += g->graph_launches;
@@ -1617,6 +1642,7 @@ static int half_step_impl(fdtd_grid* g, int phase, int part, void* stream) {
         int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(2) * a.L * sizeof(double));
         if (rc) return rc;
         a.cap = 2;
+        g->version++;  // a captured step graph holds the old table's address
         CK(cudaStreamSynchronize(g->stream));
       }
       double* st = a.d_state;

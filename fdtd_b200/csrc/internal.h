@@ -299,6 +299,8 @@ int launch_step_advance(Control* ctrl, unsigned* epoch, cudaStream_t s);
 int launch_field_diff(const void* a, int a_f32, long long rla, double sa, const void* b, int b_f32, long long rlb,
                       double sb, int nx, long long nrows, double* out, cudaStream_t s);
 int launch_chunk_start(Control* ctrl, cudaStream_t s);
+// ctrl->t = ctrl->t0 = t, on the stream
+int launch_set_step(Control* ctrl, long long t, cudaStream_t s);
 // faces with a boundary condition (kind 1 PEC, 2 PMC, 3 symmetric,
 // 4 antisymmetric, 5 periodic)
 struct BcFace {

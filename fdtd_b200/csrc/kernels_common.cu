@@ -279,6 +279,10 @@ __global__ void step_advance_kernel(Control* ctrl, unsigned* epoch) {
 }
 
 __global__ void chunk_start_kernel(Control* ctrl) { ctrl->t0 = ctrl->t; }
+__global__ void set_step_kernel(Control* ctrl, long long t) {
+  ctrl->t = t;
+  ctrl->t0 = t;
+}
 
 // Boundary conditions (include/BoundaryUpdates.hpp:230-760): on each face
 // with one, the outer cell takes the image of the interior cell next to the
@@ -351,6 +355,11 @@ int launch_boundaries(const BcFaces& f, int ft, int is_f32, void* const* fields,
 
 int launch_chunk_start(Control* ctrl, cudaStream_t s) {
   chunk_start_kernel<<<1, 1, 0, s>>>(ctrl);
+  return 1;
+}
+
+int launch_set_step(Control* ctrl, long long t, cudaStream_t s) {
+  set_step_kernel<<<1, 1, 0, s>>>(ctrl, t);
   return 1;
 }
 

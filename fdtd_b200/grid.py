@@ -202,7 +202,8 @@ class Grid:
         _check(load_library().fdtd_set_boundary(self.h, int(axis), int(side), code))
 
     def prepare(self) -> None:
-        """Lay out the deferred device state (CPML slabs, DFT buffers) now."""
+        """Lay out the deferred device state (CPML slabs, DFT buffers, TFSF
+        tables) and capture the step graph now."""
         _check(load_library().fdtd_prepare(self.h))
 
     def set_time_scheme(self, scheme: int) -> None:

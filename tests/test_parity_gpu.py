@@ -414,3 +414,29 @@ def test_forward_material_updates_refusals(fdtd):
     assert e.value.code == -3
     with pytest.raises(fdtd.FdtdError):
         g.material_explicit(2)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_step_graph_follows_new_tfsf_tables(fdtd, prec):
+    """Calls of growing length: a call of more steps than the TFSF tables hold
+    gets new tables, and the step graph captured before (whose launches hold
+    the old tables' addresses) is captured again. Graph-replayed calls give
+    the eager steps' fields bit for bit; so does a grid whose graph
+    fdtd_prepare captured."""
+    p = scenarios.td_tfsf_box()
+    a = fdtd.Grid.from_problem(p, prec)
+    b = fdtd.Grid.from_problem(p, prec)
+    b.use_graphs(False)
+    c = fdtd.Grid.from_problem(p, prec)
+    c.prepare()
+    for n in (64, 300, 70, 520):
+        for g in (a, b, c):
+            g.step(n)
+    for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        ref = b.get(n)
+        assert np.array_equal(a.get(n), ref), n
+        assert np.array_equal(c.get(n), ref), n
+    for q in range(len(p.dfts)):
+        assert np.any(b.dft(q)), q
+        assert np.array_equal(a.dft(q), b.dft(q)), q
+        assert np.array_equal(c.dft(q), b.dft(q)), q
