@@ -256,10 +256,13 @@ int fdtd_copy_plane_between(fdtd_grid* src, int which, int k_src, fdtd_grid* dst
 int fdtd_material_explicit(fdtd_grid* g, int ft, void* stream);
 /* Lays out the device state that the set-up calls defer: the CPML
  * coefficient profiles and integrator slabs (fdtd_set_pml regrades on the
- * host only) and the DFT sample buffers. fdtd_step and fdtd_step_half do it
- * themselves; call it before the first fdtd_step_static_scratch of a grid
- * that has not stepped, which allocates nothing. No counterpart in the
- * reference (its cells carry their CPML state from construction). */
+ * host only), the DFT sample buffers and the TFSF tables, and (with graphs
+ * on, between whole steps) captures the CUDA graph of 64 steps that
+ * fdtd_step replays, so that the first long call starts at once. fdtd_step
+ * and fdtd_step_half do all of it themselves; call it before the first
+ * fdtd_step_static_scratch of a grid that has not stepped, which allocates
+ * nothing. No counterpart in the reference (its cells carry their CPML state
+ * from construction). */
 int fdtd_prepare(fdtd_grid* g);
 /* fdtd_step for callers that cannot allocate device memory while stepping
  * (no counterpart in the reference, whose steps run on the host). Same
