@@ -23,7 +23,18 @@ namespace {
 using namespace f3d;
 constexpr long long kBarrierLimit = 1LL << 26;
 
-__device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+// Loads of the group updates: through L2 only (CG, the persistent kernel,
+// whose phases follow one another inside one launch), or cached in L1 as
+// well (the per-half-step launches: a launch reads nothing that another CTA
+// of the same launch writes, and L1 holds the neighbour rows of a CTA)
+template <bool CG>
+__device__ __forceinline__ float4 ldg4(const float* p) {
+  return CG ? __ldcg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+}
+template <bool CG, typename T>
+__device__ __forceinline__ T ldg1(const T* p) {
+  return CG ? __ldcg(p) : *p;
+}
 
 __device__ bool grid_barrier(BatchCtl* ctl, unsigned nblocks) {
   __syncthreads();
@@ -58,7 +69,7 @@ __device__ bool grid_barrier(BatchCtl* ctl, unsigned nblocks) {
 }
 
 // E update of one 4-cell group of a 2D grid
-template <int MODE, int MAXP>
+template <int MODE, int MAXP, bool CG>
 __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long long t) {
   const bool row_ok = j <= a.ny - 2;
   const int jl = min(j, a.ny - 2);
@@ -69,11 +80,11 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   // every operand of the group is requested before any is used: one memory
   // round trip per group (the lane-0 x neighbour and the old E included)
   const int Ie0 = MODE == kTE ? 0 : 2;
-  const float4 eo0 = ldcg4(a.E[Ie0] + c);
-  const float4 eo1 = MODE == kTE ? ldcg4(a.E[1] + c) : eo0;
-  const unsigned ids4 = a.ids ? __ldcg(reinterpret_cast<const unsigned*>(a.ids + c)) : 0u;
+  const float4 eo0 = ldg4<CG>(a.E[Ie0] + c);
+  const float4 eo1 = MODE == kTE ? ldg4<CG>(a.E[1] + c) : eo0;
+  const unsigned ids4 = a.ids ? ldg1<CG>(reinterpret_cast<const unsigned*>(a.ids + c)) : 0u;
   const int Ih = MODE == kTE ? 2 : 1;
-  const float hxm_l0 = lane == 0 ? __ldcg(a.H[Ih] + c - 1) : 0.f;
+  const float hxm_l0 = lane == 0 ? ldg1<CG>(a.H[Ih] + c - 1) : 0.f;
   const float4 fsx = ld4(a.prof[0][0].F + x4);
   const float fsy = a.prof[0][1].F[jl];
   // CPML integrators of the group, requested with the fields
@@ -81,15 +92,15 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const int sj = (row_ok && a.pml_axis[1]) ? slab_index(a.slab[1], j) : -1;
   const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
   float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (sj >= 0) psy = ldcg4(a.psi[0][Ipy][1] + piy);
+  if (sj >= 0) psy = ldg4<CG>(a.psi[0][Ipy][1] + piy);
   // the x-slab integrators of the group: one aligned float4 (Slab::lo4)
   const int sx4 = (row_ok && a.pml_axis[0]) ? slab_group4(a.slab[0], x4) : -1;
   const long long pix = static_cast<long long>(j) * a.slab[0].W4 + max(sx4, 0);
   float4 psx = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (sx4 >= 0) psx = ldcg4(a.psi[0][Ipx][0] + pix);
+  if (sx4 >= 0) psx = ldg4<CG>(a.psi[0][Ipx][0] + pix);
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
-    const float4 hz = ldcg4(a.H[2] + c), hz_ym = ldcg4(a.H[2] + c - a.pitch);
+    const float4 hz = ldg4<CG>(a.H[2] + c), hz_ym = ldg4<CG>(a.H[2] + c - a.pitch);
     float hz_xm0 = __shfl_up_sync(0xffffffffu, hz.w, 1);
     if (lane == 0) hz_xm0 = hxm_l0;
 #pragma unroll
@@ -100,7 +111,7 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
       set_el(dY, e, el(fsx, e) * el(ryx, e));
     }
   } else {
-    const float4 hx = ldcg4(a.H[0] + c), hy = ldcg4(a.H[1] + c), hx_ym = ldcg4(a.H[0] + c - a.pitch);
+    const float4 hx = ldg4<CG>(a.H[0] + c), hy = ldg4<CG>(a.H[1] + c), hx_ym = ldg4<CG>(a.H[0] + c - a.pitch);
     float hy_xm0 = __shfl_up_sync(0xffffffffu, hy.w, 1);
     if (lane == 0) hy_xm0 = hxm_l0;
 #pragma unroll
@@ -187,7 +198,7 @@ __device__ void e_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
 }
 
 // H update of one 4-cell group of a 2D grid
-template <int MODE>
+template <int MODE, bool CG>
 __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long long t) {
   const bool row_ok = j <= a.ny - 2;
   const int jl = min(j, a.ny - 2);
@@ -197,25 +208,25 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
   const long long c = static_cast<long long>(jl) * a.pitch + x4;
   // operands first, as in e_group_2d: the old H and the lane-31 x neighbour too
   const int Ih0 = MODE == kTE ? 2 : 0;
-  const float4 ho0 = ldcg4(a.H[Ih0] + c);
-  const float4 ho1 = MODE == kTE ? ho0 : ldcg4(a.H[1] + c);
+  const float4 ho0 = ldg4<CG>(a.H[Ih0] + c);
+  const float4 ho1 = MODE == kTE ? ho0 : ldg4<CG>(a.H[1] + c);
   const int Ie = MODE == kTE ? 1 : 2;
-  const float exp_l31 = lane == 31 ? __ldcg(a.E[Ie] + c + 4) : 0.f;
+  const float exp_l31 = lane == 31 ? ldg1<CG>(a.E[Ie] + c + 4) : 0.f;
   const float4 fsx = ld4(a.prof[1][0].F + x4);
   const float fsy = a.prof[1][1].F[jl];
   const int Ipy = MODE == kTE ? 2 : 0, Ipx = MODE == kTE ? 2 : 1;
   const int sj = (row_ok && a.pml_axis[1]) ? slab_index(a.slab[1], j) : -1;
   const long long piy = static_cast<long long>(max(sj, 0)) * a.pitch + x4;
   float4 psy = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (sj >= 0) psy = ldcg4(a.psi[1][Ipy][1] + piy);
+  if (sj >= 0) psy = ldg4<CG>(a.psi[1][Ipy][1] + piy);
   // the x-slab integrators of the group: one aligned float4 (Slab::lo4)
   const int sx4 = (row_ok && a.pml_axis[0]) ? slab_group4(a.slab[0], x4) : -1;
   const long long pix = static_cast<long long>(j) * a.slab[0].W4 + max(sx4, 0);
   float4 psx = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (sx4 >= 0) psx = ldcg4(a.psi[1][Ipx][0] + pix);
+  if (sx4 >= 0) psx = ldg4<CG>(a.psi[1][Ipx][0] + pix);
   float4 dX = make_float4(0.f, 0.f, 0.f, 0.f), dY = dX, dZ = dX, rxy = dX, ryx = dX, rzx = dX, rzy = dX;
   if (MODE == kTE) {
-    const float4 ex = ldcg4(a.E[0] + c), ey = ldcg4(a.E[1] + c), ex_yp = ldcg4(a.E[0] + c + a.pitch);
+    const float4 ex = ldg4<CG>(a.E[0] + c), ey = ldg4<CG>(a.E[1] + c), ex_yp = ldg4<CG>(a.E[0] + c + a.pitch);
     float ey_xp3 = __shfl_down_sync(0xffffffffu, ey.x, 1);
     if (lane == 31) ey_xp3 = exp_l31;
 #pragma unroll
@@ -225,7 +236,7 @@ __device__ void h_group_2d(const FusedArgs& a, int x4, int j, int lane, long lon
       set_el(dZ, e, el(fsx, e) * el(rzx, e) + fsy * el(rzy, e));
     }
   } else {
-    const float4 ez = ldcg4(a.E[2] + c), ez_yp = ldcg4(a.E[2] + c + a.pitch);
+    const float4 ez = ldg4<CG>(a.E[2] + c), ez_yp = ldg4<CG>(a.E[2] + c + a.pitch);
     float ez_xp3 = __shfl_down_sync(0xffffffffu, ez.x, 1);
     if (lane == 31) ez_xp3 = exp_l31;
 #pragma unroll
@@ -316,7 +327,7 @@ __global__ void __launch_bounds__(32 * ROWS) batch_kernel(const FusedArgs* __res
       const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
       const int R = a.item_rows > 0 ? a.item_rows : ROWS;
       const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
-      for (int r = 0; r < R; r += ROWS) e_group_2d<MODE, MAXP>(a, x4, j + r, lane, t);
+      for (int r = 0; r < R; r += ROWS) e_group_2d<MODE, MAXP, true>(a, x4, j + r, lane, t);
     }
     if (!grid_barrier(ctl, gridDim.x)) return;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -325,7 +336,7 @@ __global__ void __launch_bounds__(32 * ROWS) batch_kernel(const FusedArgs* __res
       const int tiles_x = a.pitch / 128, tile = static_cast<int>(w & 0xffffffu);
       const int R = a.item_rows > 0 ? a.item_rows : ROWS;
       const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
-      for (int r = 0; r < R; r += ROWS) h_group_2d<MODE>(a, x4, j + r, lane, t);
+      for (int r = 0; r < R; r += ROWS) h_group_2d<MODE, true>(a, x4, j + r, lane, t);
     }
     if (!grid_barrier(ctl, gridDim.x)) return;
   }
@@ -347,8 +358,8 @@ __global__ void __launch_bounds__(32 * ROWS) batch_phase_kernel(const FusedArgs*
   const int R = a.item_rows > 0 ? a.item_rows : ROWS;
   const int x4 = (tile % tiles_x) * 128 + 4 * lane, j = 1 + (tile / tiles_x) * R + ty;
   for (int r = 0; r < R; r += ROWS) {
-    if (PHASE == 0) e_group_2d<MODE, MAXP>(a, x4, j + r, lane, t);
-    else h_group_2d<MODE>(a, x4, j + r, lane, t);
+    if (PHASE == 0) e_group_2d<MODE, MAXP, false>(a, x4, j + r, lane, t);
+    else h_group_2d<MODE, false>(a, x4, j + r, lane, t);
   }
 }
 
