@@ -721,6 +721,10 @@ PlainArgs plain_args(fdtd_grid* g) {
   a.all_dispersive = g->mats.empty() ? 0 : 1;
   for (auto& m : g->mats)
     if (m.kind != FDTD_DRUDE && m.kind != FDTD_LORENTZ) a.all_dispersive = 0;
+  a.single_mat = g->mats.size() <= 1 ? 1 : 0;
+  a.uniform_mu = 1;
+  for (auto& m : g->mats)
+    if (m.mu_r != g->mats[0].mu_r) a.uniform_mu = 0;
   // TimePolicy constants (include/YeeUpdates.hpp:184-186, :205-215, :254-265),
   // folded by the host compiler as the reference's constexpr divisions are
   a.cc = 1.0;

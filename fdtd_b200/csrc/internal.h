@@ -155,6 +155,8 @@ struct PlainArgs {
   const double* eps_map;  // per-cell relative permittivity of non-dispersive cells (> 0), or null
   int dispersive;      // most poles of any material (Drude: 1)
   int all_dispersive;  // every material has poles: P and J are read with the fields
+  int single_mat;      // the table holds one material: no cell's id is read
+  int uniform_mu;      // every material has the same mu_r: the H half reads no id
   int nsrc;
   SourceDev src[kMaxSources];
   int nplanes;

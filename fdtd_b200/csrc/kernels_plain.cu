@@ -184,8 +184,11 @@ __device__ __forceinline__ PlainPre plain_pre_at(const PlainArgs& a, int ft, int
   PlainPre r;
   r.t = base.t;
   r.mid = 0;
-  if (a.ids) r.mid = a.ids[c];
-  else if (a.bids) r.mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
+  // the H half reads a cell's material only for its mu_r; a table of one
+  // material needs no id at all
+  const bool any = ft == 0 ? !a.single_mat : !a.uniform_mu;
+  if (any && a.ids) r.mid = a.ids[c];
+  else if (any && a.bids) r.mid = a.bids[((k >> a.bshift) * a.nby + (j >> a.bshift)) * a.nbx + (i >> a.bshift)];
   r.eps_cell = (ft == 0 && a.eps_map) ? a.eps_map[c] : 0.0;
   r.fdx[0] = base.fdx[0];
   r.fdx[1] = base.fdx[1];
@@ -376,9 +379,21 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
       ps[I][J] = B * psi + (levi(I, J, K) == 1 ? Cdx : -Cdx) * diff;
     }
   }
-  // material update
+  // material update; the row's scalars are read once, into registers (the
+  // table may alias the stored arrays as far as the compiler knows, so a
+  // member read after a store would be read again)
   const MatF64& m = a.mats[mid];
-  if (NP == 0 && m.kind >= 2) {
+  const int mkind = m.kind, mnp = m.npoles;
+  const double mden = m.den_e;
+  double mc1[NPS], mc2[NPS], mc3[NPS];
+#pragma unroll
+  for (int q = 0; q < NPS; q++) {
+    const bool used = q == 0 ? mkind >= 2 : (NP > 0 && mkind == 3);
+    mc1[q] = used ? m.c1[q] : 0.0;
+    mc2[q] = used ? m.c2[q] : 0.0;
+    mc3[q] = used ? m.c3[q] : 0.0;
+  }
+  if (NP == 0 && mkind >= 2) {
 #pragma unroll
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I)) {
@@ -391,36 +406,36 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
   for (int I = 2; I >= 0; I--) {
     if (!hasE(MODE, I)) continue;
     const double D = d[I];
-    if (m.kind <= 1) {
+    if (mkind <= 1) {
       // a per-cell permittivity replaces the ConstantUpdate K of the cell
-      const double den = (a.eps_map && eps_cell > 0.0) ? eps_cell * kEps0 : m.den_e;
+      const double den = (a.eps_map && eps_cell > 0.0) ? eps_cell * kEps0 : mden;
       e[I] = D / den;
-    } else if (m.kind == 2) {
+    } else if (mkind == 2) {
       // drude::DrudeUpdate::implicit_update (DispersiveMaterials.hpp:979-998)
       double P = pp[0][I], Jc = jj[0][I];
       P += dt * Jc;
-      const double E = (D - P) / m.den_e;
-      Jc = Jc * m.c1[0] / m.c2[0] + m.c3[0] * E;
+      const double E = (D - P) / mden;
+      Jc = Jc * mc1[0] / mc2[0] + mc3[0] * E;
       pp[0][I] = P;
       jj[0][I] = Jc;
       e[I] = E;
-    } else if (NP > 0 && m.npoles <= NP) {
+    } else if (NP > 0 && mnp <= NP) {
       // lorentz::LorentzUpdate::implicit_update (DispersiveMaterials.hpp:710-735),
       // one term per pole, on the staged poles
       double num = D;
       double P[NPS];
 #pragma unroll
       for (int q = 0; q < NPS; q++) {
-        if (q >= m.npoles) continue;
+        if (q >= mnp) continue;
         P[q] = pp[q][I] + dt * jj[q][I];
         pp[q][I] = P[q];
         num = num - P[q];
       }
-      const double E = num / m.den_e;
+      const double E = num / mden;
 #pragma unroll
       for (int q = 0; q < NPS; q++) {
-        if (q >= m.npoles) continue;
-        jj[q][I] = m.c1[q] * jj[q][I] + m.c2[q] * E - m.c3[q] * P[q];
+        if (q >= mnp) continue;
+        jj[q][I] = mc1[q] * jj[q][I] + mc2[q] * E - mc3[q] * P[q];
       }
       e[I] = E;
     } else {
@@ -466,9 +481,9 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
     for (int I = 0; I < 3; I++)
       if (hasE(MODE, I) && I != J) a.psi[0][I][J][pidx[J]] = ps[I][J];
   }
-  const bool staged = NP > 0 ? (m.kind == 2 || m.npoles <= NP) : m.kind == 2;
-  if (m.kind >= 2 && staged) {
-    const int np = m.kind == 2 ? 1 : m.npoles;
+  const bool staged = NP > 0 ? (mkind == 2 || mnp <= NP) : mkind == 2;
+  if (mkind >= 2 && staged) {
+    const int np = mkind == 2 ? 1 : mnp;
 #pragma unroll
     for (int q = 0; q < NPS; q++) {
       if (q >= np) continue;
