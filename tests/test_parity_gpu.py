@@ -81,6 +81,30 @@ def test_fused_f32_matches_oracle(fdtd, oracle, make):
             assert rel_l2(g.get(n), ref) <= SURFACE_F32_TOL, n
 
 
+PSI_F32_TOL = 1e-3
+
+
+@pytest.mark.parametrize("make", [scenarios.td_tfsf_box, scenarios.td_drude_lorentz, scenarios.te_materials,
+                                  scenarios.tm_cpml_sources], ids=lambda f: f.__name__)
+def test_fused_f32_cpml_integrators_read_back(fdtd, oracle, make):
+    """The FP32 method's CPML integrators, read through fdtd_download (the x
+    slab in its group-aligned rows, the y and z slabs in field rows), hold the
+    oracle's values at the oracle's cells: <= 1e-3 relative L2 for each
+    integrator the scenario drives."""
+    p = make()
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, "f32")
+    g.step(p.steps)
+    g.synchronize()
+    seen = 0
+    for n in oracle.PSI_NAMES:
+        ref, got = o.get(n), g.get(n)
+        if np.any(ref):
+            assert rel_l2(got, ref) <= PSI_F32_TOL, n
+            seen += 1
+    assert seen >= 2
+
+
 def test_read_quantity_boxes_and_errors(fdtd, oracle):
     """fdtd_read_quantity on sub-boxes equals the oracle's, and refuses
     quantities outside the mode and boxes that leave the interior."""
