@@ -1337,7 +1337,7 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
 
 // The TFSF aux tables for a call of nsteps steps: at least 257 rows, so that
 // calls of up to 256 steps keep them (and the step graph, whose launches hold
-// their addresses); new tables make the graph stale.
+// their addresses; dalloc and dfree make the graph stale).
 static int ensure_aux_tables(fdtd_grid* g, int nsteps) {
   for (auto& a : g->auxes) {
     if (a.cap >= nsteps + 1) continue;
@@ -1347,7 +1347,6 @@ static int ensure_aux_tables(fdtd_grid* g, int nsteps) {
     int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(cap) * a.L * sizeof(double));
     if (rc) return rc;
     a.cap = cap;
-    g->version++;
     CK(cudaStreamSynchronize(g->stream));
   }
   return FDTD_OK;
@@ -1646,7 +1645,6 @@ static int half_step_impl(fdtd_grid* g, int phase, int part, void* stream) {
         int rc = dalloc(g, reinterpret_cast<void**>(&a.d_tab), 2 * static_cast<size_t>(2) * a.L * sizeof(double));
         if (rc) return rc;
         a.cap = 2;
-        g->version++;  // a captured step graph holds the old table's address
         CK(cudaStreamSynchronize(g->stream));
       }
       double* st = a.d_state;
