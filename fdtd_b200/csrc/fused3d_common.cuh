@@ -17,17 +17,6 @@ __device__ __forceinline__ void set_el(float4& v, int e, float x) {
   else v.w = x;
 }
 
-__device__ __forceinline__ double interp_row(const double* row, int L, double loc, double dx, double shift) {
-  double nd = static_cast<double>(L) / 2.0 + loc / dx - shift;
-  unsigned long long n = static_cast<unsigned long long>(nd);
-  double frac = nd - static_cast<double>(n);
-  return (1.0 - frac) * row[n] + frac * row[n + 1];
-}
-
-__device__ __forceinline__ bool hits_slab(const Slab& s, int lo, int hi) {
-  return (s.wlo > 0 && lo <= s.wlo) || (s.W - s.wlo > 0 && hi >= s.hi0);
-}
-
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) {
   return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
 }
