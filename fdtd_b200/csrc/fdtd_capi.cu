@@ -386,18 +386,7 @@ int alloc_psi(fdtd_grid* g) {
           g->psi[ft][I][J] = nullptr;
         }
       }
-  for (int a = 0; a < 3; a++) {
-    const int wlo = g->pml[a][0] > 0 ? g->pml[a][0] + 1 : 0;
-    const int whi = g->pml[a][1] > 0 ? g->pml[a][1] + 1 : 0;
-    g->slab[a].wlo = wlo;
-    g->slab[a].hi0 = g->n[a] - 1 - whi;
-    g->slab[a].W = wlo + whi;
-    const int lo4 = wlo > 0 ? (wlo + 1 + 3) / 4 * 4 : 0;
-    const int hb = whi > 0 ? std::max(lo4, g->slab[a].hi0 / 4 * 4) : g->n[a] + 4;
-    g->slab[a].lo4 = lo4;
-    g->slab[a].hb = hb;
-    g->slab[a].W4 = lo4 + (whi > 0 ? (g->n[a] + 3) / 4 * 4 - hb : 0);
-  }
+  for (int a = 0; a < 3; a++) g->slab[a] = make_slab(g->n[a], g->pml[a][0], g->pml[a][1]);
   for (int ft = 0; ft < 2; ft++)
     for (int I = 0; I < 3; I++) {
       const bool has = ft == 0 ? hasE(g->d.mode, I) : hasH(g->d.mode, I);

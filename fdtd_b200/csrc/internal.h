@@ -75,6 +75,20 @@ __host__ __device__ inline int slab_group4(const Slab& s, int x4) {
   if (x4 >= s.hb && x4 < s.hb + (s.W4 - s.lo4)) return s.lo4 + (x4 - s.hb);
   return -1;
 }
+// The slabs of an axis of n cells with CPML of plo and phi cells at its two
+// ends (0: none): cells 1 .. plo + 1 and n - 2 - phi .. n - 2 carry integrators
+inline Slab make_slab(int n, int plo, int phi) {
+  Slab s;
+  const int wlo = plo > 0 ? plo + 1 : 0, whi = phi > 0 ? phi + 1 : 0;
+  s.wlo = wlo;
+  s.hi0 = n - 1 - whi;
+  s.W = wlo + whi;
+  s.lo4 = wlo > 0 ? (wlo + 1 + 3) / 4 * 4 : 0;
+  const int hb4 = s.hi0 / 4 * 4;
+  s.hb = whi > 0 ? (hb4 > s.lo4 ? hb4 : s.lo4) : n + 4;
+  s.W4 = s.lo4 + (whi > 0 ? (n + 3) / 4 * 4 - s.hb : 0);
+  return s;
+}
 
 // 1D CPML coefficients of one (field type, axis)
 template <typename R>
