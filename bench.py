@@ -63,13 +63,10 @@ P_STEPS = {"drude384": 1000, "lorentz768": 500, "tm256": 2000}
 
 # DRAM bytes per interior cell of one sweep launch, from ncu captures at 256^3 (profiles/)
 MEASURED_TRAFFIC = {
-    ("drude384", "staged"): {"e": 664.30848e6 / 16387064, "h": 629.359616e6 / 16387064,
+    ("drude384", "staged"): {"e": 669.810688e6 / 16387064, "h": 634.496512e6 / 16387064,
                              "source": "ncu capture at 256^3 scaled by interior cells "
-                                       "(profiles/staged_sweeps_tfsf_gather_drude256.md)"},
-    ("drude384", "flat"): {"e": 669.389568e6 / 16387064, "h": 633.131008e6 / 16387064,
-                           "source": "ncu capture at 256^3 scaled by interior cells "
-                                     "(profiles/flat_sweeps_tfsf_drude256.md)"},
-    ("lorentz768", "staged"): {"e": 7581.576e6 / 55742968, "h": 2209.036e6 / 55742968,
+                                       "(profiles/staged_sweeps_drude256.md)"},
+    ("lorentz768", "staged"): {"e": 7597.061e6 / 55742968, "h": 2221.944e6 / 55742968,
                                "source": "ncu capture at 384^3 scaled by interior cells "
                                          "(profiles/staged_sweeps_lorentz384.md)"},
 }
