@@ -39,8 +39,8 @@ __device__ __forceinline__ void cp_async4(unsigned* dst, const void* src) {
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// the x-slab CPML integrators of a group (two components) into slots
-// px[0..3], px[4..7]; only cells inside the slab are copied
+// the x-slab CPML integrators of a group (two components, one aligned
+// float4 each) into the slots px[0..3], px[4..7]
 __device__ __forceinline__ void stage_x_slab(const FusedArgs& a, const GroupCtx& g, int ft, int k, float* px) {
   if (g.sx4 < 0) return;
   const long long pi = (static_cast<long long>(k) * a.ny + g.j) * a.slab[0].W4 + g.sx4;
