@@ -8,7 +8,9 @@
 //   td: 3D, FP32 fused, 24^3, 4-cell CPML, Drude cube in a material map,
 //       x-propagating TFSF box (6 planes) with an Aux1D Gaussian;
 //   pm: the tm loop with the x-min and y-max CPML graded by
-//       PMLParameterModel(m, ma, sMax, kMax, aMax) of the caller's values.
+//       PMLParameterModel(m, ma, sMax, kMax, aMax) of the caller's values;
+//   fw: the tm loop, then Grid::apply_forward_materials of E and of H
+//       (the reference's XUpdate<Mode, ft, true>); writes Dz, Bx, By.
 // Writes the listed fields (float64, x fastest) to out.bin.
 #include <cmath>
 #include <cstdio>
@@ -59,6 +61,30 @@ int main(int argc, char** argv) {
       } catch (const gpu::Error& e) {
         if (e.code != FDTD_ERR_UNSUPPORTED) return 4;
       }
+    } else if (!strcmp(argv[1], "fw")) {
+      // the tm loop, then the forward (explicit) material updates of E and H
+      const double dt = 0.99 / std::sqrt(2.0) * dx / c0;
+      const int steps = 80;
+      gpu::Grid<TM, double> grid(40, 36, 1, dx, dt, steps);
+      grid.set_pml(Dir::X, 6);
+      grid.set_pml(Dir::Y, 6);
+      auto gauss = [dt](double t) { const double n = t / dt; return std::exp(-((n - 20.0) / 6.0) * ((n - 20.0) / 6.0)); };
+      auto src = grid.add(make_soft_source<Ez>(gauss, grid.cell(20, 18)));
+      grid.plan({YeeUpdate<TM, Dz>(dt, dx),
+                 UpdatePML<TM, FieldType::Electric, Dir::X>(dt, dx),
+                 UpdatePML<TM, FieldType::Electric, Dir::Y>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Electric>(),
+                 src,
+                 YeeUpdate<TM, Bx>(dt, dx), YeeUpdate<TM, By>(dt, dx),
+                 UpdatePML<TM, FieldType::Magnetic, Dir::X>(dt, dx),
+                 UpdatePML<TM, FieldType::Magnetic, Dir::Y>(dt, dx),
+                 VacuumUpdate<TM, FieldType::Magnetic>()});
+      grid.step(steps);
+      grid.apply_forward_materials(FieldType::Electric);
+      grid.apply_forward_materials(FieldType::Magnetic);
+      dump(out, grid.get<Dz>());
+      dump(out, grid.get<Bx>());
+      dump(out, grid.get<By>());
     } else if (!strcmp(argv[1], "pm")) {
       const double dt = 0.99 / std::sqrt(2.0) * dx / c0;
       const int steps = 80;

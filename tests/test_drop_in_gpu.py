@@ -45,6 +45,28 @@ def test_tm_plain_through_templates(drop_in, oracle, tmp_path):
         assert rel_l2(got[q], o.get(name)) <= 1e-12, name
 
 
+def test_forward_material_updates_through_templates(drop_in, oracle, tmp_path):
+    """grid.apply_forward_materials(FieldType::Electric / Magnetic) after the
+    tm loop: D and B from the fields, as the oracle's forward updates (which
+    reproduce the reference's XUpdate<Mode, ft, true>) give them (FP64,
+    <= 1e-12; the loop's source values come from the C++ signal)."""
+    from fdtd_b200.problem import TM, Problem, Source, courant_dt
+    p = Problem(TM, (40, 36, 1), 1e-6, courant_dt(1e-6, 0.99 / math.sqrt(2.0)))
+    for a in (0, 1):
+        for s in (0, 1):
+            p.pml[(a, s)] = 6
+    n = np.arange(80, dtype=np.float64)
+    p.sources.append(Source(2, (20, 18, 0), np.exp(-(((n - 20.0) / 6.0) ** 2)), "E"))
+    o = oracle.run_oracle(p, 80)
+    o.material_explicit(0)
+    o.material_explicit(1)
+    got = run(drop_in, "fw", tmp_path, 3, (1, 36, 40))
+    for q, name in enumerate(["Dz", "Bx", "By"]):
+        ref = o.get(name)
+        assert np.any(ref), name
+        assert rel_l2(got[q], ref) <= 1e-12, name
+
+
 def test_tm_custom_cpml_model_through_templates(drop_in, oracle, tmp_path):
     """grid.set_pml(d, o, n, PMLParameterModel(m, ma, sMax, kMax, aMax)):
     the user's grading reaches the GPU profiles (FP64 <= 1e-12)."""
