@@ -15,7 +15,8 @@
 //                 halos -- plus H {128 x kTY}.
 // Every mbarrier wait is bounded; on expiry the CTA records an error in the
 // control block, waits (bounded) for its outstanding copies and returns.
-// No load uses cluster multicast; the tensor maps cover this GPU's memory only.
+// Each CTA loads its own tiles (none is shared across a cluster); the tensor
+// maps cover this GPU's memory only.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
