@@ -185,6 +185,8 @@ struct fdtd_grid {
   uint8_t* d_ids = nullptr;
   uint16_t* d_bids = nullptr;
   void* d_eps_map = nullptr;  // plain: double eps; fused: float 1/eps (pitch layout)
+  double* d_tfsf_pre = nullptr;  // plain: the half step's TFSF corrections, 3 per plane cell
+  long long tfsf_cells = 0;      // cells of all TFSF planes
   int bshift = 0, nbx = 0, nby = 0, nbz = 0;
   void* d_mats = nullptr;
   int max_poles = 0;
@@ -706,6 +708,7 @@ PlainArgs plain_args(fdtd_grid* g) {
     }
   a.mats = static_cast<const MatF64*>(g->d_mats);
   a.eps_map = static_cast<const double*>(g->d_eps_map);
+  a.tfsf_pre = g->d_tfsf_pre;
   a.dispersive = g->max_poles;
   a.all_dispersive = g->mats.empty() ? 0 : 1;
   for (auto& m : g->mats)
@@ -1219,6 +1222,19 @@ int fdtd_add_tfsf_plane(fdtd_grid* g, int axis, int orient, const int* lo, const
     aux = static_cast<int>(g->auxes.size()) - 1;
   }
   p.aux = aux;
+  // the FP64 method forms each half step's corrections of all plane cells in
+  // one launch before its sweep (a table of 3 values per cell)
+  p.off = g->tfsf_cells;
+  const long long cells = static_cast<long long>(p.hi[0] - p.lo[0] + 1) * (p.hi[1] - p.lo[1] + 1) *
+                          (p.hi[2] - p.lo[2] + 1);
+  if (!g->f32) {
+    if (g->d_tfsf_pre) dfree(g, g->d_tfsf_pre);
+    g->d_tfsf_pre = nullptr;
+    const int rc = dalloc(g, reinterpret_cast<void**>(&g->d_tfsf_pre),
+                          static_cast<size_t>(g->tfsf_cells + cells) * 3 * sizeof(double));
+    if (rc) return rc;
+  }
+  g->tfsf_cells += cells;
   PlaneH ph;
   ph.dev = p;
   g->planes.push_back(ph);
@@ -1480,7 +1496,10 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
                      : use3d    ? launch_fused3d_e(fa, s)
                                 : launch_fused_e(mode, fa, s);
     }
-    else g->launches += launch_plain_e(mode, pa, s);
+    else {
+      if (!g->planes.empty()) g->launches += launch_tfsf_pre(mode, pa, 0, s);
+      g->launches += launch_plain_e(mode, pa, s);
+    }
     if (prof) CK(cudaEventRecord(ev[1], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 0, s);
     if (boxes) g->launches += launch_boxes(g, 0, 0, s);
@@ -1496,7 +1515,10 @@ static int enqueue_steps(fdtd_grid* g, int nsteps, cudaStream_t s, double* prof)
                      : use3d    ? launch_fused3d_h(fa, s)
                                 : launch_fused_h(mode, fa, s);
     }
-    else g->launches += launch_plain_h(mode, pa, s);
+    else {
+      if (!g->planes.empty()) g->launches += launch_tfsf_pre(mode, pa, 1, s);
+      g->launches += launch_plain_h(mode, pa, s);
+    }
     if (prof) CK(cudaEventRecord(ev[3], s));
     if (g->f32) g->launches += launch_tfsf_fused(mode, fa, 1, s);
     if (boxes) g->launches += launch_boxes(g, 1, 0, s);
@@ -1670,6 +1692,7 @@ static int half_step_impl(fdtd_grid* g, int phase, int part, void* stream) {
     if (phase == 0) g->launches += use3d ? launch_staged_e(fa, s) : launch_fused_e(mode, fa, s);
     else g->launches += use3d ? launch_staged_h(fa, s) : launch_fused_h(mode, fa, s);
   } else {
+    if (part != 1 && !g->planes.empty()) g->launches += launch_tfsf_pre(mode, pa, phase, s);
     g->launches += phase == 0 ? launch_plain_e(mode, pa, s) : launch_plain_h(mode, pa, s);
   }
   if (part == 0) {

@@ -132,6 +132,7 @@ struct PlaneDev {
   int axis, aux;
   int lo[3], hi[3];
   double normal[3], k[3], pol_e[3], pol_h[3], origin[3];
+  long long off;  // FP64 method: the plane's first cell in the table of precomputed corrections
 };
 
 struct AuxTab {
@@ -185,6 +186,9 @@ struct PlainArgs {
   double cc;
   double* hist[2][3][3];
   int kbeg, kend;  // 3D: the sweeps update planes kbeg .. kend-1 (all interior planes: 1 .. nz-2)
+  // the half step's TFSF corrections of every plane cell ([off + cell][3]),
+  // formed before each sweep by launch_tfsf_pre
+  double* tfsf_pre;
 };
 
 struct FusedArgs {
@@ -262,6 +266,8 @@ int launch_plain_e(int mode, const PlainArgs& a, cudaStream_t s);
 int launch_plain_h(int mode, const PlainArgs& a, cudaStream_t s);
 // the forward material updates of field type ft on every interior cell
 int launch_material_explicit(int mode, const PlainArgs& a, int ft, cudaStream_t s);
+// the TFSF corrections of half step ft for every cell of every plane into a.tfsf_pre
+int launch_tfsf_pre(int mode, const PlainArgs& a, int ft, cudaStream_t s);
 int launch_fused_e(int mode, const FusedArgs& a, cudaStream_t s);
 int launch_fused_h(int mode, const FusedArgs& a, cudaStream_t s);
 bool fused3d_supported(const FusedArgs& a);

@@ -65,6 +65,62 @@ __device__ __forceinline__ double tfsf_term(const PlaneDev& p, const AuxTab& aux
   return terms[0] + terms[1];
 }
 
+// a cell's index within a TFSF plane's box, x fastest
+__device__ __forceinline__ long long plane_cell(const PlaneDev& p, int i, int j, int k) {
+  const long long ex = p.hi[0] - p.lo[0] + 1, ey = p.hi[1] - p.lo[1] + 1;
+  return (static_cast<long long>(k - p.lo[2]) * ey + (j - p.lo[1])) * ex + (i - p.lo[0]);
+}
+
+// The TFSF corrections of half step ft for every cell of every plane:
+// ft 0 (cc*dt) * TFSFPlane::updateD's term, ft 1 (-cc*dt) * updateB's term,
+// the expressions the sweeps used to form per cell, in the same operation
+// order (this file is compiled without FMA contraction). Formed here in one
+// coalesced launch instead of by the one lane of each warp that holds an
+// x-normal face cell while the rest of the warp waits. Grid: x over a
+// plane's lower in-plane axis (128 cells per CTA), y over its other
+// in-plane axis, z over the planes.
+template <int MODE>
+__global__ void __launch_bounds__(128) tfsf_pre_kernel(const __grid_constant__ PlainArgs a, int ft) {
+  const PlaneDev& p = a.planes[blockIdx.z];
+  const int u = p.axis == 0 ? 1 : 0, v = p.axis == 2 ? 1 : 2;
+  const int uu = blockIdx.x * blockDim.x + threadIdx.x, vv = blockIdx.y;
+  if (p.lo[u] + uu > p.hi[u] || p.lo[v] + vv > p.hi[v]) return;
+  int idx[3];
+  idx[u] = p.lo[u] + uu;
+  idx[v] = p.lo[v] + vv;
+  const AuxTab& ax = a.aux[p.aux];
+  const long long row = a.ctrl->t - a.ctrl->t0 + ft;
+  const double dt = a.dt;
+  for (int w = p.lo[p.axis]; w <= p.hi[p.axis]; w++) {
+    idx[p.axis] = w;
+    double* out = a.tfsf_pre + 3 * (p.off + plane_cell(p, idx[0], idx[1], idx[2]));
+#pragma unroll
+    for (int I = 2; I >= 0; I--) {
+      if (ft == 0 ? !hasE(MODE, I) : !hasH(MODE, I)) continue;
+      out[I] = ft == 0 ? a.cc * dt * tfsf_term<MODE>(p, ax, row, 0, I, idx, a.prof, a.dx)
+                       : -a.cc * dt * tfsf_term<MODE>(p, ax, row, 1, I, idx, a.prof, a.dx);
+    }
+  }
+}
+
+int launch_tfsf_pre(int mode, const PlainArgs& a, int ft, cudaStream_t s) {
+  if (a.nplanes == 0) return 0;
+  int most_u = 1, most_v = 1;
+  for (int q = 0; q < a.nplanes; q++) {
+    const PlaneDev& p = a.planes[q];
+    const int u = p.axis == 0 ? 1 : 0, v = p.axis == 2 ? 1 : 2;
+    most_u = most_u > p.hi[u] - p.lo[u] + 1 ? most_u : p.hi[u] - p.lo[u] + 1;
+    most_v = most_v > p.hi[v] - p.lo[v] + 1 ? most_v : p.hi[v] - p.lo[v] + 1;
+  }
+  const dim3 grid(static_cast<unsigned>((most_u + 127) / 128), static_cast<unsigned>(most_v), a.nplanes);
+  switch (mode) {
+    case kTE: tfsf_pre_kernel<kTE><<<grid, 128, 0, s>>>(a, ft); break;
+    case kTM: tfsf_pre_kernel<kTM><<<grid, 128, 0, s>>>(a, ft); break;
+    default: tfsf_pre_kernel<kThreeD><<<grid, 128, 0, s>>>(a, ft); break;
+  }
+  return 1;
+}
+
 constexpr int kPlainThreads = 256;  // 32 x 8 cells per CTA (two-pole E sweep: 32 x 4)
 
 // f[comp] += v with comp known only at run time, as selects: indexing the
@@ -342,17 +398,17 @@ __device__ __forceinline__ void plain_e_cell(const PlainArgs& a, int i, int j, i
       h0[I] = old;
     }
   }
-  // TFSFPlane::updateD
+  // TFSFPlane::updateD: the corrections formed for this half step by
+  // tfsf_pre_kernel, added in plane order
   for (unsigned mq = pre.planes; mq; mq &= mq - 1) {
     const int q = __ffs(mq) - 1;
     const PlaneDev& p = a.planes[q];
     if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-    const AuxTab& ax = a.aux[p.aux];
-    const long long row = t - a.ctrl->t0;
+    const double* v = a.tfsf_pre + 3 * (p.off + plane_cell(p, i, j, k));
 #pragma unroll
     for (int I = 2; I >= 0; I--) {
       if (!hasE(MODE, I)) continue;
-      d[I] += a.cc * dt * tfsf_term<MODE>(p, ax, row, 0, I, idx, a.prof, a.dx);
+      d[I] += v[I];
     }
   }
   // SoftSource on D
@@ -642,17 +698,17 @@ __device__ __forceinline__ void plain_h_cell(const PlainArgs& a, int i, int j, i
       h0[I] = old;
     }
   }
-  // TFSFPlane::updateB (the aux grid was advanced by updateD: row + 1)
+  // TFSFPlane::updateB (the aux grid was advanced by updateD: row + 1), as
+  // formed by tfsf_pre_kernel
   for (unsigned mq = pre.planes; mq; mq &= mq - 1) {
     const int q = __ffs(mq) - 1;
     const PlaneDev& p = a.planes[q];
     if (i < p.lo[0] || i > p.hi[0] || j < p.lo[1] || j > p.hi[1] || k < p.lo[2] || k > p.hi[2]) continue;
-    const AuxTab& ax = a.aux[p.aux];
-    const long long row = t - a.ctrl->t0 + 1;
+    const double* v = a.tfsf_pre + 3 * (p.off + plane_cell(p, i, j, k));
 #pragma unroll
     for (int I = 2; I >= 0; I--) {
       if (!hasH(MODE, I)) continue;
-      b[I] += -a.cc * dt * tfsf_term<MODE>(p, ax, row, 1, I, idx, a.prof, a.dx);
+      b[I] += v[I];
     }
   }
   // SoftSource on B
