@@ -955,19 +955,25 @@ int fdtd_set_materials(fdtd_grid* g, const fdtd_material* mats, int n) try {
 int fdtd_set_material_ids(fdtd_grid* g, const uint8_t* ids) try {
   if (!g || !ids) return fail(FDTD_ERR_INVALID, "null argument");
   const long long n = static_cast<long long>(g->n[0]) * g->n[1] * g->n[2];
-  // range check in one pass, then the rows copied into the padded layout
+  // range check in one pass, then the rows copied straight into the padded
+  // device layout (the padding stays zero)
   uint8_t top = 0;
   for (long long c = 0; c < n; c++) top = ids[c] > top ? ids[c] : top;
   if (top >= g->mats.size()) return fail(FDTD_ERR_INVALID, "material id out of range of the material table");
-  std::vector<uint8_t> v(static_cast<size_t>(field_elems(g)), 0);
-  const long long rows = static_cast<long long>(g->n[1]) * g->n[2], rl = rowlen(g);
-  for (long long r = 0; r < rows; r++) memcpy(v.data() + r * rl, ids + r * g->n[0], static_cast<size_t>(g->n[0]));
+  const size_t rows = static_cast<size_t>(g->n[1]) * g->n[2], rl = static_cast<size_t>(rowlen(g));
   CK(cudaSetDevice(g->d.device));
   if (g->d_bids) {
     dfree(g, g->d_bids);
     g->d_bids = nullptr;
   }
-  return upload_vec(g, reinterpret_cast<void**>(&g->d_ids), v.data(), v.size());
+  if (g->d_ids) dfree(g, g->d_ids);
+  g->d_ids = nullptr;
+  const int rc = dalloc(g, reinterpret_cast<void**>(&g->d_ids), static_cast<size_t>(field_elems(g)));
+  if (rc) return rc;
+  CK(cudaMemcpy2DAsync(g->d_ids, rl, ids, static_cast<size_t>(g->n[0]), static_cast<size_t>(g->n[0]), rows,
+                       cudaMemcpyHostToDevice, g->stream));
+  CK(cudaStreamSynchronize(g->stream));  // the caller's array may go once the call returns
+  return FDTD_OK;
 } catch (...) {
   return host_failure();
 }
