@@ -105,6 +105,27 @@ def test_fused_f32_cpml_integrators_read_back(fdtd, oracle, make):
     assert seen >= 2
 
 
+@pytest.mark.parametrize("pml", [{(0, 0): 5}, {(0, 1): 7}, {(0, 0): 2, (0, 1): 6, (1, 1): 4}, {(1, 0): 3, (2, 1): 4}],
+                         ids=["x_low", "x_high", "x_both_y_high", "y_low_z_high"])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_one_sided_cpml(fdtd, oracle, pml, prec):
+    """CPML on some faces only (the x slab's aligned rows with one side, or
+    with ends of different widths): fields and integrators as the oracle's."""
+    p = scenarios.td_drude_lorentz()
+    p.pml = dict(pml)
+    p.name += "_" + "_".join(f"{a}{s}{n}" for (a, s), n in sorted(pml.items()))
+    o = oracle.run_oracle(p)
+    g = fdtd.Grid.from_problem(p, prec)
+    g.step(p.steps)
+    g.synchronize()
+    E, H, _, _ = mode_fields(p.mode)
+    _compare(p, g, o, E + H, FUSED_TOL if prec == "f32" else PLAIN_TOL)
+    for n in oracle.PSI_NAMES:
+        ref = o.get(n)
+        if np.any(ref):
+            assert rel_l2(g.get(n), ref) <= (PSI_F32_TOL if prec == "f32" else PLAIN_TOL), n
+
+
 def test_read_quantity_boxes_and_errors(fdtd, oracle):
     """fdtd_read_quantity on sub-boxes equals the oracle's, and refuses
     quantities outside the mode and boxes that leave the interior."""
