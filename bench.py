@@ -585,6 +585,8 @@ def run_batch(args, torch, world, rank, local, stream):
     ach = ab * args.steps / (ms / 1e3) / 1e9
     info = batch.info()
     ir = batch.item_rows()
+    tbi = batch.temporal()
+    tb = tbi["depth"]
     classes = {}
     for p_, r_, c_ in zip(probs, ir["rows"], ir["size_class"]):
         e = classes.setdefault(str(c_), {"problems": 0, "cells_min": None, "cells_max": 0, "item_rows": set()})
@@ -622,6 +624,8 @@ def run_batch(args, torch, world, rank, local, stream):
         t0 = time.perf_counter()
         ge = [G.Grid.from_problem(p, "f32", device=local) for p in probs]
         be = G.Batch(ge)
+        if tb:
+            be.set_temporal(tb)
         be.step(args.steps)
         out = [g.get("Hz") for g in ge]
         t_e2e = max_over_ranks(time.perf_counter() - t0)
@@ -632,7 +636,8 @@ def run_batch(args, torch, world, rank, local, stream):
             g.close()
         e2e = {"value": total_cells * args.steps / t_e2e / 1e9, "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "wall_s": t_e2e,
-               "note": "grid creation from host arrays, the steps without tuning, D2H of every Hz; host clock"}
+               "note": "grid creation from host arrays, the steps without tuning (the tuned temporal-blocking "
+                       "depth kept), D2H of every Hz; host clock"}
     cpu = cpu_batch_baseline(probs) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     return {
         "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -642,18 +647,24 @@ def run_batch(args, torch, world, rank, local, stream):
                    "interior_cells": total_cells, "seed": 0, "shard_imbalance": imbalance(
                        [problem_cost(p) for p in allp], shares),
                    "cpml": 10, "steps_in_config": 3000, "tile_rows": info["rows"], "ctas": info["blocks"],
-                   "launch": info["launch"],
+                   "launch": f"temporal blocking, {tb} steps per launch" if tb else info["launch"],
                    "tune_ms_per_step": info["tune_ms_per_step"],
+                   "temporal_depth": tb, "tune_ms_per_step_temporal": tbi["tune_ms_per_step"],
                    "size_classes": classes, "tuned_ms_per_step": ir["tuned_ms_per_step"],
                    "l2": "state ~290 MB > L2; no flush", "parallelism": f"problems sharded by cost over {world} GPUs" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": ("batch_kernel (persistent, all steps)" if info["launch"] == "persistent"
+        "roofline": {"bound": "hbm", "kernel": (f"batch_tb_kernel ({tb} steps per launch from shared memory; the "
+                                                "fraction counts the one-sweep bytes of every step and can exceed 1)"
+                                                if tb else "batch_kernel (persistent, all steps)"
+                                                if info["launch"] == "persistent"
                                                 else "batch_phase_kernel (E and H launches of one step)"),
                      "achieved": ach, "peak": peak,
                      "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "alg_bytes_per_step": ab,
                      "traffic": None},
         "fp64_plain": f64,
         "e2e": e2e,
-        "cpu_baseline": cpu, "gpu_launches": 2 if info["launch"] == "persistent" else 2 * args.steps + 1,
+        "cpu_baseline": cpu,
+        "gpu_launches": (args.steps // (2 * tb) * 2 + 2 * (args.steps % (2 * tb)) + 1) if tb
+        else 2 if info["launch"] == "persistent" else 2 * args.steps + 1,
         "clocks": clk.summary(),
     }
 

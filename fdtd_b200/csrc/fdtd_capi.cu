@@ -2101,6 +2101,14 @@ struct fdtd_batch {
   // measured ms per step: persistent with rows 1, 2, 4, 8, then per-phase with rows 1, 2, 4, 8
   std::vector<float> tune_ms;
   float tune_best_ms = 0.f;  // with the per-class item heights
+  // temporal blocking (fdtd_batch_set_temporal): steps per launch (0: off),
+  // the grids' arguments on the second copy of their state, the tiles
+  int tb = 0;
+  FusedArgs* d_args_b = nullptr;
+  unsigned* d_tb_items = nullptr;
+  int n_tb_items = 0;
+  std::vector<void*> tb_bufs;  // the second copy
+  std::vector<float> tb_ms;    // tuner: ms per step with 2, 3 and 4 steps per launch (0: not timed)
 };
 
 namespace {
@@ -2157,13 +2165,90 @@ int batch_items(fdtd_batch* b, int rows) {
   return FDTD_OK;
 }
 
+// Temporal blocking needs grids without poles whose sources lie inside their
+// interiors (a window applies a source only where it updates the cell).
+const char* tb_unsupported(const fdtd_batch* b) {
+  if (b->maxp != 0) return "temporal blocking takes grids without dispersive materials";
+  for (const FusedArgs& a : b->h_args)
+    for (int q = 0; q < a.nsrc; q++)
+      if (a.src[q].i < 1 || a.src[q].i > a.nx - 2 || a.src[q].j < 1 || a.src[q].j > a.ny - 2)
+        return "temporal blocking takes sources inside the grid's interior only";
+  return nullptr;
+}
+
+// The second copy of every array a step changes (fields, CPML integrators,
+// the soft sources' last values) and the grids' arguments pointing at it;
+// laid out once, a copy of the current state.
+int tb_prepare(fdtd_batch* b) {
+  if (b->d_args_b) return FDTD_OK;
+  CK(cudaDeviceSynchronize());
+  std::vector<FusedArgs> args = b->h_args;
+  for (size_t q = 0; q < b->grids.size(); q++) {
+    fdtd_grid* g = b->grids[q];
+    FusedArgs& a = args[q];
+    auto twin = [&](void* p) -> void* {
+      if (!g->sizes.count(p)) return nullptr;
+      void* d = nullptr;
+      if (cudaMalloc(&d, g->sizes[p]) != cudaSuccess) return nullptr;
+      b->tb_bufs.push_back(d);
+      if (cudaMemcpy(d, p, g->sizes[p], cudaMemcpyDeviceToDevice) != cudaSuccess) return nullptr;
+      return d;
+    };
+    for (int c = 0; c < 3; c++) {
+      if (g->E[c] && !(a.E[c] = static_cast<float*>(twin(g->E[c])))) return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
+      if (g->H[c] && !(a.H[c] = static_cast<float*>(twin(g->H[c])))) return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
+    }
+    for (int ft = 0; ft < 2; ft++)
+      for (int I = 0; I < 3; I++)
+        for (int J = 0; J < 3; J++)
+          if (g->psi[ft][I][J] && !(a.psi[ft][I][J] = static_cast<float*>(twin(g->psi[ft][I][J]))))
+            return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
+    if (g->d_src_last && !(a.src_last = static_cast<double*>(twin(g->d_src_last))))
+      return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
+  }
+  CK(cudaMalloc(&b->d_args_b, args.size() * sizeof(FusedArgs)));
+  CK(cudaMemcpy(b->d_args_b, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice));
+  return FDTD_OK;
+}
+
+// the tiles of the temporally blocked launches of depth `depth`
+int tb_items(fdtd_batch* b, int depth) {
+  int tw = 0, th = 0;
+  if (!batch_tb_tile(depth, &tw, &th)) return fail(FDTD_ERR_INVALID, "temporal blocking depth must be 2, 3 or 4");
+  std::vector<unsigned> items;
+  for (size_t q = 0; q < b->grids.size(); q++) {
+    const fdtd_grid* g = b->grids[q];
+    const long long nt = static_cast<long long>((g->n[0] + tw - 1) / tw) * ((g->n[1] + th - 1) / th);
+    if (nt >= (1 << 24)) return fail(FDTD_ERR_UNSUPPORTED, "grid too large to batch");
+    for (long long t = 0; t < nt; t++) items.push_back(static_cast<unsigned>(q) << 24 | static_cast<unsigned>(t));
+  }
+  if (b->d_tb_items) cudaFree(b->d_tb_items);
+  b->d_tb_items = nullptr;
+  b->n_tb_items = static_cast<int>(items.size());
+  CK(cudaMalloc(&b->d_tb_items, items.size() * sizeof(unsigned)));
+  CK(cudaMemcpy(b->d_tb_items, items.data(), items.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  return FDTD_OK;
+}
+
 int batch_launch(fdtd_batch* b, int nsteps, cudaStream_t s) {
   const FusedArgs* args = b->d_args;
   const unsigned* items = b->d_items;
-  if (!b->persistent) {
+  int s0 = 0;
+  if (b->tb > 0) {
+    // pairs of launches of tb steps each, there and back, so that the state
+    // ends in the grids' own arrays; the rest one kernel per half step
+    const int T = b->tb, pairs = nsteps / (2 * T);
+    for (int p = 0; p < pairs; p++) {
+      launch_batch_tb(b->mode, T, b->d_args, b->d_args_b, b->d_tb_items, b->n_tb_items, s0, s);
+      launch_batch_tb(b->mode, T, b->d_args_b, b->d_args, b->d_tb_items, b->n_tb_items, s0 + T, s);
+      s0 += 2 * T;
+    }
+    CK(cudaGetLastError());
+  }
+  if (!b->persistent || b->tb > 0) {
     void* fe = batch_phase_ptr(b->mode, b->maxp, b->rows, 0);
     void* fh = batch_phase_ptr(b->mode, b->maxp, b->rows, 1);
-    for (int q = 0; q < nsteps; q++) {
+    for (int q = s0; q < nsteps; q++) {
       void* params[] = {&args, &items, &q};
       CK(cudaLaunchKernel(fe, dim3(b->nitems), dim3(32, b->rows), params, 0, s));
       CK(cudaLaunchKernel(fh, dim3(b->nitems), dim3(32, b->rows), params, 0, s));
@@ -2275,6 +2360,9 @@ int fdtd_batch_destroy(fdtd_batch* b) try {
   cudaFree(b->d_ctrls);
   cudaFree(b->d_ctl);
   cudaFree(b->d_items);
+  cudaFree(b->d_args_b);
+  cudaFree(b->d_tb_items);
+  for (void* p : b->tb_bufs) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return FDTD_OK;
@@ -2305,6 +2393,7 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
     return FDTD_OK;
   };
   int rc = copy(true);
+  b->tb = 0;
   // candidates: the persistent kernel and the per-phase launches, each with
   // tiles of 1, 2, 4 or 8 rows
   const int cand[4] = {1, 2, 4, 8};
@@ -2365,7 +2454,38 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
     for (size_t q = 0; q < b->grids.size(); q++)
       if (b->cls[q] == c) b->mult[q] = keep;
   }
-  b->tune_best_ms = best / steps;
+  // temporal blocking with 2, 3 and 4 steps per launch, timed over whole
+  // pairs of launches
+  float best_step = best / steps;
+  int best_tb = 0;
+  b->tb_ms.assign(3, 0.f);
+  if (!rc && !tb_unsupported(b)) {
+    rc = tb_prepare(b);
+    if (!rc) rc = batch_items(b, best_rows);
+    for (int depth = 2; depth <= 4 && !rc; depth++) {
+      const int n = (steps + 2 * depth - 1) / (2 * depth) * (2 * depth);
+      rc = tb_items(b, depth);
+      b->tb = depth;
+      if (!rc) rc = batch_launch(b, 2 * depth, b->stream);  // warm-up
+      if (!rc) rc = copy(false);
+      CK(cudaEventRecord(e0, b->stream));
+      if (!rc) rc = batch_launch(b, n, b->stream);
+      CK(cudaEventRecord(e1, b->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (!rc) rc = copy(false);
+      b->tb_ms[depth - 2] = ms / n;
+      if (ms / n < best_step) {
+        best_step = ms / n;
+        best_tb = depth;
+      }
+    }
+    b->tb = 0;
+    if (!rc && best_tb) rc = tb_items(b, best_tb);
+  }
+  if (!rc) b->tb = best_tb;
+  b->tune_best_ms = best_step;
   CK(cudaStreamSynchronize(b->stream));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2382,6 +2502,36 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
   return host_failure();
 }
 
+int fdtd_batch_set_temporal(fdtd_batch* b, int depth) try {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch");
+  if (depth != 0 && depth != 2 && depth != 3 && depth != 4)
+    return fail(FDTD_ERR_INVALID, "temporal blocking depth must be 0, 2, 3 or 4");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  if (depth > 0) {
+    if (const char* why = tb_unsupported(b)) return fail(FDTD_ERR_UNSUPPORTED, why);
+    int rc = tb_prepare(b);
+    if (!rc) rc = tb_items(b, depth);
+    if (rc) return rc;
+  }
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  b->tb = depth;
+  return FDTD_OK;
+} catch (...) {
+  return host_failure();
+}
+
+int fdtd_batch_temporal(fdtd_batch* b, int* depth, float* tuned_ms) try {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch");
+  if (depth) *depth = b->tb;
+  if (tuned_ms)
+    for (int q = 0; q < 3; q++) tuned_ms[q] = q < static_cast<int>(b->tb_ms.size()) ? b->tb_ms[q] : 0.f;
+  return FDTD_OK;
+} catch (...) {
+  return host_failure();
+}
+
 int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) try {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch");
   if (rows != 1 && rows != 2 && rows != 4 && rows != 8) return fail(FDTD_ERR_INVALID, "rows must be 1, 2, 4 or 8");
@@ -2389,6 +2539,7 @@ int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) try {
   CK(cudaStreamSynchronize(b->stream));
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  b->tb = 0;
   b->persistent = persistent ? 1 : 0;
   b->mult.assign(b->grids.size(), 1);
   return batch_items(b, rows);
@@ -2459,9 +2610,11 @@ int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream) try {
     it = b->graphs.emplace(nsteps, exec).first;
   }
   CK(cudaGraphLaunch(it->second, s));
+  const long long tb_steps = b->tb > 0 ? nsteps / (2 * b->tb) * 2LL * b->tb : 0;
   for (auto* g : b->grids) {
     g->t += nsteps;
-    g->launches += b->persistent ? 2 : 2LL * nsteps + 1;
+    if (b->tb > 0) g->launches += tb_steps / b->tb + 2LL * (nsteps - tb_steps) + 1;
+    else g->launches += b->persistent ? 2 : 2LL * nsteps + 1;
   }
   // later work on any member grid's own stream follows the batch
   cudaEvent_t ev;

@@ -352,5 +352,13 @@ struct BatchCtl {
 void* batch_kernel_ptr(int mode, int maxp, int rows);
 void* batch_phase_ptr(int mode, int maxp, int rows, int phase);
 int launch_batch_advance(Control* const* ctrls, int n, int nsteps, cudaStream_t s);
+// temporal blocking of a batch (depth 2, 3 or 4 steps per launch): the exact
+// tile of a window (*tw x *th cells; 0 for an unsupported depth), and one
+// launch over the tiles `items` that reads the state through `rd` and writes
+// it through `wr` (one FusedArgs per grid each), steps s .. s + depth - 1
+// past the counters
+int batch_tb_tile(int depth, int* tw, int* th);
+int launch_batch_tb(int mode, int depth, const FusedArgs* rd, const FusedArgs* wr, const unsigned* items,
+                    int nitems, int s, cudaStream_t st);
 
 }  // namespace fdtdb

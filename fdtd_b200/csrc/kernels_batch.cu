@@ -363,6 +363,327 @@ __global__ void __launch_bounds__(32 * ROWS) batch_phase_kernel(const FusedArgs*
   }
 }
 
+// ---------------------------------------------------------------------------
+// Temporal blocking: T whole steps per launch from shared memory.
+//
+// A CTA loads a window of kTbW x kTbH cells of one grid (every field
+// component of the mode, the cells' 1/eps, the four CPML integrators) into
+// shared memory, advances the window T steps there, and writes back the
+// inner tile that T steps leave exact: a step's dependence reaches one cell
+// in every direction (E from H at i-1, j-1; H from E at i+1, j+1), so the
+// values within T cells of the window's edges (those inside the grid) go
+// stale while the tile (kTbW - 2T) x (kTbH - 2T) stays exact. The tiles
+// cover every cell of every grid once; the windows overlap, so a launch
+// reads one copy of the state and writes the other (the batch keeps a second
+// copy), and launches come in pairs that end on the grids' own arrays.
+// Non-dispersive grids with sources inside their interiors only; the per-cell
+// arithmetic is e_group_2d's and h_group_2d's, in the same order.
+constexpr int kTbW = 64, kTbH = 32, kTbTy = 4;  // window; CTA of 64 x 4 threads, 8 rows each
+constexpr int kTbRows = kTbH / kTbTy;
+
+struct TbSrc {
+  int lx, ly, q;
+};
+
+__device__ __forceinline__ double src_value(const SourceDev& sr, long long t) {
+  return t >= 0 && t < sr.nvals ? sr.vals[t] : 0.0;
+}
+
+template <int MODE, int T>
+__global__ void __launch_bounds__(kTbW * kTbTy, 3) batch_tb_kernel(const FusedArgs* __restrict__ rd,
+                                                                  const FusedArgs* __restrict__ wr,
+                                                                  const unsigned* __restrict__ items, int s) {
+  constexpr int OW = kTbW - 2 * T, OH = kTbH - 2 * T;
+  constexpr int N = kTbW * kTbH;
+  // F[0..2]: TE Ex, Ey, Hz; TM Ez, Hx, Hy. PS[0..3]: the E integrators of
+  // the y and x slabs, then H's. YP[ft][0..3][row]: F, B, C, G of the y axis.
+  extern __shared__ float tb_sm[];
+  float* F = tb_sm;
+  float* IE = tb_sm + 3 * N;
+  float* PS = tb_sm + 4 * N;
+  __shared__ float YP[2][4][kTbH];
+  __shared__ int YS[kTbH];  // the row is in the y slab
+  __shared__ TbSrc srcs[kMaxSources];
+  __shared__ int nsl;
+
+  const unsigned w = items[blockIdx.x];
+  const FusedArgs& a = rd[w >> 24];
+  const FusedArgs& b = wr[w >> 24];
+  const int nx = a.nx, ny = a.ny;
+  const long long pitch = a.pitch;
+  const int tiles_x = (nx + OW - 1) / OW, tile = static_cast<int>(w & 0xffffffu);
+  const int x0 = (tile % tiles_x) * OW - T, y0 = (tile / tiles_x) * OH - T;
+  const long long t0 = rd[0].ctrl->t + s;
+  constexpr bool TE = MODE == kTE;
+  const float* src0 = TE ? a.E[0] : a.E[2];
+  const float* src1 = TE ? a.E[1] : a.H[0];
+  const float* src2 = TE ? a.H[2] : a.H[1];
+  const float* psrc[4] = {a.psi[0][TE ? 0 : 2][1], a.psi[0][TE ? 1 : 2][0], a.psi[1][TE ? 2 : 0][1],
+                          a.psi[1][TE ? 2 : 1][0]};
+
+  const int tid = threadIdx.y * kTbW + threadIdx.x;
+  if (tid == 0) {
+    int n = 0;
+    for (int q = 0; q < a.nsrc; q++) {
+      const int lx = a.src[q].i - x0, ly = a.src[q].j - y0;
+      if (lx >= 0 && lx < kTbW && ly >= 0 && ly < kTbH) srcs[n++] = {lx, ly, q};
+    }
+    nsl = n;
+  }
+  if (tid < 2 * kTbH) {
+    const int ft = tid / kTbH, ly = tid % kTbH, gy = y0 + ly;
+    const bool rowok = gy >= 1 && gy <= ny - 2;
+    const int sj = (rowok && a.pml_axis[1]) ? slab_index(a.slab[1], gy) : -1;
+    YP[ft][0][ly] = rowok ? a.prof[ft][1].F[gy] : 0.f;
+    YP[ft][1][ly] = sj >= 0 ? a.prof[ft][1].B[gy] : 0.f;
+    YP[ft][2][ly] = sj >= 0 ? a.prof[ft][1].C[gy] : 0.f;
+    YP[ft][3][ly] = sj >= 0 ? a.prof[ft][1].G[gy] : 0.f;
+    if (ft == 0) YS[ly] = sj >= 0;
+  }
+  // this thread's column and its x profiles
+  const int lx = threadIdx.x, gx = x0 + lx;
+  const bool col_in = gx >= 0 && gx < nx;
+  const bool col_ok = gx >= 1 && gx <= nx - 2;
+  const int sx4 = (col_in && a.pml_axis[0]) ? slab_group4(a.slab[0], gx & ~3) : -1;
+  float fx[2] = {0.f, 0.f}, bx[2] = {0.f, 0.f}, cx[2] = {0.f, 0.f}, gxp[2] = {0.f, 0.f};
+#pragma unroll
+  for (int ft = 0; ft < 2; ft++) {
+    if (col_ok) fx[ft] = a.prof[ft][0].F[gx];
+    if (sx4 >= 0) {
+      bx[ft] = a.prof[ft][0].B[gx];
+      cx[ft] = a.prof[ft][0].C[gx];
+      gxp[ft] = a.prof[ft][0].G[gx];
+    }
+  }
+  const MatF32* mats = a.mats;
+#pragma unroll
+  for (int r = 0; r < kTbRows; r++) {
+    const int ly = threadIdx.y + kTbTy * r, gy = y0 + ly, l = ly * kTbW + lx;
+    const bool in = col_in && gy >= 0 && gy < ny;
+    const long long c = gy * pitch + gx;
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f, ie = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+    if (in) {
+      f0 = src0[c];
+      f1 = src1[c];
+      f2 = src2[c];
+      const int mid = a.ids ? a.ids[c] : 0;
+      ie = mats[mid].inv_eps;
+      if (a.inv_eps_map) {
+        const float v = a.inv_eps_map[c];
+        if (v > 0.f && mats[mid].npoles == 0) ie = v;
+      }
+      if (gy >= 1 && gy <= ny - 2) {
+        const int sj = a.pml_axis[1] ? slab_index(a.slab[1], gy) : -1;
+        if (sj >= 0) {
+          p0 = psrc[0][sj * pitch + gx];
+          p2 = psrc[2][sj * pitch + gx];
+        }
+        if (sx4 >= 0) {
+          const long long pi = gy * static_cast<long long>(a.slab[0].W4) + sx4 + (gx & 3);
+          p1 = psrc[1][pi];
+          p3 = psrc[3][pi];
+        }
+      }
+    }
+    F[l] = f0;
+    F[N + l] = f1;
+    F[2 * N + l] = f2;
+    IE[l] = ie;
+    PS[l] = p0;
+    PS[N + l] = p1;
+    PS[2 * N + l] = p2;
+    PS[3 * N + l] = p3;
+  }
+  __syncthreads();
+
+  for (int st = 0; st < T; st++) {
+    const long long t = t0 + st;
+    // E half
+#pragma unroll
+    for (int r = 0; r < kTbRows; r++) {
+      const int ly = threadIdx.y + kTbTy * r, gy = y0 + ly, l = ly * kTbW + lx;
+      if (!(col_ok && lx >= 1 && ly >= 1 && gy >= 1 && gy <= ny - 2)) continue;
+      const float fsy = YP[0][0][ly];
+      const bool sy = YS[ly];
+      float dX = 0.f, dY = 0.f, dZ = 0.f, rxy = 0.f, ryx = 0.f, rzx = 0.f, rzy = 0.f;
+      if (TE) {
+        const float hz = F[2 * N + l], hz_ym = F[2 * N + l - kTbW], hz_xm = F[2 * N + l - 1];
+        rxy = hz - hz_ym;
+        ryx = -(hz - hz_xm);
+        dX = fsy * rxy;
+        dY = fx[0] * ryx;
+      } else {
+        const float hx = F[N + l], hy = F[2 * N + l], hx_ym = F[N + l - kTbW], hy_xm = F[2 * N + l - 1];
+        rzx = hy - hy_xm;
+        rzy = -(hx - hx_ym);
+        dZ = fx[0] * rzx + fsy * rzy;
+      }
+      if (sy) {
+        const float B = YP[0][1][ly], Cs = YP[0][2][ly], G = YP[0][3][ly];
+        const float ps = PS[l];
+        const float raw = TE ? rxy : rzy;
+        if (TE) dX = dX + ps * G;
+        else dZ = dZ + ps * G;
+        PS[l] = B * ps + Cs * raw;
+      }
+      if (sx4 >= 0) {
+        const float p = PS[N + l];
+        const float raw = TE ? ryx : rzx;
+        if (TE) dY = dY + p * gxp[0];
+        else dZ = dZ + p * gxp[0];
+        PS[N + l] = bx[0] * p + cx[0] * raw;
+      }
+      float uX = 0.f, uY = 0.f, uZ = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
+      for (int k = 0; k < nsl; k++) {
+        if (srcs[k].lx != lx || srcs[k].ly != ly) continue;
+        const int q = srcs[k].q;
+        const SourceDev& sr = a.src[q];
+        if (sr.target > 1) continue;
+        const double v = src_value(sr, t);
+        if (sr.target == 1) {
+          const float dv = static_cast<float>(v * a.src_scale_d);
+          if (sr.comp == 0) dX = dX + dv;
+          else if (sr.comp == 1) dY = dY + dv;
+          else dZ = dZ + dv;
+        } else {
+          const float u = static_cast<float>(st == 0 ? a.src_last[q] : src_value(sr, t - 1)),
+                      ad = static_cast<float>(v);
+          if (sr.comp == 0) { uX = uX + u; aX = aX + ad; }
+          else if (sr.comp == 1) { uY = uY + u; aY = aY + ad; }
+          else { uZ = uZ + u; aZ = aZ + ad; }
+        }
+      }
+      const float ie = IE[l];
+      if (TE) {
+        const float ex = F[l] - uX, ey = F[N + l] - uY;
+        const float exn = ex + ie * dX, eyn = ey + ie * dY;
+        F[l] = exn + aX;
+        F[N + l] = eyn + aY;
+      } else {
+        const float ez = F[l] - uZ;
+        const float ezn = ez + ie * dZ;
+        F[l] = ezn + aZ;
+      }
+    }
+    __syncthreads();
+    // H half
+#pragma unroll
+    for (int r = 0; r < kTbRows; r++) {
+      const int ly = threadIdx.y + kTbTy * r, gy = y0 + ly, l = ly * kTbW + lx;
+      if (!(col_ok && lx <= kTbW - 2 && ly <= kTbH - 2 && gy >= 1 && gy <= ny - 2)) continue;
+      const float fsy = YP[1][0][ly];
+      const bool sy = YS[ly];
+      float dX = 0.f, dY = 0.f, dZ = 0.f, rxy = 0.f, ryx = 0.f, rzx = 0.f, rzy = 0.f;
+      if (TE) {
+        const float ex = F[l], ey = F[N + l], ex_yp = F[l + kTbW], ey_xp = F[N + l + 1];
+        rzx = ey_xp - ey;
+        rzy = -(ex_yp - ex);
+        dZ = fx[1] * rzx + fsy * rzy;
+      } else {
+        const float ez = F[l], ez_yp = F[l + kTbW], ez_xp = F[l + 1];
+        rxy = ez_yp - ez;
+        ryx = -(ez_xp - ez);
+        dX = fsy * rxy;
+        dY = fx[1] * ryx;
+      }
+      if (sy) {
+        const float B = YP[1][1][ly], Cs = YP[1][2][ly], G = YP[1][3][ly];
+        const float ps = PS[2 * N + l];
+        const float raw = TE ? rzy : rxy;
+        if (TE) dZ = dZ + ps * G;
+        else dX = dX + ps * G;
+        PS[2 * N + l] = B * ps + Cs * raw;
+      }
+      if (sx4 >= 0) {
+        const float p = PS[3 * N + l];
+        const float raw = TE ? rzx : ryx;
+        if (TE) dZ = dZ + p * gxp[1];
+        else dY = dY + p * gxp[1];
+        PS[3 * N + l] = bx[1] * p + cx[1] * raw;
+      }
+      float uX = 0.f, uY = 0.f, uZ = 0.f, aX = 0.f, aY = 0.f, aZ = 0.f;
+      for (int k = 0; k < nsl; k++) {
+        if (srcs[k].lx != lx || srcs[k].ly != ly) continue;
+        const int q = srcs[k].q;
+        const SourceDev& sr = a.src[q];
+        if (sr.target < 2) continue;
+        const double v = src_value(sr, t);
+        if (sr.target == 3) {
+          const float dv = static_cast<float>(v * a.src_scale_b);
+          if (sr.comp == 0) dX = dX - dv;
+          else if (sr.comp == 1) dY = dY - dv;
+          else dZ = dZ - dv;
+        } else {
+          const double last = st == 0 ? a.src_last[q] : src_value(sr, t - 1);
+          const float u = static_cast<float>(last * a.src_scale_h), ad = static_cast<float>(v * a.src_scale_h);
+          if (sr.comp == 0) { uX = uX + u; aX = aX + ad; }
+          else if (sr.comp == 1) { uY = uY + u; aY = aY + ad; }
+          else { uZ = uZ + u; aZ = aZ + ad; }
+        }
+      }
+      if (TE) {
+        F[2 * N + l] = F[2 * N + l] - uZ - dZ + aZ;
+      } else {
+        F[N + l] = F[N + l] - uX - dX + aX;
+        F[2 * N + l] = F[2 * N + l] - uY - dY + aY;
+      }
+    }
+    __syncthreads();
+  }
+
+  // the exact tile back, into the other copy of the state
+  float* dst0 = TE ? b.E[0] : b.E[2];
+  float* dst1 = TE ? b.E[1] : b.H[0];
+  float* dst2 = TE ? b.H[2] : b.H[1];
+  float* pdst[4] = {b.psi[0][TE ? 0 : 2][1], b.psi[0][TE ? 1 : 2][0], b.psi[1][TE ? 2 : 0][1],
+                    b.psi[1][TE ? 2 : 1][0]};
+  const bool col_own = col_in && lx >= T && lx < T + OW;
+#pragma unroll
+  for (int r = 0; r < kTbRows; r++) {
+    const int ly = threadIdx.y + kTbTy * r, gy = y0 + ly, l = ly * kTbW + lx;
+    if (!(col_own && ly >= T && ly < T + OH && gy >= 0 && gy < ny)) continue;
+    const long long c = gy * pitch + gx;
+    dst0[c] = F[l];
+    dst1[c] = F[N + l];
+    dst2[c] = F[2 * N + l];
+    if (gy >= 1 && gy <= ny - 2) {
+      const int sj = a.pml_axis[1] ? slab_index(a.slab[1], gy) : -1;
+      if (sj >= 0) {
+        pdst[0][sj * pitch + gx] = PS[l];
+        pdst[2][sj * pitch + gx] = PS[2 * N + l];
+      }
+      if (sx4 >= 0) {
+        const long long pi = gy * static_cast<long long>(a.slab[0].W4) + sx4 + (gx & 3);
+        pdst[1][pi] = PS[N + l];
+        pdst[3][pi] = PS[3 * N + l];
+      }
+    }
+  }
+  // the soft sources' last values, by the tile that holds the source cell
+  if (tid == 0) {
+    for (int k = 0; k < nsl; k++) {
+      const int sl = srcs[k].lx, sly = srcs[k].ly;
+      if (sl < T || sl >= T + OW || sly < T || sly >= T + OH) continue;
+      const SourceDev& sr = a.src[srcs[k].q];
+      if (sr.target == 0 || sr.target == 2) b.src_last[srcs[k].q] = src_value(sr, t0 + T - 1);
+    }
+  }
+}
+
+template <int MODE, int T>
+static int tb_launch(const FusedArgs* rd, const FusedArgs* wr, const unsigned* items, int nitems, int s,
+                     cudaStream_t st) {
+  constexpr size_t smem = 8 * kTbW * kTbH * sizeof(float);
+  auto fn = batch_tb_kernel<MODE, T>;
+  // the largest shared-memory split: three 65 KB windows per SM
+  once_per_device(reinterpret_cast<const void*>(fn), [&] {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  });
+  fn<<<nitems, dim3(kTbW, kTbTy), smem, st>>>(rd, wr, items, s);
+  return 1;
+}
+
 template <int MODE, int MAXP, int ROWS>
 static void* batch_fn() {
   return reinterpret_cast<void*>(batch_kernel<MODE, MAXP, ROWS>);
@@ -393,6 +714,25 @@ void* batch_phase_ptr(int mode, int maxp, int rows, int phase) {
   FDTD_PHASE_POLES(kTM)
 #undef FDTD_PHASE_POLES
 #undef FDTD_PHASE_ROWS
+}
+
+int batch_tb_tile(int depth, int* tw, int* th) {
+  if (depth < 1 || 2 * depth >= kTbH) return 0;
+  *tw = kTbW - 2 * depth;
+  *th = kTbH - 2 * depth;
+  return 1;
+}
+
+int launch_batch_tb(int mode, int depth, const FusedArgs* rd, const FusedArgs* wr, const unsigned* items,
+                    int nitems, int s, cudaStream_t st) {
+  if (nitems <= 0) return 0;
+  const bool te = mode == kTE;
+  switch (depth) {
+    case 2: return te ? tb_launch<kTE, 2>(rd, wr, items, nitems, s, st) : tb_launch<kTM, 2>(rd, wr, items, nitems, s, st);
+    case 3: return te ? tb_launch<kTE, 3>(rd, wr, items, nitems, s, st) : tb_launch<kTM, 3>(rd, wr, items, nitems, s, st);
+    case 4: return te ? tb_launch<kTE, 4>(rd, wr, items, nitems, s, st) : tb_launch<kTM, 4>(rd, wr, items, nitems, s, st);
+    default: return 0;
+  }
 }
 
 void* batch_kernel_ptr(int mode, int maxp, int rows) {

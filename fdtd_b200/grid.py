@@ -35,7 +35,8 @@ EXPORTS = ["fdtd_grid_create", "fdtd_grid_destroy", "fdtd_set_pml", "fdtd_set_pm
            "fdtd_dft_npoints", "fdtd_dft_read", "fdtd_read_quantity", "fdtd_step", "fdtd_prepare", "fdtd_step_static_scratch", "fdtd_step_half", "fdtd_step_half_part", "fdtd_copy_plane", "fdtd_copy_plane_between", "fdtd_material_explicit", "fdtd_profile_step", "fdtd_set_sweep_kernel", "fdtd_use_graphs", "fdtd_error_flags", "fdtd_synchronize", "fdtd_download", "fdtd_upload",
            "fdtd_check_finite", "fdtd_field_error", "fdtd_get_step", "fdtd_launch_count", "fdtd_memory_bytes",
            "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_tune", "fdtd_batch_configure", "fdtd_batch_step",
-           "fdtd_batch_info", "fdtd_batch_item_rows", "fdtd_batch_set_item_rows",
+           "fdtd_batch_info", "fdtd_batch_item_rows", "fdtd_batch_set_item_rows", "fdtd_batch_set_temporal",
+           "fdtd_batch_temporal",
            "fdtd_batch_error_flags", "fdtd_adjoint_create", "fdtd_adjoint_forward", "fdtd_adjoint_backward",
            "fdtd_adjoint_destroy", "fdtd_last_error_string"]
 
@@ -116,6 +117,8 @@ def load_library(path: str = LIB_PATH):
         "fdtd_batch_item_rows": [vp, ip, ip, ctypes.POINTER(ctypes.c_float)],
         "fdtd_batch_set_item_rows": [vp, ip],
         "fdtd_batch_configure": [vp, i, i],
+        "fdtd_batch_set_temporal": [vp, i],
+        "fdtd_batch_temporal": [vp, ip, ctypes.POINTER(ctypes.c_float)],
         "fdtd_batch_error_flags": [vp, ip],
         "fdtd_adjoint_create": [vp, ip, ip, ctypes.c_double, ip, ip, i, ctypes.POINTER(vp)],
         "fdtd_adjoint_forward": [vp, i, dp],
@@ -476,6 +479,18 @@ class Batch:
 
     def set_item_rows(self, rows_per_grid) -> None:
         _check(load_library().fdtd_batch_set_item_rows(self.h, _ip(rows_per_grid)))
+
+    def set_temporal(self, depth: int) -> None:
+        """Temporal blocking: `depth` (2, 3 or 4) steps per launch from shared
+        memory, or 0 for off (fdtd_batch_set_temporal)."""
+        _check(load_library().fdtd_batch_set_temporal(self.h, int(depth)))
+
+    def temporal(self) -> dict:
+        """The temporal-blocking depth in use (0: off) and the tuner's ms per
+        step with depths 2, 3 and 4 (0: not timed)."""
+        d, ms = ctypes.c_int(), (ctypes.c_float * 3)()
+        _check(load_library().fdtd_batch_temporal(self.h, ctypes.byref(d), ms))
+        return {"depth": d.value, "tune_ms_per_step": {str(k): float(m) for k, m in zip((2, 3, 4), ms)}}
 
     def error_flags(self) -> int:
         v = ctypes.c_int()

@@ -359,7 +359,7 @@ int fdtd_batch_destroy(fdtd_batch* b);
 int fdtd_batch_tune(fdtd_batch* b, int steps);
 /* Choose the launch mode (1: persistent, 0: one kernel per half step) and
  * the tile height (1, 2, 4 or 8) without tuning; every grid's work items are
- * one tile high. */
+ * one tile high; temporal blocking off. */
 int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows);
 /* Per grid of the batch (in creation order): the rows of its work items and
  * its size class (0 = the quarter of the grids with the fewest cells .. 3);
@@ -369,6 +369,20 @@ int fdtd_batch_item_rows(fdtd_batch* b, int* rows_per_grid, int* size_class, flo
 /* Set the work-item rows of every grid (in creation order): the tile height
  * in use times 1, 2, 4 or 8. The tuner's choice, by hand. */
 int fdtd_batch_set_item_rows(fdtd_batch* b, const int* rows_per_grid);
+/* Temporal blocking: each launch advances every grid `depth` steps (2, 3 or
+ * 4) from shared memory, reading one copy of the state and writing a second
+ * one that the batch allocates (the grids' fields, CPML integrators and
+ * source values, once more); launches come in pairs, so the state ends in the
+ * grids' own arrays, and the steps of a call beyond whole pairs run one kernel
+ * per half step. Results equal the other launch modes bit for bit. Grids
+ * without dispersive materials whose sources lie inside their interiors
+ * (FDTD_ERR_UNSUPPORTED otherwise); 0 turns it off. fdtd_batch_configure turns
+ * it off too; fdtd_batch_tune also times depths 2, 3 and 4 and keeps one if
+ * it is faster. */
+int fdtd_batch_set_temporal(fdtd_batch* b, int depth);
+/* The depth in use (0: off) and the tuner's ms per step with depths 2, 3, 4
+ * (tuned_ms[3]; 0 if not timed). Either pointer may be NULL. */
+int fdtd_batch_temporal(fdtd_batch* b, int* depth, float* tuned_ms);
 int fdtd_batch_step(fdtd_batch* b, int nsteps, void* stream);
 /* Tile height in use, CTAs per launch, work items, the launch mode (1:
  * persistent, 0: per half step), and the tuner's ms per step (tune_ms[8]:

@@ -171,3 +171,108 @@ def test_batch_of_one_matches_the_single_grid(fdtd, which):
     E, H, _, _ = mode_fields(p.mode)
     for n in E + H:
         assert rel_l2(g.get(n), a.get(n)) <= 1e-6, n
+
+
+def small_tm_dielectric_batch(steps=50):
+    """TM grids without poles: dielectric blocks, an eps map on one grid,
+    sources of all four targets, CPML on some faces only."""
+    import scenarios
+    rng = np.random.default_rng(11)
+    dt = P.courant_dt(1e-6, 0.99 / np.sqrt(2.0))
+    out = []
+    for q in range(3):
+        nx, ny = (int(v) for v in rng.integers(40, 150, size=2))
+        p = P.Problem(P.TM, (nx, ny, 1), 1e-6, dt, name=f"tmd{q}")
+        for a in (0, 1):
+            for s in (0, 1):
+                if not (q == 1 and s == 1):
+                    p.pml[(a, s)] = 5 + q
+        p.materials = [P.Material.vacuum(), P.Material.constant(4.0), P.Material.constant(2.5)]
+        ids = np.zeros((1, ny, nx), np.uint8)
+        ids[0, 12:24, 10:21] = 1
+        ids[0, ny - 20:ny - 9, nx - 23:nx - 12] = 2
+        p.ids = ids
+        p.sources += [P.Source(2, (nx // 2, ny // 2, 0), P.gaussian_pulse(steps, 20, 6), "E"),
+                      P.Source(0, (nx // 3, ny // 3, 0), 1e-3 * P.gaussian_pulse(steps, 25, 6), "H"),
+                      P.Source(2, (2 * nx // 3, ny // 4, 0), 1e-12 * P.gaussian_pulse(steps, 15, 5), "D"),
+                      P.Source(1, (nx // 4, 2 * ny // 3, 0), 1e-9 * P.gaussian_pulse(steps, 18, 5), "B"),
+                      P.Source(2, (nx // 2, ny // 2, 0), 0.5 * P.gaussian_pulse(steps, 30, 6), "E")]
+        p.steps = steps
+        out.append(p)
+    tm, _ = scenarios.tm_adjoint_small(n=56, steps=steps)
+    tm.sources = [P.Source(2, (9, 20, 0), P.sinusoid(steps, 0.05), "E")]
+    out.append(tm)
+    return out
+
+
+@pytest.mark.parametrize("make", [small_te_batch, small_tm_dielectric_batch], ids=["te", "tm"])
+@pytest.mark.parametrize("depth", [2, 3, 4])
+def test_batch_temporal_blocking_matches_per_phase(fdtd, make, depth):
+    """Temporal blocking (depth steps per launch from shared memory, the
+    windows reading one copy of the state and writing the other) gives the
+    per-half-step launches' fields bit for bit, over calls that end inside a
+    pair of launches and calls of whole pairs."""
+    probs = make()
+    E, H, _, _ = mode_fields(probs[0].mode)
+    out = []
+    for tb in (0, depth):
+        grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+        b = fdtd.Batch(grids)
+        b.configure(False, 2)
+        if tb:
+            b.set_temporal(tb)
+            assert b.temporal()["depth"] == tb
+        b.step(7)
+        b.step(4 * depth)
+        b.step(probs[0].steps - 7 - 4 * depth)
+        assert b.error_flags() == 0
+        assert all(g.step_count == probs[0].steps for g in grids)
+        out.append([g.get(n) for g in grids for n in E + H])
+        b.close()
+    for q, (a, c) in enumerate(zip(*out)):
+        assert np.array_equal(a, c), (q, float(np.abs(a - c).max()))
+
+
+def test_batch_temporal_blocking_matches_oracle(fdtd, oracle):
+    probs = small_tm_dielectric_batch(60)
+    grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+    b = fdtd.Batch(grids)
+    b.set_temporal(3)
+    b.step(60)
+    for p, g in zip(probs, grids):
+        o = oracle.run_oracle(p)
+        E, H, _, _ = mode_fields(p.mode)
+        for n in E + H:
+            r = rel_l2(g.get(n), o.get(n))
+            assert r <= 1e-4, (p.name, n, r)
+
+
+def test_batch_temporal_blocking_refusals(fdtd):
+    grids = [fdtd.Grid.from_problem(p, "f32") for p in small_tm_batch(10)]
+    b = fdtd.Batch(grids)
+    with pytest.raises(fdtd.FdtdError):
+        b.set_temporal(2)  # dispersive materials
+    b = fdtd.Batch([fdtd.Grid.from_problem(small_te_batch(10)[0], "f32")])
+    for bad in (1, 5, -1):
+        with pytest.raises(fdtd.FdtdError):
+            b.set_temporal(bad)
+    b.set_temporal(4)
+    b.configure(False, 2)
+    assert b.temporal()["depth"] == 0
+
+
+def test_batch_tuner_times_temporal_blocking(fdtd):
+    probs = small_te_batch(48)
+    out = []
+    for tune in (False, True):
+        grids = [fdtd.Grid.from_problem(p, "f32") for p in probs]
+        b = fdtd.Batch(grids)
+        if tune:
+            b.tune(6)
+            tm = b.temporal()
+            assert all(v > 0 for v in tm["tune_ms_per_step"].values())
+            assert tm["depth"] in (0, 2, 3, 4)
+        b.step(48)
+        out.append([g.get("Hz") for g in grids])
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
