@@ -355,6 +355,8 @@ int fdtd_batch_destroy(fdtd_batch* b);
  * of 128 cells) for `steps` steps on a snapshot of the grids' state; then,
  * for the fastest, each size class of grids (quartiles of the cell counts,
  * largest first) in turn with work items 1, 2, 4 or 8 times that height;
+ * then temporal blocking with 2, 3 and 4 steps per launch where the grids
+ * allow it (which lays out the second copy of the state that mode needs);
  * restores the state and keeps the fastest. */
 int fdtd_batch_tune(fdtd_batch* b, int steps);
 /* Choose the launch mode (1: persistent, 0: one kernel per half step) and
