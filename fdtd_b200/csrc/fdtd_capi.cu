@@ -2211,6 +2211,18 @@ int tb_prepare(fdtd_batch* b) {
   return FDTD_OK;
 }
 
+// frees the second copy of the state and the tiles (temporal blocking off)
+void tb_release(fdtd_batch* b) {
+  cudaFree(b->d_args_b);
+  cudaFree(b->d_tb_items);
+  for (void* p : b->tb_bufs) cudaFree(p);
+  b->d_args_b = nullptr;
+  b->d_tb_items = nullptr;
+  b->n_tb_items = 0;
+  b->tb_bufs.clear();
+  b->tb = 0;
+}
+
 // the tiles of the temporally blocked launches of depth `depth`
 int tb_items(fdtd_batch* b, int depth) {
   int tw = 0, th = 0;
@@ -2360,9 +2372,7 @@ int fdtd_batch_destroy(fdtd_batch* b) try {
   cudaFree(b->d_ctrls);
   cudaFree(b->d_ctl);
   cudaFree(b->d_items);
-  cudaFree(b->d_args_b);
-  cudaFree(b->d_tb_items);
-  for (void* p : b->tb_bufs) cudaFree(p);
+  tb_release(b);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return FDTD_OK;
@@ -2484,6 +2494,8 @@ int fdtd_batch_tune(fdtd_batch* b, int steps) try {
     b->tb = 0;
     if (!rc && best_tb) rc = tb_items(b, best_tb);
   }
+  CK(cudaStreamSynchronize(b->stream));
+  if (!best_tb) tb_release(b);  // the second copy is kept only while in use
   if (!rc) b->tb = best_tb;
   b->tune_best_ms = best_step;
   CK(cudaStreamSynchronize(b->stream));
@@ -2516,6 +2528,7 @@ int fdtd_batch_set_temporal(fdtd_batch* b, int depth) try {
   }
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  if (depth == 0) tb_release(b);
   b->tb = depth;
   return FDTD_OK;
 } catch (...) {
@@ -2539,7 +2552,7 @@ int fdtd_batch_configure(fdtd_batch* b, int persistent, int rows) try {
   CK(cudaStreamSynchronize(b->stream));
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  b->tb = 0;
+  tb_release(b);
   b->persistent = persistent ? 1 : 0;
   b->mult.assign(b->grids.size(), 1);
   return batch_items(b, rows);
