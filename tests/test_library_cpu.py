@@ -44,3 +44,15 @@ def test_create_without_gpu_fails_loudly(fdtd):
     with pytest.raises(fdtd.FdtdError) as e:
         fdtd.Grid(TM, (8, 8, 1), 1e-6, 1e-15)
     assert e.value.code == -2
+
+
+def test_batch_calls_check_their_handle_before_any_device_call(fdtd):
+    """The batch entry points refuse a null handle (FDTD_ERR_INVALID) without
+    touching a device, so they behave the same on a host with no GPU."""
+    lib = fdtd.load_library()
+    assert lib.fdtd_batch_set_temporal(None, 2) == -1
+    assert lib.fdtd_batch_temporal(None, None, None) == -1
+    assert lib.fdtd_batch_tune(None, 4) == -1
+    assert lib.fdtd_batch_configure(None, 0, 2) == -1
+    assert lib.fdtd_batch_step(None, 1, None) == -1
+    assert lib.fdtd_batch_destroy(None) == 0
