@@ -2176,41 +2176,6 @@ const char* tb_unsupported(const fdtd_batch* b) {
   return nullptr;
 }
 
-// The second copy of every array a step changes (fields, CPML integrators,
-// the soft sources' last values) and the grids' arguments pointing at it;
-// laid out once, a copy of the current state.
-int tb_prepare(fdtd_batch* b) {
-  if (b->d_args_b) return FDTD_OK;
-  CK(cudaDeviceSynchronize());
-  std::vector<FusedArgs> args = b->h_args;
-  for (size_t q = 0; q < b->grids.size(); q++) {
-    fdtd_grid* g = b->grids[q];
-    FusedArgs& a = args[q];
-    auto twin = [&](void* p) -> void* {
-      if (!g->sizes.count(p)) return nullptr;
-      void* d = nullptr;
-      if (cudaMalloc(&d, g->sizes[p]) != cudaSuccess) return nullptr;
-      b->tb_bufs.push_back(d);
-      if (cudaMemcpy(d, p, g->sizes[p], cudaMemcpyDeviceToDevice) != cudaSuccess) return nullptr;
-      return d;
-    };
-    for (int c = 0; c < 3; c++) {
-      if (g->E[c] && !(a.E[c] = static_cast<float*>(twin(g->E[c])))) return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
-      if (g->H[c] && !(a.H[c] = static_cast<float*>(twin(g->H[c])))) return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
-    }
-    for (int ft = 0; ft < 2; ft++)
-      for (int I = 0; I < 3; I++)
-        for (int J = 0; J < 3; J++)
-          if (g->psi[ft][I][J] && !(a.psi[ft][I][J] = static_cast<float*>(twin(g->psi[ft][I][J]))))
-            return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
-    if (g->d_src_last && !(a.src_last = static_cast<double*>(twin(g->d_src_last))))
-      return fail(FDTD_ERR_CUDA, "temporal blocking: out of memory");
-  }
-  CK(cudaMalloc(&b->d_args_b, args.size() * sizeof(FusedArgs)));
-  CK(cudaMemcpy(b->d_args_b, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice));
-  return FDTD_OK;
-}
-
 // frees the second copy of the state and the tiles (temporal blocking off)
 void tb_release(fdtd_batch* b) {
   cudaFree(b->d_args_b);
@@ -2221,6 +2186,47 @@ void tb_release(fdtd_batch* b) {
   b->n_tb_items = 0;
   b->tb_bufs.clear();
   b->tb = 0;
+}
+
+// The second copy of every array a step changes (fields, CPML integrators,
+// the soft sources' last values) and the grids' arguments pointing at it;
+// laid out once, a copy of the current state. On failure nothing is kept.
+int tb_prepare(fdtd_batch* b) {
+  if (b->d_args_b) return FDTD_OK;
+  CK(cudaDeviceSynchronize());
+  std::vector<FusedArgs> args = b->h_args;
+  bool ok = true;
+  for (size_t q = 0; q < b->grids.size() && ok; q++) {
+    fdtd_grid* g = b->grids[q];
+    FusedArgs& a = args[q];
+    // a same-sized copy of the state array p (null if p is not one)
+    auto twin = [&](void* p) -> void* {
+      if (!g->sizes.count(p)) return nullptr;
+      void* d = nullptr;
+      if (cudaMalloc(&d, g->sizes[p]) != cudaSuccess) return nullptr;
+      b->tb_bufs.push_back(d);
+      if (cudaMemcpy(d, p, g->sizes[p], cudaMemcpyDeviceToDevice) != cudaSuccess) return nullptr;
+      return d;
+    };
+    for (int c = 0; c < 3 && ok; c++) {
+      if (g->E[c]) ok = ok && (a.E[c] = static_cast<float*>(twin(g->E[c])));
+      if (g->H[c]) ok = ok && (a.H[c] = static_cast<float*>(twin(g->H[c])));
+    }
+    for (int ft = 0; ft < 2; ft++)
+      for (int I = 0; I < 3; I++)
+        for (int J = 0; J < 3; J++)
+          if (g->psi[ft][I][J]) ok = ok && (a.psi[ft][I][J] = static_cast<float*>(twin(g->psi[ft][I][J])));
+    if (g->d_src_last) ok = ok && (a.src_last = static_cast<double*>(twin(g->d_src_last)));
+  }
+  if (ok) ok = cudaMalloc(&b->d_args_b, args.size() * sizeof(FusedArgs)) == cudaSuccess;
+  if (ok)
+    ok = cudaMemcpy(b->d_args_b, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    const cudaError_t e = cudaGetLastError();
+    tb_release(b);
+    return fail(FDTD_ERR_CUDA, std::string("temporal blocking: the second copy of the state: ") + cudaGetErrorString(e));
+  }
+  return FDTD_OK;
 }
 
 // the tiles of the temporally blocked launches of depth `depth`
