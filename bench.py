@@ -92,6 +92,8 @@ def parse():
     ap.add_argument("--batch-mode", default="tune", choices=["tune", "persistent", "per_phase"],
                     help="batch64: autotune, or force a launch mode (with --batch-rows)")
     ap.add_argument("--batch-rows", type=int, default=4, choices=[1, 2, 4, 8])
+    ap.add_argument("--batch-temporal", type=int, default=0, choices=[0, 2, 3, 4],
+                    help="batch64 with a forced launch mode: steps per launch of temporal blocking (0: off)")
     ap.add_argument("--decompose", default="replicas", choices=["replicas", "zslab"],
                     help="single-grid workloads on N GPUs: independent replicas (weak scaling), or one grid cut "
                          "into z slabs, one per rank, ghost planes over NCCL overlapped with the interior sweep "
@@ -566,6 +568,8 @@ def run_batch(args, torch, world, rank, local, stream):
         batch.tune(4)
     else:
         batch.configure(args.batch_mode, args.batch_rows)
+        if args.batch_temporal:
+            batch.set_temporal(args.batch_temporal)
     batch.step(args.warmup, stream=stream.cuda_stream)
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
